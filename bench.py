@@ -1,0 +1,284 @@
+"""Benchmark: 3D cell-steps/s of the reference's baroclinic time step on one B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--config basin4] [--precision fp32|fp64]
+
+Workload (default): basin4 = Lm=2048, Mm=1024, N=50 (104,857,600 interior cells), dx=1 km,
+tanh shelf + two seamounts, dt=120 s, ndtfast=40 (nfast+1 barotropic substeps per step),
+closed walls, the reference's step semantics (main3d.py:118-324), starting from rest.
+One "step" is one baroclinic step including its barotropic loop.  Inputs are larger than
+L2 (each 3D field is ~0.43 GB in FP32), so no L2 flush is needed between steps.
+
+Multi-GPU (torchrun): the basin does not shard in the reference, so every rank runs an
+independent replica (weak scaling); value = all ranks' cell-steps / max-over-ranks time.
+
+--impl reference times the reference's own kernels (host-compiled, oracle/_ref) driven in
+its main3d order with OpenMP over the host cores, on a bounded sample of the same basin.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+MEASURED = os.path.join(ROOT, "MEASURED_PEAKS.json")
+METRIC = "3D cell-steps/s"
+
+
+def peaks():
+    try:
+        with open(MEASURED) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# -------------------------------------------------------------------------------------------
+# CPU (reference) measurement
+# -------------------------------------------------------------------------------------------
+def reference_cpu(config, nsteps, omp):
+    """The reference's kernels on the host; returns (cell-steps/s, cores, sample text)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    import ref_driver
+    from sailfish_b200 import configs, host
+    if not ref_driver.available():
+        raise RuntimeError("oracle/_ref is not built")
+    full = configs.CONFIGS[config]()
+    g = full["grid"]
+    # bounded sample: the same recipe on a quarter-by-quarter sub-basin (same N, dx, dt)
+    sub = configs.basin(max(g.L - 1, 8) // 8, max(g.M - 1, 8) // 8, g.N, g.pm.flat[0] ** -1,
+                        [(1.0 / 3.0, 0.6), (2.0 / 3.0, 0.6)], full["dt"], full["ndtfast"])
+    sg, B = sub["grid"], sub["boundary"]
+    og = orc.Grid(sg.L, sg.M, sg.N, sg.h, sg.pm, sg.pn, sg.on_u, sg.om_v, sg.fomn, sg.sc_r, sg.sc_w,
+                  sg.Cs_r, sg.Cs_w, sg.hc, sg.Vtransform)
+    bd = {}
+    for name in ("zetaBC", "ubarBC", "vbarBC", "uvelBC", "vvelBC"):
+        bc = getattr(B, name)
+        for fld in ("bcIdx", "bcIdx1", "bcIdx2", "bcIdxFieldIdx2", "bcIdxFieldType", "LBC"):
+            bd["%s_%s" % (name, fld)] = getattr(bc, fld)
+    for fld in ("zetaClosedOrGradientBCIdx1", "zetaClosedOrGradientBCIdx2", "zetaClampedBCIdx1",
+                "ubarClosedBCIdx1", "vbarClosedBCIdx1", "ubarClampedBCIdx1", "vbarClampedBCIdx1",
+                "ubarGradientBCIdx1", "ubarGradientBCIdx2", "vbarGradientBCIdx1", "vbarGradientBCIdx2"):
+        bd[fld] = getattr(B, fld)
+    O = orc.Ocean(og)
+    nfast, w1, w2 = host.set_weights(sub["ndtfast"])
+    ct = orc.CompTimes(sub["dt"], sub["ndtfast"], nfast, w1, w2)
+    ref_driver.main3d(og, orc.Boundary(bd), O, ct, 1, omp=omp)      # warm-up
+    t0 = time.perf_counter()
+    ref_driver.main3d(og, orc.Boundary(bd), O, ct, nsteps, omp=omp)
+    dt = time.perf_counter() - t0
+    cells = (sg.L - 1) * (sg.M - 1) * sg.N
+    sample = ("reference kernels (oracle/_ref, g++ -O2) in main3d order on a %dx%dx%d sub-basin of "
+              "%s (same recipe, dt, ndtfast), %d baroclinic steps, %d OpenMP threads"
+              % (sg.L - 1, sg.M - 1, sg.N, config, nsteps, omp))
+    return cells * nsteps / dt, omp, sample
+
+
+# -------------------------------------------------------------------------------------------
+# clocks during the timed region
+# -------------------------------------------------------------------------------------------
+class Clocks:
+    Q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index, self.rows, self.proc = index, [], None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm = [float(r[0]) for r in self.rows if len(r) >= 6 and r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if len(r) >= 6 and r[1].replace(".", "").isdigit()]
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({names[k] for r in self.rows if len(r) >= 6 for k in range(4)
+                          if r[2 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(sm)}
+
+
+# -------------------------------------------------------------------------------------------
+def algorithmic_bytes(grid, esize):
+    """Compulsory DRAM bytes per launch of each single-kernel phase: every distinct array read
+    once and written once at its stored precision (levels x rho points)."""
+    s2, N = grid.s2, grid.N
+    return {
+        "k_rhs3d": esize * (6 * N + 2 * (N + 1)) * s2,          # u,v,Huon,Hvom,W,Hz -> ru,rv
+        "k_step3d_uv": esize * (9 * N) * s2 + 16 * s2,          # u,v,ru,rv,Hz,Akv,z_r -> u,v; DU,DV
+        "k_maxflux_omega": esize * (4 * N + 3 * (N + 1)) * s2,  # u,v,Hz,z_w -> Huon,Hvom,W
+        "k_set_depth": esize * (3 * N + 1) * s2 + 16 * s2,      # Zt,h -> z_w,z_r,Hz
+    }
+
+
+def run_ours(args, rank, world):
+    import torch
+    from sailfish_b200 import configs
+    from sailfish_b200.model import Model
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    cfg = configs.CONFIGS[args.config]()
+    grid = cfg["grid"]
+    m = Model(grid, cfg["boundary"], cfg["dt"], cfg["ndtfast"], precision=args.precision)
+    esize = 4 if args.precision == "fp32" else 8
+    cells = (grid.L - 1) * (grid.M - 1) * grid.N
+    stream = torch.cuda.current_stream()
+
+    phases = {}
+
+    def hook(name):
+        ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+        phases.setdefault(name, []).append(ev)
+        return ev
+
+    m.step(args.warmup)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(torch.cuda.current_device()) as clk:
+        start.record(stream)
+        m.step(args.steps, timer=hook)
+        stop.record(stream)
+        torch.cuda.synchronize()
+    ms = start.elapsed_time(stop)
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+        torch.distributed.barrier()
+    per_phase = {k: float(np.mean([a.elapsed_time(b) for a, b in v])) for k, v in phases.items()}
+
+    # end to end: host state in pinned memory, H2D of the step's prognostic 3D inputs (u, v)
+    # and D2H of its surface elevation result, through the same public Model API
+    hu = torch.empty_like(m.u, device="cpu").pin_memory()
+    hv = torch.empty_like(m.v, device="cpu").pin_memory()
+    hz = torch.empty_like(m.zeta[0], device="cpu").pin_memory()
+    hu.copy_(m.u)
+    hv.copy_(m.v)
+    e_start, e_stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e_steps = max(1, min(args.steps, 3))
+    torch.cuda.synchronize()
+    e_start.record(stream)
+    for _ in range(e_steps):
+        m.u.copy_(hu, non_blocking=True)
+        m.v.copy_(hv, non_blocking=True)
+        m.step(1)
+        hz.copy_(m._slot("zeta", 2), non_blocking=True)
+    e_stop.record(stream)
+    torch.cuda.synchronize()
+    e_ms = e_start.elapsed_time(e_stop) / e_steps
+    bi = (hu.numel() + hv.numel()) * hu.element_size()
+    bo = hz.numel() * hz.element_size()
+
+    ab = algorithmic_bytes(grid, esize)
+    dom = max((k for k in per_phase if k in ab), key=lambda k: per_phase[k])
+    peak, kind = peaks()
+    achieved = ab[dom] / (per_phase[dom] * 1e-3) / 1e9
+    value = cells * args.steps * world / (ms * 1e-3)
+    n_launch_2d = 5 * (m.nfast + 1) + 3 * (m.nfast + 1) + 2
+    out = {
+        "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32" if args.precision == "fp32" else "f64", "data": "synthetic",
+        "config": {"workload": args.config, "Lm": grid.L - 1, "Mm": grid.M - 1, "N": grid.N,
+                   "cells": cells, "dt": m.dt, "ndtfast": m.ndtfast,
+                   "barotropic_substeps": m.nfast + 1, "semantics": "reference main3d",
+                   "initial_state": "rest, closed walls",
+                   "l2": "inputs larger than L2 (each 3D field %.2f GB)" % (m.u.numel() * esize / 1e9),
+                   "parallelism": "replicas" if world > 1 else "single"},
+        "phases_ms": per_phase,
+        "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "peak_kind": kind,
+                     "algorithmic_bytes": ab[dom], "traffic": None},
+        "e2e": {"value": cells / (e_ms * 1e-3), "unit": "cell-steps/s",
+                "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo},
+        "gpu_launches": args.steps * (4 + n_launch_2d),
+        "clocks": clk.summary(),
+    }
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="basin4")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    omp = len(os.sched_getaffinity(0))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        try:
+            v, cores, sample = reference_cpu(args.config, max(args.steps, 1), omp)
+        except Exception as e:
+            print(json.dumps({"impl": "reference", "unavailable": str(e)}))
+            return
+        print(json.dumps({
+            "impl": "reference", "metric": METRIC, "value": v, "unit": "cell-steps/s",
+            "n_gpus": 0, "steps": args.steps, "warmup": 1, "higher_is_better": True,
+            "dtype": "f64", "data": "synthetic", "config": {"workload": args.config},
+            "cpu_baseline": {"value": v, "unit": "cell-steps/s", "cores": cores,
+                             "kind": "reference", "sample": sample},
+            "e2e": {"value": v, "unit": "cell-steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}))
+        return
+
+    import torch
+    if world > 1:
+        torch.distributed.init_process_group(
+            "nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    out = run_ours(args, rank, world)
+    if rank == 0:
+        if not args.no_cpu_baseline:
+            try:
+                v, cores, sample = reference_cpu(args.config, args.cpu_steps, omp)
+                out["cpu_baseline"] = {"value": v, "unit": "cell-steps/s", "cores": cores,
+                                       "kind": "reference", "sample": sample}
+            except Exception as e:
+                out["cpu_baseline"] = {"value": None, "unavailable": str(e)}
+        print(json.dumps(out))
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,176 @@
+/*
+ * sailfish_b200.h -- C ABI of libsailfish_b200.so, the B200 (sm_100a) time-step library.
+ *
+ * Every entry point replaces one launch (or one Python routine) of the reference's time
+ * step and takes the same arrays, as raw device pointers in the reference's layout:
+ * flat C-order fields, 2D fields (M+1) x (L+1) (xi fastest), 3D fields N or N+1 levels of
+ * (M+1)*(L+1) points.  The element type of every state and metric array is the context's
+ * precision (SF_FP64: double, SF_FP32: float); the fast-time accumulators Zt_avg1, DU_avg1
+ * and DV_avg1 are double in both precisions.
+ *
+ * The reference keeps the grid in device globals set once by `initialize<<<1,1>>>`
+ * (modules/mod_cppkernels.h:154-171, bound per module in modules/mod_operators.py:31-45);
+ * here a context (sf_ctx) holds the same information plus the boundary programs.
+ *
+ * Conventions: 0 = SF_OK, negative = error (sf_last_error() describes the last one on the
+ * calling thread).  Calls are stream-ordered and asynchronous (no hidden synchronisation),
+ * buffers are caller-owned, per-context tables are context-owned.  A context is
+ * thread-compatible, not thread-safe.  No C++ exception crosses this boundary.
+ */
+#ifndef SAILFISH_B200_H
+#define SAILFISH_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct sf_ctx sf_ctx;
+typedef void *sf_stream; /* a cudaStream_t; NULL = legacy default stream */
+
+enum sf_status {
+    SF_OK = 0,
+    SF_EINVAL = -1,       /* bad size, pointer or argument */
+    SF_EDTYPE = -2,       /* unsupported precision */
+    SF_ECUDA = -3,        /* CUDA runtime error */
+    SF_ENONFINITE = -4,   /* non-finite value detected by a check */
+    SF_ETIMEOUT = -5,     /* a bounded device wait gave up */
+    SF_ENOMEM = -6,       /* device allocation failed */
+    SF_EUNSUPPORTED = -7  /* configuration the reference cannot run either */
+};
+
+enum sf_precision { SF_FP64 = 0, SF_FP32 = 1 };
+
+/* Grid, vertical coordinate and boundary description; all pointers are HOST pointers and
+ * are copied into the context by sf_ctx_create. */
+typedef struct sf_grid_desc {
+    int L, M, N;          /* rho points (M+1) x (L+1), N vertical levels (N >= 5) */
+    int precision;        /* enum sf_precision */
+    /* horizontal metrics, (M+1)*(L+1) doubles each (modules/mod_grid.py:197-243) */
+    const double *h, *pm, *pn, *on_u, *om_v, *fomn;
+    /* S-coordinate tables (nonlinear/set_coords.py:355-423): sc_r[N], sc_w[N+1], Cs_r[N],
+     * Cs_w[N+1]; critical depth hc and Vtransform (1 or 2) */
+    const double *sc_r, *sc_w, *Cs_r, *Cs_w;
+    double hc;
+    int Vtransform;
+    /* Boundary arrays built by Boundary (modules/mod_boundary.py:103-297), int32: */
+    const int32_t *zeta_field_idx2; /* zetaBC.bcIdxFieldIdx2, (M+1)*(L+1), >= 0 on the ring */
+    const int32_t *uvel_field_type; /* uvelBC.bcIdxFieldType, (M+1)*(L+1) */
+    const int32_t *vvel_field_type; /* vvelBC.bcIdxFieldType, (M+1)*(L+1) */
+    const int32_t *zeta_copy_idx1, *zeta_copy_idx2; int n_zeta_copy; /* zetaClosedOrGradientBCIdx1/2 */
+    const int32_t *ubar_closed_idx; int n_ubar_closed;                /* ubarClosedBCIdx1 */
+    const int32_t *vbar_closed_idx; int n_vbar_closed;                /* vbarClosedBCIdx1 */
+    const int32_t *ubar_clamped_idx; int n_ubar_clamped;              /* ubarClampedBCIdx1 */
+    const int32_t *ubar_grad_idx1, *ubar_grad_idx2; int n_ubar_grad;  /* ubarGradientBCIdx1/2 */
+    const int32_t *vbar_grad_idx1; int n_vbar_grad;                   /* vbarGradientBCIdx1 */
+} sf_grid_desc;
+
+/* Three time slots of the barotropic state, in (t0, t1, t2) order, as rotated by
+ * T_OCEAN.cycleTimes2D (modules/mod_ocean.py:120-154), plus the fast-time accumulators. */
+typedef struct sf_state2d {
+    void *zeta[3], *ubar[3], *vbar[3], *rzeta[3], *rubar[3], *rvbar[3];
+    double *Zt_avg1, *DU_avg1, *DV_avg1;
+} sf_state2d;
+
+/* ---- context ---------------------------------------------------------------------------
+ * sf_ctx_create replaces mod_operators.initModule (modules/mod_operators.py:31-45, which
+ * launches initialize, modules/mod_cppkernels.h:154-171) and the boundary index setup of
+ * Boundary.__init__ (modules/mod_boundary.py:237-297).  It uses the current CUDA device. */
+int sf_ctx_create(const sf_grid_desc *desc, sf_ctx **out);
+int sf_ctx_destroy(sf_ctx *ctx);
+const char *sf_last_error(void);
+int sf_version(void);
+int sf_ctx_precision(const sf_ctx *ctx);
+
+/* ---- barotropic (2D) kernels, modules/mod_cppkernels.cpp ------------------------------- */
+
+/* computeZetaRHS (mod_cppkernels.cpp:81-128).  cff1 = weight1[iif-1]; the accumulators are
+ * updated when is_predictor == 0. */
+int sf_zeta_rhs(sf_ctx *ctx, const void *zeta, const void *ubar, const void *vbar,
+                double *DU_avg1, double *DV_avg1, double *Zt_avg1, int is_predictor, double cff1,
+                void *rzeta, sf_stream stream);
+/* computeZetaPred (mod_cppkernels.cpp:134-150). */
+int sf_zeta_pred(sf_ctx *ctx, double Dt, const void *zeta_t0, void *zeta_t2, const void *rzeta_t1,
+                 sf_stream stream);
+/* computeMomentumRHSPred / computeMomentumRHSCorr (mod_cppkernels.cpp:13-77):
+ * gzeta = (1-weight)*za + weight*zb. */
+int sf_momentum_rhs(sf_ctx *ctx, void *rhs_ubar, void *rhs_vbar, const void *za, const void *zb,
+                    double g, double weight, sf_stream stream);
+/* computeMomentumPred (mod_cppkernels.cpp:156-186). */
+int sf_momentum_pred(sf_ctx *ctx, double Dt, const void *u_t1, void *u_t2, const void *v_t1,
+                     void *v_t2, const void *rhsu, const void *rhsv, const void *zeta_t1,
+                     const void *zeta_t2, sf_stream stream);
+/* AdamsMoultonCorr3rd (mod_cppkernels.cpp:191-209): v_t2 += Dt*(5/12 r2 + 8/12 r1 - 1/12 r0). */
+int sf_am3(sf_ctx *ctx, double Dt, void *v_t2, const void *r0, const void *r1, const void *r2,
+           sf_stream stream);
+/* zetabc (nonlinear/zetabc.py:5-12, copyBC of modules/mod_BC.c:16-23). */
+int sf_zetabc(sf_ctx *ctx, void *zeta, sf_stream stream);
+/* barotropicVelocityBC (nonlinear/barotropicVelocityBC.py:7-31, setBC/copyBC of
+ * modules/mod_BC.c:6-23); the clamped value is 0.05*sin(0.0002*time2D). */
+int sf_barotropic_velocity_bc(sf_ctx *ctx, void *ubar, void *vbar, double time2D, sf_stream stream);
+/* step2dPredictor (nonlinear/step2d.py:23-81): first_step selects its Forward-Euler branch. */
+int sf_step2d_predictor(sf_ctx *ctx, const sf_state2d *s, double dtfast, double time2D,
+                        int first_step, sf_stream stream);
+/* step2dCorrector (nonlinear/step2d.py:84-128), cff1 = weight1[iif-1]. */
+int sf_step2d_corrector(sf_ctx *ctx, const sf_state2d *s, double dtfast, double time2D,
+                        double cff1, sf_stream stream);
+
+/* One substep of main3d's barotropic loop (nonlinear/main3d.py:168-189) with the slots of s
+ * already rotated: step2dPredictor, step2dCorrector and vbar_t2[:] = 0 in five passes plus
+ * boundary programs.  The corrector's momentum right-hand side (rubar_t2/rvbar_t2,
+ * step2d.py:116) is overwritten by the next predictor before anything reads it, so it is
+ * evaluated only when `last` is set; every other value is the reference's. */
+int sf_barotropic_substep(sf_ctx *ctx, const sf_state2d *s, double dtfast, double time2D,
+                          double cff1, int last, sf_stream stream);
+/* The whole barotropic loop of one baroclinic step (nonlinear/main3d.py:166-189): nsub
+ * substeps (nfast+1), zeroing the accumulators before the first, rotating the slots of *s
+ * as cycleTimes2D does (the final order is written back into *s), with time2D advanced by
+ * dtfast per substep from *time2D (written back) and cff1 = weight1[iif-1] taken from the
+ * host array weight1. */
+int sf_barotropic_loop(sf_ctx *ctx, sf_state2d *s, int nsub, const double *weight1,
+                       double dtfast, double *time2D, sf_stream stream);
+
+/* ---- 3D right-hand side, nonlinear/rhs.py:16-93 + nonlinear/rhs_kernels.cpp ------------ */
+/* rhs3d: ru = rv = 0, addCoriolis (:7-35), horizontalAdvection (:71-132), verticalAdvection
+ * (:136-196), fused in one pass.  u, v, Huon, Hvom, W, ru, rv have N+1 levels, Hz has N. */
+int sf_rhs3d(sf_ctx *ctx, const void *u, const void *v, const void *Huon, const void *Hvom,
+             const void *W, const void *Hz, void *ru, void *rv, sf_stream stream);
+
+/* ---- 3D step kernels, nonlinear/step3D_uv.kernels.cpp ---------------------------------- */
+/* set_maxflux (:372-405). */
+int sf_set_maxflux(sf_ctx *ctx, const void *u, const void *v, void *Huon, void *Hvom,
+                   const void *Hz, sf_stream stream);
+/* omega (:62-165). */
+int sf_omega(sf_ctx *ctx, void *W, const void *Huon, const void *Hvom, const void *z_w,
+             sf_stream stream);
+/* set_maxflux + omega + set_zeta (:294-310) in one pass, as main3d launches them in a row
+ * (nonlinear/main3d.py:118-151).  zeta_t1/zeta_t2/Zt_avg1 may be NULL to skip set_zeta. */
+int sf_maxflux_omega(sf_ctx *ctx, const void *u, const void *v, void *Huon, void *Hvom,
+                     const void *Hz, void *W, const void *z_w, void *zeta_t1, void *zeta_t2,
+                     const double *Zt_avg1, sf_stream stream);
+/* set_zeta (:294-310). */
+int sf_set_zeta(sf_ctx *ctx, void *zeta1, void *zeta2, const double *Zt_avg1, sf_stream stream);
+/* set_depth (:225-291), evaluated in FP64 in both precisions. */
+int sf_set_depth(sf_ctx *ctx, const double *Zt_avg1, void *z_w, void *z_r, void *Hz,
+                 sf_stream stream);
+/* step3d_UV (:646-707) with its helpers (:408-639).  tmpU/tmpV are the pre-step velocities
+ * (nonlinear/main3d.py:298-299); NULL means "read u/v before overwriting them". */
+int sf_step3d_uv(sf_ctx *ctx, void *u, void *v, const void *ru, const void *rv, void *ubar_t1,
+                 void *vbar_t1, void *ubar_t2, void *vbar_t2, const void *Hz, const void *Akv,
+                 const void *z_r, const double *DU_avg1, const double *DV_avg1, const void *tmpU,
+                 const void *tmpV, int iic, int ntfirst, double lambda, double Dt,
+                 sf_stream stream);
+/* setLateralUVBCs (:314-368); the clamped value is 0.05*sin(0.0002*time). */
+int sf_lateral_uv_bc(sf_ctx *ctx, double time, void *u, void *v, sf_stream stream);
+/* step3d_UV followed by setLateralUVBCs in the same pass (nonlinear/main3d.py:304-311). */
+int sf_step3d_uv_bc(sf_ctx *ctx, void *u, void *v, const void *ru, const void *rv,
+                    void *ubar_t1, void *vbar_t1, void *ubar_t2, void *vbar_t2, const void *Hz,
+                    const void *Akv, const void *z_r, const double *DU_avg1,
+                    const double *DV_avg1, int iic, int ntfirst, double lambda, double Dt,
+                    double time, sf_stream stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SAILFISH_B200_H */

@@ -1,0 +1,163 @@
+"""The reference's own kernels (oracle/_ref, host-compiled by build_ref.py) driven in the
+order of its Python orchestration -- the reference's CPU path of the time step.
+
+TEST/BASELINE INFRASTRUCTURE: used by tests/ (to cross-check the oracle driver) and by
+bench.py's reference arm and CPU-baseline leg, never by the product.
+
+Launch geometry is the reference's (modules/mod_operators.py:40-41, utility/misc.py:10,17):
+grsz*bksz threads for most kernels and grsz*GPUMUL*(bksz/GPUMUL) for the "x GPUMUL"
+launches, which is the same count; boundary scatters use size/512+1 blocks of 512.
+With omp > 1 the thread loop of each kernel is split over OpenMP threads (timing only: the
+reference's own GPU launches are concurrent too, and the few kernels with races between
+threads, e.g. rhs_kernels.cpp:86-91, then resolve them in no fixed order).
+"""
+import ctypes
+import math
+import os
+
+import numpy as np
+
+from oracle import gzeros, P, D, Ii, G_GRAV
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF = os.path.join(HERE, "_ref")
+_vp, _d, _i, _u, _b, _l = (ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.c_uint,
+                           ctypes.c_bool, ctypes.c_long)
+SIGS = {
+    "2d": {"initialize": [_u, _u, _u] + [_vp] * 4,
+           "computeMomentumRHSPred": [_vp] * 5 + [_d, _d],
+           "computeMomentumRHSCorr": [_vp] * 6 + [_d],
+           "computeZetaRHS": [_vp] * 7 + [_b, _vp, _vp, _i, _vp],
+           "computeZetaPred": [_d] + [_vp] * 4,
+           "computeMomentumPred": [_d] + [_vp] * 9,
+           "AdamsMoultonCorr3rd": [_d] + [_vp] * 4},
+    "rhs": {"initialize": [_u, _u, _u] + [_vp] * 4,
+            "addCoriolis": [_vp] * 6, "horizontalAdvection": [_vp] * 7,
+            "verticalAdvection": [_vp] * 6},
+    "step3d": {"initialize": [_u, _u, _u] + [_vp] * 4, "setVerticalVelEq": [_vp] * 3,
+               "omega": [_vp] * 7, "set_depth": [_i] + [_vp] * 4 + [_d] + [_vp] * 5,
+               "set_zeta": [_vp] * 3, "setLateralUVBCs": [_d] + [_vp] * 6,
+               "set_maxflux": [_vp] * 5, "step3d_UV": [_vp] * 16 + [_i, _i, _d, _d, _d]},
+    "bc": {"setBC": [_vp, _vp, _u, _d], "copyBC": [_vp, _vp, _vp, _u]},
+}
+
+
+def available():
+    return all(os.path.exists(os.path.join(REF, "libsfref_%s.so" % m)) for m in SIGS)
+
+
+class RefKernels:
+    def __init__(self, omp=1):
+        self.omp = int(omp)
+        self.libs = {}
+        for mod, fns in SIGS.items():
+            lib = ctypes.CDLL(os.path.join(REF, "libsfref_%s.so" % mod))
+            for name, args in fns.items():
+                f = getattr(lib, "sfref_" + name)
+                f.argtypes = [_l, _i] + args
+                f.restype = None
+            self.libs[mod] = lib
+
+    def __call__(self, mod, name, nthreads, *args):
+        getattr(self.libs[mod], "sfref_" + name)(_l(nthreads), _i(self.omp), *args)
+
+
+def main3d(grid, B, O, ct, nsteps, omp=1, lam=1.0):
+    """nonlinear/main3d.py:25-326 with the reference's kernels (step2d.py, zetabc.py,
+    barotropicVelocityBC.py, rhs.py orchestration restated), on oracle.Grid/Ocean/CompTimes."""
+    K = RefKernels(omp)
+    N, J, I = grid.N, grid.J, grid.I
+    s2 = grid.s2
+    nt = (s2 // 512 + 1) * 512          # grsz*bksz and grsz*GPUMUL*(bksz//GPUMUL)
+    bcn = lambda n: (n // 512 + 1) * 512
+    args_init = (ctypes.c_uint(N), ctypes.c_uint(J), ctypes.c_uint(I), P(grid.on_u), P(grid.om_v),
+                 P(grid.pn), P(grid.pm))
+    for mod in ("2d", "rhs", "step3d"):
+        K(mod, "initialize", 1, *args_init)
+    eq = [gzeros((N + 1, J, I)) for _ in range(3)]
+    tmpU, tmpV = gzeros((N + 1) * J * I), gzeros((N + 1) * J * I)
+    BC = B["zetaBC_bcIdxFieldIdx2"]
+    K("step3d", "setVerticalVelEq", 1, P(eq[0]), P(eq[1]), P(eq[2]))
+
+    def set_depth():
+        K("step3d", "set_depth", nt, Ii(grid.Vtransform), P(O.Zt_avg1), P(grid.z_w), P(grid.z_r),
+          P(grid.h), D(grid.hc), P(grid.Hz), P(grid.sc_r), P(grid.sc_w), P(grid.Cs_r), P(grid.Cs_w))
+
+    def copy_bc(var, a1, a2, n):
+        K("bc", "copyBC", bcn(n), P(var), P(a1), P(a2), ctypes.c_uint(n))
+
+    def set_bc(var, a, val):
+        K("bc", "setBC", bcn(a.size), P(var), P(a), ctypes.c_uint(a.size), D(val))
+
+    def zetabc(z):
+        copy_bc(z, B["zetaClosedOrGradientBCIdx1"], B["zetaClosedOrGradientBCIdx2"],
+                B["zetaClosedOrGradientBCIdx1"].size)
+
+    def velbc(ub, vb):
+        set_bc(ub, B["ubarClosedBCIdx1"], 0.0)
+        set_bc(vb, B["vbarClosedBCIdx1"], 0.0)
+        set_bc(ub, B["ubarClampedBCIdx1"], .05 * math.sin(ct.time2D * 0.0002))
+        copy_bc(ub, B["ubarGradientBCIdx1"], B["ubarGradientBCIdx2"], B["ubarGradientBCIdx1"].size)
+        copy_bc(vb, B["vbarGradientBCIdx1"], B["ubarGradientBCIdx2"], B["vbarGradientBCIdx1"].size)
+
+    set_depth()
+    for _ in range(nsteps):
+        K("step3d", "set_maxflux", nt, P(O.t3("u")), P(O.t3("v")), P(O.Huon), P(O.Hvom), P(grid.Hz))
+        K("step3d", "omega", nt, P(O.W), P(O.t3("u")), P(O.t3("v")), P(O.Huon), P(O.Hvom),
+          P(grid.z_w), P(BC))
+        K("step3d", "set_zeta", nt, P(O.t("zeta", 1)), P(O.t("zeta", 2)), P(O.Zt_avg1))
+        ru, rv = O.t3("ru"), O.t3("rv")
+        ru[:] = 0.0
+        rv[:] = 0.0
+        K("rhs", "addCoriolis", nt, P(grid.fomn), P(O.t3("u")), P(O.t3("v")), P(ru), P(rv), P(grid.Hz))
+        K("rhs", "horizontalAdvection", nt, P(O.t3("u")), P(O.t3("v")), P(O.Huon), P(O.Hvom), P(ru),
+          P(rv), P(BC))
+        K("rhs", "verticalAdvection", nt, P(O.t3("u")), P(O.t3("v")), P(O.W), P(ru), P(rv), P(BC))
+        ct.iif = 0
+        for _ in range(ct.nfast + 1):
+            if ct.iif == 0:
+                O.Zt_avg1[:] = 0.0
+                O.DU_avg1[:] = 0.0
+                O.DV_avg1[:] = 0.0
+            ct.next2d()
+            O.cycle2d()
+            z0, z1, z2 = O.t("zeta", 0), O.t("zeta", 1), O.t("zeta", 2)
+            Dt = ct.dtfast
+            # step2dPredictor (step2d.py:23-81); iif >= 1 here, so always the leapfrog branch
+            K("2d", "computeZetaRHS", nt, P(z1), P(grid.h), P(O.t("ubar", 1)), P(O.t("vbar", 1)),
+              P(O.DU_avg1), P(O.DV_avg1), P(O.Zt_avg1), _b(True), P(ct.weight1), P(ct.weight2),
+              Ii(ct.iif), P(O.t("rzeta", 1)))
+            K("2d", "computeZetaPred", nt, D(Dt), P(z0), P(z1), P(z2), P(O.t("rzeta", 1)))
+            zetabc(z2)
+            K("2d", "computeMomentumRHSPred", nt, P(grid.h), P(O.t("rubar", 1)), P(O.t("rvbar", 1)),
+              P(z0), P(z2), D(G_GRAV), D(2.0 / 5.0))
+            K("2d", "computeMomentumPred", nt, D(Dt), P(O.t("ubar", 1)), P(O.t("ubar", 2)),
+              P(O.t("vbar", 1)), P(O.t("vbar", 2)), P(O.t("rubar", 1)), P(O.t("rvbar", 1)),
+              P(grid.h), P(z1), P(z2))
+            velbc(O.t("ubar", 2), O.t("vbar", 2))
+            # step2dCorrector (step2d.py:84-128)
+            K("2d", "computeZetaRHS", nt, P(z2), P(grid.h), P(O.t("ubar", 2)), P(O.t("vbar", 2)),
+              P(O.DU_avg1), P(O.DV_avg1), P(O.Zt_avg1), _b(False), P(ct.weight1), P(ct.weight2),
+              Ii(ct.iif), P(O.t("rzeta", 1)))
+            K("2d", "AdamsMoultonCorr3rd", nt, D(Dt), P(z2), P(O.t("rzeta", 0)), P(O.t("rzeta", 1)),
+              P(O.t("rzeta", 2)))
+            zetabc(z2)
+            K("2d", "computeMomentumRHSCorr", nt, P(grid.h), P(O.t("rubar", 2)), P(O.t("rvbar", 2)),
+              P(z0), P(z1), P(z2), D(G_GRAV))
+            K("2d", "AdamsMoultonCorr3rd", nt, D(Dt), P(O.t("ubar", 1)), P(O.t("vbar", 1)),
+              P(O.t("rubar", 0)), P(O.t("rubar", 1)))
+            velbc(O.t("ubar", 2), O.t("vbar", 2))
+            O.t("vbar", 2)[:] = 0.0
+        set_depth()
+        tmpU[:] = O.t3("u")
+        tmpV[:] = O.t3("v")
+        K("step3d", "step3d_UV", nt, P(O.t3("u")), P(O.t3("v")), P(O.t3("ru")), P(O.t3("rv")),
+          P(O.t("ubar", 1)), P(O.t("vbar", 1)), P(O.t("ubar", 2)), P(O.t("vbar", 2)), P(grid.Hz),
+          P(O.AKv), P(grid.z_r), P(O.DU_avg1), P(O.DV_avg1), P(tmpU), P(tmpV), P(grid.h),
+          Ii(ct.iic), Ii(ct.ntfirst), D(lam), D(1e-5), D(ct.dt))
+        K("step3d", "setLateralUVBCs", nt, D(ct.time), P(O.t3("u")), P(O.t3("v")),
+          P(B["uvelBC_bcIdxFieldIdx2"]), P(B["vvelBC_bcIdxFieldIdx2"]),
+          P(B["uvelBC_bcIdxFieldType"]), P(B["vvelBC_bcIdxFieldType"]))
+        K("step3d", "omega", nt, P(O.W), P(O.t3("u")), P(O.t3("v")), P(O.Huon), P(O.Hvom),
+          P(grid.z_w), P(BC))
+        ct.next3d()

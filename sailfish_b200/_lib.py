@@ -1,0 +1,96 @@
+"""ctypes binding of libsailfish_b200.so (C ABI: include/sailfish_b200.h).
+
+The library is built in tree by ``python -m sailfish_b200.build``.  There is no fallback:
+if it is missing or cannot be loaded, importing this module raises.
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libsailfish_b200.so")
+
+SF_OK, SF_EINVAL, SF_EDTYPE, SF_ECUDA, SF_ENONFINITE, SF_ETIMEOUT, SF_ENOMEM, SF_EUNSUPPORTED = \
+    0, -1, -2, -3, -4, -5, -6, -7
+SF_FP64, SF_FP32 = 0, 1
+
+_vp, _d, _i, _i32p = ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.POINTER(ctypes.c_int32)
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+class GridDesc(ctypes.Structure):
+    _fields_ = [
+        ("L", _i), ("M", _i), ("N", _i), ("precision", _i),
+        ("h", _dp), ("pm", _dp), ("pn", _dp), ("on_u", _dp), ("om_v", _dp), ("fomn", _dp),
+        ("sc_r", _dp), ("sc_w", _dp), ("Cs_r", _dp), ("Cs_w", _dp),
+        ("hc", _d), ("Vtransform", _i),
+        ("zeta_field_idx2", _i32p), ("uvel_field_type", _i32p), ("vvel_field_type", _i32p),
+        ("zeta_copy_idx1", _i32p), ("zeta_copy_idx2", _i32p), ("n_zeta_copy", _i),
+        ("ubar_closed_idx", _i32p), ("n_ubar_closed", _i),
+        ("vbar_closed_idx", _i32p), ("n_vbar_closed", _i),
+        ("ubar_clamped_idx", _i32p), ("n_ubar_clamped", _i),
+        ("ubar_grad_idx1", _i32p), ("ubar_grad_idx2", _i32p), ("n_ubar_grad", _i),
+        ("vbar_grad_idx1", _i32p), ("n_vbar_grad", _i),
+    ]
+
+
+class State2D(ctypes.Structure):
+    _fields_ = [("zeta", _vp * 3), ("ubar", _vp * 3), ("vbar", _vp * 3), ("rzeta", _vp * 3),
+                ("rubar", _vp * 3), ("rvbar", _vp * 3),
+                ("Zt_avg1", _vp), ("DU_avg1", _vp), ("DV_avg1", _vp)]
+
+
+# name -> argtypes (after the context pointer for the kernel entry points)
+SIGNATURES = {
+    "sf_ctx_create": [ctypes.POINTER(GridDesc), ctypes.POINTER(_vp)],
+    "sf_ctx_destroy": [_vp],
+    "sf_last_error": [],
+    "sf_version": [],
+    "sf_ctx_precision": [_vp],
+    "sf_zeta_rhs": [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _i, _d, _vp, _vp],
+    "sf_zeta_pred": [_vp, _d, _vp, _vp, _vp, _vp],
+    "sf_momentum_rhs": [_vp, _vp, _vp, _vp, _vp, _d, _d, _vp],
+    "sf_momentum_pred": [_vp, _d, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "sf_am3": [_vp, _d, _vp, _vp, _vp, _vp, _vp],
+    "sf_zetabc": [_vp, _vp, _vp],
+    "sf_barotropic_velocity_bc": [_vp, _vp, _vp, _d, _vp],
+    "sf_step2d_predictor": [_vp, ctypes.POINTER(State2D), _d, _d, _i, _vp],
+    "sf_step2d_corrector": [_vp, ctypes.POINTER(State2D), _d, _d, _d, _vp],
+    "sf_barotropic_substep": [_vp, ctypes.POINTER(State2D), _d, _d, _d, _i, _vp],
+    "sf_barotropic_loop": [_vp, ctypes.POINTER(State2D), _i, _dp, _d, _dp, _vp],
+    "sf_rhs3d": [_vp] * 10,
+    "sf_set_maxflux": [_vp] * 7,
+    "sf_omega": [_vp] * 6,
+    "sf_maxflux_omega": [_vp] * 12,
+    "sf_set_zeta": [_vp] * 5,
+    "sf_set_depth": [_vp] * 6,
+    "sf_step3d_uv": [_vp] * 16 + [_i, _i, _d, _d, _vp],
+    "sf_lateral_uv_bc": [_vp, _d, _vp, _vp, _vp],
+    "sf_step3d_uv_bc": [_vp] * 14 + [_i, _i, _d, _d, _d, _vp],
+}
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError("libsailfish_b200.so is not built (run: python -m sailfish_b200.build)")
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, args in SIGNATURES.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = ctypes.c_char_p if name == "sf_last_error" else ctypes.c_int
+    return lib
+
+
+lib = _load()
+
+
+class SailfishError(RuntimeError):
+    def __init__(self, code, where):
+        msg = lib.sf_last_error().decode(errors="replace")
+        super().__init__("%s failed (status %d): %s" % (where, code, msg))
+        self.code = code
+
+
+def check(code, where):
+    if code != SF_OK:
+        raise SailfishError(code, where)
+    return code

@@ -1,0 +1,63 @@
+"""Synthetic analytic basins of the benchmark and test configurations.
+
+All inputs are analytic (no external data): depth from a tanh continental shelf across y plus
+Gaussian seamounts, beta-plane Coriolis, S-coordinates with Vtransform 2 / Vstretching 4.
+
+  basin0: 2D basin, Lm=128, Mm=64, dx=dy=5 km, flat h=4000 m, dt=30 s
+  basin1: Lm=512, Mm=256, N=32, dx=2 km, theta_s=5, theta_b=0.4, hc=100 m, one seamount,
+          dt=240 s, ndtfast=30
+  basin4: Lm=2048, Mm=1024, N=50, dx=1 km, same recipe with two seamounts, dt=120 s,
+          ndtfast=40
+"""
+import numpy as np
+
+from . import host
+from .model import Grid
+
+CLOSED = {k: "Clo Clo Clo Clo" for k in ("isFsur", "isUbar", "isVbar", "isUvel", "isVvel")}
+
+
+def shelf_depth(Lm, Mm, dx, seamounts=(), shelf_frac=0.25, width_frac=0.1, hmin=50.0,
+                hmax=4000.0, sm_height=2000.0, sm_radius=20.0e3):
+    """Rho-point depth (Mm+2, Lm+2): hmin + (hmax-hmin)*tanh-shelf rising towards y=0, minus
+    Gaussian seamounts of the given relative (x, y) positions, floored at hmin."""
+    L, M = Lm + 1, Mm + 1
+    jj, ii = np.meshgrid(np.arange(M + 1), np.arange(L + 1), indexing="ij")
+    x, y = (ii - 0.5) * dx, (jj - 0.5) * dx
+    Ly = Mm * dx
+    Lx = Lm * dx
+    prof = 0.5 * (1.0 + np.tanh((y - shelf_frac * Ly) / (width_frac * Ly)))
+    h = hmin + (hmax - hmin) * prof
+    for fx, fy in seamounts:
+        h = h - sm_height * np.exp(-((x - fx * Lx) ** 2 + (y - fy * Ly) ** 2) / sm_radius ** 2)
+    return np.maximum(h, hmin), x, y
+
+
+def basin(Lm, Mm, N, dx, seamounts, dt, ndtfast, f0=1e-4, beta=2e-11, theta_s=5.0,
+          theta_b=0.4, tcline=100.0, hflat=None):
+    if hflat is None:
+        h, x, y = shelf_depth(Lm, Mm, dx, seamounts)
+    else:
+        h, x, y = shelf_depth(Lm, Mm, dx)
+        h[...] = hflat
+    f = f0 + beta * (y - 0.5 * Mm * dx)
+    grid = Grid.analytic(Lm, Mm, N, h, dx, dx, f, Vtransform=2, Vstretching=4, theta_s=theta_s,
+                         theta_b=theta_b, tcline=tcline)
+    grid.x, grid.y = x, y
+    boundary = host.Boundary(grid.L, grid.M, CLOSED)
+    return dict(grid=grid, boundary=boundary, dt=float(dt), ndtfast=int(ndtfast))
+
+
+def basin1():
+    return basin(512, 256, 32, 2.0e3, [(0.5, 0.6)], dt=240.0, ndtfast=30)
+
+
+def basin4():
+    return basin(2048, 1024, 50, 1.0e3, [(1.0 / 3.0, 0.6), (2.0 / 3.0, 0.6)], dt=120.0, ndtfast=40)
+
+
+def small(Lm=256, Mm=128, N=32):
+    return basin(Lm, Mm, N, 2.0e3, [(0.5, 0.6)], dt=240.0, ndtfast=30)
+
+
+CONFIGS = {"basin1": basin1, "basin4": basin4, "small": small}

@@ -1,0 +1,549 @@
+// C ABI of libsailfish_b200.so (declarations and reference citations: include/sailfish_b200.h).
+//
+// Host-side runtime: context creation (grid snapshot, boundary programs), argument checks,
+// precision dispatch and error reporting.  No C++ exception crosses the boundary.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <type_traits>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "sf_internal.h"
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string &msg) {
+    g_err = msg;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char *where) {
+    return fail(SF_ECUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define SF_TRY_CUDA(expr, where)                      \
+    do {                                              \
+        cudaError_t e_ = (expr);                      \
+        if (e_ != cudaSuccess) return cuda_fail(e_, where); \
+    } while (0)
+
+template <typename T>
+int upload(T **dst, const T *src, size_t n, const char *what) {
+    *dst = nullptr;
+    if (n == 0) return SF_OK;
+    if (!src) return fail(SF_EINVAL, std::string("missing host array: ") + what);
+    cudaError_t e = cudaMalloc((void **)dst, n * sizeof(T));
+    if (e != cudaSuccess) return fail(SF_ENOMEM, std::string("cudaMalloc ") + what);
+    e = cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(e, what);
+    return SF_OK;
+}
+
+int upload_real(sf_ctx *c, void **dst, const double *src, size_t n, const char *what) {
+    if (c->prec == SF_FP64) return upload(reinterpret_cast<double **>(dst), src, n, what);
+    if (!src) return fail(SF_EINVAL, std::string("missing host array: ") + what);
+    std::vector<float> tmp(n);
+    for (size_t k = 0; k < n; ++k) tmp[k] = (float)src[k];
+    return upload(reinterpret_cast<float **>(dst), tmp.data(), n, what);
+}
+
+// One boundary scatter of the reference: setBC (constant) or copyBC (node to node).
+struct BcOp {
+    const int32_t *idx1;
+    const int32_t *idx2;   // nullptr for setBC
+    int n;
+    int code;              // setBC value: -1 -> 0.0, -2 -> time-dependent value
+};
+
+// Reduces a sequence of scatters, executed in order and each in thread order (what the
+// reference's sequential launches amount to when no two threads of a launch conflict, and
+// what its host-compiled form does when they do), to one gather program (sf::BcProgram).
+int resolve(const std::vector<BcOp> &ops, long s2, std::vector<int> &dst, std::vector<int> &src) {
+    std::unordered_map<int, int> cur;   // node -> symbolic value
+    std::vector<int> order;
+    auto get = [&](int node) {
+        auto it = cur.find(node);
+        return it == cur.end() ? node : it->second;
+    };
+    for (const BcOp &op : ops) {
+        for (int k = 0; k < op.n; ++k) {
+            const int d = op.idx1[k];
+            if (d < 0 || d >= s2) return fail(SF_EINVAL, "boundary index out of range");
+            int val;
+            if (op.idx2) {
+                const int s = op.idx2[k];
+                if (s < 0 || s >= s2) return fail(SF_EINVAL, "boundary source index out of range");
+                val = get(s);
+            } else {
+                val = op.code;
+            }
+            if (cur.find(d) == cur.end()) order.push_back(d);
+            cur[d] = val;
+        }
+    }
+    dst.clear();
+    src.clear();
+    for (int d : order) {
+        const int v = cur[d];
+        if (v == d) continue;
+        dst.push_back(d);
+        src.push_back(v);
+    }
+    return SF_OK;
+}
+
+int make_program(sf::BcProgram &p, const std::vector<BcOp> &ops, long s2) {
+    std::vector<int> d, s;
+    int rc = resolve(ops, s2, d, s);
+    if (rc) return rc;
+    p.n = (int)d.size();
+    rc = upload(&p.dst, d.data(), d.size(), "boundary program");
+    if (rc) return rc;
+    return upload(&p.src, s.data(), s.size(), "boundary program");
+}
+
+void free_ctx(sf_ctx *c) {
+    if (!c) return;
+    for (void *m : c->metrics) cudaFree(m);
+    cudaFree(c->hd);
+    cudaFree(c->vert);
+    cudaFree(c->bcfield);
+    cudaFree(c->utype);
+    cudaFree(c->vtype);
+    for (sf::BcProgram *p : {&c->zbc, &c->ubc, &c->vbc}) {
+        cudaFree(p->dst);
+        cudaFree(p->src);
+    }
+    delete c;
+}
+
+inline cudaStream_t S(sf_stream s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// Dispatch a launcher on the context precision; `body` is a generic lambda taking a type tag.
+template <typename F>
+int dispatch(const sf_ctx *c, const char *name, F body) {
+    if (!c) return fail(SF_EINVAL, "null context");
+    cudaError_t e;
+    if (c->prec == SF_FP64) e = body((double *)nullptr);
+    else e = body((float *)nullptr);
+    if (e != cudaSuccess) return cuda_fail(e, name);
+    return SF_OK;
+}
+
+const double kBcOmega = 0.0002;   // fake clamped boundary (barotropicVelocityBC.py:21-22,
+                                  // step3D_uv.kernels.cpp:338-339)
+
+}  // namespace
+
+extern "C" {
+
+int sf_version(void) { return 1; }
+
+const char *sf_last_error(void) { return g_err.c_str(); }
+
+int sf_ctx_precision(const sf_ctx *ctx) { return ctx ? ctx->prec : SF_EINVAL; }
+
+int sf_ctx_create(const sf_grid_desc *d, sf_ctx **out) {
+    if (!d || !out) return fail(SF_EINVAL, "null argument");
+    *out = nullptr;
+    if (d->precision != SF_FP64 && d->precision != SF_FP32)
+        return fail(SF_EDTYPE, "precision must be SF_FP64 or SF_FP32");
+    if (d->L < 4 || d->M < 4) return fail(SF_EINVAL, "grid too small (need L, M >= 4)");
+    if (d->N < 5 || d->N > 64)
+        return fail(SF_EINVAL, "N must be in [5, 64]: the reference's verticalAdvection reads "
+                               "levels up to 5 (rhs_kernels.cpp:172) and columns are held per thread");
+    if (d->Vtransform != 1 && d->Vtransform != 2) return fail(SF_EINVAL, "Vtransform must be 1 or 2");
+    sf_ctx *c = new (std::nothrow) sf_ctx();
+    if (!c) return fail(SF_ENOMEM, "host allocation");
+    c->prec = d->precision;
+    c->L = d->L;
+    c->M = d->M;
+    c->N = d->N;
+    c->I = d->L + 1;
+    c->J = d->M + 1;
+    c->s2 = (long)c->I * c->J;
+    c->hc = d->hc;
+    c->Vtransform = d->Vtransform;
+    // horizontalAdvection is launched with (grsz*GPUMUL, bksz//GPUMUL) = 512*(s2/512 + 1)
+    // threads (nonlinear/rhs.py:62, modules/mod_operators.py:40-41, utility/misc.py:10,17).
+    c->ref_threads = 512L * (c->s2 / 512 + 1);
+    cudaGetDevice(&c->device);
+    const size_t s2 = (size_t)c->s2;
+    int rc = SF_OK;
+    const double *m[6] = {d->h, d->pm, d->pn, d->on_u, d->om_v, d->fomn};
+    const char *mn[6] = {"h", "pm", "pn", "on_u", "om_v", "fomn"};
+    for (int k = 0; k < 6 && rc == SF_OK; ++k) rc = upload_real(c, &c->metrics[k], m[k], s2, mn[k]);
+    if (rc == SF_OK) rc = upload(&c->hd, d->h, s2, "h");
+    if (rc == SF_OK) {
+        const int N = d->N;
+        if (!d->sc_r || !d->sc_w || !d->Cs_r || !d->Cs_w) rc = fail(SF_EINVAL, "missing S-coordinate tables");
+        else {
+            std::vector<double> v;
+            v.insert(v.end(), d->sc_r, d->sc_r + N);
+            v.insert(v.end(), d->sc_w, d->sc_w + N + 1);
+            v.insert(v.end(), d->Cs_r, d->Cs_r + N);
+            v.insert(v.end(), d->Cs_w, d->Cs_w + N + 1);
+            rc = upload(&c->vert, v.data(), v.size(), "S-coordinate tables");
+        }
+    }
+    if (rc == SF_OK) rc = upload(&c->bcfield, (const int *)d->zeta_field_idx2, s2, "zeta_field_idx2");
+    if (rc == SF_OK) rc = upload(&c->utype, (const int *)d->uvel_field_type, s2, "uvel_field_type");
+    if (rc == SF_OK) rc = upload(&c->vtype, (const int *)d->vvel_field_type, s2, "vvel_field_type");
+    if (rc == SF_OK) {
+        // setLateralUVBCs's gradient branch reads bcVIdxFieldIdx2[i + k*sz2D] for k >= 1, past
+        // the end of that 2D map (step3D_uv.kernels.cpp:363); it is refused here.
+        for (size_t k = 0; k < s2; ++k)
+            if (d->vvel_field_type[k] > 0 && (d->vvel_field_type[k] & (1 << 4)) == 0 &&
+                (d->vvel_field_type[k] & (1 << 3)) == 0 && (d->vvel_field_type[k] & (1 << 6)) != 0) {
+                rc = fail(SF_EUNSUPPORTED, "gradient 3D v boundary: the reference reads past the "
+                                           "boundary map (step3D_uv.kernels.cpp:363)");
+                break;
+            }
+    }
+    if (rc == SF_OK && d->n_vbar_grad > d->n_ubar_grad)
+        rc = fail(SF_EUNSUPPORTED, "vbar gradient list longer than the ubar list the reference "
+                                   "copies it from (barotropicVelocityBC.py:30-31)");
+    if (rc == SF_OK)
+        rc = make_program(c->zbc, {{d->zeta_copy_idx1, d->zeta_copy_idx2, d->n_zeta_copy, 0}}, c->s2);
+    if (rc == SF_OK)
+        rc = make_program(c->ubc,
+                          {{d->ubar_closed_idx, nullptr, d->n_ubar_closed, -1},
+                           {d->ubar_clamped_idx, nullptr, d->n_ubar_clamped, -2},
+                           {d->ubar_grad_idx1, d->ubar_grad_idx2, d->n_ubar_grad, 0}},
+                          c->s2);
+    if (rc == SF_OK)
+        rc = make_program(c->vbc,
+                          {{d->vbar_closed_idx, nullptr, d->n_vbar_closed, -1},
+                           {d->vbar_grad_idx1, d->ubar_grad_idx2, d->n_vbar_grad, 0}},
+                          c->s2);
+    if (rc == SF_OK) {
+        const size_t bytes = (size_t)(c->ubc.n + c->vbc.n) * (c->prec == SF_FP64 ? 8 : 4);
+        const size_t zbytes = (size_t)c->zbc.n * (c->prec == SF_FP64 ? 8 : 4);
+        if (bytes > 200 * 1024 || zbytes > 200 * 1024)
+            rc = fail(SF_EUNSUPPORTED, "boundary programs larger than one block's shared memory");
+    }
+    if (rc != SF_OK) {
+        free_ctx(c);
+        return rc;
+    }
+    *out = c;
+    return SF_OK;
+}
+
+int sf_ctx_destroy(sf_ctx *ctx) {
+    free_ctx(ctx);
+    return SF_OK;
+}
+
+// ---- 2D ---------------------------------------------------------------------------------
+int sf_zeta_rhs(sf_ctx *c, const void *zeta, const void *ubar, const void *vbar, double *DU,
+                double *DV, double *Zt, int is_predictor, double cff1, void *rzeta,
+                sf_stream s) {
+    if (!is_predictor && (!DU || !DV || !Zt)) return fail(SF_EINVAL, "accumulators required");
+    return dispatch(c, "sf_zeta_rhs", [&](auto *t) {
+        using R = std::remove_pointer_t<decltype(t)>;
+        return sf::Ops<R>::zeta_rhs(c, (const R *)zeta, (const R *)ubar, (const R *)vbar,
+                                    (R *)rzeta, is_predictor ? 0 : 1, cff1, Zt, DU, DV, nullptr,
+                                    nullptr, 0.0, S(s));
+    });
+}
+
+int sf_zeta_pred(sf_ctx *c, double Dt, const void *z0, void *z2, const void *rz1, sf_stream s) {
+    return dispatch(c, "sf_zeta_pred", [&](auto *t) {
+        using R = std::remove_pointer_t<decltype(t)>;
+        return sf::Ops<R>::zeta_pred(c, Dt, (const R *)z0, (R *)z2, (const R *)rz1, S(s));
+    });
+}
+
+int sf_momentum_rhs(sf_ctx *c, void *ru, void *rv, const void *za, const void *zb, double g,
+                    double weight, sf_stream s) {
+    return dispatch(c, "sf_momentum_rhs", [&](auto *t) {
+        using R = std::remove_pointer_t<decltype(t)>;
+        return sf::Ops<R>::momentum(c, (R *)ru, (R *)rv, (const R *)za, (const R *)zb, g, weight,
+                                    1, 0, 0.0, nullptr, nullptr, nullptr, nullptr, nullptr,
+                                    nullptr, S(s));
+    });
+}
+
+int sf_momentum_pred(sf_ctx *c, double Dt, const void *u_t1, void *u_t2, const void *v_t1,
+                     void *v_t2, const void *rhsu, const void *rhsv, const void *z1,
+                     const void *z2, sf_stream s) {
+    return dispatch(c, "sf_momentum_pred", [&](auto *t) {
+        using R = std::remove_pointer_t<decltype(t)>;
+        return sf::Ops<R>::momentum(c, (R *)rhsu, (R *)rhsv, nullptr, nullptr, 0.0, 0.0, 0, 1, Dt,
+                                    (const R *)u_t1, (R *)u_t2, (const R *)v_t1, (R *)v_t2,
+                                    (const R *)z1, (const R *)z2, S(s));
+    });
+}
+
+int sf_am3(sf_ctx *c, double Dt, void *v, const void *r0, const void *r1, const void *r2,
+           sf_stream s) {
+    return dispatch(c, "sf_am3", [&](auto *t) {
+        using R = std::remove_pointer_t<decltype(t)>;
+        return sf::Ops<R>::am3(c, Dt, (R *)v, (const R *)r0, (const R *)r1, (const R *)r2, S(s));
+    });
+}
+
+int sf_zetabc(sf_ctx *c, void *zeta, sf_stream s) {
+    return dispatch(c, "sf_zetabc", [&](auto *t) {
+        using R = std::remove_pointer_t<decltype(t)>;
+        sf::BcProgram none;
+        return sf::Ops<R>::bc_apply(c, c->zbc, (R *)zeta, none, nullptr, 0.0, S(s));
+    });
+}
+
+int sf_barotropic_velocity_bc(sf_ctx *c, void *ubar, void *vbar, double time2D, sf_stream s) {
+    const double val = .05 * std::sin(time2D * kBcOmega);
+    return dispatch(c, "sf_barotropic_velocity_bc", [&](auto *t) {
+        using R = std::remove_pointer_t<decltype(t)>;
+        return sf::Ops<R>::bc_apply(c, c->ubc, (R *)ubar, c->vbc, (R *)vbar, val, S(s));
+    });
+}
+
+int sf_step2d_predictor(sf_ctx *c, const sf_state2d *st, double dtfast, double time2D,
+                        int first_step, sf_stream s) {
+    if (!st) return fail(SF_EINVAL, "null state");
+    const double val = .05 * std::sin(time2D * kBcOmega);
+    return dispatch(c, "sf_step2d_predictor", [&](auto *t) -> cudaError_t {
+        using R = std::remove_pointer_t<decltype(t)>;
+        using O = sf::Ops<R>;
+        R *z0 = (R *)st->zeta[0], *z1 = (R *)st->zeta[1], *z2 = (R *)st->zeta[2];
+        cudaError_t e;
+        if (first_step) {
+            e = O::zeta_rhs(c, z1, (R *)st->ubar[1], (R *)st->vbar[1], (R *)st->rzeta[1], 0, 0.0,
+                            nullptr, nullptr, nullptr, nullptr, nullptr, 0.0, S(s));
+            if (e == cudaSuccess) e = O::zeta_euler(c, dtfast, z1, z2, (R *)st->rzeta[1], S(s));
+        } else {
+            e = O::zeta_rhs(c, z1, (R *)st->ubar[1], (R *)st->vbar[1], (R *)st->rzeta[1], 2, 0.0,
+                            nullptr, nullptr, nullptr, z0, z2, dtfast, S(s));
+        }
+        sf::BcProgram none;
+        if (e == cudaSuccess) e = O::bc_apply(c, c->zbc, z2, none, nullptr, 0.0, S(s));
+        const double w = first_step ? 0.5 : 2.0 / 5.0;
+        if (e == cudaSuccess)
+            e = O::momentum(c, (R *)st->rubar[1], (R *)st->rvbar[1], z2, z0, 10.0, w, 1, 1, dtfast,
+                            (R *)st->ubar[1], (R *)st->ubar[2], (R *)st->vbar[1], (R *)st->vbar[2],
+                            z1, z2, S(s));
+        if (e == cudaSuccess)
+            e = O::bc_apply(c, c->ubc, (R *)st->ubar[2], c->vbc, (R *)st->vbar[2], val, S(s));
+        return e;
+    });
+}
+
+int sf_step2d_corrector(sf_ctx *c, const sf_state2d *st, double dtfast, double time2D,
+                        double cff1, sf_stream s) {
+    if (!st) return fail(SF_EINVAL, "null state");
+    const double val = .05 * std::sin(time2D * kBcOmega);
+    return dispatch(c, "sf_step2d_corrector", [&](auto *t) -> cudaError_t {
+        using R = std::remove_pointer_t<decltype(t)>;
+        using O = sf::Ops<R>;
+        R *z2 = (R *)st->zeta[2];
+        cudaError_t e = O::zeta_rhs(c, z2, (R *)st->ubar[2], (R *)st->vbar[2], (R *)st->rzeta[1],
+                                    1, cff1, st->Zt_avg1, st->DU_avg1, st->DV_avg1, nullptr,
+                                    nullptr, 0.0, S(s));
+        // AdamsMoultonCorr3rd on zeta (step2d.py:109) and on ubar_t1 through the mis-bound
+        // AdamsMoultonCorr3rd2 (step2d.py:120-123); independent of zetabc and of the
+        // momentum RHS, so both run in one pass here.
+        if (e == cudaSuccess)
+            e = O::corr_point(c, dtfast, z2, (R *)st->rzeta[0], (R *)st->rzeta[1],
+                              (R *)st->rzeta[2], (R *)st->ubar[1], (R *)st->vbar[1],
+                              (R *)st->rubar[0], (R *)st->rubar[1], nullptr, S(s));
+        sf::BcProgram none;
+        if (e == cudaSuccess) e = O::bc_apply(c, c->zbc, z2, none, nullptr, 0.0, S(s));
+        if (e == cudaSuccess)
+            e = O::momentum(c, (R *)st->rubar[2], (R *)st->rvbar[2], z2, (R *)st->zeta[1], 10.0,
+                            2.0 / 5.0, 1, 0, 0.0, nullptr, nullptr, nullptr, nullptr, nullptr,
+                            nullptr, S(s));
+        if (e == cudaSuccess)
+            e = O::bc_apply(c, c->ubc, (R *)st->ubar[2], c->vbc, (R *)st->vbar[2], val, S(s));
+        return e;
+    });
+}
+
+}  // extern "C"
+
+namespace {
+template <typename R>
+cudaError_t substep(const sf_ctx *c, const sf_state2d *st, double dtfast, double time2D,
+                    double cff1, int last, cudaStream_t s) {
+    using O = sf::Ops<R>;
+    const double val = .05 * std::sin(time2D * kBcOmega);
+    R *z0 = (R *)st->zeta[0], *z1 = (R *)st->zeta[1], *z2 = (R *)st->zeta[2];
+    sf::BcProgram none;
+    // predictor (step2d.py:23-81): computeZetaRHS + computeZetaPred, zetabc,
+    // computeMomentumRHSPred + computeMomentumPred, barotropicVelocityBC
+    cudaError_t e = O::zeta_rhs(c, z1, (R *)st->ubar[1], (R *)st->vbar[1], (R *)st->rzeta[1], 2, 0.0,
+                                nullptr, nullptr, nullptr, z0, z2, dtfast, s);
+    if (e == cudaSuccess) e = O::bc_apply(c, c->zbc, z2, none, nullptr, 0.0, s);
+    if (e == cudaSuccess)
+        e = O::momentum(c, (R *)st->rubar[1], (R *)st->rvbar[1], z2, z0, 10.0, 2.0 / 5.0, 1, 1,
+                        dtfast, (R *)st->ubar[1], (R *)st->ubar[2], (R *)st->vbar[1],
+                        (R *)st->vbar[2], z1, z2, s);
+    if (e == cudaSuccess) e = O::bc_apply(c, c->ubc, (R *)st->ubar[2], c->vbc, (R *)st->vbar[2], val, s);
+    // corrector (step2d.py:84-128) and vbar_t2[:] = 0 (main3d.py:189)
+    if (e == cudaSuccess)
+        e = O::zeta_rhs(c, z2, (R *)st->ubar[2], (R *)st->vbar[2], (R *)st->rzeta[1], 1, cff1,
+                        st->Zt_avg1, st->DU_avg1, st->DV_avg1, nullptr, nullptr, 0.0, s);
+    if (e == cudaSuccess && last)   // barotropicVelocityBC of the corrector is idempotent
+        e = O::corr_point(c, dtfast, z2, (R *)st->rzeta[0], (R *)st->rzeta[1], (R *)st->rzeta[2],
+                          (R *)st->ubar[1], (R *)st->vbar[1], (R *)st->rubar[0], (R *)st->rubar[1],
+                          nullptr, s);
+    else if (e == cudaSuccess)
+        e = O::corr_point(c, dtfast, z2, (R *)st->rzeta[0], (R *)st->rzeta[1], (R *)st->rzeta[2],
+                          (R *)st->ubar[1], (R *)st->vbar[1], (R *)st->rubar[0], (R *)st->rubar[1],
+                          (R *)st->vbar[2], s);
+    if (e == cudaSuccess) e = O::bc_apply(c, c->zbc, z2, none, nullptr, 0.0, s);
+    if (e == cudaSuccess && last) {
+        e = O::momentum(c, (R *)st->rubar[2], (R *)st->rvbar[2], z2, z1, 10.0, 2.0 / 5.0, 1, 0, 0.0,
+                        nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, s);
+        if (e == cudaSuccess)
+            e = cudaMemsetAsync(st->vbar[2], 0, (size_t)c->s2 * sizeof(R), s);
+    }
+    return e;
+}
+}  // namespace
+
+extern "C" {
+
+int sf_barotropic_substep(sf_ctx *c, const sf_state2d *st, double dtfast, double time2D,
+                          double cff1, int last, sf_stream s) {
+    if (!st) return fail(SF_EINVAL, "null state");
+    return dispatch(c, "sf_barotropic_substep", [&](auto *t) {
+        using R = std::remove_pointer_t<decltype(t)>;
+        return substep<R>(c, st, dtfast, time2D, cff1, last, S(s));
+    });
+}
+
+int sf_barotropic_loop(sf_ctx *c, sf_state2d *st, int nsub, const double *weight1, double dtfast,
+                       double *time2D, sf_stream s) {
+    if (!st || !weight1 || !time2D || nsub < 1) return fail(SF_EINVAL, "bad argument");
+    const size_t n2 = (size_t)c->s2 * sizeof(double);
+    cudaError_t e = cudaMemsetAsync(st->Zt_avg1, 0, n2, S(s));
+    if (e == cudaSuccess) e = cudaMemsetAsync(st->DU_avg1, 0, n2, S(s));
+    if (e == cudaSuccess) e = cudaMemsetAsync(st->DV_avg1, 0, n2, S(s));
+    if (e != cudaSuccess) return cuda_fail(e, "sf_barotropic_loop");
+    double t2 = *time2D;
+    for (int iif = 1; iif <= nsub; ++iif) {
+        t2 += dtfast;                                  // CompTimes.next2DTimeStep
+        void **arrs[6] = {st->zeta, st->ubar, st->vbar, st->rzeta, st->rubar, st->rvbar};
+        for (void **a : arrs) {                        // T_OCEAN.cycleTimes2D
+            void *t0 = a[0];
+            a[0] = a[1];
+            a[1] = a[2];
+            a[2] = t0;
+        }
+        const int rc = sf_barotropic_substep(c, st, dtfast, t2, weight1[iif - 1], iif == nsub, s);
+        if (rc != SF_OK) return rc;
+    }
+    *time2D = t2;
+    return SF_OK;
+}
+
+// ---- 3D ---------------------------------------------------------------------------------
+int sf_rhs3d(sf_ctx *c, const void *u, const void *v, const void *Huon, const void *Hvom,
+             const void *W, const void *Hz, void *ru, void *rv, sf_stream s) {
+    return dispatch(c, "sf_rhs3d", [&](auto *t) {
+        using R = std::remove_pointer_t<decltype(t)>;
+        return sf::Ops<R>::rhs3d(c, (const R *)u, (const R *)v, (const R *)Huon, (const R *)Hvom,
+                                 (const R *)W, (const R *)Hz, (R *)ru, (R *)rv, S(s));
+    });
+}
+
+int sf_set_maxflux(sf_ctx *c, const void *u, const void *v, void *Huon, void *Hvom, const void *Hz,
+                   sf_stream s) {
+    return dispatch(c, "sf_set_maxflux", [&](auto *t) {
+        using R = std::remove_pointer_t<decltype(t)>;
+        return sf::Ops<R>::maxflux_omega(c, (const R *)u, (const R *)v, (R *)Huon, (R *)Hvom,
+                                         (const R *)Hz, nullptr, nullptr, 1, 0, nullptr, nullptr,
+                                         nullptr, S(s));
+    });
+}
+
+int sf_omega(sf_ctx *c, void *W, const void *Huon, const void *Hvom, const void *z_w,
+             sf_stream s) {
+    return dispatch(c, "sf_omega", [&](auto *t) {
+        using R = std::remove_pointer_t<decltype(t)>;
+        return sf::Ops<R>::maxflux_omega(c, nullptr, nullptr, (R *)Huon, (R *)Hvom, nullptr,
+                                         (R *)W, (const R *)z_w, 0, 1, nullptr, nullptr, nullptr,
+                                         S(s));
+    });
+}
+
+int sf_maxflux_omega(sf_ctx *c, const void *u, const void *v, void *Huon, void *Hvom,
+                     const void *Hz, void *W, const void *z_w, void *zeta_t1, void *zeta_t2,
+                     const double *Zt, sf_stream s) {
+    if ((zeta_t1 || zeta_t2 || Zt) && !(zeta_t1 && zeta_t2 && Zt))
+        return fail(SF_EINVAL, "set_zeta needs zeta_t1, zeta_t2 and Zt_avg1");
+    return dispatch(c, "sf_maxflux_omega", [&](auto *t) {
+        using R = std::remove_pointer_t<decltype(t)>;
+        return sf::Ops<R>::maxflux_omega(c, (const R *)u, (const R *)v, (R *)Huon, (R *)Hvom,
+                                         (const R *)Hz, (R *)W, (const R *)z_w, 1, 1,
+                                         (R *)zeta_t1, (R *)zeta_t2, Zt, S(s));
+    });
+}
+
+int sf_set_zeta(sf_ctx *c, void *z1, void *z2, const double *Zt, sf_stream s) {
+    return dispatch(c, "sf_set_zeta", [&](auto *t) {
+        using R = std::remove_pointer_t<decltype(t)>;
+        return sf::Ops<R>::set_zeta(c, (R *)z1, (R *)z2, Zt, S(s));
+    });
+}
+
+int sf_set_depth(sf_ctx *c, const double *Zt, void *z_w, void *z_r, void *Hz, sf_stream s) {
+    return dispatch(c, "sf_set_depth", [&](auto *t) {
+        using R = std::remove_pointer_t<decltype(t)>;
+        return sf::Ops<R>::set_depth(c, Zt, (R *)z_w, (R *)z_r, (R *)Hz, S(s));
+    });
+}
+
+static double ab3_cff(int iic, int ntfirst) {   // step3D_uv.kernels.cpp:663-666
+    if (iic == ntfirst) return 1.0;
+    if (iic == ntfirst + 1) return 3.0 / 2.0;
+    return 23.0 / 12.0;
+}
+
+int sf_step3d_uv(sf_ctx *c, void *u, void *v, const void *ru, const void *rv, void *ubar_t1,
+                 void *vbar_t1, void *ubar_t2, void *vbar_t2, const void *Hz, const void *Akv,
+                 const void *z_r, const double *DU, const double *DV, const void *tmpU,
+                 const void *tmpV, int iic, int ntfirst, double lambda, double Dt, sf_stream s) {
+    const double cff = ab3_cff(iic, ntfirst);
+    return dispatch(c, "sf_step3d_uv", [&](auto *t) {
+        using R = std::remove_pointer_t<decltype(t)>;
+        return sf::Ops<R>::step3d_uv(c, (R *)u, (R *)v, (const R *)ru, (const R *)rv, (R *)ubar_t1,
+                                     (R *)vbar_t1, (R *)ubar_t2, (R *)vbar_t2, (const R *)Hz,
+                                     (const R *)Akv, (const R *)z_r, DU, DV, (const R *)tmpU,
+                                     (const R *)tmpV, cff, lambda, Dt, 0, 0.0, S(s));
+    });
+}
+
+int sf_step3d_uv_bc(sf_ctx *c, void *u, void *v, const void *ru, const void *rv, void *ubar_t1,
+                    void *vbar_t1, void *ubar_t2, void *vbar_t2, const void *Hz, const void *Akv,
+                    const void *z_r, const double *DU, const double *DV, int iic, int ntfirst,
+                    double lambda, double Dt, double time, sf_stream s) {
+    const double cff = ab3_cff(iic, ntfirst);
+    const double val = 0.05 * std::sin(time * kBcOmega);
+    return dispatch(c, "sf_step3d_uv_bc", [&](auto *t) {
+        using R = std::remove_pointer_t<decltype(t)>;
+        return sf::Ops<R>::step3d_uv(c, (R *)u, (R *)v, (const R *)ru, (const R *)rv, (R *)ubar_t1,
+                                     (R *)vbar_t1, (R *)ubar_t2, (R *)vbar_t2, (const R *)Hz,
+                                     (const R *)Akv, (const R *)z_r, DU, DV, nullptr, nullptr,
+                                     cff, lambda, Dt, 1, val, S(s));
+    });
+}
+
+int sf_lateral_uv_bc(sf_ctx *c, double time, void *u, void *v, sf_stream s) {
+    const double val = 0.05 * std::sin(time * kBcOmega);
+    return dispatch(c, "sf_lateral_uv_bc", [&](auto *t) {
+        using R = std::remove_pointer_t<decltype(t)>;
+        return sf::Ops<R>::lateral_uv_bc(c, (R *)u, (R *)v, val, S(s));
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,98 @@
+// Internal types shared by the C-ABI layer (sf_capi.cu) and the kernel translation units
+// (sf_kernels_f64.cu, sf_kernels_f32.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/sailfish_b200.h"
+
+namespace sf {
+
+// A boundary "program": the sequential effect of the reference's boundary scatter launches
+// (setBC / copyBC, modules/mod_BC.c:6-23, run one after the other in thread order) reduced to
+// a gather dst[k] <- src[k], where src >= 0 is a node of the field as it was before the
+// program ran, src == -1 is the constant 0 and src == -2 is the time-dependent value.
+struct BcProgram {
+    int n = 0;
+    int *dst = nullptr;  // device
+    int *src = nullptr;  // device
+};
+
+// Grid view handed to kernels by value.
+template <typename R>
+struct Geo {
+    int I, J, N;  // xi points (L+1), eta points (M+1), levels
+    long s2;      // I*J
+    const R *on_u, *om_v, *pm, *pn, *h, *fomn;
+    const double *hd;                          // h in FP64 (set_depth)
+    const double *sc_r, *sc_w, *Cs_r, *Cs_w;   // S-coordinate tables
+    double hc;
+    int Vtransform;
+    const int *bcfield;   // zetaBC.bcIdxFieldIdx2
+    const int *utype, *vtype;
+    long ref_threads;     // threads of the reference's rhs3d launches (rhs_kernels.cpp:86-91)
+};
+
+}  // namespace sf
+
+struct sf_ctx {
+    int prec;
+    int L, M, N, I, J;
+    long s2;
+    int device;
+    void *metrics[6];       // h, pm, pn, on_u, om_v, fomn in the context precision
+    double *hd;             // h in FP64
+    double *vert;           // sc_r[N] | sc_w[N+1] | Cs_r[N] | Cs_w[N+1]
+    double hc;
+    int Vtransform;
+    int *bcfield, *utype, *vtype;
+    sf::BcProgram zbc, ubc, vbc;
+    long ref_threads;
+};
+
+namespace sf {
+
+// Launchers, one explicit instantiation per precision (FP64 in a translation unit built
+// without FMA contraction, so that it reproduces the reference's IEEE evaluation).
+template <typename R>
+struct Ops {
+    static Geo<R> geo(const sf_ctx *c);
+    static cudaError_t zeta_rhs(const sf_ctx *c, const R *zeta, const R *ubar, const R *vbar,
+                                R *rzeta, int mode, double cff1, double *Zt, double *DU, double *DV,
+                                const R *zeta_t0, R *zeta_t2, double Dt, cudaStream_t s);
+    static cudaError_t zeta_pred(const sf_ctx *c, double Dt, const R *z0, R *z2, const R *rz1,
+                                 cudaStream_t s);
+    static cudaError_t zeta_euler(const sf_ctx *c, double Dt, const R *z1, R *z2, const R *rz1,
+                                  cudaStream_t s);
+    static cudaError_t momentum(const sf_ctx *c, R *rhs_u, R *rhs_v, const R *za, const R *zb,
+                                double g, double weight, int do_rhs, int do_pred, double Dt,
+                                const R *u_t1, R *u_t2, const R *v_t1, R *v_t2, const R *z1,
+                                const R *z2, cudaStream_t s);
+    static cudaError_t am3(const sf_ctx *c, double Dt, R *v, const R *r0, const R *r1,
+                           const R *r2, cudaStream_t s);
+    static cudaError_t corr_point(const sf_ctx *c, double Dt, R *zeta_t2, const R *rz0,
+                                  const R *rz1, const R *rz2, R *ubar_t1, const R *vbar_t1,
+                                  const R *rub0, const R *rub1, R *vbar_t2, cudaStream_t s);
+    static cudaError_t bc_apply(const sf_ctx *c, const BcProgram &p1, R *f1,
+                                const BcProgram &p2, R *f2, double val, cudaStream_t s);
+    static cudaError_t rhs3d(const sf_ctx *c, const R *u, const R *v, const R *Huon,
+                             const R *Hvom, const R *W, const R *Hz, R *ru, R *rv,
+                             cudaStream_t s);
+    static cudaError_t maxflux_omega(const sf_ctx *c, const R *u, const R *v, R *Huon, R *Hvom,
+                                     const R *Hz, R *W, const R *z_w, int do_flux, int do_omega,
+                                     R *zeta1, R *zeta2, const double *Zt, cudaStream_t s);
+    static cudaError_t set_zeta(const sf_ctx *c, R *z1, R *z2, const double *Zt, cudaStream_t s);
+    static cudaError_t set_depth(const sf_ctx *c, const double *Zt, R *z_w, R *z_r, R *Hz,
+                                 cudaStream_t s);
+    static cudaError_t step3d_uv(const sf_ctx *c, R *u, R *v, const R *ru, const R *rv,
+                                 R *ubar_t1, R *vbar_t1, R *ubar_t2, R *vbar_t2, const R *Hz,
+                                 const R *Akv, const R *z_r, const double *DU, const double *DV,
+                                 const R *tmpU, const R *tmpV, double cff, double lambda,
+                                 double Dt, int do_bc, double bcval, cudaStream_t s);
+    static cudaError_t lateral_uv_bc(const sf_ctx *c, R *u, R *v, double val, cudaStream_t s);
+};
+
+extern template struct Ops<double>;
+extern template struct Ops<float>;
+
+}  // namespace sf

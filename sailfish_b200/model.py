@@ -1,0 +1,260 @@
+"""Device model: grid context, ocean state in HBM and the baroclinic step driver.
+
+``Model.step()`` runs one step of the reference's 3D driver (nonlinear/main3d.py:118-324):
+
+    set_maxflux + omega + set_zeta      sf_maxflux_omega        (main3d.py:118-151)
+    rhs3d                               sf_rhs3d                (main3d.py:159, rhs.py:16-93)
+    barotropic loop, nfast+1 substeps   sf_barotropic_loop      (main3d.py:166-189)
+    set_depth                           sf_set_depth            (main3d.py:290)
+    step3d_UV + setLateralUVBCs         sf_step3d_uv_bc         (main3d.py:304-311)
+    omega                               sf_omega                (main3d.py:321)
+
+Layout in HBM: the reference's flat C-order fields.  The three barotropic time slots of each
+2D field live in one (3, M+1, L+1) buffer and rotate by pointer (cycleTimes2D); the 3D
+fields u, v, ru, rv keep only the slot the reference uses (its cycleTimes3D is never called,
+so its other two slots are never read or written).
+"""
+import ctypes
+
+import numpy as np
+import torch
+
+from . import host
+from ._lib import lib, check, GridDesc, State2D, SF_FP64, SF_FP32
+
+DTYPES = {"fp64": (SF_FP64, torch.float64, np.float64), "fp32": (SF_FP32, torch.float32, np.float32)}
+
+
+def _i32(a):
+    return np.ascontiguousarray(np.asarray(a).ravel(), dtype=np.int32)
+
+
+def _f64(a):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float64).ravel())
+
+
+class Grid:
+    """Horizontal grid, metrics and vertical coordinate (host FP64 arrays)."""
+
+    def __init__(self, L, M, N, h, pm, pn, on_u, om_v, fomn, sc_r, sc_w, Cs_r, Cs_w, hc,
+                 Vtransform):
+        self.L, self.M, self.N = int(L), int(M), int(N)
+        self.I, self.J = self.L + 1, self.M + 1
+        self.s2 = self.I * self.J
+        shp = (self.J, self.I)
+        self.h, self.pm, self.pn, self.on_u, self.om_v, self.fomn = (
+            np.asarray(a, np.float64).reshape(shp) for a in (h, pm, pn, on_u, om_v, fomn))
+        self.sc_r, self.sc_w, self.Cs_r, self.Cs_w = (_f64(a) for a in (sc_r, sc_w, Cs_r, Cs_w))
+        self.hc = float(hc)
+        self.Vtransform = int(Vtransform)
+
+    @classmethod
+    def analytic(cls, Lm, Mm, N, h, dx, dy, f, Vtransform=2, Vstretching=4, theta_s=5.0,
+                 theta_b=0.4, tcline=100.0):
+        """Grid from rho-point depth h and Coriolis f ((Mm+2) x (Lm+2) arrays or scalars) on
+        uniform spacing dx, dy, with the reference's metric and S-coordinate routines."""
+        L, M = Lm + 1, Mm + 1
+        shp = (M + 1, L + 1)
+        h = np.broadcast_to(np.asarray(h, np.float64), shp).copy()
+        f = np.broadcast_to(np.asarray(f, np.float64), shp).copy()
+        pm = np.full(shp, 1.0 / dx)
+        pn = np.full(shp, 1.0 / dy)
+        m = host.update_metrics(pm, pn, f)
+        sc_r, sc_w, Cs_r, Cs_w = host.set_coords(N, Vstretching, theta_s, theta_b)
+        hc = min(h.min(), tcline) if Vtransform == 1 else tcline   # set_coords.py:355-359
+        g = cls(L, M, N, h, pm, pn, m["on_u"], m["om_v"], m["fomn"], sc_r, sc_w, Cs_r, Cs_w, hc,
+                Vtransform)
+        g.f = f
+        return g
+
+
+class Context:
+    """An sf_ctx: the grid snapshot and boundary programs on the current CUDA device."""
+
+    def __init__(self, grid, boundary, precision="fp64"):
+        if precision not in DTYPES:
+            raise ValueError("precision must be 'fp64' or 'fp32'")
+        self.precision = precision
+        self.grid = grid
+        B = boundary
+        keep = {}
+
+        def dp(name, a):
+            keep[name] = _f64(a)
+            return keep[name].ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+        def ip(name, a):
+            keep[name] = _i32(a)
+            return keep[name].ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), int(keep[name].size)
+
+        d = GridDesc()
+        d.L, d.M, d.N, d.precision = grid.L, grid.M, grid.N, DTYPES[precision][0]
+        for k in ("h", "pm", "pn", "on_u", "om_v", "fomn", "sc_r", "sc_w", "Cs_r", "Cs_w"):
+            setattr(d, k, dp(k, getattr(grid, k)))
+        d.hc, d.Vtransform = grid.hc, grid.Vtransform
+        d.zeta_field_idx2 = ip("zf", B.zetaBC.bcIdxFieldIdx2)[0]
+        d.uvel_field_type = ip("ut", B.uvelBC.bcIdxFieldType)[0]
+        d.vvel_field_type = ip("vt", B.vvelBC.bcIdxFieldType)[0]
+        d.zeta_copy_idx1, d.n_zeta_copy = ip("z1", B.zetaClosedOrGradientBCIdx1)
+        d.zeta_copy_idx2 = ip("z2", B.zetaClosedOrGradientBCIdx2)[0]
+        d.ubar_closed_idx, d.n_ubar_closed = ip("uc", B.ubarClosedBCIdx1)
+        d.vbar_closed_idx, d.n_vbar_closed = ip("vc", B.vbarClosedBCIdx1)
+        d.ubar_clamped_idx, d.n_ubar_clamped = ip("ucl", B.ubarClampedBCIdx1)
+        d.ubar_grad_idx1, d.n_ubar_grad = ip("ug1", B.ubarGradientBCIdx1)
+        d.ubar_grad_idx2 = ip("ug2", B.ubarGradientBCIdx2)[0]
+        d.vbar_grad_idx1, d.n_vbar_grad = ip("vg1", B.vbarGradientBCIdx1)
+        ptr = ctypes.c_void_p()
+        check(lib.sf_ctx_create(ctypes.byref(d), ctypes.byref(ptr)), "sf_ctx_create")
+        self.ptr = ptr
+
+    def close(self):
+        if getattr(self, "ptr", None):
+            lib.sf_ctx_destroy(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def stream_handle():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+class Model:
+    """Ocean state in HBM and the reference's baroclinic step, run by libsailfish_b200."""
+
+    NAMES2 = ("zeta", "ubar", "vbar", "rzeta", "rubar", "rvbar")
+    NAMES3 = ("u", "v", "ru", "rv", "W", "Huon", "Hvom", "AKv")
+
+    def __init__(self, grid, boundary, dt, ndtfast, precision="fp64", lam=1.0, device="cuda"):
+        self.grid = grid
+        self.ctx = Context(grid, boundary, precision)
+        self.precision = precision
+        self.tdtype = DTYPES[precision][1]
+        self.dt, self.ndtfast = float(dt), int(ndtfast)
+        self.dtfast = self.dt / self.ndtfast
+        self.nfast, self.weight1, self.weight2 = host.set_weights(self.ndtfast)
+        self._w1 = np.ascontiguousarray(self.weight1)
+        self.lam = float(lam)
+        self.iic, self.ntfirst = 0, 0
+        self.time, self.time2D = 0.0, 0.0
+        J, I, N = grid.J, grid.I, grid.N
+        z = lambda *s, dt=None: torch.zeros(*s, dtype=dt or self.tdtype, device=device)
+        for n in self.NAMES2:
+            setattr(self, n, z(3, J, I))
+        for n in self.NAMES3:
+            setattr(self, n, z(N + 1, J, I))
+        self.AKv.fill_(0.001)                     # modules/mod_ocean.py:91
+        for n in ("Zt_avg1", "DU_avg1", "DV_avg1"):
+            setattr(self, n, z(J * I, dt=torch.float64))
+        self.z_w = z(N + 1, J, I)
+        self.z_r = z(N, J, I)
+        self.Hz = z(N, J, I)
+        self.slots = [0, 1, 2]                    # (t0, t1, t2) rows of the 2D buffers
+        self._started = False
+
+    # -- state I/O ------------------------------------------------------------------------
+    def load(self, state):
+        """Copy host arrays in the reference's shapes into the device state.  3D fields may be
+        given as (3, N+1, M+1, L+1) parents, in which case their slot 2 is used."""
+        for n, a in state.items():
+            a = np.asarray(a)
+            t = getattr(self, n)
+            if n in ("u", "v", "ru", "rv") and a.ndim == 4:
+                a = a[2]
+            t.copy_(torch.from_numpy(np.ascontiguousarray(a).reshape(t.shape)).to(t.dtype))
+
+    def state(self):
+        out = {}
+        for n in self.NAMES2 + self.NAMES3 + ("Zt_avg1", "DU_avg1", "DV_avg1", "z_w", "z_r", "Hz"):
+            out[n] = getattr(self, n).double().cpu().numpy()
+        out["slots"] = list(self.slots)
+        return out
+
+    # -- pointers ---------------------------------------------------------------------------
+    def _p(self, t):
+        return ctypes.c_void_p(t.data_ptr())
+
+    def _slot(self, name, k):
+        return getattr(self, name)[self.slots[k]]
+
+    def state2d(self):
+        s = State2D()
+        for n in self.NAMES2:
+            arr = getattr(s, n)
+            for k in range(3):
+                arr[k] = self._slot(n, k).data_ptr()
+        s.Zt_avg1, s.DU_avg1, s.DV_avg1 = (self.Zt_avg1.data_ptr(), self.DU_avg1.data_ptr(),
+                                           self.DV_avg1.data_ptr())
+        return s
+
+    def _sync_slots(self, s):
+        base = {n: getattr(self, n).data_ptr() for n in self.NAMES2}
+        row = self.grid.s2 * self.zeta.element_size()
+        new = [(s.zeta[k] - base["zeta"]) // row for k in range(3)]
+        for n in self.NAMES2[1:]:
+            assert [(getattr(s, n)[k] - base[n]) // row for k in range(3)] == new
+        self.slots = new
+
+    # -- steps -------------------------------------------------------------------------------
+    def set_depth(self, stream=None):
+        st = stream or stream_handle()
+        check(lib.sf_set_depth(self.ctx.ptr, self._p(self.Zt_avg1), self._p(self.z_w),
+                               self._p(self.z_r), self._p(self.Hz), st), "sf_set_depth")
+
+    def start(self):
+        """main3d.py:62: depths from the initial Zt_avg1."""
+        self.set_depth()
+        self._started = True
+
+    def step(self, nsteps=1, final_omega=True, timer=None):
+        """`nsteps` baroclinic steps (main3d.py:118-324).  The end-of-step omega
+        (main3d.py:321) is recomputed at the start of every following step, so only the last
+        one is evaluated unless `final_omega` is False (then none).  `timer(name)`, if given,
+        returns a pair of CUDA events recorded around each phase."""
+        if not self._started:
+            self.start()
+        c, p = self.ctx.ptr, self._p
+        st = stream_handle()
+        cs = torch.cuda.current_stream()
+
+        def phase(name, fn):
+            if timer is None:
+                return fn()
+            a, b = timer(name)
+            a.record(cs)
+            r = fn()
+            b.record(cs)
+            return r
+
+        for k in range(nsteps):
+            z1, z2 = self._slot("zeta", 1), self._slot("zeta", 2)
+            phase("k_maxflux_omega", lambda: check(lib.sf_maxflux_omega(
+                c, p(self.u), p(self.v), p(self.Huon), p(self.Hvom), p(self.Hz), p(self.W),
+                p(self.z_w), p(z1), p(z2), p(self.Zt_avg1), st), "sf_maxflux_omega"))
+            phase("k_rhs3d", lambda: check(lib.sf_rhs3d(
+                c, p(self.u), p(self.v), p(self.Huon), p(self.Hvom), p(self.W), p(self.Hz),
+                p(self.ru), p(self.rv), st), "sf_rhs3d"))
+            s = self.state2d()
+            t2 = ctypes.c_double(self.time2D)
+            phase("barotropic_loop", lambda: check(lib.sf_barotropic_loop(
+                c, ctypes.byref(s), self.nfast + 1,
+                self._w1.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), self.dtfast,
+                ctypes.byref(t2), st), "sf_barotropic_loop"))
+            self._sync_slots(s)
+            self.time2D = t2.value
+            phase("k_set_depth", lambda: self.set_depth(st))
+            phase("k_step3d_uv", lambda: check(lib.sf_step3d_uv_bc(
+                c, p(self.u), p(self.v), p(self.ru), p(self.rv), p(self._slot("ubar", 1)),
+                p(self._slot("vbar", 1)), p(self._slot("ubar", 2)), p(self._slot("vbar", 2)),
+                p(self.Hz), p(self.AKv), p(self.z_r), p(self.DU_avg1), p(self.DV_avg1), self.iic,
+                self.ntfirst, self.lam, self.dt, self.time, st), "sf_step3d_uv_bc"))
+            if final_omega and k == nsteps - 1:
+                phase("k_omega", lambda: check(lib.sf_omega(
+                    c, p(self.W), p(self.Huon), p(self.Hvom), p(self.z_w), st), "sf_omega"))
+            self.iic += 1                          # CompTimes.nextTimeStep
+            self.time += self.dt
+            self.time2D = self.time

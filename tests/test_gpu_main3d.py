@@ -1,0 +1,67 @@
+"""The whole time step on the GPU against the reference's own main3d runs.
+
+FP64: bit-exact (the FP64 kernels are built without FMA contraction and evaluate every
+expression as the reference does).  FP32: stencils in FP32 with FP64 accumulators; the
+error is stated against the reference run.
+"""
+import numpy as np
+import pytest
+
+from golden_io import load, boundary_dict
+from sailfish_b200 import host
+
+NAMES = ("zeta", "ubar", "vbar", "rzeta", "rubar", "rvbar", "u", "v", "ru", "rv", "W", "Huon",
+         "Hvom", "Zt_avg1", "DU_avg1", "DV_avg1", "AKv")
+
+
+def golden_model(tag, precision):
+    from sailfish_b200.model import Grid, Model
+    d = load("main3d_%s.npz" % tag)
+    L, M, N = int(d["in_L"]), int(d["in_M"]), int(d["in_N"])
+    g = lambda k: d["in_grid_" + k]
+    grid = Grid(L, M, N, g("h"), g("pm"), g("pn"), g("on_u"), g("om_v"), g("fomn"), g("sc_r"),
+                g("sc_w"), g("Cs_r"), g("Cs_w"), float(g("hc")), int(d["in_Vtransform"]))
+    B = host.Boundary(L, M)
+    ref_b = boundary_dict(d, "in_bnd_")
+    np.testing.assert_array_equal(B.zetaClosedOrGradientBCIdx1, ref_b["zetaClosedOrGradientBCIdx1"])
+    np.testing.assert_array_equal(B.uvelBC.bcIdxFieldType, ref_b["uvelBC_bcIdxFieldType"])
+    m = Model(grid, B, float(d["in_dt"]), int(d["in_ndtfast"]), precision=precision)
+    assert m.nfast == int(d["in_nfast"])
+    m.load({n: d["in_" + n] for n in NAMES})
+    return m, d
+
+
+def out_of(d, n, slots=None):
+    a = d["out_" + n]
+    if n in ("u", "v", "ru", "rv"):
+        a = a[2]
+    return a
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("tag", ["square", "nonsquare", "vt1"])
+def test_main3d_fp64_bit_exact(tag):
+    m, d = golden_model(tag, "fp64")
+    m.step(int(d["in_nsteps"]))
+    s = m.state()
+    for n in ("zeta", "ubar", "vbar", "rzeta", "rubar", "rvbar"):
+        assert s["slots"] == list(d["out_slots_" + n])
+    for n in NAMES + ("z_w", "z_r", "Hz"):
+        np.testing.assert_array_equal(s[n].reshape(-1), out_of(d, n).reshape(-1), err_msg=n)
+    assert m.iic == int(d["out_iic"]) and m.time == float(d["out_time"])
+
+
+@pytest.mark.gpu
+def test_main3d_fp32_error_stated():
+    m, d = golden_model("square", "fp32")
+    m.step(int(d["in_nsteps"]))
+    s = m.state()
+    # Relative to each field's largest magnitude: FP32 stencils with FP64 accumulators.
+    tol = {"zeta": 2e-5, "ubar": 2e-5, "vbar": 2e-5, "u": 2e-4, "v": 2e-4, "Zt_avg1": 2e-5,
+           "DU_avg1": 2e-5, "DV_avg1": 2e-5, "z_w": 1e-6, "Hz": 1e-5}
+    for n, t in tol.items():
+        ref = out_of(d, n).reshape(-1)
+        got = s[n].reshape(-1)
+        scale = max(np.abs(ref).max(), 1e-30)
+        err = np.abs(got - ref).max() / scale
+        assert err <= t, "%s: max error %.3g of field scale (tolerance %.1g)" % (n, err, t)

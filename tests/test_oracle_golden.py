@@ -38,3 +38,21 @@ def test_oracle_main3d_matches_reference(tag):
         np.testing.assert_array_equal(getattr(grid, n).reshape(-1), d["out_" + n].reshape(-1), err_msg=n)
     assert ct.iic == int(d["out_iic"]) and ct.time == float(d["out_time"])
     assert ct.time2D == float(d["out_time2D"])
+
+
+def test_reference_driver_matches_reference_main3d():
+    """oracle/ref_driver.py (the reference's own kernels in main3d order, used as the timed CPU
+    baseline) reproduces the reference's main3d run."""
+    import ref_driver
+    if not ref_driver.available():
+        pytest.skip("oracle/_ref not built")
+    d = load("main3d_square.npz")
+    grid = _grid_from(d)
+    B = orc.Boundary(boundary_dict(d, "in_bnd_"))
+    names = ("zeta", "ubar", "vbar", "rzeta", "rubar", "rvbar", "u", "v", "ru", "rv", "W", "Huon",
+             "Hvom", "Zt_avg1", "DU_avg1", "DV_avg1", "AKv")
+    O = orc.Ocean(grid, {n: d["in_" + n] for n in names})
+    ct = orc.CompTimes(float(d["in_dt"]), int(d["in_ndtfast"]), int(d["in_nfast"]), d["in_w1"], d["in_w2"])
+    ref_driver.main3d(grid, B, O, ct, int(d["in_nsteps"]), omp=1)
+    for n in names:
+        np.testing.assert_array_equal(getattr(O, n).reshape(-1), d["out_" + n].reshape(-1), err_msg=n)
