@@ -103,10 +103,35 @@ int make_program(sf::BcProgram &p, const std::vector<BcOp> &ops, long s2) {
     std::vector<int> d, s;
     int rc = resolve(ops, s2, d, s);
     if (rc) return rc;
-    p.n = (int)d.size();
-    rc = upload(&p.dst, d.data(), d.size(), "boundary program");
-    if (rc) return rc;
-    return upload(&p.src, s.data(), s.size(), "boundary program");
+    // Partition (see sf::BcProgram): chained = entries reading another entry's destination,
+    // plus the entries writing those destinations.
+    std::unordered_map<int, int> dst_of;
+    for (size_t k = 0; k < d.size(); ++k) dst_of[d[k]] = (int)k;
+    std::vector<char> ch(d.size(), 0);
+    for (size_t k = 0; k < d.size(); ++k)
+        if (s[k] >= 0 && dst_of.count(s[k])) {
+            ch[k] = 1;
+            ch[dst_of[s[k]]] = 1;
+        }
+    std::vector<int> di, si, dc, sc;
+    for (size_t k = 0; k < d.size(); ++k) {
+        if (ch[k]) {
+            dc.push_back(d[k]);
+            sc.push_back(s[k]);
+        } else {
+            di.push_back(d[k]);
+            si.push_back(s[k]);
+        }
+    }
+    if ((int)dc.size() > sf::kMaxChained)
+        return fail(SF_EUNSUPPORTED, "boundary lists with more than 32 chained entries");
+    p.n = (int)di.size();
+    p.nch = (int)dc.size();
+    rc = upload(&p.dst, di.data(), di.size(), "boundary program");
+    if (!rc) rc = upload(&p.src, si.data(), si.size(), "boundary program");
+    if (!rc) rc = upload(&p.dst_ch, dc.data(), dc.size(), "boundary program");
+    if (!rc) rc = upload(&p.src_ch, sc.data(), sc.size(), "boundary program");
+    return rc;
 }
 
 void free_ctx(sf_ctx *c) {
@@ -120,6 +145,8 @@ void free_ctx(sf_ctx *c) {
     for (sf::BcProgram *p : {&c->zbc, &c->ubc, &c->vbc}) {
         cudaFree(p->dst);
         cudaFree(p->src);
+        cudaFree(p->dst_ch);
+        cudaFree(p->src_ch);
     }
     delete c;
 }
@@ -223,12 +250,6 @@ int sf_ctx_create(const sf_grid_desc *d, sf_ctx **out) {
                           {{d->vbar_closed_idx, nullptr, d->n_vbar_closed, -1},
                            {d->vbar_grad_idx1, d->ubar_grad_idx2, d->n_vbar_grad, 0}},
                           c->s2);
-    if (rc == SF_OK) {
-        const size_t bytes = (size_t)(c->ubc.n + c->vbc.n) * (c->prec == SF_FP64 ? 8 : 4);
-        const size_t zbytes = (size_t)c->zbc.n * (c->prec == SF_FP64 ? 8 : 4);
-        if (bytes > 200 * 1024 || zbytes > 200 * 1024)
-            rc = fail(SF_EUNSUPPORTED, "boundary programs larger than one block's shared memory");
-    }
     if (rc != SF_OK) {
         free_ctx(c);
         return rc;

@@ -12,10 +12,17 @@ namespace sf {
 // (setBC / copyBC, modules/mod_BC.c:6-23, run one after the other in thread order) reduced to
 // a gather dst[k] <- src[k], where src >= 0 is a node of the field as it was before the
 // program ran, src == -1 is the constant 0 and src == -2 is the time-dependent value.
+// Entries whose source is another entry's destination (and those destinations) form the
+// short "chained" list, applied by one thread that reads all its sources before writing;
+// all other entries are independent and applied by one thread each.
+constexpr int kMaxChained = 32;
 struct BcProgram {
-    int n = 0;
-    int *dst = nullptr;  // device
-    int *src = nullptr;  // device
+    int n = 0;                 // independent entries
+    int *dst = nullptr;        // device
+    int *src = nullptr;        // device
+    int nch = 0;               // chained entries
+    int *dst_ch = nullptr;     // device
+    int *src_ch = nullptr;     // device
 };
 
 // Grid view handed to kernels by value.

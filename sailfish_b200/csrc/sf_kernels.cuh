@@ -178,118 +178,204 @@ __global__ void __launch_bounds__(kBlock) k_corr_point(
     if (vbar_t2) vbar_t2[p] = R(0);
 }
 
-// Boundary programs (see BcProgram): one block, gather everything, barrier, scatter.
+// Boundary programs (see BcProgram): independent entries one per thread over as many blocks
+// as needed; the chained entries by thread 0 of block 0, all reads before all writes.
 template <typename R>
-__global__ void __launch_bounds__(1024) k_bc_apply(int n1, const int *__restrict__ d1,
-                                                   const int *__restrict__ s1, R *f1, int n2,
-                                                   const int *__restrict__ d2,
-                                                   const int *__restrict__ s2, R *f2, R val) {
-    extern __shared__ unsigned char smem_raw[];
-    R *buf = reinterpret_cast<R *>(smem_raw);
-    for (int k = threadIdx.x; k < n1; k += blockDim.x) {
-        const int s = s1[k];
-        buf[k] = s >= 0 ? f1[s] : (s == -1 ? R(0) : val);
+__device__ __forceinline__ R bc_value(const R *f, int s, R val) {
+    return s >= 0 ? f[s] : (s == -1 ? R(0) : val);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_bc_apply(BcProgram p1, R *f1, BcProgram p2, R *f2, R val) {
+    const long t = tid_flat();
+    if (t < p1.n) {
+        f1[p1.dst[t]] = bc_value(f1, p1.src[t], val);
+    } else if (t < (long)p1.n + p2.n) {
+        const long k = t - p1.n;
+        f2[p2.dst[k]] = bc_value(f2, p2.src[k], val);
     }
-    for (int k = threadIdx.x; k < n2; k += blockDim.x) {
-        const int s = s2[k];
-        buf[n1 + k] = s >= 0 ? f2[s] : (s == -1 ? R(0) : val);
+    if (t == 0) {
+        R buf[kMaxChained];
+        for (int k = 0; k < p1.nch; ++k) buf[k] = bc_value(f1, p1.src_ch[k], val);
+        for (int k = 0; k < p1.nch; ++k) f1[p1.dst_ch[k]] = buf[k];
+        for (int k = 0; k < p2.nch; ++k) buf[k] = bc_value(f2, p2.src_ch[k], val);
+        for (int k = 0; k < p2.nch; ++k) f2[p2.dst_ch[k]] = buf[k];
     }
-    __syncthreads();
-    for (int k = threadIdx.x; k < n1; k += blockDim.x) f1[d1[k]] = buf[k];
-    for (int k = threadIdx.x; k < n2; k += blockDim.x) f2[d2[k]] = buf[n1 + k];
 }
 
 // ------------------------------------------------------------------------------------------
 // 3D right-hand side (nonlinear/rhs.py:16-93): ru = rv = 0, addCoriolis (rhs_kernels.cpp:7-35),
 // horizontalAdvection (:71-132), verticalAdvection (:136-196), one thread per column.
 // ------------------------------------------------------------------------------------------
+
+// Tiled form: a block owns a TX x TY tile of rho points and marches over the levels; at each
+// level the tile of u, v, Huon, Hvom, Hz (level K) and W (level K+1) is staged in shared memory
+// with a halo of rows j-3..j+2 and columns i-2..i+2.  The halo is addressed by flat index
+// (j0+r)*I + (i0+c), so columns beyond the row ends wrap into the neighbouring rows exactly as
+// the reference's flat-index stencils do; reads before the array start or past its end stage 0.
+constexpr int kTX = 32, kTY = 8;
+constexpr int kHY0 = 3, kHY1 = 2, kHX0 = 2, kHX1 = 2;          // halo extents
+constexpr int kSX = kTX + kHX0 + kHX1, kSY = kTY + kHY0 + kHY1;  // staged tile 36 x 13
+constexpr int kSN = kSX * kSY;
+
 template <typename R>
-struct Hadv {
-    // Evaluates horizontalAdvection's ru and rv increments at flat node p of level base K.
-    const R *U, *V, *HU, *HV;   // level-K pointers (may be indexed below 0 at K = 0)
-    long I;
-    bool lo;                    // level 0: guard reads before the array start
-    long base;                  // K*s2, for the guard
-    __device__ __forceinline__ R u_(long q) const { return lo ? ldz(U - base, base + q) : U[q]; }
-    __device__ __forceinline__ R v_(long q) const { return lo ? ldz(V - base, base + q) : V[q]; }
-    __device__ __forceinline__ R hu(long q) const { return lo ? ldz(HU - base, base + q) : HU[q]; }
-    __device__ __forceinline__ R hv(long q) const { return lo ? ldz(HV - base, base + q) : HV[q]; }
-    __device__ __forceinline__ R uR(long q) const { return (u_(q) + u_(q + 1)) * R(0.5); }
-    __device__ __forceinline__ R uP(long q) const { return (u_(q) + u_(q - 1)) * R(0.5); }
-    __device__ __forceinline__ R vR(long q) const { return (v_(q) + v_(q + I)) * R(0.5); }
-    __device__ __forceinline__ R vP(long q) const { return (v_(q) + v_(q - I)) * R(0.5); }
-    __device__ __forceinline__ R huR(long q) const { return (hu(q) + hu(q + 1)) * R(0.5); }
-    __device__ __forceinline__ R huP(long q) const { return (hu(q) + hu(q - 1)) * R(0.5); }
-    __device__ __forceinline__ R hvP(long q) const { return (hv(q) + hv(q - I)) * R(0.5); }
-    __device__ __forceinline__ R hvR(long q) const { return (hv(q) + hv(q + I)) * R(0.5); }
-    __device__ __forceinline__ R dxxU(long q) const { return (u_(q - 1) - R(2.0) * u_(q)) + u_(q + 1); }
-    __device__ __forceinline__ R deeU(long q) const { return (u_(q - I) - R(2.0) * u_(q)) + u_(q + I); }
-    __device__ __forceinline__ R dxxHU(long q) const { return (hu(q - 1) - R(2.0) * hu(q)) + hu(q + 1); }
-    __device__ __forceinline__ R deeHU(long q) const { return (hu(q - I) - R(2.0) * hu(q)) + hu(q + I); }
-    __device__ __forceinline__ R dxxHV(long q) const { return (hv(q - 1) - R(2.0) * hv(q)) + hv(q + 1); }
-    __device__ __forceinline__ R deeHV(long q) const { return (hv(q - I) - R(2.0) * hv(q)) + hv(q + I); }
-    // upwindUtoR(DxxUtoU(u), uR) and upwindUtoP(DeeUtoU(u), HvomP), mod_cppkernels.h:624,673
-    __device__ __forceinline__ R uxxR(long q) const { return (uR(q) + uR(q + 1) >= R(0)) ? dxxU(q) : dxxU(q + 1); }
-    __device__ __forceinline__ R ueeP(long q) const { return (hvP(q) + hvP(q - I) >= R(0)) ? deeU(q) : deeU(q - I); }
-    __device__ __forceinline__ R huxxR(long q) const { return (dxxHU(q) + dxxHU(q + 1)) * R(0.5); }
-    __device__ __forceinline__ R hueeP(long q) const { return (deeHU(q) + deeHU(q - 1)) * R(0.5); }
-    __device__ __forceinline__ R hvxxP(long q) const { return (dxxHV(q) + dxxHV(q - I)) * R(0.5); }
-    __device__ __forceinline__ R hveeR(long q) const { return (deeHV(q) + deeHV(q + I)) * R(0.5); }
-    // Fluxes as written at rhs_kernels.cpp:121-125 (Gadv = -0.5).
-    __device__ __forceinline__ R ufxR(long q) const { return uR(q) + (R(-0.5) * uxxR(q)) * (huR(q) + R(-0.5) * huxxR(q)); }
-    __device__ __forceinline__ R ufeP(long q) const { return uP(q) + (R(-0.5) * ueeP(q)) * (hvP(q) + R(-0.5) * hvxxP(q)); }
-    __device__ __forceinline__ R vfxP(long q) const { return vP(q) + (R(-0.5) * ueeP(q)) * (huP(q) + R(-0.5) * hueeP(q)); }
-    __device__ __forceinline__ R vfeR(long q) const { return vR(q) + (R(-0.5) * uxxR(q)) * (hvR(q) + R(-0.5) * hveeR(q)); }
-    __device__ __forceinline__ R du(long p) const { return (ufxR(p) - ufxR(p - 1)) + (ufeP(p) - ufeP(p - I)); }
-    __device__ __forceinline__ R dv(long p) const { return (vfxP(p) - vfxP(p - 1)) + (vfeR(p) - vfeR(p - I)); }
+struct Tile {
+    const R *t;
+    int base;   // index of the thread's own node in the staged tile
+    __device__ __forceinline__ R operator()(int dr, int dc) const { return t[base + dr * kSX + dc]; }
 };
 
+// Asynchronous staging (cp.async, completes in the background while the previous level is
+// computed); out-of-range elements are zero-filled by a zero source size.
+__device__ __forceinline__ void cp_async(float *dst, const float *src, bool ok) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src), "r"(ok ? 4 : 0));
+}
+__device__ __forceinline__ void cp_async(double *dst, const double *src, bool ok) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(ok ? 8 : 0));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int n>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(n)); }
+
 template <typename R>
-__global__ void __launch_bounds__(128) k_rhs3d(Geo<R> g, const R *__restrict__ u,
-                                               const R *__restrict__ v, const R *__restrict__ Huon,
-                                               const R *__restrict__ Hvom, const R *__restrict__ W,
-                                               const R *__restrict__ Hz, R *__restrict__ ru,
-                                               R *__restrict__ rv) {
-    const long p = tid_flat();
-    if (p >= g.s2) return;
+__device__ __forceinline__ void stage(R *dst, const R *src, long lvl_off, long len, long I, long j0,
+                                      long i0, int tid) {
+    for (int e = tid; e < kSN; e += kTX * kTY) {
+        const int r = e / kSX - kHY0, c = e % kSX - kHX0;
+        const long f = lvl_off + (j0 + r) * I + (i0 + c);
+        const bool ok = f >= 0 && f < len;
+        cp_async(dst + e, ok ? src + f : src, ok);
+    }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kTX *kTY) k_rhs3d(Geo<R> g, const R *__restrict__ u,
+                                                    const R *__restrict__ v, const R *__restrict__ Huon,
+                                                    const R *__restrict__ Hvom, const R *__restrict__ W,
+                                                    const R *__restrict__ Hz, R *__restrict__ ru,
+                                                    R *__restrict__ rv) {
+    __shared__ R sbuf[2][6][kSN];
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kTX + tx;
     const long I = g.I, s2 = g.s2;
     const int N = g.N;
-    const int i = (int)(p % I), j = (int)(p / I);
-    const bool rn = rnode_(i, j);
-    const bool va = g.bcfield[p] < 0 && inner_(i, j, g.I, g.J);   // rhs_kernels.cpp:144-149
-    const R c9 = R(9.0 / 16.0), c1 = R(1.0 / 16.0);
+    const long i0 = (long)blockIdx.x * kTX, j0 = (long)blockIdx.y * kTY;
+    const int i = (int)(i0 + tx), j = (int)(j0 + ty);
+    const bool live = i < g.I && j < g.J;
+    const long p = (long)j * I + i;
+    const long len3 = (long)(N + 1) * s2, lenHz = (long)N * s2;
+    const bool rn = live && rnode_(i, j);
+    const bool va = live && g.bcfield[p] < 0 && inner_(i, j, g.I, g.J);   // rhs_kernels.cpp:144-149
+    const R c9 = R(9.0 / 16.0), c1 = R(1.0 / 16.0), G = R(-0.5);
+    const int b = (ty + kHY0) * kSX + (tx + kHX0);
 
-    // Vertical-advection helpers: 4th-order interpolations (mod_cppkernels.h:723,745,767).
-#define AT(X, k) ((X)[(long)(k) * s2 + p])
-#define U4(X, k) (c9 * (AT(X, k) + AT(X, (k) + 1)) - c1 * (AT(X, (k) - 1) + AT(X, (k) + 2)))
-#define WU4(k) (c9 * (W[(long)(k) * s2 + p] + W[(long)(k) * s2 + p + 1]) - \
-                c1 * (W[(long)(k) * s2 + p - 1] + W[(long)(k) * s2 + p + 2]))
-#define WV4(k) (c9 * (W[(long)(k) * s2 + p] + W[(long)(k) * s2 + p + I]) - \
-                c1 * (W[(long)(k) * s2 + p - I] + W[(long)(k) * s2 + p + 2 * I]))
-    R ruN3 = R(0), rvN3 = R(0), ru1 = R(0), rv1 = R(0);
-    R fu_k = R(0), fv_k = R(0);   // Fsigma at level K (vertical advection, K >= 2)
-    R uuu = R(0), uuu2 = R(0);
+    // Own-column values for the vertical advection (rhs_kernels.cpp:158-194).
+#define COL(X, k) ((X)[(long)(k) * s2 + p])
+#define U4C(a, b_, c, d) (c9 * ((b_) + (c)) - c1 * ((a) + (d)))
+#define WU4G(k) (c9 * (W[(long)(k) * s2 + p] + W[(long)(k) * s2 + p + 1]) - \
+                 c1 * (W[(long)(k) * s2 + p - 1] + W[(long)(k) * s2 + p + 2]))
+#define WV4G(k) (c9 * (W[(long)(k) * s2 + p] + W[(long)(k) * s2 + p + I]) - \
+                 c1 * (W[(long)(k) * s2 + p - I] + W[(long)(k) * s2 + p + 2 * I]))
+    R uuu = R(0), uuu2 = R(0), fv1 = R(0), fv2 = R(0), fv3 = R(0), fu2 = R(0);
+    R uw0 = R(0), uw1 = R(0), uw2 = R(0), uw3 = R(0), vw0 = R(0), vw1 = R(0), vw2 = R(0), vw3 = R(0);
     if (va) {
-        uuu = (c9 * (AT(u, 0) + AT(u, 1)) - c1 * (0 + AT(u, 2))) * WU4(1);
-        uuu2 = (c9 * (0 + AT(u, 0)) - c1 * (0 + AT(u, 1))) * WU4(0);
+        uuu = (c9 * (COL(u, 0) + COL(u, 1)) - c1 * (0 + COL(u, 2))) * WU4G(1);
+        uuu2 = (c9 * (0 + COL(u, 0)) - c1 * (0 + COL(u, 1))) * WU4G(0);
+        fv1 = U4C(COL(v, 0), COL(v, 1), COL(v, 2), COL(v, 3)) * WV4G(1);
+        fv2 = U4C(COL(v, 1), COL(v, 2), COL(v, 3), COL(v, 4)) * WV4G(2);
+        fv3 = U4C(COL(v, 2), COL(v, 3), COL(v, 4), COL(v, 5)) * WV4G(3);
+        fu2 = U4C(COL(u, 1), COL(u, 2), COL(u, 3), COL(u, 4)) * WU4G(2);
+        uw0 = COL(u, 2); uw1 = COL(u, 3); uw2 = COL(u, 4); uw3 = COL(u, 5);   // u(K..K+3), K = 2
+        vw0 = COL(v, 2); vw1 = COL(v, 3); vw2 = COL(v, 4); vw3 = COL(v, 5);
     }
+    R fu_k = fu2, fv_k = fv2;
+    R ruN3 = R(0), rvN3 = R(0), rv1 = R(0);
+    const R fp = live ? g.fomn[p] : R(0);
+    const R fw = (live && p >= 1) ? g.fomn[p - 1] : R(0);
+    const R fs = (live && p >= I) ? g.fomn[p - I] : R(0);
+
+    auto issue = [&](int K) {
+        const long o = (long)K * s2;
+        R(*bf)[kSN] = sbuf[K & 1];
+        stage(bf[0], u, o, len3, I, j0, i0, tid);
+        stage(bf[1], v, o, len3, I, j0, i0, tid);
+        stage(bf[2], Huon, o, len3, I, j0, i0, tid);
+        stage(bf[3], Hvom, o, len3, I, j0, i0, tid);
+        stage(bf[4], Hz, o, lenHz, I, j0, i0, tid);
+        stage(bf[5], W, o + s2, len3, I, j0, i0, tid);
+        cp_async_commit();
+    };
+    issue(0);
     for (int K = 0; K < N; ++K) {
         const long o = (long)K * s2;
+        if (K + 1 < N) {
+            issue(K + 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        R(*bf)[kSN] = sbuf[K & 1];
+        const Tile<R> U{bf[0], b}, V{bf[1], b}, HU{bf[2], b}, HV{bf[3], b}, HZ{bf[4], b}, WW{bf[5], b};
+        // Every thread reaches both barriers of each level: the compute is predicated on
+        // `live` rather than skipped with `continue` (an aligned barrier must not diverge).
+        if (live) {
         R aru = R(0), arv = R(0);
-        if (rn) {   // addCoriolis
-            const R cffp = Hz[o + p] * g.fomn[p], cffw = Hz[o + p - 1] * g.fomn[p - 1];
-            const R cffs = Hz[o + p - I] * g.fomn[p - I];
-            const R UFp = cffp * ((v[o + p] + v[o + p + I]) * R(0.5));
-            const R UFw = cffw * ((v[o + p - 1] + v[o + p - 1 + I]) * R(0.5));
-            const R VFp = cffp * ((u[o + p] + u[o + p + 1]) * R(0.5));
-            const R VFs = cffs * ((u[o + p - I] + u[o + p - I + 1]) * R(0.5));
+        if (rn) {   // addCoriolis (rhs_kernels.cpp:7-35)
+            const R cffp = HZ(0, 0) * fp, cffw = HZ(0, -1) * fw, cffs = HZ(-1, 0) * fs;
+            const R UFp = cffp * ((V(0, 0) + V(1, 0)) * R(0.5));
+            const R UFw = cffw * ((V(0, -1) + V(1, -1)) * R(0.5));
+            const R VFp = cffp * ((U(0, 0) + U(0, 1)) * R(0.5));
+            const R VFs = cffs * ((U(-1, 0) + U(-1, 1)) * R(0.5));
             aru = aru + (UFp + UFw) * R(0.5);
             arv = arv - (VFp + VFs) * R(0.5);
         }
-        {   // horizontalAdvection
-            Hadv<R> a{u + o, v + o, Huon + o, Hvom + o, I, K == 0, o};
-            aru = aru - a.du(p);
-            arv = arv - a.dv(p);
+        {   // horizontalAdvection (rhs_kernels.cpp:93-130), node offsets relative to (j, i)
+#define UR(r, c) ((U(r, c) + U(r, (c) + 1)) * R(0.5))
+#define UP(r, c) ((U(r, c) + U(r, (c) - 1)) * R(0.5))
+#define VR(r, c) ((V(r, c) + V((r) + 1, c)) * R(0.5))
+#define VP(r, c) ((V(r, c) + V((r) - 1, c)) * R(0.5))
+#define HUR(r, c) ((HU(r, c) + HU(r, (c) + 1)) * R(0.5))
+#define HUP(r, c) ((HU(r, c) + HU(r, (c) - 1)) * R(0.5))
+#define HVP(r, c) ((HV(r, c) + HV((r) - 1, c)) * R(0.5))
+#define HVR(r, c) ((HV(r, c) + HV((r) + 1, c)) * R(0.5))
+#define DXX(T, r, c) (((T)(r, (c) - 1) - R(2.0) * (T)(r, c)) + (T)(r, (c) + 1))
+#define DEE(T, r, c) (((T)((r) - 1, c) - R(2.0) * (T)(r, c)) + (T)((r) + 1, c))
+#define UXXR(r, c) ((UR(r, c) + UR(r, (c) + 1) >= R(0)) ? DXX(U, r, c) : DXX(U, r, (c) + 1))
+#define UEEP(r, c) ((HVP(r, c) + HVP((r) - 1, c) >= R(0)) ? DEE(U, r, c) : DEE(U, (r) - 1, c))
+#define HUXXR(r, c) ((DXX(HU, r, c) + DXX(HU, r, (c) + 1)) * R(0.5))
+#define HUEEP(r, c) ((DEE(HU, r, c) + DEE(HU, r, (c) - 1)) * R(0.5))
+#define HVXXP(r, c) ((DXX(HV, r, c) + DXX(HV, (r) - 1, c)) * R(0.5))
+#define HVEER(r, c) ((DEE(HV, r, c) + DEE(HV, (r) + 1, c)) * R(0.5))
+            const R uxx00 = UXXR(0, 0), uxx0w = UXXR(0, -1), uxxs0 = UXXR(-1, 0);
+            const R uee00 = UEEP(0, 0), ueew = UEEP(0, -1), uees = UEEP(-1, 0);
+            const R ufx0 = UR(0, 0) + (G * uxx00) * (HUR(0, 0) + G * HUXXR(0, 0));
+            const R ufxw = UR(0, -1) + (G * uxx0w) * (HUR(0, -1) + G * HUXXR(0, -1));
+            const R ufe0 = UP(0, 0) + (G * uee00) * (HVP(0, 0) + G * HVXXP(0, 0));
+            const R ufes = UP(-1, 0) + (G * uees) * (HVP(-1, 0) + G * HVXXP(-1, 0));
+            const R vfx0 = VP(0, 0) + (G * uee00) * (HUP(0, 0) + G * HUEEP(0, 0));
+            const R vfxw = VP(0, -1) + (G * ueew) * (HUP(0, -1) + G * HUEEP(0, -1));
+            const R vfe0 = VR(0, 0) + (G * uxx00) * (HVR(0, 0) + G * HVEER(0, 0));
+            const R vfes = VR(-1, 0) + (G * uxxs0) * (HVR(-1, 0) + G * HVEER(-1, 0));
+            aru = aru - ((ufx0 - ufxw) + (ufe0 - ufes));
+            arv = arv - ((vfx0 - vfxw) + (vfe0 - vfes));
+#undef HVEER
+#undef HVXXP
+#undef HUEEP
+#undef HUXXR
+#undef UEEP
+#undef UXXR
+#undef DEE
+#undef DXX
+#undef HVR
+#undef HVP
+#undef HUP
+#undef HUR
+#undef VP
+#undef VR
+#undef UP
+#undef UR
         }
         // The reference's out-of-range threads (p >= s2) store 0 at flat p, i.e. into levels
         // >= 1, after the in-range threads (rhs_kernels.cpp:86-91).
@@ -301,17 +387,19 @@ __global__ void __launch_bounds__(128) k_rhs3d(Geo<R> g, const R *__restrict__ u
             if (K == 0) {
                 aru = aru - (uuu - uuu2);
             } else if (K == 1) {
-                const R f1 = U4(v, 1) * WV4(1), f2 = U4(v, 2) * WV4(2), f3 = U4(v, 3) * WV4(3);
-                arv -= c9 * (f1 + f2) - c1 * (f1 + f3);
-                fu_k = U4(u, 2) * WU4(2);
-                fv_k = f2;
-                aru = aru - (fu_k - uuu);
+                arv -= c9 * (fv1 + fv2) - c1 * (fv1 + fv3);
+                aru = aru - (fu2 - uuu);
             } else if (K <= N - 3) {
-                const R fu1 = U4(u, K + 1) * WU4(K + 1), fv1 = U4(v, K + 1) * WV4(K + 1);
+                const R u4 = K + 4 <= N ? COL(u, K + 4) : R(0), v4 = K + 4 <= N ? COL(v, K + 4) : R(0);
+                const R wu = c9 * (WW(0, 0) + WW(0, 1)) - c1 * (WW(0, -1) + WW(0, 2));
+                const R wv = c9 * (WW(0, 0) + WW(1, 0)) - c1 * (WW(-1, 0) + WW(2, 0));
+                const R fu1 = U4C(uw0, uw1, uw2, uw3) * wu, fv1_ = U4C(vw0, vw1, vw2, vw3) * wv;
                 aru = aru - (fu1 - fu_k);
-                arv = arv - (fv1 - fv_k);
+                arv = arv - (fv1_ - fv_k);
                 fu_k = fu1;
-                fv_k = fv1;
+                fv_k = fv1_;
+                uw0 = uw1; uw1 = uw2; uw2 = uw3; uw3 = u4;
+                vw0 = vw1; vw1 = vw2; vw2 = vw3; vw3 = v4;
             } else {
                 aru = ruN3;    // ru[N-2] = ru[N-3], ru[N-1] = ru[N-2] (:189-192)
                 arv = rvN3;
@@ -320,92 +408,88 @@ __global__ void __launch_bounds__(128) k_rhs3d(Geo<R> g, const R *__restrict__ u
                 ruN3 = aru;
                 rvN3 = arv;
             }
-            if (K == 1) {
-                ru1 = aru;
-                rv1 = arv;
-            }
+            if (K == 1) rv1 = arv;
         }
         ru[o + p] = aru;
         rv[o + p] = (va && K == 0) ? R(0) : arv;   // rv[0] is set from rv[1] below
+        }
+        __syncthreads();   // the buffer of level K is refilled for level K+2 next iteration
     }
+    if (!live) return;
     const long oN = (long)N * s2;
     ru[oN + p] = va ? ruN3 : R(0);   // ru_t2[:] = 0 (rhs.py:38); ru[N] = ru[N-2] (:193)
     rv[oN + p] = va ? rvN3 : R(0);
     if (va) rv[p] = rv1;             // rv[0] = rv[1] (:183)
-    (void)ru1;
-#undef WV4
-#undef WU4
-#undef U4
-#undef AT
+#undef WV4G
+#undef WU4G
+#undef U4C
+#undef COL
 }
 
 // ------------------------------------------------------------------------------------------
 // set_maxflux (step3D_uv.kernels.cpp:372-405) + omega (:62-165) + set_zeta (:294-310)
 // ------------------------------------------------------------------------------------------
 template <typename R>
-struct Flux {
-    // Huon/Hvom at flat index f (any level): recomputed when this kernel also writes it (the
-    // value is the one its owner thread stores), read from memory otherwise.
-    const Geo<R> *g;
-    const R *u, *v, *Hz, *Huon, *Hvom;
-    bool recompute;
-    __device__ __forceinline__ R hu(long f) const {
-        if (recompute) {
-            const long K = f / g->s2, q = f - K * g->s2;
-            const int i = (int)(q % g->I), j = (int)(q / g->I);
-            if (K < g->N && unode_(i, j))
-                return (((Hz[f] + Hz[f - 1]) * R(0.5)) * u[f]) * g->on_u[q];
-        }
-        return Huon[f];
-    }
-    __device__ __forceinline__ R hv(long f) const {
-        if (recompute) {
-            const long K = f / g->s2, q = f - K * g->s2;
-            const int i = (int)(q % g->I), j = (int)(q / g->I);
-            if (K < g->N && vnode_(i, j, g->J))
-                return (((Hz[f] + Hz[f - g->I]) * R(0.5)) * v[f]) * g->om_v[q];
-        }
-        return Hvom[f];
-    }
-};
-
-template <typename R>
 __global__ void __launch_bounds__(kBlock) k_maxflux_omega(
     Geo<R> g, const R *__restrict__ u, const R *__restrict__ v, R *Huon, R *Hvom,
     const R *__restrict__ Hz, R *__restrict__ W, const R *__restrict__ z_w, int do_flux,
     int do_omega, R *__restrict__ zeta1, R *__restrict__ zeta2, const double *__restrict__ Zt) {
-    const long p = tid_flat();
-    if (p >= g.s2) return;
+    const int pi = (int)tid_flat();
+    if (pi >= g.s2) return;
+    const long p = pi;
     const long I = g.I, s2 = g.s2;
     const int N = g.N;
-    const int i = (int)(p % I), j = (int)(p / I);
+    const int i = pi % g.I, j = pi / g.I;
+    const bool un = unode_(i, j), vn = vnode_(i, j, g.J);
     if (do_flux) {
-        if (unode_(i, j))
+        const R onu = g.on_u[p], omv = g.om_v[p];
+        if (un) {
+#pragma unroll 4
             for (int K = 0; K < N; ++K) {
                 const long o = (long)K * s2 + p;
-                Huon[o] = (((Hz[o] + Hz[o - 1]) * R(0.5)) * u[o]) * g.on_u[p];
+                Huon[o] = (((Hz[o] + Hz[o - 1]) * R(0.5)) * u[o]) * onu;
             }
-        if (vnode_(i, j, g.J))
+        }
+        if (vn) {
+#pragma unroll 4
             for (int K = 0; K < N; ++K) {
                 const long o = (long)K * s2 + p;
-                Hvom[o] = (((Hz[o] + Hz[o - I]) * R(0.5)) * v[o]) * g.om_v[p];
+                Hvom[o] = (((Hz[o] + Hz[o - I]) * R(0.5)) * v[o]) * omv;
             }
+        }
     }
     if (do_omega && g.bcfield[p] < 0) {
-        Flux<R> fx{&g, u, v, Hz, Huon, Hvom, do_flux != 0};
+        // Huon at p+1 and Hvom at p+I: recomputed where this kernel also writes them (the value
+        // their owner thread stores), read from memory elsewhere.  p+1 past the row end is the
+        // next row's column 0 and p+I past the last row is row 0 of the next level; neither is
+        // a U or V node.
+        const bool rc = do_flux != 0;
+        const bool ue = rc && i + 1 < g.I && unode_(i + 1, j);
+        const bool vnn = rc && j + 1 < g.J && vnode_(i, j + 1, g.J);
+        const bool uo = rc && un, vo = rc && vn;
+        const R onu_e = ue ? g.on_u[p + 1] : R(0), omv_n = vnn ? g.om_v[p + I] : R(0);
+        const R onu_p = uo ? g.on_u[p] : R(0), omv_p = vo ? g.om_v[p] : R(0);
+        R Wc[kNMax];
         R Wk = R(0);
-        W[p] = R(0);
+        Wc[0] = R(0);
+#pragma unroll 4
         for (int K = 1; K < N; ++K) {
             const long o = (long)K * s2 + p;
-            Wk = Wk - ((fx.hu(o + 1) - fx.hu(o)) + (fx.hv(o + I) - fx.hv(o)));
-            W[o] = Wk;
+            const R hue = ue ? (((Hz[o + 1] + Hz[o]) * R(0.5)) * u[o + 1]) * onu_e : Huon[o + 1];
+            const R hup = uo ? (((Hz[o] + Hz[o - 1]) * R(0.5)) * u[o]) * onu_p : Huon[o];
+            const R hvn = vnn ? (((Hz[o + I] + Hz[o]) * R(0.5)) * v[o + I]) * omv_n : Hvom[o + I];
+            const R hvp = vo ? (((Hz[o] + Hz[o - I]) * R(0.5)) * v[o]) * omv_p : Hvom[o];
+            Wk = Wk - ((hue - hup) + (hvn - hvp));
+            Wc[K] = Wk;
         }
         const R zbed = z_w[p];
         const R h = z_w[(long)(N - 1) * s2 + p] - zbed;
         const R Ws = Wk;
-        for (int K = N - 1; K > 0; --K) {
+        W[p] = R(0);
+#pragma unroll 4
+        for (int K = 1; K < N; ++K) {
             const long o = (long)K * s2 + p;
-            W[o] = W[o] - (Ws * (z_w[o] - zbed)) / h;
+            W[o] = Wc[K] - (Ws * (z_w[o] - zbed)) / h;
         }
         W[(long)N * s2 + p] = R(0);
     }
@@ -484,8 +568,10 @@ __device__ __forceinline__ void build_matrix(const Geo<R> &g, long p, long d, R 
 #define DZ(k) (((z_r[(long)(k) * s2 + p] - z_r[(long)((k) - 1) * s2 + p]) + \
                 (z_r[(long)(k) * s2 + p - d] - z_r[(long)((k) - 1) * s2 + p - d])) * R(0.5))
     c.FC[N - 1] = R(0);
+#pragma unroll 4
     for (int K = 0; K < N - 1; ++K) c.FC[K] = (cm * AKU(K)) / DZ(K + 1);
     c.RHS[0] = R(0);
+#pragma unroll 4
     for (int K = 1; K < N; ++K) {
         const R hzu = HZU(K);
         c.RHS[K] = hzu * (uold[(long)K * s2] + (cdt * (pmU * pnU)) * ru[(long)K * s2 + p]);
@@ -498,20 +584,36 @@ __device__ __forceinline__ void build_matrix(const Geo<R> &g, long p, long d, R 
 #undef HZU
 }
 
-// solveTri (:520-565); the solution goes to loc[0..N).
+// solveTri (:520-565): forward elimination in place, back substitution into out[k*s2] with
+// `sub` subtracted from every level (correctBaroclinicMeanVel, :512-515).
 template <typename R>
-__device__ __forceinline__ void solve_tri(int N, Column<R> &c, R *loc) {
+__device__ __forceinline__ void solve_tri(int N, long s2, Column<R> &c, R *out, R sub) {
     for (int k = 1; k < N; ++k) {
         const R w = c.FC[k - 1] / c.BD[k - 1];
         c.BD[k] = c.BD[k] - w * c.FC[k - 1];
         c.RHS[k] = c.RHS[k] - w * c.RHS[k - 1];
     }
     R x = c.RHS[N - 1] / c.BD[N - 1];
-    loc[N - 1] = x;
+    out[(long)(N - 1) * s2] = x - sub;
     for (int k = N - 2; k >= 0; --k) {
         x = (c.RHS[k] - c.FC[k] * x) / c.BD[k];
-        loc[k] = x;
+        out[(long)k * s2] = x - sub;
     }
+}
+
+// correctBaroclinicMeanVel's correction (:499-508), from the pre-step velocity `old`.
+template <typename R>
+__device__ __forceinline__ R mean_correction(int N, long s2, long p, long d, const R *Hz,
+                                             const R *old, double DUp, double on) {
+    double H = 0.0, Hu = 0.0;
+#pragma unroll 4
+    for (int K = 0; K < N; ++K) {
+        const long o = (long)K * s2 + p;
+        const R hzu = (Hz[o] + Hz[o - d]) * R(0.5);
+        H += (double)hzu;
+        Hu += (double)(old[(long)K * s2] * hzu);
+    }
+    return (R)((Hu - DUp / on) / H);
 }
 
 template <typename R>
@@ -530,56 +632,35 @@ __global__ void __launch_bounds__(128) k_step3d_uv(
     const bool un = unode_(i, j), vn = vnode_(i, j, g.J);
     if (un || vn) {
         Column<R> c;
-        R unew[kNMax], vnew[kNMax];
         const R *uo = (tmpU ? tmpU : u) + p;
         const R *vo = (tmpV ? tmpV : v) + p;
         if (un) {
+            const R udiff = mean_correction(N, s2, p, 1, Hz, uo, DU[p], (double)g.on_u[p]);
             build_matrix(g, p, 1, cff, Dt, lambda, c, Hz, Akv, z_r, uo, ru);
-            solve_tri(N, c, unew);
-            // correctBaroclinicMeanVel<ntU> (:475-517), against the pre-step velocity.
-            double H = 0.0, Hu = 0.0;
-            for (int K = 0; K < N; ++K) {
-                const long o = (long)K * s2 + p;
-                const R hzu = (Hz[o] + Hz[o - 1]) * R(0.5);
-                H += (double)hzu;
-                Hu += (double)(uo[(long)K * s2] * hzu);
-            }
-            const R udiff = (R)((Hu - DU[p] / (double)g.on_u[p]) / H);
-            for (int K = 0; K < N; ++K) unew[K] = unew[K] - udiff;
+            solve_tri(N, s2, c, u + p, udiff);
         }
-        if (vn) build_matrix(g, p, I, cff, Dt, lambda, c, Hz, Akv, z_r, vo, rv);
-        bool vsolved = false;
-        if (un) {   // solveTri is gated by isUNode for both directions (:525)
-            solve_tri(N, c, vnew);
-            vsolved = true;
-        }
+        R vdiff = R(0);
         if (vn) {
-            if (!vsolved)   // no solve at this node: the correction applies to v as it is
-                for (int K = 0; K < N; ++K) vnew[K] = v[(long)K * s2 + p];
-            double H = 0.0, Hv = 0.0;
-            for (int K = 0; K < N; ++K) {
-                const long o = (long)K * s2 + p;
-                const R hzv = (Hz[o] + Hz[o - I]) * R(0.5);
-                H += (double)hzv;
-                Hv += (double)(vo[(long)K * s2] * hzv);
-            }
-            const R vdiff = (R)((Hv - DV[p] / (double)g.om_v[p]) / H);
-            for (int K = 0; K < N; ++K) vnew[K] = vnew[K] - vdiff;
+            vdiff = mean_correction(N, s2, p, I, Hz, vo, DV[p], (double)g.om_v[p]);
+            build_matrix(g, p, I, cff, Dt, lambda, c, Hz, Akv, z_r, vo, rv);
         }
-        if (un)
-            for (int K = 0; K < N; ++K) u[(long)K * s2 + p] = unew[K];
-        if (un || vn)
-            if (vsolved || vn)
-                for (int K = 0; K < N; ++K) v[(long)K * s2 + p] = vnew[K];
+        if (un) {
+            // solveTri is gated by isUNode for both directions (:525): where p is a U node
+            // but not a V node it solves the U system left in the scratch a second time.
+            solve_tri(N, s2, c, v + p, vn ? vdiff : R(0));
+        } else {
+            for (int K = 0; K < N; ++K) v[(long)K * s2 + p] = v[(long)K * s2 + p] - vdiff;
+        }
         if (un) {   // adjustBarotropicVelocity (:408-469)
             double HU = 0.0, HV = 0.0, HuU = 0.0, HvV = 0.0;
+#pragma unroll 4
             for (int K = 0; K < N; ++K) {
                 const long o = (long)K * s2 + p;
                 const R hzu = (Hz[o] + Hz[o - 1]) * R(0.5), hzv = (Hz[o] + Hz[o - I]) * R(0.5);
                 HU += (double)hzu;
                 HV += (double)hzv;
-                HuU += (double)(hzu * unew[K]);
-                HvV += (double)(hzv * vnew[K]);
+                HuU += (double)(hzu * u[o]);
+                HvV += (double)(hzv * v[o]);
             }
             const double duo = DU[p] / (double)g.on_u[p], dvo = DV[p] / (double)g.om_v[p];
             const double uUpdate = (HuU - duo) / HU;
@@ -696,21 +777,16 @@ cudaError_t Ops<R>::corr_point(const sf_ctx *c, double Dt, R *zeta_t2, const R *
 template <typename R>
 cudaError_t Ops<R>::bc_apply(const sf_ctx *c, const BcProgram &p1, R *f1, const BcProgram &p2,
                              R *f2, double val, cudaStream_t s) {
-    const int n = p1.n + p2.n;
-    if (n == 0) return cudaSuccess;
-    const size_t smem = (size_t)n * sizeof(R);
-    if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(k_bc_apply<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)smem);
-        if (e != cudaSuccess) return e;
-    }
-    k_bc_apply<R><<<1, 1024, smem, s>>>(p1.n, p1.dst, p1.src, f1, p2.n, p2.dst, p2.src, f2, (R)val);
+    const long n = (long)p1.n + p2.n;
+    if (n == 0 && p1.nch == 0 && p2.nch == 0) return cudaSuccess;
+    k_bc_apply<R><<<blocks_for(n > 0 ? n : 1, 256), 256, 0, s>>>(p1, f1, p2, f2, (R)val);
     return cudaGetLastError();
 }
 template <typename R>
 cudaError_t Ops<R>::rhs3d(const sf_ctx *c, const R *u, const R *v, const R *Huon, const R *Hvom,
                           const R *W, const R *Hz, R *ru, R *rv, cudaStream_t s) {
-    k_rhs3d<R><<<blocks_for(c->s2, 128), 128, 0, s>>>(geo(c), u, v, Huon, Hvom, W, Hz, ru, rv);
+    const dim3 grid((c->I + kTX - 1) / kTX, (c->J + kTY - 1) / kTY), block(kTX, kTY);
+    k_rhs3d<R><<<grid, block, 0, s>>>(geo(c), u, v, Huon, Hvom, W, Hz, ru, rv);
     return cudaGetLastError();
 }
 template <typename R>
