@@ -66,6 +66,16 @@ typedef struct sf_grid_desc {
     const int32_t *vbar_grad_idx1; int n_vbar_grad;                   /* vbarGradientBCIdx1 */
 } sf_grid_desc;
 
+/* GLS closure parameters (generic length scale, Umlauf and Burchard 2003): exponents p, m, n,
+ * cmu0, c1, c2, c3- (stable), c3+ (unstable), Schmidt numbers sigk, sigp, floors Kmin, Pmin,
+ * background viscosities/diffusivities, surface and bottom roughness Zos, Zob (m) and the
+ * quadratic bottom-drag coefficient rdrag2.  The reference's input file sets the k-epsilon
+ * values (utility/test.in:326-381). */
+typedef struct sf_gls_params {
+    double p, m, n, cmu0, c1, c2, c3m, c3p, sigk, sigp, Kmin, Pmin;
+    double Akv_bak, Akt_bak, Akk_bak, Akp_bak, Zos, Zob, rdrag2;
+} sf_gls_params;
+
 /* Three time slots of the barotropic state, in (t0, t1, t2) order, as rotated by
  * T_OCEAN.cycleTimes2D (modules/mod_ocean.py:120-154), plus the fast-time accumulators. */
 typedef struct sf_state2d {
@@ -169,6 +179,17 @@ int sf_step3d_uv_bc(sf_ctx *ctx, void *u, void *v, const void *ru, const void *r
                     const void *Akv, const void *z_r, const double *DU_avg1,
                     const double *DV_avg1, int iic, int ntfirst, double lambda, double Dt,
                     double time, sf_stream stream);
+
+/* ---- vertical mixing ------------------------------------------------------------------- */
+/* GLS corrector, column physics of nonlinear/gls_corrector_step.py:26-825 (ROMS pseudo-code in
+ * the reference; see sf_gls.cuh for the parts restated), on rho-interior columns.  u, v: rho
+ * levels (N+1 allocated), z_r, Hz: N levels, bvf (buoyancy frequency squared), tke, gls, Akv,
+ * Akt, Akk, Akp, Lscale: N+1 W levels, updated in place; sustr/svstr: kinematic surface stress
+ * at U/V points (m2/s2); dt: baroclinic step. */
+int sf_gls_corrector(sf_ctx *ctx, const sf_gls_params *params, double dt, const void *u,
+                     const void *v, const void *z_r, const void *Hz, const void *bvf,
+                     const void *sustr, const void *svstr, void *tke, void *gls, void *Akv,
+                     void *Akt, void *Akk, void *Akp, void *Lscale, sf_stream stream);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,209 @@
+"""GLS vertical-mixing corrector, restated in NumPy FP64 (TEST INFRASTRUCTURE: the oracle).
+
+The reference has the GLS closure only as untranslated ROMS Fortran inside .py files that do
+not parse (nonlinear/gls_corrector_step.py, nonlinear/gls_predictor_step.py), so there is no
+runnable reference to pin against: this is a restatement of that pseudo-code, vectorised over
+water columns, written independently of the CUDA kernel it checks (parity unpinned).
+
+Scope (per water column, rho-interior points i=1..L-1, j=1..M-1):
+  * the predictor's initialisation of the new time level, tke(nnew) = Hz_w * tke(nstp)
+    (gls_predictor_step.py:153-154), without the advective terms;
+  * shear^2 at W points (gls_corrector_step.py:86-96), buoyancy frequency as input (:101);
+  * production / dissipation with the buoyancy switch (:397-516);
+  * surface and bottom Dirichlet conditions (:526-564) with stresses from the wind and a
+    quadratic bottom drag on the bottom-level velocity (nonlinear/set_vbc.py:19-41);
+  * the implicit tke and gls solves and the boundary fluxes (:568-656);
+  * length-scale limitation, Galperin stability functions, Akv/Akt/Akk/Akp and Lscale
+    (:662-825).
+Horizontal and vertical advection of tke/gls (:181-388, gls_predictor_step.py:18-216) is not
+included.
+
+Layout: W-level arrays have N+1 levels (0..N), rho-level arrays N levels; index arrays are
+flat (levels, (M+1)*(L+1)) with the reference's flat neighbour offsets (p+1 east, p+I north).
+"""
+import numpy as np
+
+VONKAR = 0.41               # modules/mod_constants.py:28
+EPS = 1.0e-10               # gls_corrector_step.py:673-688 (eps)
+# Galperin et al. (1988) quasi-equilibrium stability functions with the Mellor-Yamada
+# constants A1, A2, B1, B2, C1 (published values), as the corrector uses them (:740-748).
+MY_A1, MY_A2, MY_B1, MY_B2, MY_C1 = 0.92, 0.74, 16.6, 10.1, 0.08
+MY_SH1 = MY_A2 * (1.0 - 6.0 * MY_A1 / MY_B1)
+MY_SH2 = 3.0 * MY_A2 * (6.0 * MY_A1 + MY_B2)
+MY_SM2 = 9.0 * MY_A1 * MY_A2
+MY_SM3 = MY_A1 * (1.0 - 3.0 * MY_C1 - 6.0 * MY_A1 / MY_B1)
+MY_SM4 = 18.0 * MY_A1 * MY_A1 + 9.0 * MY_A1 * MY_A2
+GH0, GHCRI, GHMIN = 0.0233, 0.02, -0.28
+
+# k-epsilon parameters of the reference's input file (utility/test.in:355-367) and its
+# background values (test.in:326-349, :380-381).
+DEFAULT = dict(p=3.0, m=1.5, n=-1.0, cmu0=0.5477, c1=1.44, c2=1.92, c3m=-0.4, c3p=1.0, sigk=1.0,
+               sigp=1.30, Kmin=7.6e-6, Pmin=1.0e-12, Akv_bak=1.0e-5, Akt_bak=1.0e-6,
+               Akk_bak=5.0e-6, Akp_bak=5.0e-6, Zos=0.02, Zob=0.02, rdrag2=3.0e-3, E2=1.33)
+
+
+def gls_corrector(P, dt, I, J, N, u, v, z_r, Hz, bvf, sustr, svstr, tke, gls, Akv, Akt, Akk, Akp,
+                  Lscale):
+    """One corrector step; returns new (tke, gls, Akv, Akt, Akk, Akp, Lscale) copies.
+    u, v: (N+1, s2) rho-level velocities (level N unused); z_r, Hz: (N, s2); bvf and the
+    turbulence fields: (N+1, s2); sustr, svstr: (s2,) kinematic surface stress at U/V points."""
+    p_, m_, n_ = P["p"], P["m"], P["n"]
+    cmu0 = P["cmu0"]
+    s2 = I * J
+    idx = np.arange(s2)
+    ii, jj = idx % I, idx // I
+    col = idx[(ii != 0) & (ii != I - 1) & (jj != 0) & (jj != J - 1)]
+    out = [a.copy() for a in (tke, gls, Akv, Akt, Akk, Akp, Lscale)]
+    tke_o, gls_o = tke[:, col], gls[:, col]
+    Akv_o, Akt_o, Akk_o, Akp_o, Ls_o = Akv[:, col], Akt[:, col], Akk[:, col], Akp[:, col], Lscale[:, col]
+    nc = col.size
+
+    L_sft = VONKAR
+    ogls_sigp = 1.0 / P["sigp"]
+    sqrt2 = np.sqrt(2.0)
+    cmu_fac1 = cmu0 ** (-p_ / n_)
+    cmu_fac2 = cmu0 ** (3.0 + p_ / n_)
+    cmu_fac3 = 1.0 / cmu0 ** 2.0
+    gls_fac2 = cmu0 ** p_ * n_ * VONKAR ** n_
+    gls_fac3 = cmu0 ** p_ * n_
+    gls_fac4 = cmu0 ** p_
+    gls_fac5 = 0.56 ** (0.5 * n_) * cmu0 ** p_
+    gls_exp1 = 1.0 / n_
+    tke_exp1 = m_ / n_
+    tke_exp2 = 0.5 + m_ / n_
+    tke_exp4 = m_ + 0.5 * n_
+    Lmy25 = p_ == 0.0 and n_ == 1.0 and m_ == 1.0
+    Zos_min = max(P["Zos"], 1.0e-4)
+    Zob_min = max(P["Zob"], 1.0e-4)
+
+    # shear^2 at W points 1..N-1 (:86-96)
+    sh2 = np.zeros((N + 1, nc))
+    for k in range(1, N):
+        cff = 0.5 / (z_r[k, col] - z_r[k - 1, col])
+        du = (u[k, col] - u[k - 1, col]) + (u[k, col + 1] - u[k - 1, col + 1])
+        dv = (v[k, col] - v[k - 1, col]) + (v[k, col + I] - v[k - 1, col + I])
+        sh2[k] = (cff * du) ** 2 + (cff * dv) ** 2
+    b2 = bvf[:, col]
+
+    # quadratic bottom stress on the bottom-level velocity at the U/V faces of the column
+    def bustr(q):
+        va = 0.25 * (v[0, q] + v[0, q + I] + v[0, q - 1] + v[0, q - 1 + I])
+        return P["rdrag2"] * u[0, q] * np.sqrt(u[0, q] * u[0, q] + va * va)
+
+    def bvstr(q):
+        ua = 0.25 * (u[0, q] + u[0, q + 1] + u[0, q - I] + u[0, q + 1 - I])
+        return P["rdrag2"] * v[0, q] * np.sqrt(ua * ua + v[0, q] * v[0, q])
+
+    # vertical mixing of the turbulent fields (:401-415)
+    FCK = np.zeros((N + 1, nc))
+    FCP = np.zeros((N + 1, nc))
+    for k in range(2, N):
+        FCK[k] = (-0.5 * dt) * (Akk_o[k] + Akk_o[k - 1]) / Hz[k - 1, col]
+        FCP[k] = (-0.5 * dt) * (Akp_o[k] + Akp_o[k - 1]) / Hz[k - 1, col]
+
+    tk = np.zeros((N + 1, nc))
+    gl = np.zeros((N + 1, nc))
+    BCK = np.zeros((N + 1, nc))
+    BCP = np.zeros((N + 1, nc))
+    zw_bot = None
+    for k in range(1, N):
+        cffz = 0.5 * (Hz[k - 1, col] + Hz[k, col])
+        tk[k] = cffz * tke_o[k]
+        gl[k] = cffz * gls_o[k]
+        strat2 = b2[k]
+        c3 = np.where(strat2 > 0.0, P["c3m"], P["c3p"])
+        dAkt = Akt_o[k] - P["Akt_bak"]
+        Kprod = sh2[k] * (Akv_o[k] - P["Akv_bak"]) - strat2 * dAkt
+        Pprod = P["c1"] * sh2[k] * (Akv_o[k] - P["Akv_bak"]) - c3 * strat2 * dAkt
+        cff1 = np.where(Kprod < 0.0, 0.0, 1.0)
+        Kprod = np.where(Kprod < 0.0, Kprod + strat2 * dAkt, Kprod)
+        cff2 = np.where(Pprod < 0.0, 0.0, 1.0)
+        Pprod = np.where(Pprod < 0.0, Pprod + c3 * strat2 * dAkt, Pprod)
+        tk[k] = tk[k] + dt * cffz * Kprod
+        gl[k] = gl[k] + dt * cffz * Pprod * gls_o[k] / np.maximum(tke_o[k], P["Kmin"])
+        wall = 1.0
+        if Lmy25:   # parabolic wall function + free-surface correction (:491-497)
+            raise NotImplementedError("wall function needs z_w; k-epsilon does not use it")
+        diss = gls_o[k] ** (-gls_exp1) * cmu_fac2 * tke_o[k] ** tke_exp2
+        BCK[k] = cffz * (1.0 + dt * diss + dt * (1.0 - cff1) * strat2 * dAkt / tke_o[k]) - FCK[k] - FCK[k + 1]
+        BCP[k] = (cffz * (1.0 + dt * P["c2"] * wall * diss + dt * (1.0 - cff2) * c3 * strat2 * dAkt / tke_o[k])
+                  - FCP[k] - FCP[k + 1])
+
+    # surface / bottom Dirichlet values (:526-564)
+    su = sustr[col] + sustr[col + 1]
+    sv = svstr[col] + svstr[col + I]
+    bu = bustr(col) + bustr(col + 1)
+    bv = bvstr(col) + bvstr(col + I)
+    tk[N] = np.maximum(cmu_fac3 * 0.5 * np.sqrt(su * su + sv * sv), P["Kmin"])
+    tk[0] = np.maximum(cmu_fac3 * 0.5 * np.sqrt(bu * bu + bv * bv), P["Kmin"])
+    Zos_eff = Zos_min
+    gl[N] = np.maximum(cmu0 ** p_ * tk[N] ** m_ * (L_sft * Zos_eff) ** n_, P["Pmin"])
+    gl[0] = np.maximum(gls_fac4 * (VONKAR * Zob_min) ** n_ * tk[0] ** m_, P["Pmin"])
+
+    # tke solve (:571-604)
+    CF = np.zeros((N + 1, nc))
+    cff = 1.0 / BCK[N - 1]
+    CF[N - 1] = cff * FCK[N - 1]
+    tk[N - 1] = cff * (tk[N - 1] + 0.0)
+    for k in range(N - 2, 0, -1):
+        cff = 1.0 / (BCK[k] - CF[k + 1] * FCK[k + 1])
+        CF[k] = cff * FCK[k]
+        tk[k] = cff * (tk[k] - FCK[k + 1] * tk[k + 1])
+    tk[1] = tk[1] - cff * 0.0
+    tk[1] = np.maximum(tk[1], P["Kmin"])
+    for k in range(2, N):
+        tk[k] = tk[k] - CF[k] * tk[k - 1]
+        tk[k] = np.maximum(tk[k], P["Kmin"])
+
+    # gls solve (:608-656)
+    cffT = 0.5 * (tk[N] + tk[N - 1])
+    fluxt = (dt * gls_fac3 * cffT ** m_ * L_sft ** n_ * (Zos_eff + 0.5 * Hz[N - 1, col]) ** (n_ - 1.0)
+             * 0.5 * (Akp_o[N] + Akp_o[N - 1]))
+    cffB = 0.5 * (tk[0] + tk[1])
+    fluxb = (dt * gls_fac2 * cffB ** m_ * (0.5 * Hz[0, col] + Zob_min) ** (n_ - 1.0)
+             * 0.5 * (Akp_o[0] + Akp_o[1]))
+    cff = 1.0 / BCP[N - 1]
+    CF[N - 1] = cff * FCP[N - 1]
+    gl[N - 1] = cff * (gl[N - 1] - fluxt)
+    for k in range(N - 2, 0, -1):
+        cff = 1.0 / (BCP[k] - CF[k + 1] * FCP[k + 1])
+        CF[k] = cff * FCP[k]
+        gl[k] = cff * (gl[k] - FCP[k + 1] * gl[k + 1])
+    gl[1] = gl[1] - cff * fluxb
+    for k in range(2, N):
+        gl[k] = gl[k] - CF[k] * gl[k - 1]
+
+    # mixing coefficients (:662-825)
+    Av, At, Ak, Ap, Ls = (np.array(a) for a in (Akv_o, Akt_o, Akk_o, Akp_o, Ls_o))
+    for k in range(1, N):
+        tk[k] = np.maximum(tk[k], P["Kmin"])
+        gl[k] = np.maximum(gl[k], P["Pmin"])
+        lim = gls_fac5 * tk[k] ** tke_exp4 * (np.sqrt(np.maximum(0.0, b2[k])) + EPS) ** (-n_)
+        gl[k] = np.minimum(gl[k], lim) if n_ >= 0.0 else np.maximum(gl[k], lim)
+        Ls_unlmt = np.maximum(EPS, gl[k] ** gls_exp1 * cmu_fac1 * tk[k] ** (-tke_exp1))
+        Ls_lmt = np.where(b2[k] > 0.0,
+                          np.minimum(Ls_unlmt, np.sqrt(0.56 * tk[k] / (np.maximum(0.0, b2[k]) + EPS))),
+                          Ls_unlmt)
+        gl[k] = np.maximum(cmu0 ** p_ * tk[k] ** m_ * Ls_lmt ** n_, P["Pmin"])
+        Gh = np.minimum(GH0, -b2[k] * Ls_lmt * Ls_lmt / (2.0 * tk[k]))
+        Gh = np.minimum(Gh, Gh - (Gh - GHCRI) ** 2 / (Gh + GH0 - 2.0 * GHCRI))
+        Gh = np.maximum(Gh, GHMIN)
+        Sh = MY_SH1 / (1.0 - MY_SH2 * Gh)
+        Sm = (MY_SM3 + Sh * Gh * MY_SM4) / (1.0 - MY_SM2 * Gh)
+        ql = sqrt2 * 0.5 * (Ls_lmt * np.sqrt(tk[k]) + Ls_o[k] * np.sqrt(tke_o[k]))
+        Av[k] = P["Akv_bak"] + Sm * ql
+        At[k] = P["Akt_bak"] + Sh * ql
+        Ak[k] = P["Akk_bak"] + Sm * ql / P["sigk"]
+        Ap[k] = P["Akp_bak"] + Sm * ql * ogls_sigp
+        Ls[k] = Ls_lmt
+    Av[N] = P["Akv_bak"] + L_sft * Zos_eff * cmu0 * np.sqrt(tk[N])
+    Av[0] = P["Akv_bak"] + VONKAR * Zob_min * cmu0 * np.sqrt(tk[0])
+    Ak[N] = P["Akk_bak"] + Av[N] / P["sigk"]
+    Ak[0] = P["Akk_bak"] + Av[0] / P["sigk"]
+    Ap[N] = P["Akp_bak"] + Av[N] * ogls_sigp
+    Ap[0] = P["Akp_bak"] + Av[0] / P["sigp"]
+    At[N] = P["Akt_bak"]
+    At[0] = P["Akt_bak"]
+    for a, b in zip(out, (tk, gl, Av, At, Ak, Ap, Ls)):
+        a[:, col] = b
+    return tuple(out)

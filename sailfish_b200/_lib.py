@@ -33,6 +33,12 @@ class GridDesc(ctypes.Structure):
     ]
 
 
+class GlsParams(ctypes.Structure):
+    _fields_ = [(n, _d) for n in ("p", "m", "n", "cmu0", "c1", "c2", "c3m", "c3p", "sigk", "sigp",
+                                   "Kmin", "Pmin", "Akv_bak", "Akt_bak", "Akk_bak", "Akp_bak",
+                                   "Zos", "Zob", "rdrag2")]
+
+
 class State2D(ctypes.Structure):
     _fields_ = [("zeta", _vp * 3), ("ubar", _vp * 3), ("vbar", _vp * 3), ("rzeta", _vp * 3),
                 ("rubar", _vp * 3), ("rvbar", _vp * 3),
@@ -66,6 +72,7 @@ SIGNATURES = {
     "sf_step3d_uv": [_vp] * 16 + [_i, _i, _d, _d, _vp],
     "sf_lateral_uv_bc": [_vp, _d, _vp, _vp, _vp],
     "sf_step3d_uv_bc": [_vp] * 14 + [_i, _i, _d, _d, _d, _vp],
+    "sf_gls_corrector": [_vp, ctypes.POINTER(GlsParams), _d] + [_vp] * 14 + [_vp],
 }
 
 

@@ -567,4 +567,22 @@ int sf_lateral_uv_bc(sf_ctx *c, double time, void *u, void *v, sf_stream s) {
     });
 }
 
+int sf_gls_corrector(sf_ctx *c, const sf_gls_params *P, double dt, const void *u, const void *v,
+                     const void *z_r, const void *Hz, const void *bvf, const void *sustr,
+                     const void *svstr, void *tke, void *gls, void *Akv, void *Akt, void *Akk,
+                     void *Akp, void *Lscale, sf_stream s) {
+    if (!P) return fail(SF_EINVAL, "null GLS parameters");
+    if (P->n == 0.0) return fail(SF_EINVAL, "GLS exponent n must be non-zero");
+    if (P->p == 0.0 && P->m == 1.0 && P->n == 1.0)
+        return fail(SF_EUNSUPPORTED, "Mellor-Yamada 2.5 (p=0, m=1, n=1) needs the wall function, "
+                                     "which is not built");
+    return dispatch(c, "sf_gls_corrector", [&](auto *t) {
+        using R = std::remove_pointer_t<decltype(t)>;
+        return sf::Ops<R>::gls_corrector(c, *P, dt, (const R *)u, (const R *)v, (const R *)z_r,
+                                         (const R *)Hz, (const R *)bvf, (const R *)sustr,
+                                         (const R *)svstr, (R *)tke, (R *)gls, (R *)Akv, (R *)Akt,
+                                         (R *)Akk, (R *)Akp, (R *)Lscale, S(s));
+    });
+}
+
 }  // extern "C"

@@ -97,6 +97,10 @@ struct Ops {
                                  const R *tmpU, const R *tmpV, double cff, double lambda,
                                  double Dt, int do_bc, double bcval, cudaStream_t s);
     static cudaError_t lateral_uv_bc(const sf_ctx *c, R *u, R *v, double val, cudaStream_t s);
+    static cudaError_t gls_corrector(const sf_ctx *c, const sf_gls_params &P, double dt,
+                                     const R *u, const R *v, const R *z_r, const R *Hz,
+                                     const R *bvf, const R *sustr, const R *svstr, R *tke, R *gls,
+                                     R *Akv, R *Akt, R *Akk, R *Akp, R *Lscale, cudaStream_t s);
 };
 
 extern template struct Ops<double>;

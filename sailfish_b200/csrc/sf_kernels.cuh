@@ -548,60 +548,97 @@ __global__ void __launch_bounds__(kBlock) k_set_depth(Geo<R> g, const double *__
 // (Thomas algorithm in per-thread arrays), baroclinic-mean correction, 2D/3D coupling, and
 // optionally setLateralUVBCs (:314-368) for the same column.
 // ------------------------------------------------------------------------------------------
+// Tridiagonal storage of one column: per-thread arrays (local memory, cached in L1), element
+// k of each at FC[k*B + t] (B = 1, t = 0 here).
 template <typename R>
-struct Column {
-    R FC[kNMax], BD[kNMax], RHS[kNMax];
+struct Tri {
+    R *FC, *BD, *RHS;
+    int B, t;
+    __device__ __forceinline__ R &fc(int k) const { return FC[k * B + t]; }
+    __device__ __forceinline__ R &bd(int k) const { return BD[k * B + t]; }
+    __device__ __forceinline__ R &rhs(int k) const { return RHS[k * B + t]; }
 };
 
-// createVertViscousOpMatrix (:568-639) for the column at p; d = 1 (U) or I (V).
+// createVertViscousOpMatrix (:568-639) for the column at p (d = 1: U, d = I: V) fused with the
+// forward elimination of solveTri (:547-554): row k is built and eliminated against row k-1
+// with the same operations, in the same order, as building the whole matrix first.  Also
+// returns H = sum HzU and Hu = sum old*HzU (correctBaroclinicMeanVel, :502-506), ascending.
 template <typename R>
-__device__ __forceinline__ void build_matrix(const Geo<R> &g, long p, long d, R cff, R Dt,
-                                             R lambda, Column<R> &c, const R *Hz, const R *Akv,
-                                             const R *z_r, const R *uold, const R *ru) {
+__device__ __forceinline__ void build_eliminate(const Geo<R> &g, long p, long d, R cff, R Dt,
+                                                R lambda, const Tri<R> &m, const R *Hz,
+                                                const R *Akv, const R *z_r, const R *old,
+                                                const R *ru, double &H, double &Hu) {
     const long s2 = g.s2;
     const int N = g.N;
     const R pmU = (g.pm[p] + g.pm[p - d]) * R(0.5), pnU = (g.pn[p] + g.pn[p - d]) * R(0.5);
     const R cdt = cff * Dt;
     const R cm = -lambda * Dt;
-#define HZU(k) ((Hz[(long)(k) * s2 + p] + Hz[(long)(k) * s2 + p - d]) * R(0.5))
-#define AKU(k) ((Akv[(long)(k) * s2 + p] + Akv[(long)(k) * s2 + p - d]) * R(0.5))
-#define DZ(k) (((z_r[(long)(k) * s2 + p] - z_r[(long)((k) - 1) * s2 + p]) + \
-                (z_r[(long)(k) * s2 + p - d] - z_r[(long)((k) - 1) * s2 + p - d])) * R(0.5))
-    c.FC[N - 1] = R(0);
-#pragma unroll 4
-    for (int K = 0; K < N - 1; ++K) c.FC[K] = (cm * AKU(K)) / DZ(K + 1);
-    c.RHS[0] = R(0);
-#pragma unroll 4
-    for (int K = 1; K < N; ++K) {
-        const R hzu = HZU(K);
-        c.RHS[K] = hzu * (uold[(long)K * s2] + (cdt * (pmU * pnU)) * ru[(long)K * s2 + p]);
-        c.BD[K] = (hzu - c.FC[K]) - c.FC[K - 1];
+    const R cmn = cdt * (pmU * pnU);
+#define AT(X, k, q) ((X)[(long)(k) * s2 + (q)])
+    R zr0 = AT(z_r, 0, p), zr0d = AT(z_r, 0, p - d);
+    R zr1 = AT(z_r, 1, p), zr1d = AT(z_r, 1, p - d);
+    R fcm = (cm * ((AT(Akv, 0, p) + AT(Akv, 0, p - d)) * R(0.5))) /
+            (((zr1 - zr0) + (zr1d - zr0d)) * R(0.5));
+    R hz = (AT(Hz, 0, p) + AT(Hz, 0, p - d)) * R(0.5);
+    R bdm = hz - R(2.0) * fcm;
+    R rhsm = R(0);
+    m.fc(0) = fcm;
+    m.bd(0) = bdm;
+    m.rhs(0) = rhsm;
+    H = (double)hz;
+    Hu = (double)(old[0] * hz);
+#pragma unroll 2
+    for (int k = 1; k < N; ++k) {
+        hz = (AT(Hz, k, p) + AT(Hz, k, p - d)) * R(0.5);
+        R fck = R(0);
+        if (k < N - 1) {
+            const R zr2 = AT(z_r, k + 1, p), zr2d = AT(z_r, k + 1, p - d);
+            fck = (cm * ((AT(Akv, k, p) + AT(Akv, k, p - d)) * R(0.5))) /
+                  (((zr2 - zr1) + (zr2d - zr1d)) * R(0.5));
+            zr1 = zr2;
+            zr1d = zr2d;
+        }
+        const R ok = old[(long)k * s2];
+        const R rhsk = hz * (ok + cmn * AT(ru, k, p));
+        const R bdk = (k < N - 1) ? (hz - fck) - fcm : hz - fcm;
+        const R w = fcm / bdm;
+        bdm = bdk - w * fcm;
+        rhsm = rhsk - w * rhsm;
+        m.fc(k) = fck;
+        m.bd(k) = bdm;
+        m.rhs(k) = rhsm;
+        fcm = fck;
+        H += (double)hz;
+        Hu += (double)(ok * hz);
     }
-    c.BD[N - 1] = HZU(N - 1) - c.FC[N - 2];
-    c.BD[0] = HZU(0) - R(2.0) * c.FC[0];
-#undef DZ
-#undef AKU
-#undef HZU
+#undef AT
 }
 
-// solveTri (:520-565): forward elimination in place, back substitution into out[k*s2] with
-// `sub` subtracted from every level (correctBaroclinicMeanVel, :512-515).
+// A second forward elimination of an already eliminated system (solveTri applied twice, :525).
 template <typename R>
-__device__ __forceinline__ void solve_tri(int N, long s2, Column<R> &c, R *out, R sub) {
+__device__ __forceinline__ void eliminate_again(int N, const Tri<R> &m) {
+    R bdm = m.bd(0), rhsm = m.rhs(0);
     for (int k = 1; k < N; ++k) {
-        const R w = c.FC[k - 1] / c.BD[k - 1];
-        c.BD[k] = c.BD[k] - w * c.FC[k - 1];
-        c.RHS[k] = c.RHS[k] - w * c.RHS[k - 1];
+        const R fcm = m.fc(k - 1);
+        const R w = fcm / bdm;
+        bdm = m.bd(k) - w * fcm;
+        rhsm = m.rhs(k) - w * rhsm;
+        m.bd(k) = bdm;
+        m.rhs(k) = rhsm;
     }
-    R x = c.RHS[N - 1] / c.BD[N - 1];
+}
+
+// Back substitution of solveTri (:557-563) into out[k*s2], minus `sub` (:512-515).
+template <typename R>
+__device__ __forceinline__ void back_substitute(int N, long s2, const Tri<R> &m, R *out, R sub) {
+    R x = m.rhs(N - 1) / m.bd(N - 1);
     out[(long)(N - 1) * s2] = x - sub;
     for (int k = N - 2; k >= 0; --k) {
-        x = (c.RHS[k] - c.FC[k] * x) / c.BD[k];
+        x = (m.rhs(k) - m.fc(k) * x) / m.bd(k);
         out[(long)k * s2] = x - sub;
     }
 }
 
-// correctBaroclinicMeanVel's correction (:499-508), from the pre-step velocity `old`.
 template <typename R>
 __device__ __forceinline__ R mean_correction(int N, long s2, long p, long d, const R *Hz,
                                              const R *old, double DUp, double on) {
@@ -617,38 +654,44 @@ __device__ __forceinline__ R mean_correction(int N, long s2, long p, long d, con
 }
 
 template <typename R>
-__global__ void __launch_bounds__(128) k_step3d_uv(
-    Geo<R> g, R *__restrict__ u, R *__restrict__ v, const R *__restrict__ ru,
-    const R *__restrict__ rv, R *__restrict__ ubar_t1, R *__restrict__ vbar_t1,
-    R *__restrict__ ubar_t2, R *__restrict__ vbar_t2, const R *__restrict__ Hz,
-    const R *__restrict__ Akv, const R *__restrict__ z_r, const double *__restrict__ DU,
-    const double *__restrict__ DV, const R *tmpU, const R *tmpV, R cff, R lambda, R Dt,
-    int do_bc, R bcval) {
-    const long p = tid_flat();
-    if (p >= g.s2) return;
-    const long I = g.I, s2 = g.s2;
+__global__ void __launch_bounds__(128) k_step3d_uv(Geo<R> g, R *__restrict__ u, R *__restrict__ v,
+                            const R *__restrict__ ru, const R *__restrict__ rv,
+                            R *__restrict__ ubar_t1, R *__restrict__ vbar_t1,
+                            R *__restrict__ ubar_t2, R *__restrict__ vbar_t2,
+                            const R *__restrict__ Hz, const R *__restrict__ Akv,
+                            const R *__restrict__ z_r, const double *__restrict__ DU,
+                            const double *__restrict__ DV, const R *tmpU, const R *tmpV, R cff,
+                            R lambda, R Dt, int do_bc, R bcval) {
     const int N = g.N;
-    const int i = (int)(p % I), j = (int)(p / I);
+    R FCa[kNMax], BDa[kNMax], RHSa[kNMax];
+    const Tri<R> m{FCa, BDa, RHSa, 1, 0};
+    const int pi = (int)tid_flat();
+    if (pi >= g.s2) return;      // no barriers below
+    const long p = pi;
+    const long I = g.I, s2 = g.s2;
+    const int i = pi % g.I, j = pi / g.I;
     const bool un = unode_(i, j), vn = vnode_(i, j, g.J);
     if (un || vn) {
-        Column<R> c;
         const R *uo = (tmpU ? tmpU : u) + p;
         const R *vo = (tmpV ? tmpV : v) + p;
         if (un) {
-            const R udiff = mean_correction(N, s2, p, 1, Hz, uo, DU[p], (double)g.on_u[p]);
-            build_matrix(g, p, 1, cff, Dt, lambda, c, Hz, Akv, z_r, uo, ru);
-            solve_tri(N, s2, c, u + p, udiff);
+            double H, Hu;
+            build_eliminate(g, p, 1, cff, Dt, lambda, m, Hz, Akv, z_r, uo, ru, H, Hu);
+            const R udiff = (R)((Hu - DU[p] / (double)g.on_u[p]) / H);
+            back_substitute(N, s2, m, u + p, udiff);
         }
-        R vdiff = R(0);
-        if (vn) {
-            vdiff = mean_correction(N, s2, p, I, Hz, vo, DV[p], (double)g.om_v[p]);
-            build_matrix(g, p, I, cff, Dt, lambda, c, Hz, Akv, z_r, vo, rv);
-        }
-        if (un) {
-            // solveTri is gated by isUNode for both directions (:525): where p is a U node
-            // but not a V node it solves the U system left in the scratch a second time.
-            solve_tri(N, s2, c, v + p, vn ? vdiff : R(0));
+        if (vn && un) {
+            double H, Hv;
+            build_eliminate(g, p, I, cff, Dt, lambda, m, Hz, Akv, z_r, vo, rv, H, Hv);
+            const R vdiff = (R)((Hv - DV[p] / (double)g.om_v[p]) / H);
+            back_substitute(N, s2, m, v + p, vdiff);
+        } else if (un) {
+            // solveTri is gated by isUNode for both directions (:525): where p is a U node but
+            // not a V node it solves the U system left in the scratch a second time.
+            eliminate_again(N, m);
+            back_substitute(N, s2, m, v + p, R(0));
         } else {
+            const R vdiff = mean_correction(N, s2, p, I, Hz, vo, DV[p], (double)g.om_v[p]);
             for (int K = 0; K < N; ++K) v[(long)K * s2 + p] = v[(long)K * s2 + p] - vdiff;
         }
         if (un) {   // adjustBarotropicVelocity (:408-469)
@@ -695,6 +738,12 @@ __global__ void __launch_bounds__(kBlock) k_lateral_uv_bc(Geo<R> g, R *__restric
     if (vt > 0 && ((vt & (1 << 4)) != 0 || (vt & (1 << 3)) != 0))
         for (int K = 0; K < g.N; ++K) v[(long)K * s2 + p] = R(0);
 }
+
+}  // namespace sf
+
+#include "sf_gls.cuh"
+
+namespace sf {
 
 // ------------------------------------------------------------------------------------------
 // Launchers
@@ -814,7 +863,8 @@ cudaError_t Ops<R>::step3d_uv(const sf_ctx *c, R *u, R *v, const R *ru, const R 
                               const R *z_r, const double *DU, const double *DV, const R *tmpU,
                               const R *tmpV, double cff, double lambda, double Dt, int do_bc,
                               double bcval, cudaStream_t s) {
-    k_step3d_uv<R><<<blocks_for(c->s2, 128), 128, 0, s>>>(
+    const int B = 128;
+    k_step3d_uv<R><<<blocks_for(c->s2, B), B, 0, s>>>(
         geo(c), u, v, ru, rv, ubar_t1, vbar_t1, ubar_t2, vbar_t2, Hz, Akv, z_r, DU, DV, tmpU, tmpV,
         (R)cff, (R)lambda, (R)Dt, do_bc, (R)bcval);
     return cudaGetLastError();
@@ -822,6 +872,17 @@ cudaError_t Ops<R>::step3d_uv(const sf_ctx *c, R *u, R *v, const R *ru, const R 
 template <typename R>
 cudaError_t Ops<R>::lateral_uv_bc(const sf_ctx *c, R *u, R *v, double val, cudaStream_t s) {
     k_lateral_uv_bc<R><<<blocks_for(c->s2, kBlock), kBlock, 0, s>>>(geo(c), u, v, (R)val);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t Ops<R>::gls_corrector(const sf_ctx *c, const sf_gls_params &P, double dt, const R *u,
+                                  const R *v, const R *z_r, const R *Hz, const R *bvf,
+                                  const R *sustr, const R *svstr, R *tke, R *gls, R *Akv, R *Akt,
+                                  R *Akk, R *Akp, R *Lscale, cudaStream_t s) {
+    k_gls_corrector<R><<<blocks_for(c->s2, 128), 128, 0, s>>>(geo(c), P, (R)dt, u, v, z_r, Hz, bvf,
+                                                              sustr, svstr, tke, gls, Akv, Akt,
+                                                              Akk, Akp, Lscale);
     return cudaGetLastError();
 }
 
