@@ -191,6 +191,52 @@ int sf_gls_corrector(sf_ctx *ctx, const sf_gls_params *params, double dt, const 
                      const void *sustr, const void *svstr, void *tke, void *gls, void *Akv,
                      void *Akt, void *Akk, void *Akp, void *Lscale, sf_stream stream);
 
+/* ---- learned closure (no counterpart in the reference) --------------------------------------
+ * A per-column MLP standing in for the GLS corrector's Akv/Akt: SF_MLP_LAYERS dense layers of
+ * width 128 (inputs and outputs zero-padded to 128), GELU between them, BF16 weights W[l]
+ * ([out][in], row-major, device) and FP32 biases b[l] (device); products on the tensor cores
+ * (tcgen05) with FP32 accumulation.  Rows are samples (one water column each), 128 FP32
+ * values per row.  `err` is a device int set to 1 if a bounded wait on the tensor cores gave
+ * up.  Error text of these entry points: sf_mlp_last_error(). */
+#define SF_MLP_LAYERS 5
+#define SF_MLP_WIDTH 128
+typedef struct sf_mlp_params {
+    const void *W[SF_MLP_LAYERS];
+    const float *b[SF_MLP_LAYERS];
+} sf_mlp_params;
+
+const char *sf_mlp_last_error(void);
+/* O[r, :] = act(A B^T + bias) for a 128-wide B: A is element (r, k) = A[r*a_rs + k*a_ks]
+ * (n_rows x K, FP32 or BF16), B likewise (128 x K); K a multiple of 16; optional pre-activation
+ * copy Z.  The dense-product building block of the forward and backward passes. */
+int sf_mlp_gemm(int n_rows, int K, const void *A, int a_bf16, long a_rs, long a_ks,
+                const void *B, int b_bf16, long b_rs, long b_ks, const float *bias, int act,
+                float *O, long ldo, float *Z, long ldz, int *err, sf_stream stream);
+/* Forward pass over n rows; `acts` ((LAYERS-1) x n x 128) and `pre` (LAYERS x n x 128) keep the
+ * hidden activations and pre-activations for the backward pass (acts required). */
+int sf_mlp_forward(const sf_mlp_params *w, int n, const float *X, float *Y, float *acts,
+                   float *pre, int *err, sf_stream stream);
+/* Backward pass: weight and bias gradients dW[l] (128 x 128 FP32), db[l] (128) for output
+ * gradient dY; `work` is 2 x n x 128 FP32 scratch; n a multiple of 16. */
+int sf_mlp_backward(const sf_mlp_params *w, int n, const float *X, const float *acts,
+                    const float *pre, const float *dY, float *const *dW, float *const *db,
+                    float *work, int *err, sf_stream stream);
+/* Mean squared error over the first nvalid outputs of each row; adds the loss into *loss. */
+int sf_mlp_mse(int n, int nvalid, const float *Y, const float *T, float *dY, float *loss,
+               sf_stream stream);
+/* Adam step on n FP32 master weights (bias-corrected, step >= 1); refreshes the BF16 copy. */
+int sf_mlp_adam(long n, float *w, const float *g, float *m, float *v, void *w_bf16, float lr,
+                float b1, float b2, int step, float eps, sf_stream stream);
+/* One feature row per water column (s2 x 128 FP32): log-scaled shear^2 and N^2 at the
+ * interior W levels (32 each), surface stress, surface buoyancy flux, depth. */
+int sf_closure_features(sf_ctx *ctx, const void *u, const void *v, const void *z_r,
+                        const void *bvf, const void *sustr, const void *svstr, float *X,
+                        sf_stream stream);
+/* Akv and Akt at the interior W levels from the network outputs (log10, clipped to
+ * [1e-6, 1e-1] m2/s), except on columns flagged in `fallback` (may be NULL). */
+int sf_closure_apply(sf_ctx *ctx, const float *Y, const uint8_t *fallback, void *Akv, void *Akt,
+                     sf_stream stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -39,6 +39,10 @@ class GlsParams(ctypes.Structure):
                                    "Zos", "Zob", "rdrag2")]
 
 
+class MlpParams(ctypes.Structure):
+    _fields_ = [("W", _vp * 5), ("b", _vp * 5)]
+
+
 class State2D(ctypes.Structure):
     _fields_ = [("zeta", _vp * 3), ("ubar", _vp * 3), ("vbar", _vp * 3), ("rzeta", _vp * 3),
                 ("rubar", _vp * 3), ("rvbar", _vp * 3),
@@ -73,6 +77,17 @@ SIGNATURES = {
     "sf_lateral_uv_bc": [_vp, _d, _vp, _vp, _vp],
     "sf_step3d_uv_bc": [_vp] * 14 + [_i, _i, _d, _d, _d, _vp],
     "sf_gls_corrector": [_vp, ctypes.POINTER(GlsParams), _d] + [_vp] * 14 + [_vp],
+    "sf_mlp_last_error": [],
+    "sf_mlp_gemm": [_i, _i, _vp, _i, ctypes.c_long, ctypes.c_long, _vp, _i, ctypes.c_long,
+                    ctypes.c_long, _vp, _i, _vp, ctypes.c_long, _vp, ctypes.c_long, _vp, _vp],
+    "sf_mlp_forward": [ctypes.POINTER(MlpParams), _i, _vp, _vp, _vp, _vp, _vp, _vp],
+    "sf_mlp_backward": [ctypes.POINTER(MlpParams), _i, _vp, _vp, _vp, _vp, ctypes.POINTER(_vp),
+                        ctypes.POINTER(_vp), _vp, _vp, _vp],
+    "sf_mlp_mse": [_i, _i, _vp, _vp, _vp, _vp, _vp],
+    "sf_mlp_adam": [ctypes.c_long, _vp, _vp, _vp, _vp, _vp, ctypes.c_float, ctypes.c_float,
+                    ctypes.c_float, _i, ctypes.c_float, _vp],
+    "sf_closure_features": [_vp] * 9,
+    "sf_closure_apply": [_vp] * 6,
 }
 
 
@@ -83,7 +98,7 @@ def _load():
     for name, args in SIGNATURES.items():
         f = getattr(lib, name)
         f.argtypes = args
-        f.restype = ctypes.c_char_p if name == "sf_last_error" else ctypes.c_int
+        f.restype = ctypes.c_char_p if name.endswith("last_error") else ctypes.c_int
     return lib
 
 

@@ -23,6 +23,7 @@ UNITS = {
     "sf_kernels_f64.cu": ["-fmad=false"],
     "sf_kernels_f32.cu": [],
     "sf_capi.cu": [],
+    "sf_mlp.cu": [],
 }
 
 

@@ -1,0 +1,480 @@
+// Learned vertical-mixing closure: a per-column MLP (5 dense layers of width 128, GELU between
+// them) with BF16 operands and FP32 accumulation on the Blackwell tensor cores (tcgen05.mma
+// with the accumulator in tensor memory), its training (forward with saved activations,
+// backward, Adam) and the feature / output mapping to the model state.
+//
+// The reference has no counterpart: its vertical mixing is a fixed analytic profile and its
+// GLS closure exists only as untranslated ROMS Fortran.  The network stands in for the GLS
+// corrector (sf_gls.cuh); plain GLS stays the fallback for columns outside the training range
+// and the judge of the network's error.
+//
+// All dense products go through one tile routine, D[128x128] (TMEM, FP32) = A[128xK] B[128xK]^T
+// with A and B staged in shared memory as BF16 in the K-major, no-swizzle "core matrix" layout
+// (8 rows x 16 bytes per core matrix), so forward layers (A = activations, B = W), input
+// gradients (A = G, B = W^T) and weight gradients (A = G^T, B = X^T) only differ in how the
+// operands are read from global memory while they are staged.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cmath>
+#include <string>
+#include <type_traits>
+
+#include "sf_internal.h"
+
+namespace sf {
+namespace mlp {
+
+constexpr int kTile = 128;         // rows of an output tile (MMA M) and width of every layer
+constexpr int kThreads = 128;      // 4 warps: warp w owns TMEM lanes 32w..32w+31
+constexpr uint32_t kTmemCols = 128;
+constexpr size_t kGemmSmem = 2 * 128 * 128 * 2;   // A and B tiles, BF16
+
+// ---- PTX wrappers ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// Shared-memory matrix descriptor, K-major, no swizzle (tcgen05 "version 1" format): start
+// address, leading byte offset (between the two 8-element K halves of a K=16 step), stride
+// byte offset (between 8-row groups), all in 16-byte units.
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+    d |= (uint64_t)1 << 46;   // descriptor version for sm_100
+    return d;                 // base offset 0, legacy LBO mode, layout SWIZZLE_NONE (0)
+}
+
+// Instruction descriptor, kind::f16: D FP32, A and B BF16, both K-major, M = 128, N = 128.
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kTile >> 3) << 17) |
+                            ((uint32_t)(kTile >> 4) << 24);
+
+__device__ __forceinline__ void tmem_alloc(uint32_t *dst_smem) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(dst_smem)),
+                 "r"(kTmemCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(kTmemCols));
+}
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::); }
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::); }
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
+        "l"(da), "l"(db), "r"(kIdesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+__device__ __forceinline__ void mma_commit(uint64_t *mbar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+        smem_u32(mbar)));
+}
+__device__ __forceinline__ void mbar_init(uint64_t *mbar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar)));
+}
+// Bounded wait on an mbarrier phase; returns false if it gave up.
+__device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t parity) {
+    const uint32_t a = smem_u32(mbar);
+    for (int it = 0; it < (1 << 24); ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(a), "r"(parity));
+        if (done) return true;
+    }
+    return false;
+}
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+        "%12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, "
+        "%30, %31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+          "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]),
+          "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]),
+          "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::);
+#pragma unroll
+    for (int k = 0; k < 32; ++k) v[k] = __uint_as_float(r[k]);
+}
+
+// Element (r, k) of a 128 x 128 BF16 tile in the core-matrix layout: 16 core matrices of
+// 8 x 8 along K per 8-row group; a core matrix is 8 rows of 16 contiguous bytes.
+__device__ __forceinline__ int cm_index(int r, int k) {
+    return (((r >> 3) * 16 + (k >> 3)) << 6) + ((r & 7) << 3) + (k & 7);
+}
+constexpr uint32_t kLBO = 128;       // next 8-element K half: next core matrix
+constexpr uint32_t kSBO = 16 * 128;  // next 8-row group
+
+// A matrix in global memory read as element (row, k) = p[row*rs + k*ks], FP32 or BF16.
+struct Mat {
+    const void *p;
+    int bf16;
+    long rs, ks;
+    long rows, cols;   // valid extent; outside it the staged value is 0
+    __device__ __forceinline__ float at(long r, long k) const {
+        if (r >= rows || k >= cols) return 0.f;
+        const long o = r * rs + k * ks;
+        return bf16 ? __bfloat162float(((const __nv_bfloat16 *)p)[o]) : ((const float *)p)[o];
+    }
+};
+
+__device__ __forceinline__ float gelu(float x) {   // tanh form of the GELU
+    const float c = 0.7978845608028654f;           // sqrt(2/pi)
+    return 0.5f * x * (1.f + tanhf(c * (x + 0.044715f * x * x * x)));
+}
+__device__ __forceinline__ float gelu_grad(float x) {
+    const float c = 0.7978845608028654f;
+    const float u = c * (x + 0.044715f * x * x * x);
+    const float t = tanhf(u);
+    return 0.5f * (1.f + t) + 0.5f * x * (1.f - t * t) * c * (1.f + 3.f * 0.044715f * x * x);
+}
+
+// D tile (blockIdx.x) = A[m0:m0+128, 0:K] B[0:128, 0:K]^T, K a multiple of 16, staged 128 K
+// at a time.  Epilogue: v = D + bias; Z[r, n] = v (optional); O[r, n] = act ? GELU(v) : v.
+__global__ void __launch_bounds__(kThreads) k_gemm(Mat A, Mat B, long Mrows, int K,
+                                                   const float *__restrict__ bias, int act,
+                                                   float *__restrict__ O, long ldo,
+                                                   float *__restrict__ Z, long ldz, int *err) {
+    extern __shared__ __align__(1024) unsigned char dsm[];
+    __nv_bfloat16 *sA = reinterpret_cast<__nv_bfloat16 *>(dsm);
+    __nv_bfloat16 *sB = sA + kTile * kTile;
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ uint32_t tmem_base;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const long m0 = (long)blockIdx.x * kTile;
+    if (warp == 0) tmem_alloc(&tmem_base);
+    if (tid == 0) {
+        mbar_init(&mbar);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::);
+    }
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem = tmem_base;
+    uint32_t phase = 0;
+    bool ok = true;
+    for (int k0 = 0; k0 < K; k0 += kTile) {
+        const int kc = min(kTile, K - k0);
+        for (int e = tid; e < kTile * kc; e += kThreads) {
+            const int r = e / kc, k = e - r * kc;
+            sA[cm_index(r, k)] = __float2bfloat16_rn(A.at(m0 + r, k0 + k));
+            sB[cm_index(r, k)] = __float2bfloat16_rn(B.at(r, k0 + k));
+        }
+        fence_proxy_async();
+        __syncthreads();
+        if (tid == 0) {
+            fence_after();
+            const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
+            for (int s = 0; s < kc / 16; ++s)
+                mma_bf16(tmem, sdesc(a0 + s * 256, kLBO, kSBO), sdesc(b0 + s * 256, kLBO, kSBO),
+                         (k0 > 0 || s > 0) ? 1u : 0u);
+            mma_commit(&mbar);
+        }
+        if (!mbar_wait(&mbar, phase)) ok = false;
+        phase ^= 1;
+        fence_after();
+        __syncthreads();
+        if (!ok) break;
+    }
+    if (ok) {
+        const long r = m0 + warp * 32 + lane;
+        for (int c = 0; c < kTile / 32; ++c) {
+            float v[32];
+            tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + c * 32, v);
+            if (r < Mrows) {
+#pragma unroll
+                for (int k = 0; k < 32; ++k) {
+                    const int n = c * 32 + k;
+                    const float z = v[k] + (bias ? bias[n] : 0.f);
+                    if (Z) Z[r * ldz + n] = z;
+                    O[r * ldo + n] = act ? gelu(z) : z;
+                }
+            }
+        }
+    } else if (tid == 0) {
+        atomicExch(err, 1);
+    }
+    fence_before();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tmem);
+}
+
+// G = dA * GELU'(Z) (elementwise, n x 128)
+__global__ void k_gelu_back(long n, const float *__restrict__ dA, const float *__restrict__ Z,
+                            float *__restrict__ G) {
+    const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < n * kTile) G[e] = dA[e] * gelu_grad(Z[e]);
+}
+
+// db[j] = sum_m G[m, j]
+__global__ void k_colsum(long n, const float *__restrict__ G, float *__restrict__ db) {
+    const int j = threadIdx.x;
+    float s = 0.f;
+    for (long m = blockIdx.x; m < n; m += gridDim.x) s += G[m * kTile + j];
+    atomicAdd(&db[j], s);
+}
+
+// MSE on the first nvalid outputs: dY = 2 (Y - T) / (n * nvalid), loss accumulated into *loss.
+__global__ void k_mse(long n, int nvalid, const float *__restrict__ Y, const float *__restrict__ T,
+                      float *__restrict__ dY, float *loss) {
+    const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    float l = 0.f;
+    if (e < n * kTile) {
+        const int j = (int)(e % kTile);
+        float g = 0.f;
+        if (j < nvalid) {
+            const float d = Y[e] - T[e];
+            g = 2.f * d / (float)(n * nvalid);
+            l = d * d / (float)(n * nvalid);
+        }
+        dY[e] = g;
+    }
+    for (int o = 16; o > 0; o >>= 1) l += __shfl_down_sync(0xffffffffu, l, o);
+    if ((threadIdx.x & 31) == 0 && l != 0.f) atomicAdd(loss, l);
+}
+
+// Adam step on FP32 master weights; refreshes the BF16 copy used by the tensor cores.
+__global__ void k_adam(long n, float *__restrict__ w, const float *__restrict__ g, float *__restrict__ m,
+                       float *__restrict__ v, __nv_bfloat16 *__restrict__ wb, float lr, float b1,
+                       float b2, float c1, float c2, float eps) {
+    const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    const float gg = g[e];
+    const float mm = b1 * m[e] + (1.f - b1) * gg;
+    const float vv = b2 * v[e] + (1.f - b2) * gg * gg;
+    m[e] = mm;
+    v[e] = vv;
+    const float ww = w[e] - lr * (mm / c1) / (sqrtf(vv / c2) + eps);
+    w[e] = ww;
+    if (wb) wb[e] = __float2bfloat16_rn(ww);
+}
+
+}  // namespace mlp
+}  // namespace sf
+
+// =============================================================================================
+// Feature extraction and output mapping (model state <-> MLP rows), one row per water column
+// =============================================================================================
+namespace sf {
+namespace mlp {
+
+// Rho-interior water column (the interior rho points of mod_cppkernels.cpp:20).
+__device__ __forceinline__ bool column_(int i, int j, int I, int J) {
+    return !(i == 0 || i == I - 1 || j == 0 || j == J - 1);
+}
+
+// Feature row of the column at p (rho-interior): 32 levels of log-scaled shear^2 and of
+// sign-preserving log-scaled N^2 at the interior W points (zero padded past N-1), then
+// log10 of the surface friction velocity squared, the surface buoyancy flux (0: no heat flux
+// in these basins) and log10 of the depth; the rest of the 128 inputs are 0.
+template <typename R>
+__global__ void k_features(Geo<R> g, const R *__restrict__ u, const R *__restrict__ v,
+                           const R *__restrict__ z_r, const R *__restrict__ bvf,
+                           const R *__restrict__ sustr, const R *__restrict__ svstr,
+                           float *__restrict__ X) {
+    const int pi = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    if (pi >= g.s2) return;
+    const long p = pi, I = g.I, s2 = g.s2;
+    const int N = g.N;
+    float *x = X + p * kTile;
+    for (int k = 0; k < kTile; ++k) x[k] = 0.f;
+    const int i = pi % g.I, j = pi / g.I;
+    if (!column_(i, j, g.I, g.J)) return;
+#define AT(A, k, q) ((float)(A)[(long)(k) * s2 + (q)])
+    for (int k = 1; k < N && k <= 32; ++k) {
+        const float cff = 0.5f / (AT(z_r, k, p) - AT(z_r, k - 1, p));
+        const float du = (AT(u, k, p) - AT(u, k - 1, p)) + (AT(u, k, p + 1) - AT(u, k - 1, p + 1));
+        const float dv = (AT(v, k, p) - AT(v, k - 1, p)) + (AT(v, k, p + I) - AT(v, k - 1, p + I));
+        const float sh2 = (cff * du) * (cff * du) + (cff * dv) * (cff * dv);
+        const float n2 = AT(bvf, k, p);
+        x[k - 1] = log10f(sh2 + 1e-12f);
+        x[32 + k - 1] = copysignf(log10f(1.f + fabsf(n2) * 1e8f), n2);
+    }
+    const float su = (float)(sustr[p] + sustr[p + 1]), sv = (float)(svstr[p] + svstr[p + I]);
+    x[64] = log10f(0.5f * sqrtf(su * su + sv * sv) + 1e-10f);
+    x[65] = 0.f;
+    x[66] = log10f((float)g.hd[p]);
+#undef AT
+}
+
+// Akv, Akt at interior W levels 1..N-1 from the outputs (log10, clipped to [-6, -1]); rows of
+// columns flagged in `fallback` (non-zero) keep the values already in Akv/Akt.
+template <typename R>
+__global__ void k_apply(Geo<R> g, const float *__restrict__ Y, const uint8_t *__restrict__ fallback,
+                        R *__restrict__ Akv, R *__restrict__ Akt) {
+    const int pi = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    if (pi >= g.s2) return;
+    const int i = pi % g.I, j = pi / g.I;
+    if (!column_(i, j, g.I, g.J)) return;
+    if (fallback && fallback[pi]) return;
+    const long p = pi, s2 = g.s2;
+    const float *y = Y + p * kTile;
+    for (int k = 1; k < g.N && k <= 32; ++k) {
+        Akv[(long)k * s2 + p] = (R)exp10f(fminf(fmaxf(y[k - 1], -6.f), -1.f));
+        Akt[(long)k * s2 + p] = (R)exp10f(fminf(fmaxf(y[32 + k - 1], -6.f), -1.f));
+    }
+}
+
+}  // namespace mlp
+}  // namespace sf
+
+// =============================================================================================
+// C ABI
+// =============================================================================================
+namespace {
+thread_local std::string g_mlp_err;
+int mfail(int code, const char *msg) {
+    g_mlp_err = msg;
+    return code;
+}
+int mcuda(cudaError_t e, const char *where) {
+    g_mlp_err = std::string(where) + ": " + cudaGetErrorString(e);
+    return SF_ECUDA;
+}
+inline cudaStream_t S(sf_stream s) { return reinterpret_cast<cudaStream_t>(s); }
+inline unsigned nblk(long n, int b) { return (unsigned)((n + b - 1) / b); }
+}  // namespace
+
+using sf::mlp::Mat;
+using sf::mlp::kTile;
+
+extern "C" {
+
+const char *sf_mlp_last_error(void) { return g_mlp_err.c_str(); }
+
+int sf_mlp_gemm(int n_rows, int K, const void *A, int a_bf16, long a_rs, long a_ks,
+                const void *B, int b_bf16, long b_rs, long b_ks, const float *bias, int act,
+                float *O, long ldo, float *Z, long ldz, int *err, sf_stream s) {
+    if (n_rows <= 0 || K <= 0 || K % 16 != 0) return mfail(SF_EINVAL, "K must be a positive multiple of 16");
+    if (!A || !B || !O || !err) return mfail(SF_EINVAL, "null pointer");
+    Mat a{A, a_bf16, a_rs, a_ks, n_rows, K}, b{B, b_bf16, b_rs, b_ks, kTile, K};
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e0 = cudaFuncSetAttribute(sf::mlp::k_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)sf::mlp::kGemmSmem);
+        if (e0 != cudaSuccess) return mcuda(e0, "sf_mlp_gemm");
+        attr = true;
+    }
+    sf::mlp::k_gemm<<<nblk(n_rows, kTile), sf::mlp::kThreads, sf::mlp::kGemmSmem, S(s)>>>(
+        a, b, n_rows, K, bias, act, O, ldo, Z, ldz, err);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? SF_OK : mcuda(e, "sf_mlp_gemm");
+}
+
+int sf_mlp_forward(const sf_mlp_params *w, int n, const float *X, float *Y, float *acts,
+                   float *pre, int *err, sf_stream s) {
+    if (!w || !X || !Y || n <= 0) return mfail(SF_EINVAL, "bad argument");
+    const long ld = kTile;
+    const float *in = X;
+    for (int l = 0; l < SF_MLP_LAYERS; ++l) {
+        const bool last = l == SF_MLP_LAYERS - 1;
+        float *out = last ? Y : (acts ? acts + (long)l * n * ld : nullptr);
+        if (!out) return mfail(SF_EINVAL, "activation buffer required");
+        float *z = pre ? pre + (long)l * n * ld : nullptr;
+        const int rc = sf_mlp_gemm(n, kTile, in, 0, ld, 1, w->W[l], 1, ld, 1, w->b[l], last ? 0 : 1,
+                                   out, ld, z, ld, err, s);
+        if (rc) return rc;
+        in = out;
+    }
+    return SF_OK;
+}
+
+int sf_mlp_backward(const sf_mlp_params *w, int n, const float *X, const float *acts,
+                    const float *pre, const float *dY, float *const *dW, float *const *db,
+                    float *work, int *err, sf_stream s) {
+    if (!w || !X || !acts || !pre || !dY || !dW || !db || !work || n <= 0 || n % 16)
+        return mfail(SF_EINVAL, "bad argument (n must be a multiple of 16)");
+    const long ld = kTile;
+    float *G = work, *dA = work + (long)n * ld;
+    const float *g_in = dY;   // gradient w.r.t. the current layer's output
+    for (int l = SF_MLP_LAYERS - 1; l >= 0; --l) {
+        const bool last = l == SF_MLP_LAYERS - 1;
+        if (!last) {
+            sf::mlp::k_gelu_back<<<nblk((long)n * ld, 256), 256, 0, S(s)>>>(n, g_in, pre + (long)l * n * ld, G);
+        } else {
+            cudaMemcpyAsync(G, g_in, sizeof(float) * n * ld, cudaMemcpyDeviceToDevice, S(s));
+        }
+        const float *Xl = l == 0 ? X : acts + (long)(l - 1) * n * ld;
+        // dW[out, in] = sum_m G[m, out] Xl[m, in]
+        int rc = sf_mlp_gemm(kTile, n, G, 0, 1, ld, Xl, 0, 1, ld, nullptr, 0, dW[l], ld, nullptr, 0,
+                             err, s);
+        if (rc) return rc;
+        cudaMemsetAsync(db[l], 0, sizeof(float) * kTile, S(s));
+        sf::mlp::k_colsum<<<256, kTile, 0, S(s)>>>(n, G, db[l]);
+        if (l > 0) {   // dA[m, in] = sum_out G[m, out] W[out, in]
+            rc = sf_mlp_gemm(n, kTile, G, 0, ld, 1, w->W[l], 1, 1, ld, nullptr, 0, dA, ld, nullptr, 0,
+                             err, s);
+            if (rc) return rc;
+            g_in = dA;
+            // the next iteration reads dA into G before dA is written again
+        }
+    }
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? SF_OK : mcuda(e, "sf_mlp_backward");
+}
+
+int sf_mlp_mse(int n, int nvalid, const float *Y, const float *T, float *dY, float *loss, sf_stream s) {
+    if (n <= 0 || !Y || !T || !dY || !loss) return mfail(SF_EINVAL, "bad argument");
+    sf::mlp::k_mse<<<nblk((long)n * kTile, 256), 256, 0, S(s)>>>(n, nvalid, Y, T, dY, loss);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? SF_OK : mcuda(e, "sf_mlp_mse");
+}
+
+int sf_mlp_adam(long n, float *w, const float *g, float *m, float *v, void *w_bf16, float lr,
+                float b1, float b2, int step, float eps, sf_stream s) {
+    if (n <= 0 || !w || !g || !m || !v || step < 1) return mfail(SF_EINVAL, "bad argument");
+    const float c1 = 1.f - powf(b1, (float)step), c2 = 1.f - powf(b2, (float)step);
+    sf::mlp::k_adam<<<nblk(n, 256), 256, 0, S(s)>>>(n, w, g, m, v, (__nv_bfloat16 *)w_bf16, lr, b1, b2,
+                                                     c1, c2, eps);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? SF_OK : mcuda(e, "sf_mlp_adam");
+}
+
+int sf_closure_features(sf_ctx *c, const void *u, const void *v, const void *z_r, const void *bvf,
+                        const void *sustr, const void *svstr, float *X, sf_stream s) {
+    if (!c || !X) return mfail(SF_EINVAL, "bad argument");
+    cudaError_t e;
+    if (c->prec == SF_FP64) {
+        auto g = sf::Ops<double>::geo(c);
+        sf::mlp::k_features<double><<<nblk(c->s2, 128), 128, 0, S(s)>>>(
+            g, (const double *)u, (const double *)v, (const double *)z_r, (const double *)bvf,
+            (const double *)sustr, (const double *)svstr, X);
+    } else {
+        auto g = sf::Ops<float>::geo(c);
+        sf::mlp::k_features<float><<<nblk(c->s2, 128), 128, 0, S(s)>>>(
+            g, (const float *)u, (const float *)v, (const float *)z_r, (const float *)bvf,
+            (const float *)sustr, (const float *)svstr, X);
+    }
+    e = cudaGetLastError();
+    return e == cudaSuccess ? SF_OK : mcuda(e, "sf_closure_features");
+}
+
+int sf_closure_apply(sf_ctx *c, const float *Y, const uint8_t *fallback, void *Akv, void *Akt,
+                     sf_stream s) {
+    if (!c || !Y) return mfail(SF_EINVAL, "bad argument");
+    if (c->prec == SF_FP64) {
+        auto g = sf::Ops<double>::geo(c);
+        sf::mlp::k_apply<double><<<nblk(c->s2, 128), 128, 0, S(s)>>>(g, Y, fallback, (double *)Akv,
+                                                                      (double *)Akt);
+    } else {
+        auto g = sf::Ops<float>::geo(c);
+        sf::mlp::k_apply<float><<<nblk(c->s2, 128), 128, 0, S(s)>>>(g, Y, fallback, (float *)Akv,
+                                                                     (float *)Akt);
+    }
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? SF_OK : mcuda(e, "sf_closure_apply");
+}
+
+}  // extern "C"
