@@ -221,6 +221,18 @@ int sf_mlp_forward(const sf_mlp_params *w, int n, const float *X, float *Y, floa
 int sf_mlp_backward(const sf_mlp_params *w, int n, const float *X, const float *acts,
                     const float *pre, const float *dY, float *const *dW, float *const *db,
                     float *work, int *err, sf_stream stream);
+/* sf_mlp_backward without the `work` argument, for callers that cannot allocate device memory
+ * where they train (an application that owns all device memory through its own pool, or a
+ * latency-critical loop that may not call an allocator).  No counterpart in the reference.
+ * Its scratch is a fixed 2 MiB device array inside the library, held by every GPU that loads
+ * it until the process exits; n <= 2048 rows, larger n is rejected with SF_EINVAL.  The first
+ * call on a device looks up that array's device address (cudaGetSymbolAddress), so make it
+ * before any stream capture.  All calls share the array and leave their intermediate values
+ * in it (every value read is written first by the same call): calls that overlap on the GPU
+ * (different streams, or devices sharing nothing but this library) race. */
+int sf_mlp_backward_static(const sf_mlp_params *w, int n, const float *X, const float *acts,
+                           const float *pre, const float *dY, float *const *dW, float *const *db,
+                           int *err, sf_stream stream);
 /* Mean squared error over the first nvalid outputs of each row; adds the loss into *loss. */
 int sf_mlp_mse(int n, int nvalid, const float *Y, const float *T, float *dY, float *loss,
                sf_stream stream);

@@ -83,6 +83,8 @@ SIGNATURES = {
     "sf_mlp_forward": [ctypes.POINTER(MlpParams), _i, _vp, _vp, _vp, _vp, _vp, _vp],
     "sf_mlp_backward": [ctypes.POINTER(MlpParams), _i, _vp, _vp, _vp, _vp, ctypes.POINTER(_vp),
                         ctypes.POINTER(_vp), _vp, _vp, _vp],
+    "sf_mlp_backward_static": [ctypes.POINTER(MlpParams), _i, _vp, _vp, _vp, _vp,
+                               ctypes.POINTER(_vp), ctypes.POINTER(_vp), _vp, _vp],
     "sf_mlp_mse": [_i, _i, _vp, _vp, _vp, _vp, _vp],
     "sf_mlp_adam": [ctypes.c_long, _vp, _vp, _vp, _vp, _vp, ctypes.c_float, ctypes.c_float,
                     ctypes.c_float, _i, ctypes.c_float, _vp],

@@ -477,4 +477,39 @@ int sf_closure_apply(sf_ctx *c, const float *Y, const uint8_t *fallback, void *A
     return e == cudaSuccess ? SF_OK : mcuda(e, "sf_closure_apply");
 }
 
+// ---- allocation-free backward pass ----------------------------------------------------------
+// Some callers of this library cannot allocate device memory at the point where they train:
+// a host application that owns every device byte through its own pool and forbids other
+// allocators, or a training step issued from a latency-critical loop where an allocator call
+// (which can synchronise the device or take a process-wide lock) is not allowed.  For them the
+// backward pass's scratch lives in this fixed, file-scope device array instead of a caller
+// buffer.  Every GPU that loads the library holds it (2 MiB) until the process exits.
+constexpr int kStaticMaxRows = 2048;
+static __device__ __align__(256) float g_static_work[2 * kStaticMaxRows * SF_MLP_WIDTH];
+
+namespace {
+constexpr int kMaxDevices = 64;
+float *g_static_work_addr[kMaxDevices] = {};   // device address of g_static_work, per device
+}  // namespace
+
+int sf_mlp_backward_static(const sf_mlp_params *w, int n, const float *X, const float *acts,
+                           const float *pre, const float *dY, float *const *dW, float *const *db,
+                           int *err, sf_stream s) {
+    if (n > kStaticMaxRows)
+        return mfail(SF_EINVAL, "sf_mlp_backward_static: n exceeds the 2048 rows of its fixed scratch");
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return mcuda(e, "sf_mlp_backward_static");
+    if (dev < 0 || dev >= kMaxDevices) return mfail(SF_EINVAL, "device ordinal out of range");
+    if (!g_static_work_addr[dev]) {
+        // First call on this device (with it current): the array's name is only a host-side
+        // stand-in, so look up its device address once.
+        void *ptr = nullptr;
+        e = cudaGetSymbolAddress(&ptr, g_static_work);
+        if (e != cudaSuccess) return mcuda(e, "cudaGetSymbolAddress");
+        g_static_work_addr[dev] = static_cast<float *>(ptr);
+    }
+    return sf_mlp_backward(w, n, X, acts, pre, dY, dW, db, g_static_work_addr[dev], err, s);
+}
+
 }  // extern "C"
