@@ -31,6 +31,37 @@ MEASURED = os.path.join(ROOT, "MEASURED_PEAKS.json")
 METRIC = "3D cell-steps/s"
 
 
+class _StdoutToStderr:
+    """Sends the process's C-level stdout to stderr for the duration (the reference's host
+    kernels print from C), so that stdout carries the JSON line alone."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        os.dup2(2, 1)
+
+    def __exit__(self, *a):
+        sys.stdout.flush()
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+
+
+def traffic_per_launch(kernel, grid):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary (profiles/), scaled
+    from its basin to this grid by the number of 3D points; None if not recorded."""
+    path = os.path.join(ROOT, "profiles", "k3d_basin4q_fp32.md")
+    try:
+        with open(path) as f:
+            for line in f:
+                t = line.split()
+                if len(t) == 6 and t[0] == "traffic" and t[1] == kernel:
+                    rd, wr, s2, n = (float(x) for x in t[2:])
+                    return (rd + wr) * (grid.s2 * grid.N) / (s2 * n)
+    except OSError:
+        pass
+    return None
+
+
 def peaks():
     try:
         with open(MEASURED) as f:
@@ -71,10 +102,11 @@ def reference_cpu(config, nsteps, omp):
     O = orc.Ocean(og)
     nfast, w1, w2 = host.set_weights(sub["ndtfast"])
     ct = orc.CompTimes(sub["dt"], sub["ndtfast"], nfast, w1, w2)
-    ref_driver.main3d(og, orc.Boundary(bd), O, ct, 1, omp=omp)      # warm-up
-    t0 = time.perf_counter()
-    ref_driver.main3d(og, orc.Boundary(bd), O, ct, nsteps, omp=omp)
-    dt = time.perf_counter() - t0
+    with _StdoutToStderr():
+        ref_driver.main3d(og, orc.Boundary(bd), O, ct, 1, omp=omp)      # warm-up
+        t0 = time.perf_counter()
+        ref_driver.main3d(og, orc.Boundary(bd), O, ct, nsteps, omp=omp)
+        dt = time.perf_counter() - t0
     cells = (sg.L - 1) * (sg.M - 1) * sg.N
     sample = ("reference kernels (oracle/_ref, g++ -O2) in main3d order on a %dx%dx%d sub-basin of "
               "%s (same recipe, dt, ndtfast), %d baroclinic steps, %d OpenMP threads"
@@ -97,7 +129,7 @@ class Clocks:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
-                 "--format=csv,noheader,nounits", "-lms", "100"],
+                 "--format=csv,noheader,nounits", "-lms", "20"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -138,6 +170,72 @@ def algorithmic_bytes(grid, esize):
         "k_maxflux_omega": esize * (4 * N + 3 * (N + 1)) * s2,  # u,v,Hz,z_w -> Huon,Hvom,W
         "k_set_depth": esize * (3 * N + 1) * s2 + 16 * s2,      # Zt,h -> z_w,z_r,Hz
     }
+
+
+def time_steps(m, steps, warmup):
+    """Device time (ms) of `steps` baroclinic steps after `warmup` untimed ones."""
+    import torch
+    stream = torch.cuda.current_stream()
+    m.step(warmup)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    m.step(steps)
+    b.record(stream)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b)
+
+
+def plain_fp64(args):
+    """The same workload through the FP64 path, whose results are bit-identical to the
+    reference's own kernels (the 'plain FP64 step' the FP32 form is compared with)."""
+    import torch
+    from sailfish_b200 import configs
+    from sailfish_b200.model import Model
+    cfg = configs.CONFIGS[args.config]()
+    g = cfg["grid"]
+    m = Model(g, cfg["boundary"], cfg["dt"], cfg["ndtfast"], precision="fp64")
+    steps = max(1, min(args.steps, 3))
+    ms = time_steps(m, steps, 3)
+    cells = (g.L - 1) * (g.M - 1) * g.N
+    del m
+    torch.cuda.empty_cache()
+    return {"value": cells * steps / (ms * 1e-3), "unit": "cell-steps/s",
+            "ms_per_step": ms / steps, "steps": steps, "warmup": 3, "dtype": "f64",
+            "semantics": "bit-identical to the reference kernels"}
+
+
+def error_vs_fp64():
+    """One baroclinic step of a 512x512x32 basin (basin1's recipe, square so that the
+    reference's flat-index guards stay inside the fields) from a 1 mm Gaussian surface bump,
+    FP32 form against the FP64 path from identical inputs: RMS and max absolute error."""
+    import torch
+    from sailfish_b200 import configs
+    from sailfish_b200.model import Model
+    cfg = configs.basin(512, 512, 32, 2.0e3, [(0.5, 0.6)], dt=240.0, ndtfast=30)
+    g = cfg["grid"]
+    x, y = g.x, g.y
+    bump = 1e-3 * np.exp(-((x - x.max() / 2) ** 2 + (y - y.max() / 3) ** 2) / (50e3) ** 2)
+    res = {}
+    for prec in ("fp64", "fp32"):
+        m = Model(g, cfg["boundary"], cfg["dt"], cfg["ndtfast"], precision=prec)
+        m.Zt_avg1.copy_(torch.from_numpy(bump.ravel()))
+        m.step(1)
+        torch.cuda.synchronize()
+        res[prec] = {"zeta": m._slot("zeta", 2).double().cpu().numpy(),
+                     "ubar": m._slot("ubar", 2).double().cpu().numpy(),
+                     "u": m.u.double().cpu().numpy(), "v": m.v.double().cpu().numpy()}
+        del m
+    out = {"case": "512x512x32 basin, dx 2 km, dt 240 s, ndtfast 30, 1 mm bump, 1 step",
+           "units": {"zeta": "m", "ubar": "m/s", "u": "m/s", "v": "m/s"}}
+    for k in ("zeta", "ubar", "u", "v"):
+        a, b = res["fp64"][k], res["fp32"][k]
+        d = b - a
+        out[k] = {"rms": float(np.sqrt(np.mean(d * d))), "max": float(np.abs(d).max()),
+                  "rms_fp64_field": float(np.sqrt(np.mean(a * a))),
+                  "finite": bool(np.isfinite(b).all() and np.isfinite(a).all())}
+    torch.cuda.empty_cache()
+    return out
 
 
 def run_ours(args, rank, world):
@@ -205,7 +303,10 @@ def run_ours(args, rank, world):
     peak, kind = peaks()
     achieved = ab[dom] / (per_phase[dom] * 1e-3) / 1e9
     value = cells * args.steps * world / (ms * 1e-3)
-    n_launch_2d = 5 * (m.nfast + 1) + 3 * (m.nfast + 1) + 2
+    # per baroclinic step: maxflux_omega, rhs3d, set_depth, step3d_uv, and per barotropic
+    # substep 2 zeta_rhs + 1 momentum + 1 corrector point + 3 boundary programs, plus the
+    # closing momentum RHS; one omega at the end of the timed call
+    per_step = 4 + 7 * (m.nfast + 1) + 1
     out = {
         "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
@@ -220,10 +321,13 @@ def run_ours(args, rank, world):
         "phases_ms": per_phase,
         "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_kind": kind,
-                     "algorithmic_bytes": ab[dom], "traffic": None},
+                     "algorithmic_bytes": ab[dom],
+                     "traffic": traffic_per_launch(dom, grid) if args.precision == "fp32" else None,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum on basin4q "
+                                       "(profiles/k3d_basin4q_fp32.md), scaled by 3D points"},
         "e2e": {"value": cells / (e_ms * 1e-3), "unit": "cell-steps/s",
                 "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo},
-        "gpu_launches": args.steps * (4 + n_launch_2d),
+        "gpu_launches": args.steps * per_step + 1,
         "clocks": clk.summary(),
     }
     return out
@@ -232,13 +336,15 @@ def run_ours(args, rank, world):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="basin4")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
-    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--cpu-steps", type=int, default=40)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 timing")
+    ap.add_argument("--no-error", action="store_true", help="skip the FP32-vs-FP64 error case")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -268,6 +374,12 @@ def main():
             "nccl", timeout=__import__("datetime").timedelta(seconds=120))
     out = run_ours(args, rank, world)
     if rank == 0:
+        if args.precision == "fp32" and not args.no_fp64:
+            torch.cuda.empty_cache()
+            out["plain_fp64"] = plain_fp64(args)
+            out["plain_fp64"]["speedup_of_value"] = out["value"] / world / out["plain_fp64"]["value"]
+        if not args.no_error:
+            out["error_vs_fp64"] = error_vs_fp64()
         if not args.no_cpu_baseline:
             try:
                 v, cores, sample = reference_cpu(args.config, args.cpu_steps, omp)

@@ -190,6 +190,20 @@ int sf_gls_corrector(sf_ctx *ctx, const sf_gls_params *params, double dt, const 
                      const void *v, const void *z_r, const void *Hz, const void *bvf,
                      const void *sustr, const void *svstr, void *tke, void *gls, void *Akv,
                      void *Akt, void *Akk, void *Akp, void *Lscale, sf_stream stream);
+/* sf_gls_corrector on the rho-interior columns p with columns[p] != 0 only (the closure's
+ * fallback columns); the other columns' fields are left as they are.  No counterpart in the
+ * reference. */
+int sf_gls_corrector_cols(sf_ctx *ctx, const sf_gls_params *params, double dt, const void *u,
+                          const void *v, const void *z_r, const void *Hz, const void *bvf,
+                          const void *sustr, const void *svstr, void *tke, void *gls, void *Akv,
+                          void *Akt, void *Akk, void *Akp, void *Lscale, const uint8_t *columns,
+                          sf_stream stream);
+/* Buoyancy frequency squared at all N+1 W levels of a linear equation of state in temperature
+ * (alpha, 1/degC) with the analytic profile T(z) = T0 + dT exp(z/zscale):
+ * bvf = g alpha dT/zscale exp(z_w/zscale).  The stratification of the analytic basins, whose
+ * tracers are not stepped (the reference's time step has no tracer equation either). */
+int sf_analytic_bvf(sf_ctx *ctx, const void *z_w, double dT, double zscale, double alpha, double g,
+                    void *bvf, sf_stream stream);
 
 /* ---- learned closure (no counterpart in the reference) --------------------------------------
  * A per-column MLP standing in for the GLS corrector's Akv/Akt: SF_MLP_LAYERS dense layers of
@@ -216,6 +230,11 @@ int sf_mlp_gemm(int n_rows, int K, const void *A, int a_bf16, long a_rs, long a_
  * hidden activations and pre-activations for the backward pass (acts required). */
 int sf_mlp_forward(const sf_mlp_params *w, int n, const float *X, float *Y, float *acts,
                    float *pre, int *err, sf_stream stream);
+/* Inference only: the same outputs as sf_mlp_forward (up to the GELU's hardware tanh) from one
+ * fused pass that keeps every layer's weights and the tile's activations on chip, reading X
+ * and writing Y only (n x 128 FP32 each, 16-byte aligned rows). */
+int sf_mlp_infer(const sf_mlp_params *w, int n, const float *X, float *Y, int *err,
+                 sf_stream stream);
 /* Backward pass: weight and bias gradients dW[l] (128 x 128 FP32), db[l] (128) for output
  * gradient dY; `work` is 2 x n x 128 FP32 scratch; n a multiple of 16. */
 int sf_mlp_backward(const sf_mlp_params *w, int n, const float *X, const float *acts,
@@ -244,6 +263,11 @@ int sf_mlp_adam(long n, float *w, const float *g, float *m, float *v, void *w_bf
 int sf_closure_features(sf_ctx *ctx, const void *u, const void *v, const void *z_r,
                         const void *bvf, const void *sustr, const void *svstr, float *X,
                         sf_stream stream);
+/* mask[p] = 1 for each rho-interior column whose feature row (from sf_closure_features) has
+ * any of its first nfeat features outside [lo[k], hi[k]] (NaN included): the columns the
+ * network was not trained for, which plain GLS handles (sf_gls_corrector_cols); else 0. */
+int sf_closure_range_mask(sf_ctx *ctx, const float *X, int nfeat, const float *lo,
+                          const float *hi, uint8_t *mask, sf_stream stream);
 /* Akv and Akt at the interior W levels from the network outputs (log10, clipped to
  * [1e-6, 1e-1] m2/s), except on columns flagged in `fallback` (may be NULL). */
 int sf_closure_apply(sf_ctx *ctx, const float *Y, const uint8_t *fallback, void *Akv, void *Akt,

@@ -77,10 +77,13 @@ SIGNATURES = {
     "sf_lateral_uv_bc": [_vp, _d, _vp, _vp, _vp],
     "sf_step3d_uv_bc": [_vp] * 14 + [_i, _i, _d, _d, _d, _vp],
     "sf_gls_corrector": [_vp, ctypes.POINTER(GlsParams), _d] + [_vp] * 14 + [_vp],
+    "sf_gls_corrector_cols": [_vp, ctypes.POINTER(GlsParams), _d] + [_vp] * 15 + [_vp],
+    "sf_analytic_bvf": [_vp, _vp, _d, _d, _d, _d, _vp, _vp],
     "sf_mlp_last_error": [],
     "sf_mlp_gemm": [_i, _i, _vp, _i, ctypes.c_long, ctypes.c_long, _vp, _i, ctypes.c_long,
                     ctypes.c_long, _vp, _i, _vp, ctypes.c_long, _vp, ctypes.c_long, _vp, _vp],
     "sf_mlp_forward": [ctypes.POINTER(MlpParams), _i, _vp, _vp, _vp, _vp, _vp, _vp],
+    "sf_mlp_infer": [ctypes.POINTER(MlpParams), _i, _vp, _vp, _vp, _vp],
     "sf_mlp_backward": [ctypes.POINTER(MlpParams), _i, _vp, _vp, _vp, _vp, ctypes.POINTER(_vp),
                         ctypes.POINTER(_vp), _vp, _vp, _vp],
     "sf_mlp_backward_static": [ctypes.POINTER(MlpParams), _i, _vp, _vp, _vp, _vp,
@@ -90,6 +93,7 @@ SIGNATURES = {
                     ctypes.c_float, _i, ctypes.c_float, _vp],
     "sf_closure_features": [_vp] * 9,
     "sf_closure_apply": [_vp] * 6,
+    "sf_closure_range_mask": [_vp, _vp, _i, _vp, _vp, _vp, _vp],
 }
 
 

@@ -8,6 +8,7 @@ Gaussian seamounts, beta-plane Coriolis, S-coordinates with Vtransform 2 / Vstre
           dt=240 s, ndtfast=30
   basin4: Lm=2048, Mm=1024, N=50, dx=1 km, same recipe with two seamounts, dt=120 s,
           ndtfast=40
+  basin4q: Lm=1024, Mm=512, N=50, dx=2 km, basin4's recipe at a quarter of its area
 """
 import numpy as np
 
@@ -56,8 +57,15 @@ def basin4():
     return basin(2048, 1024, 50, 1.0e3, [(1.0 / 3.0, 0.6), (2.0 / 3.0, 0.6)], dt=120.0, ndtfast=40)
 
 
+def basin4q():
+    """A quarter of basin4 (Lm=1024, Mm=512, N=50, dx=2 km): the profiling case, with 3D
+    fields of ~0.1 GB (FP32) so that kernels stream from DRAM rather than L2."""
+    return basin(1024, 512, 50, 2.0e3, [(1.0 / 3.0, 0.6), (2.0 / 3.0, 0.6)], dt=120.0,
+                 ndtfast=40)
+
+
 def small(Lm=256, Mm=128, N=32):
     return basin(Lm, Mm, N, 2.0e3, [(0.5, 0.6)], dt=240.0, ndtfast=30)
 
 
-CONFIGS = {"basin1": basin1, "basin4": basin4, "small": small}
+CONFIGS = {"basin1": basin1, "basin4": basin4, "basin4q": basin4q, "small": small}

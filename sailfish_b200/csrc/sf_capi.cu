@@ -571,6 +571,15 @@ int sf_gls_corrector(sf_ctx *c, const sf_gls_params *P, double dt, const void *u
                      const void *z_r, const void *Hz, const void *bvf, const void *sustr,
                      const void *svstr, void *tke, void *gls, void *Akv, void *Akt, void *Akk,
                      void *Akp, void *Lscale, sf_stream s) {
+    return sf_gls_corrector_cols(c, P, dt, u, v, z_r, Hz, bvf, sustr, svstr, tke, gls, Akv, Akt,
+                                 Akk, Akp, Lscale, nullptr, s);
+}
+
+int sf_gls_corrector_cols(sf_ctx *c, const sf_gls_params *P, double dt, const void *u,
+                          const void *v, const void *z_r, const void *Hz, const void *bvf,
+                          const void *sustr, const void *svstr, void *tke, void *gls, void *Akv,
+                          void *Akt, void *Akk, void *Akp, void *Lscale, const uint8_t *columns,
+                          sf_stream s) {
     if (!P) return fail(SF_EINVAL, "null GLS parameters");
     if (P->n == 0.0) return fail(SF_EINVAL, "GLS exponent n must be non-zero");
     if (P->p == 0.0 && P->m == 1.0 && P->n == 1.0)
@@ -581,7 +590,16 @@ int sf_gls_corrector(sf_ctx *c, const sf_gls_params *P, double dt, const void *u
         return sf::Ops<R>::gls_corrector(c, *P, dt, (const R *)u, (const R *)v, (const R *)z_r,
                                          (const R *)Hz, (const R *)bvf, (const R *)sustr,
                                          (const R *)svstr, (R *)tke, (R *)gls, (R *)Akv, (R *)Akt,
-                                         (R *)Akk, (R *)Akp, (R *)Lscale, S(s));
+                                         (R *)Akk, (R *)Akp, (R *)Lscale, columns, S(s));
+    });
+}
+
+int sf_analytic_bvf(sf_ctx *c, const void *z_w, double dT, double zscale, double alpha, double g,
+                    void *bvf, sf_stream s) {
+    if (!(zscale > 0.0)) return fail(SF_EINVAL, "zscale must be positive");
+    return dispatch(c, "sf_analytic_bvf", [&](auto *t) {
+        using R = std::remove_pointer_t<decltype(t)>;
+        return sf::Ops<R>::analytic_bvf(c, (const R *)z_w, dT, zscale, g * alpha, (R *)bvf, S(s));
     });
 }
 

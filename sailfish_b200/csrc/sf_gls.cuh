@@ -34,11 +34,12 @@ __global__ void __launch_bounds__(128) k_gls_corrector(
     Geo<R> g, sf_gls_params P, R dt, const R *__restrict__ u, const R *__restrict__ v,
     const R *__restrict__ z_r, const R *__restrict__ Hz, const R *__restrict__ bvf,
     const R *__restrict__ sustr, const R *__restrict__ svstr, R *tke, R *gls, R *Akv, R *Akt,
-    R *Akk, R *Akp, R *Lscale) {
+    R *Akk, R *Akp, R *Lscale, const uint8_t *__restrict__ sel) {
     const int pi = (int)tid_flat();
     if (pi >= g.s2) return;
     const int i = pi % g.I, j = pi / g.I;
     if (!rint_(i, j, g.I, g.J)) return;
+    if (sel && !sel[pi]) return;   // column not selected: left as it is
     const long p = pi, I = g.I, s2 = g.s2;
     const int N = g.N;
     R FCK[kNMax + 1], FCP[kNMax + 1], BCK[kNMax + 1], BCP[kNMax + 1], tk[kNMax + 1], gl[kNMax + 1],

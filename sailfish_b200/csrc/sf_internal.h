@@ -100,7 +100,10 @@ struct Ops {
     static cudaError_t gls_corrector(const sf_ctx *c, const sf_gls_params &P, double dt,
                                      const R *u, const R *v, const R *z_r, const R *Hz,
                                      const R *bvf, const R *sustr, const R *svstr, R *tke, R *gls,
-                                     R *Akv, R *Akt, R *Akk, R *Akp, R *Lscale, cudaStream_t s);
+                                     R *Akv, R *Akt, R *Akk, R *Akp, R *Lscale,
+                                     const uint8_t *sel, cudaStream_t s);
+    static cudaError_t analytic_bvf(const sf_ctx *c, const R *z_w, double dT, double zscale,
+                                    double galpha, R *bvf, cudaStream_t s);
 };
 
 extern template struct Ops<double>;

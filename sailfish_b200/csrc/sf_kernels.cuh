@@ -879,10 +879,30 @@ template <typename R>
 cudaError_t Ops<R>::gls_corrector(const sf_ctx *c, const sf_gls_params &P, double dt, const R *u,
                                   const R *v, const R *z_r, const R *Hz, const R *bvf,
                                   const R *sustr, const R *svstr, R *tke, R *gls, R *Akv, R *Akt,
-                                  R *Akk, R *Akp, R *Lscale, cudaStream_t s) {
+                                  R *Akk, R *Akp, R *Lscale, const uint8_t *sel,
+                                  cudaStream_t s) {
     k_gls_corrector<R><<<blocks_for(c->s2, 128), 128, 0, s>>>(geo(c), P, (R)dt, u, v, z_r, Hz, bvf,
                                                               sustr, svstr, tke, gls, Akv, Akt,
-                                                              Akk, Akp, Lscale);
+                                                              Akk, Akp, Lscale, sel);
+    return cudaGetLastError();
+}
+
+
+// Buoyancy frequency squared at every W level for a linear equation of state in temperature
+// alone, with T(z) = T0 + dT exp(z / zscale): N^2 = g alpha dT/dz.  The stratification of the
+// analytic basins (their tracers are not stepped, so N^2 follows z_w).
+template <typename R>
+__global__ void k_analytic_bvf(long n, const R *__restrict__ z_w, double dT, double zscale,
+                               double galpha, R *__restrict__ bvf) {
+    const long e = tid_flat();
+    if (e >= n) return;
+    bvf[e] = (R)(galpha * (dT / zscale) * exp((double)z_w[e] / zscale));
+}
+template <typename R>
+cudaError_t Ops<R>::analytic_bvf(const sf_ctx *c, const R *z_w, double dT, double zscale,
+                                 double galpha, R *bvf, cudaStream_t s) {
+    const long n = (long)(c->N + 1) * c->s2;
+    k_analytic_bvf<R><<<blocks_for(n, kBlock), kBlock, 0, s>>>(n, z_w, dT, zscale, galpha, bvf);
     return cudaGetLastError();
 }
 

@@ -261,6 +261,129 @@ __global__ void k_adam(long n, float *__restrict__ w, const float *__restrict__ 
     if (wb) wb[e] = __float2bfloat16_rn(ww);
 }
 
+// ---- fused inference -----------------------------------------------------------------------
+// All SF_MLP_LAYERS layers of a 128-row tile in one pass: the BF16 weights of every layer stay
+// in shared memory for the life of the (persistent, one per SM) CTA, the activations of the
+// tile stay in shared memory between layers, and only the input rows are read and the output
+// rows written.  Per layer: 8 MMAs (K = 128) into the TMEM accumulator, then 8 warps read it
+// back (warp w: TMEM lanes 32(w%4).., columns 64(w/4)..), add the bias, apply the GELU and
+// write the next layer's BF16 operand in place of the current one.
+constexpr int kInferThreads = 256;
+constexpr size_t kInferSmem = (size_t)(1 + SF_MLP_LAYERS) * kTile * kTile * 2;
+
+struct InferW {
+    const __nv_bfloat16 *W[SF_MLP_LAYERS];
+    const float *b[SF_MLP_LAYERS];
+};
+
+// GELU, tanh form, with the hardware tanh approximation (relative error ~2^-11, below the BF16
+// rounding of the activations it feeds).
+__device__ __forceinline__ float gelu_fast(float x) {
+    const float c = 0.7978845608028654f;
+    float t;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(c * (x + 0.044715f * x * x * x)));
+    return 0.5f * x * (1.f + t);
+}
+
+__global__ void __launch_bounds__(kInferThreads, 1) k_infer(InferW w, long n,
+                                                            const float *__restrict__ X,
+                                                            float *__restrict__ Y, int *err) {
+    extern __shared__ __align__(1024) unsigned char dsm[];
+    __nv_bfloat16 *sA = reinterpret_cast<__nv_bfloat16 *>(dsm);
+    __nv_bfloat16 *sW = sA + kTile * kTile;
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ uint32_t tmem_base;
+    __shared__ float sbias[SF_MLP_LAYERS][kTile];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (warp == 0) tmem_alloc(&tmem_base);
+    if (tid == 0) {
+        mbar_init(&mbar);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::);
+    }
+    for (int l = 0; l < SF_MLP_LAYERS; ++l) {
+        for (int e = tid; e < kTile * kTile; e += kInferThreads)
+            sW[l * kTile * kTile + cm_index(e >> 7, e & 127)] = w.W[l][e];
+        for (int e = tid; e < kTile; e += kInferThreads) sbias[l][e] = w.b[l] ? w.b[l][e] : 0.f;
+    }
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem = tmem_base;
+    const int rl = (warp & 3) * 32 + lane;        // tile row of this thread in the epilogue
+    const int cb = (warp >> 2) * 64;              // first of its 64 columns
+    const uint32_t trow = (uint32_t)((warp & 3) * 32) << 16;
+    uint32_t phase = 0;
+    bool ok = true;
+    const long ntiles = (n + kTile - 1) / kTile;
+    for (long t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+        const long m0 = t * kTile;
+        // stage the input tile: 16 float4 in flight per thread, then BF16 into the operand
+        {
+            float4 q[16];
+#pragma unroll
+            for (int u = 0; u < 16; ++u) {
+                const int e4 = tid + u * kInferThreads;   // float4 index in the 128 x 32 tile
+                const long r = m0 + (e4 >> 5);
+                q[u] = r < n ? reinterpret_cast<const float4 *>(X + r * kTile)[e4 & 31]
+                             : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+#pragma unroll
+            for (int u = 0; u < 16; ++u) {
+                const int e4 = tid + u * kInferThreads;
+                const int r = e4 >> 5, k = (e4 & 31) * 4;
+                sA[cm_index(r, k + 0)] = __float2bfloat16_rn(q[u].x);
+                sA[cm_index(r, k + 1)] = __float2bfloat16_rn(q[u].y);
+                sA[cm_index(r, k + 2)] = __float2bfloat16_rn(q[u].z);
+                sA[cm_index(r, k + 3)] = __float2bfloat16_rn(q[u].w);
+            }
+        }
+        for (int l = 0; l < SF_MLP_LAYERS; ++l) {
+            fence_proxy_async();
+            __syncthreads();
+            if (tid == 0) {
+                fence_after();
+                const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sW + l * kTile * kTile);
+                for (int s = 0; s < kTile / 16; ++s)
+                    mma_bf16(tmem, sdesc(a0 + s * 256, kLBO, kSBO), sdesc(b0 + s * 256, kLBO, kSBO),
+                             s > 0 ? 1u : 0u);
+                mma_commit(&mbar);
+            }
+            const bool done = mbar_wait(&mbar, phase);
+            phase ^= 1;
+            fence_after();
+            if (__syncthreads_or(!done)) {
+                ok = false;
+                break;
+            }
+            const bool last = l == SF_MLP_LAYERS - 1;
+            const long r = m0 + rl;
+            for (int c = 0; c < 2; ++c) {
+                float v[32];
+                tmem_ld32(tmem + trow + cb + c * 32, v);
+                const int n0 = cb + c * 32;
+                if (!last) {
+#pragma unroll
+                    for (int k = 0; k < 32; ++k)
+                        sA[cm_index(rl, n0 + k)] = __float2bfloat16_rn(gelu_fast(v[k] + sbias[l][n0 + k]));
+                } else if (r < n) {
+                    float4 *y = reinterpret_cast<float4 *>(Y + r * kTile + n0);
+#pragma unroll
+                    for (int k = 0; k < 8; ++k)
+                        y[k] = make_float4(v[4 * k] + sbias[l][n0 + 4 * k],
+                                           v[4 * k + 1] + sbias[l][n0 + 4 * k + 1],
+                                           v[4 * k + 2] + sbias[l][n0 + 4 * k + 2],
+                                           v[4 * k + 3] + sbias[l][n0 + 4 * k + 3]);
+                }
+            }
+            fence_before();
+        }
+    }
+    if (!ok && tid == 0) atomicExch(err, 1);
+    fence_before();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tmem);
+}
+
 }  // namespace mlp
 }  // namespace sf
 
@@ -273,6 +396,22 @@ namespace mlp {
 // Rho-interior water column (the interior rho points of mod_cppkernels.cpp:20).
 __device__ __forceinline__ bool column_(int i, int j, int I, int J) {
     return !(i == 0 || i == I - 1 || j == 0 || j == J - 1);
+}
+
+// mask[p] = 1 for a rho-interior column whose feature row leaves the box [lo, hi] in any of
+// its first nfeat features (a column outside the range the network was trained on), else 0.
+__global__ void k_range_mask(long s2, int I, int J, int nfeat, const float *__restrict__ X,
+                             const float *__restrict__ lo, const float *__restrict__ hi,
+                             uint8_t *__restrict__ mask) {
+    const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= s2) return;
+    uint8_t out = 0;
+    if (column_((int)(p % I), (int)(p / I), I, J)) {
+        const float *x = X + p * kTile;
+        for (int k = 0; k < nfeat; ++k)
+            if (!(x[k] >= lo[k] && x[k] <= hi[k])) out = 1;   // NaN counts as outside
+    }
+    mask[p] = out;
 }
 
 // Feature row of the column at p (rho-interior): 32 levels of log-scaled shear^2 and of
@@ -475,6 +614,44 @@ int sf_closure_apply(sf_ctx *c, const float *Y, const uint8_t *fallback, void *A
     }
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? SF_OK : mcuda(e, "sf_closure_apply");
+}
+
+int sf_mlp_infer(const sf_mlp_params *w, int n, const float *X, float *Y, int *err, sf_stream s) {
+    if (!w || !X || !Y || !err || n < 0) return mfail(SF_EINVAL, "bad argument");
+    if (n == 0) return SF_OK;
+    sf::mlp::InferW iw;
+    for (int l = 0; l < SF_MLP_LAYERS; ++l) {
+        if (!w->W[l]) return mfail(SF_EINVAL, "null weight matrix");
+        iw.W[l] = static_cast<const __nv_bfloat16 *>(w->W[l]);
+        iw.b[l] = w->b[l];
+    }
+    static bool attr_set[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return mcuda(e, "sf_mlp_infer");
+    if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+        e = cudaFuncSetAttribute(sf::mlp::k_infer, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sf::mlp::kInferSmem);
+        if (e != cudaSuccess) return mcuda(e, "cudaFuncSetAttribute");
+        attr_set[dev] = true;
+    }
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const long tiles = ((long)n + kTile - 1) / kTile;
+    const unsigned grid = (unsigned)(tiles < sms ? tiles : sms);
+    sf::mlp::k_infer<<<grid, sf::mlp::kInferThreads, sf::mlp::kInferSmem, S(s)>>>(iw, n, X, Y, err);
+    e = cudaGetLastError();
+    return e == cudaSuccess ? SF_OK : mcuda(e, "sf_mlp_infer");
+}
+
+int sf_closure_range_mask(sf_ctx *c, const float *X, int nfeat, const float *lo, const float *hi,
+                          uint8_t *mask, sf_stream s) {
+    if (!c || !X || !lo || !hi || !mask || nfeat < 0 || nfeat > kTile)
+        return mfail(SF_EINVAL, "bad argument");
+    sf::mlp::k_range_mask<<<nblk(c->s2, 256), 256, 0, S(s)>>>(c->s2, c->I, c->J, nfeat, X, lo, hi,
+                                                               mask);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? SF_OK : mcuda(e, "sf_closure_range_mask");
 }
 
 // ---- allocation-free backward pass ----------------------------------------------------------
