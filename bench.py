@@ -5,7 +5,10 @@
 
 Workload (default): basin4 = Lm=2048, Mm=1024, N=50 (104,857,600 interior cells), dx=1 km,
 tanh shelf + two seamounts, dt=120 s, ndtfast=40 (nfast+1 barotropic substeps per step),
-closed walls, the reference's step semantics (main3d.py:118-324), starting from rest.
+closed walls, the reference's step semantics (main3d.py:118-324), starting from rest, plus
+vertical mixing every step: the learned closure (FP32 form; plain GLS on its fallback
+columns) under wind tau_x = 0.15 cos(pi y/Ly) and T = 4 + 20 exp(z/500).  plain_fp64 is the
+same workload in FP64 (bit-identical to the reference kernels) with plain GLS.
 One "step" is one baroclinic step including its barotropic loop.  Inputs are larger than
 L2 (each 3D field is ~0.43 GB in FP32), so no L2 flush is needed between steps.
 
@@ -195,6 +198,8 @@ def plain_fp64(args):
     cfg = configs.CONFIGS[args.config]()
     g = cfg["grid"]
     m = Model(g, cfg["boundary"], cfg["dt"], cfg["ndtfast"], precision="fp64")
+    mixing = "none" if args.closure == "none" else "gls"
+    install_mixing(m, mixing, args.config)
     steps = max(1, min(args.steps, 3))
     ms = time_steps(m, steps, 3)
     cells = (g.L - 1) * (g.M - 1) * g.N
@@ -202,7 +207,9 @@ def plain_fp64(args):
     torch.cuda.empty_cache()
     return {"value": cells * steps / (ms * 1e-3), "unit": "cell-steps/s",
             "ms_per_step": ms / steps, "steps": steps, "warmup": 3, "dtype": "f64",
-            "semantics": "bit-identical to the reference kernels"}
+            "semantics": "bit-identical to the reference kernels",
+            "vertical_mixing": "plain GLS k-epsilon every step, FP64" if mixing == "gls"
+                               else "AKv constant (the reference's step)"}
 
 
 def error_vs_fp64():
@@ -238,6 +245,59 @@ def error_vs_fp64():
     return out
 
 
+WEIGHTS_FOR = {"basin4q": "basin4"}   # basins sharing a recipe (and N) share the closure
+
+
+def closure_weights(config):
+    name = WEIGHTS_FOR.get(config, config)
+    path = os.path.join(ROOT, "sailfish_b200", "weights", "closure_%s.npz" % name)
+    return path if os.path.exists(path) else None
+
+
+def install_mixing(m, mode, config):
+    """Vertical mixing for the step: 'mlp' (the learned closure with plain GLS on fallback
+    columns), 'gls' (plain GLS) or 'none' (AKv constant, the reference's step)."""
+    from sailfish_b200 import closure
+    if mode == "none":
+        return None
+    net = None
+    if mode == "mlp":
+        path = closure_weights(config)
+        if path is None:
+            raise SystemExit("no trained closure weights for %s (sailfish_b200/weights/); "
+                             "train them with python -m sailfish_b200.train_closure" % config)
+        net = closure.Network.load(path)
+    return closure.mixing_for(m, mode, net)
+
+
+def closure_error(m, steps=40):
+    """Learned closure against plain GLS at the bench state: GLS spun up for `steps`
+    iterations on the same columns, then the network's Akv/Akt (in-range columns) against
+    GLS's, log10 RMS over the interior columns and levels 1..N-1."""
+    import torch
+    from sailfish_b200 import closure
+    c = m.mixing
+    g = m.grid
+    ref = closure.Closure(m, "gls")
+    closure.basin_forcing(m, ref.cols)
+    for _ in range(steps):
+        ref()
+    akv_g, akt_g = m.AKv.clone(), ref.cols.Akt.clone()
+    c()
+    torch.cuda.synchronize()
+    N, s2 = g.N, g.s2
+    cols = closure.interior_columns(g, m.u.device)
+    inr = cols[c.mask[cols] == 0]
+    lg = lambda a: torch.log10(a.reshape(N + 1, s2)[1:N][:, inr].double().clamp(1e-6, 1e-1))
+    ev = (lg(m.AKv) - lg(akv_g)).pow(2).mean().sqrt()
+    et = (lg(c.cols.Akt) - lg(akt_g)).pow(2).mean().sqrt()
+    cv = (lg(akv_g) + 3.0).pow(2).mean().sqrt()
+    return {"akv_log10_rms_vs_gls": float(ev), "akt_log10_rms_vs_gls": float(et),
+            "constant_akv_log10_rms_vs_gls": float(cv),
+            "fallback_columns": int(c.mask.sum()), "columns": int(cols.numel()),
+            "gls_spinup_iterations": steps}
+
+
 def run_ours(args, rank, world):
     import torch
     from sailfish_b200 import configs
@@ -247,6 +307,8 @@ def run_ours(args, rank, world):
     cfg = configs.CONFIGS[args.config]()
     grid = cfg["grid"]
     m = Model(grid, cfg["boundary"], cfg["dt"], cfg["ndtfast"], precision=args.precision)
+    mixing = args.closure or ("mlp" if args.precision == "fp32" else "gls")
+    install_mixing(m, mixing, args.config)
     esize = 4 if args.precision == "fp32" else 8
     cells = (grid.L - 1) * (grid.M - 1) * grid.N
     stream = torch.cuda.current_stream()
@@ -306,7 +368,7 @@ def run_ours(args, rank, world):
     # per baroclinic step: maxflux_omega, rhs3d, set_depth, step3d_uv, and per barotropic
     # substep 2 zeta_rhs + 1 momentum + 1 corrector point + 3 boundary programs, plus the
     # closing momentum RHS; one omega at the end of the timed call
-    per_step = 4 + 7 * (m.nfast + 1) + 1
+    per_step = 4 + 7 * (m.nfast + 1) + 1 + {"none": 0, "gls": 1, "mlp": 2}[mixing]
     out = {
         "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
@@ -316,6 +378,12 @@ def run_ours(args, rank, world):
                    "cells": cells, "dt": m.dt, "ndtfast": m.ndtfast,
                    "barotropic_substeps": m.nfast + 1, "semantics": "reference main3d",
                    "initial_state": "rest, closed walls",
+                   "vertical_mixing": {"none": "AKv constant (the reference's step)",
+                                       "gls": "plain GLS k-epsilon every step",
+                                       "mlp": "learned closure, plain GLS on fallback columns"
+                                       }[mixing],
+                   "forcing": "closure: wind tau_x = 0.15 cos(pi y/Ly) N/m2, T = 4 + 20 exp(z/500)"
+                              if mixing != "none" else None,
                    "l2": "inputs larger than L2 (each 3D field %.2f GB)" % (m.u.numel() * esize / 1e9),
                    "parallelism": "replicas" if world > 1 else "single"},
         "phases_ms": per_phase,
@@ -330,6 +398,8 @@ def run_ours(args, rank, world):
         "gpu_launches": args.steps * per_step + 1,
         "clocks": clk.summary(),
     }
+    if mixing == "mlp" and not args.no_error:
+        out["closure_error"] = closure_error(m)
     return out
 
 
@@ -344,6 +414,8 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=40)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 timing")
+    ap.add_argument("--closure", choices=["mlp", "gls", "none"], default=None,
+                    help="vertical mixing in the step (default: mlp for fp32, gls for fp64)")
     ap.add_argument("--no-error", action="store_true", help="skip the FP32-vs-FP64 error case")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -190,6 +190,19 @@ int sf_gls_corrector(sf_ctx *ctx, const sf_gls_params *params, double dt, const 
                      const void *v, const void *z_r, const void *Hz, const void *bvf,
                      const void *sustr, const void *svstr, void *tke, void *gls, void *Akv,
                      void *Akt, void *Akk, void *Akp, void *Lscale, sf_stream stream);
+/* GLS predictor, nonlinear/gls_predictor_step.py:18-216 (ROMS pseudo-code in the reference):
+ * the auxiliary advective half step of tke and gls at W levels 1..N-1 on the rho-interior
+ * points — fourth-order centred horizontal advection (:62-127), the LF step interpolated
+ * back half a step with AM3 weights (Gamma = 1/6; first_step: forward half step, :133-157)
+ * and fourth-order vertical advection (:162-208) — into tke_aux/gls_aux (time level 3) with
+ * the half-step box height Hz_half; tke_nnew/gls_nnew = Hz_w * tke/gls(nstp) (:153-154).  A
+ * zero-gradient lateral condition is applied to the auxiliary level (tkebc_tile is not in the
+ * reference; edges take the adjacent interior value, corners the diagonal one).  Huon, Hvom:
+ * U/V fluxes at rho levels (N used); W, tke*, gls*, Hz_half: N+1 W levels; Hz: N levels. */
+int sf_gls_predictor(sf_ctx *ctx, double dt, int first_step, const void *Huon, const void *Hvom,
+                     const void *W, const void *Hz, const void *tke_nstp, const void *tke_indx,
+                     void *tke_aux, void *tke_nnew, const void *gls_nstp, const void *gls_indx,
+                     void *gls_aux, void *gls_nnew, void *Hz_half, sf_stream stream);
 /* sf_gls_corrector on the rho-interior columns p with columns[p] != 0 only (the closure's
  * fallback columns); the other columns' fields are left as they are.  No counterpart in the
  * reference. */
@@ -198,6 +211,15 @@ int sf_gls_corrector_cols(sf_ctx *ctx, const sf_gls_params *params, double dt, c
                           const void *sustr, const void *svstr, void *tke, void *gls, void *Akv,
                           void *Akt, void *Akk, void *Akp, void *Lscale, const uint8_t *columns,
                           sf_stream stream);
+/* sf_gls_corrector on the columns list[0 .. *count) (flat indices; *count read on the device,
+ * so a kernel earlier on the stream may produce both), e.g. the closure's fallback columns
+ * compacted by sf_closure_step: the cost follows the number of columns, not where they are.
+ * No counterpart in the reference. */
+int sf_gls_corrector_list(sf_ctx *ctx, const sf_gls_params *params, double dt, const void *u,
+                          const void *v, const void *z_r, const void *Hz, const void *bvf,
+                          const void *sustr, const void *svstr, void *tke, void *gls, void *Akv,
+                          void *Akt, void *Akk, void *Akp, void *Lscale, const int *list,
+                          const int *count, sf_stream stream);
 /* Buoyancy frequency squared at all N+1 W levels of a linear equation of state in temperature
  * (alpha, 1/degC) with the analytic profile T(z) = T0 + dT exp(z/zscale):
  * bvf = g alpha dT/zscale exp(z_w/zscale).  The stratification of the analytic basins, whose
@@ -258,8 +280,9 @@ int sf_mlp_mse(int n, int nvalid, const float *Y, const float *T, float *dY, flo
 /* Adam step on n FP32 master weights (bias-corrected, step >= 1); refreshes the BF16 copy. */
 int sf_mlp_adam(long n, float *w, const float *g, float *m, float *v, void *w_bf16, float lr,
                 float b1, float b2, int step, float eps, sf_stream stream);
-/* One feature row per water column (s2 x 128 FP32): log-scaled shear^2 and N^2 at the
- * interior W levels (32 each), surface stress, surface buoyancy flux, depth. */
+/* One feature row per water column (s2 x 128 FP32), nl = N-1 interior W levels (N <= 63):
+ * log-scaled shear^2 in [0, nl), log-scaled N^2 in [nl, 2nl), then log10 surface friction
+ * velocity squared, surface buoyancy flux and log10 depth; non-interior columns are 0. */
 int sf_closure_features(sf_ctx *ctx, const void *u, const void *v, const void *z_r,
                         const void *bvf, const void *sustr, const void *svstr, float *X,
                         sf_stream stream);
@@ -268,8 +291,21 @@ int sf_closure_features(sf_ctx *ctx, const void *u, const void *v, const void *z
  * network was not trained for, which plain GLS handles (sf_gls_corrector_cols); else 0. */
 int sf_closure_range_mask(sf_ctx *ctx, const float *X, int nfeat, const float *lo,
                           const float *hi, uint8_t *mask, sf_stream stream);
-/* Akv and Akt at the interior W levels from the network outputs (log10, clipped to
- * [1e-6, 1e-1] m2/s), except on columns flagged in `fallback` (may be NULL). */
+/* The closure for one step in one fused pass: for every rho-interior column, its feature row
+ * (as sf_closure_features), the range check against [lo, hi] over the first nfeat features
+ * (as sf_closure_range_mask, written to `fallback`), the network (as sf_mlp_infer) and, for
+ * the columns in range, Akv/Akt at levels 1..N-1 (as sf_closure_apply).  Columns flagged in
+ * `fallback` keep their Akv/Akt for plain GLS; if fallback_list/fallback_count are given (s2
+ * ints, one int), the flagged columns are also listed there, in no particular order, with
+ * *fallback_count zeroed first, for sf_gls_corrector_list.  No counterpart in the reference. */
+int sf_closure_step(sf_ctx *ctx, const sf_mlp_params *w, const void *u, const void *v,
+                    const void *z_r, const void *bvf, const void *sustr, const void *svstr,
+                    int nfeat, const float *lo, const float *hi, uint8_t *fallback,
+                    int *fallback_list, int *fallback_count, void *Akv, void *Akt, int *err,
+                    sf_stream stream);
+/* Akv and Akt at the interior W levels 1..N-1 from the network outputs [0, nl) and [nl, 2nl)
+ * (log10, clipped to [1e-6, 1e-1] m2/s), except on columns flagged in `fallback` (may be
+ * NULL). */
 int sf_closure_apply(sf_ctx *ctx, const float *Y, const uint8_t *fallback, void *Akv, void *Akt,
                      sf_stream stream);
 

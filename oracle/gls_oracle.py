@@ -207,3 +207,104 @@ def gls_corrector(P, dt, I, J, N, u, v, z_r, Hz, bvf, sustr, svstr, tke, gls, Ak
     for a, b in zip(out, (tk, gl, Av, At, Ak, Ap, Ls)):
         a[:, col] = b
     return tuple(out)
+
+
+# ---------------------------------------------------------------------------------------------
+# GLS predictor: the auxiliary advective half step of tke and gls
+# ---------------------------------------------------------------------------------------------
+GAMMA = 1.0 / 6.0   # AM3 weight of the half-step interpolation (ROMS mod_scalars Gamma)
+
+
+def _edge_grad(q, axis):
+    """grad(i) = q(i) - q(i-1) on i = 0..n (n+1 values, with one ghost on either side): the
+    first/last differences repeated at the domain edges (gls_predictor_step.py:68-80,97-108)."""
+    d = np.diff(q, axis=axis)                        # grad at i = 1..n-1 (in q's index)
+    first = np.take(d, [0], axis=axis)
+    last = np.take(d, [-1], axis=axis)
+    return np.concatenate([first, d, last], axis=axis)   # grad(0) := grad(1), grad(n) := grad(n-1)
+
+
+def gls_prestep(dt, first, I, J, N, pm, pn, Huon, Hvom, W, Hz, tke_nstp, tke_indx, gls_nstp,
+                gls_indx, gamma=GAMMA):
+    """nonlinear/gls_predictor_step.py:18-216 (fourth-order centred horizontal advection,
+    AM3-interpolated half step with Hz_half, fourth-order vertical advection) on the
+    rho-interior points, W levels 1..N-1, followed by a zero-gradient lateral condition on the
+    auxiliary level (edges from the adjacent interior point, corners from the diagonal one).
+
+    Arrays: Huon, Hvom (>= N rho levels, U/V points), W (N+1), Hz (N), tke/gls (N+1), all
+    flat (levels, J*I); pm, pn flat (J*I).  Returns (tke_aux, gls_aux, tke_nnew, gls_nnew,
+    Hz_half) as (N+1, J*I) arrays (levels 0 and N and the points not written are 0)."""
+    sh = (J, I)
+    pm2, pn2 = pm.reshape(sh), pn.reshape(sh)
+    if first:
+        c1, c2, c3 = 1.0, 0.0, 0.5 * dt
+        tke_indx, gls_indx = tke_nstp, gls_nstp
+    else:
+        c1, c2, c3 = 0.5 + gamma, 0.5 - gamma, (1.0 - gamma) * dt
+    out_t = np.zeros((N + 1, J * I))
+    out_g = np.zeros((N + 1, J * I))
+    new_t = np.zeros((N + 1, J * I))
+    new_g = np.zeros((N + 1, J * I))
+    Hh = np.zeros((N + 1, J * I))
+    Wl = W.reshape(N + 1, J, I)
+    T, G = tke_nstp.reshape(N + 1, J, I), gls_nstp.reshape(N + 1, J, I)
+    Ti, Gi = tke_indx.reshape(N + 1, J, I), gls_indx.reshape(N + 1, J, I)
+    # vertical fluxes at rho levels 1..N (Fortran numbering), CF(k) = (W(k) + W(k-1)) / 2
+    CF = np.zeros((N + 2, J, I))
+    FCt = np.zeros((N + 2, J, I))
+    FCg = np.zeros((N + 2, J, I))
+    for k in range(1, N + 1):
+        CF[k] = 0.5 * (Wl[k] + Wl[k - 1])
+    for q, F in ((T, FCt), (G, FCg)):
+        for k in range(2, N):
+            F[k] = CF[k] * (7.0 / 12.0 * (q[k - 1] + q[k]) - 1.0 / 12.0 * (q[k - 2] + q[k + 1]))
+        F[1] = CF[1] * (q[0] / 3.0 + 5.0 / 6.0 * q[1] - q[2] / 6.0)
+        F[N] = CF[N] * (q[N] / 3.0 + 5.0 / 6.0 * q[N - 1] - q[N - 2] / 6.0)
+    ii = slice(1, I - 1)
+    jj = slice(1, J - 1)
+    for k in range(1, N):
+        HU = Huon.reshape(-1, J, I)[k - 1]
+        HU2 = Huon.reshape(-1, J, I)[k]
+        HV = Hvom.reshape(-1, J, I)[k - 1]
+        HV2 = Hvom.reshape(-1, J, I)[k]
+        XF = 0.5 * (HU + HU2)                 # at U points i (between rho i-1 and i)
+        EF = 0.5 * (HV + HV2)                 # at V points j
+        res = []
+        for q, qi, F in ((T[k], Ti[k], FCt), (G[k], Gi[k], FCg)):
+            gx = _edge_grad(q, 1)             # (J, I+1): index i -> grad(i), i = 0..I
+            gy = _edge_grad(q, 0)             # (J+1, I)
+            # FX(i), i = 1..I-1: XF(i) (q(i-1)+q(i) - (grad(i+1)-grad(i-1))/6) / 2
+            FX = np.zeros(sh)
+            FX[:, 1:] = XF[:, 1:] * 0.5 * (q[:, :-1] + q[:, 1:] - (gx[:, 2:] - gx[:, :-2]) / 6.0)
+            FE = np.zeros(sh)
+            FE[1:, :] = EF[1:, :] * 0.5 * (q[:-1, :] + q[1:, :] - (gy[2:, :] - gy[:-2, :]) / 6.0)
+            res.append((FX, FE, qi))
+        cff = 0.5 * (Hz.reshape(N, J, I)[k - 1] + Hz.reshape(N, J, I)[k])
+        cff4 = c3 * pm2 * pn2
+        divX = np.zeros(sh)
+        divE = np.zeros(sh)
+        divX[jj, ii] = XF[jj, 2:] - XF[jj, 1:-1]
+        divE[jj, ii] = EF[2:, ii] - EF[1:-1, ii]
+        hh = cff - cff4 * (divX + divE) - cff4 * (CF[k + 1] - CF[k])
+        Hh[k].reshape(sh)[jj, ii] = hh[jj, ii]
+        for (FX, FE, qi), q, out, new, F in ((res[0], T[k], out_t, new_t, FCt),
+                                              (res[1], G[k], out_g, new_g, FCg)):
+            dX = np.zeros(sh)
+            dE = np.zeros(sh)
+            dX[jj, ii] = FX[jj, 2:] - FX[jj, 1:-1]
+            dE[jj, ii] = FE[2:, ii] - FE[1:-1, ii]
+            val = cff * (c1 * q + c2 * qi) - cff4 * (dX + dE)
+            val = (val - cff4 * (F[k + 1] - F[k])) / hh
+            out[k].reshape(sh)[jj, ii] = val[jj, ii]
+            new[k].reshape(sh)[jj, ii] = (cff * q)[jj, ii]
+    for out in (out_t, out_g):               # zero-gradient edges of the auxiliary level
+        a = out.reshape(N + 1, J, I)
+        a[1:N, jj, 0] = a[1:N, jj, 1]
+        a[1:N, jj, I - 1] = a[1:N, jj, I - 2]
+        a[1:N, 0, ii] = a[1:N, 1, ii]
+        a[1:N, J - 1, ii] = a[1:N, J - 2, ii]
+        a[1:N, 0, 0] = a[1:N, 1, 1]
+        a[1:N, 0, I - 1] = a[1:N, 1, I - 2]
+        a[1:N, J - 1, 0] = a[1:N, J - 2, 1]
+        a[1:N, J - 1, I - 1] = a[1:N, J - 2, I - 2]
+    return out_t, out_g, new_t, new_g, Hh

@@ -78,7 +78,9 @@ SIGNATURES = {
     "sf_step3d_uv_bc": [_vp] * 14 + [_i, _i, _d, _d, _d, _vp],
     "sf_gls_corrector": [_vp, ctypes.POINTER(GlsParams), _d] + [_vp] * 14 + [_vp],
     "sf_gls_corrector_cols": [_vp, ctypes.POINTER(GlsParams), _d] + [_vp] * 15 + [_vp],
+    "sf_gls_corrector_list": [_vp, ctypes.POINTER(GlsParams), _d] + [_vp] * 16 + [_vp],
     "sf_analytic_bvf": [_vp, _vp, _d, _d, _d, _d, _vp, _vp],
+    "sf_gls_predictor": [_vp, _d, _i] + [_vp] * 13 + [_vp],
     "sf_mlp_last_error": [],
     "sf_mlp_gemm": [_i, _i, _vp, _i, ctypes.c_long, ctypes.c_long, _vp, _i, ctypes.c_long,
                     ctypes.c_long, _vp, _i, _vp, ctypes.c_long, _vp, ctypes.c_long, _vp, _vp],
@@ -94,6 +96,7 @@ SIGNATURES = {
     "sf_closure_features": [_vp] * 9,
     "sf_closure_apply": [_vp] * 6,
     "sf_closure_range_mask": [_vp, _vp, _i, _vp, _vp, _vp, _vp],
+    "sf_closure_step": [_vp, ctypes.POINTER(MlpParams)] + [_vp] * 6 + [_i] + [_vp] * 9,
 }
 
 
@@ -112,7 +115,14 @@ lib = _load()
 
 
 class SailfishError(RuntimeError):
-    def __init__(self, code, where):
+    """A failed library call (status code and the library's error text), or a caller error
+    found on the host (message only, status SF_EINVAL)."""
+
+    def __init__(self, code, where=None):
+        if where is None:
+            super().__init__(str(code))
+            self.code = SF_EINVAL
+            return
         msg = lib.sf_last_error().decode(errors="replace")
         super().__init__("%s failed (status %d): %s" % (where, code, msg))
         self.code = code

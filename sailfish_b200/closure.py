@@ -7,10 +7,10 @@ modules/mod_ocean.py:91 (its GLS closure, nonlinear/gls_corrector_step.py, is un
 ROMS Fortran).  Plain GLS (sf_gls_corrector) is this package's closure; the network stands in
 for its Akv/Akt at a fraction of the cost, and GLS remains the judge of its error.
 
-Rows: one water column each, 128 FP32 features from sf_closure_features (log10 shear^2 and
-signed log N^2 at the interior W levels 1..N-1, log10 surface friction velocity squared,
-surface buoyancy flux, log10 depth).  Targets: log10 Akv at levels 1..N-1 in outputs 0..,
-log10 Akt in outputs 32.. (N <= 33).
+Rows: one water column each, 128 FP32 features from sf_closure_features; with nl = N-1
+interior W levels: log10 shear^2 in [0, nl), signed log N^2 in [nl, 2nl), then log10 surface
+friction velocity squared, surface buoyancy flux and log10 depth.  Targets: log10 Akv at
+levels 1..N-1 in outputs [0, nl), log10 Akt in [nl, 2nl).  A network serves one N (N <= 63).
 """
 import ctypes
 import math
@@ -20,11 +20,21 @@ import torch
 
 from . import configs
 from ._lib import GlsParams, MlpParams, check, lib
-from .model import Context, Model, stream_handle
+from .model import Model, stream_handle
 
 LAYERS, WIDTH = 5, 128
-NFEAT = 67           # features used of the 128 (64 level features + 3 scalars)
-NOUT = 64            # outputs trained (Akv levels 0..31, Akt levels 32..63)
+
+
+def nfeat(N):
+    """Features used of the 128 for N levels: two per interior W level, three scalars."""
+    return 2 * (N - 1) + 3
+
+
+def nout(N):
+    """Outputs trained for N levels: Akv and Akt at each interior W level."""
+    return 2 * (N - 1)
+
+
 RHO0 = 1025.0        # modules/mod_constants.py:25
 G = 10.0             # modules/mod_constants.py:26
 ALPHA = 1.7e-4       # linear EOS thermal expansion, utility/test.in:453
@@ -86,6 +96,15 @@ class Columns:
             _p(self.Akt), _p(self.Akk), _p(self.Akp), _p(self.Lscale), _p(columns),
             stream_handle()), "sf_gls_corrector_cols")
 
+    def gls_step_list(self, lst, count):
+        """Plain GLS on the columns lst[0 .. count) (device int32 list and count)."""
+        m = self.m
+        check(lib.sf_gls_corrector_list(
+            m.ctx.ptr, ctypes.byref(self.P), m.dt, _p(m.u), _p(m.v), _p(m.z_r), _p(m.Hz),
+            _p(self.bvf), _p(self.sustr), _p(self.svstr), _p(self.tke), _p(self.gls), _p(m.AKv),
+            _p(self.Akt), _p(self.Akk), _p(self.Akp), _p(self.Lscale), _p(lst), _p(count),
+            stream_handle()), "sf_gls_corrector_list")
+
     def features(self, X):
         m = self.m
         check(lib.sf_closure_features(m.ctx.ptr, _p(m.u), _p(m.v), _p(m.z_r), _p(self.bvf),
@@ -99,16 +118,29 @@ def interior_columns(grid, device):
     return idx[(i != 0) & (i != grid.I - 1) & (j != 0) & (j != grid.J - 1)]
 
 
-def wind_driven_state(model, cols, tau, angle, zscale, rng):
+def wind_driven_state(model, cols, tau, angle, zscale, rng, current=True, pattern=False):
     """A wind-driven, stratified column state on the model's grid: surface stress tau (N/m2)
-    at `angle`, a surface-intensified current decaying over an Ekman-like depth with a basin-
-    scale gyre pattern and seeded small-scale noise, and the stratification of zscale."""
+    at `angle` (times cos(pi y / Ly) if `pattern`, the basins' wind), a surface-intensified
+    current decaying over an Ekman-like depth with a basin-scale gyre pattern and seeded
+    small-scale noise (none if `current` is False: an ocean at rest under the wind), and the
+    stratification of zscale."""
     g = model.grid
     dev = model.u.device
     dt = model.tdtype
     ustar2 = tau / RHO0
-    cols.sustr.fill_(ustar2 * math.cos(angle))
-    cols.svstr.fill_(ustar2 * math.sin(angle))
+    if pattern:
+        y = (torch.arange(g.J, device=dev, dtype=torch.float64) - 0.5) / max(g.J - 2, 1)
+        shape = torch.cos(math.pi * y)[:, None].expand(g.J, g.I)
+        cols.sustr.copy_((ustar2 * math.cos(angle) * shape).to(cols.sustr.dtype))
+        cols.svstr.copy_((ustar2 * math.sin(angle) * shape).to(cols.svstr.dtype))
+    else:
+        cols.sustr.fill_(ustar2 * math.cos(angle))
+        cols.svstr.fill_(ustar2 * math.sin(angle))
+    if not current:
+        model.u.zero_()
+        model.v.zero_()
+        cols.stratify(zscale)
+        return
     ustar = math.sqrt(ustar2)
     d = max(5.0, 0.4 * ustar / 1e-4)                      # Ekman depth u*/f scale
     U0 = 40.0 * ustar2 / max(ustar, 1e-4) + 0.02          # surface drift ~ u*-proportional
@@ -130,16 +162,37 @@ def wind_driven_state(model, cols, tau, angle, zscale, rng):
     cols.stratify(zscale)
 
 
+def basin_forcing(model, cols, tau0=0.15, zscale=500.0):
+    """The analytic basins' forcing for the closure: zonal wind stress tau0 cos(pi y / Ly)
+    (N/m2, kinematic after division by rho0) and the stratification T = 4 + 20 exp(z/zscale)."""
+    g = model.grid
+    J = g.J
+    y = (torch.arange(J, device=model.u.device, dtype=torch.float64) - 0.5) / max(J - 2, 1)
+    tau = tau0 * torch.cos(math.pi * y) / RHO0
+    cols.sustr.copy_(tau[:, None].expand(J, g.I).to(cols.sustr.dtype))
+    cols.svstr.zero_()
+    cols.stratify(zscale)
+
+
+def mixing_for(model, mode, net=None, tau0=0.15, zscale=500.0):
+    """A Closure for `model` ('gls' or 'mlp') under basin_forcing, installed as model.mixing."""
+    c = Closure(model, mode, net)
+    basin_forcing(model, c.cols, tau0, zscale)
+    model.mixing = c
+    return c
+
+
 def generate(config="basin1", runs=4, spin=30, keep=4, every=5, seed=0, precision="fp32",
-             tau_range=(0.0, 0.3), zscale_range=(200.0, 1000.0)):
+             tau_range=(0.0, 0.3), zscale_range=(200.0, 1000.0), rest_runs=0, pattern=False):
     """Training snapshots from plain GLS runs on `config`'s grid: each run draws a wind stress
     and a stratification scale, spins GLS up for `spin` steps at fixed forcing and then keeps
-    `keep` snapshots `every` steps apart.  Returns (X, T) on the device: feature rows and
-    target rows (log10 Akv / Akt) of the rho-interior columns."""
+    `keep` snapshots `every` steps apart.  The last `rest_runs` of the runs have no current
+    (an ocean at rest under the wind); with `pattern` the wind varies as cos(pi y / Ly).  Returns (X, T) on the device: feature rows and target
+    rows (log10 Akv / Akt) of the rho-interior columns."""
     cfg = configs.CONFIGS[config]() if isinstance(config, str) else config
     g = cfg["grid"]
-    if g.N - 1 > 32:
-        raise ValueError("the closure's rows hold at most 32 interior W levels")
+    if nfeat(g.N) > WIDTH:
+        raise ValueError("the closure's rows hold at most 62 interior W levels")
     model = Model(g, cfg["boundary"], cfg["dt"], cfg["ndtfast"], precision=precision)
     model.start()
     dev = model.u.device
@@ -152,7 +205,8 @@ def generate(config="basin1", runs=4, spin=30, keep=4, every=5, seed=0, precisio
         tau = float(rng.uniform(*tau_range))
         zscale = float(rng.uniform(*zscale_range))
         angle = float(rng.uniform(0.0, 2.0 * math.pi))
-        wind_driven_state(model, cols, tau, angle, zscale, rng)
+        wind_driven_state(model, cols, tau, angle, zscale, rng, current=r < runs - rest_runs,
+                          pattern=pattern)
         model.AKv.fill_(cols.P.Akv_bak)
         for it in range(spin + keep * every):
             cols.gls_step()
@@ -165,13 +219,15 @@ def generate(config="basin1", runs=4, spin=30, keep=4, every=5, seed=0, precisio
 
 
 def targets(Akv, Akt, N):
-    """Target rows (s2 x 128): log10 Akv at W levels 1..N-1 in 0.., log10 Akt in 32.."""
+    """Target rows (s2 x 128): log10 Akv at W levels 1..N-1 in [0, N-1), log10 Akt in
+    [N-1, 2N-2)."""
     s2 = Akv[0].numel()
+    nl = N - 1
     T = torch.zeros((s2, WIDTH), device=Akv.device)
-    lv = torch.log10(Akv[1:N].reshape(N - 1, s2).float().clamp(1e-6, 1e-1))
-    lt = torch.log10(Akt[1:N].reshape(N - 1, s2).float().clamp(1e-6, 1e-1))
-    T[:, :N - 1] = lv.T
-    T[:, 32:32 + N - 1] = lt.T
+    lv = torch.log10(Akv[1:N].reshape(nl, s2).float().clamp(1e-6, 1e-1))
+    lt = torch.log10(Akt[1:N].reshape(nl, s2).float().clamp(1e-6, 1e-1))
+    T[:, :nl] = lv.T
+    T[:, nl:2 * nl] = lt.T
     return T
 
 
@@ -183,7 +239,10 @@ class Network:
     tensor cores.  Inputs are normalised with the training set's per-feature mean and spread,
     which `inference_params()` folds into the first layer."""
 
-    def __init__(self, seed=0, device="cuda"):
+    def __init__(self, N, seed=0, device="cuda"):
+        if nfeat(N) > WIDTH:
+            raise ValueError("the closure's rows hold at most 62 interior W levels")
+        self.N = int(N)
         gen = torch.Generator().manual_seed(seed)
         self.W = [(torch.randn(WIDTH, WIDTH, generator=gen) * math.sqrt(2.0 / WIDTH)).to(device)
                   for _ in range(LAYERS)]
@@ -224,14 +283,14 @@ class Network:
         sd = X.std(0)
         self.mu = torch.where(sd > 1e-6, mu, torch.zeros_like(mu))
         self.isd = torch.where(sd > 1e-6, 1.0 / sd, torch.zeros_like(sd))
-        self.mu[NFEAT:] = 0.0
-        self.isd[NFEAT:] = 0.0
+        self.mu[nfeat(self.N):] = 0.0
+        self.isd[nfeat(self.N):] = 0.0
         lo, hi = X.min(0).values, X.max(0).values
         pad = 0.05 * (hi - lo) + 1e-3
         self.lo, self.hi = (lo - pad).contiguous(), (hi + pad).contiguous()
 
     def train(self, X, T, steps=2000, batch=2048, lr=2e-3, seed=0, log_every=0):
-        """Adam on the MSE of the NOUT trained outputs, minibatches drawn with a seeded
+        """Adam on the MSE of the nout(N) trained outputs, minibatches drawn with a seeded
         permutation; every product on the tensor cores through sf_mlp_forward/backward."""
         dev = X.device
         n = X.shape[0]
@@ -264,7 +323,8 @@ class Network:
             loss.zero_()
             check(lib.sf_mlp_forward(ctypes.byref(P), batch, _p(xb), _p(Y), _p(acts), _p(pre),
                                      _p(self.err), st), "sf_mlp_forward")
-            check(lib.sf_mlp_mse(batch, NOUT, _p(Y), _p(tb), _p(dY), _p(loss), st), "sf_mlp_mse")
+            check(lib.sf_mlp_mse(batch, nout(self.N), _p(Y), _p(tb), _p(dY), _p(loss), st),
+                  "sf_mlp_mse")
             check(lib.sf_mlp_backward(ctypes.byref(P), batch, _p(xb), _p(acts), _p(pre), _p(dY),
                                       pdW, pdb, _p(work), _p(self.err), st), "sf_mlp_backward")
             self.step_count += 1
@@ -283,6 +343,24 @@ class Network:
             raise RuntimeError("a tensor-core wait gave up during training")
         return history
 
+    def save(self, path, **meta):
+        """Master weights, normalisation and training range (NumPy .npz) plus `meta`."""
+        np.savez(path, N=self.N, W=np.stack([w.cpu().numpy() for w in self.W]),
+                 b=np.stack([b.cpu().numpy() for b in self.b]), mu=self.mu.cpu().numpy(),
+                 isd=self.isd.cpu().numpy(), lo=self.lo.cpu().numpy(), hi=self.hi.cpu().numpy(),
+                 **{k: np.asarray(v) for k, v in meta.items()})
+
+    @classmethod
+    def load(cls, path, device="cuda"):
+        d = np.load(path)
+        net = cls(int(d["N"]), device=device)
+        t = lambda a: torch.tensor(np.asarray(a, np.float32), device=device)
+        net.W = [t(w) for w in d["W"]]
+        net.b = [t(b) for b in d["b"]]
+        net.Wb = [w.to(torch.bfloat16) for w in net.W]
+        net.mu, net.isd, net.lo, net.hi = t(d["mu"]), t(d["isd"]), t(d["lo"]), t(d["hi"])
+        return net
+
     def infer(self, X):
         """Outputs for raw feature rows X (n x 128) through the fused inference kernel."""
         P, keep = self.inference_params()
@@ -294,8 +372,9 @@ class Network:
 
 def log_rms(Y, T, N):
     """RMS log10 error of Akv and Akt over the trained outputs (levels 1..N-1)."""
-    ev = (Y[:, :N - 1] - T[:, :N - 1]).double()
-    et = (Y[:, 32:32 + N - 1] - T[:, 32:32 + N - 1]).double()
+    nl = N - 1
+    ev = (Y[:, :nl] - T[:, :nl]).double()
+    et = (Y[:, nl:2 * nl] - T[:, nl:2 * nl]).double()
     return float(ev.pow(2).mean().sqrt()), float(et.pow(2).mean().sqrt())
 
 
@@ -304,21 +383,28 @@ def log_rms(Y, T, N):
 # -------------------------------------------------------------------------------------------
 class Closure:
     """Per-step vertical mixing for a Model: 'gls' runs plain GLS on every column; 'mlp' runs
-    the network on every column and plain GLS on the columns outside its training range."""
+    the network on every column and plain GLS on the columns outside its training range
+    (fused: one sf_closure_step pass; otherwise features, range mask, sf_mlp_infer and
+    sf_closure_apply as separate launches)."""
 
-    def __init__(self, model, mode="mlp", net=None):
+    def __init__(self, model, mode="mlp", net=None, fused=True):
         if mode not in ("gls", "mlp"):
             raise ValueError("mode must be 'gls' or 'mlp'")
         if mode == "mlp" and net is None:
             raise ValueError("mode 'mlp' needs a trained Network")
-        self.m, self.mode, self.net = model, mode, net
+        if mode == "mlp" and net.N != model.grid.N:
+            raise ValueError("the network was trained for N=%d levels" % net.N)
+        self.m, self.mode, self.net, self.fused = model, mode, net, fused
         self.cols = Columns(model)
         g = model.grid
         dev = model.u.device
         if mode == "mlp":
-            self.X = torch.zeros((g.s2, WIDTH), device=dev)
-            self.Y = torch.zeros((g.s2, WIDTH), device=dev)
+            if not fused:   # the unfused composition: features, mask, inference, update
+                self.X = torch.zeros((g.s2, WIDTH), device=dev)
+                self.Y = torch.zeros((g.s2, WIDTH), device=dev)
             self.mask = torch.zeros(g.s2, dtype=torch.uint8, device=dev)
+            self.flist = torch.zeros(g.s2, dtype=torch.int32, device=dev)
+            self.fcount = torch.zeros(1, dtype=torch.int32, device=dev)
             self.P, self._keep = net.inference_params()
             self.lo = net.lo.contiguous()
             self.hi = net.hi.contiguous()
@@ -329,11 +415,21 @@ class Closure:
             c.gls_step()
             return
         st = stream_handle()
-        c.features(self.X)
-        check(lib.sf_closure_range_mask(m.ctx.ptr, _p(self.X), NFEAT, _p(self.lo), _p(self.hi),
-                                        _p(self.mask), st), "sf_closure_range_mask")
-        check(lib.sf_mlp_infer(ctypes.byref(self.P), m.grid.s2, _p(self.X), _p(self.Y),
-                               _p(self.net.err), st), "sf_mlp_infer")
-        check(lib.sf_closure_apply(m.ctx.ptr, _p(self.Y), _p(self.mask), _p(m.AKv), _p(c.Akt),
-                                   st), "sf_closure_apply")
+        if self.fused:
+            check(lib.sf_closure_step(m.ctx.ptr, ctypes.byref(self.P), _p(m.u), _p(m.v),
+                                      _p(m.z_r), _p(c.bvf), _p(c.sustr), _p(c.svstr),
+                                      nfeat(m.grid.N), _p(self.lo), _p(self.hi), _p(self.mask),
+                                      _p(self.flist), _p(self.fcount), _p(m.AKv), _p(c.Akt),
+                                      _p(self.net.err), st), "sf_closure_step")
+            c.gls_step_list(self.flist, self.fcount)   # plain GLS on the fallback columns
+            return
+        else:
+            c.features(self.X)
+            check(lib.sf_closure_range_mask(m.ctx.ptr, _p(self.X), nfeat(m.grid.N), _p(self.lo),
+                                            _p(self.hi), _p(self.mask), st),
+                  "sf_closure_range_mask")
+            check(lib.sf_mlp_infer(ctypes.byref(self.P), m.grid.s2, _p(self.X), _p(self.Y),
+                                   _p(self.net.err), st), "sf_mlp_infer")
+            check(lib.sf_closure_apply(m.ctx.ptr, _p(self.Y), _p(self.mask), _p(m.AKv),
+                                       _p(c.Akt), st), "sf_closure_apply")
         c.gls_step(self.mask)       # plain GLS on the fallback columns only

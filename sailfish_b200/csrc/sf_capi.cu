@@ -575,22 +575,75 @@ int sf_gls_corrector(sf_ctx *c, const sf_gls_params *P, double dt, const void *u
                                  Akk, Akp, Lscale, nullptr, s);
 }
 
-int sf_gls_corrector_cols(sf_ctx *c, const sf_gls_params *P, double dt, const void *u,
-                          const void *v, const void *z_r, const void *Hz, const void *bvf,
-                          const void *sustr, const void *svstr, void *tke, void *gls, void *Akv,
-                          void *Akt, void *Akk, void *Akp, void *Lscale, const uint8_t *columns,
-                          sf_stream s) {
+namespace {
+int gls_checks(const sf_gls_params *P) {
     if (!P) return fail(SF_EINVAL, "null GLS parameters");
     if (P->n == 0.0) return fail(SF_EINVAL, "GLS exponent n must be non-zero");
     if (P->p == 0.0 && P->m == 1.0 && P->n == 1.0)
         return fail(SF_EUNSUPPORTED, "Mellor-Yamada 2.5 (p=0, m=1, n=1) needs the wall function, "
                                      "which is not built");
+    return SF_OK;
+}
+}  // namespace
+
+int sf_gls_corrector_list(sf_ctx *c, const sf_gls_params *P, double dt, const void *u,
+                          const void *v, const void *z_r, const void *Hz, const void *bvf,
+                          const void *sustr, const void *svstr, void *tke, void *gls, void *Akv,
+                          void *Akt, void *Akk, void *Akp, void *Lscale, const int *list,
+                          const int *count, sf_stream s) {
+    if (!list || !count) return fail(SF_EINVAL, "null column list");
+    if (const int rc = gls_checks(P)) return rc;
+    return dispatch(c, "sf_gls_corrector_list", [&](auto *t) {
+        using R = std::remove_pointer_t<decltype(t)>;
+        return sf::Ops<R>::gls_corrector(c, *P, dt, (const R *)u, (const R *)v, (const R *)z_r,
+                                         (const R *)Hz, (const R *)bvf, (const R *)sustr,
+                                         (const R *)svstr, (R *)tke, (R *)gls, (R *)Akv, (R *)Akt,
+                                         (R *)Akk, (R *)Akp, (R *)Lscale, nullptr, list, count,
+                                         S(s));
+    });
+}
+
+int sf_gls_corrector_cols(sf_ctx *c, const sf_gls_params *P, double dt, const void *u,
+                          const void *v, const void *z_r, const void *Hz, const void *bvf,
+                          const void *sustr, const void *svstr, void *tke, void *gls, void *Akv,
+                          void *Akt, void *Akk, void *Akp, void *Lscale, const uint8_t *columns,
+                          sf_stream s) {
+    if (const int rc = gls_checks(P)) return rc;
     return dispatch(c, "sf_gls_corrector", [&](auto *t) {
         using R = std::remove_pointer_t<decltype(t)>;
         return sf::Ops<R>::gls_corrector(c, *P, dt, (const R *)u, (const R *)v, (const R *)z_r,
                                          (const R *)Hz, (const R *)bvf, (const R *)sustr,
                                          (const R *)svstr, (R *)tke, (R *)gls, (R *)Akv, (R *)Akt,
-                                         (R *)Akk, (R *)Akp, (R *)Lscale, columns, S(s));
+                                         (R *)Akk, (R *)Akp, (R *)Lscale, columns, nullptr,
+                                         nullptr, S(s));
+    });
+}
+
+int sf_gls_predictor(sf_ctx *c, double dt, int first_step, const void *Huon, const void *Hvom,
+                     const void *W, const void *Hz, const void *tke_nstp, const void *tke_indx,
+                     void *tke_aux, void *tke_nnew, const void *gls_nstp, const void *gls_indx,
+                     void *gls_aux, void *gls_nnew, void *Hz_half, sf_stream s) {
+    if (c && c->N < 3) return fail(SF_EUNSUPPORTED, "the GLS predictor needs N >= 3 levels");
+    constexpr double kGamma = 1.0 / 6.0;   // AM3 weight of the half-step interpolation
+    sf::GlsPre pc;
+    if (first_step) {
+        pc.c1 = 1.0;
+        pc.c2 = 0.0;
+        pc.c3 = 0.5 * dt;
+        tke_indx = tke_nstp;
+        gls_indx = gls_nstp;
+    } else {
+        pc.c1 = 0.5 + kGamma;
+        pc.c2 = 0.5 - kGamma;
+        pc.c3 = (1.0 - kGamma) * dt;
+    }
+    return dispatch(c, "sf_gls_predictor", [&](auto *t) {
+        using R = std::remove_pointer_t<decltype(t)>;
+        return sf::Ops<R>::gls_prestep(c, pc, (const R *)Huon, (const R *)Hvom,
+                                         (const R *)W, (const R *)Hz, (const R *)tke_nstp,
+                                         (const R *)tke_indx, (R *)tke_aux, (R *)tke_nnew,
+                                         (const R *)gls_nstp, (const R *)gls_indx, (R *)gls_aux,
+                                         (R *)gls_nnew, (R *)Hz_half, S(s));
     });
 }
 

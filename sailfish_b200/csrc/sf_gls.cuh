@@ -34,8 +34,13 @@ __global__ void __launch_bounds__(128) k_gls_corrector(
     Geo<R> g, sf_gls_params P, R dt, const R *__restrict__ u, const R *__restrict__ v,
     const R *__restrict__ z_r, const R *__restrict__ Hz, const R *__restrict__ bvf,
     const R *__restrict__ sustr, const R *__restrict__ svstr, R *tke, R *gls, R *Akv, R *Akt,
-    R *Akk, R *Akp, R *Lscale, const uint8_t *__restrict__ sel) {
-    const int pi = (int)tid_flat();
+    R *Akk, R *Akp, R *Lscale, const uint8_t *__restrict__ sel, const int *__restrict__ list,
+    const int *__restrict__ count) {
+    int pi = (int)tid_flat();
+    if (list) {                    // a compacted list of columns: thread t takes list[t]
+        if (pi >= *count) return;
+        pi = list[pi];
+    }
     if (pi >= g.s2) return;
     const int i = pi % g.I, j = pi / g.I;
     if (!rint_(i, j, g.I, g.J)) return;
@@ -180,6 +185,131 @@ __global__ void __launch_bounds__(128) k_gls_corrector(
     AT(gls, N, p) = gl[N];
     AT(gls, 0, p) = gl[0];
 #undef AT
+}
+
+
+// ---------------------------------------------------------------------------------------------
+// GLS predictor (nonlinear/gls_predictor_step.py:18-216, ROMS pseudo-code in the reference): the
+// auxiliary advective half step of tke and gls at W levels 1..N-1 on the rho-interior points.
+// Fourth-order centred horizontal fluxes FX/FE with the edge differences repeated at the domain
+// edges (:62-127); the LF step interpolated back half a step with the AM3 weights cff1..cff3
+// and the half-step box height Hz_half (:133-157); fourth-order vertical fluxes with the
+// one-sided third-order forms at the bottom and surface (:162-208).  Also tke/gls(nnew) =
+// Hz_w * tke/gls(nstp), the start of the corrector's update (:153-154).
+// ---------------------------------------------------------------------------------------------
+template <typename R>
+__device__ __forceinline__ R vflux_(const R *q, const R *W, long p, long s2, int m, int N) {
+    // FC at rho level m (1..N, Fortran numbering) of the W-level field q
+#define Q(k) (q[(long)(k) * s2 + p])
+    const R cf = R(0.5) * (W[(long)m * s2 + p] + W[(long)(m - 1) * s2 + p]);
+    if (m == 1) return cf * (Q(0) / R(3) + R(5.0 / 6.0) * Q(1) - Q(2) / R(6));
+    if (m == N) return cf * (Q(N) / R(3) + R(5.0 / 6.0) * Q(N - 1) - Q(N - 2) / R(6));
+    return cf * (R(7.0 / 12.0) * (Q(m - 1) + Q(m)) - R(1.0 / 12.0) * (Q(m - 2) + Q(m + 1)));
+#undef Q
+}
+
+// One tracer's horizontal flux divergence FX(i+1)-FX(i) + FE(j+1)-FE(j) at (i, j), level k.
+template <typename R>
+__device__ __forceinline__ R hdiv_(const R *q, const R *XF0, const R *XF1, const R *EF0,
+                                   const R *EF1, long p, int i, int j, int I, int J, long s2,
+                                   int k) {
+    const R *qk = q + (long)k * s2;
+    auto gx = [&](int m) -> R {   // grad(m) = q(m) - q(m-1), edges repeated
+        m = m < 1 ? 1 : (m > I - 1 ? I - 1 : m);
+        return qk[(long)j * I + m] - qk[(long)j * I + m - 1];
+    };
+    auto gy = [&](int m) -> R {
+        m = m < 1 ? 1 : (m > J - 1 ? J - 1 : m);
+        return qk[(long)m * I + i] - qk[(long)(m - 1) * I + i];
+    };
+    auto FX = [&](int a) -> R {   // at U point a of row j
+        const long u = (long)j * I + a;
+        const R xf = R(0.5) * (XF0[u] + XF1[u]);
+        return xf * R(0.5) * (qk[u - 1] + qk[u] - (gx(a + 1) - gx(a - 1)) / R(6));
+    };
+    auto FE = [&](int b) -> R {   // at V point b of column i
+        const long v = (long)b * I + i;
+        const R ef = R(0.5) * (EF0[v] + EF1[v]);
+        return ef * R(0.5) * (qk[v - I] + qk[v] - (gy(b + 1) - gy(b - 1)) / R(6));
+    };
+    (void)p;
+    return (FX(i + 1) - FX(i)) + (FE(j + 1) - FE(j));
+}
+
+template <typename R>
+__global__ void __launch_bounds__(128) k_gls_prestep(Geo<R> g, GlsPre c, const R *__restrict__ Huon,
+        const R *__restrict__ Hvom, const R *__restrict__ W, const R *__restrict__ Hz,
+        const R *__restrict__ tke0, const R *__restrict__ tkei, R *__restrict__ tke3,
+        R *__restrict__ tken, const R *__restrict__ gls0, const R *__restrict__ glsi,
+        R *__restrict__ gls3, R *__restrict__ glsn, R *__restrict__ Hz_half) {
+    const int pi = (int)tid_flat();
+    if (pi >= g.s2) return;
+    const int I = g.I, J = g.J, N = g.N;
+    const int i = pi % I, j = pi / I;
+    if (i < 1 || i > I - 2 || j < 1 || j > J - 2) return;
+    const long p = pi, s2 = g.s2;
+    const R cff4 = (R)c.c3 * (g.pm[p] * g.pn[p]);
+    R FCt = vflux_(tke0, W, p, s2, 1, N), FCg = vflux_(gls0, W, p, s2, 1, N);
+    R CFk = R(0.5) * (W[s2 + p] + W[p]);
+    for (int k = 1; k < N; ++k) {
+        const R *XF0 = Huon + (long)(k - 1) * s2, *XF1 = Huon + (long)k * s2;
+        const R *EF0 = Hvom + (long)(k - 1) * s2, *EF1 = Hvom + (long)k * s2;
+        const long o = (long)k * s2 + p;
+        const R cff = R(0.5) * (Hz[o - s2] + Hz[o]);
+        const long u = (long)j * I + i, v = u;
+        const R divUV = (R(0.5) * (XF0[u + 1] + XF1[u + 1]) - R(0.5) * (XF0[u] + XF1[u])) +
+                        (R(0.5) * (EF0[v + I] + EF1[v + I]) - R(0.5) * (EF0[v] + EF1[v]));
+        const R CFk1 = R(0.5) * (W[o + s2] + W[o]);
+        R hh = cff - cff4 * divUV;
+        hh = hh - cff4 * (CFk1 - CFk);
+        const R FCt1 = vflux_(tke0, W, p, s2, k + 1, N), FCg1 = vflux_(gls0, W, p, s2, k + 1, N);
+        const R ht = hdiv_(tke0, XF0, XF1, EF0, EF1, p, i, j, I, J, s2, k);
+        const R hg = hdiv_(gls0, XF0, XF1, EF0, EF1, p, i, j, I, J, s2, k);
+        const R t = (cff * ((R)c.c1 * tke0[o] + (R)c.c2 * tkei[o]) - cff4 * ht) - cff4 * (FCt1 - FCt);
+        const R q = (cff * ((R)c.c1 * gls0[o] + (R)c.c2 * glsi[o]) - cff4 * hg) - cff4 * (FCg1 - FCg);
+        tke3[o] = t / hh;
+        gls3[o] = q / hh;
+        tken[o] = cff * tke0[o];
+        glsn[o] = cff * gls0[o];
+        Hz_half[o] = hh;
+        FCt = FCt1;
+        FCg = FCg1;
+        CFk = CFk1;
+    }
+}
+
+// Zero-gradient lateral condition on the auxiliary level (edges from the adjacent interior
+// point, corners from the diagonal one), W levels 1..N-1.
+template <typename R>
+__global__ void k_gls_aux_bc(Geo<R> g, R *__restrict__ tke3, R *__restrict__ gls3) {
+    const int I = g.I, J = g.J;
+    const int nb = 2 * I + 2 * (J - 2);
+    const long e = tid_flat();
+    if (e >= (long)nb * (g.N - 1)) return;
+    const int k = 1 + (int)(e / nb), b = (int)(e % nb);
+    int i, j;
+    if (b < I) { i = b; j = 0; }
+    else if (b < 2 * I) { i = b - I; j = J - 1; }
+    else if (b < 2 * I + J - 2) { i = 0; j = 1 + (b - 2 * I); }
+    else { i = I - 1; j = 1 + (b - 2 * I - (J - 2)); }
+    const int si = i == 0 ? 1 : (i == I - 1 ? I - 2 : i);
+    const int sj = j == 0 ? 1 : (j == J - 1 ? J - 2 : j);
+    const long o = (long)k * g.s2;
+    tke3[o + (long)j * I + i] = tke3[o + (long)sj * I + si];
+    gls3[o + (long)j * I + i] = gls3[o + (long)sj * I + si];
+}
+
+template <typename R>
+cudaError_t Ops<R>::gls_prestep(const sf_ctx *ctx, GlsPre c, const R *Huon, const R *Hvom,
+                                const R *W, const R *Hz, const R *tke0, const R *tkei, R *tke3,
+                                R *tken, const R *gls0, const R *glsi, R *gls3, R *glsn,
+                                R *Hz_half, cudaStream_t s) {
+    const Geo<R> g = geo(ctx);
+    k_gls_prestep<R><<<(unsigned)((g.s2 + 127) / 128), 128, 0, s>>>(
+        g, c, Huon, Hvom, W, Hz, tke0, tkei, tke3, tken, gls0, glsi, gls3, glsn, Hz_half);
+    const long nb = (long)(2 * g.I + 2 * (g.J - 2)) * (g.N - 1);
+    k_gls_aux_bc<R><<<(unsigned)((nb + 255) / 256), 256, 0, s>>>(g, tke3, gls3);
+    return cudaGetLastError();
 }
 
 }  // namespace sf

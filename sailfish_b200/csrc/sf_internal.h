@@ -25,6 +25,12 @@ struct BcProgram {
     int *src_ch = nullptr;     // device
 };
 
+// Coefficients of the GLS predictor's half step: cff1, cff2 of the LF/AM3 interpolation and
+// cff3, the time step of the advective terms (gls_predictor_step.py:133-146).
+struct GlsPre {
+    double c1, c2, c3;
+};
+
 // Grid view handed to kernels by value.
 template <typename R>
 struct Geo {
@@ -101,7 +107,12 @@ struct Ops {
                                      const R *u, const R *v, const R *z_r, const R *Hz,
                                      const R *bvf, const R *sustr, const R *svstr, R *tke, R *gls,
                                      R *Akv, R *Akt, R *Akk, R *Akp, R *Lscale,
-                                     const uint8_t *sel, cudaStream_t s);
+                                     const uint8_t *sel, const int *list, const int *count,
+                                     cudaStream_t s);
+    static cudaError_t gls_prestep(const sf_ctx *c, GlsPre pc, const R *Huon, const R *Hvom,
+                                   const R *W, const R *Hz, const R *tke0, const R *tkei, R *tke3,
+                                   R *tken, const R *gls0, const R *glsi, R *gls3, R *glsn,
+                                   R *Hz_half, cudaStream_t s);
     static cudaError_t analytic_bvf(const sf_ctx *c, const R *z_w, double dT, double zscale,
                                     double galpha, R *bvf, cudaStream_t s);
 };

@@ -17,6 +17,7 @@
 // fast-time accumulators (Zt_avg1, DU_avg1, DV_avg1), the column sums of the 3D/2D
 // coupling and the depth recomputation (set_depth) stay in FP64.
 #pragma once
+#include <type_traits>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -724,6 +725,213 @@ __global__ void __launch_bounds__(128) k_step3d_uv(Geo<R> g, R *__restrict__ u, 
     }
 }
 
+// ---- FP32 form of step3d_UV: a pipelined column solve --------------------------------------
+// The same systems as build_eliminate/back_substitute for a tile of 64 consecutive flat points.
+// Memory and arithmetic are decoupled: the block streams the levels of its tile through a
+// ring of kPipeDepth shared-memory slots with cp.async (Hz, Akv, z_r at p, p-1 and p-I; the
+// old velocities and ru/rv at p), several levels ahead of the elimination, so that the bytes
+// in flight do not depend on how many threads an SM holds.  The U and V systems are
+// eliminated in one pass in the normalised Thomas form (c'_k = c_k / m_k,
+// d'_k = (r_k - a_k d'_{k-1}) / m_k, x_k = d'_k - c'_k x_{k+1}) with c', d' in shared memory,
+// and the barotropic sums of adjustBarotropicVelocity come from the column identity
+// sum_k hz_k x_k = sum_k r_k + fc_0 x_0 (the rows of the system summed: the off-diagonal terms
+// telescope, the bottom row keeps -fc_0 x_0), so the back-substitution reads nothing from
+// memory.  Rounding differs from the FP64 kernel's order of operations, within the FP32
+// form's tolerance.  Columns on the rows where the reference solves the U system a second
+// time for V (solveTri gated by isUNode, :525) and where V gets only the mean correction take
+// the general path above after the pipelined part.
+constexpr int kPipeCols = 64;
+constexpr int kPipeDepth = 6;
+constexpr int kPipeSlot = 3 * (2 * kPipeCols + 1) + 4 * kPipeCols;   // floats per level
+
+__host__ __device__ constexpr size_t pipe_smem_bytes(int N) {
+    return sizeof(float) * ((size_t)4 * N * kPipeCols + (size_t)kPipeDepth * kPipeSlot);
+}
+
+template <typename R>   // R = float only: the FP32 form
+__global__ void __launch_bounds__(kPipeCols) k_step3d_uv_pipe(Geo<R> g, float *__restrict__ u,
+        float *__restrict__ v, const float *__restrict__ ru, const float *__restrict__ rv,
+        float *__restrict__ ubar_t1, float *__restrict__ vbar_t1, float *__restrict__ ubar_t2,
+        float *__restrict__ vbar_t2, const float *__restrict__ Hz, const float *__restrict__ Akv,
+        const float *__restrict__ z_r, const double *__restrict__ DU,
+        const double *__restrict__ DV, const float *tmpU, const float *tmpV, float cff,
+        float lambda, float Dt, int do_bc, float bcval) {
+    extern __shared__ float spipe[];
+    const int N = g.N;
+    const long I = g.I, s2 = g.s2;
+    const int t = threadIdx.x;
+    const long p0 = (long)blockIdx.x * kPipeCols;
+    const long p = p0 + t;
+    float *cU = spipe + t, *dU = cU + N * kPipeCols, *cV = dU + N * kPipeCols,
+          *dV = cV + N * kPipeCols;
+    float *ring = spipe + 4 * N * kPipeCols;
+    const float *uo_all = tmpU ? tmpU : u, *vo_all = tmpV ? tmpV : v;
+    const long nHz = (long)N * s2, nAk = (long)(N + 1) * s2;
+
+    // level k into slot: Hz(k), Akv(k), z_r(k+1) at [p0-1, p0+63] and [p0-I, p0-I+63]; old
+    // u, v and ru, rv at level k on [p0, p0+63].  Out-of-range sources are zero-filled.
+    auto issue = [&](int k) {
+        float *sl = ring + (k % kPipeDepth) * kPipeSlot;
+        const long o = (long)k * s2;
+        for (int e = t; e < kPipeSlot; e += kPipeCols) {
+            const float *src;
+            long idx, lim;
+            if (e < 3 * (2 * kPipeCols + 1)) {
+                const int f = e / (2 * kPipeCols + 1), r = e % (2 * kPipeCols + 1);
+                const long q = r <= kPipeCols ? p0 - 1 + r : p0 - I + (r - kPipeCols - 1);
+                if (f == 0) { src = Hz; idx = o + q; lim = nHz; }
+                else if (f == 1) { src = Akv; idx = o + q; lim = nAk; }
+                else { src = z_r; idx = o + s2 + q; lim = k + 1 < N ? nHz : 0; }
+            } else {
+                const int f = (e - 3 * (2 * kPipeCols + 1)) / kPipeCols;
+                const int r = (e - 3 * (2 * kPipeCols + 1)) % kPipeCols;
+                src = f == 0 ? uo_all : (f == 1 ? vo_all : (f == 2 ? ru : rv));
+                idx = o + p0 + r;
+                lim = nAk;
+            }
+            const bool ok = idx >= 0 && idx < lim;
+            cp_async(sl + e, ok ? src + idx : src, ok);
+        }
+    };
+    const int i = (int)(p % I), j = (int)(p / I);
+    const bool live = p < s2;
+    const bool un = live && unode_(i, j), vn = live && vnode_(i, j, g.J);
+    const bool both = un && vn;
+
+    for (int k = 0; k < kPipeDepth; ++k) {
+        if (k < N) issue(k);
+        cp_async_commit();
+    }
+    const float cm = -lambda * Dt;
+    float cmnU = 0.f, cmnV = 0.f, zP = 0.f, zW = 0.f, zS = 0.f;
+    if (both) {
+        cmnU = cff * Dt * (((g.pm[p] + g.pm[p - 1]) * 0.5f) * ((g.pn[p] + g.pn[p - 1]) * 0.5f));
+        cmnV = cff * Dt * (((g.pm[p] + g.pm[p - I]) * 0.5f) * ((g.pn[p] + g.pn[p - I]) * 0.5f));
+        zP = z_r[p];
+        zW = z_r[p - 1];
+        zS = z_r[p - I];
+    }
+    float fu = 0.f, fv = 0.f, fu0 = 0.f, fv0 = 0.f, ccu = 0.f, ccv = 0.f, ddu = 0.f, ddv = 0.f;
+    double HU = 0.0, HV = 0.0, OU = 0.0, OV = 0.0, RU = 0.0, RV = 0.0;
+    for (int k = 0; k < N; ++k) {
+        cp_async_wait<kPipeDepth - 1>();
+        __syncthreads();
+        if (both) {
+            const float *sl = ring + (k % kPipeDepth) * kPipeSlot;
+            const float *sHz = sl, *sAk = sl + (2 * kPipeCols + 1), *sZr = sl + 2 * (2 * kPipeCols + 1);
+            const float *sUo = sl + 3 * (2 * kPipeCols + 1), *sVo = sUo + kPipeCols,
+                        *sRu = sVo + kPipeCols, *sRv = sRu + kPipeCols;
+            const float hP = sHz[t + 1];
+            const float hu = (hP + sHz[t]) * 0.5f, hv = (hP + sHz[kPipeCols + 1 + t]) * 0.5f;
+            float gu = 0.f, gv = 0.f;
+            if (k < N - 1) {
+                const float zP1 = sZr[t + 1], zW1 = sZr[t], zS1 = sZr[kPipeCols + 1 + t];
+                const float a = sAk[t + 1];
+                gu = (cm * ((a + sAk[t]) * 0.5f)) / (((zP1 - zP) + (zW1 - zW)) * 0.5f);
+                gv = (cm * ((a + sAk[kPipeCols + 1 + t]) * 0.5f)) / (((zP1 - zP) + (zS1 - zS)) * 0.5f);
+                zP = zP1;
+                zW = zW1;
+                zS = zS1;
+            }
+            const float ou = sUo[t], ov = sVo[t];
+            if (k == 0) {   // bottom row: right-hand side forced to 0 (:610)
+                fu0 = gu;
+                fv0 = gv;
+                ccu = gu / (hu - 2.f * gu);
+                ccv = gv / (hv - 2.f * gv);
+                ddu = 0.f;
+                ddv = 0.f;
+            } else {
+                const float r_u = hu * (ou + cmnU * sRu[t]);
+                const float r_v = hv * (ov + cmnV * sRv[t]);
+                const float bu = (k < N - 1) ? (hu - gu) - fu : hu - fu;
+                const float bv = (k < N - 1) ? (hv - gv) - fv : hv - fv;
+                const float iu = 1.f / (bu - fu * ccu), iv = 1.f / (bv - fv * ccv);
+                ccu = gu * iu;
+                ccv = gv * iv;
+                ddu = (r_u - fu * ddu) * iu;
+                ddv = (r_v - fv * ddv) * iv;
+                RU += (double)r_u;
+                RV += (double)r_v;
+            }
+            cU[k * kPipeCols] = ccu;
+            dU[k * kPipeCols] = ddu;
+            cV[k * kPipeCols] = ccv;
+            dV[k * kPipeCols] = ddv;
+            fu = gu;
+            fv = gv;
+            HU += (double)hu;
+            HV += (double)hv;
+            OU += (double)(ou * hu);
+            OV += (double)(ov * hv);
+        }
+        __syncthreads();                 // slot k % depth is free again
+        if (k + kPipeDepth < N) issue(k + kPipeDepth);
+        cp_async_commit();
+    }
+    cp_async_wait<0>();
+    if (both) {
+        const double duo = DU[p] / (double)g.on_u[p], dvo = DV[p] / (double)g.om_v[p];
+        const float subU = (float)((OU - duo) / HU), subV = (float)((OV - dvo) / HV);
+        float xu = ddu, xv = ddv;
+        float *up = u + p, *vp = v + p;
+        up[(long)(N - 1) * s2] = xu - subU;
+        vp[(long)(N - 1) * s2] = xv - subV;
+        for (int k = N - 2; k >= 0; --k) {
+            xu = dU[k * kPipeCols] - cU[k * kPipeCols] * xu;
+            xv = dV[k * kPipeCols] - cV[k * kPipeCols] * xv;
+            up[(long)k * s2] = xu - subU;
+            vp[(long)k * s2] = xv - subV;
+        }
+        const double HuU = RU + (double)fu0 * (double)xu - (double)subU * HU;
+        const double HvV = RV + (double)fv0 * (double)xv - (double)subV * HV;
+        const float ub = (float)(duo / HU + (HuU - duo) / HU);
+        const float vb = (float)(dvo / HV + (HvV - dvo) / HV);
+        ubar_t2[p] = ub;
+        vbar_t2[p] = vb;
+        ubar_t1[p] = ub;
+        vbar_t1[p] = vb;
+    } else if (un || vn) {
+        const float *uo = uo_all + p, *vo = vo_all + p;
+        float FCa[kNMax], BDa[kNMax], RHSa[kNMax];
+        const Tri<float> m{FCa, BDa, RHSa, 1, 0};
+        if (un) {
+            double H, Hu;
+            build_eliminate(g, p, 1, cff, Dt, lambda, m, Hz, Akv, z_r, uo, ru, H, Hu);
+            const float udiff = (float)((Hu - DU[p] / (double)g.on_u[p]) / H);
+            back_substitute(N, s2, m, u + p, udiff);
+            eliminate_again(N, m);
+            back_substitute(N, s2, m, v + p, 0.f);
+            double HU2 = 0.0, HV2 = 0.0, HuU = 0.0, HvV = 0.0;
+            for (int K = 0; K < N; ++K) {
+                const long o = (long)K * s2 + p;
+                const float hzu = (Hz[o] + Hz[o - 1]) * 0.5f, hzv = (Hz[o] + Hz[o - I]) * 0.5f;
+                HU2 += (double)hzu;
+                HV2 += (double)hzv;
+                HuU += (double)(hzu * u[o]);
+                HvV += (double)(hzv * v[o]);
+            }
+            const double duo = DU[p] / (double)g.on_u[p], dvo = DV[p] / (double)g.om_v[p];
+            const float ub = (float)(duo / HU2 + (HuU - duo) / HU2);
+            const float vb = (float)(dvo / HV2 + (HvV - dvo) / HV2);
+            ubar_t2[p] = ub;
+            vbar_t2[p] = vb;
+            ubar_t1[p] = ub;
+            vbar_t1[p] = vb;
+        } else {
+            const float vdiff = mean_correction(N, s2, p, I, Hz, vo, DV[p], (double)g.om_v[p]);
+            for (int K = 0; K < N; ++K) v[(long)K * s2 + p] = v[(long)K * s2 + p] - vdiff;
+        }
+    }
+    if (do_bc && live) {
+        const int ut = g.utype[p], vt = g.vtype[p];
+        if (ut > 0 && (ut & (1 << 4)) == 0 && (ut & (1 << 3)) != 0)
+            for (int K = 0; K < N; ++K) u[(long)K * s2 + p] = bcval;
+        if (vt > 0 && ((vt & (1 << 4)) != 0 || (vt & (1 << 3)) != 0))
+            for (int K = 0; K < N; ++K) v[(long)K * s2 + p] = 0.f;
+    }
+}
+
 // setLateralUVBCs alone (step3D_uv.kernels.cpp:314-368).
 template <typename R>
 __global__ void __launch_bounds__(kBlock) k_lateral_uv_bc(Geo<R> g, R *__restrict__ u,
@@ -864,6 +1072,23 @@ cudaError_t Ops<R>::step3d_uv(const sf_ctx *c, R *u, R *v, const R *ru, const R 
                               const R *tmpV, double cff, double lambda, double Dt, int do_bc,
                               double bcval, cudaStream_t s) {
     const int B = 128;
+    if constexpr (std::is_same<R, float>::value) {
+        static bool attr_set[64] = {};
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+            const cudaError_t e = cudaFuncSetAttribute(k_step3d_uv_pipe<float>,
+                                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                       (int)pipe_smem_bytes(kNMax));
+            if (e != cudaSuccess) return e;
+            attr_set[dev] = true;
+        }
+        k_step3d_uv_pipe<float><<<blocks_for(c->s2, kPipeCols), kPipeCols, pipe_smem_bytes(c->N),
+                                  s>>>(geo(c), u, v, ru, rv, ubar_t1, vbar_t1, ubar_t2, vbar_t2,
+                                       Hz, Akv, z_r, DU, DV, tmpU, tmpV, (float)cff,
+                                       (float)lambda, (float)Dt, do_bc, (float)bcval);
+        return cudaGetLastError();
+    }
     k_step3d_uv<R><<<blocks_for(c->s2, B), B, 0, s>>>(
         geo(c), u, v, ru, rv, ubar_t1, vbar_t1, ubar_t2, vbar_t2, Hz, Akv, z_r, DU, DV, tmpU, tmpV,
         (R)cff, (R)lambda, (R)Dt, do_bc, (R)bcval);
@@ -880,10 +1105,10 @@ cudaError_t Ops<R>::gls_corrector(const sf_ctx *c, const sf_gls_params &P, doubl
                                   const R *v, const R *z_r, const R *Hz, const R *bvf,
                                   const R *sustr, const R *svstr, R *tke, R *gls, R *Akv, R *Akt,
                                   R *Akk, R *Akp, R *Lscale, const uint8_t *sel,
-                                  cudaStream_t s) {
+                                  const int *list, const int *count, cudaStream_t s) {
     k_gls_corrector<R><<<blocks_for(c->s2, 128), 128, 0, s>>>(geo(c), P, (R)dt, u, v, z_r, Hz, bvf,
                                                               sustr, svstr, tke, gls, Akv, Akt,
-                                                              Akk, Akp, Lscale, sel);
+                                                              Akk, Akp, Lscale, sel, list, count);
     return cudaGetLastError();
 }
 

@@ -285,6 +285,24 @@ __device__ __forceinline__ float gelu_fast(float x) {
     return 0.5f * x * (1.f + t);
 }
 
+// GELU(v + bias) of 32 consecutive outputs of row r, as the next layer's BF16 operand: four
+// 16-byte stores, one per core-matrix row segment.
+__device__ __forceinline__ void store_act8x4(__nv_bfloat16 *sA, int r, int n0, const float *v,
+                                             const float *bias) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        uint32_t pk[4];
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {
+            const int k = 8 * q + 2 * h;
+            const __nv_bfloat162 b2 = __floats2bfloat162_rn(gelu_fast(v[k] + bias[n0 + k]),
+                                                            gelu_fast(v[k + 1] + bias[n0 + k + 1]));
+            pk[h] = *reinterpret_cast<const uint32_t *>(&b2);
+        }
+        *reinterpret_cast<uint4 *>(&sA[cm_index(r, n0 + 8 * q)]) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+    }
+}
+
 __global__ void __launch_bounds__(kInferThreads, 1) k_infer(InferW w, long n,
                                                             const float *__restrict__ X,
                                                             float *__restrict__ Y, int *err) {
@@ -362,9 +380,7 @@ __global__ void __launch_bounds__(kInferThreads, 1) k_infer(InferW w, long n,
                 tmem_ld32(tmem + trow + cb + c * 32, v);
                 const int n0 = cb + c * 32;
                 if (!last) {
-#pragma unroll
-                    for (int k = 0; k < 32; ++k)
-                        sA[cm_index(rl, n0 + k)] = __float2bfloat16_rn(gelu_fast(v[k] + sbias[l][n0 + k]));
+                    store_act8x4(sA, rl, n0, v, sbias[l]);
                 } else if (r < n) {
                     float4 *y = reinterpret_cast<float4 *>(Y + r * kTile + n0);
 #pragma unroll
@@ -414,10 +430,10 @@ __global__ void k_range_mask(long s2, int I, int J, int nfeat, const float *__re
     mask[p] = out;
 }
 
-// Feature row of the column at p (rho-interior): 32 levels of log-scaled shear^2 and of
-// sign-preserving log-scaled N^2 at the interior W points (zero padded past N-1), then
-// log10 of the surface friction velocity squared, the surface buoyancy flux (0: no heat flux
-// in these basins) and log10 of the depth; the rest of the 128 inputs are 0.
+// Feature row of the column at p (rho-interior), nl = N-1 interior W levels: log-scaled shear^2
+// at levels 1..N-1 in x[0, nl), sign-preserving log-scaled N^2 in x[nl, 2nl), then log10 of
+// the surface friction velocity squared, the surface buoyancy flux (0: no heat flux in these
+// basins) and log10 of the depth in x[2nl], x[2nl+1], x[2nl+2]; the rest of the 128 are 0.
 template <typename R>
 __global__ void k_features(Geo<R> g, const R *__restrict__ u, const R *__restrict__ v,
                            const R *__restrict__ z_r, const R *__restrict__ bvf,
@@ -432,24 +448,25 @@ __global__ void k_features(Geo<R> g, const R *__restrict__ u, const R *__restric
     const int i = pi % g.I, j = pi / g.I;
     if (!column_(i, j, g.I, g.J)) return;
 #define AT(A, k, q) ((float)(A)[(long)(k) * s2 + (q)])
-    for (int k = 1; k < N && k <= 32; ++k) {
+    const int nl = N - 1;   // interior W levels; 2 nl + 3 <= 128 is checked by the caller
+    for (int k = 1; k < N; ++k) {
         const float cff = 0.5f / (AT(z_r, k, p) - AT(z_r, k - 1, p));
         const float du = (AT(u, k, p) - AT(u, k - 1, p)) + (AT(u, k, p + 1) - AT(u, k - 1, p + 1));
         const float dv = (AT(v, k, p) - AT(v, k - 1, p)) + (AT(v, k, p + I) - AT(v, k - 1, p + I));
         const float sh2 = (cff * du) * (cff * du) + (cff * dv) * (cff * dv);
         const float n2 = AT(bvf, k, p);
         x[k - 1] = log10f(sh2 + 1e-12f);
-        x[32 + k - 1] = copysignf(log10f(1.f + fabsf(n2) * 1e8f), n2);
+        x[nl + k - 1] = copysignf(log10f(1.f + fabsf(n2) * 1e8f), n2);
     }
     const float su = (float)(sustr[p] + sustr[p + 1]), sv = (float)(svstr[p] + svstr[p + I]);
-    x[64] = log10f(0.5f * sqrtf(su * su + sv * sv) + 1e-10f);
-    x[65] = 0.f;
-    x[66] = log10f((float)g.hd[p]);
+    x[2 * nl] = log10f(0.5f * sqrtf(su * su + sv * sv) + 1e-10f);
+    x[2 * nl + 1] = 0.f;
+    x[2 * nl + 2] = log10f((float)g.hd[p]);
 #undef AT
 }
 
-// Akv, Akt at interior W levels 1..N-1 from the outputs (log10, clipped to [-6, -1]); rows of
-// columns flagged in `fallback` (non-zero) keep the values already in Akv/Akt.
+// Akv, Akt at interior W levels 1..N-1 from the outputs y[0, nl) and y[nl, 2nl) (log10,
+// clipped to [-6, -1]); columns flagged in `fallback` (non-zero) keep the values in Akv/Akt.
 template <typename R>
 __global__ void k_apply(Geo<R> g, const float *__restrict__ Y, const uint8_t *__restrict__ fallback,
                         R *__restrict__ Akv, R *__restrict__ Akt) {
@@ -460,12 +477,176 @@ __global__ void k_apply(Geo<R> g, const float *__restrict__ Y, const uint8_t *__
     if (fallback && fallback[pi]) return;
     const long p = pi, s2 = g.s2;
     const float *y = Y + p * kTile;
-    for (int k = 1; k < g.N && k <= 32; ++k) {
+    const int nl = g.N - 1;
+    for (int k = 1; k < g.N; ++k) {
         Akv[(long)k * s2 + p] = (R)exp10f(fminf(fmaxf(y[k - 1], -6.f), -1.f));
-        Akt[(long)k * s2 + p] = (R)exp10f(fminf(fmaxf(y[32 + k - 1], -6.f), -1.f));
+        Akt[(long)k * s2 + p] = (R)exp10f(fminf(fmaxf(y[nl + k - 1], -6.f), -1.f));
     }
 }
 
+
+// ---- the closure in one pass -----------------------------------------------------------------
+// Features, range check, all layers and the coefficient update for a tile of 128 consecutive
+// flat columns: the feature row of each column is computed straight into the BF16 operand in
+// shared memory (threads along the columns, so every level of u, v, z_r, bvf is read
+// coalesced), the network runs as in k_infer, and the epilogue writes Akv/Akt level by level
+// (lanes along the columns: coalesced) for the in-range interior columns.  fallback[p] is set
+// for interior columns with a feature outside [lo, hi] (those keep Akv/Akt for plain GLS).
+template <typename R>
+__device__ __forceinline__ float feature_(const Geo<R> &g, long p, int f, int nl,
+                                          const R *__restrict__ u, const R *__restrict__ v,
+                                          const R *__restrict__ z_r, const R *__restrict__ bvf,
+                                          const R *__restrict__ sustr, const R *__restrict__ svstr) {
+    const long I = g.I, s2 = g.s2;
+#define AT(A, k, q) ((float)(A)[(long)(k) * s2 + (q)])
+    if (f < nl) {
+        const int k = f + 1;
+        const float cff = 0.5f / (AT(z_r, k, p) - AT(z_r, k - 1, p));
+        const float du = (AT(u, k, p) - AT(u, k - 1, p)) + (AT(u, k, p + 1) - AT(u, k - 1, p + 1));
+        const float dv = (AT(v, k, p) - AT(v, k - 1, p)) + (AT(v, k, p + I) - AT(v, k - 1, p + I));
+        const float sh2 = (cff * du) * (cff * du) + (cff * dv) * (cff * dv);
+        return log10f(sh2 + 1e-12f);
+    }
+    if (f < 2 * nl) {
+        const float n2 = AT(bvf, f - nl + 1, p);
+        return copysignf(log10f(1.f + fabsf(n2) * 1e8f), n2);
+    }
+#undef AT
+    if (f == 2 * nl) {
+        const float su = (float)(sustr[p] + sustr[p + 1]), sv = (float)(svstr[p] + svstr[p + I]);
+        return log10f(0.5f * sqrtf(su * su + sv * sv) + 1e-10f);
+    }
+    if (f == 2 * nl + 2) return log10f((float)g.hd[p]);
+    return 0.f;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kInferThreads, 1) k_closure(Geo<R> g, InferW w,
+        const R *__restrict__ u, const R *__restrict__ v, const R *__restrict__ z_r,
+        const R *__restrict__ bvf, const R *__restrict__ sustr, const R *__restrict__ svstr,
+        int nfeat, const float *__restrict__ lo, const float *__restrict__ hi,
+        uint8_t *__restrict__ fallback, int *__restrict__ flist, int *__restrict__ fcount,
+        R *__restrict__ Akv, R *__restrict__ Akt, int *err) {
+    extern __shared__ __align__(1024) unsigned char dsm[];
+    __nv_bfloat16 *sA = reinterpret_cast<__nv_bfloat16 *>(dsm);
+    __nv_bfloat16 *sW = sA + kTile * kTile;
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ uint32_t tmem_base;
+    __shared__ float sbias[SF_MLP_LAYERS][kTile];
+    __shared__ float slo[kTile], shi[kTile];
+    __shared__ uint8_t sflag[2][kTile];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int nl = g.N - 1;
+    const long s2 = g.s2;
+    if (warp == 0) tmem_alloc(&tmem_base);
+    if (tid == 0) {
+        mbar_init(&mbar);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::);
+    }
+    for (int l = 0; l < SF_MLP_LAYERS; ++l) {
+        for (int e = tid; e < kTile * kTile; e += kInferThreads)
+            sW[l * kTile * kTile + cm_index(e >> 7, e & 127)] = w.W[l][e];
+        for (int e = tid; e < kTile; e += kInferThreads) sbias[l][e] = w.b[l] ? w.b[l][e] : 0.f;
+    }
+    for (int e = tid; e < kTile; e += kInferThreads) {
+        slo[e] = lo[e];
+        shi[e] = hi[e];
+    }
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem = tmem_base;
+    const int rl = (warp & 3) * 32 + lane;
+    const int cb = (warp >> 2) * 64;
+    const uint32_t trow = (uint32_t)((warp & 3) * 32) << 16;
+    uint32_t phase = 0;
+    bool ok = true;
+    const long ntiles = (s2 + kTile - 1) / kTile;
+    for (long t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+        const long m0 = t * kTile;
+        __syncthreads();   // the previous tile's fallback flags have been read
+        {   // feature rows into the operand; thread (c, half) takes the 8-feature groups
+            // half, half+2, ... (16-byte stores of a core-matrix row)
+            const int c = tid & (kTile - 1), half = tid >> 7;
+            const long p = m0 + c;
+            const bool col = p < s2 && column_((int)(p % g.I), (int)(p / g.I), g.I, g.J);
+            uint8_t out = 0;
+            for (int f0 = 8 * half; f0 < kTile; f0 += 16) {
+                uint32_t pk[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    float x2[2];
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const int f = f0 + 2 * q + h;
+                        const float x =
+                            col ? feature_(g, p, f, nl, u, v, z_r, bvf, sustr, svstr) : 0.f;
+                        if (col && f < nfeat && !(x >= slo[f] && x <= shi[f])) out = 1;
+                        x2[h] = x;
+                    }
+                    const __nv_bfloat162 b2 = __floats2bfloat162_rn(x2[0], x2[1]);
+                    pk[q] = *reinterpret_cast<const uint32_t *>(&b2);
+                }
+                *reinterpret_cast<uint4 *>(&sA[cm_index(c, f0)]) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+            }
+            sflag[half][c] = out;
+        }
+        for (int l = 0; l < SF_MLP_LAYERS; ++l) {
+            fence_proxy_async();
+            __syncthreads();
+            if (tid == 0) {
+                fence_after();
+                const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sW + l * kTile * kTile);
+                for (int s = 0; s < kTile / 16; ++s)
+                    mma_bf16(tmem, sdesc(a0 + s * 256, kLBO, kSBO), sdesc(b0 + s * 256, kLBO, kSBO),
+                             s > 0 ? 1u : 0u);
+                mma_commit(&mbar);
+            }
+            const bool done = mbar_wait(&mbar, phase);
+            phase ^= 1;
+            fence_after();
+            if (__syncthreads_or(!done)) {
+                ok = false;
+                break;
+            }
+            const long p = m0 + rl;
+            const bool last = l == SF_MLP_LAYERS - 1;
+            bool apply = false;
+            if (last && p < s2) {
+                apply = column_((int)(p % g.I), (int)(p / g.I), g.I, g.J) &&
+                        !(sflag[0][rl] | sflag[1][rl]);
+            }
+            for (int c = 0; c < 2; ++c) {
+                float vv[32];
+                tmem_ld32(tmem + trow + cb + c * 32, vv);
+                const int n0 = cb + c * 32;
+                if (!last) {
+                    store_act8x4(sA, rl, n0, vv, sbias[l]);
+                } else if (apply) {
+#pragma unroll 8
+                    for (int k = 0; k < 32; ++k) {
+                        const int n = n0 + k;
+                        const float y = exp10f(fminf(fmaxf(vv[k] + sbias[l][n], -6.f), -1.f));
+                        if (n < nl) Akv[(long)(n + 1) * s2 + p] = (R)y;
+                        else if (n < 2 * nl) Akt[(long)(n - nl + 1) * s2 + p] = (R)y;
+                    }
+                }
+            }
+            fence_before();
+        }
+        if (ok && tid < kTile && m0 + tid < s2) {
+            const long p = m0 + tid;
+            const bool fb = column_((int)(p % g.I), (int)(p / g.I), g.I, g.J) &&
+                            (sflag[0][tid] | sflag[1][tid]);
+            fallback[p] = fb ? 1 : 0;
+            if (fb && flist) flist[atomicAdd(fcount, 1)] = (int)p;
+        }
+    }
+    if (!ok && tid == 0) atomicExch(err, 1);
+    fence_before();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tmem);
+}
 }  // namespace mlp
 }  // namespace sf
 
@@ -584,6 +765,7 @@ int sf_mlp_adam(long n, float *w, const float *g, float *m, float *v, void *w_bf
 int sf_closure_features(sf_ctx *c, const void *u, const void *v, const void *z_r, const void *bvf,
                         const void *sustr, const void *svstr, float *X, sf_stream s) {
     if (!c || !X) return mfail(SF_EINVAL, "bad argument");
+    if (2 * (c->N - 1) + 3 > kTile) return mfail(SF_EUNSUPPORTED, "closure rows hold N <= 63 levels");
     cudaError_t e;
     if (c->prec == SF_FP64) {
         auto g = sf::Ops<double>::geo(c);
@@ -603,6 +785,7 @@ int sf_closure_features(sf_ctx *c, const void *u, const void *v, const void *z_r
 int sf_closure_apply(sf_ctx *c, const float *Y, const uint8_t *fallback, void *Akv, void *Akt,
                      sf_stream s) {
     if (!c || !Y) return mfail(SF_EINVAL, "bad argument");
+    if (2 * (c->N - 1) > kTile) return mfail(SF_EUNSUPPORTED, "closure rows hold N <= 63 levels");
     if (c->prec == SF_FP64) {
         auto g = sf::Ops<double>::geo(c);
         sf::mlp::k_apply<double><<<nblk(c->s2, 128), 128, 0, S(s)>>>(g, Y, fallback, (double *)Akv,
@@ -642,6 +825,59 @@ int sf_mlp_infer(const sf_mlp_params *w, int n, const float *X, float *Y, int *e
     sf::mlp::k_infer<<<grid, sf::mlp::kInferThreads, sf::mlp::kInferSmem, S(s)>>>(iw, n, X, Y, err);
     e = cudaGetLastError();
     return e == cudaSuccess ? SF_OK : mcuda(e, "sf_mlp_infer");
+}
+
+int sf_closure_step(sf_ctx *c, const sf_mlp_params *w, const void *u, const void *v,
+                    const void *z_r, const void *bvf, const void *sustr, const void *svstr,
+                    int nfeat, const float *lo, const float *hi, uint8_t *fallback,
+                    int *fallback_list, int *fallback_count, void *Akv, void *Akt, int *err,
+                    sf_stream s) {
+    if (!c || !w || !u || !v || !z_r || !bvf || !sustr || !svstr || !lo || !hi || !fallback ||
+        !Akv || !Akt || !err || nfeat < 0 || nfeat > kTile || (!fallback_list != !fallback_count))
+        return mfail(SF_EINVAL, "bad argument");
+    if (2 * (c->N - 1) + 3 > kTile) return mfail(SF_EUNSUPPORTED, "closure rows hold N <= 63 levels");
+    sf::mlp::InferW iw;
+    for (int l = 0; l < SF_MLP_LAYERS; ++l) {
+        if (!w->W[l]) return mfail(SF_EINVAL, "null weight matrix");
+        iw.W[l] = static_cast<const __nv_bfloat16 *>(w->W[l]);
+        iw.b[l] = w->b[l];
+    }
+    static bool attr_set[2][64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return mcuda(e, "sf_closure_step");
+    const int pi = c->prec == SF_FP64 ? 1 : 0;
+    if (dev >= 0 && dev < 64 && !attr_set[pi][dev]) {
+        e = pi ? cudaFuncSetAttribute(sf::mlp::k_closure<double>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)sf::mlp::kInferSmem)
+               : cudaFuncSetAttribute(sf::mlp::k_closure<float>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)sf::mlp::kInferSmem);
+        if (e != cudaSuccess) return mcuda(e, "cudaFuncSetAttribute");
+        attr_set[pi][dev] = true;
+    }
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const long tiles = (c->s2 + kTile - 1) / kTile;
+    const unsigned grid = (unsigned)(tiles < sms ? tiles : sms);
+    if (fallback_count) {
+        e = cudaMemsetAsync(fallback_count, 0, sizeof(int), S(s));
+        if (e != cudaSuccess) return mcuda(e, "sf_closure_step");
+    }
+    if (pi) {
+        sf::mlp::k_closure<double><<<grid, sf::mlp::kInferThreads, sf::mlp::kInferSmem, S(s)>>>(
+            sf::Ops<double>::geo(c), iw, (const double *)u, (const double *)v, (const double *)z_r,
+            (const double *)bvf, (const double *)sustr, (const double *)svstr, nfeat, lo, hi,
+            fallback, fallback_list, fallback_count, (double *)Akv, (double *)Akt, err);
+    } else {
+        sf::mlp::k_closure<float><<<grid, sf::mlp::kInferThreads, sf::mlp::kInferSmem, S(s)>>>(
+            sf::Ops<float>::geo(c), iw, (const float *)u, (const float *)v, (const float *)z_r,
+            (const float *)bvf, (const float *)sustr, (const float *)svstr, nfeat, lo, hi,
+            fallback, fallback_list, fallback_count, (float *)Akv, (float *)Akt, err);
+    }
+    e = cudaGetLastError();
+    return e == cudaSuccess ? SF_OK : mcuda(e, "sf_closure_step");
 }
 
 int sf_closure_range_mask(sf_ctx *c, const float *X, int nfeat, const float *lo, const float *hi,

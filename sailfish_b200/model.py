@@ -7,6 +7,7 @@
     barotropic loop, nfast+1 substeps   sf_barotropic_loop      (main3d.py:166-189)
     set_depth                           sf_set_depth            (main3d.py:290)
     step3d_UV + setLateralUVBCs         sf_step3d_uv_bc         (main3d.py:304-311)
+    vertical mixing (optional)          Model.mixing            (GLS or the learned closure)
     omega                               sf_omega                (main3d.py:321)
 
 Layout in HBM: the reference's flat C-order fields.  The three barotropic time slots of each
@@ -155,6 +156,9 @@ class Model:
         self.Hz = z(N, J, I)
         self.slots = [0, 1, 2]                    # (t0, t1, t2) rows of the 2D buffers
         self._started = False
+        # vertical mixing per step (closure.Closure), after step3d_UV; None keeps AKv as it is,
+        # as the reference's step does (modules/mod_ocean.py:91)
+        self.mixing = None
 
     # -- state I/O ------------------------------------------------------------------------
     def load(self, state):
@@ -252,6 +256,8 @@ class Model:
                 p(self._slot("vbar", 1)), p(self._slot("ubar", 2)), p(self._slot("vbar", 2)),
                 p(self.Hz), p(self.AKv), p(self.z_r), p(self.DU_avg1), p(self.DV_avg1), self.iic,
                 self.ntfirst, self.lam, self.dt, self.time, st), "sf_step3d_uv_bc"))
+            if self.mixing is not None:
+                phase("closure", self.mixing)
             if final_omega and k == nsteps - 1:
                 phase("k_omega", lambda: check(lib.sf_omega(
                     c, p(self.W), p(self.Huon), p(self.Hvom), p(self.z_w), st), "sf_omega"))

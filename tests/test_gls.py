@@ -97,3 +97,112 @@ def test_gls_fp32_within_tolerance():
     for k in ("Akv", "Akt", "tke"):
         rel = np.abs(got[k][:, col] - ref[k][:, col]) / np.abs(ref[k][:, col])
         assert rel.max() < 2e-3, (k, rel.max())
+
+
+# ---- GLS predictor (gls_predictor_step.py:18-216) -------------------------------------------
+def predictor_case(I=13, J=9, N=8, seed=3):
+    rng = np.random.default_rng(seed)
+    s2 = I * J
+    pm = 1.0 / (1000.0 * (1.0 + 0.2 * rng.random(s2)))
+    pn = 1.0 / (1200.0 * (1.0 + 0.2 * rng.random(s2)))
+    Hz = 5.0 + 3.0 * rng.random((N, s2))
+    Huon = 200.0 * rng.standard_normal((N + 1, s2))
+    Hvom = 200.0 * rng.standard_normal((N + 1, s2))
+    W = 20.0 * rng.standard_normal((N + 1, s2))
+    t0 = 1e-4 * (1.0 + rng.random((N + 1, s2)))
+    ti = 1e-4 * (1.0 + rng.random((N + 1, s2)))
+    g0 = 1e-7 * (1.0 + rng.random((N + 1, s2)))
+    gi = 1e-7 * (1.0 + rng.random((N + 1, s2)))
+    return dict(I=I, J=J, N=N, pm=pm, pn=pn, Hz=Hz, Huon=Huon, Hvom=Hvom, W=W, t0=t0, ti=ti,
+                g0=g0, gi=gi)
+
+
+def test_predictor_oracle_preserves_constants():
+    """With a constant tke and no horizontal flux divergence the half step keeps the constant
+    (the scheme is constancy preserving, gls_predictor_step.py:9-13)."""
+    c = predictor_case()
+    I, J, N = c["I"], c["J"], c["N"]
+    s2 = I * J
+    ones = np.full((N + 1, s2), 3e-4)
+    Huon = np.tile(np.linspace(1.0, 2.0, N + 1)[:, None], (1, s2))   # uniform along i and j
+    Hvom = np.zeros((N + 1, s2))
+    W = np.zeros((N + 1, s2))
+    t3, g3, tn, gn, hh = go.gls_prestep(60.0, False, I, J, N, c["pm"], c["pn"], Huon, Hvom, W,
+                                        c["Hz"], ones, ones, ones, ones)
+    a = t3.reshape(N + 1, J, I)[1:N, 1:J - 1, 1:I - 1]
+    np.testing.assert_allclose(a, 3e-4, rtol=1e-12)
+
+
+def gpu_predictor(c, precision, first):
+    import ctypes
+    import torch
+    from sailfish_b200 import host as H
+    from sailfish_b200._lib import lib, check
+    from sailfish_b200.model import Context, Grid
+    I, J, N = c["I"], c["J"], c["N"]
+    L, M = I - 1, J - 1
+    z = np.zeros(I * J)
+    sc_r, sc_w, Cs_r, Cs_w = H.set_coords(N, 4, 5.0, 0.4)
+    grid = Grid(L, M, N, z + 50.0, c["pm"], c["pn"], z + 1.0, z + 1.0, z, sc_r, sc_w, Cs_r,
+                Cs_w, 10.0, 2)
+    ctx = Context(grid, H.Boundary(L, M), precision)
+    dt_ = torch.float64 if precision == "fp64" else torch.float32
+    T = {k: torch.tensor(np.ascontiguousarray(c[k]), dtype=dt_, device="cuda")
+         for k in ("Huon", "Hvom", "W", "Hz", "t0", "ti", "g0", "gi")}
+    out = {k: torch.zeros((N + 1, I * J), dtype=dt_, device="cuda")
+           for k in ("t3", "tn", "g3", "gn", "hh")}
+    ptr = lambda t: ctypes.c_void_p(t.data_ptr())
+    check(lib.sf_gls_predictor(ctx.ptr, 60.0, int(first), ptr(T["Huon"]), ptr(T["Hvom"]),
+                               ptr(T["W"]), ptr(T["Hz"]), ptr(T["t0"]), ptr(T["ti"]),
+                               ptr(out["t3"]), ptr(out["tn"]), ptr(T["g0"]), ptr(T["gi"]),
+                               ptr(out["g3"]), ptr(out["gn"]), ptr(out["hh"]),
+                               ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)),
+          "sf_gls_predictor")
+    torch.cuda.synchronize()
+    return {k: v.double().cpu().numpy() for k, v in out.items()}
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("first", [False, True])
+@pytest.mark.parametrize("precision,rtol", [("fp64", 1e-12), ("fp32", 2e-4)])
+def test_gls_predictor_matches_oracle(precision, rtol, first):
+    c = predictor_case()
+    ref = go.gls_prestep(60.0, first, c["I"], c["J"], c["N"], c["pm"], c["pn"], c["Huon"],
+                         c["Hvom"], c["W"], c["Hz"], c["t0"], c["ti"], c["g0"], c["gi"])
+    got = gpu_predictor(c, precision, first)
+    N, s2 = c["N"], c["I"] * c["J"]
+    for name, r in zip(("t3", "g3", "tn", "gn", "hh"), ref):
+        g = got[name][1:N]
+        np.testing.assert_allclose(g, r[1:N], rtol=rtol, atol=rtol * np.abs(r[1:N]).max(),
+                                   err_msg=name)
+
+
+@pytest.mark.gpu
+def test_gls_on_a_column_list_matches_the_mask():
+    """sf_gls_corrector_list over a compacted list gives the masked result exactly."""
+    import ctypes
+    import torch
+    from sailfish_b200 import closure, configs
+    from sailfish_b200.model import Model
+    cfg = configs.small(24, 16, 12)
+    out = []
+    for use_list in (False, True):
+        m = Model(cfg["grid"], cfg["boundary"], cfg["dt"], cfg["ndtfast"], precision="fp32")
+        m.start()
+        cols = closure.Columns(m)
+        closure.wind_driven_state(m, cols, 0.1, 0.3, 500.0, np.random.default_rng(1))
+        s2 = m.grid.s2
+        sel = torch.zeros(s2, dtype=torch.uint8, device="cuda")
+        sel[5::7] = 1
+        if use_list:
+            idx = torch.nonzero(sel).flatten().flip(0).to(torch.int32).contiguous()
+            lst = torch.zeros(s2, dtype=torch.int32, device="cuda")
+            lst[:idx.numel()] = idx
+            cnt = torch.tensor([idx.numel()], dtype=torch.int32, device="cuda")
+            cols.gls_step_list(lst, cnt)
+        else:
+            cols.gls_step(sel)
+        torch.cuda.synchronize()
+        out.append((m.AKv.clone(), cols.tke.clone(), cols.Akt.clone()))
+    for a, b in zip(*out):
+        torch.testing.assert_close(a, b, rtol=0, atol=0)
