@@ -172,6 +172,9 @@ def algorithmic_bytes(grid, esize):
         "k_step3d_uv": esize * (9 * N) * s2 + 16 * s2,          # u,v,ru,rv,Hz,Akv,z_r -> u,v; DU,DV
         "k_maxflux_omega": esize * (4 * N + 3 * (N + 1)) * s2,  # u,v,Hz,z_w -> Huon,Hvom,W
         "k_set_depth": esize * (3 * N + 1) * s2 + 16 * s2,      # Zt,h -> z_w,z_r,Hz
+        # the learned closure (k_closure + GLS on its fallback columns), per interior column:
+        # u, v, z_r (N levels), bvf (N-1 interior W levels), sustr, svstr, h -> Akv, Akt (N-1)
+        "closure": (esize * (4 * N - 1) + 3 * esize + 2 * esize * (N - 1)) * (grid.L - 1) * (grid.M - 1),
     }
 
 
@@ -270,7 +273,7 @@ def install_mixing(m, mode, config):
     return closure.mixing_for(m, mode, net)
 
 
-def closure_error(m, steps=40):
+def closure_error(m, steps=300):
     """Learned closure against plain GLS at the bench state: GLS spun up for `steps`
     iterations on the same columns, then the network's Akv/Akt (in-range columns) against
     GLS's, log10 RMS over the interior columns and levels 1..N-1."""

@@ -140,6 +140,12 @@ int sf_barotropic_substep(sf_ctx *ctx, const sf_state2d *s, double dtfast, doubl
  * host array weight1. */
 int sf_barotropic_loop(sf_ctx *ctx, sf_state2d *s, int nsub, const double *weight1,
                        double dtfast, double *time2D, sf_stream stream);
+/* Turn the CUDA-graph replay of sf_barotropic_loop on (default) or off.  With graphs on, the
+ * loop's launches are captured once per (slot pointers, weights, time step) — at most three
+ * captures, as the slots rotate with period 3 — and replayed as one graph launch; the clamped
+ * boundary values, which depend on time2D, are written to the device before each replay.
+ * Results are identical either way.  No counterpart in the reference. */
+int sf_ctx_set_graphs(sf_ctx *ctx, int enable);
 
 /* ---- 3D right-hand side, nonlinear/rhs.py:16-93 + nonlinear/rhs_kernels.cpp ------------ */
 /* rhs3d: ru = rv = 0, addCoriolis (:7-35), horizontalAdvection (:71-132), verticalAdvection
@@ -220,6 +226,15 @@ int sf_gls_corrector_list(sf_ctx *ctx, const sf_gls_params *params, double dt, c
                           const void *sustr, const void *svstr, void *tke, void *gls, void *Akv,
                           void *Akt, void *Akk, void *Akp, void *Lscale, const int *list,
                           const int *count, sf_stream stream);
+/* obc_volcons (nonlinear/obc_volcons.py:6-69, ROMS pseudo-code in the reference): the
+ * cross-section area and volume flux through the open edges selected by `edges` (W=1, E=2,
+ * S=4, N=8), out[0] = area, out[1] = flux (inflow positive), out[2] = ubar_xs = flux/area,
+ * accumulated in FP64 with compensated summation in a fixed order (deterministic).  With
+ * `correct`, conserve_mass_tile follows: ubar on W/E and vbar on S/N open edges corrected by
+ * -/+ ubar_xs so that the net flux through them vanishes.  zeta: the time level in use;
+ * the depths come from the context's h. */
+int sf_obc_volcons(sf_ctx *ctx, const void *zeta, void *ubar, void *vbar, int edges, int correct,
+                   double *out, sf_stream stream);
 /* Buoyancy frequency squared at all N+1 W levels of a linear equation of state in temperature
  * (alpha, 1/degC) with the analytic profile T(z) = T0 + dT exp(z/zscale):
  * bvf = g alpha dT/zscale exp(z_w/zscale).  The stratification of the analytic basins, whose

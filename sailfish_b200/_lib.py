@@ -81,6 +81,8 @@ SIGNATURES = {
     "sf_gls_corrector_list": [_vp, ctypes.POINTER(GlsParams), _d] + [_vp] * 16 + [_vp],
     "sf_analytic_bvf": [_vp, _vp, _d, _d, _d, _d, _vp, _vp],
     "sf_gls_predictor": [_vp, _d, _i] + [_vp] * 13 + [_vp],
+    "sf_obc_volcons": [_vp, _vp, _vp, _vp, _i, _i, _vp, _vp],
+    "sf_ctx_set_graphs": [_vp, _i],
     "sf_mlp_last_error": [],
     "sf_mlp_gemm": [_i, _i, _vp, _i, ctypes.c_long, ctypes.c_long, _vp, _i, ctypes.c_long,
                     ctypes.c_long, _vp, _i, _vp, ctypes.c_long, _vp, ctypes.c_long, _vp, _vp],

@@ -142,6 +142,10 @@ void free_ctx(sf_ctx *c) {
     cudaFree(c->bcfield);
     cudaFree(c->utype);
     cudaFree(c->vtype);
+    for (auto &g : c->graphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+    if (c->cap) cudaStreamDestroy(c->cap);
+    cudaFree(c->d_bcval);
     for (sf::BcProgram *p : {&c->zbc, &c->ubc, &c->vbc}) {
         cudaFree(p->dst);
         cudaFree(p->src);
@@ -393,7 +397,7 @@ int sf_step2d_corrector(sf_ctx *c, const sf_state2d *st, double dtfast, double t
 namespace {
 template <typename R>
 cudaError_t substep(const sf_ctx *c, const sf_state2d *st, double dtfast, double time2D,
-                    double cff1, int last, cudaStream_t s) {
+                    double cff1, int last, cudaStream_t s, const double *dval = nullptr) {
     using O = sf::Ops<R>;
     const double val = .05 * std::sin(time2D * kBcOmega);
     R *z0 = (R *)st->zeta[0], *z1 = (R *)st->zeta[1], *z2 = (R *)st->zeta[2];
@@ -407,7 +411,8 @@ cudaError_t substep(const sf_ctx *c, const sf_state2d *st, double dtfast, double
         e = O::momentum(c, (R *)st->rubar[1], (R *)st->rvbar[1], z2, z0, 10.0, 2.0 / 5.0, 1, 1,
                         dtfast, (R *)st->ubar[1], (R *)st->ubar[2], (R *)st->vbar[1],
                         (R *)st->vbar[2], z1, z2, s);
-    if (e == cudaSuccess) e = O::bc_apply(c, c->ubc, (R *)st->ubar[2], c->vbc, (R *)st->vbar[2], val, s);
+    if (e == cudaSuccess)
+        e = O::bc_apply(c, c->ubc, (R *)st->ubar[2], c->vbc, (R *)st->vbar[2], val, s, dval);
     // corrector (step2d.py:84-128) and vbar_t2[:] = 0 (main3d.py:189)
     if (e == cudaSuccess)
         e = O::zeta_rhs(c, z2, (R *)st->ubar[2], (R *)st->vbar[2], (R *)st->rzeta[1], 1, cff1,
@@ -442,9 +447,138 @@ int sf_barotropic_substep(sf_ctx *c, const sf_state2d *st, double dtfast, double
     });
 }
 
+}  // extern "C"
+
+namespace {
+// The clamped boundary values of the substeps of one loop, passed by value to a one-block
+// kernel that writes them to the context's device array before the captured loop replays.
+struct BcVals {
+    double v[256];
+};
+__global__ void k_set_bcvals(BcVals vals, int n, double *dst) {
+    for (int k = threadIdx.x; k < n; k += blockDim.x) dst[k] = vals.v[k];
+}
+
+void rotate(sf_state2d *st) {   // T_OCEAN.cycleTimes2D
+    void **arrs[6] = {st->zeta, st->ubar, st->vbar, st->rzeta, st->rubar, st->rvbar};
+    for (void **a : arrs) {
+        void *t0 = a[0];
+        a[0] = a[1];
+        a[1] = a[2];
+        a[2] = t0;
+    }
+}
+
+bool graph_matches(const sf_loop_graph &g, const sf_state2d *st, int nsub, const double *w,
+                   double dtfast) {
+    if (!g.exec || g.nsub != nsub || g.dtfast != dtfast) return false;
+    void *const *arrs[6] = {st->zeta, st->ubar, st->vbar, st->rzeta, st->rubar, st->rvbar};
+    for (int a = 0; a < 6; ++a)
+        for (int k = 0; k < 3; ++k)
+            if (g.slots[3 * a + k] != arrs[a][k]) return false;
+    if (g.acc[0] != st->Zt_avg1 || g.acc[1] != st->DU_avg1 || g.acc[2] != st->DV_avg1) return false;
+    for (int k = 0; k < nsub; ++k)
+        if (g.w[k] != w[k]) return false;
+    return true;
+}
+
+// The loop's launches in order on stream s; with `dval` the clamped boundary values are read
+// from dval[iif-1] on the device instead of being passed by value.
+int loop_body(sf_ctx *c, sf_state2d *st, int nsub, const double *weight1, double dtfast,
+              double t2, cudaStream_t s, const double *dval) {
+    const size_t n2 = (size_t)c->s2 * sizeof(double);
+    cudaError_t e = cudaMemsetAsync(st->Zt_avg1, 0, n2, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(st->DU_avg1, 0, n2, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(st->DV_avg1, 0, n2, s);
+    if (e != cudaSuccess) return cuda_fail(e, "sf_barotropic_loop");
+    for (int iif = 1; iif <= nsub; ++iif) {
+        t2 += dtfast;
+        rotate(st);
+        const double *dv = dval ? dval + (iif - 1) : nullptr;
+        e = c->prec == SF_FP64
+                ? substep<double>(c, st, dtfast, t2, weight1[iif - 1], iif == nsub, s, dv)
+                : substep<float>(c, st, dtfast, t2, weight1[iif - 1], iif == nsub, s, dv);
+        if (e != cudaSuccess) return cuda_fail(e, "sf_barotropic_loop");
+    }
+    return SF_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int sf_ctx_set_graphs(sf_ctx *c, int enable) {
+    if (!c) return fail(SF_EINVAL, "null context");
+    c->use_graphs = enable ? 1 : 0;
+    return SF_OK;
+}
+
 int sf_barotropic_loop(sf_ctx *c, sf_state2d *st, int nsub, const double *weight1, double dtfast,
                        double *time2D, sf_stream s) {
     if (!st || !weight1 || !time2D || nsub < 1) return fail(SF_EINVAL, "bad argument");
+    if (!c) return fail(SF_EINVAL, "null context");
+    if (c->use_graphs && nsub <= 256) {
+        // Replay a captured loop: the same launches with the same arguments; only the clamped
+        // boundary values (a function of time2D) change, and they are read on the device.
+        sf_loop_graph *g = nullptr;
+        for (auto &cand : c->graphs)
+            if (graph_matches(cand, st, nsub, weight1, dtfast)) g = &cand;
+        cudaError_t e = cudaSuccess;
+        if (!g) {
+            if (!c->cap) {
+                e = cudaStreamCreateWithFlags(&c->cap, cudaStreamNonBlocking);
+                if (e != cudaSuccess) return cuda_fail(e, "cudaStreamCreate");
+            }
+            if (!c->d_bcval) {
+                e = cudaMalloc(&c->d_bcval, 256 * sizeof(double));
+                if (e != cudaSuccess) return fail(SF_ENOMEM, "cudaMalloc bcval");
+            }
+            g = &c->graphs[c->graph_next];
+            c->graph_next = (c->graph_next + 1) % 3;
+            if (g->exec) {
+                cudaGraphExecDestroy(g->exec);
+                g->exec = nullptr;
+            }
+            sf_state2d tmp = *st;
+            e = cudaStreamBeginCapture(c->cap, cudaStreamCaptureModeThreadLocal);
+            if (e != cudaSuccess) return cuda_fail(e, "cudaStreamBeginCapture");
+            const int rc = loop_body(c, &tmp, nsub, weight1, dtfast, 0.0, c->cap, c->d_bcval);
+            cudaGraph_t graph = nullptr;
+            e = cudaStreamEndCapture(c->cap, &graph);
+            if (rc != SF_OK) {
+                if (graph) cudaGraphDestroy(graph);
+                return rc;
+            }
+            if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+            e = cudaGraphInstantiate(&g->exec, graph, 0);
+            cudaGraphDestroy(graph);
+            if (e != cudaSuccess) {
+                g->exec = nullptr;
+                return cuda_fail(e, "cudaGraphInstantiate");
+            }
+            g->nsub = nsub;
+            g->dtfast = dtfast;
+            void *const *arrs[6] = {st->zeta, st->ubar, st->vbar, st->rzeta, st->rubar, st->rvbar};
+            for (int a = 0; a < 6; ++a)
+                for (int k = 0; k < 3; ++k) g->slots[3 * a + k] = arrs[a][k];
+            g->acc[0] = st->Zt_avg1;
+            g->acc[1] = st->DU_avg1;
+            g->acc[2] = st->DV_avg1;
+            for (int k = 0; k < nsub; ++k) g->w[k] = weight1[k];
+        }
+        BcVals vals;
+        double t2 = *time2D;
+        for (int iif = 1; iif <= nsub; ++iif) {
+            t2 += dtfast;                              // CompTimes.next2DTimeStep
+            vals.v[iif - 1] = .05 * std::sin(t2 * kBcOmega);
+            rotate(st);
+        }
+        k_set_bcvals<<<1, 256, 0, S(s)>>>(vals, nsub, c->d_bcval);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaGraphLaunch(g->exec, S(s));
+        if (e != cudaSuccess) return cuda_fail(e, "sf_barotropic_loop (graph)");
+        *time2D = t2;
+        return SF_OK;
+    }
     const size_t n2 = (size_t)c->s2 * sizeof(double);
     cudaError_t e = cudaMemsetAsync(st->Zt_avg1, 0, n2, S(s));
     if (e == cudaSuccess) e = cudaMemsetAsync(st->DU_avg1, 0, n2, S(s));
@@ -644,6 +778,17 @@ int sf_gls_predictor(sf_ctx *c, double dt, int first_step, const void *Huon, con
                                          (const R *)tke_indx, (R *)tke_aux, (R *)tke_nnew,
                                          (const R *)gls_nstp, (const R *)gls_indx, (R *)gls_aux,
                                          (R *)gls_nnew, (R *)Hz_half, S(s));
+    });
+}
+
+int sf_obc_volcons(sf_ctx *c, const void *zeta, void *ubar, void *vbar, int edges, int correct,
+                   double *out, sf_stream s) {
+    if (!out) return fail(SF_EINVAL, "null output");
+    if (edges < 0 || edges > 15) return fail(SF_EINVAL, "edges is a mask of W=1, E=2, S=4, N=8");
+    return dispatch(c, "sf_obc_volcons", [&](auto *t) {
+        using R = std::remove_pointer_t<decltype(t)>;
+        return sf::Ops<R>::obc_volcons(c, (const R *)zeta, (R *)ubar, (R *)vbar, edges, correct,
+                                       out, S(s));
     });
 }
 

@@ -48,6 +48,17 @@ struct Geo {
 
 }  // namespace sf
 
+// A captured barotropic loop (sf_barotropic_loop): valid for the slot pointers, weights and
+// time step it was captured with.
+struct sf_loop_graph {
+    cudaGraphExec_t exec = nullptr;
+    int nsub = 0;
+    double dtfast = 0.0;
+    void *slots[18] = {};
+    double *acc[3] = {};
+    double w[256] = {};
+};
+
 struct sf_ctx {
     int prec;
     int L, M, N, I, J;
@@ -61,6 +72,14 @@ struct sf_ctx {
     int *bcfield, *utype, *vtype;
     sf::BcProgram zbc, ubc, vbc;
     long ref_threads;
+    // CUDA-graph replay of the barotropic loop: a capture stream, the per-substep clamped
+    // boundary values (device, written before each replay), and up to 3 captured loops (the
+    // slot rotation cycles with period 3).
+    int use_graphs = 1;
+    cudaStream_t cap = nullptr;
+    double *d_bcval = nullptr;
+    sf_loop_graph graphs[3];
+    int graph_next = 0;
 };
 
 namespace sf {
@@ -87,7 +106,8 @@ struct Ops {
                                   const R *rz1, const R *rz2, R *ubar_t1, const R *vbar_t1,
                                   const R *rub0, const R *rub1, R *vbar_t2, cudaStream_t s);
     static cudaError_t bc_apply(const sf_ctx *c, const BcProgram &p1, R *f1,
-                                const BcProgram &p2, R *f2, double val, cudaStream_t s);
+                                const BcProgram &p2, R *f2, double val, cudaStream_t s,
+                                const double *valp = nullptr);
     static cudaError_t rhs3d(const sf_ctx *c, const R *u, const R *v, const R *Huon,
                              const R *Hvom, const R *W, const R *Hz, R *ru, R *rv,
                              cudaStream_t s);
@@ -113,6 +133,8 @@ struct Ops {
                                    const R *W, const R *Hz, const R *tke0, const R *tkei, R *tke3,
                                    R *tken, const R *gls0, const R *glsi, R *gls3, R *glsn,
                                    R *Hz_half, cudaStream_t s);
+    static cudaError_t obc_volcons(const sf_ctx *c, const R *zeta, R *ubar, R *vbar, int edges,
+                                   int correct, double *out, cudaStream_t s);
     static cudaError_t analytic_bvf(const sf_ctx *c, const R *z_w, double dT, double zscale,
                                     double galpha, R *bvf, cudaStream_t s);
 };

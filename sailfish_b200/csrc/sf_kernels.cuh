@@ -187,7 +187,9 @@ __device__ __forceinline__ R bc_value(const R *f, int s, R val) {
 }
 
 template <typename R>
-__global__ void __launch_bounds__(256) k_bc_apply(BcProgram p1, R *f1, BcProgram p2, R *f2, R val) {
+__global__ void __launch_bounds__(256) k_bc_apply(BcProgram p1, R *f1, BcProgram p2, R *f2, R val0,
+                                                  const double *valp) {
+    const R val = valp ? (R)valp[0] : val0;   // time-dependent value from the device (graphs)
     const long t = tid_flat();
     if (t < p1.n) {
         f1[p1.dst[t]] = bc_value(f1, p1.src[t], val);
@@ -766,32 +768,33 @@ __global__ void __launch_bounds__(kPipeCols) k_step3d_uv_pipe(Geo<R> g, float *_
           *dV = cV + N * kPipeCols;
     float *ring = spipe + 4 * N * kPipeCols;
     const float *uo_all = tmpU ? tmpU : u, *vo_all = tmpV ? tmpV : v;
-    const long nHz = (long)N * s2, nAk = (long)(N + 1) * s2;
 
     // level k into slot: Hz(k), Akv(k), z_r(k+1) at [p0-1, p0+63] and [p0-I, p0-I+63]; old
-    // u, v and ru, rv at level k on [p0, p0+63].  Out-of-range sources are zero-filled.
+    // u, v and ru, rv at level k on [p0, p0+63].  Thread t copies the element at t of every
+    // segment (thread 0 also the 65th of the shifted rows); sources outside [0, s2) in the
+    // plane are zero-filled (their columns are not U/V nodes).
+    const long qW = p0 - 1 + t, qS = p0 - I + t, qE = p0 + kPipeCols - 1;
+    const bool okW = qW >= 0 && qW < s2, okS = qS >= 0 && qS < s2, okP = p < s2;
+    const bool okE = t == 0 && qE < s2;
+    constexpr int kRow = 2 * kPipeCols + 1;
     auto issue = [&](int k) {
         float *sl = ring + (k % kPipeDepth) * kPipeSlot;
         const long o = (long)k * s2;
-        for (int e = t; e < kPipeSlot; e += kPipeCols) {
-            const float *src;
-            long idx, lim;
-            if (e < 3 * (2 * kPipeCols + 1)) {
-                const int f = e / (2 * kPipeCols + 1), r = e % (2 * kPipeCols + 1);
-                const long q = r <= kPipeCols ? p0 - 1 + r : p0 - I + (r - kPipeCols - 1);
-                if (f == 0) { src = Hz; idx = o + q; lim = nHz; }
-                else if (f == 1) { src = Akv; idx = o + q; lim = nAk; }
-                else { src = z_r; idx = o + s2 + q; lim = k + 1 < N ? nHz : 0; }
-            } else {
-                const int f = (e - 3 * (2 * kPipeCols + 1)) / kPipeCols;
-                const int r = (e - 3 * (2 * kPipeCols + 1)) % kPipeCols;
-                src = f == 0 ? uo_all : (f == 1 ? vo_all : (f == 2 ? ru : rv));
-                idx = o + p0 + r;
-                lim = nAk;
-            }
-            const bool ok = idx >= 0 && idx < lim;
-            cp_async(sl + e, ok ? src + idx : src, ok);
+        const bool zr = k + 1 < N;
+        const float *fld[3] = {Hz + o, Akv + o, z_r + o + s2};
+#pragma unroll
+        for (int f = 0; f < 3; ++f) {
+            const bool on = f < 2 || zr;
+            float *d = sl + f * kRow;
+            cp_async(d + t, fld[f] + (okW && on ? qW : 0), okW && on);
+            cp_async(d + kPipeCols + 1 + t, fld[f] + (okS && on ? qS : 0), okS && on);
+            if (t == 0) cp_async(d + kPipeCols, fld[f] + (okE && on ? qE : 0), okE && on);
         }
+        float *d = sl + 3 * kRow;
+        cp_async(d + t, uo_all + o + (okP ? p : 0), okP);
+        cp_async(d + kPipeCols + t, vo_all + o + (okP ? p : 0), okP);
+        cp_async(d + 2 * kPipeCols + t, ru + o + (okP ? p : 0), okP);
+        cp_async(d + 3 * kPipeCols + t, rv + o + (okP ? p : 0), okP);
     };
     const int i = (int)(p % I), j = (int)(p / I);
     const bool live = p < s2;
@@ -932,6 +935,114 @@ __global__ void __launch_bounds__(kPipeCols) k_step3d_uv_pipe(Geo<R> g, float *_
     }
 }
 
+// ---- obc_volcons (nonlinear/obc_volcons.py:6-69, ROMS pseudo-code in the reference) -------
+// Area and volume flux through the open edges (W=1, E=2, S=4, N=8 in `edges`), in FP64 with
+// compensated (two-sum) accumulation in a fixed order, so the result is deterministic:
+//   W: cff = (D(0,j) + D(1,j))/2 on_u(1,j),    flux += cff ubar(1,j)
+//   E: cff = (D(L-1,j) + D(L,j))/2 on_u(L,j),  flux -= cff ubar(L,j)
+//   S: cff = (D(i,0) + D(i,1))/2 om_v(i,1),    flux += cff vbar(i,1)
+//   N: cff = (D(i,M-1) + D(i,M))/2 om_v(i,M),  flux -= cff vbar(i,M)
+// with D = zeta + h, j = 1..M-1, i = 1..L-1; ubar_xs = flux / area.
+struct TwoSum {
+    double s = 0.0, c = 0.0;
+    __device__ void add(double x) {       // Neumaier's compensated summation
+        const double t = s + x;
+        c += fabs(s) >= fabs(x) ? (s - t) + x : (x - t) + s;
+        s = t;
+    }
+    __device__ double value() const { return s + c; }
+};
+
+constexpr int kVolThreads = 256;
+
+template <typename R>
+__global__ void __launch_bounds__(kVolThreads) k_obc_volcons(Geo<R> g, const R *__restrict__ zeta,
+                                                             const R *__restrict__ ubar,
+                                                             const R *__restrict__ vbar, int edges,
+                                                             double *__restrict__ out) {
+    const int I = g.I, J = g.J, L = I - 1, M = J - 1;
+    const int nj = M - 1, ni = L - 1;          // interior rows / columns
+    TwoSum area, flux;
+    const int n = 2 * nj + 2 * ni;
+    for (int e = threadIdx.x; e < n; e += kVolThreads) {
+        int side, a;
+        if (e < nj) { side = 0; a = 1 + e; }
+        else if (e < 2 * nj) { side = 1; a = 1 + e - nj; }
+        else if (e < 2 * nj + ni) { side = 2; a = 1 + e - 2 * nj; }
+        else { side = 3; a = 1 + e - 2 * nj - ni; }
+        if (!(edges & (1 << side))) continue;
+        long q0, q1, f;
+        double metric, vel, sgn;
+        if (side < 2) {
+            const int i1 = side == 0 ? 1 : L;
+            q0 = (long)a * I + i1 - 1;
+            q1 = q0 + 1;
+            f = (long)a * I + i1;
+            metric = (double)g.on_u[f];
+            vel = (double)ubar[f];
+            sgn = side == 0 ? 1.0 : -1.0;
+        } else {
+            const int j1 = side == 2 ? 1 : M;
+            q0 = (long)(j1 - 1) * I + a;
+            q1 = q0 + I;
+            f = (long)j1 * I + a;
+            metric = (double)g.om_v[f];
+            vel = (double)vbar[f];
+            sgn = side == 2 ? 1.0 : -1.0;
+        }
+        const double cff = 0.5 * (((double)zeta[q0] + g.hd[q0]) + ((double)zeta[q1] + g.hd[q1])) * metric;
+        area.add(cff);
+        flux.add(sgn * cff * vel);
+    }
+    __shared__ double sa[kVolThreads], sf[kVolThreads];
+    sa[threadIdx.x] = area.value();
+    sf[threadIdx.x] = flux.value();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        TwoSum A, F;
+        for (int t = 0; t < kVolThreads; ++t) {
+            A.add(sa[t]);
+            F.add(sf[t]);
+        }
+        const double a = A.value(), fl = F.value();
+        out[0] = a;
+        out[1] = fl;
+        out[2] = a > 0.0 ? fl / a : 0.0;     // ubar_xs
+    }
+}
+
+// conserve_mass_tile: the normal velocity on the open edges corrected by ubar_xs.
+template <typename R>
+__global__ void k_conserve_mass(Geo<R> g, R *__restrict__ ubar, R *__restrict__ vbar, int edges,
+                                const double *__restrict__ xs_in) {
+    const int I = g.I, J = g.J, L = I - 1, M = J - 1;
+    const int nj = M - 1, ni = L - 1;
+    const int e = (int)tid_flat();
+    if (e >= 2 * nj + 2 * ni) return;
+    const double xs = xs_in[2];
+    if (e < nj) {
+        if (edges & 1) ubar[(long)(1 + e) * I + 1] -= (R)xs;
+    } else if (e < 2 * nj) {
+        if (edges & 2) ubar[(long)(1 + e - nj) * I + L] += (R)xs;
+    } else if (e < 2 * nj + ni) {
+        if (edges & 4) vbar[(long)1 * I + 1 + e - 2 * nj] -= (R)xs;
+    } else {
+        if (edges & 8) vbar[(long)M * I + 1 + e - 2 * nj - ni] += (R)xs;
+    }
+}
+
+template <typename R>
+cudaError_t Ops<R>::obc_volcons(const sf_ctx *c, const R *zeta, R *ubar, R *vbar, int edges,
+                                int correct, double *out, cudaStream_t s) {
+    k_obc_volcons<R><<<1, kVolThreads, 0, s>>>(geo(c), zeta, ubar, vbar, edges, out);
+    if (correct) {
+        const int n = 2 * (c->J - 2) + 2 * (c->I - 2);
+        k_conserve_mass<R><<<(unsigned)((n + kBlock - 1) / kBlock), kBlock, 0, s>>>(geo(c), ubar,
+                                                                                  vbar, edges, out);
+    }
+    return cudaGetLastError();
+}
+
 // setLateralUVBCs alone (step3D_uv.kernels.cpp:314-368).
 template <typename R>
 __global__ void __launch_bounds__(kBlock) k_lateral_uv_bc(Geo<R> g, R *__restrict__ u,
@@ -1033,10 +1144,10 @@ cudaError_t Ops<R>::corr_point(const sf_ctx *c, double Dt, R *zeta_t2, const R *
 }
 template <typename R>
 cudaError_t Ops<R>::bc_apply(const sf_ctx *c, const BcProgram &p1, R *f1, const BcProgram &p2,
-                             R *f2, double val, cudaStream_t s) {
+                             R *f2, double val, cudaStream_t s, const double *valp) {
     const long n = (long)p1.n + p2.n;
     if (n == 0 && p1.nch == 0 && p2.nch == 0) return cudaSuccess;
-    k_bc_apply<R><<<blocks_for(n > 0 ? n : 1, 256), 256, 0, s>>>(p1, f1, p2, f2, (R)val);
+    k_bc_apply<R><<<blocks_for(n > 0 ? n : 1, 256), 256, 0, s>>>(p1, f1, p2, f2, (R)val, valp);
     return cudaGetLastError();
 }
 template <typename R>

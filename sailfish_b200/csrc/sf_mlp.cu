@@ -493,34 +493,6 @@ __global__ void k_apply(Geo<R> g, const float *__restrict__ Y, const uint8_t *__
 // (lanes along the columns: coalesced) for the in-range interior columns.  fallback[p] is set
 // for interior columns with a feature outside [lo, hi] (those keep Akv/Akt for plain GLS).
 template <typename R>
-__device__ __forceinline__ float feature_(const Geo<R> &g, long p, int f, int nl,
-                                          const R *__restrict__ u, const R *__restrict__ v,
-                                          const R *__restrict__ z_r, const R *__restrict__ bvf,
-                                          const R *__restrict__ sustr, const R *__restrict__ svstr) {
-    const long I = g.I, s2 = g.s2;
-#define AT(A, k, q) ((float)(A)[(long)(k) * s2 + (q)])
-    if (f < nl) {
-        const int k = f + 1;
-        const float cff = 0.5f / (AT(z_r, k, p) - AT(z_r, k - 1, p));
-        const float du = (AT(u, k, p) - AT(u, k - 1, p)) + (AT(u, k, p + 1) - AT(u, k - 1, p + 1));
-        const float dv = (AT(v, k, p) - AT(v, k - 1, p)) + (AT(v, k, p + I) - AT(v, k - 1, p + I));
-        const float sh2 = (cff * du) * (cff * du) + (cff * dv) * (cff * dv);
-        return log10f(sh2 + 1e-12f);
-    }
-    if (f < 2 * nl) {
-        const float n2 = AT(bvf, f - nl + 1, p);
-        return copysignf(log10f(1.f + fabsf(n2) * 1e8f), n2);
-    }
-#undef AT
-    if (f == 2 * nl) {
-        const float su = (float)(sustr[p] + sustr[p + 1]), sv = (float)(svstr[p] + svstr[p + I]);
-        return log10f(0.5f * sqrtf(su * su + sv * sv) + 1e-10f);
-    }
-    if (f == 2 * nl + 2) return log10f((float)g.hd[p]);
-    return 0.f;
-}
-
-template <typename R>
 __global__ void __launch_bounds__(kInferThreads, 1) k_closure(Geo<R> g, InferW w,
         const R *__restrict__ u, const R *__restrict__ v, const R *__restrict__ z_r,
         const R *__restrict__ bvf, const R *__restrict__ sustr, const R *__restrict__ svstr,
@@ -565,30 +537,56 @@ __global__ void __launch_bounds__(kInferThreads, 1) k_closure(Geo<R> g, InferW w
     for (long t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
         const long m0 = t * kTile;
         __syncthreads();   // the previous tile's fallback flags have been read
-        {   // feature rows into the operand; thread (c, half) takes the 8-feature groups
-            // half, half+2, ... (16-byte stores of a core-matrix row)
+        {   // feature rows into the operand: thread (c, half) marches up half of column c's
+            // levels, carrying the level below in registers (6 loads per level)
             const int c = tid & (kTile - 1), half = tid >> 7;
             const long p = m0 + c;
             const bool col = p < s2 && column_((int)(p % g.I), (int)(p / g.I), g.I, g.J);
+            const int nh = (nl + 1) / 2;
+            const int k0 = half ? nh + 1 : 1, k1 = half ? nl : nh;   // levels k0..k1
             uint8_t out = 0;
-            for (int f0 = 8 * half; f0 < kTile; f0 += 16) {
-                uint32_t pk[4];
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    float x2[2];
-#pragma unroll
-                    for (int h = 0; h < 2; ++h) {
-                        const int f = f0 + 2 * q + h;
-                        const float x =
-                            col ? feature_(g, p, f, nl, u, v, z_r, bvf, sustr, svstr) : 0.f;
-                        if (col && f < nfeat && !(x >= slo[f] && x <= shi[f])) out = 1;
-                        x2[h] = x;
-                    }
-                    const __nv_bfloat162 b2 = __floats2bfloat162_rn(x2[0], x2[1]);
-                    pk[q] = *reinterpret_cast<const uint32_t *>(&b2);
+            auto put = [&](int f, float x) {
+                if (col && f < nfeat && !(x >= slo[f] && x <= shi[f])) out = 1;
+                sA[cm_index(c, f)] = __float2bfloat16_rn(x);
+            };
+            if (col) {
+                const long I = g.I;
+#define AT(A, k, q) ((float)(A)[(long)(k) * s2 + (q)])
+                float zb = AT(z_r, k0 - 1, p), ub = AT(u, k0 - 1, p), ube = AT(u, k0 - 1, p + 1);
+                float vb = AT(v, k0 - 1, p), vbn = AT(v, k0 - 1, p + I);
+#pragma unroll 4
+                for (int k = k0; k <= k1; ++k) {
+                    const float zt = AT(z_r, k, p), ut = AT(u, k, p), ute = AT(u, k, p + 1);
+                    const float vt = AT(v, k, p), vtn = AT(v, k, p + I), n2 = AT(bvf, k, p);
+                    const float cff = 0.5f / (zt - zb);
+                    const float du = (ut - ub) + (ute - ube), dv = (vt - vb) + (vtn - vbn);
+                    const float sh2 = (cff * du) * (cff * du) + (cff * dv) * (cff * dv);
+                    put(k - 1, log10f(sh2 + 1e-12f));
+                    put(nl + k - 1, copysignf(log10f(1.f + fabsf(n2) * 1e8f), n2));
+                    zb = zt;
+                    ub = ut;
+                    ube = ute;
+                    vb = vt;
+                    vbn = vtn;
                 }
-                *reinterpret_cast<uint4 *>(&sA[cm_index(c, f0)]) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+#undef AT
+                if (half) {
+                    const float su = (float)(sustr[p] + sustr[p + 1]);
+                    const float sv = (float)(svstr[p] + svstr[p + I]);
+                    put(2 * nl, log10f(0.5f * sqrtf(su * su + sv * sv) + 1e-10f));
+                    put(2 * nl + 1, 0.f);
+                    put(2 * nl + 2, log10f((float)g.hd[p]));
+                }
+            } else {
+                for (int k = k0; k <= k1; ++k) {
+                    sA[cm_index(c, k - 1)] = __float2bfloat16_rn(0.f);
+                    sA[cm_index(c, nl + k - 1)] = __float2bfloat16_rn(0.f);
+                }
+                if (half)
+                    for (int f = 2 * nl; f < 2 * nl + 3; ++f) sA[cm_index(c, f)] = __float2bfloat16_rn(0.f);
             }
+            // the padding features (the previous tile's activations are in the operand)
+            for (int f = 2 * nl + 3 + half; f < kTile; f += 2) sA[cm_index(c, f)] = __float2bfloat16_rn(0.f);
             sflag[half][c] = out;
         }
         for (int l = 0; l < SF_MLP_LAYERS; ++l) {

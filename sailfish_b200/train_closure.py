@@ -26,12 +26,15 @@ RECIPES = {
 }
 
 
-def train(config, out, runs=16, rest_runs=8, steps=6000, batch=4096, lr=1e-3, seed=1):
+def train(config, out, runs=16, rest_runs=8, spin=300, every=25, steps=6000, batch=4096, lr=1e-3,
+          seed=1):
+    """GLS is spun up `spin` steps at fixed forcing (10 h at dt = 120 s: the turbulence fields
+    settle to their forced state), then 4 snapshots `every` steps apart are kept."""
     cfg = RECIPES[config]()
     N = cfg["grid"].N
-    X, T = closure.generate(cfg, runs=runs, spin=30, keep=4, every=5, seed=seed,
+    X, T = closure.generate(cfg, runs=runs, spin=spin, keep=4, every=every, seed=seed,
                             rest_runs=rest_runs, pattern=True)
-    Xv, Tv = closure.generate(cfg, runs=4, spin=30, keep=2, every=5, seed=seed + 1000,
+    Xv, Tv = closure.generate(cfg, runs=4, spin=spin, keep=2, every=every, seed=seed + 1000,
                               rest_runs=2, pattern=True)
     net = closure.Network(N, seed=seed)
     net.fit_normalisation(X)
@@ -42,7 +45,7 @@ def train(config, out, runs=16, rest_runs=8, steps=6000, batch=4096, lr=1e-3, se
     const[:, N - 1:2 * (N - 1)] = -6.0
     ec = closure.log_rms(const, Tv, N)
     report = {"config": config, "N": N, "rows": int(X.shape[0]), "heldout_rows": int(Xv.shape[0]),
-              "steps": steps, "batch": batch, "loss": hist,
+              "gls_spinup": spin, "steps": steps, "batch": batch, "loss": hist,
               "heldout_log10_rms_akv": e[0], "heldout_log10_rms_akt": e[1],
               "constant_log10_rms_akv": ec[0], "constant_log10_rms_akt": ec[1]}
     os.makedirs(os.path.dirname(os.path.abspath(out)), exist_ok=True)
