@@ -146,6 +146,7 @@ void free_ctx(sf_ctx *c) {
         if (g.exec) cudaGraphExecDestroy(g.exec);
     if (c->cap) cudaStreamDestroy(c->cap);
     cudaFree(c->d_bcval);
+    cudaFree(c->closure_x);
     for (sf::BcProgram *p : {&c->zbc, &c->ubc, &c->vbc}) {
         cudaFree(p->dst);
         cudaFree(p->src);

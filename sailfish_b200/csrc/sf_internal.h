@@ -80,6 +80,9 @@ struct sf_ctx {
     double *d_bcval = nullptr;
     sf_loop_graph graphs[3];
     int graph_next = 0;
+    // the learned closure's feature-row tiles (sf_closure_step), allocated on first use
+    void *closure_x = nullptr;
+    size_t closure_x_bytes = 0;
 };
 
 namespace sf {

@@ -485,44 +485,125 @@ __global__ void k_apply(Geo<R> g, const float *__restrict__ Y, const uint8_t *__
 }
 
 
-// ---- the closure in one pass -----------------------------------------------------------------
-// Features, range check, all layers and the coefficient update for a tile of 128 consecutive
-// flat columns: the feature row of each column is computed straight into the BF16 operand in
-// shared memory (threads along the columns, so every level of u, v, z_r, bvf is read
-// coalesced), the network runs as in k_infer, and the epilogue writes Akv/Akt level by level
-// (lanes along the columns: coalesced) for the in-range interior columns.  fallback[p] is set
-// for interior columns with a feature outside [lo, hi] (those keep Akv/Akt for plain GLS).
+// ---- the closure: feature rows, then the network over row tiles ------------------------------
+// k_closure_rows: one thread per flat column (full occupancy, so the level loads of many columns
+// are in flight): it marches up the column carrying the level below in registers (6 loads per
+// level), writes the BF16 feature row straight into a 128-row tile stored in the MMA operand's
+// core-matrix layout (16-byte stores), checks the row against [lo, hi] and flags/lists the
+// columns outside it.  k_closure_mlp: persistent, one CTA per SM holding every layer's weights
+// in shared memory; each tile's operand arrives with one bulk copy (cp.async.bulk, 32 KB),
+// issued for the next tile as soon as the last layer's products have read the current one, so
+// it overlaps the output epilogue; the epilogue writes Akv/Akt level by level (lanes along the
+// columns: coalesced) for the interior columns in range.
 template <typename R>
-__global__ void __launch_bounds__(kInferThreads, 1) k_closure(Geo<R> g, InferW w,
-        const R *__restrict__ u, const R *__restrict__ v, const R *__restrict__ z_r,
-        const R *__restrict__ bvf, const R *__restrict__ sustr, const R *__restrict__ svstr,
-        int nfeat, const float *__restrict__ lo, const float *__restrict__ hi,
-        uint8_t *__restrict__ fallback, int *__restrict__ flist, int *__restrict__ fcount,
+__global__ void __launch_bounds__(128) k_closure_rows(Geo<R> g, const R *__restrict__ u,
+        const R *__restrict__ v, const R *__restrict__ z_r, const R *__restrict__ bvf,
+        const R *__restrict__ sustr, const R *__restrict__ svstr, int nfeat,
+        const float *__restrict__ lo, const float *__restrict__ hi, uint8_t *__restrict__ fallback,
+        int *__restrict__ flist, int *__restrict__ fcount, __nv_bfloat16 *__restrict__ Xt, long nrows) {
+    const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= nrows) return;
+    const long s2 = g.s2, I = g.I;
+    const int nl = g.N - 1;
+    __nv_bfloat16 *tile = Xt + (p / kTile) * (long)(kTile * kTile);
+    const int r = (int)(p % kTile);
+    const bool col = p < s2 && column_((int)(p % g.I), (int)(p / g.I), g.I, g.J);
+    bool out = false;
+#define AT(A, k, q) ((float)(A)[(long)(k) * s2 + (q)])
+    float zb = 0.f, ub = 0.f, ube = 0.f, vb = 0.f, vbn = 0.f;
+    if (col) {
+        zb = AT(z_r, 0, p);
+        ub = AT(u, 0, p);
+        ube = AT(u, 0, p + 1);
+        vb = AT(v, 0, p);
+        vbn = AT(v, 0, p + I);
+    }
+    int ks = 1;   // next shear level
+    for (int f0 = 0; f0 < kTile; f0 += 8) {
+        float x[8];
+#pragma unroll
+        for (int h = 0; h < 8; ++h) {
+            const int f = f0 + h;
+            float val = 0.f;
+            if (col) {
+                if (f < nl) {                       // shear^2 at W level ks = f + 1
+                    const int k = ks++;
+                    const float zt = AT(z_r, k, p), ut = AT(u, k, p), ute = AT(u, k, p + 1);
+                    const float vt = AT(v, k, p), vtn = AT(v, k, p + I);
+                    const float cff = 0.5f / (zt - zb);
+                    const float du = (ut - ub) + (ute - ube), dv = (vt - vb) + (vtn - vbn);
+                    const float sh2 = (cff * du) * (cff * du) + (cff * dv) * (cff * dv);
+                    val = log10f(sh2 + 1e-12f);
+                    zb = zt;
+                    ub = ut;
+                    ube = ute;
+                    vb = vt;
+                    vbn = vtn;
+                } else if (f < 2 * nl) {
+                    const float n2 = AT(bvf, f - nl + 1, p);
+                    val = copysignf(log10f(1.f + fabsf(n2) * 1e8f), n2);
+                } else if (f == 2 * nl) {
+                    const float su = (float)(sustr[p] + sustr[p + 1]);
+                    const float sv = (float)(svstr[p] + svstr[p + I]);
+                    val = log10f(0.5f * sqrtf(su * su + sv * sv) + 1e-10f);
+                } else if (f == 2 * nl + 2) {
+                    val = log10f((float)g.hd[p]);
+                }
+                if (f < nfeat && !(val >= lo[f] && val <= hi[f])) out = true;
+            }
+            x[h] = val;
+        }
+        uint32_t pk[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const __nv_bfloat162 b2 = __floats2bfloat162_rn(x[2 * q], x[2 * q + 1]);
+            pk[q] = *reinterpret_cast<const uint32_t *>(&b2);
+        }
+        *reinterpret_cast<uint4 *>(tile + cm_index(r, f0)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+    }
+#undef AT
+    if (p < s2) {
+        fallback[p] = out ? 1 : 0;
+        if (out && flist) flist[atomicAdd(fcount, 1)] = (int)p;
+    }
+}
+
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *mbar) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(mbar)),
+                 "r"(bytes));
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(mbar))
+        : "memory");
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kInferThreads, 1) k_closure_mlp(Geo<R> g, InferW w,
+        const __nv_bfloat16 *__restrict__ Xt, long ntiles, const uint8_t *__restrict__ fallback,
         R *__restrict__ Akv, R *__restrict__ Akt, int *err) {
     extern __shared__ __align__(1024) unsigned char dsm[];
     __nv_bfloat16 *sA = reinterpret_cast<__nv_bfloat16 *>(dsm);
     __nv_bfloat16 *sW = sA + kTile * kTile;
-    __shared__ __align__(8) uint64_t mbar;
+    __shared__ __align__(8) uint64_t mbar, xbar;
     __shared__ uint32_t tmem_base;
     __shared__ float sbias[SF_MLP_LAYERS][kTile];
-    __shared__ float slo[kTile], shi[kTile];
-    __shared__ uint8_t sflag[2][kTile];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int nl = g.N - 1;
     const long s2 = g.s2;
     if (warp == 0) tmem_alloc(&tmem_base);
     if (tid == 0) {
         mbar_init(&mbar);
+        mbar_init(&xbar);
         asm volatile("fence.mbarrier_init.release.cluster;" ::);
+        fence_proxy_async();
+        if ((long)blockIdx.x < ntiles)     // the first tile's operand, while the weights load
+            bulk_load(sA, Xt + (long)blockIdx.x * kTile * kTile, kTile * kTile * 2, &xbar);
     }
     for (int l = 0; l < SF_MLP_LAYERS; ++l) {
         for (int e = tid; e < kTile * kTile; e += kInferThreads)
             sW[l * kTile * kTile + cm_index(e >> 7, e & 127)] = w.W[l][e];
         for (int e = tid; e < kTile; e += kInferThreads) sbias[l][e] = w.b[l] ? w.b[l][e] : 0.f;
-    }
-    for (int e = tid; e < kTile; e += kInferThreads) {
-        slo[e] = lo[e];
-        shi[e] = hi[e];
     }
     fence_before();
     __syncthreads();
@@ -531,63 +612,17 @@ __global__ void __launch_bounds__(kInferThreads, 1) k_closure(Geo<R> g, InferW w
     const int rl = (warp & 3) * 32 + lane;
     const int cb = (warp >> 2) * 64;
     const uint32_t trow = (uint32_t)((warp & 3) * 32) << 16;
-    uint32_t phase = 0;
+    uint32_t phase = 0, xphase = 0;
     bool ok = true;
-    const long ntiles = (s2 + kTile - 1) / kTile;
     for (long t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
         const long m0 = t * kTile;
-        __syncthreads();   // the previous tile's fallback flags have been read
-        {   // feature rows into the operand: thread (c, half) marches up half of column c's
-            // levels, carrying the level below in registers (6 loads per level)
-            const int c = tid & (kTile - 1), half = tid >> 7;
-            const long p = m0 + c;
-            const bool col = p < s2 && column_((int)(p % g.I), (int)(p / g.I), g.I, g.J);
-            const int nh = (nl + 1) / 2;
-            const int k0 = half ? nh + 1 : 1, k1 = half ? nl : nh;   // levels k0..k1
-            uint8_t out = 0;
-            auto put = [&](int f, float x) {
-                if (col && f < nfeat && !(x >= slo[f] && x <= shi[f])) out = 1;
-                sA[cm_index(c, f)] = __float2bfloat16_rn(x);
-            };
-            if (col) {
-                const long I = g.I;
-#define AT(A, k, q) ((float)(A)[(long)(k) * s2 + (q)])
-                float zb = AT(z_r, k0 - 1, p), ub = AT(u, k0 - 1, p), ube = AT(u, k0 - 1, p + 1);
-                float vb = AT(v, k0 - 1, p), vbn = AT(v, k0 - 1, p + I);
-#pragma unroll 4
-                for (int k = k0; k <= k1; ++k) {
-                    const float zt = AT(z_r, k, p), ut = AT(u, k, p), ute = AT(u, k, p + 1);
-                    const float vt = AT(v, k, p), vtn = AT(v, k, p + I), n2 = AT(bvf, k, p);
-                    const float cff = 0.5f / (zt - zb);
-                    const float du = (ut - ub) + (ute - ube), dv = (vt - vb) + (vtn - vbn);
-                    const float sh2 = (cff * du) * (cff * du) + (cff * dv) * (cff * dv);
-                    put(k - 1, log10f(sh2 + 1e-12f));
-                    put(nl + k - 1, copysignf(log10f(1.f + fabsf(n2) * 1e8f), n2));
-                    zb = zt;
-                    ub = ut;
-                    ube = ute;
-                    vb = vt;
-                    vbn = vtn;
-                }
-#undef AT
-                if (half) {
-                    const float su = (float)(sustr[p] + sustr[p + 1]);
-                    const float sv = (float)(svstr[p] + svstr[p + I]);
-                    put(2 * nl, log10f(0.5f * sqrtf(su * su + sv * sv) + 1e-10f));
-                    put(2 * nl + 1, 0.f);
-                    put(2 * nl + 2, log10f((float)g.hd[p]));
-                }
-            } else {
-                for (int k = k0; k <= k1; ++k) {
-                    sA[cm_index(c, k - 1)] = __float2bfloat16_rn(0.f);
-                    sA[cm_index(c, nl + k - 1)] = __float2bfloat16_rn(0.f);
-                }
-                if (half)
-                    for (int f = 2 * nl; f < 2 * nl + 3; ++f) sA[cm_index(c, f)] = __float2bfloat16_rn(0.f);
+        {   // this tile's operand has landed (bounded wait)
+            const bool got = mbar_wait(&xbar, xphase);
+            xphase ^= 1;
+            if (__syncthreads_or(!got)) {
+                ok = false;
+                break;
             }
-            // the padding features (the previous tile's activations are in the operand)
-            for (int f = 2 * nl + 3 + half; f < kTile; f += 2) sA[cm_index(c, f)] = __float2bfloat16_rn(0.f);
-            sflag[half][c] = out;
         }
         for (int l = 0; l < SF_MLP_LAYERS; ++l) {
             fence_proxy_async();
@@ -595,9 +630,9 @@ __global__ void __launch_bounds__(kInferThreads, 1) k_closure(Geo<R> g, InferW w
             if (tid == 0) {
                 fence_after();
                 const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sW + l * kTile * kTile);
-                for (int s = 0; s < kTile / 16; ++s)
-                    mma_bf16(tmem, sdesc(a0 + s * 256, kLBO, kSBO), sdesc(b0 + s * 256, kLBO, kSBO),
-                             s > 0 ? 1u : 0u);
+                for (int q = 0; q < kTile / 16; ++q)
+                    mma_bf16(tmem, sdesc(a0 + q * 256, kLBO, kSBO), sdesc(b0 + q * 256, kLBO, kSBO),
+                             q > 0 ? 1u : 0u);
                 mma_commit(&mbar);
             }
             const bool done = mbar_wait(&mbar, phase);
@@ -607,13 +642,12 @@ __global__ void __launch_bounds__(kInferThreads, 1) k_closure(Geo<R> g, InferW w
                 ok = false;
                 break;
             }
-            const long p = m0 + rl;
             const bool last = l == SF_MLP_LAYERS - 1;
-            bool apply = false;
-            if (last && p < s2) {
-                apply = column_((int)(p % g.I), (int)(p / g.I), g.I, g.J) &&
-                        !(sflag[0][rl] | sflag[1][rl]);
-            }
+            if (last && tid == 0 && t + gridDim.x < ntiles)   // the products have read sA
+                bulk_load(sA, Xt + (t + gridDim.x) * kTile * kTile, kTile * kTile * 2, &xbar);
+            const long p = m0 + rl;
+            const bool apply = last && p < s2 &&
+                               column_((int)(p % g.I), (int)(p / g.I), g.I, g.J) && !fallback[p];
             for (int c = 0; c < 2; ++c) {
                 float vv[32];
                 tmem_ld32(tmem + trow + cb + c * 32, vv);
@@ -632,15 +666,10 @@ __global__ void __launch_bounds__(kInferThreads, 1) k_closure(Geo<R> g, InferW w
             }
             fence_before();
         }
-        if (ok && tid < kTile && m0 + tid < s2) {
-            const long p = m0 + tid;
-            const bool fb = column_((int)(p % g.I), (int)(p / g.I), g.I, g.J) &&
-                            (sflag[0][tid] | sflag[1][tid]);
-            fallback[p] = fb ? 1 : 0;
-            if (fb && flist) flist[atomicAdd(fcount, 1)] = (int)p;
-        }
     }
     if (!ok && tid == 0) atomicExch(err, 1);
+    // an operand copy still in flight (only after a failed wait) is waited for, with a bound
+    if (!ok && tid == 0) (void)mbar_wait(&xbar, xphase);
     fence_before();
     __syncthreads();
     if (warp == 0) tmem_dealloc(tmem);
@@ -840,16 +869,27 @@ int sf_closure_step(sf_ctx *c, const sf_mlp_params *w, const void *u, const void
         iw.W[l] = static_cast<const __nv_bfloat16 *>(w->W[l]);
         iw.b[l] = w->b[l];
     }
+    const long tiles = (c->s2 + kTile - 1) / kTile;
+    const size_t xbytes = (size_t)tiles * kTile * kTile * sizeof(__nv_bfloat16);
+    cudaError_t e;
+    if (c->closure_x_bytes < xbytes) {   // context-owned scratch: the feature-row tiles
+        if (c->closure_x) cudaFree(c->closure_x);
+        c->closure_x = nullptr;
+        c->closure_x_bytes = 0;
+        e = cudaMalloc(&c->closure_x, xbytes);
+        if (e != cudaSuccess) return mfail(SF_ENOMEM, "sf_closure_step: feature tiles");
+        c->closure_x_bytes = xbytes;
+    }
     static bool attr_set[2][64] = {};
     int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
+    e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return mcuda(e, "sf_closure_step");
     const int pi = c->prec == SF_FP64 ? 1 : 0;
     if (dev >= 0 && dev < 64 && !attr_set[pi][dev]) {
-        e = pi ? cudaFuncSetAttribute(sf::mlp::k_closure<double>,
+        e = pi ? cudaFuncSetAttribute(sf::mlp::k_closure_mlp<double>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)sf::mlp::kInferSmem)
-               : cudaFuncSetAttribute(sf::mlp::k_closure<float>,
+               : cudaFuncSetAttribute(sf::mlp::k_closure_mlp<float>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)sf::mlp::kInferSmem);
         if (e != cudaSuccess) return mcuda(e, "cudaFuncSetAttribute");
@@ -857,22 +897,29 @@ int sf_closure_step(sf_ctx *c, const sf_mlp_params *w, const void *u, const void
     }
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const long tiles = (c->s2 + kTile - 1) / kTile;
     const unsigned grid = (unsigned)(tiles < sms ? tiles : sms);
     if (fallback_count) {
         e = cudaMemsetAsync(fallback_count, 0, sizeof(int), S(s));
         if (e != cudaSuccess) return mcuda(e, "sf_closure_step");
     }
+    auto *X = static_cast<__nv_bfloat16 *>(c->closure_x);
+    const long nrows = tiles * kTile;
     if (pi) {
-        sf::mlp::k_closure<double><<<grid, sf::mlp::kInferThreads, sf::mlp::kInferSmem, S(s)>>>(
-            sf::Ops<double>::geo(c), iw, (const double *)u, (const double *)v, (const double *)z_r,
-            (const double *)bvf, (const double *)sustr, (const double *)svstr, nfeat, lo, hi,
-            fallback, fallback_list, fallback_count, (double *)Akv, (double *)Akt, err);
+        auto g = sf::Ops<double>::geo(c);
+        sf::mlp::k_closure_rows<double><<<nblk(nrows, 128), 128, 0, S(s)>>>(
+            g, (const double *)u, (const double *)v, (const double *)z_r, (const double *)bvf,
+            (const double *)sustr, (const double *)svstr, nfeat, lo, hi, fallback, fallback_list,
+            fallback_count, X, nrows);
+        sf::mlp::k_closure_mlp<double><<<grid, sf::mlp::kInferThreads, sf::mlp::kInferSmem, S(s)>>>(
+            g, iw, X, tiles, fallback, (double *)Akv, (double *)Akt, err);
     } else {
-        sf::mlp::k_closure<float><<<grid, sf::mlp::kInferThreads, sf::mlp::kInferSmem, S(s)>>>(
-            sf::Ops<float>::geo(c), iw, (const float *)u, (const float *)v, (const float *)z_r,
-            (const float *)bvf, (const float *)sustr, (const float *)svstr, nfeat, lo, hi,
-            fallback, fallback_list, fallback_count, (float *)Akv, (float *)Akt, err);
+        auto g = sf::Ops<float>::geo(c);
+        sf::mlp::k_closure_rows<float><<<nblk(nrows, 128), 128, 0, S(s)>>>(
+            g, (const float *)u, (const float *)v, (const float *)z_r, (const float *)bvf,
+            (const float *)sustr, (const float *)svstr, nfeat, lo, hi, fallback, fallback_list,
+            fallback_count, X, nrows);
+        sf::mlp::k_closure_mlp<float><<<grid, sf::mlp::kInferThreads, sf::mlp::kInferSmem, S(s)>>>(
+            g, iw, X, tiles, fallback, (float *)Akv, (float *)Akt, err);
     }
     e = cudaGetLastError();
     return e == cudaSuccess ? SF_OK : mcuda(e, "sf_closure_step");
