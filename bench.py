@@ -301,6 +301,153 @@ def closure_error(m, steps=300):
             "gls_spinup_iterations": steps}
 
 
+def max_over_ranks(ms, world, device):
+    """The slowest rank's time: replicas and ensemble shards run without any collective on
+    the data path; only this timing reduction crosses ranks."""
+    if world <= 1:
+        return ms
+    import torch
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def run_ensemble(args, rank, world):
+    """Config 2: 256 basins of uneven size (seeded), FP32 with FP64 accumulators, stepped
+    together by the pooled, block-mapped kernels; the barotropic loop replays as one CUDA graph
+    and the 3D right-hand side's tile shape is autotuned."""
+    import torch
+    from sailfish_b200 import autotune, ensemble
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    # weak scaling: args.members per GPU, rank r taking members r, r + world, ... of the
+    # world * args.members drawn from the seed
+    members = ensemble.ensemble_members(seed=args.seed, n=args.members * world)[rank::world]
+    m = ensemble.make(members, precision=args.precision)
+    stream = torch.cuda.current_stream()
+    m.step(1)
+    tune = autotune.tune_rhs3d(m, reps=3)
+    phases = {}
+
+    def hook(name):
+        ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+        phases.setdefault(name, []).append(ev)
+        return ev
+
+    m.step(max(args.warmup - 1, 0))
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(torch.cuda.current_device()) as clk:
+        start.record(stream)
+        m.step(args.steps, timer=hook)
+        stop.record(stream)
+        torch.cuda.synchronize()
+    ms = max_over_ranks(start.elapsed_time(stop), world, dev)
+    if world > 1:
+        torch.distributed.barrier()
+    per_phase = {k: float(np.mean([a.elapsed_time(b) for a, b in v])) for k, v in phases.items()}
+    grids = m.members_grids
+    esize = 4 if args.precision == "fp32" else 8
+    ab = {}
+    for g in grids:
+        for k, v in algorithmic_bytes(g, esize).items():
+            if k != "closure":
+                ab[k] = ab.get(k, 0) + v
+    dom = max((k for k in per_phase if k in ab), key=lambda k: per_phase[k])
+    peak, kind = peaks()
+    achieved = ab[dom] / (per_phase[dom] * 1e-3) / 1e9
+    cells = m.cells
+    all_cells = cells
+    if world > 1:   # every rank's own members (host-side count, no data on the path)
+        all_cells = sum((g.L - 1) * (g.M - 1) * g.N for g, _, _ in
+                        ensemble.ensemble_members(seed=args.seed, n=args.members * world))
+    # end to end: u, v pools in from pinned host memory, the zeta pool out, every step
+    hu = torch.empty_like(m.u, device="cpu").pin_memory()
+    hv = torch.empty_like(m.v, device="cpu").pin_memory()
+    hz = torch.empty_like(m.zeta[0], device="cpu").pin_memory()
+    hu.copy_(m.u)
+    hv.copy_(m.v)
+    e_steps = max(1, min(args.steps, 3))
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e_steps):
+        m.u.copy_(hu, non_blocking=True)
+        m.v.copy_(hv, non_blocking=True)
+        m.step(1)
+        hz.copy_(m._slot("zeta", 2), non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e_ms = e0.elapsed_time(e1) / e_steps
+    per_step = 4 + 7 * (m.nfast + 1) + 1
+    out = {
+        "metric": METRIC, "value": all_cells * args.steps / (ms * 1e-3), "unit": "cell-steps/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32" if args.precision == "fp32" else "f64",
+        "data": "synthetic",
+        "config": {"workload": "ensemble%d" % args.members, "members": args.members,
+                   "seed": args.seed, "cells": cells,
+                   "Lm": [g.L - 1 for g in grids][:8] + ["..."],
+                   "N": {"16": sum(g.N == 16 for g in grids), "32": sum(g.N == 32 for g in grids)},
+                   "dt": m.dt, "ndtfast": m.ndtfast, "barotropic_substeps": m.nfast + 1,
+                   "semantics": "reference main3d per member",
+                   "initial_state": "Gaussian surface bump per member (seeded), closed walls",
+                   "vertical_mixing": "AKv constant (the reference's step)",
+                   "l2": "inputs larger than L2 (3D pools %.2f GB each)" % (m.u.numel() * esize / 1e9),
+                   "parallelism": "replicas" if world > 1 else "single",
+                   "rhs3d_tile_autotune_ms": {str(autotune.TILES[k]): v for k, v in tune.items()},
+                   "rhs3d_tile": str(autotune.TILES[m.rhs_tile])},
+        "phases_ms": per_phase,
+        "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "peak_kind": kind,
+                     "algorithmic_bytes": ab[dom], "traffic": None},
+        "e2e": {"value": cells / (e_ms * 1e-3), "unit": "cell-steps/s",
+                "h2d_bytes_per_step": (hu.numel() + hv.numel()) * hu.element_size(),
+                "d2h_bytes_per_step": hz.numel() * hz.element_size()},
+        "gpu_launches": args.steps * per_step + 1,
+        "clocks": clk.summary(),
+    }
+    del m
+    torch.cuda.empty_cache()
+    if not args.no_error and rank == 0:
+        out["error_vs_fp64"] = ensemble_error(members)
+    return out
+
+
+def ensemble_error(members):
+    """One step of every member from its bump, FP32 form against FP64 from identical inputs:
+    per-member RMS differences of zeta, u, v; members whose FP64 step is not finite (the
+    reference's semantics on non-square grids) are counted and left out."""
+    import torch
+    from sailfish_b200 import ensemble
+    res = {}
+    for prec in ("fp64", "fp32"):
+        m = ensemble.make(members, precision=prec)
+        m.step(1)
+        torch.cuda.synchronize()
+        res[prec] = [{k: m.member(k, i).double().cpu().numpy() for k in ("zeta", "u", "v")}
+                     for i in range(len(members))]
+        del m
+        torch.cuda.empty_cache()
+    rms = {"zeta": [], "u": [], "v": []}
+    finite = 0
+    for a, b in zip(res["fp64"], res["fp32"]):
+        if not all(np.isfinite(a[k]).all() for k in a):
+            continue
+        finite += 1
+        for k in rms:
+            d = b[k] - a[k]
+            rms[k].append(float(np.sqrt(np.mean(d * d))))
+    out = {"case": "1 step from each member's bump", "members_finite": finite,
+           "members": len(members)}
+    for k, v in rms.items():
+        out[k] = {"rms_max": max(v) if v else None, "rms_median": float(np.median(v)) if v else None}
+    return out
+
+
 def run_ours(args, rank, world):
     import torch
     from sailfish_b200 import configs
@@ -333,11 +480,8 @@ def run_ours(args, rank, world):
         m.step(args.steps, timer=hook)
         stop.record(stream)
         torch.cuda.synchronize()
-    ms = start.elapsed_time(stop)
+    ms = max_over_ranks(start.elapsed_time(stop), world, dev)
     if world > 1:
-        t = torch.tensor([ms], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
         torch.distributed.barrier()
     per_phase = {k: float(np.mean([a.elapsed_time(b) for a, b in v])) for k, v in phases.items()}
 
@@ -417,6 +561,8 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=40)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 timing")
+    ap.add_argument("--members", type=int, default=256, help="ensemble members (config ensemble)")
+    ap.add_argument("--seed", type=int, default=0, help="ensemble seed (config ensemble)")
     ap.add_argument("--closure", choices=["mlp", "gls", "none"], default=None,
                     help="vertical mixing in the step (default: mlp for fp32, gls for fp64)")
     ap.add_argument("--no-error", action="store_true", help="skip the FP32-vs-FP64 error case")
@@ -447,6 +593,13 @@ def main():
     if world > 1:
         torch.distributed.init_process_group(
             "nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    if args.config == "ensemble":
+        out = run_ensemble(args, rank, world)
+        if rank == 0:
+            print(json.dumps(out))
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return
     out = run_ours(args, rank, world)
     if rank == 0:
         if args.precision == "fp32" and not args.no_fp64:

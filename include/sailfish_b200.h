@@ -89,6 +89,23 @@ typedef struct sf_state2d {
  * Boundary.__init__ (modules/mod_boundary.py:237-297).  It uses the current CUDA device. */
 int sf_ctx_create(const sf_grid_desc *desc, sf_ctx **out);
 int sf_ctx_destroy(sf_ctx *ctx);
+/* An ensemble context: n independent grids (members) of possibly different sizes and N,
+ * stepped together.  Their fields live in shared pools, member after member (layout from
+ * sf_ctx_member_layout); the time-step entry points (sf_maxflux_omega, sf_rhs3d,
+ * sf_barotropic_loop and its parts, sf_set_depth, sf_step3d_uv(_bc), sf_omega) then take the
+ * pool pointers and run every member in each launch (each block finds its member from a block
+ * map).  The reference runs one grid per process; this is config 2's fused ensemble.  All
+ * members share the precision; nothing else needs to match. */
+int sf_ctx_create_ensemble(const sf_grid_desc *descs, int n, sf_ctx **out);
+/* Tile shape of the tiled 3D right-hand side (sf_rhs3d) for this context: 0 = 32 x 8 rho points
+ * (default), 1 = 32 x 4, 2 = 64 x 4.  Results do not
+ * depend on it; the autotuner (sailfish_b200.autotune) times the variants and picks one. */
+int sf_ctx_set_tile(sf_ctx *ctx, int variant);
+/* Number of members (1 for sf_ctx_create). */
+int sf_ctx_members(const sf_ctx *ctx);
+/* Offsets (elements) of each member in the pools of 2D fields, of N+1-level fields and of
+ * N-level fields, and the pool sizes totals[0..2]; any pointer may be NULL. */
+int sf_ctx_member_layout(const sf_ctx *ctx, long *off2, long *off3, long *offN, long *totals);
 const char *sf_last_error(void);
 int sf_version(void);
 int sf_ctx_precision(const sf_ctx *ctx);

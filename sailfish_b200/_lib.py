@@ -83,6 +83,10 @@ SIGNATURES = {
     "sf_gls_predictor": [_vp, _d, _i] + [_vp] * 13 + [_vp],
     "sf_obc_volcons": [_vp, _vp, _vp, _vp, _i, _i, _vp, _vp],
     "sf_ctx_set_graphs": [_vp, _i],
+    "sf_ctx_create_ensemble": [ctypes.POINTER(GridDesc), _i, ctypes.POINTER(_vp)],
+    "sf_ctx_members": [_vp],
+    "sf_ctx_set_tile": [_vp, _i],
+    "sf_ctx_member_layout": [_vp, _vp, _vp, _vp, _vp],
     "sf_mlp_last_error": [],
     "sf_mlp_gemm": [_i, _i, _vp, _i, ctypes.c_long, ctypes.c_long, _vp, _i, ctypes.c_long,
                     ctypes.c_long, _vp, _i, _vp, ctypes.c_long, _vp, ctypes.c_long, _vp, _vp],

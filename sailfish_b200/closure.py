@@ -83,10 +83,16 @@ class Columns:
         self.Akp.fill_(P.Akp_bak)
 
     def stratify(self, zscale, dT=20.0):
-        """N^2 of T = 4 + dT exp(z/zscale) with the linear EOS, from the model's z_w."""
+        """N^2 of T = 4 + dT exp(z/zscale) with the linear EOS, from the model's z_w.  zscale is
+        a number, or a (J, I) array of scales varying across the basin."""
         m = self.m
-        check(lib.sf_analytic_bvf(m.ctx.ptr, _p(m.z_w), dT, zscale, ALPHA, G, _p(self.bvf),
-                                  stream_handle()), "sf_analytic_bvf")
+        if np.ndim(zscale) == 0:
+            check(lib.sf_analytic_bvf(m.ctx.ptr, _p(m.z_w), dT, float(zscale), ALPHA, G,
+                                      _p(self.bvf), stream_handle()), "sf_analytic_bvf")
+            return
+        zs = torch.as_tensor(np.asarray(zscale, np.float64), device=self.bvf.device)
+        zw = m.z_w.double()
+        self.bvf.copy_((G * ALPHA * (dT / zs) * torch.exp(zw / zs)).to(self.bvf.dtype))
 
     def gls_step(self, columns=None):
         m = self.m
@@ -183,11 +189,13 @@ def mixing_for(model, mode, net=None, tau0=0.15, zscale=500.0):
 
 
 def generate(config="basin1", runs=4, spin=30, keep=4, every=5, seed=0, precision="fp32",
-             tau_range=(0.0, 0.3), zscale_range=(200.0, 1000.0), rest_runs=0, pattern=False):
+             tau_range=(0.0, 0.3), zscale_range=(200.0, 1000.0), rest_runs=0, pattern=False,
+             spread=False):
     """Training snapshots from plain GLS runs on `config`'s grid: each run draws a wind stress
     and a stratification scale, spins GLS up for `spin` steps at fixed forcing and then keeps
     `keep` snapshots `every` steps apart.  The last `rest_runs` of the runs have no current
-    (an ocean at rest under the wind); with `pattern` the wind varies as cos(pi y / Ly).  Returns (X, T) on the device: feature rows and target
+    (an ocean at rest under the wind); with `pattern` the wind varies as cos(pi y / Ly), and
+    with `spread` the stratification scale varies across xi over all of zscale_range.  Returns (X, T) on the device: feature rows and target
     rows (log10 Akv / Akt) of the rho-interior columns."""
     cfg = configs.CONFIGS[config]() if isinstance(config, str) else config
     g = cfg["grid"]
@@ -203,8 +211,15 @@ def generate(config="basin1", runs=4, spin=30, keep=4, every=5, seed=0, precisio
     for r in range(runs):
         cols = Columns(model)
         tau = float(rng.uniform(*tau_range))
-        zscale = float(rng.uniform(*zscale_range))
         angle = float(rng.uniform(0.0, 2.0 * math.pi))
+        if spread:   # the stratification scale varies linearly across xi over the whole range
+            lo, hi = zscale_range
+            ramp = np.linspace(0.0, 1.0, g.I)[None, :] * np.ones((g.J, 1))
+            if rng.random() < 0.5:
+                ramp = 1.0 - ramp
+            zscale = lo + (hi - lo) * ramp
+        else:
+            zscale = float(rng.uniform(*zscale_range))
         wind_driven_state(model, cols, tau, angle, zscale, rng, current=r < runs - rest_runs,
                           pattern=pattern)
         model.AKv.fill_(cols.P.Akv_bak)

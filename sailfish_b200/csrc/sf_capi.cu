@@ -99,7 +99,25 @@ int resolve(const std::vector<BcOp> &ops, long s2, std::vector<int> &dst, std::v
     return SF_OK;
 }
 
-int make_program(sf::BcProgram &p, const std::vector<BcOp> &ops, long s2) {
+// A boundary program on the host: independent entries (di <- si), chained entries (dc <- sc)
+// in groups [gofs[g], gofs[g+1]).
+struct ProgHost {
+    std::vector<int> di, si, dc, sc, gofs;
+};
+
+int upload_program(sf::BcProgram &p, const ProgHost &h) {
+    p.n = (int)h.di.size();
+    p.nch = (int)h.dc.size();
+    p.ngr = h.gofs.empty() ? 0 : (int)h.gofs.size() - 1;
+    int rc = upload(&p.dst, h.di.data(), h.di.size(), "boundary program");
+    if (!rc) rc = upload(&p.src, h.si.data(), h.si.size(), "boundary program");
+    if (!rc) rc = upload(&p.dst_ch, h.dc.data(), h.dc.size(), "boundary program");
+    if (!rc) rc = upload(&p.src_ch, h.sc.data(), h.sc.size(), "boundary program");
+    if (!rc && p.ngr > 0) rc = upload(&p.gofs, h.gofs.data(), h.gofs.size(), "boundary program");
+    return rc;
+}
+
+int build_program(ProgHost &out, const std::vector<BcOp> &ops, long s2) {
     std::vector<int> d, s;
     int rc = resolve(ops, s2, d, s);
     if (rc) return rc;
@@ -125,13 +143,35 @@ int make_program(sf::BcProgram &p, const std::vector<BcOp> &ops, long s2) {
     }
     if ((int)dc.size() > sf::kMaxChained)
         return fail(SF_EUNSUPPORTED, "boundary lists with more than 32 chained entries");
-    p.n = (int)di.size();
-    p.nch = (int)dc.size();
-    rc = upload(&p.dst, di.data(), di.size(), "boundary program");
-    if (!rc) rc = upload(&p.src, si.data(), si.size(), "boundary program");
-    if (!rc) rc = upload(&p.dst_ch, dc.data(), dc.size(), "boundary program");
-    if (!rc) rc = upload(&p.src_ch, sc.data(), sc.size(), "boundary program");
-    return rc;
+    out.di = std::move(di);
+    out.si = std::move(si);
+    out.dc = std::move(dc);
+    out.sc = std::move(sc);
+    out.gofs.clear();
+    if (!out.dc.empty()) out.gofs = {0, (int)out.dc.size()};
+    return SF_OK;
+}
+
+int make_program(sf::BcProgram &p, const std::vector<BcOp> &ops, long s2) {
+    ProgHost h;
+    const int rc = build_program(h, ops, s2);
+    return rc ? rc : upload_program(p, h);
+}
+
+// Appends a member's program to an ensemble's, its node indices offset into the pools.
+void append_program(ProgHost &all, const ProgHost &m, long off) {
+    auto sh = [&](int v) { return v >= 0 ? (int)(v + off) : v; };
+    for (size_t k = 0; k < m.di.size(); ++k) {
+        all.di.push_back(sh(m.di[k]));
+        all.si.push_back(sh(m.si[k]));
+    }
+    if (m.dc.empty()) return;
+    if (all.gofs.empty()) all.gofs.push_back(0);
+    for (size_t k = 0; k < m.dc.size(); ++k) {
+        all.dc.push_back(sh(m.dc[k]));
+        all.sc.push_back(sh(m.sc[k]));
+    }
+    all.gofs.push_back((int)all.dc.size());
 }
 
 void free_ctx(sf_ctx *c) {
@@ -152,7 +192,16 @@ void free_ctx(sf_ctx *c) {
         cudaFree(p->src);
         cudaFree(p->dst_ch);
         cudaFree(p->src_ch);
+        cudaFree(p->gofs);
     }
+    cudaFree(c->members);
+    cudaFree(c->bm_pt);
+    cudaFree(c->bm_128);
+    for (int2 *b : c->bm_tile) cudaFree(b);
+    cudaFree(c->bm_pipe);
+    delete[] c->h_off2;
+    delete[] c->h_off3;
+    delete[] c->h_offN;
     delete c;
 }
 
@@ -181,6 +230,246 @@ int sf_version(void) { return 1; }
 const char *sf_last_error(void) { return g_err.c_str(); }
 
 int sf_ctx_precision(const sf_ctx *ctx) { return ctx ? ctx->prec : SF_EINVAL; }
+
+}  // extern "C"
+
+namespace {
+int validate_desc(const sf_grid_desc *d) {
+    if (d->precision != SF_FP64 && d->precision != SF_FP32)
+        return fail(SF_EDTYPE, "precision must be SF_FP64 or SF_FP32");
+    if (d->L < 4 || d->M < 4) return fail(SF_EINVAL, "grid too small (need L, M >= 4)");
+    if (d->N < 5 || d->N > 64)
+        return fail(SF_EINVAL, "N must be in [5, 64]: the reference's verticalAdvection reads "
+                               "levels up to 5 (rhs_kernels.cpp:172) and columns are held per thread");
+    if (d->Vtransform != 1 && d->Vtransform != 2) return fail(SF_EINVAL, "Vtransform must be 1 or 2");
+    if (!d->h || !d->pm || !d->pn || !d->on_u || !d->om_v || !d->fomn)
+        return fail(SF_EINVAL, "missing metric arrays");
+    if (!d->sc_r || !d->sc_w || !d->Cs_r || !d->Cs_w) return fail(SF_EINVAL, "missing S-coordinate tables");
+    if (!d->zeta_field_idx2 || !d->uvel_field_type || !d->vvel_field_type)
+        return fail(SF_EINVAL, "missing boundary maps");
+    const long s2 = (long)(d->L + 1) * (d->M + 1);
+    for (long k = 0; k < s2; ++k)
+        if (d->vvel_field_type[k] > 0 && (d->vvel_field_type[k] & (1 << 4)) == 0 &&
+            (d->vvel_field_type[k] & (1 << 3)) == 0 && (d->vvel_field_type[k] & (1 << 6)) != 0)
+            return fail(SF_EUNSUPPORTED, "gradient 3D v boundary: the reference reads past the "
+                                         "boundary map (step3D_uv.kernels.cpp:363)");
+    if (d->n_vbar_grad > d->n_ubar_grad)
+        return fail(SF_EUNSUPPORTED, "vbar gradient list longer than the ubar list the reference "
+                                     "copies it from (barotropicVelocityBC.py:30-31)");
+    return SF_OK;
+}
+
+// The three boundary programs of one grid, on the host.
+int build_programs(const sf_grid_desc *d, long s2, ProgHost &z, ProgHost &u, ProgHost &v) {
+    int rc = build_program(z, {{d->zeta_copy_idx1, d->zeta_copy_idx2, d->n_zeta_copy, 0}}, s2);
+    if (!rc)
+        rc = build_program(u,
+                           {{d->ubar_closed_idx, nullptr, d->n_ubar_closed, -1},
+                            {d->ubar_clamped_idx, nullptr, d->n_ubar_clamped, -2},
+                            {d->ubar_grad_idx1, d->ubar_grad_idx2, d->n_ubar_grad, 0}},
+                           s2);
+    if (!rc)
+        rc = build_program(v,
+                           {{d->vbar_closed_idx, nullptr, d->n_vbar_closed, -1},
+                            {d->vbar_grad_idx1, d->ubar_grad_idx2, d->n_vbar_grad, 0}},
+                           s2);
+    return rc;
+}
+
+template <typename R>
+int upload_members(sf_ctx *c, const sf_grid_desc *d, int n, const std::vector<long> &off2,
+                   const std::vector<long> &off3, const std::vector<long> &offN,
+                   const std::vector<long> &voff) {
+    std::vector<sf::Member<R>> mt(n);
+    for (int m = 0; m < n; ++m) {
+        sf::Geo<R> &g = mt[m].g;
+        g.I = d[m].L + 1;
+        g.J = d[m].M + 1;
+        g.N = d[m].N;
+        g.s2 = (long)g.I * g.J;
+        const R *const *mp = reinterpret_cast<const R *const *>(c->metrics);
+        g.h = mp[0] + off2[m];
+        g.pm = mp[1] + off2[m];
+        g.pn = mp[2] + off2[m];
+        g.on_u = mp[3] + off2[m];
+        g.om_v = mp[4] + off2[m];
+        g.fomn = mp[5] + off2[m];
+        g.hd = c->hd + off2[m];
+        g.sc_r = c->vert + voff[m];
+        g.sc_w = g.sc_r + g.N;
+        g.Cs_r = g.sc_w + g.N + 1;
+        g.Cs_w = g.Cs_r + g.N;
+        g.hc = d[m].hc;
+        g.Vtransform = d[m].Vtransform;
+        g.bcfield = c->bcfield + off2[m];
+        g.utype = c->utype + off2[m];
+        g.vtype = c->vtype + off2[m];
+        g.ref_threads = 512L * (g.s2 / 512 + 1);
+        mt[m].off2 = off2[m];
+        mt[m].off3 = off3[m];
+        mt[m].offN = offN[m];
+        for (int v = 0; v < sf::kRhsTiles; ++v)
+            mt[m].ntx[v] = (g.I + sf::kRhsTileX[v] - 1) / sf::kRhsTileX[v];
+    }
+    return upload(reinterpret_cast<sf::Member<R> **>(&c->members), mt.data(), mt.size(), "members");
+}
+}  // namespace
+
+extern "C" {
+
+int sf_ctx_create_ensemble(const sf_grid_desc *d, int n, sf_ctx **out) {
+    if (!d || !out || n < 1) return fail(SF_EINVAL, "null argument");
+    *out = nullptr;
+    for (int m = 0; m < n; ++m) {
+        if (d[m].precision != d[0].precision) return fail(SF_EDTYPE, "members differ in precision");
+        if (const int rc = validate_desc(&d[m])) return rc;
+    }
+    sf_ctx *c = new (std::nothrow) sf_ctx();
+    if (!c) return fail(SF_ENOMEM, "host allocation");
+    c->prec = d[0].precision;
+    c->nmem = n;
+    cudaGetDevice(&c->device);
+    // pool layout: members one after another, each region padded to 32 elements
+    auto pad = [](long x) { return (x + 31) / 32 * 32; };
+    std::vector<long> off2(n), off3(n), offN(n), voff(n);
+    long t2 = 0, t3 = 0, tN = 0, tv = 0;
+    for (int m = 0; m < n; ++m) {
+        const long s2 = (long)(d[m].L + 1) * (d[m].M + 1);
+        off2[m] = t2;
+        off3[m] = t3;
+        offN[m] = tN;
+        voff[m] = tv;
+        t2 += pad(s2);
+        t3 += pad((d[m].N + 1) * s2);
+        tN += pad(d[m].N * s2);
+        tv += 4 * d[m].N + 2;
+        if (d[m].N > c->maxN) c->maxN = d[m].N;
+    }
+    c->tot2 = t2;
+    c->tot3 = t3;
+    c->totN = tN;
+    c->s2 = t2;            // pool-wide operations (accumulator clears) cover every member
+    c->N = c->maxN;
+    c->I = c->J = 0;
+    c->L = c->M = 0;
+    c->h_off2 = new long[n];
+    c->h_off3 = new long[n];
+    c->h_offN = new long[n];
+    for (int m = 0; m < n; ++m) {
+        c->h_off2[m] = off2[m];
+        c->h_off3[m] = off3[m];
+        c->h_offN[m] = offN[m];
+    }
+    int rc = SF_OK;
+    {   // metric pools
+        const char *mn[6] = {"h", "pm", "pn", "on_u", "om_v", "fomn"};
+        for (int k = 0; k < 6 && rc == SF_OK; ++k) {
+            std::vector<double> pool(t2, 0.0);
+            for (int m = 0; m < n; ++m) {
+                const double *src[6] = {d[m].h, d[m].pm, d[m].pn, d[m].on_u, d[m].om_v, d[m].fomn};
+                const long s2 = (long)(d[m].L + 1) * (d[m].M + 1);
+                std::copy(src[k], src[k] + s2, pool.begin() + off2[m]);
+            }
+            rc = upload_real(c, &c->metrics[k], pool.data(), (size_t)t2, mn[k]);
+            if (k == 0 && rc == SF_OK) rc = upload(&c->hd, pool.data(), (size_t)t2, "h");
+        }
+    }
+    if (rc == SF_OK) {
+        std::vector<double> v;
+        for (int m = 0; m < n; ++m) {
+            const int N = d[m].N;
+            v.insert(v.end(), d[m].sc_r, d[m].sc_r + N);
+            v.insert(v.end(), d[m].sc_w, d[m].sc_w + N + 1);
+            v.insert(v.end(), d[m].Cs_r, d[m].Cs_r + N);
+            v.insert(v.end(), d[m].Cs_w, d[m].Cs_w + N + 1);
+        }
+        rc = upload(&c->vert, v.data(), v.size(), "S-coordinate tables");
+    }
+    if (rc == SF_OK) {
+        std::vector<int> bf(t2, 0), ut(t2, 0), vt(t2, 0);
+        for (int m = 0; m < n; ++m) {
+            const long s2 = (long)(d[m].L + 1) * (d[m].M + 1);
+            std::copy(d[m].zeta_field_idx2, d[m].zeta_field_idx2 + s2, bf.begin() + off2[m]);
+            std::copy(d[m].uvel_field_type, d[m].uvel_field_type + s2, ut.begin() + off2[m]);
+            std::copy(d[m].vvel_field_type, d[m].vvel_field_type + s2, vt.begin() + off2[m]);
+        }
+        rc = upload(&c->bcfield, bf.data(), bf.size(), "zeta_field_idx2");
+        if (rc == SF_OK) rc = upload(&c->utype, ut.data(), ut.size(), "uvel_field_type");
+        if (rc == SF_OK) rc = upload(&c->vtype, vt.data(), vt.size(), "vvel_field_type");
+    }
+    if (rc == SF_OK) {
+        ProgHost Z, U, V;
+        for (int m = 0; m < n && rc == SF_OK; ++m) {
+            ProgHost z, u, v;
+            const long s2 = (long)(d[m].L + 1) * (d[m].M + 1);
+            rc = build_programs(&d[m], s2, z, u, v);
+            append_program(Z, z, off2[m]);
+            append_program(U, u, off2[m]);
+            append_program(V, v, off2[m]);
+        }
+        if (rc == SF_OK) rc = upload_program(c->zbc, Z);
+        if (rc == SF_OK) rc = upload_program(c->ubc, U);
+        if (rc == SF_OK) rc = upload_program(c->vbc, V);
+    }
+    if (rc == SF_OK)
+        rc = c->prec == SF_FP64 ? upload_members<double>(c, d, n, off2, off3, offN, voff)
+                                : upload_members<float>(c, d, n, off2, off3, offN, voff);
+    if (rc == SF_OK) {   // block maps
+        std::vector<int2> pt, b128, pipe, tile[sf::kRhsTiles];
+        for (int m = 0; m < n; ++m) {
+            const int I = d[m].L + 1, J = d[m].M + 1;
+            const long s2 = (long)I * J;
+            for (long b = 0; b < (s2 + sf::kPointBlock - 1) / sf::kPointBlock; ++b) pt.push_back({m, (int)b});
+            for (long b = 0; b < (s2 + 127) / 128; ++b) b128.push_back({m, (int)b});
+            for (int v = 0; v < sf::kRhsTiles; ++v) {
+                const int ntx = (I + sf::kRhsTileX[v] - 1) / sf::kRhsTileX[v];
+                const int nty = (J + sf::kRhsTileY[v] - 1) / sf::kRhsTileY[v];
+                for (int b = 0; b < ntx * nty; ++b) tile[v].push_back({m, b});
+            }
+            for (long b = 0; b < (s2 + sf::kPipeTile - 1) / sf::kPipeTile; ++b) pipe.push_back({m, (int)b});
+        }
+        c->nbm_pt = (int)pt.size();
+        c->nbm_128 = (int)b128.size();
+        c->nbm_pipe = (int)pipe.size();
+        rc = upload(&c->bm_pt, pt.data(), pt.size(), "block map");
+        if (rc == SF_OK) rc = upload(&c->bm_128, b128.data(), b128.size(), "block map");
+        if (rc == SF_OK) rc = upload(&c->bm_pipe, pipe.data(), pipe.size(), "block map");
+        for (int v = 0; v < sf::kRhsTiles && rc == SF_OK; ++v) {
+            c->nbm_tile[v] = (int)tile[v].size();
+            rc = upload(&c->bm_tile[v], tile[v].data(), tile[v].size(), "block map");
+        }
+    }
+    if (rc != SF_OK) {
+        free_ctx(c);
+        return rc;
+    }
+    *out = c;
+    return SF_OK;
+}
+
+int sf_ctx_members(const sf_ctx *c) { return c ? c->nmem : 0; }
+
+int sf_ctx_set_tile(sf_ctx *c, int variant) {
+    if (!c) return fail(SF_EINVAL, "null context");
+    if (variant < 0 || variant >= sf::kRhsTiles) return fail(SF_EINVAL, "tile variant is 0, 1 or 2");
+    c->rhs_tile = variant;
+    return SF_OK;
+}
+
+int sf_ctx_member_layout(const sf_ctx *c, long *off2, long *off3, long *offN, long *totals) {
+    if (!c) return fail(SF_EINVAL, "null context");
+    for (int m = 0; m < c->nmem; ++m) {
+        if (off2) off2[m] = c->nmem > 1 ? c->h_off2[m] : 0;
+        if (off3) off3[m] = c->nmem > 1 ? c->h_off3[m] : 0;
+        if (offN) offN[m] = c->nmem > 1 ? c->h_offN[m] : 0;
+    }
+    if (totals) {
+        totals[0] = c->nmem > 1 ? c->tot2 : c->s2;
+        totals[1] = c->nmem > 1 ? c->tot3 : (long)(c->N + 1) * c->s2;
+        totals[2] = c->nmem > 1 ? c->totN : (long)c->N * c->s2;
+    }
+    return SF_OK;
+}
 
 int sf_ctx_create(const sf_grid_desc *d, sf_ctx **out) {
     if (!d || !out) return fail(SF_EINVAL, "null argument");

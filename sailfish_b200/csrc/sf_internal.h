@@ -23,6 +23,8 @@ struct BcProgram {
     int nch = 0;               // chained entries
     int *dst_ch = nullptr;     // device
     int *src_ch = nullptr;     // device
+    int ngr = 0;               // groups of chained entries (one per ensemble member that has
+    int *gofs = nullptr;       // any): group g is [gofs[g], gofs[g+1]), device
 };
 
 // Coefficients of the GLS predictor's half step: cff1, cff2 of the LF/AM3 interpolation and
@@ -44,6 +46,23 @@ struct Geo {
     const int *bcfield;   // zetaBC.bcIdxFieldIdx2
     const int *utype, *vtype;
     long ref_threads;     // threads of the reference's rhs3d launches (rhs_kernels.cpp:86-91)
+};
+
+// Launch geometry shared by the kernels and the host code that builds block maps.
+constexpr int kPointBlock = 256;           // threads per block of the point kernels
+constexpr int kTileX = 32, kTileY = 8;     // tile of the tiled 3D right-hand side
+constexpr int kPipeTile = 64;              // columns per block of the pipelined column solve
+
+// One member of an ensemble context: its grid view (metric pointers into the context's
+// pools) and the offsets of its fields in the state pools: 2D fields (off2), fields of N+1
+// levels (off3) and of N levels (offN); ntx = tiles along xi of the tiled kernels.
+constexpr int kRhsTiles = 3;
+constexpr int kRhsTileX[kRhsTiles] = {32, 32, 64}, kRhsTileY[kRhsTiles] = {8, 4, 4};
+template <typename R>
+struct Member {
+    Geo<R> g;
+    long off2, off3, offN;
+    int ntx[kRhsTiles];   // tiles along xi for each tile variant of the 3D right-hand side
 };
 
 }  // namespace sf
@@ -83,6 +102,23 @@ struct sf_ctx {
     // the learned closure's feature-row tiles (sf_closure_step), allocated on first use
     void *closure_x = nullptr;
     size_t closure_x_bytes = 0;
+    // Ensembles (sf_ctx_create_ensemble): nmem > 1 members whose fields live in shared pools;
+    // the step kernels take the pools and find their member from a block map (member, local
+    // block).  For a single grid nmem = 1 and the kernels take the arrays directly.
+    int nmem = 1;
+    int maxN = 0;
+    void *members = nullptr;     // device sf::Member<R>[nmem]
+    int2 *bm_pt = nullptr;       // blocks of kBlock points
+    int nbm_pt = 0;
+    int2 *bm_128 = nullptr;      // blocks of 128 points
+    int nbm_128 = 0;
+    int2 *bm_tile[sf::kRhsTiles] = {};   // tiles of the tiled 3D right-hand side, per variant
+    int nbm_tile[sf::kRhsTiles] = {};
+    int rhs_tile = 0;            // variant of the tiled 3D right-hand side (sf_ctx_set_tile)
+    int2 *bm_pipe = nullptr;     // 64-point tiles of the pipelined column solve
+    int nbm_pipe = 0;
+    long tot2 = 0, tot3 = 0, totN = 0;   // pool sizes
+    long *h_off2 = nullptr, *h_off3 = nullptr, *h_offN = nullptr;   // host copies
 };
 
 namespace sf {

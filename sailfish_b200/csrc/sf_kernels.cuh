@@ -25,7 +25,7 @@
 
 namespace sf {
 
-constexpr int kBlock = 256;
+constexpr int kBlock = kPointBlock;
 constexpr int kNMax = 64;    // largest N of the column kernels' register/local arrays
 
 __device__ __forceinline__ long tid_flat() { return (long)blockIdx.x * blockDim.x + threadIdx.x; }
@@ -53,12 +53,11 @@ __device__ __forceinline__ R ldz(const R *a, long idx) {   // read, 0 before the
 // computeZetaRHS (mod_cppkernels.cpp:81-128), optionally fused with the leapfrog of
 // computeZetaPred (:134-150, mode 2) or with the corrector's fast-time averages (mode 1).
 template <typename R>
-__global__ void __launch_bounds__(kBlock) k_zeta_rhs(
-    Geo<R> g, const R *__restrict__ zeta, const R *__restrict__ ubar, const R *__restrict__ vbar,
+__device__ __forceinline__ void zeta_rhs_body(
+    const Geo<R> &g, const R *__restrict__ zeta, const R *__restrict__ ubar, const R *__restrict__ vbar,
     R *__restrict__ rzeta, int mode, double cff1, double *__restrict__ Zt,
     double *__restrict__ DU, double *__restrict__ DV, const R *__restrict__ zeta_t0,
-    R *__restrict__ zeta_t2, R Dt) {
-    const long p = tid_flat();
+    R *__restrict__ zeta_t2, R Dt, const long p) {
     if (p >= g.s2) return;
     const long I = g.I;
     const int i = (int)(p % I), j = (int)(p / I);
@@ -111,12 +110,11 @@ __global__ void __launch_bounds__(kBlock) k_zeta_euler(Geo<R> g, R Dt, const R *
 // computeMomentumRHSPred/Corr (mod_cppkernels.cpp:13-77) fused with computeMomentumPred
 // (:156-186), whose guard tests the flat index against szJ, the row count (:162).
 template <typename R>
-__global__ void __launch_bounds__(kBlock) k_momentum(
-    Geo<R> g, R *__restrict__ rhs_u, R *__restrict__ rhs_v, const R *__restrict__ za,
+__device__ __forceinline__ void momentum_body(
+    const Geo<R> &g, R *__restrict__ rhs_u, R *__restrict__ rhs_v, const R *__restrict__ za,
     const R *__restrict__ zb, R grav, R w1, R w, int do_rhs, int do_pred, R Dt,
     const R *__restrict__ u_t1, R *__restrict__ u_t2, const R *__restrict__ v_t1,
-    R *__restrict__ v_t2, const R *__restrict__ z1, const R *__restrict__ z2) {
-    const long p = tid_flat();
+    R *__restrict__ v_t2, const R *__restrict__ z1, const R *__restrict__ z2, const long p) {
     if (p >= g.s2) return;
     const long I = g.I, J = g.J;
     const int i = (int)(p % I), j = (int)(p / I);
@@ -167,11 +165,10 @@ __global__ void __launch_bounds__(kBlock) k_am3(Geo<R> g, R Dt, R *__restrict__ 
 //   ubar_t1 += Dt*(5/12 rubar_t1 + 8/12 rubar_t0 - 1/12 vbar_t1)   (the mis-bound
 //              AdamsMoultonCorr3rd2 of modules/mod_operators.py:146 reads these five args)
 template <typename R>
-__global__ void __launch_bounds__(kBlock) k_corr_point(
-    Geo<R> g, R Dt, R *__restrict__ zeta_t2, const R *__restrict__ rz0, const R *__restrict__ rz1,
+__device__ __forceinline__ void corr_point_body(
+    const Geo<R> &g, R Dt, R *__restrict__ zeta_t2, const R *__restrict__ rz0, const R *__restrict__ rz1,
     const R *__restrict__ rz2, R *__restrict__ ubar_t1, const R *__restrict__ vbar_t1,
-    const R *__restrict__ rub0, const R *__restrict__ rub1, R *__restrict__ vbar_t2) {
-    const long p = tid_flat();
+    const R *__restrict__ rub0, const R *__restrict__ rub1, R *__restrict__ vbar_t2, const long p) {
     if (p >= g.s2) return;
     const R A2 = R(5.0 / 12.0), A1 = R(8.0 / 12.0), A0 = R(-1.0 / 12.0);
     zeta_t2[p] = zeta_t2[p] + Dt * ((A2 * rz2[p] + A1 * rz1[p]) + A0 * rz0[p]);
@@ -180,7 +177,7 @@ __global__ void __launch_bounds__(kBlock) k_corr_point(
 }
 
 // Boundary programs (see BcProgram): independent entries one per thread over as many blocks
-// as needed; the chained entries by thread 0 of block 0, all reads before all writes.
+// as needed; each group of chained entries by one thread, all reads before all writes.
 template <typename R>
 __device__ __forceinline__ R bc_value(const R *f, int s, R val) {
     return s >= 0 ? f[s] : (s == -1 ? R(0) : val);
@@ -197,12 +194,17 @@ __global__ void __launch_bounds__(256) k_bc_apply(BcProgram p1, R *f1, BcProgram
         const long k = t - p1.n;
         f2[p2.dst[k]] = bc_value(f2, p2.src[k], val);
     }
-    if (t == 0) {
-        R buf[kMaxChained];
-        for (int k = 0; k < p1.nch; ++k) buf[k] = bc_value(f1, p1.src_ch[k], val);
-        for (int k = 0; k < p1.nch; ++k) f1[p1.dst_ch[k]] = buf[k];
-        for (int k = 0; k < p2.nch; ++k) buf[k] = bc_value(f2, p2.src_ch[k], val);
-        for (int k = 0; k < p2.nch; ++k) f2[p2.dst_ch[k]] = buf[k];
+    // chained entries: group g (one per member) by thread g, all reads before all writes
+    R buf[kMaxChained];
+    if (t < p1.ngr) {
+        const int a = p1.gofs[t], b = p1.gofs[t + 1];
+        for (int k = a; k < b; ++k) buf[k - a] = bc_value(f1, p1.src_ch[k], val);
+        for (int k = a; k < b; ++k) f1[p1.dst_ch[k]] = buf[k - a];
+    }
+    if (t < p2.ngr) {
+        const int a = p2.gofs[t], b = p2.gofs[t + 1];
+        for (int k = a; k < b; ++k) buf[k - a] = bc_value(f2, p2.src_ch[k], val);
+        for (int k = a; k < b; ++k) f2[p2.dst_ch[k]] = buf[k - a];
     }
 }
 
@@ -216,16 +218,27 @@ __global__ void __launch_bounds__(256) k_bc_apply(BcProgram p1, R *f1, BcProgram
 // with a halo of rows j-3..j+2 and columns i-2..i+2.  The halo is addressed by flat index
 // (j0+r)*I + (i0+c), so columns beyond the row ends wrap into the neighbouring rows exactly as
 // the reference's flat-index stencils do; reads before the array start or past its end stage 0.
-constexpr int kTX = 32, kTY = 8;
+// Tile shapes (TX x TY): 32 x 8 (the default), 32 x 4 and 64 x 4, chosen per context
+// (sf_ctx_set_tile, e.g. by the autotuner); the staged tile adds the halo.
+constexpr int kTX = kTileX, kTY = kTileY;
 constexpr int kHY0 = 3, kHY1 = 2, kHX0 = 2, kHX1 = 2;          // halo extents
-constexpr int kSX = kTX + kHX0 + kHX1, kSY = kTY + kHY0 + kHY1;  // staged tile 36 x 13
-constexpr int kSN = kSX * kSY;
+template <int TX, int TY>
+struct RhsTile {
+    static constexpr int SX = TX + kHX0 + kHX1, SY = TY + kHY0 + kHY1, SN = SX * SY;
+    static constexpr int FX = TX + 1, FN = (TX + 1) * (TY + 1);   // face-flux tile
+};
+// Dynamic shared memory of the tiled right-hand side: two staging buffers of 6 fields and the
+// four face-flux arrays.
+template <typename R, int TX, int TY>
+constexpr size_t rhs_smem_bytes() {
+    return sizeof(R) * ((size_t)2 * 6 * RhsTile<TX, TY>::SN + 4 * (size_t)RhsTile<TX, TY>::FN);
+}
 
-template <typename R>
+template <typename R, int SX>
 struct Tile {
     const R *t;
     int base;   // index of the thread's own node in the staged tile
-    __device__ __forceinline__ R operator()(int dr, int dc) const { return t[base + dr * kSX + dc]; }
+    __device__ __forceinline__ R operator()(int dr, int dc) const { return t[base + dr * SX + dc]; }
 };
 
 // Asynchronous staging (cp.async, completes in the background while the previous level is
@@ -242,28 +255,33 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int n>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(n)); }
 
-template <typename R>
+template <typename R, int TX, int TY>
 __device__ __forceinline__ void stage(R *dst, const R *src, long lvl_off, long len, long I, long j0,
                                       long i0, int tid) {
-    for (int e = tid; e < kSN; e += kTX * kTY) {
-        const int r = e / kSX - kHY0, c = e % kSX - kHX0;
+    using T = RhsTile<TX, TY>;
+    for (int e = tid; e < T::SN; e += TX * TY) {
+        const int r = e / T::SX - kHY0, c = e % T::SX - kHX0;
         const long f = lvl_off + (j0 + r) * I + (i0 + c);
         const bool ok = f >= 0 && f < len;
         cp_async(dst + e, ok ? src + f : src, ok);
     }
 }
 
-template <typename R>
-__global__ void __launch_bounds__(kTX *kTY) k_rhs3d(Geo<R> g, const R *__restrict__ u,
-                                                    const R *__restrict__ v, const R *__restrict__ Huon,
-                                                    const R *__restrict__ Hvom, const R *__restrict__ W,
-                                                    const R *__restrict__ Hz, R *__restrict__ ru,
-                                                    R *__restrict__ rv) {
-    __shared__ R sbuf[2][6][kSN];
-    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kTX + tx;
+template <typename R, int TX, int TY>
+__device__ __forceinline__ void rhs3d_body(const Geo<R> &g, const R *__restrict__ u,
+                                           const R *__restrict__ v, const R *__restrict__ Huon,
+                                           const R *__restrict__ Hvom, const R *__restrict__ W,
+                                           const R *__restrict__ Hz, R *__restrict__ ru,
+                                           R *__restrict__ rv, const int bx, const int by) {
+    using T = RhsTile<TX, TY>;
+    constexpr int kSX = T::SX, kSN = T::SN, kFX = T::FX, kFN = T::FN;
+    extern __shared__ __align__(16) unsigned char rhs_smem[];
+    R(*sbuf)[6][kSN] = reinterpret_cast<R(*)[6][kSN]>(rhs_smem);
+    R *sF = reinterpret_cast<R *>(rhs_smem) + 2 * 6 * kSN;   // [4][kFN] face fluxes
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
     const long I = g.I, s2 = g.s2;
     const int N = g.N;
-    const long i0 = (long)blockIdx.x * kTX, j0 = (long)blockIdx.y * kTY;
+    const long i0 = (long)bx * TX, j0 = (long)by * TY;
     const int i = (int)(i0 + tx), j = (int)(j0 + ty);
     const bool live = i < g.I && j < g.J;
     const long p = (long)j * I + i;
@@ -301,12 +319,12 @@ __global__ void __launch_bounds__(kTX *kTY) k_rhs3d(Geo<R> g, const R *__restric
     auto issue = [&](int K) {
         const long o = (long)K * s2;
         R(*bf)[kSN] = sbuf[K & 1];
-        stage(bf[0], u, o, len3, I, j0, i0, tid);
-        stage(bf[1], v, o, len3, I, j0, i0, tid);
-        stage(bf[2], Huon, o, len3, I, j0, i0, tid);
-        stage(bf[3], Hvom, o, len3, I, j0, i0, tid);
-        stage(bf[4], Hz, o, lenHz, I, j0, i0, tid);
-        stage(bf[5], W, o + s2, len3, I, j0, i0, tid);
+        stage<R, TX, TY>(bf[0], u, o, len3, I, j0, i0, tid);
+        stage<R, TX, TY>(bf[1], v, o, len3, I, j0, i0, tid);
+        stage<R, TX, TY>(bf[2], Huon, o, len3, I, j0, i0, tid);
+        stage<R, TX, TY>(bf[3], Hvom, o, len3, I, j0, i0, tid);
+        stage<R, TX, TY>(bf[4], Hz, o, lenHz, I, j0, i0, tid);
+        stage<R, TX, TY>(bf[5], W, o + s2, len3, I, j0, i0, tid);
         cp_async_commit();
     };
     issue(0);
@@ -320,11 +338,11 @@ __global__ void __launch_bounds__(kTX *kTY) k_rhs3d(Geo<R> g, const R *__restric
         }
         __syncthreads();
         R(*bf)[kSN] = sbuf[K & 1];
-        const Tile<R> U{bf[0], b}, V{bf[1], b}, HU{bf[2], b}, HV{bf[3], b}, HZ{bf[4], b}, WW{bf[5], b};
+        const Tile<R, kSX> U{bf[0], b}, V{bf[1], b}, HU{bf[2], b}, HV{bf[3], b}, HZ{bf[4], b}, WW{bf[5], b};
         // Every thread reaches both barriers of each level: the compute is predicated on
         // `live` rather than skipped with `continue` (an aligned barrier must not diverge).
-        if (live) {
         R aru = R(0), arv = R(0);
+        if (live) {
         if (rn) {   // addCoriolis (rhs_kernels.cpp:7-35)
             const R cffp = HZ(0, 0) * fp, cffw = HZ(0, -1) * fw, cffs = HZ(-1, 0) * fs;
             const R UFp = cffp * ((V(0, 0) + V(1, 0)) * R(0.5));
@@ -334,7 +352,12 @@ __global__ void __launch_bounds__(kTX *kTY) k_rhs3d(Geo<R> g, const R *__restric
             aru = aru + (UFp + UFw) * R(0.5);
             arv = arv - (VFp + VFs) * R(0.5);
         }
-        {   // horizontalAdvection (rhs_kernels.cpp:93-130), node offsets relative to (j, i)
+        }   // (the live region closes before the flux barrier; it reopens below)
+        // horizontalAdvection (rhs_kernels.cpp:93-130) in two phases.  Each cell's divergence
+        // is "own face flux minus the west (south) neighbour's", and the neighbour's face flux
+        // is the same expression evaluated at the neighbour: phase 1 evaluates every face flux
+        // once (the tile's cells plus the west column and south row of halo cells) into shared
+        // memory, phase 2 differences them, with the reference's operations in its order.
 #define UR(r, c) ((U(r, c) + U(r, (c) + 1)) * R(0.5))
 #define UP(r, c) ((U(r, c) + U(r, (c) - 1)) * R(0.5))
 #define VR(r, c) ((V(r, c) + V((r) + 1, c)) * R(0.5))
@@ -351,18 +374,28 @@ __global__ void __launch_bounds__(kTX *kTY) k_rhs3d(Geo<R> g, const R *__restric
 #define HUEEP(r, c) ((DEE(HU, r, c) + DEE(HU, r, (c) - 1)) * R(0.5))
 #define HVXXP(r, c) ((DXX(HV, r, c) + DXX(HV, (r) - 1, c)) * R(0.5))
 #define HVEER(r, c) ((DEE(HV, r, c) + DEE(HV, (r) + 1, c)) * R(0.5))
-            const R uxx00 = UXXR(0, 0), uxx0w = UXXR(0, -1), uxxs0 = UXXR(-1, 0);
-            const R uee00 = UEEP(0, 0), ueew = UEEP(0, -1), uees = UEEP(-1, 0);
-            const R ufx0 = UR(0, 0) + (G * uxx00) * (HUR(0, 0) + G * HUXXR(0, 0));
-            const R ufxw = UR(0, -1) + (G * uxx0w) * (HUR(0, -1) + G * HUXXR(0, -1));
-            const R ufe0 = UP(0, 0) + (G * uee00) * (HVP(0, 0) + G * HVXXP(0, 0));
-            const R ufes = UP(-1, 0) + (G * uees) * (HVP(-1, 0) + G * HVXXP(-1, 0));
-            const R vfx0 = VP(0, 0) + (G * uee00) * (HUP(0, 0) + G * HUEEP(0, 0));
-            const R vfxw = VP(0, -1) + (G * ueew) * (HUP(0, -1) + G * HUEEP(0, -1));
-            const R vfe0 = VR(0, 0) + (G * uxx00) * (HVR(0, 0) + G * HVEER(0, 0));
-            const R vfes = VR(-1, 0) + (G * uxxs0) * (HVR(-1, 0) + G * HVEER(-1, 0));
+        for (int e = tid; e < kFN; e += TX * TY) {   // phase 1: face fluxes of cell (r, c)
+            const int r = e / kFX - 1, c = e % kFX - 1;
+            if (r < 0 && c < 0) continue;            // the corner cell is nobody's neighbour
+            const int bb = (r + kHY0) * kSX + (c + kHX0);
+            const Tile<R, kSX> U{bf[0], bb}, V{bf[1], bb}, HU{bf[2], bb}, HV{bf[3], bb};
+            const R uxx = UXXR(0, 0), uee = UEEP(0, 0);
+            sF[0 * kFN + e] = UR(0, 0) + (G * uxx) * (HUR(0, 0) + G * HUXXR(0, 0));   // ufx
+            sF[1 * kFN + e] = UP(0, 0) + (G * uee) * (HVP(0, 0) + G * HVXXP(0, 0));   // ufe
+            sF[2 * kFN + e] = VP(0, 0) + (G * uee) * (HUP(0, 0) + G * HUEEP(0, 0));   // vfx
+            sF[3 * kFN + e] = VR(0, 0) + (G * uxx) * (HVR(0, 0) + G * HVEER(0, 0));   // vfe
+        }
+        __syncthreads();
+        if (live) {
+        {   // phase 2: this cell's divergence
+            const int e0 = (ty + 1) * kFX + (tx + 1), ew = e0 - 1, es = e0 - kFX;
+            const R ufx0 = sF[e0], ufxw = sF[ew];
+            const R ufe0 = sF[kFN + e0], ufes = sF[kFN + es];
+            const R vfx0 = sF[2 * kFN + e0], vfxw = sF[2 * kFN + ew];
+            const R vfe0 = sF[3 * kFN + e0], vfes = sF[3 * kFN + es];
             aru = aru - ((ufx0 - ufxw) + (ufe0 - ufes));
             arv = arv - ((vfx0 - vfxw) + (vfe0 - vfes));
+        }
 #undef HVEER
 #undef HVXXP
 #undef HUEEP
@@ -379,7 +412,6 @@ __global__ void __launch_bounds__(kTX *kTY) k_rhs3d(Geo<R> g, const R *__restric
 #undef VR
 #undef UP
 #undef UR
-        }
         // The reference's out-of-range threads (p >= s2) store 0 at flat p, i.e. into levels
         // >= 1, after the in-range threads (rhs_kernels.cpp:86-91).
         if (K >= 1 && o + p < g.ref_threads) {
@@ -433,12 +465,13 @@ __global__ void __launch_bounds__(kTX *kTY) k_rhs3d(Geo<R> g, const R *__restric
 // set_maxflux (step3D_uv.kernels.cpp:372-405) + omega (:62-165) + set_zeta (:294-310)
 // ------------------------------------------------------------------------------------------
 template <typename R>
-__global__ void __launch_bounds__(kBlock) k_maxflux_omega(
-    Geo<R> g, const R *__restrict__ u, const R *__restrict__ v, R *Huon, R *Hvom,
+__device__ __forceinline__ void maxflux_omega_body(
+    const Geo<R> &g, const R *__restrict__ u, const R *__restrict__ v, R *Huon, R *Hvom,
     const R *__restrict__ Hz, R *__restrict__ W, const R *__restrict__ z_w, int do_flux,
-    int do_omega, R *__restrict__ zeta1, R *__restrict__ zeta2, const double *__restrict__ Zt) {
-    const int pi = (int)tid_flat();
-    if (pi >= g.s2) return;
+    int do_omega, R *__restrict__ zeta1, R *__restrict__ zeta2, const double *__restrict__ Zt,
+    const long pl) {
+    if (pl >= g.s2) return;
+    const int pi = (int)pl;
     const long p = pi;
     const long I = g.I, s2 = g.s2;
     const int N = g.N;
@@ -516,10 +549,9 @@ __global__ void __launch_bounds__(kBlock) k_set_zeta(Geo<R> g, R *__restrict__ z
 
 // set_depth (step3D_uv.kernels.cpp:225-291), FP64 arithmetic.
 template <typename R>
-__global__ void __launch_bounds__(kBlock) k_set_depth(Geo<R> g, const double *__restrict__ Zt,
-                                                      R *__restrict__ z_w, R *__restrict__ z_r,
-                                                      R *__restrict__ Hz) {
-    const long p = tid_flat();
+__device__ __forceinline__ void set_depth_body(const Geo<R> &g, const double *__restrict__ Zt,
+                                               R *__restrict__ z_w, R *__restrict__ z_r,
+                                               R *__restrict__ Hz, const long p) {
     if (p >= g.s2) return;
     const long s2 = g.s2;
     const int N = g.N;
@@ -657,19 +689,19 @@ __device__ __forceinline__ R mean_correction(int N, long s2, long p, long d, con
 }
 
 template <typename R>
-__global__ void __launch_bounds__(128) k_step3d_uv(Geo<R> g, R *__restrict__ u, R *__restrict__ v,
+__device__ __forceinline__ void step3d_uv_body(const Geo<R> &g, R *__restrict__ u, R *__restrict__ v,
                             const R *__restrict__ ru, const R *__restrict__ rv,
                             R *__restrict__ ubar_t1, R *__restrict__ vbar_t1,
                             R *__restrict__ ubar_t2, R *__restrict__ vbar_t2,
                             const R *__restrict__ Hz, const R *__restrict__ Akv,
                             const R *__restrict__ z_r, const double *__restrict__ DU,
                             const double *__restrict__ DV, const R *tmpU, const R *tmpV, R cff,
-                            R lambda, R Dt, int do_bc, R bcval) {
+                            R lambda, R Dt, int do_bc, R bcval, const long pl) {
     const int N = g.N;
     R FCa[kNMax], BDa[kNMax], RHSa[kNMax];
     const Tri<R> m{FCa, BDa, RHSa, 1, 0};
-    const int pi = (int)tid_flat();
-    if (pi >= g.s2) return;      // no barriers below
+    if (pl >= g.s2) return;      // no barriers below
+    const int pi = (int)pl;
     const long p = pi;
     const long I = g.I, s2 = g.s2;
     const int i = pi % g.I, j = pi / g.I;
@@ -742,41 +774,42 @@ __global__ void __launch_bounds__(128) k_step3d_uv(Geo<R> g, R *__restrict__ u, 
 // form's tolerance.  Columns on the rows where the reference solves the U system a second
 // time for V (solveTri gated by isUNode, :525) and where V gets only the mean correction take
 // the general path above after the pipelined part.
-constexpr int kPipeCols = 64;
+constexpr int kPipeCols = kPipeTile;
 constexpr int kPipeDepth = 6;
+constexpr int kPipeThreads = 2 * kPipeCols;   // one thread per system (U, V) and column
 constexpr int kPipeSlot = 3 * (2 * kPipeCols + 1) + 4 * kPipeCols;   // floats per level
 
 __host__ __device__ constexpr size_t pipe_smem_bytes(int N) {
-    return sizeof(float) * ((size_t)4 * N * kPipeCols + (size_t)kPipeDepth * kPipeSlot);
+    return sizeof(float) * ((size_t)2 * N * kPipeThreads + (size_t)kPipeDepth * kPipeSlot);
 }
 
 template <typename R>   // R = float only: the FP32 form
-__global__ void __launch_bounds__(kPipeCols) k_step3d_uv_pipe(Geo<R> g, float *__restrict__ u,
+__device__ __forceinline__ void step3d_uv_pipe_body(const Geo<R> &g, float *__restrict__ u,
         float *__restrict__ v, const float *__restrict__ ru, const float *__restrict__ rv,
         float *__restrict__ ubar_t1, float *__restrict__ vbar_t1, float *__restrict__ ubar_t2,
         float *__restrict__ vbar_t2, const float *__restrict__ Hz, const float *__restrict__ Akv,
         const float *__restrict__ z_r, const double *__restrict__ DU,
         const double *__restrict__ DV, const float *tmpU, const float *tmpV, float cff,
-        float lambda, float Dt, int do_bc, float bcval) {
+        float lambda, float Dt, int do_bc, float bcval, const long tile) {
     extern __shared__ float spipe[];
     const int N = g.N;
     const long I = g.I, s2 = g.s2;
-    const int t = threadIdx.x;
-    const long p0 = (long)blockIdx.x * kPipeCols;
-    const long p = p0 + t;
-    float *cU = spipe + t, *dU = cU + N * kPipeCols, *cV = dU + N * kPipeCols,
-          *dV = cV + N * kPipeCols;
-    float *ring = spipe + 4 * N * kPipeCols;
+    // two threads per column: sys 0 solves the U system of column col, sys 1 its V system
+    const int col = threadIdx.x & (kPipeCols - 1), sys = threadIdx.x / kPipeCols;
+    const long p0 = tile * kPipeCols;
+    const long p = p0 + col;
+    float *cc = spipe + threadIdx.x, *dd = cc + N * kPipeThreads;   // [level][thread]
+    float *ring = spipe + 2 * N * kPipeThreads;
     const float *uo_all = tmpU ? tmpU : u, *vo_all = tmpV ? tmpV : v;
 
-    // level k into slot: Hz(k), Akv(k), z_r(k+1) at [p0-1, p0+63] and [p0-I, p0-I+63]; old
-    // u, v and ru, rv at level k on [p0, p0+63].  Thread t copies the element at t of every
-    // segment (thread 0 also the 65th of the shifted rows); sources outside [0, s2) in the
-    // plane are zero-filled (their columns are not U/V nodes).
-    const long qW = p0 - 1 + t, qS = p0 - I + t, qE = p0 + kPipeCols - 1;
-    const bool okW = qW >= 0 && qW < s2, okS = qS >= 0 && qS < s2, okP = p < s2;
-    const bool okE = t == 0 && qE < s2;
+    // level k into slot: Hz(k), Akv(k), z_r(k+1) at [p0-1, p0+63] (sys 0 copies these, plus
+    // old u and ru) and [p0-I, p0-I+63] (sys 1, plus old v and rv); sources outside [0, s2) in
+    // the plane are zero-filled (their columns are not U/V nodes).
+    const long q = sys == 0 ? p0 - 1 + col : p0 - I + col, qE = p0 + kPipeCols - 1;
+    const bool okq = q >= 0 && q < s2, okP = p < s2;
+    const bool okE = sys == 0 && col == 0 && qE < s2;
     constexpr int kRow = 2 * kPipeCols + 1;
+    const int seg = sys == 0 ? col : kPipeCols + 1 + col;
     auto issue = [&](int k) {
         float *sl = ring + (k % kPipeDepth) * kPipeSlot;
         const long o = (long)k * s2;
@@ -786,87 +819,67 @@ __global__ void __launch_bounds__(kPipeCols) k_step3d_uv_pipe(Geo<R> g, float *_
         for (int f = 0; f < 3; ++f) {
             const bool on = f < 2 || zr;
             float *d = sl + f * kRow;
-            cp_async(d + t, fld[f] + (okW && on ? qW : 0), okW && on);
-            cp_async(d + kPipeCols + 1 + t, fld[f] + (okS && on ? qS : 0), okS && on);
-            if (t == 0) cp_async(d + kPipeCols, fld[f] + (okE && on ? qE : 0), okE && on);
+            cp_async(d + seg, fld[f] + (okq && on ? q : 0), okq && on);
+            if (sys == 0 && col == 0) cp_async(d + kPipeCols, fld[f] + (okE && on ? qE : 0), okE && on);
         }
         float *d = sl + 3 * kRow;
-        cp_async(d + t, uo_all + o + (okP ? p : 0), okP);
-        cp_async(d + kPipeCols + t, vo_all + o + (okP ? p : 0), okP);
-        cp_async(d + 2 * kPipeCols + t, ru + o + (okP ? p : 0), okP);
-        cp_async(d + 3 * kPipeCols + t, rv + o + (okP ? p : 0), okP);
+        const float *a = sys == 0 ? uo_all : vo_all, *r = sys == 0 ? ru : rv;
+        cp_async(d + sys * kPipeCols + col, a + o + (okP ? p : 0), okP);
+        cp_async(d + (2 + sys) * kPipeCols + col, r + o + (okP ? p : 0), okP);
     };
     const int i = (int)(p % I), j = (int)(p / I);
     const bool live = p < s2;
     const bool un = live && unode_(i, j), vn = live && vnode_(i, j, g.J);
     const bool both = un && vn;
+    const long d = sys == 0 ? 1 : I;   // the neighbour of this system's face
 
     for (int k = 0; k < kPipeDepth; ++k) {
         if (k < N) issue(k);
         cp_async_commit();
     }
     const float cm = -lambda * Dt;
-    float cmnU = 0.f, cmnV = 0.f, zP = 0.f, zW = 0.f, zS = 0.f;
+    float cmn = 0.f, zP = 0.f, zQ = 0.f;
     if (both) {
-        cmnU = cff * Dt * (((g.pm[p] + g.pm[p - 1]) * 0.5f) * ((g.pn[p] + g.pn[p - 1]) * 0.5f));
-        cmnV = cff * Dt * (((g.pm[p] + g.pm[p - I]) * 0.5f) * ((g.pn[p] + g.pn[p - I]) * 0.5f));
+        cmn = cff * Dt * (((g.pm[p] + g.pm[p - d]) * 0.5f) * ((g.pn[p] + g.pn[p - d]) * 0.5f));
         zP = z_r[p];
-        zW = z_r[p - 1];
-        zS = z_r[p - I];
+        zQ = z_r[p - d];
     }
-    float fu = 0.f, fv = 0.f, fu0 = 0.f, fv0 = 0.f, ccu = 0.f, ccv = 0.f, ddu = 0.f, ddv = 0.f;
-    double HU = 0.0, HV = 0.0, OU = 0.0, OV = 0.0, RU = 0.0, RV = 0.0;
+    float fc = 0.f, fc0 = 0.f, ccp = 0.f, ddp = 0.f;
+    double H = 0.0, O = 0.0, Rs = 0.0;
+    const int qi = sys == 0 ? col : kPipeCols + 1 + col;   // this system's neighbour in a row
     for (int k = 0; k < N; ++k) {
         cp_async_wait<kPipeDepth - 1>();
         __syncthreads();
         if (both) {
             const float *sl = ring + (k % kPipeDepth) * kPipeSlot;
-            const float *sHz = sl, *sAk = sl + (2 * kPipeCols + 1), *sZr = sl + 2 * (2 * kPipeCols + 1);
-            const float *sUo = sl + 3 * (2 * kPipeCols + 1), *sVo = sUo + kPipeCols,
-                        *sRu = sVo + kPipeCols, *sRv = sRu + kPipeCols;
-            const float hP = sHz[t + 1];
-            const float hu = (hP + sHz[t]) * 0.5f, hv = (hP + sHz[kPipeCols + 1 + t]) * 0.5f;
-            float gu = 0.f, gv = 0.f;
+            const float *sHz = sl, *sAk = sl + kRow, *sZr = sl + 2 * kRow;
+            const float *sO = sl + 3 * kRow + sys * kPipeCols, *sR = sl + 3 * kRow + (2 + sys) * kPipeCols;
+            const float hz = (sHz[col + 1] + sHz[qi]) * 0.5f;
+            float gk = 0.f;
             if (k < N - 1) {
-                const float zP1 = sZr[t + 1], zW1 = sZr[t], zS1 = sZr[kPipeCols + 1 + t];
-                const float a = sAk[t + 1];
-                gu = (cm * ((a + sAk[t]) * 0.5f)) / (((zP1 - zP) + (zW1 - zW)) * 0.5f);
-                gv = (cm * ((a + sAk[kPipeCols + 1 + t]) * 0.5f)) / (((zP1 - zP) + (zS1 - zS)) * 0.5f);
+                const float zP1 = sZr[col + 1], zQ1 = sZr[qi];
+                gk = (cm * ((sAk[col + 1] + sAk[qi]) * 0.5f)) / (((zP1 - zP) + (zQ1 - zQ)) * 0.5f);
                 zP = zP1;
-                zW = zW1;
-                zS = zS1;
+                zQ = zQ1;
             }
-            const float ou = sUo[t], ov = sVo[t];
+            const float ok = sO[col];
             if (k == 0) {   // bottom row: right-hand side forced to 0 (:610)
-                fu0 = gu;
-                fv0 = gv;
-                ccu = gu / (hu - 2.f * gu);
-                ccv = gv / (hv - 2.f * gv);
-                ddu = 0.f;
-                ddv = 0.f;
+                fc0 = gk;
+                ccp = gk / (hz - 2.f * gk);
+                ddp = 0.f;
             } else {
-                const float r_u = hu * (ou + cmnU * sRu[t]);
-                const float r_v = hv * (ov + cmnV * sRv[t]);
-                const float bu = (k < N - 1) ? (hu - gu) - fu : hu - fu;
-                const float bv = (k < N - 1) ? (hv - gv) - fv : hv - fv;
-                const float iu = 1.f / (bu - fu * ccu), iv = 1.f / (bv - fv * ccv);
-                ccu = gu * iu;
-                ccv = gv * iv;
-                ddu = (r_u - fu * ddu) * iu;
-                ddv = (r_v - fv * ddv) * iv;
-                RU += (double)r_u;
-                RV += (double)r_v;
+                const float rr = hz * (ok + cmn * sR[col]);
+                const float bd = (k < N - 1) ? (hz - gk) - fc : hz - fc;
+                const float iv = 1.f / (bd - fc * ccp);
+                ccp = gk * iv;
+                ddp = (rr - fc * ddp) * iv;
+                Rs += (double)rr;
             }
-            cU[k * kPipeCols] = ccu;
-            dU[k * kPipeCols] = ddu;
-            cV[k * kPipeCols] = ccv;
-            dV[k * kPipeCols] = ddv;
-            fu = gu;
-            fv = gv;
-            HU += (double)hu;
-            HV += (double)hv;
-            OU += (double)(ou * hu);
-            OV += (double)(ov * hv);
+            cc[k * kPipeThreads] = ccp;
+            dd[k * kPipeThreads] = ddp;
+            fc = gk;
+            H += (double)hz;
+            O += (double)(ok * hz);
         }
         __syncthreads();                 // slot k % depth is free again
         if (k + kPipeDepth < N) issue(k + kPipeDepth);
@@ -874,34 +887,33 @@ __global__ void __launch_bounds__(kPipeCols) k_step3d_uv_pipe(Geo<R> g, float *_
     }
     cp_async_wait<0>();
     if (both) {
-        const double duo = DU[p] / (double)g.on_u[p], dvo = DV[p] / (double)g.om_v[p];
-        const float subU = (float)((OU - duo) / HU), subV = (float)((OV - dvo) / HV);
-        float xu = ddu, xv = ddv;
-        float *up = u + p, *vp = v + p;
-        up[(long)(N - 1) * s2] = xu - subU;
-        vp[(long)(N - 1) * s2] = xv - subV;
+        const double dbar = sys == 0 ? DU[p] / (double)g.on_u[p] : DV[p] / (double)g.om_v[p];
+        const float sub = (float)((O - dbar) / H);
+        float x = ddp;
+        float *out = (sys == 0 ? u : v) + p;
+        out[(long)(N - 1) * s2] = x - sub;
         for (int k = N - 2; k >= 0; --k) {
-            xu = dU[k * kPipeCols] - cU[k * kPipeCols] * xu;
-            xv = dV[k * kPipeCols] - cV[k * kPipeCols] * xv;
-            up[(long)k * s2] = xu - subU;
-            vp[(long)k * s2] = xv - subV;
+            x = dd[k * kPipeThreads] - cc[k * kPipeThreads] * x;
+            out[(long)k * s2] = x - sub;
         }
-        const double HuU = RU + (double)fu0 * (double)xu - (double)subU * HU;
-        const double HvV = RV + (double)fv0 * (double)xv - (double)subV * HV;
-        const float ub = (float)(duo / HU + (HuU - duo) / HU);
-        const float vb = (float)(dvo / HV + (HvV - dvo) / HV);
-        ubar_t2[p] = ub;
-        vbar_t2[p] = vb;
-        ubar_t1[p] = ub;
-        vbar_t1[p] = vb;
-    } else if (un || vn) {
+        // sum_k hz_k (x_k - sub) from the column identity
+        const double Hx = Rs + (double)fc0 * (double)x - (double)sub * H;
+        const float bar = (float)(dbar / H + (Hx - dbar) / H);
+        if (sys == 0) {
+            ubar_t2[p] = bar;
+            ubar_t1[p] = bar;
+        } else {
+            vbar_t2[p] = bar;
+            vbar_t1[p] = bar;
+        }
+    } else if ((un || vn) && sys == 0) {
         const float *uo = uo_all + p, *vo = vo_all + p;
         float FCa[kNMax], BDa[kNMax], RHSa[kNMax];
         const Tri<float> m{FCa, BDa, RHSa, 1, 0};
         if (un) {
-            double H, Hu;
-            build_eliminate(g, p, 1, cff, Dt, lambda, m, Hz, Akv, z_r, uo, ru, H, Hu);
-            const float udiff = (float)((Hu - DU[p] / (double)g.on_u[p]) / H);
+            double Hh, Hu;
+            build_eliminate(g, p, 1, cff, Dt, lambda, m, Hz, Akv, z_r, uo, ru, Hh, Hu);
+            const float udiff = (float)((Hu - DU[p] / (double)g.on_u[p]) / Hh);
             back_substitute(N, s2, m, u + p, udiff);
             eliminate_again(N, m);
             back_substitute(N, s2, m, v + p, 0.f);
@@ -926,11 +938,11 @@ __global__ void __launch_bounds__(kPipeCols) k_step3d_uv_pipe(Geo<R> g, float *_
             for (int K = 0; K < N; ++K) v[(long)K * s2 + p] = v[(long)K * s2 + p] - vdiff;
         }
     }
-    if (do_bc && live) {
+    if (do_bc && live) {   // each system's thread its own field
         const int ut = g.utype[p], vt = g.vtype[p];
-        if (ut > 0 && (ut & (1 << 4)) == 0 && (ut & (1 << 3)) != 0)
+        if (sys == 0 && ut > 0 && (ut & (1 << 4)) == 0 && (ut & (1 << 3)) != 0)
             for (int K = 0; K < N; ++K) u[(long)K * s2 + p] = bcval;
-        if (vt > 0 && ((vt & (1 << 4)) != 0 || (vt & (1 << 3)) != 0))
+        if (sys == 1 && vt > 0 && ((vt & (1 << 4)) != 0 || (vt & (1 << 3)) != 0))
             for (int K = 0; K < N; ++K) v[(long)K * s2 + p] = 0.f;
     }
 }
@@ -1065,9 +1077,168 @@ __global__ void __launch_bounds__(kBlock) k_lateral_uv_bc(Geo<R> g, R *__restric
 namespace sf {
 
 // ------------------------------------------------------------------------------------------
+// Kernels: one grid (the arrays as given) and ensembles (pools; each block finds its member
+// and its block within the member from a block map, and offsets the pools by the member's
+// 2D / N+1-level / N-level offsets).  Both run the same bodies.
+// ------------------------------------------------------------------------------------------
+#define SF_MEMBER(bm)                                 \
+    const int2 mb_ = (bm)[blockIdx.x];                 \
+    const Member<R> &M_ = mt[mb_.x];                   \
+    const Geo<R> g = M_.g;                             \
+    const long o2 = M_.off2, o3 = M_.off3, oN = M_.offN; \
+    (void)o2; (void)o3; (void)oN;
+#define O2(x) ((x) ? (x) + o2 : (x))
+#define O3(x) ((x) ? (x) + o3 : (x))
+#define ON(x) ((x) ? (x) + oN : (x))
+
+template <typename R>
+__global__ void __launch_bounds__(kBlock) k_zeta_rhs(
+    Geo<R> g, const R *zeta, const R *ubar, const R *vbar, R *rzeta, int mode, double cff1,
+    double *Zt, double *DU, double *DV, const R *zeta_t0, R *zeta_t2, R Dt) {
+    zeta_rhs_body(g, zeta, ubar, vbar, rzeta, mode, cff1, Zt, DU, DV, zeta_t0, zeta_t2, Dt,
+                  (long)tid_flat());
+}
+template <typename R>
+__global__ void __launch_bounds__(kBlock) kb_zeta_rhs(
+    const Member<R> *mt, const int2 *bm, const R *zeta, const R *ubar, const R *vbar, R *rzeta,
+    int mode, double cff1, double *Zt, double *DU, double *DV, const R *zeta_t0, R *zeta_t2,
+    R Dt) {
+    SF_MEMBER(bm)
+    zeta_rhs_body(g, O2(zeta), O2(ubar), O2(vbar), O2(rzeta), mode, cff1, O2(Zt), O2(DU), O2(DV),
+                  O2(zeta_t0), O2(zeta_t2), Dt, (long)mb_.y * kBlock + threadIdx.x);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kBlock) k_momentum(
+    Geo<R> g, R *rhs_u, R *rhs_v, const R *za, const R *zb, R grav, R w1, R w, int do_rhs,
+    int do_pred, R Dt, const R *u_t1, R *u_t2, const R *v_t1, R *v_t2, const R *z1,
+    const R *z2) {
+    momentum_body(g, rhs_u, rhs_v, za, zb, grav, w1, w, do_rhs, do_pred, Dt, u_t1, u_t2, v_t1,
+                  v_t2, z1, z2, (long)tid_flat());
+}
+template <typename R>
+__global__ void __launch_bounds__(kBlock) kb_momentum(
+    const Member<R> *mt, const int2 *bm, R *rhs_u, R *rhs_v, const R *za, const R *zb, R grav,
+    R w1, R w, int do_rhs, int do_pred, R Dt, const R *u_t1, R *u_t2, const R *v_t1, R *v_t2,
+    const R *z1, const R *z2) {
+    SF_MEMBER(bm)
+    momentum_body(g, O2(rhs_u), O2(rhs_v), O2(za), O2(zb), grav, w1, w, do_rhs, do_pred, Dt,
+                  O2(u_t1), O2(u_t2), O2(v_t1), O2(v_t2), O2(z1), O2(z2),
+                  (long)mb_.y * kBlock + threadIdx.x);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kBlock) k_corr_point(
+    Geo<R> g, R Dt, R *zeta_t2, const R *rz0, const R *rz1, const R *rz2, R *ubar_t1,
+    const R *vbar_t1, const R *rub0, const R *rub1, R *vbar_t2) {
+    corr_point_body(g, Dt, zeta_t2, rz0, rz1, rz2, ubar_t1, vbar_t1, rub0, rub1, vbar_t2,
+                    (long)tid_flat());
+}
+template <typename R>
+__global__ void __launch_bounds__(kBlock) kb_corr_point(
+    const Member<R> *mt, const int2 *bm, R Dt, R *zeta_t2, const R *rz0, const R *rz1,
+    const R *rz2, R *ubar_t1, const R *vbar_t1, const R *rub0, const R *rub1, R *vbar_t2) {
+    SF_MEMBER(bm)
+    corr_point_body(g, Dt, O2(zeta_t2), O2(rz0), O2(rz1), O2(rz2), O2(ubar_t1), O2(vbar_t1),
+                    O2(rub0), O2(rub1), O2(vbar_t2), (long)mb_.y * kBlock + threadIdx.x);
+}
+
+template <typename R, int TX, int TY>
+__global__ void __launch_bounds__(TX *TY) k_rhs3d(Geo<R> g, const R *u, const R *v,
+                                                  const R *Huon, const R *Hvom, const R *W,
+                                                  const R *Hz, R *ru, R *rv) {
+    rhs3d_body<R, TX, TY>(g, u, v, Huon, Hvom, W, Hz, ru, rv, (int)blockIdx.x, (int)blockIdx.y);
+}
+template <typename R, int TX, int TY>
+__global__ void __launch_bounds__(TX *TY) kb_rhs3d(const Member<R> *mt, const int2 *bm, int var,
+                                                   const R *u, const R *v, const R *Huon,
+                                                   const R *Hvom, const R *W, const R *Hz,
+                                                   R *ru, R *rv) {
+    SF_MEMBER(bm)
+    const int ntx = M_.ntx[var];
+    rhs3d_body<R, TX, TY>(g, O3(u), O3(v), O3(Huon), O3(Hvom), O3(W), ON(Hz), O3(ru), O3(rv),
+                          mb_.y % ntx, mb_.y / ntx);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kBlock) k_maxflux_omega(
+    Geo<R> g, const R *u, const R *v, R *Huon, R *Hvom, const R *Hz, R *W, const R *z_w,
+    int do_flux, int do_omega, R *zeta1, R *zeta2, const double *Zt) {
+    maxflux_omega_body(g, u, v, Huon, Hvom, Hz, W, z_w, do_flux, do_omega, zeta1, zeta2, Zt,
+                       (long)tid_flat());
+}
+template <typename R>
+__global__ void __launch_bounds__(kBlock) kb_maxflux_omega(
+    const Member<R> *mt, const int2 *bm, const R *u, const R *v, R *Huon, R *Hvom, const R *Hz,
+    R *W, const R *z_w, int do_flux, int do_omega, R *zeta1, R *zeta2, const double *Zt) {
+    SF_MEMBER(bm)
+    maxflux_omega_body(g, O3(u), O3(v), O3(Huon), O3(Hvom), ON(Hz), O3(W), O3(z_w), do_flux,
+                       do_omega, O2(zeta1), O2(zeta2), O2(Zt), (long)mb_.y * kBlock + threadIdx.x);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kBlock) k_set_depth(Geo<R> g, const double *Zt, R *z_w, R *z_r,
+                                                      R *Hz) {
+    set_depth_body(g, Zt, z_w, z_r, Hz, (long)tid_flat());
+}
+template <typename R>
+__global__ void __launch_bounds__(kBlock) kb_set_depth(const Member<R> *mt, const int2 *bm,
+                                                       const double *Zt, R *z_w, R *z_r, R *Hz) {
+    SF_MEMBER(bm)
+    set_depth_body(g, O2(Zt), O3(z_w), ON(z_r), ON(Hz), (long)mb_.y * kBlock + threadIdx.x);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(128) k_step3d_uv(
+    Geo<R> g, R *u, R *v, const R *ru, const R *rv, R *ubar_t1, R *vbar_t1, R *ubar_t2,
+    R *vbar_t2, const R *Hz, const R *Akv, const R *z_r, const double *DU, const double *DV,
+    const R *tmpU, const R *tmpV, R cff, R lambda, R Dt, int do_bc, R bcval) {
+    step3d_uv_body(g, u, v, ru, rv, ubar_t1, vbar_t1, ubar_t2, vbar_t2, Hz, Akv, z_r, DU, DV,
+                   tmpU, tmpV, cff, lambda, Dt, do_bc, bcval, (long)tid_flat());
+}
+template <typename R>
+__global__ void __launch_bounds__(128) kb_step3d_uv(
+    const Member<R> *mt, const int2 *bm, R *u, R *v, const R *ru, const R *rv, R *ubar_t1,
+    R *vbar_t1, R *ubar_t2, R *vbar_t2, const R *Hz, const R *Akv, const R *z_r,
+    const double *DU, const double *DV, const R *tmpU, const R *tmpV, R cff, R lambda, R Dt,
+    int do_bc, R bcval) {
+    SF_MEMBER(bm)
+    step3d_uv_body(g, O3(u), O3(v), O3(ru), O3(rv), O2(ubar_t1), O2(vbar_t1), O2(ubar_t2),
+                   O2(vbar_t2), ON(Hz), O3(Akv), ON(z_r), O2(DU), O2(DV), O3(tmpU), O3(tmpV), cff,
+                   lambda, Dt, do_bc, bcval, (long)mb_.y * 128 + threadIdx.x);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kPipeThreads) k_step3d_uv_pipe(
+    Geo<R> g, float *u, float *v, const float *ru, const float *rv, float *ubar_t1,
+    float *vbar_t1, float *ubar_t2, float *vbar_t2, const float *Hz, const float *Akv,
+    const float *z_r, const double *DU, const double *DV, const float *tmpU, const float *tmpV,
+    float cff, float lambda, float Dt, int do_bc, float bcval) {
+    step3d_uv_pipe_body(g, u, v, ru, rv, ubar_t1, vbar_t1, ubar_t2, vbar_t2, Hz, Akv, z_r, DU, DV,
+                        tmpU, tmpV, cff, lambda, Dt, do_bc, bcval, (long)blockIdx.x);
+}
+template <typename R>
+__global__ void __launch_bounds__(kPipeThreads) kb_step3d_uv_pipe(
+    const Member<R> *mt, const int2 *bm, float *u, float *v, const float *ru, const float *rv,
+    float *ubar_t1, float *vbar_t1, float *ubar_t2, float *vbar_t2, const float *Hz,
+    const float *Akv, const float *z_r, const double *DU, const double *DV, const float *tmpU,
+    const float *tmpV, float cff, float lambda, float Dt, int do_bc, float bcval) {
+    SF_MEMBER(bm)
+    step3d_uv_pipe_body(g, O3(u), O3(v), O3(ru), O3(rv), O2(ubar_t1), O2(vbar_t1), O2(ubar_t2),
+                        O2(vbar_t2), ON(Hz), O3(Akv), ON(z_r), O2(DU), O2(DV), O3(tmpU), O3(tmpV),
+                        cff, lambda, Dt, do_bc, bcval, (long)mb_.y);
+}
+#undef ON
+#undef O3
+#undef O2
+#undef SF_MEMBER
+
+// ------------------------------------------------------------------------------------------
 // Launchers
 // ------------------------------------------------------------------------------------------
 inline unsigned blocks_for(long n, int b) { return (unsigned)((n + b - 1) / b); }
+template <typename R>
+inline const Member<R> *mt(const sf_ctx *c) { return static_cast<const Member<R> *>(c->members); }
 
 template <typename R>
 Geo<R> Ops<R>::geo(const sf_ctx *c) {
@@ -1100,6 +1271,11 @@ template <typename R>
 cudaError_t Ops<R>::zeta_rhs(const sf_ctx *c, const R *zeta, const R *ubar, const R *vbar,
                              R *rzeta, int mode, double cff1, double *Zt, double *DU, double *DV,
                              const R *zeta_t0, R *zeta_t2, double Dt, cudaStream_t s) {
+    if (c->nmem > 1) {
+        kb_zeta_rhs<R><<<c->nbm_pt, kBlock, 0, s>>>(mt<R>(c), c->bm_pt, zeta, ubar, vbar, rzeta, mode,
+                                                   cff1, Zt, DU, DV, zeta_t0, zeta_t2, (R)Dt);
+        return cudaGetLastError();
+    }
     k_zeta_rhs<R><<<blocks_for(c->s2, kBlock), kBlock, 0, s>>>(geo(c), zeta, ubar, vbar, rzeta,
                                                                mode, cff1, Zt, DU, DV, zeta_t0,
                                                                zeta_t2, (R)Dt);
@@ -1123,6 +1299,12 @@ cudaError_t Ops<R>::momentum(const sf_ctx *c, R *rhs_u, R *rhs_v, const R *za, c
                              const R *u_t1, R *u_t2, const R *v_t1, R *v_t2, const R *z1,
                              const R *z2, cudaStream_t s) {
     const double w1 = 1 - weight;
+    if (c->nmem > 1) {
+        kb_momentum<R><<<c->nbm_pt, kBlock, 0, s>>>(
+            mt<R>(c), c->bm_pt, rhs_u, rhs_v, za, zb, (R)g, (R)w1, (R)weight, do_rhs, do_pred, (R)Dt,
+            u_t1, u_t2, v_t1, v_t2, z1, z2);
+        return cudaGetLastError();
+    }
     k_momentum<R><<<blocks_for(c->s2, kBlock), kBlock, 0, s>>>(
         geo(c), rhs_u, rhs_v, za, zb, (R)g, (R)w1, (R)weight, do_rhs, do_pred, (R)Dt, u_t1, u_t2,
         v_t1, v_t2, z1, z2);
@@ -1138,6 +1320,11 @@ template <typename R>
 cudaError_t Ops<R>::corr_point(const sf_ctx *c, double Dt, R *zeta_t2, const R *rz0,
                                const R *rz1, const R *rz2, R *ubar_t1, const R *vbar_t1,
                                const R *rub0, const R *rub1, R *vbar_t2, cudaStream_t s) {
+    if (c->nmem > 1) {
+        kb_corr_point<R><<<c->nbm_pt, kBlock, 0, s>>>(mt<R>(c), c->bm_pt, (R)Dt, zeta_t2, rz0, rz1,
+                                                     rz2, ubar_t1, vbar_t1, rub0, rub1, vbar_t2);
+        return cudaGetLastError();
+    }
     k_corr_point<R><<<blocks_for(c->s2, kBlock), kBlock, 0, s>>>(
         geo(c), (R)Dt, zeta_t2, rz0, rz1, rz2, ubar_t1, vbar_t1, rub0, rub1, vbar_t2);
     return cudaGetLastError();
@@ -1145,22 +1332,61 @@ cudaError_t Ops<R>::corr_point(const sf_ctx *c, double Dt, R *zeta_t2, const R *
 template <typename R>
 cudaError_t Ops<R>::bc_apply(const sf_ctx *c, const BcProgram &p1, R *f1, const BcProgram &p2,
                              R *f2, double val, cudaStream_t s, const double *valp) {
-    const long n = (long)p1.n + p2.n;
+    long n = (long)p1.n + p2.n;
     if (n == 0 && p1.nch == 0 && p2.nch == 0) return cudaSuccess;
+    if (n < p1.ngr) n = p1.ngr;
+    if (n < p2.ngr) n = p2.ngr;
     k_bc_apply<R><<<blocks_for(n > 0 ? n : 1, 256), 256, 0, s>>>(p1, f1, p2, f2, (R)val, valp);
     return cudaGetLastError();
 }
 template <typename R>
 cudaError_t Ops<R>::rhs3d(const sf_ctx *c, const R *u, const R *v, const R *Huon, const R *Hvom,
                           const R *W, const R *Hz, R *ru, R *rv, cudaStream_t s) {
-    const dim3 grid((c->I + kTX - 1) / kTX, (c->J + kTY - 1) / kTY), block(kTX, kTY);
-    k_rhs3d<R><<<grid, block, 0, s>>>(geo(c), u, v, Huon, Hvom, W, Hz, ru, rv);
+    // tile variant: 0 = 32 x 8, 1 = 32 x 4, 2 = 64 x 4
+    const int var = c->rhs_tile;
+    auto run = [&](auto tx, auto ty) {
+        constexpr int TX = decltype(tx)::value, TY = decltype(ty)::value;
+        constexpr size_t smem = rhs_smem_bytes<R, TX, TY>();
+        static bool attr_set[64] = {};
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+            cudaFuncSetAttribute(k_rhs3d<R, TX, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem);
+            cudaFuncSetAttribute(kb_rhs3d<R, TX, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem);
+            attr_set[dev] = true;
+        }
+        if (c->nmem > 1) {
+            kb_rhs3d<R, TX, TY><<<c->nbm_tile[var], dim3(TX, TY), smem, s>>>(
+                mt<R>(c), c->bm_tile[var], var, u, v, Huon, Hvom, W, Hz, ru, rv);
+        } else {
+            const dim3 grid((c->I + TX - 1) / TX, (c->J + TY - 1) / TY), block(TX, TY);
+            k_rhs3d<R, TX, TY><<<grid, block, smem, s>>>(geo(c), u, v, Huon, Hvom, W, Hz, ru, rv);
+        }
+    };
+    using I32 = std::integral_constant<int, 32>;
+    using I8 = std::integral_constant<int, 8>;
+    using I4 = std::integral_constant<int, 4>;
+    using I64 = std::integral_constant<int, 64>;
+    if (var == 1) {
+        run(I32{}, I4{});
+    } else if (var == 2) {
+        run(I64{}, I4{});
+    } else {
+        run(I32{}, I8{});
+    }
     return cudaGetLastError();
 }
 template <typename R>
 cudaError_t Ops<R>::maxflux_omega(const sf_ctx *c, const R *u, const R *v, R *Huon, R *Hvom,
                                   const R *Hz, R *W, const R *z_w, int do_flux, int do_omega,
                                   R *zeta1, R *zeta2, const double *Zt, cudaStream_t s) {
+    if (c->nmem > 1) {
+        kb_maxflux_omega<R><<<c->nbm_pt, kBlock, 0, s>>>(mt<R>(c), c->bm_pt, u, v, Huon, Hvom, Hz, W,
+                                                        z_w, do_flux, do_omega, zeta1, zeta2, Zt);
+        return cudaGetLastError();
+    }
     k_maxflux_omega<R><<<blocks_for(c->s2, kBlock), kBlock, 0, s>>>(
         geo(c), u, v, Huon, Hvom, Hz, W, z_w, do_flux, do_omega, zeta1, zeta2, Zt);
     return cudaGetLastError();
@@ -1173,6 +1399,10 @@ cudaError_t Ops<R>::set_zeta(const sf_ctx *c, R *z1, R *z2, const double *Zt, cu
 template <typename R>
 cudaError_t Ops<R>::set_depth(const sf_ctx *c, const double *Zt, R *z_w, R *z_r, R *Hz,
                               cudaStream_t s) {
+    if (c->nmem > 1) {
+        kb_set_depth<R><<<c->nbm_pt, kBlock, 0, s>>>(mt<R>(c), c->bm_pt, Zt, z_w, z_r, Hz);
+        return cudaGetLastError();
+    }
     k_set_depth<R><<<blocks_for(c->s2, kBlock), kBlock, 0, s>>>(geo(c), Zt, z_w, z_r, Hz);
     return cudaGetLastError();
 }
@@ -1188,16 +1418,32 @@ cudaError_t Ops<R>::step3d_uv(const sf_ctx *c, R *u, R *v, const R *ru, const R 
         int dev = 0;
         cudaGetDevice(&dev);
         if (dev >= 0 && dev < 64 && !attr_set[dev]) {
-            const cudaError_t e = cudaFuncSetAttribute(k_step3d_uv_pipe<float>,
-                                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                       (int)pipe_smem_bytes(kNMax));
+            cudaError_t e = cudaFuncSetAttribute(k_step3d_uv_pipe<float>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)pipe_smem_bytes(kNMax));
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(kb_step3d_uv_pipe<float>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)pipe_smem_bytes(kNMax));
             if (e != cudaSuccess) return e;
             attr_set[dev] = true;
         }
-        k_step3d_uv_pipe<float><<<blocks_for(c->s2, kPipeCols), kPipeCols, pipe_smem_bytes(c->N),
+        if (c->nmem > 1) {
+            kb_step3d_uv_pipe<float><<<c->nbm_pipe, kPipeThreads, pipe_smem_bytes(c->maxN), s>>>(
+                mt<R>(c), c->bm_pipe, u, v, ru, rv, ubar_t1, vbar_t1, ubar_t2, vbar_t2, Hz, Akv, z_r,
+                DU, DV, tmpU, tmpV, (float)cff, (float)lambda, (float)Dt, do_bc, (float)bcval);
+            return cudaGetLastError();
+        }
+        k_step3d_uv_pipe<float><<<blocks_for(c->s2, kPipeCols), kPipeThreads, pipe_smem_bytes(c->N),
                                   s>>>(geo(c), u, v, ru, rv, ubar_t1, vbar_t1, ubar_t2, vbar_t2,
                                        Hz, Akv, z_r, DU, DV, tmpU, tmpV, (float)cff,
                                        (float)lambda, (float)Dt, do_bc, (float)bcval);
+        return cudaGetLastError();
+    }
+    if (c->nmem > 1) {
+        kb_step3d_uv<R><<<c->nbm_128, B, 0, s>>>(mt<R>(c), c->bm_128, u, v, ru, rv, ubar_t1, vbar_t1,
+                                                ubar_t2, vbar_t2, Hz, Akv, z_r, DU, DV, tmpU, tmpV,
+                                                (R)cff, (R)lambda, (R)Dt, do_bc, (R)bcval);
         return cudaGetLastError();
     }
     k_step3d_uv<R><<<blocks_for(c->s2, B), B, 0, s>>>(

@@ -69,6 +69,38 @@ class Grid:
         return g
 
 
+def grid_desc(grid, boundary, precision, keep):
+    """An sf_grid_desc for `grid` and `boundary`; the host arrays it points to are kept alive
+    in the dict `keep`."""
+    B = boundary
+
+    def dp(name, a):
+        keep[name] = _f64(a)
+        return keep[name].ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+    def ip(name, a):
+        keep[name] = _i32(a)
+        return keep[name].ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), int(keep[name].size)
+
+    d = GridDesc()
+    d.L, d.M, d.N, d.precision = grid.L, grid.M, grid.N, DTYPES[precision][0]
+    for k in ("h", "pm", "pn", "on_u", "om_v", "fomn", "sc_r", "sc_w", "Cs_r", "Cs_w"):
+        setattr(d, k, dp(k, getattr(grid, k)))
+    d.hc, d.Vtransform = grid.hc, grid.Vtransform
+    d.zeta_field_idx2 = ip("zf", B.zetaBC.bcIdxFieldIdx2)[0]
+    d.uvel_field_type = ip("ut", B.uvelBC.bcIdxFieldType)[0]
+    d.vvel_field_type = ip("vt", B.vvelBC.bcIdxFieldType)[0]
+    d.zeta_copy_idx1, d.n_zeta_copy = ip("z1", B.zetaClosedOrGradientBCIdx1)
+    d.zeta_copy_idx2 = ip("z2", B.zetaClosedOrGradientBCIdx2)[0]
+    d.ubar_closed_idx, d.n_ubar_closed = ip("uc", B.ubarClosedBCIdx1)
+    d.vbar_closed_idx, d.n_vbar_closed = ip("vc", B.vbarClosedBCIdx1)
+    d.ubar_clamped_idx, d.n_ubar_clamped = ip("ucl", B.ubarClampedBCIdx1)
+    d.ubar_grad_idx1, d.n_ubar_grad = ip("ug1", B.ubarGradientBCIdx1)
+    d.ubar_grad_idx2 = ip("ug2", B.ubarGradientBCIdx2)[0]
+    d.vbar_grad_idx1, d.n_vbar_grad = ip("vg1", B.vbarGradientBCIdx1)
+    return d
+
+
 class Context:
     """An sf_ctx: the grid snapshot and boundary programs on the current CUDA device."""
 
@@ -77,33 +109,8 @@ class Context:
             raise ValueError("precision must be 'fp64' or 'fp32'")
         self.precision = precision
         self.grid = grid
-        B = boundary
         keep = {}
-
-        def dp(name, a):
-            keep[name] = _f64(a)
-            return keep[name].ctypes.data_as(ctypes.POINTER(ctypes.c_double))
-
-        def ip(name, a):
-            keep[name] = _i32(a)
-            return keep[name].ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), int(keep[name].size)
-
-        d = GridDesc()
-        d.L, d.M, d.N, d.precision = grid.L, grid.M, grid.N, DTYPES[precision][0]
-        for k in ("h", "pm", "pn", "on_u", "om_v", "fomn", "sc_r", "sc_w", "Cs_r", "Cs_w"):
-            setattr(d, k, dp(k, getattr(grid, k)))
-        d.hc, d.Vtransform = grid.hc, grid.Vtransform
-        d.zeta_field_idx2 = ip("zf", B.zetaBC.bcIdxFieldIdx2)[0]
-        d.uvel_field_type = ip("ut", B.uvelBC.bcIdxFieldType)[0]
-        d.vvel_field_type = ip("vt", B.vvelBC.bcIdxFieldType)[0]
-        d.zeta_copy_idx1, d.n_zeta_copy = ip("z1", B.zetaClosedOrGradientBCIdx1)
-        d.zeta_copy_idx2 = ip("z2", B.zetaClosedOrGradientBCIdx2)[0]
-        d.ubar_closed_idx, d.n_ubar_closed = ip("uc", B.ubarClosedBCIdx1)
-        d.vbar_closed_idx, d.n_vbar_closed = ip("vc", B.vbarClosedBCIdx1)
-        d.ubar_clamped_idx, d.n_ubar_clamped = ip("ucl", B.ubarClampedBCIdx1)
-        d.ubar_grad_idx1, d.n_ubar_grad = ip("ug1", B.ubarGradientBCIdx1)
-        d.ubar_grad_idx2 = ip("ug2", B.ubarGradientBCIdx2)[0]
-        d.vbar_grad_idx1, d.n_vbar_grad = ip("vg1", B.vbarGradientBCIdx1)
+        d = grid_desc(grid, boundary, precision, keep)
         ptr = ctypes.c_void_p()
         check(lib.sf_ctx_create(ctypes.byref(d), ctypes.byref(ptr)), "sf_ctx_create")
         self.ptr = ptr

@@ -4,9 +4,9 @@
 
 Training data are plain-GLS runs (closure.generate) on a sub-basin of the recipe (same N, dx,
 dt, depth profile): peak wind stress from U[0, 0.3] N/m2 in a random direction, varying
-across the basin as the basins' wind does (cos(pi y / Ly)), stratification scale from
-U[200, 1000] m, wind-driven currents in half of the runs and an ocean at rest under the wind
-in the other half.  Training is on the GPU with the library's own tensor-core kernels.  A
+across the basin as the basins' wind does (cos(pi y / Ly)), the stratification scale varying
+across the basin over [200, 1000] m, wind-driven currents in half of the runs and an ocean at
+rest under the wind in the other half.  Training is on the GPU with the library's own tensor-core kernels.  A
 held-out set of runs with other seeds gives the stated error: log10 RMS of Akv/Akt against
 plain GLS, next to the reference's constant AKv = 1e-3 m2/s (modules/mod_ocean.py:91).
 """
@@ -33,9 +33,9 @@ def train(config, out, runs=16, rest_runs=8, spin=300, every=25, steps=6000, bat
     cfg = RECIPES[config]()
     N = cfg["grid"].N
     X, T = closure.generate(cfg, runs=runs, spin=spin, keep=4, every=every, seed=seed,
-                            rest_runs=rest_runs, pattern=True)
+                            rest_runs=rest_runs, pattern=True, spread=True)
     Xv, Tv = closure.generate(cfg, runs=4, spin=spin, keep=2, every=every, seed=seed + 1000,
-                              rest_runs=2, pattern=True)
+                              rest_runs=2, pattern=True, spread=True)
     net = closure.Network(N, seed=seed)
     net.fit_normalisation(X)
     hist = net.train(X, T, steps=steps, batch=batch, lr=lr, seed=seed, log_every=500)

@@ -151,8 +151,11 @@ def test_trained_network_gains_over_the_method_without_it():
     from sailfish_b200 import closure, configs
     cfg = configs.small(48, 32, 16)
     N = cfg["grid"].N
-    X, T = closure.generate(cfg, runs=6, spin=20, keep=3, every=4, seed=11)
-    Xv, Tv = closure.generate(cfg, runs=2, spin=20, keep=2, every=4, seed=99)
+    # every run spans the wind and stratification ranges across its basin
+    X, T = closure.generate(cfg, runs=6, spin=20, keep=3, every=4, seed=11, pattern=True,
+                            spread=True)
+    Xv, Tv = closure.generate(cfg, runs=2, spin=20, keep=2, every=4, seed=99, pattern=True,
+                              spread=True)
     net = closure.Network(N, seed=0)
     net.fit_normalisation(X)
     Y0 = net.infer(Xv)
