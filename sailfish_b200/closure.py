@@ -130,6 +130,8 @@ def wind_driven_state(model, cols, tau, angle, zscale, rng, current=True, patter
     current decaying over an Ekman-like depth with a basin-scale gyre pattern and seeded
     small-scale noise (none if `current` is False: an ocean at rest under the wind), and the
     stratification of zscale."""
+    if not model._started:
+        model.start()
     g = model.grid
     dev = model.u.device
     dt = model.tdtype
@@ -170,7 +172,10 @@ def wind_driven_state(model, cols, tau, angle, zscale, rng, current=True, patter
 
 def basin_forcing(model, cols, tau0=0.15, zscale=500.0):
     """The analytic basins' forcing for the closure: zonal wind stress tau0 cos(pi y / Ly)
-    (N/m2, kinematic after division by rho0) and the stratification T = 4 + 20 exp(z/zscale)."""
+    (N/m2, kinematic after division by rho0) and the stratification T = 4 + 20 exp(z/zscale)
+    (N^2 from the model's z_w, so the depths are set first)."""
+    if not model._started:
+        model.start()
     g = model.grid
     J = g.J
     y = (torch.arange(J, device=model.u.device, dtype=torch.float64) - 0.5) / max(J - 2, 1)

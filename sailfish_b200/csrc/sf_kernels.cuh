@@ -255,15 +255,36 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int n>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(n)); }
 
+// The staged elements of a thread: e = tid + q*TX*TY, q < kPer; their flat offsets within a
+// level are computed once per block (the division by the staged row length is not repeated
+// for every level and field).
+template <int TX, int TY>
+struct StageMap {
+    static constexpr int kPer = (RhsTile<TX, TY>::SN + TX * TY - 1) / (TX * TY);
+    long rel[kPer];
+    __device__ __forceinline__ StageMap(long I, long j0, long i0, int tid) {
+        using T = RhsTile<TX, TY>;
+#pragma unroll
+        for (int q = 0; q < kPer; ++q) {
+            const int e = tid + q * TX * TY;
+            const int r = e / T::SX - kHY0, c = e % T::SX - kHX0;
+            rel[q] = (j0 + r) * I + (i0 + c);
+        }
+    }
+};
+
 template <typename R, int TX, int TY>
-__device__ __forceinline__ void stage(R *dst, const R *src, long lvl_off, long len, long I, long j0,
-                                      long i0, int tid) {
+__device__ __forceinline__ void stage(R *dst, const R *src, long lvl_off, long len,
+                                      const StageMap<TX, TY> &sm, int tid) {
     using T = RhsTile<TX, TY>;
-    for (int e = tid; e < T::SN; e += TX * TY) {
-        const int r = e / T::SX - kHY0, c = e % T::SX - kHX0;
-        const long f = lvl_off + (j0 + r) * I + (i0 + c);
-        const bool ok = f >= 0 && f < len;
-        cp_async(dst + e, ok ? src + f : src, ok);
+#pragma unroll
+    for (int q = 0; q < StageMap<TX, TY>::kPer; ++q) {
+        const int e = tid + q * TX * TY;
+        if (e < T::SN) {
+            const long f = lvl_off + sm.rel[q];
+            const bool ok = f >= 0 && f < len;
+            cp_async(dst + e, ok ? src + f : src, ok);
+        }
     }
 }
 
@@ -316,15 +337,16 @@ __device__ __forceinline__ void rhs3d_body(const Geo<R> &g, const R *__restrict_
     const R fw = (live && p >= 1) ? g.fomn[p - 1] : R(0);
     const R fs = (live && p >= I) ? g.fomn[p - I] : R(0);
 
+    const StageMap<TX, TY> smap(I, j0, i0, tid);
     auto issue = [&](int K) {
         const long o = (long)K * s2;
         R(*bf)[kSN] = sbuf[K & 1];
-        stage<R, TX, TY>(bf[0], u, o, len3, I, j0, i0, tid);
-        stage<R, TX, TY>(bf[1], v, o, len3, I, j0, i0, tid);
-        stage<R, TX, TY>(bf[2], Huon, o, len3, I, j0, i0, tid);
-        stage<R, TX, TY>(bf[3], Hvom, o, len3, I, j0, i0, tid);
-        stage<R, TX, TY>(bf[4], Hz, o, lenHz, I, j0, i0, tid);
-        stage<R, TX, TY>(bf[5], W, o + s2, len3, I, j0, i0, tid);
+        stage<R, TX, TY>(bf[0], u, o, len3, smap, tid);
+        stage<R, TX, TY>(bf[1], v, o, len3, smap, tid);
+        stage<R, TX, TY>(bf[2], Huon, o, len3, smap, tid);
+        stage<R, TX, TY>(bf[3], Hvom, o, len3, smap, tid);
+        stage<R, TX, TY>(bf[4], Hz, o, lenHz, smap, tid);
+        stage<R, TX, TY>(bf[5], W, o + s2, len3, smap, tid);
         cp_async_commit();
     };
     issue(0);
@@ -505,9 +527,13 @@ __device__ __forceinline__ void maxflux_omega_body(
         const bool uo = rc && un, vo = rc && vn;
         const R onu_e = ue ? g.on_u[p + 1] : R(0), omv_n = vnn ? g.om_v[p + I] : R(0);
         const R onu_p = uo ? g.on_u[p] : R(0), omv_p = vo ? g.om_v[p] : R(0);
-        R Wc[kNMax];
+        // the running integral in shared memory ([level][thread]), not in per-thread local
+        // memory, whose footprint over all resident threads spills out of L1 and L2
+        extern __shared__ __align__(16) unsigned char mo_smem[];
+        R *Wcol = reinterpret_cast<R *>(mo_smem) + threadIdx.x;
+#define Wc(K) Wcol[(K) * (int)blockDim.x]
         R Wk = R(0);
-        Wc[0] = R(0);
+        Wc(0) = R(0);
 #pragma unroll 4
         for (int K = 1; K < N; ++K) {
             const long o = (long)K * s2 + p;
@@ -516,7 +542,7 @@ __device__ __forceinline__ void maxflux_omega_body(
             const R hvn = vnn ? (((Hz[o + I] + Hz[o]) * R(0.5)) * v[o + I]) * omv_n : Hvom[o + I];
             const R hvp = vo ? (((Hz[o] + Hz[o - I]) * R(0.5)) * v[o]) * omv_p : Hvom[o];
             Wk = Wk - ((hue - hup) + (hvn - hvp));
-            Wc[K] = Wk;
+            Wc(K) = Wk;
         }
         const R zbed = z_w[p];
         const R h = z_w[(long)(N - 1) * s2 + p] - zbed;
@@ -525,8 +551,9 @@ __device__ __forceinline__ void maxflux_omega_body(
 #pragma unroll 4
         for (int K = 1; K < N; ++K) {
             const long o = (long)K * s2 + p;
-            W[o] = Wc[K] - (Ws * (z_w[o] - zbed)) / h;
+            W[o] = Wc(K) - (Ws * (z_w[o] - zbed)) / h;
         }
+#undef Wc
         W[(long)N * s2 + p] = R(0);
     }
     if (zeta1 && rnode_(i, j)) {
@@ -938,11 +965,12 @@ __device__ __forceinline__ void step3d_uv_pipe_body(const Geo<R> &g, float *__re
             for (int K = 0; K < N; ++K) v[(long)K * s2 + p] = v[(long)K * s2 + p] - vdiff;
         }
     }
-    if (do_bc && live) {   // each system's thread its own field
+    if (do_bc && live) {   // by the thread that wrote the column's field last
+        const bool uown = sys == 0, vown = both ? sys == 1 : sys == 0;
         const int ut = g.utype[p], vt = g.vtype[p];
-        if (sys == 0 && ut > 0 && (ut & (1 << 4)) == 0 && (ut & (1 << 3)) != 0)
+        if (uown && ut > 0 && (ut & (1 << 4)) == 0 && (ut & (1 << 3)) != 0)
             for (int K = 0; K < N; ++K) u[(long)K * s2 + p] = bcval;
-        if (sys == 1 && vt > 0 && ((vt & (1 << 4)) != 0 || (vt & (1 << 3)) != 0))
+        if (vown && vt > 0 && ((vt & (1 << 4)) != 0 || (vt & (1 << 3)) != 0))
             for (int K = 0; K < N; ++K) v[(long)K * s2 + p] = 0.f;
     }
 }
@@ -1093,15 +1121,15 @@ namespace sf {
 
 template <typename R>
 __global__ void __launch_bounds__(kBlock) k_zeta_rhs(
-    Geo<R> g, const R *zeta, const R *ubar, const R *vbar, R *rzeta, int mode, double cff1,
-    double *Zt, double *DU, double *DV, const R *zeta_t0, R *zeta_t2, R Dt) {
+    Geo<R> g, const R *__restrict__ zeta, const R *__restrict__ ubar, const R *__restrict__ vbar, R *__restrict__ rzeta, int mode, double cff1,
+    double *__restrict__ Zt, double *__restrict__ DU, double *__restrict__ DV, const R *__restrict__ zeta_t0, R *__restrict__ zeta_t2, R Dt) {
     zeta_rhs_body(g, zeta, ubar, vbar, rzeta, mode, cff1, Zt, DU, DV, zeta_t0, zeta_t2, Dt,
                   (long)tid_flat());
 }
 template <typename R>
 __global__ void __launch_bounds__(kBlock) kb_zeta_rhs(
-    const Member<R> *mt, const int2 *bm, const R *zeta, const R *ubar, const R *vbar, R *rzeta,
-    int mode, double cff1, double *Zt, double *DU, double *DV, const R *zeta_t0, R *zeta_t2,
+    const Member<R> *mt, const int2 *bm, const R *__restrict__ zeta, const R *__restrict__ ubar, const R *__restrict__ vbar, R *__restrict__ rzeta,
+    int mode, double cff1, double *__restrict__ Zt, double *__restrict__ DU, double *__restrict__ DV, const R *__restrict__ zeta_t0, R *__restrict__ zeta_t2,
     R Dt) {
     SF_MEMBER(bm)
     zeta_rhs_body(g, O2(zeta), O2(ubar), O2(vbar), O2(rzeta), mode, cff1, O2(Zt), O2(DU), O2(DV),
@@ -1110,17 +1138,17 @@ __global__ void __launch_bounds__(kBlock) kb_zeta_rhs(
 
 template <typename R>
 __global__ void __launch_bounds__(kBlock) k_momentum(
-    Geo<R> g, R *rhs_u, R *rhs_v, const R *za, const R *zb, R grav, R w1, R w, int do_rhs,
-    int do_pred, R Dt, const R *u_t1, R *u_t2, const R *v_t1, R *v_t2, const R *z1,
-    const R *z2) {
+    Geo<R> g, R *__restrict__ rhs_u, R *__restrict__ rhs_v, const R *__restrict__ za, const R *__restrict__ zb, R grav, R w1, R w, int do_rhs,
+    int do_pred, R Dt, const R *__restrict__ u_t1, R *__restrict__ u_t2, const R *__restrict__ v_t1, R *__restrict__ v_t2, const R *__restrict__ z1,
+    const R *__restrict__ z2) {
     momentum_body(g, rhs_u, rhs_v, za, zb, grav, w1, w, do_rhs, do_pred, Dt, u_t1, u_t2, v_t1,
                   v_t2, z1, z2, (long)tid_flat());
 }
 template <typename R>
 __global__ void __launch_bounds__(kBlock) kb_momentum(
-    const Member<R> *mt, const int2 *bm, R *rhs_u, R *rhs_v, const R *za, const R *zb, R grav,
-    R w1, R w, int do_rhs, int do_pred, R Dt, const R *u_t1, R *u_t2, const R *v_t1, R *v_t2,
-    const R *z1, const R *z2) {
+    const Member<R> *mt, const int2 *bm, R *__restrict__ rhs_u, R *__restrict__ rhs_v, const R *__restrict__ za, const R *__restrict__ zb, R grav,
+    R w1, R w, int do_rhs, int do_pred, R Dt, const R *__restrict__ u_t1, R *__restrict__ u_t2, const R *__restrict__ v_t1, R *__restrict__ v_t2,
+    const R *__restrict__ z1, const R *__restrict__ z2) {
     SF_MEMBER(bm)
     momentum_body(g, O2(rhs_u), O2(rhs_v), O2(za), O2(zb), grav, w1, w, do_rhs, do_pred, Dt,
                   O2(u_t1), O2(u_t2), O2(v_t1), O2(v_t2), O2(z1), O2(z2),
@@ -1129,31 +1157,31 @@ __global__ void __launch_bounds__(kBlock) kb_momentum(
 
 template <typename R>
 __global__ void __launch_bounds__(kBlock) k_corr_point(
-    Geo<R> g, R Dt, R *zeta_t2, const R *rz0, const R *rz1, const R *rz2, R *ubar_t1,
-    const R *vbar_t1, const R *rub0, const R *rub1, R *vbar_t2) {
+    Geo<R> g, R Dt, R *__restrict__ zeta_t2, const R *__restrict__ rz0, const R *__restrict__ rz1, const R *__restrict__ rz2, R *__restrict__ ubar_t1,
+    const R *__restrict__ vbar_t1, const R *__restrict__ rub0, const R *__restrict__ rub1, R *__restrict__ vbar_t2) {
     corr_point_body(g, Dt, zeta_t2, rz0, rz1, rz2, ubar_t1, vbar_t1, rub0, rub1, vbar_t2,
                     (long)tid_flat());
 }
 template <typename R>
 __global__ void __launch_bounds__(kBlock) kb_corr_point(
-    const Member<R> *mt, const int2 *bm, R Dt, R *zeta_t2, const R *rz0, const R *rz1,
-    const R *rz2, R *ubar_t1, const R *vbar_t1, const R *rub0, const R *rub1, R *vbar_t2) {
+    const Member<R> *mt, const int2 *bm, R Dt, R *__restrict__ zeta_t2, const R *__restrict__ rz0, const R *__restrict__ rz1,
+    const R *__restrict__ rz2, R *__restrict__ ubar_t1, const R *__restrict__ vbar_t1, const R *__restrict__ rub0, const R *__restrict__ rub1, R *__restrict__ vbar_t2) {
     SF_MEMBER(bm)
     corr_point_body(g, Dt, O2(zeta_t2), O2(rz0), O2(rz1), O2(rz2), O2(ubar_t1), O2(vbar_t1),
                     O2(rub0), O2(rub1), O2(vbar_t2), (long)mb_.y * kBlock + threadIdx.x);
 }
 
 template <typename R, int TX, int TY>
-__global__ void __launch_bounds__(TX *TY) k_rhs3d(Geo<R> g, const R *u, const R *v,
-                                                  const R *Huon, const R *Hvom, const R *W,
-                                                  const R *Hz, R *ru, R *rv) {
+__global__ void __launch_bounds__(TX *TY) k_rhs3d(Geo<R> g, const R *__restrict__ u, const R *__restrict__ v,
+                                                  const R *Huon, const R *Hvom, const R *__restrict__ W,
+                                                  const R *__restrict__ Hz, R *__restrict__ ru, R *__restrict__ rv) {
     rhs3d_body<R, TX, TY>(g, u, v, Huon, Hvom, W, Hz, ru, rv, (int)blockIdx.x, (int)blockIdx.y);
 }
 template <typename R, int TX, int TY>
 __global__ void __launch_bounds__(TX *TY) kb_rhs3d(const Member<R> *mt, const int2 *bm, int var,
-                                                   const R *u, const R *v, const R *Huon,
-                                                   const R *Hvom, const R *W, const R *Hz,
-                                                   R *ru, R *rv) {
+                                                   const R *__restrict__ u, const R *__restrict__ v, const R *Huon,
+                                                   const R *Hvom, const R *__restrict__ W, const R *__restrict__ Hz,
+                                                   R *__restrict__ ru, R *__restrict__ rv) {
     SF_MEMBER(bm)
     const int ntx = M_.ntx[var];
     rhs3d_body<R, TX, TY>(g, O3(u), O3(v), O3(Huon), O3(Hvom), O3(W), ON(Hz), O3(ru), O3(rv),
@@ -1162,45 +1190,45 @@ __global__ void __launch_bounds__(TX *TY) kb_rhs3d(const Member<R> *mt, const in
 
 template <typename R>
 __global__ void __launch_bounds__(kBlock) k_maxflux_omega(
-    Geo<R> g, const R *u, const R *v, R *Huon, R *Hvom, const R *Hz, R *W, const R *z_w,
-    int do_flux, int do_omega, R *zeta1, R *zeta2, const double *Zt) {
+    Geo<R> g, const R *__restrict__ u, const R *__restrict__ v, R *Huon, R *Hvom, const R *__restrict__ Hz, R *__restrict__ W, const R *__restrict__ z_w,
+    int do_flux, int do_omega, R *__restrict__ zeta1, R *__restrict__ zeta2, const double *__restrict__ Zt) {
     maxflux_omega_body(g, u, v, Huon, Hvom, Hz, W, z_w, do_flux, do_omega, zeta1, zeta2, Zt,
                        (long)tid_flat());
 }
 template <typename R>
 __global__ void __launch_bounds__(kBlock) kb_maxflux_omega(
-    const Member<R> *mt, const int2 *bm, const R *u, const R *v, R *Huon, R *Hvom, const R *Hz,
-    R *W, const R *z_w, int do_flux, int do_omega, R *zeta1, R *zeta2, const double *Zt) {
+    const Member<R> *mt, const int2 *bm, const R *__restrict__ u, const R *__restrict__ v, R *Huon, R *Hvom, const R *__restrict__ Hz,
+    R *__restrict__ W, const R *__restrict__ z_w, int do_flux, int do_omega, R *__restrict__ zeta1, R *__restrict__ zeta2, const double *__restrict__ Zt) {
     SF_MEMBER(bm)
     maxflux_omega_body(g, O3(u), O3(v), O3(Huon), O3(Hvom), ON(Hz), O3(W), O3(z_w), do_flux,
                        do_omega, O2(zeta1), O2(zeta2), O2(Zt), (long)mb_.y * kBlock + threadIdx.x);
 }
 
 template <typename R>
-__global__ void __launch_bounds__(kBlock) k_set_depth(Geo<R> g, const double *Zt, R *z_w, R *z_r,
-                                                      R *Hz) {
+__global__ void __launch_bounds__(kBlock) k_set_depth(Geo<R> g, const double *__restrict__ Zt, R *__restrict__ z_w, R *__restrict__ z_r,
+                                                      R *__restrict__ Hz) {
     set_depth_body(g, Zt, z_w, z_r, Hz, (long)tid_flat());
 }
 template <typename R>
 __global__ void __launch_bounds__(kBlock) kb_set_depth(const Member<R> *mt, const int2 *bm,
-                                                       const double *Zt, R *z_w, R *z_r, R *Hz) {
+                                                       const double *__restrict__ Zt, R *__restrict__ z_w, R *__restrict__ z_r, R *__restrict__ Hz) {
     SF_MEMBER(bm)
     set_depth_body(g, O2(Zt), O3(z_w), ON(z_r), ON(Hz), (long)mb_.y * kBlock + threadIdx.x);
 }
 
 template <typename R>
 __global__ void __launch_bounds__(128) k_step3d_uv(
-    Geo<R> g, R *u, R *v, const R *ru, const R *rv, R *ubar_t1, R *vbar_t1, R *ubar_t2,
-    R *vbar_t2, const R *Hz, const R *Akv, const R *z_r, const double *DU, const double *DV,
+    Geo<R> g, R *__restrict__ u, R *__restrict__ v, const R *__restrict__ ru, const R *__restrict__ rv, R *__restrict__ ubar_t1, R *__restrict__ vbar_t1, R *__restrict__ ubar_t2,
+    R *__restrict__ vbar_t2, const R *__restrict__ Hz, const R *__restrict__ Akv, const R *__restrict__ z_r, const double *__restrict__ DU, const double *__restrict__ DV,
     const R *tmpU, const R *tmpV, R cff, R lambda, R Dt, int do_bc, R bcval) {
     step3d_uv_body(g, u, v, ru, rv, ubar_t1, vbar_t1, ubar_t2, vbar_t2, Hz, Akv, z_r, DU, DV,
                    tmpU, tmpV, cff, lambda, Dt, do_bc, bcval, (long)tid_flat());
 }
 template <typename R>
 __global__ void __launch_bounds__(128) kb_step3d_uv(
-    const Member<R> *mt, const int2 *bm, R *u, R *v, const R *ru, const R *rv, R *ubar_t1,
-    R *vbar_t1, R *ubar_t2, R *vbar_t2, const R *Hz, const R *Akv, const R *z_r,
-    const double *DU, const double *DV, const R *tmpU, const R *tmpV, R cff, R lambda, R Dt,
+    const Member<R> *mt, const int2 *bm, R *__restrict__ u, R *__restrict__ v, const R *__restrict__ ru, const R *__restrict__ rv, R *__restrict__ ubar_t1,
+    R *__restrict__ vbar_t1, R *__restrict__ ubar_t2, R *__restrict__ vbar_t2, const R *__restrict__ Hz, const R *__restrict__ Akv, const R *__restrict__ z_r,
+    const double *__restrict__ DU, const double *__restrict__ DV, const R *tmpU, const R *tmpV, R cff, R lambda, R Dt,
     int do_bc, R bcval) {
     SF_MEMBER(bm)
     step3d_uv_body(g, O3(u), O3(v), O3(ru), O3(rv), O2(ubar_t1), O2(vbar_t1), O2(ubar_t2),
@@ -1210,18 +1238,18 @@ __global__ void __launch_bounds__(128) kb_step3d_uv(
 
 template <typename R>
 __global__ void __launch_bounds__(kPipeThreads) k_step3d_uv_pipe(
-    Geo<R> g, float *u, float *v, const float *ru, const float *rv, float *ubar_t1,
-    float *vbar_t1, float *ubar_t2, float *vbar_t2, const float *Hz, const float *Akv,
-    const float *z_r, const double *DU, const double *DV, const float *tmpU, const float *tmpV,
+    Geo<R> g, float *__restrict__ u, float *__restrict__ v, const float *__restrict__ ru, const float *__restrict__ rv, float *__restrict__ ubar_t1,
+    float *__restrict__ vbar_t1, float *__restrict__ ubar_t2, float *__restrict__ vbar_t2, const float *__restrict__ Hz, const float *__restrict__ Akv,
+    const float *__restrict__ z_r, const double *__restrict__ DU, const double *__restrict__ DV, const float *tmpU, const float *tmpV,
     float cff, float lambda, float Dt, int do_bc, float bcval) {
     step3d_uv_pipe_body(g, u, v, ru, rv, ubar_t1, vbar_t1, ubar_t2, vbar_t2, Hz, Akv, z_r, DU, DV,
                         tmpU, tmpV, cff, lambda, Dt, do_bc, bcval, (long)blockIdx.x);
 }
 template <typename R>
 __global__ void __launch_bounds__(kPipeThreads) kb_step3d_uv_pipe(
-    const Member<R> *mt, const int2 *bm, float *u, float *v, const float *ru, const float *rv,
-    float *ubar_t1, float *vbar_t1, float *ubar_t2, float *vbar_t2, const float *Hz,
-    const float *Akv, const float *z_r, const double *DU, const double *DV, const float *tmpU,
+    const Member<R> *mt, const int2 *bm, float *__restrict__ u, float *__restrict__ v, const float *__restrict__ ru, const float *__restrict__ rv,
+    float *__restrict__ ubar_t1, float *__restrict__ vbar_t1, float *__restrict__ ubar_t2, float *__restrict__ vbar_t2, const float *__restrict__ Hz,
+    const float *__restrict__ Akv, const float *__restrict__ z_r, const double *__restrict__ DU, const double *__restrict__ DV, const float *tmpU,
     const float *tmpV, float cff, float lambda, float Dt, int do_bc, float bcval) {
     SF_MEMBER(bm)
     step3d_uv_pipe_body(g, O3(u), O3(v), O3(ru), O3(rv), O2(ubar_t1), O2(vbar_t1), O2(ubar_t2),
@@ -1382,12 +1410,23 @@ template <typename R>
 cudaError_t Ops<R>::maxflux_omega(const sf_ctx *c, const R *u, const R *v, R *Huon, R *Hvom,
                                   const R *Hz, R *W, const R *z_w, int do_flux, int do_omega,
                                   R *zeta1, R *zeta2, const double *Zt, cudaStream_t s) {
+    const size_t smem = do_omega ? sizeof(R) * (size_t)kBlock * (c->nmem > 1 ? c->maxN : c->N) : 0;
+    static bool attr_set[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+        const int most = (int)(sizeof(R) * kBlock * kNMax);
+        cudaFuncSetAttribute(k_maxflux_omega<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
+        cudaFuncSetAttribute(kb_maxflux_omega<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
+        attr_set[dev] = true;
+    }
     if (c->nmem > 1) {
-        kb_maxflux_omega<R><<<c->nbm_pt, kBlock, 0, s>>>(mt<R>(c), c->bm_pt, u, v, Huon, Hvom, Hz, W,
-                                                        z_w, do_flux, do_omega, zeta1, zeta2, Zt);
+        kb_maxflux_omega<R><<<c->nbm_pt, kBlock, smem, s>>>(mt<R>(c), c->bm_pt, u, v, Huon, Hvom, Hz,
+                                                           W, z_w, do_flux, do_omega, zeta1, zeta2,
+                                                           Zt);
         return cudaGetLastError();
     }
-    k_maxflux_omega<R><<<blocks_for(c->s2, kBlock), kBlock, 0, s>>>(
+    k_maxflux_omega<R><<<blocks_for(c->s2, kBlock), kBlock, smem, s>>>(
         geo(c), u, v, Huon, Hvom, Hz, W, z_w, do_flux, do_omega, zeta1, zeta2, Zt);
     return cudaGetLastError();
 }
