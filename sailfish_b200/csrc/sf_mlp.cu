@@ -130,6 +130,12 @@ struct Mat {
     }
 };
 
+// The closure's feature and output maps use the hardware approximations (relative error
+// ~2^-21, far below the BF16 rounding of the network's operands); features for training and
+// for inference go through the same functions.
+__device__ __forceinline__ float flog10(float x) { return __log10f(x); }
+__device__ __forceinline__ float fexp10(float x) { return __exp10f(x); }
+
 __device__ __forceinline__ float gelu(float x) {   // tanh form of the GELU
     const float c = 0.7978845608028654f;           // sqrt(2/pi)
     return 0.5f * x * (1.f + tanhf(c * (x + 0.044715f * x * x * x)));
@@ -295,8 +301,8 @@ __device__ __forceinline__ void store_act8x4(__nv_bfloat16 *sA, int r, int n0, c
 #pragma unroll
         for (int h = 0; h < 4; ++h) {
             const int k = 8 * q + 2 * h;
-            const __nv_bfloat162 b2 = __floats2bfloat162_rn(gelu_fast(v[k] + bias[n0 + k]),
-                                                            gelu_fast(v[k + 1] + bias[n0 + k + 1]));
+            const float b0 = bias ? bias[n0 + k] : 0.f, b1 = bias ? bias[n0 + k + 1] : 0.f;
+            const __nv_bfloat162 b2 = __floats2bfloat162_rn(gelu_fast(v[k] + b0), gelu_fast(v[k + 1] + b1));
             pk[h] = *reinterpret_cast<const uint32_t *>(&b2);
         }
         *reinterpret_cast<uint4 *>(&sA[cm_index(r, n0 + 8 * q)]) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
@@ -455,13 +461,13 @@ __global__ void k_features(Geo<R> g, const R *__restrict__ u, const R *__restric
         const float dv = (AT(v, k, p) - AT(v, k - 1, p)) + (AT(v, k, p + I) - AT(v, k - 1, p + I));
         const float sh2 = (cff * du) * (cff * du) + (cff * dv) * (cff * dv);
         const float n2 = AT(bvf, k, p);
-        x[k - 1] = log10f(sh2 + 1e-12f);
-        x[nl + k - 1] = copysignf(log10f(1.f + fabsf(n2) * 1e8f), n2);
+        x[k - 1] = flog10(sh2 + 1e-12f);
+        x[nl + k - 1] = copysignf(flog10(1.f + fabsf(n2) * 1e8f), n2);
     }
     const float su = (float)(sustr[p] + sustr[p + 1]), sv = (float)(svstr[p] + svstr[p + I]);
-    x[2 * nl] = log10f(0.5f * sqrtf(su * su + sv * sv) + 1e-10f);
+    x[2 * nl] = flog10(0.5f * sqrtf(su * su + sv * sv) + 1e-10f);
     x[2 * nl + 1] = 0.f;
-    x[2 * nl + 2] = log10f((float)g.hd[p]);
+    x[2 * nl + 2] = flog10((float)g.hd[p]);
 #undef AT
 }
 
@@ -479,8 +485,8 @@ __global__ void k_apply(Geo<R> g, const float *__restrict__ Y, const uint8_t *__
     const float *y = Y + p * kTile;
     const int nl = g.N - 1;
     for (int k = 1; k < g.N; ++k) {
-        Akv[(long)k * s2 + p] = (R)exp10f(fminf(fmaxf(y[k - 1], -6.f), -1.f));
-        Akt[(long)k * s2 + p] = (R)exp10f(fminf(fmaxf(y[nl + k - 1], -6.f), -1.f));
+        Akv[(long)k * s2 + p] = (R)fexp10(fminf(fmaxf(y[k - 1], -6.f), -1.f));
+        Akt[(long)k * s2 + p] = (R)fexp10(fminf(fmaxf(y[nl + k - 1], -6.f), -1.f));
     }
 }
 
@@ -519,40 +525,24 @@ __global__ void __launch_bounds__(128) k_closure_rows(Geo<R> g, const R *__restr
         vbn = AT(v, 0, p + I);
     }
     int ks = 1;   // next shear level
-    for (int f0 = 0; f0 < kTile; f0 += 8) {
-        float x[8];
-#pragma unroll
-        for (int h = 0; h < 8; ++h) {
-            const int f = f0 + h;
-            float val = 0.f;
-            if (col) {
-                if (f < nl) {                       // shear^2 at W level ks = f + 1
-                    const int k = ks++;
-                    const float zt = AT(z_r, k, p), ut = AT(u, k, p), ute = AT(u, k, p + 1);
-                    const float vt = AT(v, k, p), vtn = AT(v, k, p + I);
-                    const float cff = 0.5f / (zt - zb);
-                    const float du = (ut - ub) + (ute - ube), dv = (vt - vb) + (vtn - vbn);
-                    const float sh2 = (cff * du) * (cff * du) + (cff * dv) * (cff * dv);
-                    val = log10f(sh2 + 1e-12f);
-                    zb = zt;
-                    ub = ut;
-                    ube = ute;
-                    vb = vt;
-                    vbn = vtn;
-                } else if (f < 2 * nl) {
-                    const float n2 = AT(bvf, f - nl + 1, p);
-                    val = copysignf(log10f(1.f + fabsf(n2) * 1e8f), n2);
-                } else if (f == 2 * nl) {
-                    const float su = (float)(sustr[p] + sustr[p + 1]);
-                    const float sv = (float)(svstr[p] + svstr[p + I]);
-                    val = log10f(0.5f * sqrtf(su * su + sv * sv) + 1e-10f);
-                } else if (f == 2 * nl + 2) {
-                    val = log10f((float)g.hd[p]);
-                }
-                if (f < nfeat && !(val >= lo[f] && val <= hi[f])) out = true;
-            }
-            x[h] = val;
-        }
+    auto shear = [&](int k) {   // feature of W level k, carrying level k into the registers
+        const float zt = AT(z_r, k, p), ut = AT(u, k, p), ute = AT(u, k, p + 1);
+        const float vt = AT(v, k, p), vtn = AT(v, k, p + I);
+        const float cff = 0.5f / (zt - zb);
+        const float du = (ut - ub) + (ute - ube), dv = (vt - vb) + (vtn - vbn);
+        const float sh2 = (cff * du) * (cff * du) + (cff * dv) * (cff * dv);
+        zb = zt;
+        ub = ut;
+        ube = ute;
+        vb = vt;
+        vbn = vtn;
+        return flog10(sh2 + 1e-12f);
+    };
+    auto n2f = [&](int k) {
+        const float n2 = AT(bvf, k, p);
+        return copysignf(flog10(1.f + fabsf(n2) * 1e8f), n2);
+    };
+    auto put8 = [&](int f0, const float *x) {
         uint32_t pk[4];
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
@@ -560,6 +550,52 @@ __global__ void __launch_bounds__(128) k_closure_rows(Geo<R> g, const R *__restr
             pk[q] = *reinterpret_cast<const uint32_t *>(&b2);
         }
         *reinterpret_cast<uint4 *>(tile + cm_index(r, f0)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+    };
+    auto check8 = [&](int f0, const float *x) {
+#pragma unroll
+        for (int h = 0; h < 8; ++h) {
+            const int f = f0 + h;
+            if (f < nfeat && !(x[h] >= lo[f] && x[h] <= hi[f])) out = true;
+        }
+    };
+    int f0 = 0;
+    if (col) {   // whole groups of 8 shear features (straight-line: the loads can be hoisted)
+        for (; f0 + 8 <= nl; f0 += 8) {
+            float x[8];
+#pragma unroll
+            for (int h = 0; h < 8; ++h) x[h] = shear(ks++);
+            check8(f0, x);
+            put8(f0, x);
+        }
+    }
+    for (; f0 < kTile; f0 += 8) {
+        float x[8];
+        if (col && f0 >= nl && f0 + 8 <= 2 * nl) {   // whole groups of 8 N^2 features
+#pragma unroll
+            for (int h = 0; h < 8; ++h) x[h] = n2f(f0 + h - nl + 1);
+        } else {
+#pragma unroll
+            for (int h = 0; h < 8; ++h) {
+                const int f = f0 + h;
+                float val = 0.f;
+                if (col) {
+                    if (f < nl) {
+                        val = shear(ks++);
+                    } else if (f < 2 * nl) {
+                        val = n2f(f - nl + 1);
+                    } else if (f == 2 * nl) {
+                        const float su = (float)(sustr[p] + sustr[p + 1]);
+                        const float sv = (float)(svstr[p] + svstr[p + I]);
+                        val = flog10(0.5f * sqrtf(su * su + sv * sv) + 1e-10f);
+                    } else if (f == 2 * nl + 2) {
+                        val = flog10((float)g.hd[p]);
+                    }
+                }
+                x[h] = val;
+            }
+        }
+        if (col) check8(f0, x);
+        put8(f0, x);
     }
 #undef AT
     if (p < s2) {
@@ -578,8 +614,13 @@ __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t b
         : "memory");
 }
 
+// 16 warps: warp w reads TMEM lanes 32(w%4).. (its rows) and columns 32(w/4).. (its outputs),
+// so each thread takes 32 outputs of a row per layer and four warps share each scheduler.
+constexpr int kClosureThreads = 512;
+constexpr size_t kClosureSmem = (size_t)(1 + SF_MLP_LAYERS) * kTile * kTile * 2;
+
 template <typename R>
-__global__ void __launch_bounds__(kInferThreads, 1) k_closure_mlp(Geo<R> g, InferW w,
+__global__ void __launch_bounds__(kClosureThreads, 1) k_closure_mlp(Geo<R> g, InferW w,
         const __nv_bfloat16 *__restrict__ Xt, long ntiles, const uint8_t *__restrict__ fallback,
         R *__restrict__ Akv, R *__restrict__ Akt, int *err) {
     extern __shared__ __align__(1024) unsigned char dsm[];
@@ -601,16 +642,16 @@ __global__ void __launch_bounds__(kInferThreads, 1) k_closure_mlp(Geo<R> g, Infe
             bulk_load(sA, Xt + (long)blockIdx.x * kTile * kTile, kTile * kTile * 2, &xbar);
     }
     for (int l = 0; l < SF_MLP_LAYERS; ++l) {
-        for (int e = tid; e < kTile * kTile; e += kInferThreads)
+        for (int e = tid; e < kTile * kTile; e += kClosureThreads)
             sW[l * kTile * kTile + cm_index(e >> 7, e & 127)] = w.W[l][e];
-        for (int e = tid; e < kTile; e += kInferThreads) sbias[l][e] = w.b[l] ? w.b[l][e] : 0.f;
+        for (int e = tid; e < kTile; e += kClosureThreads) sbias[l][e] = w.b[l] ? w.b[l][e] : 0.f;
     }
     fence_before();
     __syncthreads();
     fence_after();
     const uint32_t tmem = tmem_base;
     const int rl = (warp & 3) * 32 + lane;
-    const int cb = (warp >> 2) * 64;
+    const int n0 = (warp >> 2) * 32;
     const uint32_t trow = (uint32_t)((warp & 3) * 32) << 16;
     uint32_t phase = 0, xphase = 0;
     bool ok = true;
@@ -624,6 +665,9 @@ __global__ void __launch_bounds__(kInferThreads, 1) k_closure_mlp(Geo<R> g, Infe
                 break;
             }
         }
+        const long p = m0 + rl;
+        const bool inrow = p < s2 && column_((int)(p % g.I), (int)(p / g.I), g.I, g.J);
+        const bool apply = inrow && !fallback[p];
         for (int l = 0; l < SF_MLP_LAYERS; ++l) {
             fence_proxy_async();
             __syncthreads();
@@ -645,35 +689,31 @@ __global__ void __launch_bounds__(kInferThreads, 1) k_closure_mlp(Geo<R> g, Infe
             const bool last = l == SF_MLP_LAYERS - 1;
             if (last && tid == 0 && t + gridDim.x < ntiles)   // the products have read sA
                 bulk_load(sA, Xt + (t + gridDim.x) * kTile * kTile, kTile * kTile * 2, &xbar);
-            const long p = m0 + rl;
-            const bool apply = last && p < s2 &&
-                               column_((int)(p % g.I), (int)(p / g.I), g.I, g.J) && !fallback[p];
-            for (int c = 0; c < 2; ++c) {
-                float vv[32];
-                tmem_ld32(tmem + trow + cb + c * 32, vv);
-                const int n0 = cb + c * 32;
-                if (!last) {
-                    store_act8x4(sA, rl, n0, vv, sbias[l]);
-                } else if (apply) {
+            float vv[32];
+            tmem_ld32(tmem + trow + n0, vv);
+            if (!last) {
+                store_act8x4(sA, rl, n0, vv, sbias[l]);
+            } else if (apply) {
 #pragma unroll 8
-                    for (int k = 0; k < 32; ++k) {
-                        const int n = n0 + k;
-                        const float y = exp10f(fminf(fmaxf(vv[k] + sbias[l][n], -6.f), -1.f));
-                        if (n < nl) Akv[(long)(n + 1) * s2 + p] = (R)y;
-                        else if (n < 2 * nl) Akt[(long)(n - nl + 1) * s2 + p] = (R)y;
-                    }
+                for (int k = 0; k < 32; ++k) {
+                    const int n = n0 + k;
+                    const float y = fexp10(fminf(fmaxf(vv[k] + sbias[l][n], -6.f), -1.f));
+                    if (n < nl) Akv[(long)(n + 1) * s2 + p] = (R)y;
+                    else if (n < 2 * nl) Akt[(long)(n - nl + 1) * s2 + p] = (R)y;
                 }
             }
             fence_before();
         }
     }
-    if (!ok && tid == 0) atomicExch(err, 1);
-    // an operand copy still in flight (only after a failed wait) is waited for, with a bound
-    if (!ok && tid == 0) (void)mbar_wait(&xbar, xphase);
+    if (!ok && tid == 0) {
+        atomicExch(err, 1);
+        (void)mbar_wait(&xbar, xphase);   // an operand copy in flight, bounded
+    }
     fence_before();
     __syncthreads();
     if (warp == 0) tmem_dealloc(tmem);
 }
+
 }  // namespace mlp
 }  // namespace sf
 
@@ -888,10 +928,10 @@ int sf_closure_step(sf_ctx *c, const sf_mlp_params *w, const void *u, const void
     if (dev >= 0 && dev < 64 && !attr_set[pi][dev]) {
         e = pi ? cudaFuncSetAttribute(sf::mlp::k_closure_mlp<double>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)sf::mlp::kInferSmem)
+                                      (int)sf::mlp::kClosureSmem)
                : cudaFuncSetAttribute(sf::mlp::k_closure_mlp<float>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)sf::mlp::kInferSmem);
+                                      (int)sf::mlp::kClosureSmem);
         if (e != cudaSuccess) return mcuda(e, "cudaFuncSetAttribute");
         attr_set[pi][dev] = true;
     }
@@ -910,7 +950,7 @@ int sf_closure_step(sf_ctx *c, const sf_mlp_params *w, const void *u, const void
             g, (const double *)u, (const double *)v, (const double *)z_r, (const double *)bvf,
             (const double *)sustr, (const double *)svstr, nfeat, lo, hi, fallback, fallback_list,
             fallback_count, X, nrows);
-        sf::mlp::k_closure_mlp<double><<<grid, sf::mlp::kInferThreads, sf::mlp::kInferSmem, S(s)>>>(
+        sf::mlp::k_closure_mlp<double><<<grid, sf::mlp::kClosureThreads, sf::mlp::kClosureSmem, S(s)>>>(
             g, iw, X, tiles, fallback, (double *)Akv, (double *)Akt, err);
     } else {
         auto g = sf::Ops<float>::geo(c);
@@ -918,7 +958,7 @@ int sf_closure_step(sf_ctx *c, const sf_mlp_params *w, const void *u, const void
             g, (const float *)u, (const float *)v, (const float *)z_r, (const float *)bvf,
             (const float *)sustr, (const float *)svstr, nfeat, lo, hi, fallback, fallback_list,
             fallback_count, X, nrows);
-        sf::mlp::k_closure_mlp<float><<<grid, sf::mlp::kInferThreads, sf::mlp::kInferSmem, S(s)>>>(
+        sf::mlp::k_closure_mlp<float><<<grid, sf::mlp::kClosureThreads, sf::mlp::kClosureSmem, S(s)>>>(
             g, iw, X, tiles, fallback, (float *)Akv, (float *)Akt, err);
     }
     e = cudaGetLastError();
