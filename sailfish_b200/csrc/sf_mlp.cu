@@ -616,30 +616,51 @@ __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t b
 
 // 16 warps: warp w reads TMEM lanes 32(w%4).. (its rows) and columns 32(w/4).. (its outputs),
 // so each thread takes 32 outputs of a row per layer and four warps share each scheduler.
+// Two tiles are in flight: tile A's epilogue of layer l runs while the tensor cores compute
+// tile B's layer l and the other way round (two operand buffers, two TMEM accumulators of 128
+// columns), so the products hide behind the epilogues.
 constexpr int kClosureThreads = 512;
-constexpr size_t kClosureSmem = (size_t)(1 + SF_MLP_LAYERS) * kTile * kTile * 2;
+constexpr size_t kClosureSmem = (size_t)(2 + SF_MLP_LAYERS) * kTile * kTile * 2;
+constexpr uint32_t kTmemCols2 = 256;
+
+__device__ __forceinline__ void tmem_alloc256(uint32_t *dst_smem) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(dst_smem)),
+                 "r"(kTmemCols2));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+}
+__device__ __forceinline__ void tmem_dealloc256(uint32_t taddr) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(kTmemCols2));
+}
 
 template <typename R>
 __global__ void __launch_bounds__(kClosureThreads, 1) k_closure_mlp(Geo<R> g, InferW w,
         const __nv_bfloat16 *__restrict__ Xt, long ntiles, const uint8_t *__restrict__ fallback,
         R *__restrict__ Akv, R *__restrict__ Akt, int *err) {
     extern __shared__ __align__(1024) unsigned char dsm[];
-    __nv_bfloat16 *sA = reinterpret_cast<__nv_bfloat16 *>(dsm);
-    __nv_bfloat16 *sW = sA + kTile * kTile;
-    __shared__ __align__(8) uint64_t mbar, xbar;
+    __nv_bfloat16 *const sA0 = reinterpret_cast<__nv_bfloat16 *>(dsm);
+    __nv_bfloat16 *const sA1 = sA0 + kTile * kTile;
+    __nv_bfloat16 *const sW = sA1 + kTile * kTile;
+    __shared__ __align__(8) uint64_t mbar[2], xbar[2];
     __shared__ uint32_t tmem_base;
     __shared__ float sbias[SF_MLP_LAYERS][kTile];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int nl = g.N - 1;
-    const long s2 = g.s2;
-    if (warp == 0) tmem_alloc(&tmem_base);
+    const long s2 = g.s2, G = gridDim.x;
+    // this CTA's tiles are blockIdx.x + G*q; pair pq holds q = 2pq (slot 0) and 2pq + 1 (slot 1)
+    auto tile_of = [&](long q) { return (long)blockIdx.x + G * q; };
+    auto buf = [&](int b) { return b ? sA1 : sA0; };
+    if (warp == 0) tmem_alloc256(&tmem_base);
     if (tid == 0) {
-        mbar_init(&mbar);
-        mbar_init(&xbar);
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&mbar[b]);
+            mbar_init(&xbar[b]);
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::);
         fence_proxy_async();
-        if ((long)blockIdx.x < ntiles)     // the first tile's operand, while the weights load
-            bulk_load(sA, Xt + (long)blockIdx.x * kTile * kTile, kTile * kTile * 2, &xbar);
+        for (int b = 0; b < 2; ++b)   // the first pair's operands, while the weights load
+            if (tile_of(b) < ntiles)
+                bulk_load(buf(b), Xt + tile_of(b) * kTile * kTile, kTile * kTile * 2, &xbar[b]);
     }
     for (int l = 0; l < SF_MLP_LAYERS; ++l) {
         for (int e = tid; e < kTile * kTile; e += kClosureThreads)
@@ -653,65 +674,91 @@ __global__ void __launch_bounds__(kClosureThreads, 1) k_closure_mlp(Geo<R> g, In
     const int rl = (warp & 3) * 32 + lane;
     const int n0 = (warp >> 2) * 32;
     const uint32_t trow = (uint32_t)((warp & 3) * 32) << 16;
-    uint32_t phase = 0, xphase = 0;
+    uint32_t ph[2] = {0, 0}, xph[2] = {0, 0};
     bool ok = true;
-    for (long t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
-        const long m0 = t * kTile;
-        {   // this tile's operand has landed (bounded wait)
-            const bool got = mbar_wait(&xbar, xphase);
-            xphase ^= 1;
+    auto issue_mma = [&](int b, int l) {   // thread 0: slot b's layer l into accumulator b
+        fence_after();
+        const uint32_t a0 = smem_u32(buf(b)), b0 = smem_u32(sW + l * kTile * kTile);
+        for (int q = 0; q < kTile / 16; ++q)
+            mma_bf16(tmem + (uint32_t)(b * kTile), sdesc(a0 + q * 256, kLBO, kSBO),
+                     sdesc(b0 + q * 256, kLBO, kSBO), q > 0 ? 1u : 0u);
+        mma_commit(&mbar[b]);
+    };
+    for (long pq = 0; tile_of(2 * pq) < ntiles && ok; ++pq) {
+        const long t0 = tile_of(2 * pq), t1 = tile_of(2 * pq + 1);
+        const bool has1 = t1 < ntiles;
+        {   // operands landed (bounded waits)
+            bool got = mbar_wait(&xbar[0], xph[0]);
+            xph[0] ^= 1;
+            if (has1) {
+                got = mbar_wait(&xbar[1], xph[1]) && got;
+                xph[1] ^= 1;
+            }
             if (__syncthreads_or(!got)) {
                 ok = false;
                 break;
             }
         }
-        const long p = m0 + rl;
-        const bool inrow = p < s2 && column_((int)(p % g.I), (int)(p / g.I), g.I, g.J);
-        const bool apply = inrow && !fallback[p];
-        for (int l = 0; l < SF_MLP_LAYERS; ++l) {
-            fence_proxy_async();
-            __syncthreads();
-            if (tid == 0) {
-                fence_after();
-                const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sW + l * kTile * kTile);
-                for (int q = 0; q < kTile / 16; ++q)
-                    mma_bf16(tmem, sdesc(a0 + q * 256, kLBO, kSBO), sdesc(b0 + q * 256, kLBO, kSBO),
-                             q > 0 ? 1u : 0u);
-                mma_commit(&mbar);
-            }
-            const bool done = mbar_wait(&mbar, phase);
-            phase ^= 1;
-            fence_after();
-            if (__syncthreads_or(!done)) {
-                ok = false;
-                break;
-            }
+        fence_proxy_async();
+        __syncthreads();
+        if (tid == 0) {
+            issue_mma(0, 0);
+            if (has1) issue_mma(1, 0);
+        }
+        long pr[2];
+        bool apply[2];
+        for (int b = 0; b < 2; ++b) {
+            const long p = (b ? t1 : t0) * kTile + rl;
+            pr[b] = p;
+            apply[b] = (b == 0 || has1) && p < s2 &&
+                       column_((int)(p % g.I), (int)(p / g.I), g.I, g.J) && !fallback[p];
+        }
+        for (int l = 0; l < SF_MLP_LAYERS && ok; ++l) {
             const bool last = l == SF_MLP_LAYERS - 1;
-            if (last && tid == 0 && t + gridDim.x < ntiles)   // the products have read sA
-                bulk_load(sA, Xt + (t + gridDim.x) * kTile * kTile, kTile * kTile * 2, &xbar);
-            float vv[32];
-            tmem_ld32(tmem + trow + n0, vv);
-            if (!last) {
-                store_act8x4(sA, rl, n0, vv, sbias[l]);
-            } else if (apply) {
+            for (int b = 0; b < 2; ++b) {
+                if (b == 1 && !has1) continue;
+                const bool done = mbar_wait(&mbar[b], ph[b]);
+                ph[b] ^= 1;
+                fence_after();
+                if (__syncthreads_or(!done)) {
+                    ok = false;
+                    break;
+                }
+                if (last && tid == 0) {   // the products have read this operand: refill it
+                    const long nt = tile_of(2 * (pq + 1) + b);
+                    if (nt < ntiles) bulk_load(buf(b), Xt + nt * kTile * kTile, kTile * kTile * 2, &xbar[b]);
+                }
+                float vv[32];
+                tmem_ld32(tmem + (uint32_t)(b * kTile) + trow + n0, vv);
+                if (!last) {
+                    store_act8x4(buf(b), rl, n0, vv, sbias[l]);
+                    fence_before();
+                    fence_proxy_async();
+                    __syncthreads();
+                    if (tid == 0) issue_mma(b, l + 1);   // overlaps the other slot's epilogue
+                } else if (apply[b]) {
+                    const long p = pr[b];
 #pragma unroll 8
-                for (int k = 0; k < 32; ++k) {
-                    const int n = n0 + k;
-                    const float y = fexp10(fminf(fmaxf(vv[k] + sbias[l][n], -6.f), -1.f));
-                    if (n < nl) Akv[(long)(n + 1) * s2 + p] = (R)y;
-                    else if (n < 2 * nl) Akt[(long)(n - nl + 1) * s2 + p] = (R)y;
+                    for (int k = 0; k < 32; ++k) {
+                        const int n = n0 + k;
+                        const float y = fexp10(fminf(fmaxf(vv[k] + sbias[l][n], -6.f), -1.f));
+                        if (n < nl) Akv[(long)(n + 1) * s2 + p] = (R)y;
+                        else if (n < 2 * nl) Akt[(long)(n - nl + 1) * s2 + p] = (R)y;
+                    }
+                    fence_before();
+                } else {
+                    fence_before();
                 }
             }
-            fence_before();
         }
     }
     if (!ok && tid == 0) {
         atomicExch(err, 1);
-        (void)mbar_wait(&xbar, xphase);   // an operand copy in flight, bounded
+        for (int b = 0; b < 2; ++b) (void)mbar_wait(&xbar[b], xph[b]);   // bounded
     }
     fence_before();
     __syncthreads();
-    if (warp == 0) tmem_dealloc(tmem);
+    if (warp == 0) tmem_dealloc256(tmem);
 }
 
 }  // namespace mlp
