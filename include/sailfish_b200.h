@@ -220,12 +220,37 @@ int sf_gls_corrector(sf_ctx *ctx, const sf_gls_params *params, double dt, const 
  * and fourth-order vertical advection (:162-208) — into tke_aux/gls_aux (time level 3) with
  * the half-step box height Hz_half; tke_nnew/gls_nnew = Hz_w * tke/gls(nstp) (:153-154).  A
  * zero-gradient lateral condition is applied to the auxiliary level (tkebc_tile is not in the
- * reference; edges take the adjacent interior value, corners the diagonal one).  Huon, Hvom:
+ * reference; edges take the adjacent interior value, corners the diagonal one); its levels 0
+ * and N take the nstp values at the interior points (the corrector's vertical fluxes read
+ * them, gls_corrector_step.py:349-372).  Huon, Hvom:
  * U/V fluxes at rho levels (N used); W, tke*, gls*, Hz_half: N+1 W levels; Hz: N levels. */
 int sf_gls_predictor(sf_ctx *ctx, double dt, int first_step, const void *Huon, const void *Hvom,
                      const void *W, const void *Hz, const void *tke_nstp, const void *tke_indx,
                      void *tke_aux, void *tke_nnew, const void *gls_nstp, const void *gls_indx,
                      void *gls_aux, void *gls_nnew, void *Hz_half, sf_stream stream);
+/* GLS corrector's advective terms, nonlinear/gls_corrector_step.py:172-388 (ROMS pseudo-code in
+ * the reference): tke_nnew/gls_nnew (the Hz_w-weighted new level from sf_gls_predictor) less
+ * dt*pm*pn times the horizontal divergence of third-order upstream-biased fluxes of the
+ * auxiliary level tke_aux/gls_aux (:181-298), floored at params->Kmin/Pmin (:300-317), then less
+ * the fourth-order vertical flux divergence (:329-377) and floored again (:378-388); W levels
+ * 1..N-1 on the rho-interior points, in place.  gadv weighs the upstream curvature term; the
+ * reference's pseudo-code uses Gadv without defining it (:236, :290): 1/3 is the third-order
+ * upstream-biased scheme the comment at :214-215 names.  The vertical fluxes at rho levels 1
+ * and N read levels 0 and N of the auxiliary level, which sf_gls_predictor fills with the nstp
+ * values.  Huon, Hvom: U/V fluxes at rho levels; W and the tke/gls levels: N+1 W levels. */
+int sf_gls_advect(sf_ctx *ctx, const sf_gls_params *params, double dt, double gadv,
+                  const void *Huon, const void *Hvom, const void *W, const void *tke_aux,
+                  const void *gls_aux, void *tke_nnew, void *gls_nnew, sf_stream stream);
+/* sf_gls_corrector whose new level starts from tke_nnew/gls_nnew (after sf_gls_advect: the
+ * corrector's production terms add to tke(nnew), gls_corrector_step.py:447-450) instead of
+ * Hz_w * tke/gls(nstp); tke/gls hold nstp on entry and the new level on return, as in
+ * sf_gls_corrector.  With tke_nnew = Hz_w * tke (sf_gls_predictor's, no advection) the result
+ * is sf_gls_corrector's.  tke_nnew/gls_nnew must not alias tke/gls. */
+int sf_gls_corrector_nnew(sf_ctx *ctx, const sf_gls_params *params, double dt, const void *u,
+                          const void *v, const void *z_r, const void *Hz, const void *bvf,
+                          const void *sustr, const void *svstr, const void *tke_nnew,
+                          const void *gls_nnew, void *tke, void *gls, void *Akv, void *Akt,
+                          void *Akk, void *Akp, void *Lscale, sf_stream stream);
 /* sf_gls_corrector on the rho-interior columns p with columns[p] != 0 only (the closure's
  * fallback columns); the other columns' fields are left as they are.  No counterpart in the
  * reference. */

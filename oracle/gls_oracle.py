@@ -15,8 +15,10 @@ Scope (per water column, rho-interior points i=1..L-1, j=1..M-1):
   * the implicit tke and gls solves and the boundary fluxes (:568-656);
   * length-scale limitation, Galperin stability functions, Akv/Akt/Akk/Akp and Lscale
     (:662-825).
-Horizontal and vertical advection of tke/gls (:181-388, gls_predictor_step.py:18-216) is not
-included.
+The advective terms are restated separately: the predictor's auxiliary half step
+(gls_prestep, gls_predictor_step.py:18-216) and the corrector's third-order upstream horizontal
+and fourth-order vertical advection of the new level (gls_advect, :172-388); gls_corrector takes
+the advected new level as its start (tke_nnew/gls_nnew).
 
 Layout: W-level arrays have N+1 levels (0..N), rho-level arrays N levels; index arrays are
 flat (levels, (M+1)*(L+1)) with the reference's flat neighbour offsets (p+1 east, p+I north).
@@ -43,10 +45,12 @@ DEFAULT = dict(p=3.0, m=1.5, n=-1.0, cmu0=0.5477, c1=1.44, c2=1.92, c3m=-0.4, c3
 
 
 def gls_corrector(P, dt, I, J, N, u, v, z_r, Hz, bvf, sustr, svstr, tke, gls, Akv, Akt, Akk, Akp,
-                  Lscale):
+                  Lscale, tke_nnew=None, gls_nnew=None):
     """One corrector step; returns new (tke, gls, Akv, Akt, Akk, Akp, Lscale) copies.
     u, v: (N+1, s2) rho-level velocities (level N unused); z_r, Hz: (N, s2); bvf and the
-    turbulence fields: (N+1, s2); sustr, svstr: (s2,) kinematic surface stress at U/V points."""
+    turbulence fields: (N+1, s2); sustr, svstr: (s2,) kinematic surface stress at U/V points.
+    tke_nnew/gls_nnew (N+1, s2): the new level after advection (gls_advect), to which the
+    production terms add (:447-450); by default Hz_w * tke/gls (no advection)."""
     p_, m_, n_ = P["p"], P["m"], P["n"]
     cmu0 = P["cmu0"]
     s2 = I * J
@@ -108,8 +112,8 @@ def gls_corrector(P, dt, I, J, N, u, v, z_r, Hz, bvf, sustr, svstr, tke, gls, Ak
     zw_bot = None
     for k in range(1, N):
         cffz = 0.5 * (Hz[k - 1, col] + Hz[k, col])
-        tk[k] = cffz * tke_o[k]
-        gl[k] = cffz * gls_o[k]
+        tk[k] = cffz * tke_o[k] if tke_nnew is None else tke_nnew[k, col]
+        gl[k] = cffz * gls_o[k] if gls_nnew is None else gls_nnew[k, col]
         strat2 = b2[k]
         c3 = np.where(strat2 > 0.0, P["c3m"], P["c3p"])
         dAkt = Akt_o[k] - P["Akt_bak"]
@@ -224,6 +228,14 @@ def _edge_grad(q, axis):
     return np.concatenate([first, d, last], axis=axis)   # grad(0) := grad(1), grad(n) := grad(n-1)
 
 
+def _vflux_ends(q, CF, N):
+    """One-sided third-order vertical fluxes at rho levels 1 and N (gls_predictor_step.py:180-189,
+    gls_corrector_step.py:349-372): CF * (q0/3 + 5/6 q1 - q2/6) from the boundary inwards."""
+    c1, c2, c3 = 1.0 / 3.0, 5.0 / 6.0, 1.0 / 6.0
+    return (CF[1] * (c1 * q[0] + c2 * q[1] - c3 * q[2]),
+            CF[N] * (c1 * q[N] + c2 * q[N - 1] - c3 * q[N - 2]))
+
+
 def gls_prestep(dt, first, I, J, N, pm, pn, Huon, Hvom, W, Hz, tke_nstp, tke_indx, gls_nstp,
                 gls_indx, gamma=GAMMA):
     """nonlinear/gls_predictor_step.py:18-216 (fourth-order centred horizontal advection,
@@ -258,8 +270,7 @@ def gls_prestep(dt, first, I, J, N, pm, pn, Huon, Hvom, W, Hz, tke_nstp, tke_ind
     for q, F in ((T, FCt), (G, FCg)):
         for k in range(2, N):
             F[k] = CF[k] * (7.0 / 12.0 * (q[k - 1] + q[k]) - 1.0 / 12.0 * (q[k - 2] + q[k + 1]))
-        F[1] = CF[1] * (q[0] / 3.0 + 5.0 / 6.0 * q[1] - q[2] / 6.0)
-        F[N] = CF[N] * (q[N] / 3.0 + 5.0 / 6.0 * q[N - 1] - q[N - 2] / 6.0)
+        F[1], F[N] = _vflux_ends(q, CF, N)
     ii = slice(1, I - 1)
     jj = slice(1, J - 1)
     for k in range(1, N):
@@ -275,9 +286,9 @@ def gls_prestep(dt, first, I, J, N, pm, pn, Huon, Hvom, W, Hz, tke_nstp, tke_ind
             gy = _edge_grad(q, 0)             # (J+1, I)
             # FX(i), i = 1..I-1: XF(i) (q(i-1)+q(i) - (grad(i+1)-grad(i-1))/6) / 2
             FX = np.zeros(sh)
-            FX[:, 1:] = XF[:, 1:] * 0.5 * (q[:, :-1] + q[:, 1:] - (gx[:, 2:] - gx[:, :-2]) / 6.0)
+            FX[:, 1:] = XF[:, 1:] * 0.5 * (q[:, :-1] + q[:, 1:] - (1.0 / 6.0) * (gx[:, 2:] - gx[:, :-2]))
             FE = np.zeros(sh)
-            FE[1:, :] = EF[1:, :] * 0.5 * (q[:-1, :] + q[1:, :] - (gy[2:, :] - gy[:-2, :]) / 6.0)
+            FE[1:, :] = EF[1:, :] * 0.5 * (q[:-1, :] + q[1:, :] - (1.0 / 6.0) * (gy[2:, :] - gy[:-2, :]))
             res.append((FX, FE, qi))
         cff = 0.5 * (Hz.reshape(N, J, I)[k - 1] + Hz.reshape(N, J, I)[k])
         cff4 = c3 * pm2 * pn2
@@ -297,6 +308,9 @@ def gls_prestep(dt, first, I, J, N, pm, pn, Huon, Hvom, W, Hz, tke_nstp, tke_ind
             val = (val - cff4 * (F[k + 1] - F[k])) / hh
             out[k].reshape(sh)[jj, ii] = val[jj, ii]
             new[k].reshape(sh)[jj, ii] = (cff * q)[jj, ii]
+    for out, q in ((out_t, T), (out_g, G)):  # bottom/surface of the auxiliary level: nstp values
+        for k in (0, N):
+            out[k].reshape(sh)[jj, ii] = q[k][jj, ii]
     for out in (out_t, out_g):               # zero-gradient edges of the auxiliary level
         a = out.reshape(N + 1, J, I)
         a[1:N, jj, 0] = a[1:N, jj, 1]
@@ -308,3 +322,56 @@ def gls_prestep(dt, first, I, J, N, pm, pn, Huon, Hvom, W, Hz, tke_nstp, tke_ind
         a[1:N, J - 1, 0] = a[1:N, J - 2, 1]
         a[1:N, J - 1, I - 1] = a[1:N, J - 2, I - 2]
     return out_t, out_g, new_t, new_g, Hh
+
+
+# ---------------------------------------------------------------------------------------------
+# GLS corrector, advective terms
+# ---------------------------------------------------------------------------------------------
+GADV = 1.0 / 3.0    # third-order upstream-biased weight (gls_corrector_step.py:214-215, :236)
+
+
+def gls_advect(dt, I, J, N, pm, pn, Huon, Hvom, W, tke_aux, gls_aux, tke_nnew, gls_nnew, Kmin,
+               Pmin, gadv=GADV):
+    """nonlinear/gls_corrector_step.py:172-388 on the rho-interior points, W levels 1..N-1:
+    the new level less dt*pm*pn times the horizontal divergence of the third-order
+    upstream-biased fluxes of the auxiliary level (:181-298; the curvature from the upstream
+    side of the W-level flux, differences repeated at the domain edges), floored at Kmin/Pmin
+    (:300-317), then less the fourth-order vertical flux divergence (:329-377), floored again
+    (:378-388).  Arrays flat (levels, J*I) as in gls_prestep; returns new (tke_nnew, gls_nnew)."""
+    sh = (J, I)
+    cff = (dt * pm.reshape(sh)) * pn.reshape(sh)
+    ii = slice(1, I - 1)
+    jj = slice(1, J - 1)
+    Wl = W.reshape(N + 1, J, I)
+    CF = np.zeros((N + 2, J, I))
+    for k in range(1, N + 1):
+        CF[k] = 0.5 * (Wl[k] + Wl[k - 1])
+    outs = []
+    for aux, new, floor in ((tke_aux, tke_nnew, Kmin), (gls_aux, gls_nnew, Pmin)):
+        q3 = aux.reshape(N + 1, J, I)
+        out = new.copy().reshape(N + 1, J, I)
+        FC = np.zeros((N + 2, J, I))
+        for k in range(2, N):
+            FC[k] = CF[k] * (7.0 / 12.0 * (q3[k - 1] + q3[k]) - 1.0 / 12.0 * (q3[k - 2] + q3[k + 1]))
+        FC[1], FC[N] = _vflux_ends(q3, CF, N)
+        for k in range(1, N):
+            q = q3[k]
+            XF = 0.5 * (Huon.reshape(-1, J, I)[k - 1] + Huon.reshape(-1, J, I)[k])
+            EF = 0.5 * (Hvom.reshape(-1, J, I)[k - 1] + Hvom.reshape(-1, J, I)[k])
+            gx = _edge_grad(q, 1)             # (J, I+1): grad(i), i = 0..I
+            gy = _edge_grad(q, 0)             # (J+1, I)
+            cx = gx[:, 1:] - gx[:, :-1]       # curv(i) = grad(i+1) - grad(i), i = 0..I-1
+            cy = gy[1:, :] - gy[:-1, :]
+            FX = np.zeros(sh)                 # FX(i) at U point i = 1..I-1
+            up = np.where(XF[:, 1:] > 0.0, cx[:, :-1], cx[:, 1:])
+            FX[:, 1:] = XF[:, 1:] * 0.5 * (q[:, :-1] + q[:, 1:] - gadv * up)
+            FE = np.zeros(sh)
+            up = np.where(EF[1:, :] > 0.0, cy[:-1, :], cy[1:, :])
+            FE[1:, :] = EF[1:, :] * 0.5 * (q[:-1, :] + q[1:, :] - gadv * up)
+            div = np.zeros(sh)
+            div[jj, ii] = FX[jj, 2:] - FX[jj, 1:-1] + FE[2:, ii] - FE[1:-1, ii]
+            t = np.maximum(out[k] - cff * div, floor)
+            t = np.maximum(t - cff * (FC[k + 1] - FC[k]), floor)
+            out[k][jj, ii] = t[jj, ii]
+        outs.append(out.reshape(N + 1, J * I))
+    return outs[0], outs[1]

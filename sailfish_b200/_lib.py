@@ -81,6 +81,8 @@ SIGNATURES = {
     "sf_gls_corrector_list": [_vp, ctypes.POINTER(GlsParams), _d] + [_vp] * 16 + [_vp],
     "sf_analytic_bvf": [_vp, _vp, _d, _d, _d, _d, _vp, _vp],
     "sf_gls_predictor": [_vp, _d, _i] + [_vp] * 13 + [_vp],
+    "sf_gls_advect": [_vp, ctypes.POINTER(GlsParams), _d, _d] + [_vp] * 7 + [_vp],
+    "sf_gls_corrector_nnew": [_vp, ctypes.POINTER(GlsParams), _d] + [_vp] * 16 + [_vp],
     "sf_obc_volcons": [_vp, _vp, _vp, _vp, _i, _i, _vp, _vp],
     "sf_ctx_set_graphs": [_vp, _i],
     "sf_ctx_create_ensemble": [ctypes.POINTER(GridDesc), _i, ctypes.POINTER(_vp)],

@@ -1022,8 +1022,8 @@ int sf_gls_corrector_list(sf_ctx *c, const sf_gls_params *P, double dt, const vo
         return sf::Ops<R>::gls_corrector(c, *P, dt, (const R *)u, (const R *)v, (const R *)z_r,
                                          (const R *)Hz, (const R *)bvf, (const R *)sustr,
                                          (const R *)svstr, (R *)tke, (R *)gls, (R *)Akv, (R *)Akt,
-                                         (R *)Akk, (R *)Akp, (R *)Lscale, nullptr, list, count,
-                                         S(s));
+                                         (R *)Akk, (R *)Akp, (R *)Lscale, nullptr, nullptr,
+                                         nullptr, list, count, S(s));
     });
 }
 
@@ -1038,8 +1038,43 @@ int sf_gls_corrector_cols(sf_ctx *c, const sf_gls_params *P, double dt, const vo
         return sf::Ops<R>::gls_corrector(c, *P, dt, (const R *)u, (const R *)v, (const R *)z_r,
                                          (const R *)Hz, (const R *)bvf, (const R *)sustr,
                                          (const R *)svstr, (R *)tke, (R *)gls, (R *)Akv, (R *)Akt,
-                                         (R *)Akk, (R *)Akp, (R *)Lscale, columns, nullptr,
-                                         nullptr, S(s));
+                                         (R *)Akk, (R *)Akp, (R *)Lscale, nullptr, nullptr,
+                                         columns, nullptr, nullptr, S(s));
+    });
+}
+
+int sf_gls_corrector_nnew(sf_ctx *c, const sf_gls_params *P, double dt, const void *u,
+                          const void *v, const void *z_r, const void *Hz, const void *bvf,
+                          const void *sustr, const void *svstr, const void *tke_nnew,
+                          const void *gls_nnew, void *tke, void *gls, void *Akv, void *Akt,
+                          void *Akk, void *Akp, void *Lscale, sf_stream s) {
+    if (const int rc = gls_checks(P)) return rc;
+    if (!tke_nnew || !gls_nnew) return fail(SF_EINVAL, "null tke_nnew/gls_nnew");
+    if (tke_nnew == tke || gls_nnew == gls || tke_nnew == gls || gls_nnew == tke)
+        return fail(SF_EINVAL, "tke_nnew/gls_nnew must not alias tke/gls (the old level is read "
+                               "after the new one is formed)");
+    return dispatch(c, "sf_gls_corrector_nnew", [&](auto *t) {
+        using R = std::remove_pointer_t<decltype(t)>;
+        return sf::Ops<R>::gls_corrector(c, *P, dt, (const R *)u, (const R *)v, (const R *)z_r,
+                                         (const R *)Hz, (const R *)bvf, (const R *)sustr,
+                                         (const R *)svstr, (R *)tke, (R *)gls, (R *)Akv, (R *)Akt,
+                                         (R *)Akk, (R *)Akp, (R *)Lscale, (const R *)tke_nnew,
+                                         (const R *)gls_nnew, nullptr, nullptr, nullptr, S(s));
+    });
+}
+
+int sf_gls_advect(sf_ctx *c, const sf_gls_params *P, double dt, double gadv, const void *Huon,
+                  const void *Hvom, const void *W, const void *tke_aux, const void *gls_aux,
+                  void *tke_nnew, void *gls_nnew, sf_stream s) {
+    if (!P) return fail(SF_EINVAL, "null GLS parameters");
+    if (c && c->N < 3) return fail(SF_EUNSUPPORTED, "GLS advection needs N >= 3 levels");
+    if (tke_aux == tke_nnew || gls_aux == gls_nnew || tke_aux == gls_nnew || gls_aux == tke_nnew)
+        return fail(SF_EINVAL, "the auxiliary and new levels must be distinct arrays");
+    return dispatch(c, "sf_gls_advect", [&](auto *t) {
+        using R = std::remove_pointer_t<decltype(t)>;
+        return sf::Ops<R>::gls_advect(c, dt, gadv, P->Kmin, P->Pmin, (const R *)Huon,
+                                      (const R *)Hvom, (const R *)W, (const R *)tke_aux,
+                                      (const R *)gls_aux, (R *)tke_nnew, (R *)gls_nnew, S(s));
     });
 }
 

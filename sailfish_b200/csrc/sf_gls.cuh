@@ -34,8 +34,8 @@ __global__ void __launch_bounds__(128) k_gls_corrector(
     Geo<R> g, sf_gls_params P, R dt, const R *__restrict__ u, const R *__restrict__ v,
     const R *__restrict__ z_r, const R *__restrict__ Hz, const R *__restrict__ bvf,
     const R *__restrict__ sustr, const R *__restrict__ svstr, R *tke, R *gls, R *Akv, R *Akt,
-    R *Akk, R *Akp, R *Lscale, const uint8_t *__restrict__ sel, const int *__restrict__ list,
-    const int *__restrict__ count) {
+    R *Akk, R *Akp, R *Lscale, const R *__restrict__ tkn0, const R *__restrict__ gln0,
+    const uint8_t *__restrict__ sel, const int *__restrict__ list, const int *__restrict__ count) {
     int pi = (int)tid_flat();
     if (list) {                    // a compacted list of columns: thread t takes list[t]
         if (pi >= *count) return;
@@ -92,8 +92,12 @@ __global__ void __launch_bounds__(128) k_gls_corrector(
             Pprod = Pprod + c3 * strat2 * dAkt;
             cff2 = R(0);
         }
-        tk[k] = cffz * tko + dt * cffz * Kprod;
-        gl[k] = cffz * glo + dt * cffz * Pprod * glo / fmax(tko, Kmin);
+        // the new level starts from tke/gls(nnew) after advection when given, else from
+        // Hz_w * tke/gls(nstp) (the predictor's start without the advective terms)
+        const R tst = tkn0 ? AT(tkn0, k, p) : cffz * tko;
+        const R gst = gln0 ? AT(gln0, k, p) : cffz * glo;
+        tk[k] = tst + dt * cffz * Kprod;
+        gl[k] = gst + dt * cffz * Pprod * glo / fmax(tko, Kmin);
         const R diss = qpow(glo, -gls_exp1) * cmu_fac2 * qpow(tko, tke_exp2);
         BCK[k] = cffz * (R(1) + dt * diss + dt * (R(1) - cff1) * strat2 * dAkt / tko) - FCK[k] -
                  (k + 1 <= N ? FCK[k + 1] : R(0));
@@ -202,8 +206,9 @@ __device__ __forceinline__ R vflux_(const R *q, const R *W, long p, long s2, int
     // FC at rho level m (1..N, Fortran numbering) of the W-level field q
 #define Q(k) (q[(long)(k) * s2 + p])
     const R cf = R(0.5) * (W[(long)m * s2 + p] + W[(long)(m - 1) * s2 + p]);
-    if (m == 1) return cf * (Q(0) / R(3) + R(5.0 / 6.0) * Q(1) - Q(2) / R(6));
-    if (m == N) return cf * (Q(N) / R(3) + R(5.0 / 6.0) * Q(N - 1) - Q(N - 2) / R(6));
+    if (m == 1) return cf * (R(1.0 / 3.0) * Q(0) + R(5.0 / 6.0) * Q(1) - R(1.0 / 6.0) * Q(2));
+    if (m == N)
+        return cf * (R(1.0 / 3.0) * Q(N) + R(5.0 / 6.0) * Q(N - 1) - R(1.0 / 6.0) * Q(N - 2));
     return cf * (R(7.0 / 12.0) * (Q(m - 1) + Q(m)) - R(1.0 / 12.0) * (Q(m - 2) + Q(m + 1)));
 #undef Q
 }
@@ -225,12 +230,12 @@ __device__ __forceinline__ R hdiv_(const R *q, const R *XF0, const R *XF1, const
     auto FX = [&](int a) -> R {   // at U point a of row j
         const long u = (long)j * I + a;
         const R xf = R(0.5) * (XF0[u] + XF1[u]);
-        return xf * R(0.5) * (qk[u - 1] + qk[u] - (gx(a + 1) - gx(a - 1)) / R(6));
+        return xf * R(0.5) * (qk[u - 1] + qk[u] - R(1.0 / 6.0) * (gx(a + 1) - gx(a - 1)));
     };
     auto FE = [&](int b) -> R {   // at V point b of column i
         const long v = (long)b * I + i;
         const R ef = R(0.5) * (EF0[v] + EF1[v]);
-        return ef * R(0.5) * (qk[v - I] + qk[v] - (gy(b + 1) - gy(b - 1)) / R(6));
+        return ef * R(0.5) * (qk[v - I] + qk[v] - R(1.0 / 6.0) * (gy(b + 1) - gy(b - 1)));
     };
     (void)p;
     return (FX(i + 1) - FX(i)) + (FE(j + 1) - FE(j));
@@ -276,6 +281,12 @@ __global__ void __launch_bounds__(128) k_gls_prestep(Geo<R> g, GlsPre c, const R
         FCg = FCg1;
         CFk = CFk1;
     }
+    // the auxiliary level's bottom and surface values are the nstp ones (no advective update
+    // there); the corrector's vertical fluxes at rho levels 1 and N read them
+    tke3[p] = tke0[p];
+    gls3[p] = gls0[p];
+    tke3[(long)N * s2 + p] = tke0[(long)N * s2 + p];
+    gls3[(long)N * s2 + p] = gls0[(long)N * s2 + p];
 }
 
 // Zero-gradient lateral condition on the auxiliary level (edges from the adjacent interior
@@ -297,6 +308,83 @@ __global__ void k_gls_aux_bc(Geo<R> g, R *__restrict__ tke3, R *__restrict__ gls
     const long o = (long)k * g.s2;
     tke3[o + (long)j * I + i] = tke3[o + (long)sj * I + si];
     gls3[o + (long)j * I + i] = gls3[o + (long)sj * I + si];
+}
+
+// ---------------------------------------------------------------------------------------------
+// GLS corrector, advective terms (nonlinear/gls_corrector_step.py:172-388): tke/gls(nnew), the
+// Hz_w-weighted new level the predictor starts, less the horizontal flux divergence of the
+// auxiliary level (time level 3) — third-order upstream-biased fluxes whose curvature term
+// comes from the upstream side of the W-level U/V flux, weighted by Gadv (:181-298; the
+// one-sided differences repeated at the domain edges, :196-212, :253-268) — then floored at
+// Kmin/Pmin (:300-317); then less the vertical flux divergence of the auxiliary level
+// (fourth-order, with the one-sided third-order forms at the bottom and surface, :329-377) and
+// floored again (:378-388).  W levels 1..N-1 on the rho-interior points.
+// ---------------------------------------------------------------------------------------------
+template <typename R>
+__device__ __forceinline__ R hdiv_up3_(const R *qk, const R *XF0, const R *XF1, const R *EF0,
+                                       const R *EF1, int i, int j, int I, int J, R gadv) {
+    auto gx = [&](int m) -> R {   // grad(m) = q(m) - q(m-1), edges repeated
+        m = m < 1 ? 1 : (m > I - 1 ? I - 1 : m);
+        return qk[(long)j * I + m] - qk[(long)j * I + m - 1];
+    };
+    auto gy = [&](int m) -> R {
+        m = m < 1 ? 1 : (m > J - 1 ? J - 1 : m);
+        return qk[(long)m * I + i] - qk[(long)(m - 1) * I + i];
+    };
+    auto FX = [&](int a) -> R {   // at U point a of row j: curv(a-1) if the flux is eastward
+        const long u = (long)j * I + a;
+        const R xf = R(0.5) * (XF0[u] + XF1[u]);
+        const R curv = xf > R(0) ? gx(a) - gx(a - 1) : gx(a + 1) - gx(a);
+        return xf * R(0.5) * (qk[u - 1] + qk[u] - gadv * curv);
+    };
+    auto FE = [&](int b) -> R {   // at V point b of column i
+        const long v = (long)b * I + i;
+        const R ef = R(0.5) * (EF0[v] + EF1[v]);
+        const R curv = ef > R(0) ? gy(b) - gy(b - 1) : gy(b + 1) - gy(b);
+        return ef * R(0.5) * (qk[v - I] + qk[v] - gadv * curv);
+    };
+    return FX(i + 1) - FX(i) + FE(j + 1) - FE(j);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(128) k_gls_advect(Geo<R> g, R dt, R gadv, R Kmin, R Pmin,
+        const R *__restrict__ Huon, const R *__restrict__ Hvom, const R *__restrict__ W,
+        const R *__restrict__ tke3, const R *__restrict__ gls3, R *__restrict__ tken,
+        R *__restrict__ glsn) {
+    const int pi = (int)tid_flat();
+    if (pi >= g.s2) return;
+    const int I = g.I, J = g.J, N = g.N;
+    const int i = pi % I, j = pi / I;
+    if (i < 1 || i > I - 2 || j < 1 || j > J - 2) return;
+    const long p = pi, s2 = g.s2;
+    const R cff = dt * g.pm[p] * g.pn[p];
+    R FCt = vflux_(tke3, W, p, s2, 1, N), FCg = vflux_(gls3, W, p, s2, 1, N);
+    for (int k = 1; k < N; ++k) {
+        const R *XF0 = Huon + (long)(k - 1) * s2, *XF1 = Huon + (long)k * s2;
+        const R *EF0 = Hvom + (long)(k - 1) * s2, *EF1 = Hvom + (long)k * s2;
+        const long o = (long)k * s2 + p;
+        const R ht = hdiv_up3_(tke3 + (long)k * s2, XF0, XF1, EF0, EF1, i, j, I, J, gadv);
+        const R hg = hdiv_up3_(gls3 + (long)k * s2, XF0, XF1, EF0, EF1, i, j, I, J, gadv);
+        const R FCt1 = vflux_(tke3, W, p, s2, k + 1, N), FCg1 = vflux_(gls3, W, p, s2, k + 1, N);
+        R t = fmax(tken[o] - cff * ht, Kmin);
+        R q = fmax(glsn[o] - cff * hg, Pmin);
+        t = fmax(t - cff * (FCt1 - FCt), Kmin);
+        q = fmax(q - cff * (FCg1 - FCg), Pmin);
+        tken[o] = t;
+        glsn[o] = q;
+        FCt = FCt1;
+        FCg = FCg1;
+    }
+}
+
+template <typename R>
+cudaError_t Ops<R>::gls_advect(const sf_ctx *ctx, double dt, double gadv, double Kmin,
+                               double Pmin, const R *Huon, const R *Hvom, const R *W,
+                               const R *tke3, const R *gls3, R *tken, R *glsn, cudaStream_t s) {
+    const Geo<R> g = geo(ctx);
+    k_gls_advect<R><<<(unsigned)((g.s2 + 127) / 128), 128, 0, s>>>(
+        g, (R)dt, (R)gadv, (R)Kmin, (R)Pmin, Huon, Hvom, W, tke3, gls3, tken, glsn);
+    return cudaGetLastError();
 }
 
 template <typename R>

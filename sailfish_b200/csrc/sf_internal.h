@@ -166,8 +166,11 @@ struct Ops {
                                      const R *u, const R *v, const R *z_r, const R *Hz,
                                      const R *bvf, const R *sustr, const R *svstr, R *tke, R *gls,
                                      R *Akv, R *Akt, R *Akk, R *Akp, R *Lscale,
-                                     const uint8_t *sel, const int *list, const int *count,
-                                     cudaStream_t s);
+                                     const R *tkn0, const R *gln0, const uint8_t *sel,
+                                     const int *list, const int *count, cudaStream_t s);
+    static cudaError_t gls_advect(const sf_ctx *c, double dt, double gadv, double Kmin,
+                                  double Pmin, const R *Huon, const R *Hvom, const R *W,
+                                  const R *tke3, const R *gls3, R *tken, R *glsn, cudaStream_t s);
     static cudaError_t gls_prestep(const sf_ctx *c, GlsPre pc, const R *Huon, const R *Hvom,
                                    const R *W, const R *Hz, const R *tke0, const R *tkei, R *tke3,
                                    R *tken, const R *gls0, const R *glsi, R *gls3, R *glsn,

@@ -1500,11 +1500,12 @@ template <typename R>
 cudaError_t Ops<R>::gls_corrector(const sf_ctx *c, const sf_gls_params &P, double dt, const R *u,
                                   const R *v, const R *z_r, const R *Hz, const R *bvf,
                                   const R *sustr, const R *svstr, R *tke, R *gls, R *Akv, R *Akt,
-                                  R *Akk, R *Akp, R *Lscale, const uint8_t *sel,
-                                  const int *list, const int *count, cudaStream_t s) {
-    k_gls_corrector<R><<<blocks_for(c->s2, 128), 128, 0, s>>>(geo(c), P, (R)dt, u, v, z_r, Hz, bvf,
-                                                              sustr, svstr, tke, gls, Akv, Akt,
-                                                              Akk, Akp, Lscale, sel, list, count);
+                                  R *Akk, R *Akp, R *Lscale, const R *tkn0,
+                                  const R *gln0, const uint8_t *sel, const int *list,
+                                  const int *count, cudaStream_t s) {
+    k_gls_corrector<R><<<blocks_for(c->s2, 128), 128, 0, s>>>(
+        geo(c), P, (R)dt, u, v, z_r, Hz, bvf, sustr, svstr, tke, gls, Akv, Akt, Akk, Akp, Lscale,
+        tkn0, gln0, sel, list, count);
     return cudaGetLastError();
 }
 

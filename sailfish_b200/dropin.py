@@ -20,8 +20,9 @@ ignored, each call launches its own:
                DV_avg1, tmpU, tmpV, h, iic, ntfirst, lambda, AK, dt))               :646-707
     setLateralUVBCs((time, u, v, uIdx, vIdx, uType, vType))                          :314-368
 
-plus ``gls_corrector_step(compTimes, GRID, OCEAN, MIXING, FORCES)``, which the reference
-names (nonlinear/gls_corrector_step.py) but never made runnable.
+plus ``gls_predictor_step(compTimes, GRID, OCEAN, MIXING)`` and
+``gls_corrector_step(compTimes, GRID, OCEAN, MIXING, FORCES)``, which the reference names
+(nonlinear/gls_predictor_step.py, nonlinear/gls_corrector_step.py) but never made runnable.
 
 Arrays are any CUDA array exposing ``__cuda_array_interface__`` (CuPy arrays as the
 reference allocates them, torch CUDA tensors, ...), C-contiguous, in the reference's flat
@@ -246,16 +247,60 @@ setLateralUVBCs = _Kernel("setLateralUVBCs", _setLateralUVBCs)
 
 
 # ---- GLS ------------------------------------------------------------------------------------
+GADV = 1.0 / 3.0   # third-order upstream-biased weight (gls_corrector_step.py:214-215, :236)
+
+
+def gls_predictor_step(compTimes, GRID, OCEAN, MIXING):
+    """GLS predictor (nonlinear/gls_predictor_step.py:18-216) on the reference's state objects.
+    MIXING: tke, gls (time level nstp), optional tke_old/gls_old (level indx, the previous
+    step's; the forward first step when absent or compTimes.iic == compTimes.ntfirst), and the
+    caller's arrays tke_aux, gls_aux (time level 3), tke_nnew, gls_nnew and Hz_half, written
+    here ((N+1) W levels each).  Huon, Hvom and W are OCEAN's, Hz is GRID's."""
+    c = _need()
+    old_t = getattr(MIXING, "tke_old", None)
+    old_g = getattr(MIXING, "gls_old", None)
+    first = (old_t is None or old_g is None or
+             getattr(compTimes, "iic", 0) == getattr(compTimes, "ntfirst", 0))
+    check(lib.sf_gls_predictor(
+        c.ptr, float(compTimes.dt), int(first), _ptr(OCEAN.Huon, "Huon"),
+        _ptr(OCEAN.Hvom, "Hvom"), _ptr(OCEAN.W, "W"), _ptr(GRID.Hz, "Hz"),
+        _ptr(MIXING.tke, "tke"), _ptr(MIXING.tke if first else old_t, "tke_old"),
+        _ptr(MIXING.tke_aux, "tke_aux"), _ptr(MIXING.tke_nnew, "tke_nnew"),
+        _ptr(MIXING.gls, "gls"), _ptr(MIXING.gls if first else old_g, "gls_old"),
+        _ptr(MIXING.gls_aux, "gls_aux"), _ptr(MIXING.gls_nnew, "gls_nnew"),
+        _ptr(MIXING.Hz_half, "Hz_half"), stream), "gls_predictor_step")
+
+
 def gls_corrector_step(compTimes, GRID, OCEAN, MIXING, FORCES):
     """GLS corrector on the reference's state objects.  MIXING: tke, gls, Akt, Akk, Akp,
     Lscale and bvf ((N+1) W levels each), optional `params` (GlsParams; k-epsilon defaults);
     Akv is OCEAN.AKv.  FORCES: sustr, svstr (kinematic surface stress at U/V points).  u, v
-    are OCEAN.u_t2/v_t2; z_r and Hz come from GRID."""
+    are OCEAN.u_t2/v_t2; z_r and Hz come from GRID.  When MIXING holds tke_nnew (after
+    gls_predictor_step), the new level is first advected (gls_corrector_step.py:172-388, with
+    MIXING.gadv, default 1/3, and OCEAN's Huon, Hvom, W) and the corrector starts from it;
+    otherwise it starts from Hz_w * tke (no advection)."""
     from .closure import gls_defaults
     c = _need()
     P = getattr(MIXING, "params", None) or gls_defaults()
     if not isinstance(P, GlsParams):
         raise SailfishError("MIXING.params must be a GlsParams")
+    if getattr(MIXING, "tke_nnew", None) is not None:
+        # after gls_predictor_step: advect the new level, then start the corrector from it
+        check(lib.sf_gls_advect(
+            c.ptr, ctypes.byref(P), float(compTimes.dt), float(getattr(MIXING, "gadv", GADV)),
+            _ptr(OCEAN.Huon, "Huon"), _ptr(OCEAN.Hvom, "Hvom"), _ptr(OCEAN.W, "W"),
+            _ptr(MIXING.tke_aux, "tke_aux"), _ptr(MIXING.gls_aux, "gls_aux"),
+            _ptr(MIXING.tke_nnew, "tke_nnew"), _ptr(MIXING.gls_nnew, "gls_nnew"), stream),
+            "gls_corrector_step")
+        check(lib.sf_gls_corrector_nnew(
+            c.ptr, ctypes.byref(P), float(compTimes.dt), _ptr(OCEAN.u_t2, "u_t2"),
+            _ptr(OCEAN.v_t2, "v_t2"), _ptr(GRID.z_r, "z_r"), _ptr(GRID.Hz, "Hz"),
+            _ptr(MIXING.bvf, "bvf"), _ptr(FORCES.sustr, "sustr"), _ptr(FORCES.svstr, "svstr"),
+            _ptr(MIXING.tke_nnew, "tke_nnew"), _ptr(MIXING.gls_nnew, "gls_nnew"),
+            _ptr(MIXING.tke, "tke"), _ptr(MIXING.gls, "gls"), _ptr(OCEAN.AKv, "AKv"),
+            _ptr(MIXING.Akt, "Akt"), _ptr(MIXING.Akk, "Akk"), _ptr(MIXING.Akp, "Akp"),
+            _ptr(MIXING.Lscale, "Lscale"), stream), "gls_corrector_step")
+        return
     check(lib.sf_gls_corrector(
         c.ptr, ctypes.byref(P), float(compTimes.dt), _ptr(OCEAN.u_t2, "u_t2"),
         _ptr(OCEAN.v_t2, "v_t2"), _ptr(GRID.z_r, "z_r"), _ptr(GRID.Hz, "Hz"),
