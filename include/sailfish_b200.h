@@ -163,6 +163,17 @@ int sf_barotropic_loop(sf_ctx *ctx, sf_state2d *s, int nsub, const double *weigh
  * boundary values, which depend on time2D, are written to the device before each replay.
  * Results are identical either way.  No counterpart in the reference. */
 int sf_ctx_set_graphs(sf_ctx *ctx, int enable);
+/* Turn programmatic dependent launch of the barotropic loop's kernels on (default) or off:
+ * with it each kernel's blocks become resident while its predecessor's last wave runs and wait
+ * on the device for its completion.  Results are identical either way. */
+int sf_ctx_set_pdl(sf_ctx *ctx, int enable);
+/* Use the fused barotropic predictor (default on): one kernel per substep for computeZetaRHS +
+ * computeZetaPred, zetabc, the momentum predictor and barotropicVelocityBC, for single grids
+ * whose boundary programs write only the outer two-cell ring (sf_ctx_fused_available).  FP64
+ * results are identical either way. */
+int sf_ctx_set_fused(sf_ctx *ctx, int enable);
+/* 1 if the context can use the fused predictor, else 0. */
+int sf_ctx_fused_available(const sf_ctx *ctx);
 
 /* ---- 3D right-hand side, nonlinear/rhs.py:16-93 + nonlinear/rhs_kernels.cpp ------------ */
 /* rhs3d: ru = rv = 0, addCoriolis (:7-35), horizontalAdvection (:71-132), verticalAdvection

@@ -85,6 +85,9 @@ SIGNATURES = {
     "sf_gls_corrector_nnew": [_vp, ctypes.POINTER(GlsParams), _d] + [_vp] * 16 + [_vp],
     "sf_obc_volcons": [_vp, _vp, _vp, _vp, _i, _i, _vp, _vp],
     "sf_ctx_set_graphs": [_vp, _i],
+    "sf_ctx_set_pdl": [_vp, _i],
+    "sf_ctx_set_fused": [_vp, _i],
+    "sf_ctx_fused_available": [_vp],
     "sf_ctx_create_ensemble": [ctypes.POINTER(GridDesc), _i, ctypes.POINTER(_vp)],
     "sf_ctx_members": [_vp],
     "sf_ctx_set_tile": [_vp, _i],

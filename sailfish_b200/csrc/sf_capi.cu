@@ -152,12 +152,6 @@ int build_program(ProgHost &out, const std::vector<BcOp> &ops, long s2) {
     return SF_OK;
 }
 
-int make_program(sf::BcProgram &p, const std::vector<BcOp> &ops, long s2) {
-    ProgHost h;
-    const int rc = build_program(h, ops, s2);
-    return rc ? rc : upload_program(p, h);
-}
-
 // Appends a member's program to an ensemble's, its node indices offset into the pools.
 void append_program(ProgHost &all, const ProgHost &m, long off) {
     auto sh = [&](int v) { return v >= 0 ? (int)(v + off) : v; };
@@ -187,6 +181,8 @@ void free_ctx(sf_ctx *c) {
     if (c->cap) cudaStreamDestroy(c->cap);
     cudaFree(c->d_bcval);
     cudaFree(c->closure_x);
+    cudaFree(c->bcmap);
+    cudaFree(c->pred_counter);
     for (sf::BcProgram *p : {&c->zbc, &c->ubc, &c->vbc}) {
         cudaFree(p->dst);
         cudaFree(p->src);
@@ -248,6 +244,7 @@ int validate_desc(const sf_grid_desc *d) {
     if (!d->zeta_field_idx2 || !d->uvel_field_type || !d->vvel_field_type)
         return fail(SF_EINVAL, "missing boundary maps");
     const long s2 = (long)(d->L + 1) * (d->M + 1);
+    if (s2 >= (1L << 31)) return fail(SF_EINVAL, "grid too large: (L+1)(M+1) must be below 2^31");
     for (long k = 0; k < s2; ++k)
         if (d->vvel_field_type[k] > 0 && (d->vvel_field_type[k] & (1 << 4)) == 0 &&
             (d->vvel_field_type[k] & (1 << 3)) == 0 && (d->vvel_field_type[k] & (1 << 6)) != 0)
@@ -276,6 +273,41 @@ int build_programs(const sf_grid_desc *d, long s2, ProgHost &z, ProgHost &u, Pro
     return rc;
 }
 
+// Per-node maps of the three boundary programs for the fused predictor (sf_pred2d.cuh): code
+// (source + 2) | chained flag at each destination, kBcNone elsewhere.  The fused form is used
+// only when every destination lies in the outer two-cell ring of the grid and no node is a
+// destination twice; otherwise the context keeps the four-launch predictor.
+int build_pred_maps(sf_ctx *c, const ProgHost &Z, const ProgHost &U, const ProgHost &V) {
+    c->pred_ok = 0;
+    const long s2 = c->s2;
+    const int I = c->I, J = c->J;
+    if (s2 >= (1L << 29) || I < 6 || J < 6) return SF_OK;
+    std::vector<int> map(3 * (size_t)s2, sf::kBcNone);
+    const ProgHost *ps[3] = {&Z, &U, &V};
+    for (int f = 0; f < 3; ++f) {
+        const ProgHost &p = *ps[f];
+        for (int ch = 0; ch < 2; ++ch) {
+            const std::vector<int> &dd = ch ? p.dc : p.di, &ss = ch ? p.sc : p.si;
+            for (size_t k = 0; k < dd.size(); ++k) {
+                const int x = dd[k], i = x % I, j = x / I;
+                if (i >= 2 && i <= I - 3 && j >= 2 && j <= J - 3) return SF_OK;
+                int &m = map[(size_t)f * s2 + x];
+                if (m != sf::kBcNone) return SF_OK;
+                m = (ss[k] + 2) | (ch ? sf::kBcChained : 0);
+            }
+        }
+    }
+    int rc = upload(&c->bcmap, map.data(), map.size(), "boundary maps");
+    if (rc == SF_OK) {
+        if (cudaMalloc(&c->pred_counter, sizeof(int)) != cudaSuccess)
+            return fail(SF_ENOMEM, "cudaMalloc predictor counter");
+        if (cudaMemset(c->pred_counter, 0, sizeof(int)) != cudaSuccess)
+            return fail(SF_ECUDA, "cudaMemset predictor counter");
+        c->pred_ok = 1;
+    }
+    return rc;
+}
+
 template <typename R>
 int upload_members(sf_ctx *c, const sf_grid_desc *d, int n, const std::vector<long> &off2,
                    const std::vector<long> &off3, const std::vector<long> &offN,
@@ -285,6 +317,8 @@ int upload_members(sf_ctx *c, const sf_grid_desc *d, int n, const std::vector<lo
         sf::Geo<R> &g = mt[m].g;
         g.I = d[m].L + 1;
         g.J = d[m].M + 1;
+        g.dI = sf::make_fastdiv(g.I);
+        g.dJ = sf::make_fastdiv(g.J);
         g.N = d[m].N;
         g.s2 = (long)g.I * g.J;
         const R *const *mp = reinterpret_cast<const R *const *>(c->metrics);
@@ -531,19 +565,12 @@ int sf_ctx_create(const sf_grid_desc *d, sf_ctx **out) {
     if (rc == SF_OK && d->n_vbar_grad > d->n_ubar_grad)
         rc = fail(SF_EUNSUPPORTED, "vbar gradient list longer than the ubar list the reference "
                                    "copies it from (barotropicVelocityBC.py:30-31)");
-    if (rc == SF_OK)
-        rc = make_program(c->zbc, {{d->zeta_copy_idx1, d->zeta_copy_idx2, d->n_zeta_copy, 0}}, c->s2);
-    if (rc == SF_OK)
-        rc = make_program(c->ubc,
-                          {{d->ubar_closed_idx, nullptr, d->n_ubar_closed, -1},
-                           {d->ubar_clamped_idx, nullptr, d->n_ubar_clamped, -2},
-                           {d->ubar_grad_idx1, d->ubar_grad_idx2, d->n_ubar_grad, 0}},
-                          c->s2);
-    if (rc == SF_OK)
-        rc = make_program(c->vbc,
-                          {{d->vbar_closed_idx, nullptr, d->n_vbar_closed, -1},
-                           {d->vbar_grad_idx1, d->ubar_grad_idx2, d->n_vbar_grad, 0}},
-                          c->s2);
+    ProgHost Z, U, V;
+    if (rc == SF_OK) rc = build_programs(d, c->s2, Z, U, V);
+    if (rc == SF_OK) rc = upload_program(c->zbc, Z);
+    if (rc == SF_OK) rc = upload_program(c->ubc, U);
+    if (rc == SF_OK) rc = upload_program(c->vbc, V);
+    if (rc == SF_OK) rc = build_pred_maps(c, Z, U, V);
     if (rc != SF_OK) {
         free_ctx(c);
         return rc;
@@ -694,15 +721,22 @@ cudaError_t substep(const sf_ctx *c, const sf_state2d *st, double dtfast, double
     sf::BcProgram none;
     // predictor (step2d.py:23-81): computeZetaRHS + computeZetaPred, zetabc,
     // computeMomentumRHSPred + computeMomentumPred, barotropicVelocityBC
-    cudaError_t e = O::zeta_rhs(c, z1, (R *)st->ubar[1], (R *)st->vbar[1], (R *)st->rzeta[1], 2, 0.0,
-                                nullptr, nullptr, nullptr, z0, z2, dtfast, s);
-    if (e == cudaSuccess) e = O::bc_apply(c, c->zbc, z2, none, nullptr, 0.0, s);
-    if (e == cudaSuccess)
-        e = O::momentum(c, (R *)st->rubar[1], (R *)st->rvbar[1], z2, z0, 10.0, 2.0 / 5.0, 1, 1,
-                        dtfast, (R *)st->ubar[1], (R *)st->ubar[2], (R *)st->vbar[1],
-                        (R *)st->vbar[2], z1, z2, s);
-    if (e == cudaSuccess)
-        e = O::bc_apply(c, c->ubc, (R *)st->ubar[2], c->vbc, (R *)st->vbar[2], val, s, dval);
+    cudaError_t e = cudaSuccess;
+    if (c->nmem == 1 && c->pred_ok && c->use_fused) {
+        e = O::pred2d(c, z0, z1, z2, (R *)st->ubar[1], (R *)st->vbar[1], (R *)st->ubar[2],
+                      (R *)st->vbar[2], (R *)st->rzeta[1], (R *)st->rubar[1], (R *)st->rvbar[1],
+                      dtfast, 2.0 / 5.0, val, dval, s);
+    } else {
+        e = O::zeta_rhs(c, z1, (R *)st->ubar[1], (R *)st->vbar[1], (R *)st->rzeta[1], 2, 0.0,
+                        nullptr, nullptr, nullptr, z0, z2, dtfast, s);
+        if (e == cudaSuccess) e = O::bc_apply(c, c->zbc, z2, none, nullptr, 0.0, s);
+        if (e == cudaSuccess)
+            e = O::momentum(c, (R *)st->rubar[1], (R *)st->rvbar[1], z2, z0, 10.0, 2.0 / 5.0, 1,
+                            1, dtfast, (R *)st->ubar[1], (R *)st->ubar[2], (R *)st->vbar[1],
+                            (R *)st->vbar[2], z1, z2, s);
+        if (e == cudaSuccess)
+            e = O::bc_apply(c, c->ubc, (R *)st->ubar[2], c->vbc, (R *)st->vbar[2], val, s, dval);
+    }
     // corrector (step2d.py:84-128) and vbar_t2[:] = 0 (main3d.py:189)
     if (e == cudaSuccess)
         e = O::zeta_rhs(c, z2, (R *)st->ubar[2], (R *)st->vbar[2], (R *)st->rzeta[1], 1, cff1,
@@ -799,6 +833,32 @@ extern "C" {
 int sf_ctx_set_graphs(sf_ctx *c, int enable) {
     if (!c) return fail(SF_EINVAL, "null context");
     c->use_graphs = enable ? 1 : 0;
+    return SF_OK;
+}
+
+int sf_ctx_set_fused(sf_ctx *c, int enable) {
+    if (!c) return fail(SF_EINVAL, "null context");
+    if (c->use_fused != (enable ? 1 : 0)) {
+        for (auto &g : c->graphs) {   // captured loops hold the other form
+            if (g.exec) cudaGraphExecDestroy(g.exec);
+            g.exec = nullptr;
+        }
+    }
+    c->use_fused = enable ? 1 : 0;
+    return SF_OK;
+}
+
+int sf_ctx_fused_available(const sf_ctx *c) { return c && c->nmem == 1 && c->pred_ok ? 1 : 0; }
+
+int sf_ctx_set_pdl(sf_ctx *c, int enable) {
+    if (!c) return fail(SF_EINVAL, "null context");
+    if (c->use_pdl != (enable ? 1 : 0)) {
+        for (auto &g : c->graphs) {   // captured loops hold the old launch attribute
+            if (g.exec) cudaGraphExecDestroy(g.exec);
+            g.exec = nullptr;
+        }
+    }
+    c->use_pdl = enable ? 1 : 0;
     return SF_OK;
 }
 

@@ -16,6 +16,10 @@ namespace sf {
 // short "chained" list, applied by one thread that reads all its sources before writing;
 // all other entries are independent and applied by one thread each.
 constexpr int kMaxChained = 32;
+// Per-node boundary-program maps of the fused predictor: kBcNone (no destination) or
+// (source + 2) | kBcChained when the entry belongs to the chained group.
+constexpr int kBcNone = 0x7FFFFFFF;
+constexpr int kBcChained = 1 << 30;
 struct BcProgram {
     int n = 0;                 // independent entries
     int *dst = nullptr;        // device
@@ -33,10 +37,31 @@ struct GlsPre {
     double c1, c2, c3;
 };
 
+// floor(n / d) for 0 <= n < 2^31 by one 64-bit multiply and a shift: with 2^(l-1) < d <= 2^l
+// and m = ceil(2^(31+l) / d), floor(n * m / 2^(31+l)) = floor(n / d) (Granlund and
+// Montgomery, "Division by invariant integers using multiplication", PLDI 1994, the N+l-bit
+// multiplier form).  Used for the flat index's row and column in the 2D kernels.
+struct FastDiv {
+    unsigned long long m;
+    int shift;   // 31 + l
+};
+inline FastDiv make_fastdiv(int d) {
+    int l = 0;
+    while ((1LL << l) < d) ++l;
+    FastDiv f;
+    f.shift = 31 + l;
+    f.m = ((1ULL << f.shift) + (unsigned long long)d - 1) / (unsigned long long)d;
+    return f;
+}
+__host__ __device__ __forceinline__ int fdiv(int n, FastDiv f) {
+    return (int)(((unsigned long long)(unsigned)n * f.m) >> f.shift);
+}
+
 // Grid view handed to kernels by value.
 template <typename R>
 struct Geo {
     int I, J, N;  // xi points (L+1), eta points (M+1), levels
+    FastDiv dI, dJ;   // division by I and by J
     long s2;      // I*J
     const R *on_u, *om_v, *pm, *pn, *h, *fomn;
     const double *hd;                          // h in FP64 (set_depth)
@@ -95,6 +120,17 @@ struct sf_ctx {
     // boundary values (device, written before each replay), and up to 3 captured loops (the
     // slot rotation cycles with period 3).
     int use_graphs = 1;
+    // Programmatic dependent launch of the barotropic kernels (sf_ctx_set_pdl): each kernel
+    // lets its successor's blocks become resident while its own last wave runs; the successor
+    // waits (griddepcontrol.wait) for its completion before touching any field.
+    int use_pdl = 1;
+    // The fused barotropic predictor (sf::Ops::pred2d) for single grids whose boundary
+    // programs write only the outer two-cell ring: per-node program maps (zeta, ubar, vbar;
+    // device, 3 * s2), the last-block counter, and whether the fused form is used.
+    int *bcmap = nullptr;
+    int *pred_counter = nullptr;
+    int pred_ok = 0;
+    int use_fused = 1;
     cudaStream_t cap = nullptr;
     double *d_bcval = nullptr;
     sf_loop_graph graphs[3];
@@ -122,6 +158,31 @@ struct sf_ctx {
 };
 
 namespace sf {
+
+// Kernels launched through launch_dep (programmatic dependent launch) start with pdl_enter():
+// it lets the next kernel on the stream begin launching its blocks, then waits until this
+// kernel's predecessor has completed and its writes are visible.  Both are no-ops when the
+// kernel was launched without the attribute.
+__device__ __forceinline__ void pdl_enter() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_dep(const sf_ctx *c, void (*kern)(KArgs...), dim3 grid, dim3 block,
+                              size_t smem, cudaStream_t s, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = c->use_pdl ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+}
 
 // Launchers, one explicit instantiation per precision (FP64 in a translation unit built
 // without FMA contraction, so that it reproduces the reference's IEEE evaluation).
@@ -175,6 +236,9 @@ struct Ops {
                                    const R *W, const R *Hz, const R *tke0, const R *tkei, R *tke3,
                                    R *tken, const R *gls0, const R *glsi, R *gls3, R *glsn,
                                    R *Hz_half, cudaStream_t s);
+    static cudaError_t pred2d(const sf_ctx *c, R *z0, R *z1, R *z2, R *ub1, R *vb1, R *ub2,
+                              R *vb2, R *rz, R *ru, R *rv, double Dt, double weight, double val,
+                              const double *valp, cudaStream_t s);
     static cudaError_t obc_volcons(const sf_ctx *c, const R *zeta, R *ubar, R *vbar, int edges,
                                    int correct, double *out, cudaStream_t s);
     static cudaError_t analytic_bvf(const sf_ctx *c, const R *z_w, double dT, double zscale,

@@ -46,6 +46,16 @@ __device__ __forceinline__ R ldz(const R *a, long idx) {   // read, 0 before the
     return idx >= 0 ? a[idx] : R(0);
 }
 
+// Division by a depth or a layer thickness (the momentum predictors, the vertical velocity
+// integral): IEEE division in FP64 (the reference's arithmetic); in FP32 the hardware
+// reciprocal form __fdividef (2 ulp for divisors in [2^-126, 2^126]; depths and thicknesses
+// here are centimetres to kilometres), a few instructions instead of the IEEE sequence, well
+// inside the FP32 form's stated per-field tolerances.
+template <typename R>
+__device__ __forceinline__ R ddiv(R a, R b) { return a / b; }
+template <>
+__device__ __forceinline__ float ddiv<float>(float a, float b) { return __fdividef(a, b); }
+
 // ------------------------------------------------------------------------------------------
 // 2D barotropic kernels
 // ------------------------------------------------------------------------------------------
@@ -60,7 +70,7 @@ __device__ __forceinline__ void zeta_rhs_body(
     R *__restrict__ zeta_t2, R Dt, const long p) {
     if (p >= g.s2) return;
     const long I = g.I;
-    const int i = (int)(p % I), j = (int)(p / I);
+    const int j = fdiv((int)p, g.dI), i = (int)p - j * g.I;
     const bool in = rint_(i, j, g.I, g.J);
     R rz = R(0);
     if (in) {
@@ -117,7 +127,7 @@ __device__ __forceinline__ void momentum_body(
     R *__restrict__ v_t2, const R *__restrict__ z1, const R *__restrict__ z2, const long p) {
     if (p >= g.s2) return;
     const long I = g.I, J = g.J;
-    const int i = (int)(p % I), j = (int)(p / I);
+    const int j = fdiv((int)p, g.dI), i = (int)p - j * g.I;
     const R *h = g.h;
     const bool in = do_rhs && rint_(i, j, g.I, g.J);
     R ru = R(0), rv = R(0);
@@ -130,7 +140,7 @@ __device__ __forceinline__ void momentum_body(
         rhs_u[p] = ru;
         rhs_v[p] = rv;
     }
-    if (do_pred && (p % J) != 0 && p >= J) {
+    if (do_pred && (int)p - fdiv((int)p, g.dJ) * g.J != 0 && p >= J) {   // p % J != 0
         if (!in) {
             ru = rhs_u[p];
             rv = rhs_v[p];
@@ -143,8 +153,8 @@ __device__ __forceinline__ void momentum_body(
         // vbar_t2[:] = 0 (nonlinear/main3d.py:189) before anything reads it.
         const R D1V = (D1p + (ldz(z1, p - I) + ldz(h, p - I))) * R(0.5);
         const R D2V = (D2p + (ldz(z2, p - I) + ldz(h, p - I))) * R(0.5);
-        u_t2[p] = (u_t1[p] * D1U + ((Dt * ru) * g.pm[p]) * g.pn[p]) / D2U;
-        v_t2[p] = (v_t1[p] * D1V + ((Dt * rv) * g.pm[p]) * g.pn[p]) / D2V;
+        u_t2[p] = ddiv(u_t1[p] * D1U + ((Dt * ru) * g.pm[p]) * g.pn[p], D2U);
+        v_t2[p] = ddiv(v_t1[p] * D1V + ((Dt * rv) * g.pm[p]) * g.pn[p], D2V);
     }
 }
 
@@ -176,6 +186,285 @@ __device__ __forceinline__ void corr_point_body(
     if (vbar_t2) vbar_t2[p] = R(0);
 }
 
+// ------------------------------------------------------------------------------------------
+// Four-point forms of the 2D kernels (single grids): thread t owns the flat points
+// p0 = 4t .. 4t+3 and loads each array's four values with 16-byte vector loads where the
+// address allows it (checked at run time; the check is uniform across a warp), the
+// neighbours p0-1 and p0+4 with scalar loads.  Each point's arithmetic is the scalar body's,
+// operation for operation.  Threads whose stencil would reach outside the arrays (the first
+// and last rows) run the scalar body on their four points.
+// ------------------------------------------------------------------------------------------
+template <typename R>
+__device__ __forceinline__ void ld4(const R *__restrict__ a, long p, R (&o)[4]) {
+    const R *q = a + p;
+    const uintptr_t ad = reinterpret_cast<uintptr_t>(q);
+    if constexpr (sizeof(R) == 4) {
+        if ((ad & 15) == 0) {
+            const float4 t = *reinterpret_cast<const float4 *>(q);
+            o[0] = t.x; o[1] = t.y; o[2] = t.z; o[3] = t.w;
+            return;
+        }
+        if ((ad & 7) == 0) {
+            const float2 t0 = reinterpret_cast<const float2 *>(q)[0];
+            const float2 t1 = reinterpret_cast<const float2 *>(q)[1];
+            o[0] = t0.x; o[1] = t0.y; o[2] = t1.x; o[3] = t1.y;
+            return;
+        }
+    } else {
+        if ((ad & 15) == 0) {
+            const double2 t0 = reinterpret_cast<const double2 *>(q)[0];
+            const double2 t1 = reinterpret_cast<const double2 *>(q)[1];
+            o[0] = t0.x; o[1] = t0.y; o[2] = t1.x; o[3] = t1.y;
+            return;
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) o[u] = q[u];
+}
+
+// Stores the lanes u with (mask >> u) & 1; one vector store when all four are set and aligned.
+template <typename R>
+__device__ __forceinline__ void st4(R *__restrict__ a, long p, const R (&v)[4], unsigned mask) {
+    R *q = a + p;
+    const uintptr_t ad = reinterpret_cast<uintptr_t>(q);
+    if (mask == 15u) {
+        if constexpr (sizeof(R) == 4) {
+            if ((ad & 15) == 0) {
+                *reinterpret_cast<float4 *>(q) = make_float4(v[0], v[1], v[2], v[3]);
+                return;
+            }
+        } else {
+            if ((ad & 15) == 0) {
+                reinterpret_cast<double2 *>(q)[0] = make_double2(v[0], v[1]);
+                reinterpret_cast<double2 *>(q)[1] = make_double2(v[2], v[3]);
+                return;
+            }
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+        if ((mask >> u) & 1u) q[u] = v[u];
+}
+
+// (i, j) of the four points from those of the first: one wrap to the next row at most (I >= 5).
+__device__ __forceinline__ void ij4(int i0, int j0, int I, int (&i)[4], int (&j)[4]) {
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const int a = i0 + u;
+        const bool w = a >= I;
+        i[u] = w ? a - I : a;
+        j[u] = w ? j0 + 1 : j0;
+    }
+}
+
+template <typename R>
+__device__ __forceinline__ void zeta_rhs4(
+    const Geo<R> &g, const R *__restrict__ zeta, const R *__restrict__ ubar,
+    const R *__restrict__ vbar, R *__restrict__ rzeta, int mode, double cff1,
+    double *__restrict__ Zt, double *__restrict__ DU, double *__restrict__ DV,
+    const R *__restrict__ zeta_t0, R *__restrict__ zeta_t2, R Dt, const long p0) {
+    const long I = g.I, s2 = g.s2;
+    if (p0 >= s2) return;
+    if (p0 < I || p0 + 3 + I >= s2) {
+        for (int u = 0; u < 4; ++u)
+            zeta_rhs_body(g, zeta, ubar, vbar, rzeta, mode, cff1, Zt, DU, DV, zeta_t0, zeta_t2,
+                          Dt, p0 + u);
+        return;
+    }
+    const int j0 = fdiv((int)p0, g.dI), i0 = (int)p0 - j0 * g.I;
+    int ii[4], jj[4];
+    ij4(i0, j0, g.I, ii, jj);
+    unsigned inm = 0;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) inm |= (rint_(ii[u], jj[u], g.I, g.J) ? 1u : 0u) << u;
+    R rz[4] = {R(0), R(0), R(0), R(0)};
+    double DUp_[4], DVp_[4];
+    if (inm) {
+        const R *h = g.h;
+        R z[4], zs[4], zn[4], hh[4], hs[4], hn[4], ub[4], vb[4], vn[4], ou[4], ov[4], ovn[4],
+            pm[4], pn[4];
+        ld4(zeta, p0, z);
+        ld4(zeta, p0 - I, zs);
+        ld4(zeta, p0 + I, zn);
+        ld4(h, p0, hh);
+        ld4(h, p0 - I, hs);
+        ld4(h, p0 + I, hn);
+        ld4(ubar, p0, ub);
+        ld4(vbar, p0, vb);
+        ld4(vbar, p0 + I, vn);
+        ld4(g.on_u, p0, ou);
+        ld4(g.om_v, p0, ov);
+        ld4(g.om_v, p0 + I, ovn);
+        ld4(g.pm, p0, pm);
+        ld4(g.pn, p0, pn);
+        const R zw = zeta[p0 - 1], ze = zeta[p0 + 4], hw = h[p0 - 1], he = h[p0 + 4];
+        const R ue = ubar[p0 + 4], oue = g.on_u[p0 + 4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const R Dp = z[u] + hh[u];
+            const R Dw = u == 0 ? zw + hw : z[u - 1] + hh[u - 1];
+            const R De = u == 3 ? ze + he : z[u + 1] + hh[u + 1];
+            const R Ds = zs[u] + hs[u], Dn = zn[u] + hn[u];
+            const R DUp = ub[u] * ((Dp + Dw) * R(0.5));
+            const R DUe = (u == 3 ? ue : ub[u + 1]) * ((De + Dp) * R(0.5));
+            const R DVp = vb[u] * ((Dp + Ds) * R(0.5));
+            const R DVn = vn[u] * ((Dn + Dp) * R(0.5));
+            const R oe = u == 3 ? oue : ou[u + 1];
+            rz[u] = (((DUe * oe - DUp * ou[u]) + (DVn * ovn[u] - DVp * ov[u])) * pm[u]) * pn[u];
+            DUp_[u] = (cff1 * (double)DUp) * (double)ou[u];
+            DVp_[u] = (cff1 * (double)DVp) * (double)ov[u];
+        }
+        st4(rzeta, p0, rz, inm);
+        if (mode == 1) {
+            double zt[4], du[4], dv[4];
+            ld4(Zt, p0, zt);
+            ld4(DU, p0, du);
+            ld4(DV, p0, dv);
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                zt[u] = zt[u] + cff1 * (double)z[u];
+                du[u] = du[u] + DUp_[u];
+                dv[u] = dv[u] + DVp_[u];
+            }
+            st4(Zt, p0, zt, inm);
+            st4(DU, p0, du, inm);
+            st4(DV, p0, dv, inm);
+        }
+    }
+    if (mode == 2) {
+        unsigned wm = 0;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) wm |= (ii[u] != 0 && jj[u] != 0 ? 1u : 0u) << u;
+        R z0[4], out[4];
+        ld4(zeta_t0, p0, z0);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const R r = ((inm >> u) & 1u) ? rz[u] : (((wm >> u) & 1u) ? rzeta[p0 + u] : R(0));
+            out[u] = z0[u] + Dt * r;
+        }
+        st4(zeta_t2, p0, out, wm);
+    }
+}
+
+template <typename R>
+__device__ __forceinline__ void momentum4(
+    const Geo<R> &g, R *__restrict__ rhs_u, R *__restrict__ rhs_v, const R *__restrict__ za,
+    const R *__restrict__ zb, R grav, R w1, R w, int do_rhs, int do_pred, R Dt,
+    const R *__restrict__ u_t1, R *__restrict__ u_t2, const R *__restrict__ v_t1,
+    R *__restrict__ v_t2, const R *__restrict__ z1, const R *__restrict__ z2, const long p0) {
+    const long I = g.I, J = g.J, s2 = g.s2;
+    if (p0 >= s2) return;
+    if (p0 < I + 1 || p0 + 3 >= s2) {
+        for (int u = 0; u < 4; ++u)
+            momentum_body(g, rhs_u, rhs_v, za, zb, grav, w1, w, do_rhs, do_pred, Dt, u_t1, u_t2,
+                          v_t1, v_t2, z1, z2, p0 + u);
+        return;
+    }
+    const R *h = g.h;
+    const int j0 = fdiv((int)p0, g.dI), i0 = (int)p0 - j0 * g.I;
+    int ii[4], jj[4];
+    ij4(i0, j0, g.I, ii, jj);
+    unsigned inm = 0, pdm = 0;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const int q = (int)p0 + u;
+        inm |= (do_rhs && rint_(ii[u], jj[u], g.I, g.J) ? 1u : 0u) << u;
+        pdm |= (do_pred && q - fdiv(q, g.dJ) * g.J != 0 && q >= J ? 1u : 0u) << u;
+    }
+    R hh[4], hs[4];
+    ld4(h, p0, hh);
+    ld4(h, p0 - I, hs);
+    const R hw = h[p0 - 1];
+    R ru[4] = {R(0), R(0), R(0), R(0)}, rv[4] = {R(0), R(0), R(0), R(0)};
+    if (inm) {
+        R a[4], as[4], b[4], bs[4], ou[4], ov[4];
+        ld4(za, p0, a);
+        ld4(za, p0 - I, as);
+        ld4(zb, p0, b);
+        ld4(zb, p0 - I, bs);
+        ld4(g.on_u, p0, ou);
+        ld4(g.om_v, p0, ov);
+        const R aw = za[p0 - 1], bw = zb[p0 - 1];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const R gp = w1 * a[u] + w * b[u];
+            const R gw = u == 0 ? w1 * aw + w * bw : w1 * a[u - 1] + w * b[u - 1];
+            const R gs = w1 * as[u] + w * bs[u];
+            const R hwu = u == 0 ? hw : hh[u - 1];
+            ru[u] = (grav * ou[u]) * (((hh[u] + hwu) * R(0.5)) * (gp - gw) + R(0.5) * (gp * gp - gw * gw));
+            rv[u] = (grav * ov[u]) * (((hh[u] + hs[u]) * R(0.5)) * (gp - gs) + R(0.5) * (gp * gp - gs * gs));
+        }
+        st4(rhs_u, p0, ru, inm);
+        st4(rhs_v, p0, rv, inm);
+    }
+    if (pdm) {
+        R c1[4], c1s[4], c2[4], c2s[4], ut[4], vt[4], pm[4], pn[4], uo[4], vo[4];
+        ld4(z1, p0, c1);
+        ld4(z1, p0 - I, c1s);
+        ld4(z2, p0, c2);
+        ld4(z2, p0 - I, c2s);
+        ld4(u_t1, p0, ut);
+        ld4(v_t1, p0, vt);
+        ld4(g.pm, p0, pm);
+        ld4(g.pn, p0, pn);
+        const R c1w = z1[p0 - 1], c2w = z2[p0 - 1];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            R fu = ru[u], fv = rv[u];
+            if (((pdm >> u) & 1u) && !((inm >> u) & 1u)) {
+                fu = rhs_u[p0 + u];
+                fv = rhs_v[p0 + u];
+            }
+            const R hwu = u == 0 ? hw : hh[u - 1];
+            const R D1p = c1[u] + hh[u], D2p = c2[u] + hh[u];
+            const R D1U = (D1p + ((u == 0 ? c1w : c1[u - 1]) + hwu)) * R(0.5);
+            const R D2U = (D2p + ((u == 0 ? c2w : c2[u - 1]) + hwu)) * R(0.5);
+            const R D1V = (D1p + (c1s[u] + hs[u])) * R(0.5);
+            const R D2V = (D2p + (c2s[u] + hs[u])) * R(0.5);
+            uo[u] = ddiv(ut[u] * D1U + ((Dt * fu) * pm[u]) * pn[u], D2U);
+            vo[u] = ddiv(vt[u] * D1V + ((Dt * fv) * pm[u]) * pn[u], D2V);
+        }
+        st4(u_t2, p0, uo, pdm);
+        st4(v_t2, p0, vo, pdm);
+    }
+}
+
+template <typename R>
+__device__ __forceinline__ void corr_point4(
+    const Geo<R> &g, R Dt, R *__restrict__ zeta_t2, const R *__restrict__ rz0,
+    const R *__restrict__ rz1, const R *__restrict__ rz2, R *__restrict__ ubar_t1,
+    const R *__restrict__ vbar_t1, const R *__restrict__ rub0, const R *__restrict__ rub1,
+    R *__restrict__ vbar_t2, const long p0) {
+    if (p0 >= g.s2) return;
+    if (p0 + 3 >= g.s2) {
+        for (int u = 0; u < 4; ++u)
+            corr_point_body(g, Dt, zeta_t2, rz0, rz1, rz2, ubar_t1, vbar_t1, rub0, rub1, vbar_t2,
+                            p0 + u);
+        return;
+    }
+    const R A2 = R(5.0 / 12.0), A1 = R(8.0 / 12.0), A0 = R(-1.0 / 12.0);
+    R z[4], r0[4], r1[4], r2[4], ub[4], vb[4], b0[4], b1[4];
+    ld4(zeta_t2, p0, z);
+    ld4(rz0, p0, r0);
+    ld4(rz1, p0, r1);
+    ld4(rz2, p0, r2);
+    ld4(ubar_t1, p0, ub);
+    ld4(vbar_t1, p0, vb);
+    ld4(rub0, p0, b0);
+    ld4(rub1, p0, b1);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        z[u] = z[u] + Dt * ((A2 * r2[u] + A1 * r1[u]) + A0 * r0[u]);
+        ub[u] = ub[u] + Dt * ((A2 * b1[u] + A1 * b0[u]) + A0 * vb[u]);
+    }
+    st4(zeta_t2, p0, z, 15u);
+    st4(ubar_t1, p0, ub, 15u);
+    if (vbar_t2) {
+        const R zero[4] = {R(0), R(0), R(0), R(0)};
+        st4(vbar_t2, p0, zero, 15u);
+    }
+}
+
 // Boundary programs (see BcProgram): independent entries one per thread over as many blocks
 // as needed; each group of chained entries by one thread, all reads before all writes.
 template <typename R>
@@ -186,6 +475,7 @@ __device__ __forceinline__ R bc_value(const R *f, int s, R val) {
 template <typename R>
 __global__ void __launch_bounds__(256) k_bc_apply(BcProgram p1, R *f1, BcProgram p2, R *f2, R val0,
                                                   const double *valp) {
+    pdl_enter();
     const R val = valp ? (R)valp[0] : val0;   // time-dependent value from the device (graphs)
     const long t = tid_flat();
     if (t < p1.n) {
@@ -551,7 +841,7 @@ __device__ __forceinline__ void maxflux_omega_body(
 #pragma unroll 4
         for (int K = 1; K < N; ++K) {
             const long o = (long)K * s2 + p;
-            W[o] = Wc(K) - (Ws * (z_w[o] - zbed)) / h;
+            W[o] = Wc(K) - ddiv(Ws * (z_w[o] - zbed), h);
         }
 #undef Wc
         W[(long)N * s2 + p] = R(0);
@@ -885,19 +1175,20 @@ __device__ __forceinline__ void step3d_uv_pipe_body(const Geo<R> &g, float *__re
             float gk = 0.f;
             if (k < N - 1) {
                 const float zP1 = sZr[col + 1], zQ1 = sZr[qi];
-                gk = (cm * ((sAk[col + 1] + sAk[qi]) * 0.5f)) / (((zP1 - zP) + (zQ1 - zQ)) * 0.5f);
+                // divisions by layer spacings and pivots (metres): the reciprocal form, as ddiv
+                gk = __fdividef(cm * ((sAk[col + 1] + sAk[qi]) * 0.5f), ((zP1 - zP) + (zQ1 - zQ)) * 0.5f);
                 zP = zP1;
                 zQ = zQ1;
             }
             const float ok = sO[col];
             if (k == 0) {   // bottom row: right-hand side forced to 0 (:610)
                 fc0 = gk;
-                ccp = gk / (hz - 2.f * gk);
+                ccp = __fdividef(gk, hz - 2.f * gk);
                 ddp = 0.f;
             } else {
                 const float rr = hz * (ok + cmn * sR[col]);
                 const float bd = (k < N - 1) ? (hz - gk) - fc : hz - fc;
-                const float iv = 1.f / (bd - fc * ccp);
+                const float iv = __fdividef(1.f, bd - fc * ccp);
                 ccp = gk * iv;
                 ddp = (rr - fc * ddp) * iv;
                 Rs += (double)rr;
@@ -1101,6 +1392,7 @@ __global__ void __launch_bounds__(kBlock) k_lateral_uv_bc(Geo<R> g, R *__restric
 }  // namespace sf
 
 #include "sf_gls.cuh"
+#include "sf_pred2d.cuh"
 
 namespace sf {
 
@@ -1120,35 +1412,39 @@ namespace sf {
 #define ON(x) ((x) ? (x) + oN : (x))
 
 template <typename R>
-__global__ void __launch_bounds__(kBlock) k_zeta_rhs(
+__global__ void __launch_bounds__(kBlock, 4) k_zeta_rhs(
     Geo<R> g, const R *__restrict__ zeta, const R *__restrict__ ubar, const R *__restrict__ vbar, R *__restrict__ rzeta, int mode, double cff1,
     double *__restrict__ Zt, double *__restrict__ DU, double *__restrict__ DV, const R *__restrict__ zeta_t0, R *__restrict__ zeta_t2, R Dt) {
-    zeta_rhs_body(g, zeta, ubar, vbar, rzeta, mode, cff1, Zt, DU, DV, zeta_t0, zeta_t2, Dt,
-                  (long)tid_flat());
+    pdl_enter();
+    zeta_rhs4(g, zeta, ubar, vbar, rzeta, mode, cff1, Zt, DU, DV, zeta_t0, zeta_t2, Dt,
+              4 * (long)tid_flat());
 }
 template <typename R>
 __global__ void __launch_bounds__(kBlock) kb_zeta_rhs(
     const Member<R> *mt, const int2 *bm, const R *__restrict__ zeta, const R *__restrict__ ubar, const R *__restrict__ vbar, R *__restrict__ rzeta,
     int mode, double cff1, double *__restrict__ Zt, double *__restrict__ DU, double *__restrict__ DV, const R *__restrict__ zeta_t0, R *__restrict__ zeta_t2,
     R Dt) {
+    pdl_enter();
     SF_MEMBER(bm)
     zeta_rhs_body(g, O2(zeta), O2(ubar), O2(vbar), O2(rzeta), mode, cff1, O2(Zt), O2(DU), O2(DV),
                   O2(zeta_t0), O2(zeta_t2), Dt, (long)mb_.y * kBlock + threadIdx.x);
 }
 
 template <typename R>
-__global__ void __launch_bounds__(kBlock) k_momentum(
+__global__ void __launch_bounds__(kBlock, 4) k_momentum(
     Geo<R> g, R *__restrict__ rhs_u, R *__restrict__ rhs_v, const R *__restrict__ za, const R *__restrict__ zb, R grav, R w1, R w, int do_rhs,
     int do_pred, R Dt, const R *__restrict__ u_t1, R *__restrict__ u_t2, const R *__restrict__ v_t1, R *__restrict__ v_t2, const R *__restrict__ z1,
     const R *__restrict__ z2) {
-    momentum_body(g, rhs_u, rhs_v, za, zb, grav, w1, w, do_rhs, do_pred, Dt, u_t1, u_t2, v_t1,
-                  v_t2, z1, z2, (long)tid_flat());
+    pdl_enter();
+    momentum4(g, rhs_u, rhs_v, za, zb, grav, w1, w, do_rhs, do_pred, Dt, u_t1, u_t2, v_t1, v_t2,
+              z1, z2, 4 * (long)tid_flat());
 }
 template <typename R>
 __global__ void __launch_bounds__(kBlock) kb_momentum(
     const Member<R> *mt, const int2 *bm, R *__restrict__ rhs_u, R *__restrict__ rhs_v, const R *__restrict__ za, const R *__restrict__ zb, R grav,
     R w1, R w, int do_rhs, int do_pred, R Dt, const R *__restrict__ u_t1, R *__restrict__ u_t2, const R *__restrict__ v_t1, R *__restrict__ v_t2,
     const R *__restrict__ z1, const R *__restrict__ z2) {
+    pdl_enter();
     SF_MEMBER(bm)
     momentum_body(g, O2(rhs_u), O2(rhs_v), O2(za), O2(zb), grav, w1, w, do_rhs, do_pred, Dt,
                   O2(u_t1), O2(u_t2), O2(v_t1), O2(v_t2), O2(z1), O2(z2),
@@ -1159,13 +1455,15 @@ template <typename R>
 __global__ void __launch_bounds__(kBlock) k_corr_point(
     Geo<R> g, R Dt, R *__restrict__ zeta_t2, const R *__restrict__ rz0, const R *__restrict__ rz1, const R *__restrict__ rz2, R *__restrict__ ubar_t1,
     const R *__restrict__ vbar_t1, const R *__restrict__ rub0, const R *__restrict__ rub1, R *__restrict__ vbar_t2) {
-    corr_point_body(g, Dt, zeta_t2, rz0, rz1, rz2, ubar_t1, vbar_t1, rub0, rub1, vbar_t2,
-                    (long)tid_flat());
+    pdl_enter();
+    corr_point4(g, Dt, zeta_t2, rz0, rz1, rz2, ubar_t1, vbar_t1, rub0, rub1, vbar_t2,
+                4 * (long)tid_flat());
 }
 template <typename R>
 __global__ void __launch_bounds__(kBlock) kb_corr_point(
     const Member<R> *mt, const int2 *bm, R Dt, R *__restrict__ zeta_t2, const R *__restrict__ rz0, const R *__restrict__ rz1,
     const R *__restrict__ rz2, R *__restrict__ ubar_t1, const R *__restrict__ vbar_t1, const R *__restrict__ rub0, const R *__restrict__ rub1, R *__restrict__ vbar_t2) {
+    pdl_enter();
     SF_MEMBER(bm)
     corr_point_body(g, Dt, O2(zeta_t2), O2(rz0), O2(rz1), O2(rz2), O2(ubar_t1), O2(vbar_t1),
                     O2(rub0), O2(rub1), O2(vbar_t2), (long)mb_.y * kBlock + threadIdx.x);
@@ -1273,6 +1571,8 @@ Geo<R> Ops<R>::geo(const sf_ctx *c) {
     Geo<R> g;
     g.I = c->I;
     g.J = c->J;
+    g.dI = make_fastdiv(c->I);
+    g.dJ = make_fastdiv(c->J);
     g.N = c->N;
     g.s2 = c->s2;
     g.h = (const R *)c->metrics[0];
@@ -1300,14 +1600,11 @@ cudaError_t Ops<R>::zeta_rhs(const sf_ctx *c, const R *zeta, const R *ubar, cons
                              R *rzeta, int mode, double cff1, double *Zt, double *DU, double *DV,
                              const R *zeta_t0, R *zeta_t2, double Dt, cudaStream_t s) {
     if (c->nmem > 1) {
-        kb_zeta_rhs<R><<<c->nbm_pt, kBlock, 0, s>>>(mt<R>(c), c->bm_pt, zeta, ubar, vbar, rzeta, mode,
-                                                   cff1, Zt, DU, DV, zeta_t0, zeta_t2, (R)Dt);
-        return cudaGetLastError();
+        return launch_dep(c, kb_zeta_rhs<R>, c->nbm_pt, kBlock, 0, s, mt<R>(c), c->bm_pt, zeta,
+                          ubar, vbar, rzeta, mode, cff1, Zt, DU, DV, zeta_t0, zeta_t2, (R)Dt);
     }
-    k_zeta_rhs<R><<<blocks_for(c->s2, kBlock), kBlock, 0, s>>>(geo(c), zeta, ubar, vbar, rzeta,
-                                                               mode, cff1, Zt, DU, DV, zeta_t0,
-                                                               zeta_t2, (R)Dt);
-    return cudaGetLastError();
+    return launch_dep(c, k_zeta_rhs<R>, blocks_for((c->s2 + 3) / 4, kBlock), kBlock, 0, s, geo(c), zeta,
+                      ubar, vbar, rzeta, mode, cff1, Zt, DU, DV, zeta_t0, zeta_t2, (R)Dt);
 }
 template <typename R>
 cudaError_t Ops<R>::zeta_pred(const sf_ctx *c, double Dt, const R *z0, R *z2, const R *rz1,
@@ -1328,15 +1625,13 @@ cudaError_t Ops<R>::momentum(const sf_ctx *c, R *rhs_u, R *rhs_v, const R *za, c
                              const R *z2, cudaStream_t s) {
     const double w1 = 1 - weight;
     if (c->nmem > 1) {
-        kb_momentum<R><<<c->nbm_pt, kBlock, 0, s>>>(
-            mt<R>(c), c->bm_pt, rhs_u, rhs_v, za, zb, (R)g, (R)w1, (R)weight, do_rhs, do_pred, (R)Dt,
-            u_t1, u_t2, v_t1, v_t2, z1, z2);
-        return cudaGetLastError();
+        return launch_dep(c, kb_momentum<R>, c->nbm_pt, kBlock, 0, s, mt<R>(c), c->bm_pt, rhs_u,
+                          rhs_v, za, zb, (R)g, (R)w1, (R)weight, do_rhs, do_pred, (R)Dt, u_t1,
+                          u_t2, v_t1, v_t2, z1, z2);
     }
-    k_momentum<R><<<blocks_for(c->s2, kBlock), kBlock, 0, s>>>(
-        geo(c), rhs_u, rhs_v, za, zb, (R)g, (R)w1, (R)weight, do_rhs, do_pred, (R)Dt, u_t1, u_t2,
-        v_t1, v_t2, z1, z2);
-    return cudaGetLastError();
+    return launch_dep(c, k_momentum<R>, blocks_for((c->s2 + 3) / 4, kBlock), kBlock, 0, s, geo(c), rhs_u,
+                      rhs_v, za, zb, (R)g, (R)w1, (R)weight, do_rhs, do_pred, (R)Dt, u_t1, u_t2,
+                      v_t1, v_t2, z1, z2);
 }
 template <typename R>
 cudaError_t Ops<R>::am3(const sf_ctx *c, double Dt, R *v, const R *r0, const R *r1, const R *r2,
@@ -1349,13 +1644,11 @@ cudaError_t Ops<R>::corr_point(const sf_ctx *c, double Dt, R *zeta_t2, const R *
                                const R *rz1, const R *rz2, R *ubar_t1, const R *vbar_t1,
                                const R *rub0, const R *rub1, R *vbar_t2, cudaStream_t s) {
     if (c->nmem > 1) {
-        kb_corr_point<R><<<c->nbm_pt, kBlock, 0, s>>>(mt<R>(c), c->bm_pt, (R)Dt, zeta_t2, rz0, rz1,
-                                                     rz2, ubar_t1, vbar_t1, rub0, rub1, vbar_t2);
-        return cudaGetLastError();
+        return launch_dep(c, kb_corr_point<R>, c->nbm_pt, kBlock, 0, s, mt<R>(c), c->bm_pt, (R)Dt,
+                          zeta_t2, rz0, rz1, rz2, ubar_t1, vbar_t1, rub0, rub1, vbar_t2);
     }
-    k_corr_point<R><<<blocks_for(c->s2, kBlock), kBlock, 0, s>>>(
-        geo(c), (R)Dt, zeta_t2, rz0, rz1, rz2, ubar_t1, vbar_t1, rub0, rub1, vbar_t2);
-    return cudaGetLastError();
+    return launch_dep(c, k_corr_point<R>, blocks_for((c->s2 + 3) / 4, kBlock), kBlock, 0, s, geo(c), (R)Dt,
+                      zeta_t2, rz0, rz1, rz2, ubar_t1, vbar_t1, rub0, rub1, vbar_t2);
 }
 template <typename R>
 cudaError_t Ops<R>::bc_apply(const sf_ctx *c, const BcProgram &p1, R *f1, const BcProgram &p2,
@@ -1364,8 +1657,8 @@ cudaError_t Ops<R>::bc_apply(const sf_ctx *c, const BcProgram &p1, R *f1, const 
     if (n == 0 && p1.nch == 0 && p2.nch == 0) return cudaSuccess;
     if (n < p1.ngr) n = p1.ngr;
     if (n < p2.ngr) n = p2.ngr;
-    k_bc_apply<R><<<blocks_for(n > 0 ? n : 1, 256), 256, 0, s>>>(p1, f1, p2, f2, (R)val, valp);
-    return cudaGetLastError();
+    return launch_dep(c, k_bc_apply<R>, blocks_for(n > 0 ? n : 1, 256), 256, 0, s, p1, f1, p2, f2,
+                      (R)val, valp);
 }
 template <typename R>
 cudaError_t Ops<R>::rhs3d(const sf_ctx *c, const R *u, const R *v, const R *Huon, const R *Hvom,

@@ -1,0 +1,391 @@
+// The barotropic predictor of one substep as one kernel (single grids): computeZetaRHS +
+// computeZetaPred, zetabc, computeMomentumRHSPred + computeMomentumPred, barotropicVelocityBC
+// (nonlinear/step2d.py:23-81 with the kernels of mod_cppkernels.cpp:13-186), replacing four
+// launches whose intermediate fields each went through DRAM.
+//
+// A block owns a tile of 32 x 16 rho points (32 x 8 threads, two rows each).  Phase 1
+// computes the predicted zeta on the tile and on a halo of one row (south) and one column
+// (west) into shared memory; phase 2 computes the momentum right-hand side and the
+// predicted ubar/vbar from it.  Interior points with two cells of margin (the "deep" region,
+// 2 <= i <= I-3, 2 <= j <= J-3) hold no boundary destination, so they take the fast path.
+// Points of the outer two-cell ring evaluate everything as pure functions of the step's inputs:
+// a field's value after its boundary program at node x is, by the program's gather semantics
+// (all sources read before any destination is written), its pre-program value at the source
+// node of x (or 0, or the clamped value), and a pre-program value is either computed from the
+// inputs or, where the predictor does not write the node, the node's old content.  So no block
+// waits for another.  Destinations are written with their final values, except those of
+// chained entries (a destination that is also a source, e.g. at corners), whose old content
+// other blocks may still read: the last block to finish writes them.
+#pragma once
+#include "sf_internal.h"
+
+namespace sf {
+
+constexpr int kPredTX = 32, kPredTY = 16;   // tile (nodes); 32 x 8 threads, two rows each
+
+template <typename R>
+struct PredArgs {
+    Geo<R> g;
+    const R *z0, *z1, *ub1, *vb1;   // inputs (zeta_t0, zeta_t1, ubar_t1, vbar_t1)
+    R *z2, *rz, *ru, *rv, *ub2, *vb2;   // outputs (zeta_t2, rzeta_t1, rubar_t1, rvbar_t1, ...)
+    const int *mz, *mu, *mv;        // per-node program maps (kBcNone or code)
+    R Dt, w1, w, grav;
+    R val;                          // clamped value of the ubar/vbar programs
+    const double *valp;             // ... or read from the device (graph replay)
+    BcProgram pz, pu, pv;           // for the chained entries
+    int *counter;                   // blocks done (last-block detection), reset by the last
+};
+
+__device__ __forceinline__ int bc_src(int m) { return (m & (kBcChained - 1)) - 2; }
+
+// computeZetaRHS at an interior node (mod_cppkernels.cpp:81-128), as zeta_rhs_body.
+template <typename R>
+__device__ __forceinline__ R prd_rz(const PredArgs<R> &a, long x) {
+    const Geo<R> &g = a.g;
+    const long I = g.I;
+    const R *h = g.h, *zeta = a.z1;
+    const R Dp = zeta[x] + h[x], Dw = zeta[x - 1] + h[x - 1], De = zeta[x + 1] + h[x + 1];
+    const R Ds = zeta[x - I] + h[x - I], Dn = zeta[x + I] + h[x + I];
+    const R DUp = a.ub1[x] * ((Dp + Dw) * R(0.5));
+    const R DUe = a.ub1[x + 1] * ((De + Dp) * R(0.5));
+    const R DVp = a.vb1[x] * ((Dp + Ds) * R(0.5));
+    const R DVn = a.vb1[x + I] * ((Dn + Dp) * R(0.5));
+    return (((DUe * g.on_u[x + 1] - DUp * g.on_u[x]) + (DVn * g.om_v[x + I] - DVp * g.om_v[x])) *
+            g.pm[x]) * g.pn[x];
+}
+
+// zeta_t2 at x before zetabc: zeta_t0 + Dt * rzeta where i != 0 and j != 0 (rzeta as the
+// node's old value off the interior), else the node's old content (not written).
+template <typename R>
+__device__ __forceinline__ R prd_z2p(const PredArgs<R> &a, long x) {
+    const int j = fdiv((int)x, a.g.dI), i = (int)x - j * a.g.I;
+    if (i == 0 || j == 0) return a.z2[x];
+    const R r = rint_(i, j, a.g.I, a.g.J) ? prd_rz(a, x) : a.rz[x];
+    return a.z0[x] + a.Dt * r;
+}
+
+// zeta_t2 at x after zetabc (its program has no clamped entries: value 0).
+template <typename R>
+__device__ __forceinline__ R prd_z2b(const PredArgs<R> &a, long x) {
+    const int m = a.mz[x];
+    if (m == kBcNone) return prd_z2p(a, x);
+    const int s = bc_src(m);
+    return s >= 0 ? prd_z2p(a, s) : R(0);
+}
+
+// zeta_t2 after zetabc at x from the block's shared tile when x lies in it (the tile and its
+// south/west halo hold exactly these values), else through the pure functions.
+template <typename R>
+struct PrdTile {
+    const R (*s)[kPredTX + 1];
+    int i0, j0;
+};
+template <typename R>
+__device__ __forceinline__ R prd_zb(const PredArgs<R> &a, const PrdTile<R> &t, long x) {
+    const int j = fdiv((int)x, a.g.dI), i = (int)x - j * a.g.I;
+    const int r = j - t.j0 + 1, c = i - t.i0 + 1;
+    if (r >= 0 && r <= kPredTY && c >= 0 && c <= kPredTX && (r | c) != 0) return t.s[r][c];
+    return prd_z2b(a, x);
+}
+
+// computeMomentumRHSPred + computeMomentumPred at x (momentum_body) with zeta_t2 after zetabc.
+template <typename R>
+struct PrdMom {
+    R ru, rv, u2, v2;
+    bool in, pd;
+};
+template <typename R>
+__device__ __forceinline__ PrdMom<R> prd_mom(const PredArgs<R> &a, const PrdTile<R> &t, long x) {
+    const Geo<R> &g = a.g;
+    const long I = g.I, J = g.J;
+    const int j = fdiv((int)x, g.dI), i = (int)x - j * g.I;
+    const R *h = g.h;
+    PrdMom<R> o;
+    o.ru = o.rv = o.u2 = o.v2 = R(0);
+    o.in = rint_(i, j, g.I, g.J);
+    o.pd = (int)x - fdiv((int)x, g.dJ) * g.J != 0 && x >= J;
+    if (!o.in && !o.pd) return o;
+    // x >= 1 here (interior, or x % J != 0)
+    const R zp = prd_zb(a, t, x), zw = prd_zb(a, t, x - 1);
+    const R zs = x - I >= 0 ? prd_zb(a, t, x - I) : R(0);
+    if (o.in) {
+        const R gp = a.w1 * zp + a.w * a.z0[x];
+        const R gw = a.w1 * zw + a.w * a.z0[x - 1];
+        const R gs = a.w1 * zs + a.w * a.z0[x - I];
+        o.ru = (a.grav * g.on_u[x]) * (((h[x] + h[x - 1]) * R(0.5)) * (gp - gw) + R(0.5) * (gp * gp - gw * gw));
+        o.rv = (a.grav * g.om_v[x]) * (((h[x] + h[x - I]) * R(0.5)) * (gp - gs) + R(0.5) * (gp * gp - gs * gs));
+    }
+    if (o.pd) {
+        R ru = o.ru, rv = o.rv;
+        if (!o.in) {
+            ru = a.ru[x];
+            rv = a.rv[x];
+        }
+        const R D1p = a.z1[x] + h[x], D2p = zp + h[x];
+        const R D1U = (D1p + (a.z1[x - 1] + h[x - 1])) * R(0.5);
+        const R D2U = (D2p + (zw + h[x - 1])) * R(0.5);
+        const R hs = ldz(h, x - I);
+        const R D1V = (D1p + (ldz(a.z1, x - I) + hs)) * R(0.5);
+        const R D2V = (D2p + (zs + hs)) * R(0.5);
+        o.u2 = ddiv(a.ub1[x] * D1U + ((a.Dt * ru) * g.pm[x]) * g.pn[x], D2U);
+        o.v2 = ddiv(a.vb1[x] * D1V + ((a.Dt * rv) * g.pm[x]) * g.pn[x], D2V);
+    }
+    return o;
+}
+
+// ubar_t2 / vbar_t2 at x before barotropicVelocityBC (the old content where not predicted).
+template <typename R>
+__device__ __forceinline__ R prd_u2p(const PredArgs<R> &a, const PrdTile<R> &t, long x, int comp) {
+    const PrdMom<R> m = prd_mom(a, t, x);
+    if (m.pd) return comp ? m.v2 : m.u2;
+    return comp ? a.vb2[x] : a.ub2[x];
+}
+
+template <typename R>
+__device__ __forceinline__ R prd_val(const PredArgs<R> &a) {
+    return a.valp ? (R)a.valp[0] : a.val;
+}
+
+// Value after the program of field f (0 zeta, 1 ubar, 2 vbar) at a destination whose source
+// code is s.
+template <typename R>
+__device__ __noinline__ R prd_bc_value(const PredArgs<R> &a, const PrdTile<R> &t, int f, int s) {
+    if (s == -1) return R(0);
+    if (s == -2) return f == 0 ? R(0) : prd_val(a);
+    return f == 0 ? prd_z2p(a, s) : prd_u2p(a, t, s, f - 1);
+}
+
+// An edge-ring node: everything through the pure functions (or the tile); writes its own
+// outputs.
+template <typename R>
+__device__ __noinline__ void prd_edge_node(const PredArgs<R> &a, const PrdTile<R> &t, long x) {
+    const Geo<R> &g = a.g;
+    const int j = fdiv((int)x, g.dI), i = (int)x - j * g.I;
+    const bool in = rint_(i, j, g.I, g.J);
+    // zeta: rzeta (interior), zeta_t2 (i, j != 0), then zetabc
+    R rzx = R(0);
+    if (in) rzx = prd_rz(a, x);
+    const int mz = a.mz[x];
+    R z2v;
+    bool wz;
+    if (mz == kBcNone) {
+        wz = i != 0 && j != 0;
+        z2v = wz ? a.z0[x] + a.Dt * (in ? rzx : a.rz[x]) : R(0);
+    } else {
+        wz = !(mz & kBcChained);
+        z2v = wz ? prd_bc_value(a, t, 0, bc_src(mz)) : R(0);
+    }
+    const PrdMom<R> m = prd_mom(a, t, x);
+    const int mu = a.mu[x], mv = a.mv[x];
+    R u2 = m.u2, v2 = m.v2;
+    bool wu = m.pd, wv = m.pd;
+    if (mu != kBcNone) {
+        wu = !(mu & kBcChained);
+        if (wu) u2 = prd_bc_value(a, t, 1, bc_src(mu));
+    }
+    if (mv != kBcNone) {
+        wv = !(mv & kBcChained);
+        if (wv) v2 = prd_bc_value(a, t, 2, bc_src(mv));
+    }
+    // every read of old contents above; the writes touch only this node
+    if (in) a.rz[x] = rzx;
+    if (wz) a.z2[x] = z2v;
+    if (m.in) {
+        a.ru[x] = m.ru;
+        a.rv[x] = m.rv;
+    }
+    if (wu) a.ub2[x] = u2;
+    if (wv) a.vb2[x] = v2;
+}
+
+__device__ __forceinline__ bool prd_deep(int i, int j, int I, int J) {
+    return i >= 2 && i <= I - 3 && j >= 2 && j <= J - 3;
+}
+
+// computeZetaRHS at a deep node through per-node base pointers (the neighbours at constant
+// offsets), as prd_rz.
+template <typename R>
+__device__ __forceinline__ R prd_rz_deep(const PredArgs<R> &a, long x) {
+    const Geo<R> &g = a.g;
+    const int I = g.I;
+    const R *z = a.z1 + x, *h = g.h + x, *ub = a.ub1 + x, *vb = a.vb1 + x, *ou = g.on_u + x,
+            *ov = g.om_v + x;
+    const R *zN = z + I, *zS = z - I, *hN = h + I, *hS = h - I;
+    const R Dp = z[0] + h[0], Dw = z[-1] + h[-1], De = z[1] + h[1];
+    const R Ds = zS[0] + hS[0], Dn = zN[0] + hN[0];
+    const R DUp = ub[0] * ((Dp + Dw) * R(0.5));
+    const R DUe = ub[1] * ((De + Dp) * R(0.5));
+    const R DVp = vb[0] * ((Dp + Ds) * R(0.5));
+    const R DVn = vb[I] * ((Dn + Dp) * R(0.5));
+    return (((DUe * ou[1] - DUp * ou[0]) + (DVn * ov[I] - DVp * ov[0])) * g.pm[x]) * g.pn[x];
+}
+
+// The fast path of a deep node: momentum from the tile's zeta_t2 at x, x-1 and x-I.
+template <typename R>
+__device__ __forceinline__ void prd_deep_mom(const PredArgs<R> &a, long x, bool pd, R zp, R zw,
+                                             R zs) {
+    const Geo<R> &g = a.g;
+    const int I = g.I;
+    const R *h = g.h + x, *z0 = a.z0 + x, *z1 = a.z1 + x;
+    const R hp = h[0], hw = h[-1], hs = h[-I];
+    const R gp = a.w1 * zp + a.w * z0[0];
+    const R gw = a.w1 * zw + a.w * z0[-1];
+    const R gs = a.w1 * zs + a.w * z0[-I];
+    const R ru = (a.grav * g.on_u[x]) * (((hp + hw) * R(0.5)) * (gp - gw) + R(0.5) * (gp * gp - gw * gw));
+    const R rv = (a.grav * g.om_v[x]) * (((hp + hs) * R(0.5)) * (gp - gs) + R(0.5) * (gp * gp - gs * gs));
+    a.ru[x] = ru;
+    a.rv[x] = rv;
+    if (pd) {
+        const R D1p = z1[0] + hp, D2p = zp + hp;
+        const R D1U = (D1p + (z1[-1] + hw)) * R(0.5);
+        const R D2U = (D2p + (zw + hw)) * R(0.5);
+        const R D1V = (D1p + (z1[-I] + hs)) * R(0.5);
+        const R D2V = (D2p + (zs + hs)) * R(0.5);
+        const R pm = g.pm[x], pn = g.pn[x];
+        a.ub2[x] = ddiv(a.ub1[x] * D1U + ((a.Dt * ru) * pm) * pn, D2U);
+        a.vb2[x] = ddiv(a.vb1[x] * D1V + ((a.Dt * rv) * pm) * pn, D2V);
+    }
+}
+
+// The ring nodes: 4 I nodes of rows 0, 1, J-2, J-1, then 4 (J-4) of columns 0, 1, I-2, I-1.
+__device__ __forceinline__ long prd_ring_node(int e, int I, int J) {
+    if (e < 4 * I) {
+        const int r = e / I, i = e - r * I;
+        const int j = r < 2 ? r : J - 4 + r;
+        return (long)j * I + i;
+    }
+    const int f = e - 4 * I, c = f / (J - 4);
+    const int i = c < 2 ? c : I - 4 + c;
+    return (long)(2 + f - c * (J - 4)) * I + i;
+}
+
+// The first `ring_blocks` blocks take one ring node per thread through the pure functions;
+// the others own tiles of 32 x 16 nodes, lane tx taking column i0+tx of rows j0+ty and
+// j0+ty+8, so every load of a warp is 32 consecutive nodes of one row.  A tile block fills
+// its shared zeta_t2 for ring nodes too (the deep nodes next to the ring read them) but
+// leaves their outputs to the ring blocks.
+template <typename R>
+__global__ void __launch_bounds__(256) k_pred2d(const __grid_constant__ PredArgs<R> a,
+                                                int ring_blocks, int tiles_x) {
+    pdl_enter();
+    __shared__ R sZ[kPredTY + 1][kPredTX + 1];   // zeta_t2 after zetabc, (j0-1.., i0-1..)
+    __shared__ int s_last;
+    const Geo<R> &g = a.g;
+    const int I = g.I, J = g.J;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int tid = ty * 32 + tx;
+    const int bid = (int)blockIdx.x;
+    int i0 = -kPredTX - 2, j0 = -kPredTY - 2;   // ring blocks: a tile no node falls in
+    if (bid < ring_blocks) {
+        const int e = bid * 256 + tid;
+        if (e < 4 * I + 4 * (J - 4)) prd_edge_node(a, PrdTile<R>{sZ, i0, j0}, prd_ring_node(e, I, J));
+    } else {
+        const int tb = bid - ring_blocks;
+        i0 = (tb % tiles_x) * kPredTX;
+        j0 = (tb / tiles_x) * kPredTY;
+        const int i = i0 + tx;
+        // ---- phase 1: zeta_t2 (after zetabc) on the tile and its south/west halo ------------
+#pragma unroll
+        for (int h = 0; h < kPredTY; h += 8) {
+            const int j = j0 + ty + h;
+            if (i < I && j < J) {
+                const long x = (long)j * I + i;
+                R z;
+                if (prd_deep(i, j, I, J)) {
+                    const R r = prd_rz_deep(a, x);
+                    z = a.z0[x] + a.Dt * r;
+                    a.rz[x] = r;
+                    a.z2[x] = z;
+                } else {
+                    z = prd_z2b(a, x);
+                }
+                sZ[ty + h + 1][tx + 1] = z;
+            }
+        }
+        if (ty == 0 && j0 >= 1 && i < I) {   // south halo row
+            const long x = (long)(j0 - 1) * I + i;
+            sZ[0][tx + 1] = prd_deep(i, j0 - 1, I, J) ? a.z0[x] + a.Dt * prd_rz_deep(a, x) : prd_z2b(a, x);
+        }
+        if (ty == 1 && tx < kPredTY && i0 >= 1 && j0 + tx < J) {   // west halo column
+            const long x = (long)(j0 + tx) * I + i0 - 1;
+            sZ[tx + 1][0] = prd_deep(i0 - 1, j0 + tx, I, J) ? a.z0[x] + a.Dt * prd_rz_deep(a, x)
+                                                              : prd_z2b(a, x);
+        }
+        __syncthreads();
+        // ---- phase 2: momentum of the deep nodes ---------------------------------------------
+#pragma unroll
+        for (int h = 0; h < kPredTY; h += 8) {
+            const int j = j0 + ty + h;
+            if (i < I && j < J && prd_deep(i, j, I, J)) {
+                const int q = j * I + i;
+                const bool pd = q - fdiv(q, g.dJ) * J != 0 && q >= J;   // q % J != 0 (szJ)
+                const int r = ty + h + 1, c = tx + 1;
+                prd_deep_mom(a, (long)q, pd, sZ[r][c], sZ[r][c - 1], sZ[r - 1][c]);
+            }
+        }
+    }
+
+    // ---- chained destinations: the last block, after every block's reads -------------------
+    // A thread reaches the barrier only after each of its loads has returned (every loaded
+    // value feeds a store or a branch before it), so once a block has counted itself, none of
+    // its reads of old contents is pending and the last block may overwrite them.
+    __syncthreads();
+    if (tid == 0) s_last = atomicAdd(a.counter, 1) == (int)gridDim.x - 1;
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    const PrdTile<R> t{sZ, i0, j0};
+    const BcProgram *ps[3] = {&a.pz, &a.pu, &a.pv};
+    R v[3] = {R(0), R(0), R(0)};
+    int d[3] = {-1, -1, -1};
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+        const BcProgram &p = *ps[f];
+        if (tid < p.nch) {
+            d[f] = p.dst_ch[tid];
+            v[f] = prd_bc_value(a, t, f, p.src_ch[tid]);
+        }
+    }
+    __syncthreads();
+    if (d[0] >= 0) a.z2[d[0]] = v[0];
+    if (d[1] >= 0) a.ub2[d[1]] = v[1];
+    if (d[2] >= 0) a.vb2[d[2]] = v[2];
+    if (tid == 0) *a.counter = 0;
+}
+
+template <typename R>
+cudaError_t Ops<R>::pred2d(const sf_ctx *c, R *z0, R *z1, R *z2, R *ub1, R *vb1, R *ub2, R *vb2,
+                           R *rz, R *ru, R *rv, double Dt, double weight, double val,
+                           const double *valp, cudaStream_t s) {
+    PredArgs<R> a;
+    a.g = geo(c);
+    a.z0 = z0;
+    a.z1 = z1;
+    a.ub1 = ub1;
+    a.vb1 = vb1;
+    a.z2 = z2;
+    a.rz = rz;
+    a.ru = ru;
+    a.rv = rv;
+    a.ub2 = ub2;
+    a.vb2 = vb2;
+    a.mz = c->bcmap;
+    a.mu = c->bcmap + c->s2;
+    a.mv = c->bcmap + 2 * c->s2;
+    a.Dt = (R)Dt;
+    a.w1 = (R)(1.0 - weight);
+    a.w = (R)weight;
+    a.grav = (R)10.0;
+    a.val = (R)val;
+    a.valp = valp;
+    a.pz = c->zbc;
+    a.pu = c->ubc;
+    a.pv = c->vbc;
+    a.counter = c->pred_counter;
+    const int tiles_x = (c->I + kPredTX - 1) / kPredTX, tiles_y = (c->J + kPredTY - 1) / kPredTY;
+    const int ring_blocks = (4 * c->I + 4 * (c->J - 4) + 255) / 256;
+    return launch_dep(c, k_pred2d<R>, dim3((unsigned)(ring_blocks + tiles_x * tiles_y)), dim3(32, 8),
+                      0, s, a, ring_blocks, tiles_x);
+}
+
+}  // namespace sf

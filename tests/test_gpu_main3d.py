@@ -68,10 +68,12 @@ def test_main3d_fp32_error_stated():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("ndtfast", [4, 5, 7, 30])
-def test_graph_replay_of_the_barotropic_loop_is_identical(ndtfast):
+@pytest.mark.parametrize("ndtfast,precision", [(4, "fp64"), (5, "fp64"), (7, "fp64"),
+                                               (30, "fp64"), (30, "fp32")])
+def test_graph_replay_of_the_barotropic_loop_is_identical(ndtfast, precision):
     """sf_barotropic_loop replayed from captured CUDA graphs (the default) against plain
-    launches, over steps whose slot rotation cycles through all three phases."""
+    launches, with and without programmatic dependent launch and the fused predictor, over
+    steps whose slot rotation cycles through all three phases: bit-identical in FP64."""
     import numpy as np
     import torch
     from sailfish_b200 import configs
@@ -81,13 +83,21 @@ def test_graph_replay_of_the_barotropic_loop_is_identical(ndtfast):
     g = cfg["grid"]
     bump = 1e-3 * np.exp(-((g.x - g.x.max() / 2) ** 2 + (g.y - g.y.max() / 2) ** 2) / (1e5) ** 2)
     out = []
-    for graphs in (1, 0):
-        m = Model(g, cfg["boundary"], cfg["dt"], cfg["ndtfast"], precision="fp64")
+    for graphs, pdl, fused in ((0, 0, 0), (1, 1, 1), (0, 1, 1), (1, 0, 0), (0, 0, 1)):
+        m = Model(g, cfg["boundary"], cfg["dt"], cfg["ndtfast"], precision=precision)
+        assert lib.sf_ctx_fused_available(m.ctx.ptr) == 1
         assert lib.sf_ctx_set_graphs(m.ctx.ptr, graphs) == 0
+        assert lib.sf_ctx_set_pdl(m.ctx.ptr, pdl) == 0
+        assert lib.sf_ctx_set_fused(m.ctx.ptr, fused) == 0
         m.Zt_avg1.copy_(torch.from_numpy(bump.ravel()))
         m.step(4)
         torch.cuda.synchronize()
         out.append(m.state())
-    for k in ("zeta", "ubar", "vbar", "u", "v", "Zt_avg1", "DU_avg1", "W"):
-        np.testing.assert_array_equal(out[0][k], out[1][k], err_msg=k)
-    assert out[0]["slots"] == out[1]["slots"]
+    for o in out[1:]:
+        for k in ("zeta", "ubar", "vbar", "u", "v", "Zt_avg1", "DU_avg1", "W"):
+            if precision == "fp64":
+                np.testing.assert_array_equal(o[k], out[0][k], err_msg=k)
+            else:   # the fused predictor's FP32 contractions may differ from the unfused ones
+                scale = max(np.abs(out[0][k]).max(), 1e-30)
+                assert np.abs(o[k] - out[0][k]).max() <= 1e-5 * scale, k
+        assert o["slots"] == out[0]["slots"]
