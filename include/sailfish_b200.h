@@ -297,20 +297,25 @@ int sf_analytic_bvf(sf_ctx *ctx, const void *z_w, double dT, double zscale, doub
 
 /* ---- learned closure (no counterpart in the reference) --------------------------------------
  * A per-column MLP standing in for the GLS corrector's Akv/Akt: SF_MLP_LAYERS dense layers of
- * width 128 (inputs and outputs zero-padded to 128), GELU between them, BF16 weights W[l]
+ * width 128 (inputs and outputs zero-padded to 128), GELU or ReLU (`act`) between them, BF16
+ * weights W[l]
  * ([out][in], row-major, device) and FP32 biases b[l] (device); products on the tensor cores
  * (tcgen05) with FP32 accumulation.  Rows are samples (one water column each), 128 FP32
  * values per row.  `err` is a device int set to 1 if a bounded wait on the tensor cores gave
  * up.  Error text of these entry points: sf_mlp_last_error(). */
 #define SF_MLP_LAYERS 5
 #define SF_MLP_WIDTH 128
+#define SF_MLP_GELU 0   /* tanh form */
+#define SF_MLP_RELU 1
 typedef struct sf_mlp_params {
     const void *W[SF_MLP_LAYERS];
     const float *b[SF_MLP_LAYERS];
+    int act;   /* SF_MLP_GELU (0, the zero-initialised default) or SF_MLP_RELU */
 } sf_mlp_params;
 
 const char *sf_mlp_last_error(void);
-/* O[r, :] = act(A B^T + bias) for a 128-wide B: A is element (r, k) = A[r*a_rs + k*a_ks]
+/* O[r, :] = act(A B^T + bias) for a 128-wide B (act 0: none, 1: GELU, 2: ReLU): A is element
+ * (r, k) = A[r*a_rs + k*a_ks]
  * (n_rows x K, FP32 or BF16), B likewise (128 x K); K a multiple of 16; optional pre-activation
  * copy Z.  The dense-product building block of the forward and backward passes. */
 int sf_mlp_gemm(int n_rows, int K, const void *A, int a_bf16, long a_rs, long a_ks,

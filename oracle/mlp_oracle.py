@@ -26,35 +26,46 @@ def gelu_grad(x):
     return 0.5 * (1.0 + t) + 0.5 * x * (1.0 - t * t) * C_GELU * (1.0 + 3.0 * 0.044715 * x * x)
 
 
-def gemm(A, B, bias=None, act=False):
-    """act(bf16(A) bf16(B)^T + bias)."""
+def relu(x):
+    return np.maximum(x, 0.0)
+
+
+def relu_grad(x):
+    return (x > 0.0).astype(np.float64)
+
+
+ACTS = {"gelu": (gelu, gelu_grad), "relu": (relu, relu_grad)}
+
+
+def gemm(A, B, bias=None, act=False, kind="gelu"):
+    """act(bf16(A) bf16(B)^T + bias), act GELU (tanh form) or ReLU."""
     z = bf16(A) @ bf16(B).T
     if bias is not None:
         z = z + bias
-    return (gelu(z) if act else z), z
+    return (ACTS[kind][0](z) if act else z), z
 
 
-def forward(W, b, X):
+def forward(W, b, X, kind="gelu"):
     """Returns output, list of layer inputs, list of pre-activations."""
     a = np.asarray(X, np.float64)
     ins, pres = [], []
     for l in range(len(W)):
         last = l == len(W) - 1
         ins.append(a)
-        a, z = gemm(a, W[l], b[l], act=not last)
+        a, z = gemm(a, W[l], b[l], act=not last, kind=kind)
         pres.append(z)
         if not last:
             a = a.astype(np.float32).astype(np.float64)   # activations are stored in FP32
     return a, ins, pres
 
 
-def backward(W, ins, pres, dY):
+def backward(W, ins, pres, dY, kind="gelu"):
     """Gradients (dW, db) for output gradient dY, products with BF16-rounded operands."""
     L = len(W)
     dW, db = [None] * L, [None] * L
     g = np.asarray(dY, np.float64)
     for l in range(L - 1, -1, -1):
-        G = g if l == L - 1 else g * gelu_grad(pres[l])
+        G = g if l == L - 1 else g * ACTS[kind][1](pres[l])
         G = G.astype(np.float32).astype(np.float64)
         dW[l] = bf16(G).T @ bf16(ins[l])
         db[l] = G.sum(axis=0)

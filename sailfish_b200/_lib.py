@@ -40,7 +40,10 @@ class GlsParams(ctypes.Structure):
 
 
 class MlpParams(ctypes.Structure):
-    _fields_ = [("W", _vp * 5), ("b", _vp * 5)]
+    _fields_ = [("W", _vp * 5), ("b", _vp * 5), ("act", ctypes.c_int)]
+
+
+MLP_ACT = {"gelu": 0, "relu": 1}   # sf_mlp_params.act
 
 
 class State2D(ctypes.Structure):

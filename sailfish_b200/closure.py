@@ -19,7 +19,7 @@ import numpy as np
 import torch
 
 from . import configs
-from ._lib import GlsParams, MlpParams, check, lib
+from ._lib import MLP_ACT, GlsParams, MlpParams, check, lib
 from .model import Model, stream_handle
 
 LAYERS, WIDTH = 5, 128
@@ -255,14 +255,17 @@ def targets(Akv, Akt, N):
 # the network and its training
 # -------------------------------------------------------------------------------------------
 class Network:
-    """SF_MLP_LAYERS x 128 network: FP32 master weights and Adam moments, BF16 copies for the
-    tensor cores.  Inputs are normalised with the training set's per-feature mean and spread,
+    """SF_MLP_LAYERS x 128 network (ReLU between layers by default, or GELU): FP32 master weights
+    and Adam moments, BF16 copies for the tensor cores.  Inputs are normalised with the training set's per-feature mean and spread,
     which `inference_params()` folds into the first layer."""
 
-    def __init__(self, N, seed=0, device="cuda"):
+    def __init__(self, N, seed=0, device="cuda", act="relu"):
         if nfeat(N) > WIDTH:
             raise ValueError("the closure's rows hold at most 62 interior W levels")
+        if act not in MLP_ACT:
+            raise ValueError("act must be one of %s" % sorted(MLP_ACT))
         self.N = int(N)
+        self.act = act
         gen = torch.Generator().manual_seed(seed)
         self.W = [(torch.randn(WIDTH, WIDTH, generator=gen) * math.sqrt(2.0 / WIDTH)).to(device)
                   for _ in range(LAYERS)]
@@ -287,6 +290,7 @@ class Network:
         for l in range(LAYERS):
             P.W[l] = W[l].data_ptr()
             P.b[l] = b[l].data_ptr()
+        P.act = MLP_ACT[self.act]
         return P
 
     def inference_params(self):
@@ -365,7 +369,7 @@ class Network:
 
     def save(self, path, **meta):
         """Master weights, normalisation and training range (NumPy .npz) plus `meta`."""
-        np.savez(path, N=self.N, W=np.stack([w.cpu().numpy() for w in self.W]),
+        np.savez(path, N=self.N, act=self.act, W=np.stack([w.cpu().numpy() for w in self.W]),
                  b=np.stack([b.cpu().numpy() for b in self.b]), mu=self.mu.cpu().numpy(),
                  isd=self.isd.cpu().numpy(), lo=self.lo.cpu().numpy(), hi=self.hi.cpu().numpy(),
                  **{k: np.asarray(v) for k, v in meta.items()})
@@ -373,7 +377,8 @@ class Network:
     @classmethod
     def load(cls, path, device="cuda"):
         d = np.load(path)
-        net = cls(int(d["N"]), device=device)
+        # files without an activation entry hold GELU networks
+        net = cls(int(d["N"]), device=device, act=str(d["act"]) if "act" in d else "gelu")
         t = lambda a: torch.tensor(np.asarray(a, np.float32), device=device)
         net.W = [t(w) for w in d["W"]]
         net.b = [t(b) for b in d["b"]]

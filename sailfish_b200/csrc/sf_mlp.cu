@@ -146,9 +146,15 @@ __device__ __forceinline__ float gelu_grad(float x) {
     const float t = tanhf(u);
     return 0.5f * (1.f + t) + 0.5f * x * (1.f - t * t) * c * (1.f + 3.f * 0.044715f * x * x);
 }
+// Activation codes of k_gemm and the backward pass: 0 none, 1 GELU, 2 ReLU.
+constexpr int kActNone = 0, kActGelu = 1, kActRelu = 2;
+__device__ __forceinline__ float act_apply(float z, int act) {
+    return act == kActGelu ? gelu(z) : (act == kActRelu ? fmaxf(z, 0.f) : z);
+}
+inline int act_code(const sf_mlp_params *w) { return w->act == SF_MLP_RELU ? kActRelu : kActGelu; }
 
 // D tile (blockIdx.x) = A[m0:m0+128, 0:K] B[0:128, 0:K]^T, K a multiple of 16, staged 128 K
-// at a time.  Epilogue: v = D + bias; Z[r, n] = v (optional); O[r, n] = act ? GELU(v) : v.
+// at a time.  Epilogue: v = D + bias; Z[r, n] = v (optional); O[r, n] = act(v).
 __global__ void __launch_bounds__(kThreads) k_gemm(Mat A, Mat B, long Mrows, int K,
                                                    const float *__restrict__ bias, int act,
                                                    float *__restrict__ O, long ldo,
@@ -205,7 +211,7 @@ __global__ void __launch_bounds__(kThreads) k_gemm(Mat A, Mat B, long Mrows, int
                     const int n = c * 32 + k;
                     const float z = v[k] + (bias ? bias[n] : 0.f);
                     if (Z) Z[r * ldz + n] = z;
-                    O[r * ldo + n] = act ? gelu(z) : z;
+                    O[r * ldo + n] = act_apply(z, act);
                 }
             }
         }
@@ -217,11 +223,14 @@ __global__ void __launch_bounds__(kThreads) k_gemm(Mat A, Mat B, long Mrows, int
     if (warp == 0) tmem_dealloc(tmem);
 }
 
-// G = dA * GELU'(Z) (elementwise, n x 128)
-__global__ void k_gelu_back(long n, const float *__restrict__ dA, const float *__restrict__ Z,
-                            float *__restrict__ G) {
+// G = dA * act'(Z) (elementwise, n x 128; ReLU' taken as 0 at 0)
+__global__ void k_act_back(long n, const float *__restrict__ dA, const float *__restrict__ Z,
+                           float *__restrict__ G, int act) {
     const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e < n * kTile) G[e] = dA[e] * gelu_grad(Z[e]);
+    if (e < n * kTile) {
+        const float z = Z[e];
+        G[e] = dA[e] * (act == kActRelu ? (z > 0.f ? 1.f : 0.f) : gelu_grad(z));
+    }
 }
 
 // db[j] = sum_m G[m, j]
@@ -291,24 +300,36 @@ __device__ __forceinline__ float gelu_fast(float x) {
     return 0.5f * x * (1.f + t);
 }
 
-// GELU(v + bias) of 32 consecutive outputs of row r, as the next layer's BF16 operand: four
+template <int ACT>
+__device__ __forceinline__ float act_fast(float x) {
+    if constexpr (ACT == kActRelu) return fmaxf(x, 0.f);
+    else return gelu_fast(x);
+}
+
+// act(v + bias) of 32 consecutive outputs of row r, as the next layer's BF16 operand: four
 // 16-byte stores, one per core-matrix row segment.
+template <int ACT>
 __device__ __forceinline__ void store_act8x4(__nv_bfloat16 *sA, int r, int n0, const float *v,
                                              const float *bias) {
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
+        // the 8 biases of this segment as two 16-byte loads (bias is 16-byte aligned, n0 % 32 == 0)
+        const float4 ba = reinterpret_cast<const float4 *>(bias + n0 + 8 * q)[0];
+        const float4 bb = reinterpret_cast<const float4 *>(bias + n0 + 8 * q)[1];
+        const float bv[8] = {ba.x, ba.y, ba.z, ba.w, bb.x, bb.y, bb.z, bb.w};
         uint32_t pk[4];
 #pragma unroll
         for (int h = 0; h < 4; ++h) {
             const int k = 8 * q + 2 * h;
-            const float b0 = bias ? bias[n0 + k] : 0.f, b1 = bias ? bias[n0 + k + 1] : 0.f;
-            const __nv_bfloat162 b2 = __floats2bfloat162_rn(gelu_fast(v[k] + b0), gelu_fast(v[k + 1] + b1));
+            const __nv_bfloat162 b2 = __floats2bfloat162_rn(act_fast<ACT>(v[k] + bv[2 * h]),
+                                                            act_fast<ACT>(v[k + 1] + bv[2 * h + 1]));
             pk[h] = *reinterpret_cast<const uint32_t *>(&b2);
         }
         *reinterpret_cast<uint4 *>(&sA[cm_index(r, n0 + 8 * q)]) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
     }
 }
 
+template <int ACT>
 __global__ void __launch_bounds__(kInferThreads, 1) k_infer(InferW w, long n,
                                                             const float *__restrict__ X,
                                                             float *__restrict__ Y, int *err) {
@@ -317,7 +338,7 @@ __global__ void __launch_bounds__(kInferThreads, 1) k_infer(InferW w, long n,
     __nv_bfloat16 *sW = sA + kTile * kTile;
     __shared__ __align__(8) uint64_t mbar;
     __shared__ uint32_t tmem_base;
-    __shared__ float sbias[SF_MLP_LAYERS][kTile];
+    __shared__ __align__(16) float sbias[SF_MLP_LAYERS][kTile];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (warp == 0) tmem_alloc(&tmem_base);
     if (tid == 0) {
@@ -386,7 +407,7 @@ __global__ void __launch_bounds__(kInferThreads, 1) k_infer(InferW w, long n,
                 tmem_ld32(tmem + trow + cb + c * 32, v);
                 const int n0 = cb + c * 32;
                 if (!last) {
-                    store_act8x4(sA, rl, n0, v, sbias[l]);
+                    store_act8x4<ACT>(sA, rl, n0, v, sbias[l]);
                 } else if (r < n) {
                     float4 *y = reinterpret_cast<float4 *>(Y + r * kTile + n0);
 #pragma unroll
@@ -456,7 +477,7 @@ __global__ void k_features(Geo<R> g, const R *__restrict__ u, const R *__restric
 #define AT(A, k, q) ((float)(A)[(long)(k) * s2 + (q)])
     const int nl = N - 1;   // interior W levels; 2 nl + 3 <= 128 is checked by the caller
     for (int k = 1; k < N; ++k) {
-        const float cff = 0.5f / (AT(z_r, k, p) - AT(z_r, k - 1, p));
+        const float cff = __fdividef(0.5f, AT(z_r, k, p) - AT(z_r, k - 1, p));
         const float du = (AT(u, k, p) - AT(u, k - 1, p)) + (AT(u, k, p + 1) - AT(u, k - 1, p + 1));
         const float dv = (AT(v, k, p) - AT(v, k - 1, p)) + (AT(v, k, p + I) - AT(v, k - 1, p + I));
         const float sh2 = (cff * du) * (cff * du) + (cff * dv) * (cff * dv);
@@ -507,6 +528,12 @@ __global__ void __launch_bounds__(128) k_closure_rows(Geo<R> g, const R *__restr
         const R *__restrict__ sustr, const R *__restrict__ svstr, int nfeat,
         const float *__restrict__ lo, const float *__restrict__ hi, uint8_t *__restrict__ fallback,
         int *__restrict__ flist, int *__restrict__ fcount, __nv_bfloat16 *__restrict__ Xt, long nrows) {
+    __shared__ float slo[kTile], shi[kTile];   // the range box, read by every feature check
+    for (int f = threadIdx.x; f < kTile; f += blockDim.x) {
+        slo[f] = f < nfeat ? lo[f] : 0.f;
+        shi[f] = f < nfeat ? hi[f] : 0.f;
+    }
+    __syncthreads();
     const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= nrows) return;
     const long s2 = g.s2, I = g.I;
@@ -515,20 +542,23 @@ __global__ void __launch_bounds__(128) k_closure_rows(Geo<R> g, const R *__restr
     const int r = (int)(p % kTile);
     const bool col = p < s2 && column_((int)(p % g.I), (int)(p / g.I), g.I, g.J);
     bool out = false;
-#define AT(A, k, q) ((float)(A)[(long)(k) * s2 + (q)])
+    // column pointers, advanced one level (s2) per shear feature; the level below in registers
+    const R *zc = z_r + p, *uc = u + p, *vc = v + p;
     float zb = 0.f, ub = 0.f, ube = 0.f, vb = 0.f, vbn = 0.f;
     if (col) {
-        zb = AT(z_r, 0, p);
-        ub = AT(u, 0, p);
-        ube = AT(u, 0, p + 1);
-        vb = AT(v, 0, p);
-        vbn = AT(v, 0, p + I);
+        zb = (float)zc[0];
+        ub = (float)uc[0];
+        ube = (float)uc[1];
+        vb = (float)vc[0];
+        vbn = (float)vc[I];
     }
-    int ks = 1;   // next shear level
-    auto shear = [&](int k) {   // feature of W level k, carrying level k into the registers
-        const float zt = AT(z_r, k, p), ut = AT(u, k, p), ute = AT(u, k, p + 1);
-        const float vt = AT(v, k, p), vtn = AT(v, k, p + I);
-        const float cff = 0.5f / (zt - zb);
+    auto shear = [&]() {   // feature of the next W level, carrying that level into registers
+        zc += s2;
+        uc += s2;
+        vc += s2;
+        const float zt = (float)zc[0], ut = (float)uc[0], ute = (float)uc[1];
+        const float vt = (float)vc[0], vtn = (float)vc[I];
+        const float cff = __fdividef(0.5f, zt - zb);
         const float du = (ut - ub) + (ute - ube), dv = (vt - vb) + (vtn - vbn);
         const float sh2 = (cff * du) * (cff * du) + (cff * dv) * (cff * dv);
         zb = zt;
@@ -539,7 +569,7 @@ __global__ void __launch_bounds__(128) k_closure_rows(Geo<R> g, const R *__restr
         return flog10(sh2 + 1e-12f);
     };
     auto n2f = [&](int k) {
-        const float n2 = AT(bvf, k, p);
+        const float n2 = (float)bvf[(long)k * s2 + p];
         return copysignf(flog10(1.f + fabsf(n2) * 1e8f), n2);
     };
     auto put8 = [&](int f0, const float *x) {
@@ -555,7 +585,7 @@ __global__ void __launch_bounds__(128) k_closure_rows(Geo<R> g, const R *__restr
 #pragma unroll
         for (int h = 0; h < 8; ++h) {
             const int f = f0 + h;
-            if (f < nfeat && !(x[h] >= lo[f] && x[h] <= hi[f])) out = true;
+            if (f < nfeat && !(x[h] >= slo[f] && x[h] <= shi[f])) out = true;
         }
     };
     int f0 = 0;
@@ -563,7 +593,7 @@ __global__ void __launch_bounds__(128) k_closure_rows(Geo<R> g, const R *__restr
         for (; f0 + 8 <= nl; f0 += 8) {
             float x[8];
 #pragma unroll
-            for (int h = 0; h < 8; ++h) x[h] = shear(ks++);
+            for (int h = 0; h < 8; ++h) x[h] = shear();
             check8(f0, x);
             put8(f0, x);
         }
@@ -580,7 +610,7 @@ __global__ void __launch_bounds__(128) k_closure_rows(Geo<R> g, const R *__restr
                 float val = 0.f;
                 if (col) {
                     if (f < nl) {
-                        val = shear(ks++);
+                        val = shear();
                     } else if (f < 2 * nl) {
                         val = n2f(f - nl + 1);
                     } else if (f == 2 * nl) {
@@ -597,7 +627,6 @@ __global__ void __launch_bounds__(128) k_closure_rows(Geo<R> g, const R *__restr
         if (col) check8(f0, x);
         put8(f0, x);
     }
-#undef AT
     if (p < s2) {
         fallback[p] = out ? 1 : 0;
         if (out && flist) flist[atomicAdd(fcount, 1)] = (int)p;
@@ -633,7 +662,7 @@ __device__ __forceinline__ void tmem_dealloc256(uint32_t taddr) {
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(kTmemCols2));
 }
 
-template <typename R>
+template <typename R, int ACT>
 __global__ void __launch_bounds__(kClosureThreads, 1) k_closure_mlp(Geo<R> g, InferW w,
         const __nv_bfloat16 *__restrict__ Xt, long ntiles, const uint8_t *__restrict__ fallback,
         R *__restrict__ Akv, R *__restrict__ Akt, int *err) {
@@ -643,7 +672,7 @@ __global__ void __launch_bounds__(kClosureThreads, 1) k_closure_mlp(Geo<R> g, In
     __nv_bfloat16 *const sW = sA1 + kTile * kTile;
     __shared__ __align__(8) uint64_t mbar[2], xbar[2];
     __shared__ uint32_t tmem_base;
-    __shared__ float sbias[SF_MLP_LAYERS][kTile];
+    __shared__ __align__(16) float sbias[SF_MLP_LAYERS][kTile];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int nl = g.N - 1;
     const long s2 = g.s2, G = gridDim.x;
@@ -731,19 +760,29 @@ __global__ void __launch_bounds__(kClosureThreads, 1) k_closure_mlp(Geo<R> g, In
                 float vv[32];
                 tmem_ld32(tmem + (uint32_t)(b * kTile) + trow + n0, vv);
                 if (!last) {
-                    store_act8x4(buf(b), rl, n0, vv, sbias[l]);
+                    store_act8x4<ACT>(buf(b), rl, n0, vv, sbias[l]);
                     fence_before();
                     fence_proxy_async();
                     __syncthreads();
                     if (tid == 0) issue_mma(b, l + 1);   // overlaps the other slot's epilogue
                 } else if (apply[b]) {
+                    // outputs n0.. of this column: Akv at levels n+1 for n < nl, then Akt at
+                    // levels n-nl+1 for n < 2nl; the destination advances one level (s2) a step
                     const long p = pr[b];
-#pragma unroll 8
-                    for (int k = 0; k < 32; ++k) {
-                        const int n = n0 + k;
-                        const float y = fexp10(fminf(fmaxf(vv[k] + sbias[l][n], -6.f), -1.f));
-                        if (n < nl) Akv[(long)(n + 1) * s2 + p] = (R)y;
-                        else if (n < 2 * nl) Akt[(long)(n - nl + 1) * s2 + p] = (R)y;
+                    R *dst = n0 < nl ? Akv + (long)(n0 + 1) * s2 + p
+                                     : Akt + (long)(n0 - nl + 1) * s2 + p;
+#pragma unroll
+                    for (int k = 0; k < 32; k += 4) {
+                        const float4 bq = *reinterpret_cast<const float4 *>(&sbias[l][n0 + k]);
+                        const float bv[4] = {bq.x, bq.y, bq.z, bq.w};
+#pragma unroll
+                        for (int h = 0; h < 4; ++h) {
+                            const int n = n0 + k + h;
+                            if (n == nl) dst = Akt + s2 + p;
+                            if (n < 2 * nl)
+                                *dst = (R)fexp10(fminf(fmaxf(vv[k + h] + bv[h], -6.f), -1.f));
+                            dst += s2;
+                        }
                     }
                     fence_before();
                 } else {
@@ -817,7 +856,8 @@ int sf_mlp_forward(const sf_mlp_params *w, int n, const float *X, float *Y, floa
         float *out = last ? Y : (acts ? acts + (long)l * n * ld : nullptr);
         if (!out) return mfail(SF_EINVAL, "activation buffer required");
         float *z = pre ? pre + (long)l * n * ld : nullptr;
-        const int rc = sf_mlp_gemm(n, kTile, in, 0, ld, 1, w->W[l], 1, ld, 1, w->b[l], last ? 0 : 1,
+        const int rc = sf_mlp_gemm(n, kTile, in, 0, ld, 1, w->W[l], 1, ld, 1, w->b[l],
+                                   last ? sf::mlp::kActNone : sf::mlp::act_code(w),
                                    out, ld, z, ld, err, s);
         if (rc) return rc;
         in = out;
@@ -836,7 +876,8 @@ int sf_mlp_backward(const sf_mlp_params *w, int n, const float *X, const float *
     for (int l = SF_MLP_LAYERS - 1; l >= 0; --l) {
         const bool last = l == SF_MLP_LAYERS - 1;
         if (!last) {
-            sf::mlp::k_gelu_back<<<nblk((long)n * ld, 256), 256, 0, S(s)>>>(n, g_in, pre + (long)l * n * ld, G);
+            sf::mlp::k_act_back<<<nblk((long)n * ld, 256), 256, 0, S(s)>>>(
+                n, g_in, pre + (long)l * n * ld, G, sf::mlp::act_code(w));
         } else {
             cudaMemcpyAsync(G, g_in, sizeof(float) * n * ld, cudaMemcpyDeviceToDevice, S(s));
         }
@@ -927,8 +968,12 @@ int sf_mlp_infer(const sf_mlp_params *w, int n, const float *X, float *Y, int *e
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return mcuda(e, "sf_mlp_infer");
     if (dev >= 0 && dev < 64 && !attr_set[dev]) {
-        e = cudaFuncSetAttribute(sf::mlp::k_infer, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)sf::mlp::kInferSmem);
+        e = cudaFuncSetAttribute(sf::mlp::k_infer<sf::mlp::kActGelu>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sf::mlp::kInferSmem);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(sf::mlp::k_infer<sf::mlp::kActRelu>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)sf::mlp::kInferSmem);
         if (e != cudaSuccess) return mcuda(e, "cudaFuncSetAttribute");
         attr_set[dev] = true;
     }
@@ -936,7 +981,12 @@ int sf_mlp_infer(const sf_mlp_params *w, int n, const float *X, float *Y, int *e
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const long tiles = ((long)n + kTile - 1) / kTile;
     const unsigned grid = (unsigned)(tiles < sms ? tiles : sms);
-    sf::mlp::k_infer<<<grid, sf::mlp::kInferThreads, sf::mlp::kInferSmem, S(s)>>>(iw, n, X, Y, err);
+    if (w->act == SF_MLP_RELU)
+        sf::mlp::k_infer<sf::mlp::kActRelu><<<grid, sf::mlp::kInferThreads, sf::mlp::kInferSmem, S(s)>>>(
+            iw, n, X, Y, err);
+    else
+        sf::mlp::k_infer<sf::mlp::kActGelu><<<grid, sf::mlp::kInferThreads, sf::mlp::kInferSmem, S(s)>>>(
+            iw, n, X, Y, err);
     e = cudaGetLastError();
     return e == cudaSuccess ? SF_OK : mcuda(e, "sf_mlp_infer");
 }
@@ -972,13 +1022,18 @@ int sf_closure_step(sf_ctx *c, const sf_mlp_params *w, const void *u, const void
     e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return mcuda(e, "sf_closure_step");
     const int pi = c->prec == SF_FP64 ? 1 : 0;
+    using sf::mlp::k_closure_mlp;
+    using sf::mlp::kActGelu;
+    using sf::mlp::kActRelu;
+    const bool relu = w->act == SF_MLP_RELU;
     if (dev >= 0 && dev < 64 && !attr_set[pi][dev]) {
-        e = pi ? cudaFuncSetAttribute(sf::mlp::k_closure_mlp<double>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)sf::mlp::kClosureSmem)
-               : cudaFuncSetAttribute(sf::mlp::k_closure_mlp<float>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)sf::mlp::kClosureSmem);
+        const int sm = (int)sf::mlp::kClosureSmem;
+        const auto at = cudaFuncAttributeMaxDynamicSharedMemorySize;
+        e = pi ? cudaFuncSetAttribute(k_closure_mlp<double, kActGelu>, at, sm)
+               : cudaFuncSetAttribute(k_closure_mlp<float, kActGelu>, at, sm);
+        if (e == cudaSuccess)
+            e = pi ? cudaFuncSetAttribute(k_closure_mlp<double, kActRelu>, at, sm)
+                   : cudaFuncSetAttribute(k_closure_mlp<float, kActRelu>, at, sm);
         if (e != cudaSuccess) return mcuda(e, "cudaFuncSetAttribute");
         attr_set[pi][dev] = true;
     }
@@ -997,16 +1052,18 @@ int sf_closure_step(sf_ctx *c, const sf_mlp_params *w, const void *u, const void
             g, (const double *)u, (const double *)v, (const double *)z_r, (const double *)bvf,
             (const double *)sustr, (const double *)svstr, nfeat, lo, hi, fallback, fallback_list,
             fallback_count, X, nrows);
-        sf::mlp::k_closure_mlp<double><<<grid, sf::mlp::kClosureThreads, sf::mlp::kClosureSmem, S(s)>>>(
-            g, iw, X, tiles, fallback, (double *)Akv, (double *)Akt, err);
+        (relu ? k_closure_mlp<double, kActRelu> : k_closure_mlp<double, kActGelu>)
+            <<<grid, sf::mlp::kClosureThreads, sf::mlp::kClosureSmem, S(s)>>>(
+                g, iw, X, tiles, fallback, (double *)Akv, (double *)Akt, err);
     } else {
         auto g = sf::Ops<float>::geo(c);
         sf::mlp::k_closure_rows<float><<<nblk(nrows, 128), 128, 0, S(s)>>>(
             g, (const float *)u, (const float *)v, (const float *)z_r, (const float *)bvf,
             (const float *)sustr, (const float *)svstr, nfeat, lo, hi, fallback, fallback_list,
             fallback_count, X, nrows);
-        sf::mlp::k_closure_mlp<float><<<grid, sf::mlp::kClosureThreads, sf::mlp::kClosureSmem, S(s)>>>(
-            g, iw, X, tiles, fallback, (float *)Akv, (float *)Akt, err);
+        (relu ? k_closure_mlp<float, kActRelu> : k_closure_mlp<float, kActGelu>)
+            <<<grid, sf::mlp::kClosureThreads, sf::mlp::kClosureSmem, S(s)>>>(
+                g, iw, X, tiles, fallback, (float *)Akv, (float *)Akt, err);
     }
     e = cudaGetLastError();
     return e == cudaSuccess ? SF_OK : mcuda(e, "sf_closure_step");

@@ -27,7 +27,7 @@ RECIPES = {
 
 
 def train(config, out, runs=16, rest_runs=8, spin=300, every=25, steps=6000, batch=4096, lr=1e-3,
-          seed=1):
+          seed=1, act="relu"):
     """GLS is spun up `spin` steps at fixed forcing (10 h at dt = 120 s: the turbulence fields
     settle to their forced state), then 4 snapshots `every` steps apart are kept."""
     cfg = RECIPES[config]()
@@ -36,7 +36,7 @@ def train(config, out, runs=16, rest_runs=8, spin=300, every=25, steps=6000, bat
                             rest_runs=rest_runs, pattern=True, spread=True)
     Xv, Tv = closure.generate(cfg, runs=4, spin=spin, keep=2, every=every, seed=seed + 1000,
                               rest_runs=2, pattern=True, spread=True)
-    net = closure.Network(N, seed=seed)
+    net = closure.Network(N, seed=seed, act=act)
     net.fit_normalisation(X)
     hist = net.train(X, T, steps=steps, batch=batch, lr=lr, seed=seed, log_every=500)
     e = closure.log_rms(net.infer(Xv), Tv, N)
@@ -44,7 +44,8 @@ def train(config, out, runs=16, rest_runs=8, spin=300, every=25, steps=6000, bat
     const[:, :N - 1] = -3.0
     const[:, N - 1:2 * (N - 1)] = -6.0
     ec = closure.log_rms(const, Tv, N)
-    report = {"config": config, "N": N, "rows": int(X.shape[0]), "heldout_rows": int(Xv.shape[0]),
+    report = {"config": config, "N": N, "act": act, "rows": int(X.shape[0]),
+              "heldout_rows": int(Xv.shape[0]),
               "gls_spinup": spin, "steps": steps, "batch": batch, "loss": hist,
               "heldout_log10_rms_akv": e[0], "heldout_log10_rms_akt": e[1],
               "constant_log10_rms_akv": ec[0], "constant_log10_rms_akt": ec[1]}
@@ -59,8 +60,9 @@ def main():
     ap.add_argument("--out", required=True)
     ap.add_argument("--steps", type=int, default=6000)
     ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--act", default="relu", choices=["relu", "gelu"])
     a = ap.parse_args()
-    print(json.dumps(train(a.config, a.out, steps=a.steps, seed=a.seed)))
+    print(json.dumps(train(a.config, a.out, steps=a.steps, seed=a.seed, act=a.act)))
 
 
 if __name__ == "__main__":

@@ -36,9 +36,10 @@ def _st():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["gelu", "relu"])
 @pytest.mark.parametrize("n", [128, 300, 4096 + 77])
-def test_fused_inference_matches_oracle(n):
-    from sailfish_b200._lib import MlpParams, lib
+def test_fused_inference_matches_oracle(n, kind):
+    from sailfish_b200._lib import MLP_ACT, MlpParams, lib
     rng = np.random.default_rng(n)
     W = [mo.bf16(rng.standard_normal((128, 128)) / np.sqrt(128)) for _ in range(5)]
     b = [rng.standard_normal(128) * 0.05 for _ in range(5)]
@@ -48,6 +49,7 @@ def test_fused_inference_matches_oracle(n):
     P = MlpParams()
     for l in range(5):
         P.W[l], P.b[l] = tW[l].data_ptr(), tb[l].data_ptr()
+    P.act = MLP_ACT[kind]
     tX = torch.tensor(X, device="cuda")
     Y = torch.full((n, 128), float("nan"), device="cuda")
     err = torch.zeros(1, dtype=torch.int32, device="cuda")
@@ -55,7 +57,7 @@ def test_fused_inference_matches_oracle(n):
         lib.sf_mlp_last_error()
     torch.cuda.synchronize()
     assert int(err.item()) == 0
-    ref, _, _ = mo.forward(W, b, X)
+    ref, _, _ = mo.forward(W, b, X, kind)
     got = Y.cpu().numpy()
     assert np.isfinite(got).all()
     # BF16 activations between layers; the hardware tanh differs from tanhf by ~2^-11

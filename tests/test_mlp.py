@@ -102,15 +102,17 @@ class Net:
 
 
 @pytest.mark.gpu
-def test_mlp_forward_and_backward_match_oracle():
+@pytest.mark.parametrize("kind", ["gelu", "relu"])
+def test_mlp_forward_and_backward_match_oracle(kind):
     torch = _cuda()
-    from sailfish_b200._lib import lib
+    from sailfish_b200._lib import lib, MLP_ACT
     n = 256
     rng = np.random.default_rng(3)
     X = rng.standard_normal((n, 128)).astype(np.float32)
     dY = (rng.standard_normal((n, 128)) * 1e-2).astype(np.float32)
     net = Net()
     P = net.device()
+    P.act = MLP_ACT[kind]
     tX, tdY = _t(X), _t(dY)
     Y = torch.zeros((n, 128), device="cuda")
     acts = torch.zeros((4, n, 128), device="cuda")
@@ -127,10 +129,10 @@ def test_mlp_forward_and_backward_match_oracle():
                                _p(work), _p(err), _stream()) == 0, lib.sf_mlp_last_error()
     torch.cuda.synchronize()
     assert int(err.item()) == 0
-    ref, ins, pres = mo.forward(net.W, net.b, X)
+    ref, ins, pres = mo.forward(net.W, net.b, X, kind)
     got = Y.cpu().numpy()
     np.testing.assert_allclose(got, ref, rtol=0, atol=2e-2 * np.abs(ref).max())
-    rdW, rdb = mo.backward(net.W, ins, pres, dY)
+    rdW, rdb = mo.backward(net.W, ins, pres, dY, kind)
     for l in range(5):
         g = dW[l].cpu().numpy()
         assert np.abs(g - rdW[l]).max() <= 3e-2 * np.abs(rdW[l]).max(), l
