@@ -1412,7 +1412,7 @@ namespace sf {
 #define ON(x) ((x) ? (x) + oN : (x))
 
 template <typename R>
-__global__ void __launch_bounds__(kBlock, 4) k_zeta_rhs(
+__global__ void __launch_bounds__(kBlock, 3) k_zeta_rhs(
     Geo<R> g, const R *__restrict__ zeta, const R *__restrict__ ubar, const R *__restrict__ vbar, R *__restrict__ rzeta, int mode, double cff1,
     double *__restrict__ Zt, double *__restrict__ DU, double *__restrict__ DV, const R *__restrict__ zeta_t0, R *__restrict__ zeta_t2, R Dt) {
     pdl_enter();
@@ -1431,7 +1431,7 @@ __global__ void __launch_bounds__(kBlock) kb_zeta_rhs(
 }
 
 template <typename R>
-__global__ void __launch_bounds__(kBlock, 4) k_momentum(
+__global__ void __launch_bounds__(kBlock) k_momentum(
     Geo<R> g, R *__restrict__ rhs_u, R *__restrict__ rhs_v, const R *__restrict__ za, const R *__restrict__ zb, R grav, R w1, R w, int do_rhs,
     int do_pred, R Dt, const R *__restrict__ u_t1, R *__restrict__ u_t2, const R *__restrict__ v_t1, R *__restrict__ v_t2, const R *__restrict__ z1,
     const R *__restrict__ z2) {

@@ -265,7 +265,7 @@ __device__ __forceinline__ long prd_ring_node(int e, int I, int J) {
 // its shared zeta_t2 for ring nodes too (the deep nodes next to the ring read them) but
 // leaves their outputs to the ring blocks.
 template <typename R>
-__global__ void __launch_bounds__(256) k_pred2d(const __grid_constant__ PredArgs<R> a,
+__global__ void __launch_bounds__(256, 5) k_pred2d(const __grid_constant__ PredArgs<R> a,
                                                 int ring_blocks, int tiles_x) {
     pdl_enter();
     __shared__ R sZ[kPredTY + 1][kPredTX + 1];   // zeta_t2 after zetabc, (j0-1.., i0-1..)
