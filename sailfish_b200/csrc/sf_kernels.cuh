@@ -789,34 +789,35 @@ __device__ __forceinline__ void maxflux_omega_body(
     const int N = g.N;
     const int i = pi % g.I, j = pi / g.I;
     const bool un = unode_(i, j), vn = vnode_(i, j, g.J);
-    if (do_flux) {
-        const R onu = g.on_u[p], omv = g.om_v[p];
-        if (un) {
+    const bool om = do_omega && g.bcfield[p] < 0;
+    const bool fu = do_flux && un, fv = do_flux && vn;   // this thread writes Huon / Hvom
+    const R onu = fu ? g.on_u[p] : R(0), omv = fv ? g.om_v[p] : R(0);
+    if (!om) {   // fluxes only
+        if (fu) {
 #pragma unroll 4
             for (int K = 0; K < N; ++K) {
                 const long o = (long)K * s2 + p;
                 Huon[o] = (((Hz[o] + Hz[o - 1]) * R(0.5)) * u[o]) * onu;
             }
         }
-        if (vn) {
+        if (fv) {
 #pragma unroll 4
             for (int K = 0; K < N; ++K) {
                 const long o = (long)K * s2 + p;
                 Hvom[o] = (((Hz[o] + Hz[o - I]) * R(0.5)) * v[o]) * omv;
             }
         }
-    }
-    if (do_omega && g.bcfield[p] < 0) {
-        // Huon at p+1 and Hvom at p+I: recomputed where this kernel also writes them (the value
-        // their owner thread stores), read from memory elsewhere.  p+1 past the row end is the
-        // next row's column 0 and p+I past the last row is row 0 of the next level; neither is
-        // a U or V node.
+    } else {
+        // One pass over the levels: this column's fluxes (written where this kernel computes
+        // them) and the running integral of the flux divergence.  Huon at p+1 and Hvom at p+I
+        // are recomputed where this kernel also writes them (the value their owner thread
+        // stores), read from memory elsewhere (nobody writes them here).  p+1 past the row end
+        // is the next row's column 0 and p+I past the last row is row 0 of the next level;
+        // neither is a U or V node.
         const bool rc = do_flux != 0;
         const bool ue = rc && i + 1 < g.I && unode_(i + 1, j);
         const bool vnn = rc && j + 1 < g.J && vnode_(i, j + 1, g.J);
-        const bool uo = rc && un, vo = rc && vn;
         const R onu_e = ue ? g.on_u[p + 1] : R(0), omv_n = vnn ? g.om_v[p + I] : R(0);
-        const R onu_p = uo ? g.on_u[p] : R(0), omv_p = vo ? g.om_v[p] : R(0);
         // the running integral in shared memory ([level][thread]), not in per-thread local
         // memory, whose footprint over all resident threads spills out of L1 and L2
         extern __shared__ __align__(16) unsigned char mo_smem[];
@@ -825,14 +826,19 @@ __device__ __forceinline__ void maxflux_omega_body(
         R Wk = R(0);
         Wc(0) = R(0);
 #pragma unroll 4
-        for (int K = 1; K < N; ++K) {
+        for (int K = 0; K < N; ++K) {
             const long o = (long)K * s2 + p;
-            const R hue = ue ? (((Hz[o + 1] + Hz[o]) * R(0.5)) * u[o + 1]) * onu_e : Huon[o + 1];
-            const R hup = uo ? (((Hz[o] + Hz[o - 1]) * R(0.5)) * u[o]) * onu_p : Huon[o];
-            const R hvn = vnn ? (((Hz[o + I] + Hz[o]) * R(0.5)) * v[o + I]) * omv_n : Hvom[o + I];
-            const R hvp = vo ? (((Hz[o] + Hz[o - I]) * R(0.5)) * v[o]) * omv_p : Hvom[o];
-            Wk = Wk - ((hue - hup) + (hvn - hvp));
-            Wc(K) = Wk;
+            const R hzp = rc ? Hz[o] : R(0);   // Hz is given (and used) only with the fluxes
+            const R hup = fu ? (((hzp + Hz[o - 1]) * R(0.5)) * u[o]) * onu : Huon[o];
+            const R hvp = fv ? (((hzp + Hz[o - I]) * R(0.5)) * v[o]) * omv : Hvom[o];
+            if (fu) Huon[o] = hup;
+            if (fv) Hvom[o] = hvp;
+            if (K >= 1) {
+                const R hue = ue ? (((Hz[o + 1] + hzp) * R(0.5)) * u[o + 1]) * onu_e : Huon[o + 1];
+                const R hvn = vnn ? (((Hz[o + I] + hzp) * R(0.5)) * v[o + I]) * omv_n : Hvom[o + I];
+                Wk = Wk - ((hue - hup) + (hvn - hvp));
+                Wc(K) = Wk;
+            }
         }
         const R zbed = z_w[p];
         const R h = z_w[(long)(N - 1) * s2 + p] - zbed;
@@ -1470,7 +1476,7 @@ __global__ void __launch_bounds__(kBlock) kb_corr_point(
 }
 
 template <typename R, int TX, int TY>
-__global__ void __launch_bounds__(TX *TY) k_rhs3d(Geo<R> g, const R *__restrict__ u, const R *__restrict__ v,
+__global__ void __launch_bounds__(TX * TY, 5) k_rhs3d(Geo<R> g, const R *__restrict__ u, const R *__restrict__ v,
                                                   const R *Huon, const R *Hvom, const R *__restrict__ W,
                                                   const R *__restrict__ Hz, R *__restrict__ ru, R *__restrict__ rv) {
     rhs3d_body<R, TX, TY>(g, u, v, Huon, Hvom, W, Hz, ru, rv, (int)blockIdx.x, (int)blockIdx.y);
