@@ -43,6 +43,18 @@ DEFAULT = dict(p=3.0, m=1.5, n=-1.0, cmu0=0.5477, c1=1.44, c2=1.92, c3m=-0.4, c3
                sigp=1.30, Kmin=7.6e-6, Pmin=1.0e-12, Akv_bak=1.0e-5, Akt_bak=1.0e-6,
                Akk_bak=5.0e-6, Akp_bak=5.0e-6, Zos=0.02, Zob=0.02, rdrag2=3.0e-3, E2=1.33)
 
+# Other members of the GLS family with the same backgrounds and floors (Warner et al. 2005,
+# Ocean Modelling 8, Table 1): k-omega, and the generic psi = cmu0^p k^m l^n model of Umlauf and
+# Burchard (2003), p = 2, m = 1, n = -0.67 ("gen", the k-psi closure).
+PRESETS = {
+    "k-epsilon": DEFAULT,
+    "k-omega": dict(DEFAULT, p=-1.0, m=0.5, n=-1.0, cmu0=0.5477, c1=0.555, c2=0.833, c3m=-0.6,
+                    c3p=1.0, sigk=2.0, sigp=2.0),
+    "gen": dict(DEFAULT, p=2.0, m=1.0, n=-0.67, cmu0=0.5544, c1=1.0, c2=1.22, c3m=0.05, c3p=1.0,
+                sigk=0.8, sigp=1.07),
+}
+PRESETS["k-psi"] = PRESETS["gen"]
+
 
 def gls_corrector(P, dt, I, J, N, u, v, z_r, Hz, bvf, sustr, svstr, tke, gls, Akv, Akt, Akk, Akp,
                   Lscale, tke_nnew=None, gls_nnew=None):

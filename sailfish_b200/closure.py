@@ -40,16 +40,37 @@ G = 10.0             # modules/mod_constants.py:26
 ALPHA = 1.7e-4       # linear EOS thermal expansion, utility/test.in:453
 
 
+_GLS_BASE = dict(Kmin=7.6e-6, Pmin=1.0e-12, Akv_bak=1.0e-5, Akt_bak=1.0e-6, Akk_bak=5.0e-6,
+                 Akp_bak=5.0e-6, Zos=0.02, Zob=0.02, rdrag2=3.0e-3)
+# Members of the GLS family (psi = cmu0^p k^m l^n), with the floors and backgrounds above:
+# k-epsilon as the reference's input file selects it (utility/test.in:355-367); k-omega and the
+# generic k-psi model of Umlauf and Burchard (2003) ("gen": p = 2, m = 1, n = -0.67) with the
+# constants of Warner et al. (2005, Ocean Modelling 8, Table 1).
+GLS_PRESETS = {
+    "k-epsilon": dict(p=3.0, m=1.5, n=-1.0, cmu0=0.5477, c1=1.44, c2=1.92, c3m=-0.4, c3p=1.0,
+                      sigk=1.0, sigp=1.30),
+    "k-omega": dict(p=-1.0, m=0.5, n=-1.0, cmu0=0.5477, c1=0.555, c2=0.833, c3m=-0.6, c3p=1.0,
+                    sigk=2.0, sigp=2.0),
+    "gen": dict(p=2.0, m=1.0, n=-0.67, cmu0=0.5544, c1=1.0, c2=1.22, c3m=0.05, c3p=1.0,
+                sigk=0.8, sigp=1.07),
+}
+GLS_PRESETS["k-psi"] = GLS_PRESETS["gen"]
+
+
+def gls_preset(name="k-epsilon"):
+    """GlsParams of a named GLS model (GLS_PRESETS)."""
+    if name not in GLS_PRESETS:
+        raise ValueError("GLS model must be one of %s" % sorted(GLS_PRESETS))
+    P = GlsParams()
+    for k, v in dict(_GLS_BASE, **GLS_PRESETS[name]).items():
+        setattr(P, k, v)
+    return P
+
+
 def gls_defaults():
     """k-epsilon GLS (p=3, m=1.5, n=-1: utility/test.in:355-367) with the background and floor
     values of the GLS oracle."""
-    P = GlsParams()
-    for k, v in dict(p=3.0, m=1.5, n=-1.0, cmu0=0.5477, c1=1.44, c2=1.92, c3m=-0.4, c3p=1.0,
-                     sigk=1.0, sigp=1.30, Kmin=7.6e-6, Pmin=1.0e-12, Akv_bak=1.0e-5,
-                     Akt_bak=1.0e-6, Akk_bak=5.0e-6, Akp_bak=5.0e-6, Zos=0.02, Zob=0.02,
-                     rdrag2=3.0e-3).items():
-        setattr(P, k, v)
-    return P
+    return gls_preset("k-epsilon")
 
 
 def _p(t):

@@ -273,17 +273,22 @@ def gls_predictor_step(compTimes, GRID, OCEAN, MIXING):
 
 def gls_corrector_step(compTimes, GRID, OCEAN, MIXING, FORCES):
     """GLS corrector on the reference's state objects.  MIXING: tke, gls, Akt, Akk, Akp,
-    Lscale and bvf ((N+1) W levels each), optional `params` (GlsParams; k-epsilon defaults);
+    Lscale and bvf ((N+1) W levels each), optional `params` (a GlsParams, or the name of a
+    model in closure.GLS_PRESETS: "k-epsilon" (the default), "k-omega", "gen"/"k-psi");
     Akv is OCEAN.AKv.  FORCES: sustr, svstr (kinematic surface stress at U/V points).  u, v
     are OCEAN.u_t2/v_t2; z_r and Hz come from GRID.  When MIXING holds tke_nnew (after
     gls_predictor_step), the new level is first advected (gls_corrector_step.py:172-388, with
     MIXING.gadv, default 1/3, and OCEAN's Huon, Hvom, W) and the corrector starts from it;
     otherwise it starts from Hz_w * tke (no advection)."""
-    from .closure import gls_defaults
+    from .closure import GLS_PRESETS, gls_defaults, gls_preset
     c = _need()
     P = getattr(MIXING, "params", None) or gls_defaults()
+    if isinstance(P, str):
+        if P not in GLS_PRESETS:
+            raise SailfishError("MIXING.params: GLS model must be one of %s" % sorted(GLS_PRESETS))
+        P = gls_preset(P)
     if not isinstance(P, GlsParams):
-        raise SailfishError("MIXING.params must be a GlsParams")
+        raise SailfishError("MIXING.params must be a GlsParams or a GLS model name")
     if getattr(MIXING, "tke_nnew", None) is not None:
         # after gls_predictor_step: advect the new level, then start the corrector from it
         check(lib.sf_gls_advect(

@@ -14,8 +14,8 @@ from gls_case import make
 FIELDS = ("tke", "gls", "Akv", "Akt", "Akk", "Akp", "Lscale")
 
 
-def run_oracle(c, dt=240.0):
-    return go.gls_corrector(go.DEFAULT, dt, c["I"], c["J"], c["N"], c["u"], c["v"], c["z_r"], c["Hz"],
+def run_oracle(c, dt=240.0, P=go.DEFAULT):
+    return go.gls_corrector(P, dt, c["I"], c["J"], c["N"], c["u"], c["v"], c["z_r"], c["Hz"],
                             c["bvf"], c["sustr"], c["svstr"], c["tke"], c["gls"], c["Akv"], c["Akt"],
                             c["Akk"], c["Akp"], c["Lscale"])
 
@@ -54,7 +54,7 @@ def test_oracle_stronger_shear_mixes_more():
     assert np.mean(more["tke"][1:-1, col]) > np.mean(base["tke"][1:-1, col])
 
 
-def gpu_run(c, precision, dt=240.0):
+def gpu_run(c, precision, dt=240.0, preset=go.DEFAULT):
     import ctypes
     import torch
     from sailfish_b200 import host as H
@@ -69,7 +69,7 @@ def gpu_run(c, precision, dt=240.0):
     dt_ = torch.float64 if precision == "fp64" else torch.float32
     T = {k: torch.tensor(np.ascontiguousarray(c[k]), dtype=dt_, device="cuda")
          for k in ("u", "v", "z_r", "Hz", "bvf", "sustr", "svstr") + FIELDS}
-    P = GlsParams(**{k: go.DEFAULT[k] for k, _ in GlsParams._fields_})
+    P = GlsParams(**{k: preset[k] for k, _ in GlsParams._fields_})
     ptr = lambda t: ctypes.c_void_p(t.data_ptr())
     check(lib.sf_gls_corrector(ctx.ptr, ctypes.byref(P), dt, *[ptr(T[k]) for k in
                                ("u", "v", "z_r", "Hz", "bvf", "sustr", "svstr") + FIELDS],
@@ -77,6 +77,41 @@ def gpu_run(c, precision, dt=240.0):
           "sf_gls_corrector")
     torch.cuda.synchronize()
     return {k: T[k].double().cpu().numpy() for k in FIELDS}
+
+
+def test_presets_match_between_library_and_oracle():
+    """The library's named GLS models carry the oracle's constants."""
+    from sailfish_b200 import closure
+    for name in ("k-epsilon", "k-omega", "gen", "k-psi"):
+        P = closure.gls_preset(name)
+        for k, _ in type(P)._fields_:
+            assert getattr(P, k) == go.PRESETS[name][k], (name, k)
+
+
+@pytest.mark.parametrize("name", ["k-omega", "gen"])
+def test_oracle_other_models_floors_and_surface(name):
+    """Other GLS models in the oracle: finite coefficients above their backgrounds and floors,
+    and the surface tke u*^2/cmu0^2 of each model's cmu0 (gls_corrector_step.py:541-544)."""
+    P = go.PRESETS[name]
+    c = make()
+    out = dict(zip(FIELDS, run_oracle(c, P=P)))
+    col = interior(c)
+    assert np.all(np.isfinite(out["Akv"][:, col])) and np.all(np.isfinite(out["gls"][:, col]))
+    assert np.all(out["tke"][:, col] >= P["Kmin"]) and np.all(out["gls"][:, col] >= P["Pmin"])
+    assert np.all(out["Akv"][:, col] >= P["Akv_bak"]) and np.all(out["Akt"][:, col] >= P["Akt_bak"])
+    ustar2 = np.hypot(2 * c["sustr"][col], 2 * c["svstr"][col]) * 0.5
+    np.testing.assert_allclose(out["tke"][-1, col], ustar2 / P["cmu0"] ** 2, rtol=1e-12)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["k-omega", "gen"])
+def test_gls_other_models_fp64_match_oracle(name):
+    """The corrector kernel with the k-omega and generic (k-psi) constants: FP64 within 1e-9."""
+    c = make()
+    ref = dict(zip(FIELDS, run_oracle(c, P=go.PRESETS[name])))
+    got = gpu_run(c, "fp64", preset=go.PRESETS[name])
+    for k in FIELDS:
+        np.testing.assert_allclose(got[k], ref[k], rtol=1e-9, atol=0, err_msg=k)
 
 
 @pytest.mark.gpu
