@@ -466,7 +466,7 @@ __device__ __forceinline__ void corr_point4(
 }
 
 // Boundary programs (see BcProgram): independent entries one per thread over as many blocks
-// as needed; each group of chained entries by one thread, all reads before all writes.
+// as needed; each group of chained entries by one warp, all reads before all writes.
 template <typename R>
 __device__ __forceinline__ R bc_value(const R *f, int s, R val) {
     return s >= 0 ? f[s] : (s == -1 ? R(0) : val);
@@ -484,17 +484,25 @@ __global__ void __launch_bounds__(256) k_bc_apply(BcProgram p1, R *f1, BcProgram
         const long k = t - p1.n;
         f2[p2.dst[k]] = bc_value(f2, p2.src[k], val);
     }
-    // chained entries: group g (one per member) by thread g, all reads before all writes
-    R buf[kMaxChained];
-    if (t < p1.ngr) {
-        const int a = p1.gofs[t], b = p1.gofs[t + 1];
-        for (int k = a; k < b; ++k) buf[k - a] = bc_value(f1, p1.src_ch[k], val);
-        for (int k = a; k < b; ++k) f1[p1.dst_ch[k]] = buf[k - a];
-    }
-    if (t < p2.ngr) {
-        const int a = p2.gofs[t], b = p2.gofs[t + 1];
-        for (int k = a; k < b; ++k) buf[k - a] = bc_value(f2, p2.src_ch[k], val);
-        for (int k = a; k < b; ++k) f2[p2.dst_ch[k]] = buf[k - a];
+    // chained entries: group g (one per member, at most 32 entries) by warp g of the grid, one
+    // entry per lane; every lane reads, the warp synchronises, then every lane writes, so all
+    // reads come before all writes.  (Independent entries neither read nor write a node of a
+    // chained group, so the two parts need no ordering.)
+    const long w = t >> 5;
+    if (w < (long)p1.ngr + p2.ngr) {   // uniform across the warp
+        const bool first = w < p1.ngr;
+        const BcProgram &pp = first ? p1 : p2;
+        R *f = first ? f1 : f2;
+        const int g = (int)(first ? w : w - p1.ngr), lane = (int)(t & 31);
+        const int a = pp.gofs[g], b = pp.gofs[g + 1];
+        int d = -1;
+        R x = R(0);
+        if (lane < b - a) {
+            d = pp.dst_ch[a + lane];
+            x = bc_value(f, pp.src_ch[a + lane], val);
+        }
+        __syncwarp();
+        if (d >= 0) f[d] = x;
     }
 }
 
@@ -1661,8 +1669,8 @@ cudaError_t Ops<R>::bc_apply(const sf_ctx *c, const BcProgram &p1, R *f1, const 
                              R *f2, double val, cudaStream_t s, const double *valp) {
     long n = (long)p1.n + p2.n;
     if (n == 0 && p1.nch == 0 && p2.nch == 0) return cudaSuccess;
-    if (n < p1.ngr) n = p1.ngr;
-    if (n < p2.ngr) n = p2.ngr;
+    const long nw = 32L * ((long)p1.ngr + p2.ngr);   // one warp per chained group
+    if (n < nw) n = nw;
     return launch_dep(c, k_bc_apply<R>, blocks_for(n > 0 ? n : 1, 256), 256, 0, s, p1, f1, p2, f2,
                       (R)val, valp);
 }
