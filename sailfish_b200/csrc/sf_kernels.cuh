@@ -1106,7 +1106,8 @@ __device__ __forceinline__ void step3d_uv_body(const Geo<R> &g, R *__restrict__ 
 // time for V (solveTri gated by isUNode, :525) and where V gets only the mean correction take
 // the general path above after the pipelined part.
 constexpr int kPipeCols = kPipeTile;
-constexpr int kPipeDepth = 6;
+constexpr int kPipeGroup = 2;               // levels consumed per barrier pair
+constexpr int kPipeDepth = 3 * kPipeGroup;  // levels in flight (shared-memory ring slots)
 constexpr int kPipeThreads = 2 * kPipeCols;   // one thread per system (U, V) and column
 constexpr int kPipeSlot = 3 * (2 * kPipeCols + 1) + 4 * kPipeCols;   // floats per level
 
@@ -1178,44 +1179,56 @@ __device__ __forceinline__ void step3d_uv_pipe_body(const Geo<R> &g, float *__re
     float fc = 0.f, fc0 = 0.f, ccp = 0.f, ddp = 0.f;
     double H = 0.0, O = 0.0, Rs = 0.0;
     const int qi = sys == 0 ? col : kPipeCols + 1 + col;   // this system's neighbour in a row
-    for (int k = 0; k < N; ++k) {
-        cp_async_wait<kPipeDepth - 1>();
+    // levels in groups of kPipeGroup: one wait and two barriers per group (kPipeDepth is a
+    // multiple of it, so a group's slots are free together and refilled with the group
+    // kPipeDepth levels up)
+    static_assert(kPipeDepth % kPipeGroup == 0, "levels are consumed in whole groups");
+    auto level = [&](int k) {
+        const float *sl = ring + (k % kPipeDepth) * kPipeSlot;
+        const float *sHz = sl, *sAk = sl + kRow, *sZr = sl + 2 * kRow;
+        const float *sO = sl + 3 * kRow + sys * kPipeCols, *sR = sl + 3 * kRow + (2 + sys) * kPipeCols;
+        const float hz = (sHz[col + 1] + sHz[qi]) * 0.5f;
+        float gk = 0.f;
+        if (k < N - 1) {
+            const float zP1 = sZr[col + 1], zQ1 = sZr[qi];
+            // divisions by layer spacings and pivots (metres): the reciprocal form, as ddiv
+            gk = __fdividef(cm * ((sAk[col + 1] + sAk[qi]) * 0.5f), ((zP1 - zP) + (zQ1 - zQ)) * 0.5f);
+            zP = zP1;
+            zQ = zQ1;
+        }
+        const float ok = sO[col];
+        if (k == 0) {   // bottom row: right-hand side forced to 0 (:610)
+            fc0 = gk;
+            ccp = __fdividef(gk, hz - 2.f * gk);
+            ddp = 0.f;
+        } else {
+            const float rr = hz * (ok + cmn * sR[col]);
+            const float bd = (k < N - 1) ? (hz - gk) - fc : hz - fc;
+            const float iv = __fdividef(1.f, bd - fc * ccp);
+            ccp = gk * iv;
+            ddp = (rr - fc * ddp) * iv;
+            Rs += (double)rr;
+        }
+        cc[k * kPipeThreads] = ccp;
+        dd[k * kPipeThreads] = ddp;
+        fc = gk;
+        H += (double)hz;
+        O += (double)(ok * hz);
+    };
+    for (int k0 = 0; k0 < N; k0 += kPipeGroup) {
+        cp_async_wait<kPipeDepth - kPipeGroup>();
         __syncthreads();
         if (both) {
-            const float *sl = ring + (k % kPipeDepth) * kPipeSlot;
-            const float *sHz = sl, *sAk = sl + kRow, *sZr = sl + 2 * kRow;
-            const float *sO = sl + 3 * kRow + sys * kPipeCols, *sR = sl + 3 * kRow + (2 + sys) * kPipeCols;
-            const float hz = (sHz[col + 1] + sHz[qi]) * 0.5f;
-            float gk = 0.f;
-            if (k < N - 1) {
-                const float zP1 = sZr[col + 1], zQ1 = sZr[qi];
-                // divisions by layer spacings and pivots (metres): the reciprocal form, as ddiv
-                gk = __fdividef(cm * ((sAk[col + 1] + sAk[qi]) * 0.5f), ((zP1 - zP) + (zQ1 - zQ)) * 0.5f);
-                zP = zP1;
-                zQ = zQ1;
-            }
-            const float ok = sO[col];
-            if (k == 0) {   // bottom row: right-hand side forced to 0 (:610)
-                fc0 = gk;
-                ccp = __fdividef(gk, hz - 2.f * gk);
-                ddp = 0.f;
-            } else {
-                const float rr = hz * (ok + cmn * sR[col]);
-                const float bd = (k < N - 1) ? (hz - gk) - fc : hz - fc;
-                const float iv = __fdividef(1.f, bd - fc * ccp);
-                ccp = gk * iv;
-                ddp = (rr - fc * ddp) * iv;
-                Rs += (double)rr;
-            }
-            cc[k * kPipeThreads] = ccp;
-            dd[k * kPipeThreads] = ddp;
-            fc = gk;
-            H += (double)hz;
-            O += (double)(ok * hz);
+#pragma unroll
+            for (int h = 0; h < kPipeGroup; ++h)
+                if (k0 + h < N) level(k0 + h);
         }
-        __syncthreads();                 // slot k % depth is free again
-        if (k + kPipeDepth < N) issue(k + kPipeDepth);
-        cp_async_commit();
+        __syncthreads();                 // the group's slots are free again
+#pragma unroll
+        for (int h = 0; h < kPipeGroup; ++h) {
+            if (k0 + kPipeDepth + h < N) issue(k0 + kPipeDepth + h);
+            cp_async_commit();
+        }
     }
     cp_async_wait<0>();
     if (both) {
