@@ -441,6 +441,9 @@ class Closure:
         if mode == "mlp" and net.N != model.grid.N:
             raise ValueError("the network was trained for N=%d levels" % net.N)
         self.m, self.mode, self.net, self.fused = model, mode, net, fused
+        # Model.step may run it beside the next step's first phases: it reads u, v, z_r, Hz,
+        # bvf and the surface stress, and writes AKv and its own turbulence fields only
+        self.overlappable = True
         self.cols = Columns(model)
         g = model.grid
         dev = model.u.device

@@ -221,40 +221,91 @@ class Model:
         self.set_depth()
         self._started = True
 
+    def _streams(self):
+        """(loop, side, mix): a high-priority stream for the barotropic loop and two
+        low-priority ones for rhs3d and the mixing, created once per model."""
+        if getattr(self, "_strm", None) is None:
+            lo, hi = torch.cuda.Stream.priority_range()
+            dev = self.u.device
+            self._strm = (torch.cuda.Stream(dev, priority=hi), torch.cuda.Stream(dev, priority=lo),
+                          torch.cuda.Stream(dev, priority=lo))
+        return self._strm
+
     def step(self, nsteps=1, final_omega=True, timer=None):
         """`nsteps` baroclinic steps (main3d.py:118-324).  The end-of-step omega
         (main3d.py:321) is recomputed at the start of every following step, so only the last
         one is evaluated unless `final_omega` is False (then none).  `timer(name)`, if given,
-        returns a pair of CUDA events recorded around each phase."""
+        returns a pair of CUDA events recorded around each phase (on the phase's stream).
+
+        With `overlap` (off by default) the phases that share no field run concurrently: rhs3d
+        (u, v, the fluxes, Hz -> ru, rv) beside the barotropic loop (2D state only), on their
+        own streams (the loop's at high priority), both after set_maxflux/omega/set_zeta; and a
+        mixing hook that declares `overlappable` (the package's closure: reads u, v, z_r, Hz,
+        its own fields; writes AKv and its own fields) beside the next step's first phases,
+        with set_depth (which rewrites z_r, Hz) and step3d (which reads AKv) waiting for it.
+        Results are identical either way; the call returns with all its work queued on the
+        current stream's order.  Measured on one B200 it does not pay: basin4 with the learned
+        closure 11.85 ms per step sequential, 11.95 with the mixing overlapped, 13.04 with
+        rhs3d beside the loop too (the closure's network holds a whole SM's shared memory and
+        rhs3d its issue slots; the loop's short kernels lose more than is hidden); `overlap_rhs3d`
+        = False keeps rhs3d in line."""
         if not self._started:
             self.start()
         c, p = self.ctx.ptr, self._p
-        st = stream_handle()
         cs = torch.cuda.current_stream()
+        st = ctypes.c_void_p(cs.cuda_stream)
+        ovl = getattr(self, "overlap", False)
+        ovl_rhs = ovl and getattr(self, "overlap_rhs3d", True)
+        if ovl:
+            s_loop, s_side, s_mix = self._streams()
+        h = lambda strm: ctypes.c_void_p(strm.cuda_stream)
+        mix_ovl = ovl and self.mixing is not None and getattr(self.mixing, "overlappable", False)
+        ev_mix = None
 
-        def phase(name, fn):
+        def phase(name, fn, strm=cs):
             if timer is None:
                 return fn()
             a, b = timer(name)
-            a.record(cs)
+            a.record(strm)
             r = fn()
-            b.record(cs)
+            b.record(strm)
             return r
+
+        def after(strm, *events):
+            for e in events:
+                if e is not None:
+                    strm.wait_event(e)
+
+        def mark(strm):
+            e = torch.cuda.Event()
+            e.record(strm)
+            return e
 
         for k in range(nsteps):
             z1, z2 = self._slot("zeta", 1), self._slot("zeta", 2)
             phase("k_maxflux_omega", lambda: check(lib.sf_maxflux_omega(
                 c, p(self.u), p(self.v), p(self.Huon), p(self.Hvom), p(self.Hz), p(self.W),
                 p(self.z_w), p(z1), p(z2), p(self.Zt_avg1), st), "sf_maxflux_omega"))
-            phase("k_rhs3d", lambda: check(lib.sf_rhs3d(
-                c, p(self.u), p(self.v), p(self.Huon), p(self.Hvom), p(self.W), p(self.Hz),
-                p(self.ru), p(self.rv), st), "sf_rhs3d"))
             s = self.state2d()
             t2 = ctypes.c_double(self.time2D)
-            phase("barotropic_loop", lambda: check(lib.sf_barotropic_loop(
+            rhs = lambda sh: check(lib.sf_rhs3d(
+                c, p(self.u), p(self.v), p(self.Huon), p(self.Hvom), p(self.W), p(self.Hz),
+                p(self.ru), p(self.rv), sh), "sf_rhs3d")
+            loop = lambda sh: check(lib.sf_barotropic_loop(
                 c, ctypes.byref(s), self.nfast + 1,
                 self._w1.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), self.dtfast,
-                ctypes.byref(t2), st), "sf_barotropic_loop"))
+                ctypes.byref(t2), sh), "sf_barotropic_loop")
+            if ovl_rhs:
+                e_flux = mark(cs)
+                after(s_side, e_flux)
+                phase("k_rhs3d", lambda: rhs(h(s_side)), s_side)
+                after(s_loop, e_flux)
+                phase("barotropic_loop", lambda: loop(h(s_loop)), s_loop)
+                after(cs, mark(s_side), mark(s_loop), ev_mix)
+            else:
+                phase("k_rhs3d", lambda: rhs(st))
+                phase("barotropic_loop", lambda: loop(st))
+                after(cs, ev_mix)
             self._sync_slots(s)
             self.time2D = t2.value
             phase("k_set_depth", lambda: self.set_depth(st))
@@ -264,10 +315,18 @@ class Model:
                 p(self.Hz), p(self.AKv), p(self.z_r), p(self.DU_avg1), p(self.DV_avg1), self.iic,
                 self.ntfirst, self.lam, self.dt, self.time, st), "sf_step3d_uv_bc"))
             if self.mixing is not None:
-                phase("closure", self.mixing)
+                if mix_ovl:
+                    after(s_mix, mark(cs))
+                    with torch.cuda.stream(s_mix):
+                        phase("closure", self.mixing, s_mix)
+                    ev_mix = mark(s_mix)
+                else:
+                    phase("closure", self.mixing)
             if final_omega and k == nsteps - 1:
                 phase("k_omega", lambda: check(lib.sf_omega(
                     c, p(self.W), p(self.Huon), p(self.Hvom), p(self.z_w), st), "sf_omega"))
             self.iic += 1                          # CompTimes.nextTimeStep
             self.time += self.dt
             self.time2D = self.time
+        if ev_mix is not None:   # the caller's stream sees the last mixing too
+            cs.wait_event(ev_mix)

@@ -101,3 +101,33 @@ def test_graph_replay_of_the_barotropic_loop_is_identical(ndtfast, precision):
                 scale = max(np.abs(out[0][k]).max(), 1e-30)
                 assert np.abs(o[k] - out[0][k]).max() <= 1e-5 * scale, k
         assert o["slots"] == out[0]["slots"]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision,mode", [("fp64", "gls"), ("fp32", "gls")])
+def test_overlapped_phases_give_the_same_step(precision, mode):
+    """Model.step with rhs3d beside the barotropic loop and the closure beside the next step's
+    first phases (the default) against the phases one after another: identical fields after
+    several steps, including the mixing's own."""
+    import numpy as np
+    import torch
+    from sailfish_b200 import closure, configs
+    from sailfish_b200.model import Model
+    cfg = configs.basin(40, 24, 8, 2.0e3, [(0.5, 0.5)], dt=120.0, ndtfast=10)
+    g = cfg["grid"]
+    bump = 1e-3 * np.exp(-((g.x - g.x.max() / 2) ** 2 + (g.y - g.y.max() / 2) ** 2) / (2e4) ** 2)
+    out = []
+    for overlap in (False, True):
+        m = Model(g, cfg["boundary"], cfg["dt"], cfg["ndtfast"], precision=precision)
+        m.overlap = overlap
+        m.Zt_avg1.copy_(torch.from_numpy(bump.ravel()))
+        m.mixing = closure.Closure(m, mode)
+        closure.wind_driven_state(m, m.mixing.cols, 0.1, 0.3, 500.0, np.random.default_rng(2))
+        m.step(3)
+        torch.cuda.synchronize()
+        st = m.state()
+        st["tke"] = m.mixing.cols.tke.cpu().numpy()
+        st["AKv"] = m.AKv.cpu().numpy()
+        out.append(st)
+    for k in ("zeta", "ubar", "vbar", "u", "v", "W", "Zt_avg1", "AKv", "tke"):
+        np.testing.assert_array_equal(out[1][k], out[0][k], err_msg=k)
