@@ -245,6 +245,15 @@ def step2d_corrector(grid, B, O, ct):       # nonlinear/step2d.py:84-128
     barotropic_velocity_bc(grid, B, O.t("ubar", 2), O.t("vbar", 2), ct.time2D)
 
 
+def main2d(grid, B, O, ct, nsteps):         # nonlinear/main2d.py:9-88
+    """Per 2D step: next2DTimeStep, cycleTimes2D, step2dPredictor, step2dCorrector."""
+    for _ in range(nsteps):
+        ct.next2d()
+        O.cycle2d()
+        step2d_predictor(grid, B, O, ct)
+        step2d_corrector(grid, B, O, ct)
+
+
 def rhs3d(grid, B, O):                      # nonlinear/rhs.py:16-93
     L = lib()
     BC = B["zetaBC_bcIdxFieldIdx2"]

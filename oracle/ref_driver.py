@@ -62,26 +62,44 @@ class RefKernels:
         getattr(self.libs[mod], "sfref_" + name)(_l(nthreads), _i(self.omp), *args)
 
 
-def main3d(grid, B, O, ct, nsteps, omp=1, lam=1.0):
-    """nonlinear/main3d.py:25-326 with the reference's kernels (step2d.py, zetabc.py,
-    barotropicVelocityBC.py, rhs.py orchestration restated), on oracle.Grid/Ocean/CompTimes."""
-    K = RefKernels(omp)
-    N, J, I = grid.N, grid.J, grid.I
-    s2 = grid.s2
-    nt = (s2 // 512 + 1) * 512          # grsz*bksz and grsz*GPUMUL*(bksz//GPUMUL)
-    bcn = lambda n: (n // 512 + 1) * 512
-    args_init = (ctypes.c_uint(N), ctypes.c_uint(J), ctypes.c_uint(I), P(grid.on_u), P(grid.om_v),
-                 P(grid.pn), P(grid.pm))
-    for mod in ("2d", "rhs", "step3d"):
-        K(mod, "initialize", 1, *args_init)
-    eq = [gzeros((N + 1, J, I)) for _ in range(3)]
-    tmpU, tmpV = gzeros((N + 1) * J * I), gzeros((N + 1) * J * I)
-    BC = B["zetaBC_bcIdxFieldIdx2"]
-    K("step3d", "setVerticalVelEq", 1, P(eq[0]), P(eq[1]), P(eq[2]))
+def _step2d_pair(K, grid, B, O, ct, nt, zetabc, velbc):
+    """step2dPredictor (step2d.py:23-81) and step2dCorrector (:84-128) with the reference's
+    kernels, on the current slot views of O; the predictor's leapfrog branch (iif >= 1)."""
+    def pred():
+        z0, z1, z2 = O.t("zeta", 0), O.t("zeta", 1), O.t("zeta", 2)
+        Dt = ct.dtfast
+        K("2d", "computeZetaRHS", nt, P(z1), P(grid.h), P(O.t("ubar", 1)), P(O.t("vbar", 1)),
+          P(O.DU_avg1), P(O.DV_avg1), P(O.Zt_avg1), _b(True), P(ct.weight1), P(ct.weight2),
+          Ii(ct.iif), P(O.t("rzeta", 1)))
+        K("2d", "computeZetaPred", nt, D(Dt), P(z0), P(z1), P(z2), P(O.t("rzeta", 1)))
+        zetabc(z2)
+        K("2d", "computeMomentumRHSPred", nt, P(grid.h), P(O.t("rubar", 1)), P(O.t("rvbar", 1)),
+          P(z0), P(z2), D(G_GRAV), D(2.0 / 5.0))
+        K("2d", "computeMomentumPred", nt, D(Dt), P(O.t("ubar", 1)), P(O.t("ubar", 2)),
+          P(O.t("vbar", 1)), P(O.t("vbar", 2)), P(O.t("rubar", 1)), P(O.t("rvbar", 1)),
+          P(grid.h), P(z1), P(z2))
+        velbc(O.t("ubar", 2), O.t("vbar", 2))
 
-    def set_depth():
-        K("step3d", "set_depth", nt, Ii(grid.Vtransform), P(O.Zt_avg1), P(grid.z_w), P(grid.z_r),
-          P(grid.h), D(grid.hc), P(grid.Hz), P(grid.sc_r), P(grid.sc_w), P(grid.Cs_r), P(grid.Cs_w))
+    def corr():
+        z0, z1, z2 = O.t("zeta", 0), O.t("zeta", 1), O.t("zeta", 2)
+        Dt = ct.dtfast
+        K("2d", "computeZetaRHS", nt, P(z2), P(grid.h), P(O.t("ubar", 2)), P(O.t("vbar", 2)),
+          P(O.DU_avg1), P(O.DV_avg1), P(O.Zt_avg1), _b(False), P(ct.weight1), P(ct.weight2),
+          Ii(ct.iif), P(O.t("rzeta", 1)))
+        K("2d", "AdamsMoultonCorr3rd", nt, D(Dt), P(z2), P(O.t("rzeta", 0)), P(O.t("rzeta", 1)),
+          P(O.t("rzeta", 2)))
+        zetabc(z2)
+        K("2d", "computeMomentumRHSCorr", nt, P(grid.h), P(O.t("rubar", 2)), P(O.t("rvbar", 2)),
+          P(z0), P(z1), P(z2), D(G_GRAV))
+        K("2d", "AdamsMoultonCorr3rd", nt, D(Dt), P(O.t("ubar", 1)), P(O.t("vbar", 1)),
+          P(O.t("rubar", 0)), P(O.t("rubar", 1)))
+        velbc(O.t("ubar", 2), O.t("vbar", 2))
+
+    return pred, corr
+
+
+def _bc_fns(K, B, ct):
+    bcn = lambda n: (n // 512 + 1) * 512
 
     def copy_bc(var, a1, a2, n):
         K("bc", "copyBC", bcn(n), P(var), P(a1), P(a2), ctypes.c_uint(n))
@@ -100,6 +118,48 @@ def main3d(grid, B, O, ct, nsteps, omp=1, lam=1.0):
         copy_bc(ub, B["ubarGradientBCIdx1"], B["ubarGradientBCIdx2"], B["ubarGradientBCIdx1"].size)
         copy_bc(vb, B["vbarGradientBCIdx1"], B["ubarGradientBCIdx2"], B["vbarGradientBCIdx1"].size)
 
+    return zetabc, velbc
+
+
+def main2d(grid, B, O, ct, nsteps, omp=1):
+    """nonlinear/main2d.py:9-88 with the reference's kernels: per 2D step next2DTimeStep,
+    cycleTimes2D, step2dPredictor, step2dCorrector (no accumulator reset, vbar_t2 kept)."""
+    K = RefKernels(omp)
+    nt = (grid.s2 // 512 + 1) * 512
+    args_init = (ctypes.c_uint(grid.N), ctypes.c_uint(grid.J), ctypes.c_uint(grid.I),
+                 P(grid.on_u), P(grid.om_v), P(grid.pn), P(grid.pm))
+    K("2d", "initialize", 1, *args_init)
+    zetabc, velbc = _bc_fns(K, B, ct)
+    pred, corr = _step2d_pair(K, grid, B, O, ct, nt, zetabc, velbc)
+    for _ in range(nsteps):
+        ct.next2d()
+        O.cycle2d()
+        pred()
+        corr()
+
+
+def main3d(grid, B, O, ct, nsteps, omp=1, lam=1.0):
+    """nonlinear/main3d.py:25-326 with the reference's kernels (step2d.py, zetabc.py,
+    barotropicVelocityBC.py, rhs.py orchestration restated), on oracle.Grid/Ocean/CompTimes."""
+    K = RefKernels(omp)
+    N, J, I = grid.N, grid.J, grid.I
+    s2 = grid.s2
+    nt = (s2 // 512 + 1) * 512          # grsz*bksz and grsz*GPUMUL*(bksz//GPUMUL)
+    args_init = (ctypes.c_uint(N), ctypes.c_uint(J), ctypes.c_uint(I), P(grid.on_u), P(grid.om_v),
+                 P(grid.pn), P(grid.pm))
+    for mod in ("2d", "rhs", "step3d"):
+        K(mod, "initialize", 1, *args_init)
+    eq = [gzeros((N + 1, J, I)) for _ in range(3)]
+    tmpU, tmpV = gzeros((N + 1) * J * I), gzeros((N + 1) * J * I)
+    BC = B["zetaBC_bcIdxFieldIdx2"]
+    K("step3d", "setVerticalVelEq", 1, P(eq[0]), P(eq[1]), P(eq[2]))
+
+    def set_depth():
+        K("step3d", "set_depth", nt, Ii(grid.Vtransform), P(O.Zt_avg1), P(grid.z_w), P(grid.z_r),
+          P(grid.h), D(grid.hc), P(grid.Hz), P(grid.sc_r), P(grid.sc_w), P(grid.Cs_r), P(grid.Cs_w))
+
+    zetabc, velbc = _bc_fns(K, B, ct)
+    pred, corr = _step2d_pair(K, grid, B, O, ct, nt, zetabc, velbc)
     set_depth()
     for _ in range(nsteps):
         K("step3d", "set_maxflux", nt, P(O.t3("u")), P(O.t3("v")), P(O.Huon), P(O.Hvom), P(grid.Hz))
@@ -121,32 +181,8 @@ def main3d(grid, B, O, ct, nsteps, omp=1, lam=1.0):
                 O.DV_avg1[:] = 0.0
             ct.next2d()
             O.cycle2d()
-            z0, z1, z2 = O.t("zeta", 0), O.t("zeta", 1), O.t("zeta", 2)
-            Dt = ct.dtfast
-            # step2dPredictor (step2d.py:23-81); iif >= 1 here, so always the leapfrog branch
-            K("2d", "computeZetaRHS", nt, P(z1), P(grid.h), P(O.t("ubar", 1)), P(O.t("vbar", 1)),
-              P(O.DU_avg1), P(O.DV_avg1), P(O.Zt_avg1), _b(True), P(ct.weight1), P(ct.weight2),
-              Ii(ct.iif), P(O.t("rzeta", 1)))
-            K("2d", "computeZetaPred", nt, D(Dt), P(z0), P(z1), P(z2), P(O.t("rzeta", 1)))
-            zetabc(z2)
-            K("2d", "computeMomentumRHSPred", nt, P(grid.h), P(O.t("rubar", 1)), P(O.t("rvbar", 1)),
-              P(z0), P(z2), D(G_GRAV), D(2.0 / 5.0))
-            K("2d", "computeMomentumPred", nt, D(Dt), P(O.t("ubar", 1)), P(O.t("ubar", 2)),
-              P(O.t("vbar", 1)), P(O.t("vbar", 2)), P(O.t("rubar", 1)), P(O.t("rvbar", 1)),
-              P(grid.h), P(z1), P(z2))
-            velbc(O.t("ubar", 2), O.t("vbar", 2))
-            # step2dCorrector (step2d.py:84-128)
-            K("2d", "computeZetaRHS", nt, P(z2), P(grid.h), P(O.t("ubar", 2)), P(O.t("vbar", 2)),
-              P(O.DU_avg1), P(O.DV_avg1), P(O.Zt_avg1), _b(False), P(ct.weight1), P(ct.weight2),
-              Ii(ct.iif), P(O.t("rzeta", 1)))
-            K("2d", "AdamsMoultonCorr3rd", nt, D(Dt), P(z2), P(O.t("rzeta", 0)), P(O.t("rzeta", 1)),
-              P(O.t("rzeta", 2)))
-            zetabc(z2)
-            K("2d", "computeMomentumRHSCorr", nt, P(grid.h), P(O.t("rubar", 2)), P(O.t("rvbar", 2)),
-              P(z0), P(z1), P(z2), D(G_GRAV))
-            K("2d", "AdamsMoultonCorr3rd", nt, D(Dt), P(O.t("ubar", 1)), P(O.t("vbar", 1)),
-              P(O.t("rubar", 0)), P(O.t("rubar", 1)))
-            velbc(O.t("ubar", 2), O.t("vbar", 2))
+            pred()
+            corr()
             O.t("vbar", 2)[:] = 0.0
         set_depth()
         tmpU[:] = O.t3("u")

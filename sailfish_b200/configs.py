@@ -3,7 +3,7 @@
 All inputs are analytic (no external data): depth from a tanh continental shelf across y plus
 Gaussian seamounts, beta-plane Coriolis, S-coordinates with Vtransform 2 / Vstretching 4.
 
-  basin0: 2D basin, Lm=128, Mm=64, dx=dy=5 km, flat h=4000 m, dt=30 s
+  basin0: config 0's 2D basin, Lm=128, Mm=64, dx=dy=5 km, flat h=4000 m, beta-plane f, dt=30 s
   basin1: Lm=512, Mm=256, N=32, dx=2 km, theta_s=5, theta_b=0.4, hc=100 m, one seamount,
           dt=240 s, ndtfast=30
   basin4: Lm=2048, Mm=1024, N=50, dx=1 km, same recipe with two seamounts, dt=120 s,
@@ -49,6 +49,13 @@ def basin(Lm, Mm, N, dx, seamounts, dt, ndtfast, f0=1e-4, beta=2e-11, theta_s=5.
     return dict(grid=grid, boundary=boundary, dt=float(dt), ndtfast=int(ndtfast))
 
 
+def basin0():
+    """Config 0's grid: a flat 4000 m closed rectangle, Lm=128, Mm=64, dx=dy=5 km, beta-plane f,
+    dt=30 s (one 2D step per call: ndtfast=1).  The 2D step uses no vertical levels; N=5 only
+    satisfies the context's minimum."""
+    return basin(128, 64, 5, 5.0e3, [], dt=30.0, ndtfast=1, hflat=4000.0)
+
+
 def basin1():
     return basin(512, 256, 32, 2.0e3, [(0.5, 0.6)], dt=240.0, ndtfast=30)
 
@@ -68,4 +75,4 @@ def small(Lm=256, Mm=128, N=32):
     return basin(Lm, Mm, N, 2.0e3, [(0.5, 0.6)], dt=240.0, ndtfast=30)
 
 
-CONFIGS = {"basin1": basin1, "basin4": basin4, "basin4q": basin4q, "small": small}
+CONFIGS = {"basin0": basin0, "basin1": basin1, "basin4": basin4, "basin4q": basin4q, "small": small}
