@@ -525,11 +525,17 @@ struct RhsTile {
     static constexpr int SX = TX + kHX0 + kHX1, SY = TY + kHY0 + kHY1, SN = SX * SY;
     static constexpr int FX = TX + 1, FN = (TX + 1) * (TY + 1);   // face-flux tile
 };
-// Dynamic shared memory of the tiled right-hand side: two staging buffers of 6 fields and the
-// four face-flux arrays.
+// Dynamic shared memory of the tiled right-hand side: rhs_bufs<R>() staging buffers of 6
+// fields and the four face-flux arrays.  FP32 keeps three buffers: level K+2 is issued after
+// the first barrier of level K, when every thread has finished level K-1 (its reads of the
+// buffer being refilled and of the face fluxes), so a level needs two barriers.  FP64, whose
+// buffers are twice the size, keeps two (three blocks per SM) and a third barrier per level.
+template <typename R>
+__host__ __device__ constexpr int rhs_bufs() { return sizeof(R) == 4 ? 3 : 2; }
 template <typename R, int TX, int TY>
 constexpr size_t rhs_smem_bytes() {
-    return sizeof(R) * ((size_t)2 * 6 * RhsTile<TX, TY>::SN + 4 * (size_t)RhsTile<TX, TY>::FN);
+    return sizeof(R) * ((size_t)rhs_bufs<R>() * 6 * RhsTile<TX, TY>::SN +
+                        4 * (size_t)RhsTile<TX, TY>::FN);
 }
 
 template <typename R, int SX>
@@ -596,7 +602,8 @@ __device__ __forceinline__ void rhs3d_body(const Geo<R> &g, const R *__restrict_
     constexpr int kSX = T::SX, kSN = T::SN, kFX = T::FX, kFN = T::FN;
     extern __shared__ __align__(16) unsigned char rhs_smem[];
     R(*sbuf)[6][kSN] = reinterpret_cast<R(*)[6][kSN]>(rhs_smem);
-    R *sF = reinterpret_cast<R *>(rhs_smem) + 2 * 6 * kSN;   // [4][kFN] face fluxes
+    constexpr int kBufs = rhs_bufs<R>();
+    R *sF = reinterpret_cast<R *>(rhs_smem) + kBufs * 6 * kSN;   // [4][kFN] face fluxes
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
     const long I = g.I, s2 = g.s2;
     const int N = g.N;
@@ -638,7 +645,7 @@ __device__ __forceinline__ void rhs3d_body(const Geo<R> &g, const R *__restrict_
     const StageMap<TX, TY> smap(I, j0, i0, tid);
     auto issue = [&](int K) {
         const long o = (long)K * s2;
-        R(*bf)[kSN] = sbuf[K & 1];
+        R(*bf)[kSN] = sbuf[K % kBufs];
         stage<R, TX, TY>(bf[0], u, o, len3, smap, tid);
         stage<R, TX, TY>(bf[1], v, o, len3, smap, tid);
         stage<R, TX, TY>(bf[2], Huon, o, len3, smap, tid);
@@ -648,16 +655,27 @@ __device__ __forceinline__ void rhs3d_body(const Geo<R> &g, const R *__restrict_
         cp_async_commit();
     };
     issue(0);
+    if constexpr (kBufs == 3) {
+        if (N > 1) issue(1);
+        else cp_async_commit();
+    }
     for (int K = 0; K < N; ++K) {
         const long o = (long)K * s2;
-        if (K + 1 < N) {
-            issue(K + 1);
-            cp_async_wait<1>();
+        if constexpr (kBufs == 3) {
+            cp_async_wait<1>();   // level K's group (level K+1's may still be in flight)
+            __syncthreads();      // ... and every thread is done with level K-1
+            if (K + 2 < N) issue(K + 2);
+            else cp_async_commit();
         } else {
-            cp_async_wait<0>();
+            if (K + 1 < N) {
+                issue(K + 1);
+                cp_async_wait<1>();
+            } else {
+                cp_async_wait<0>();
+            }
+            __syncthreads();
         }
-        __syncthreads();
-        R(*bf)[kSN] = sbuf[K & 1];
+        R(*bf)[kSN] = sbuf[K % kBufs];
         const Tile<R, kSX> U{bf[0], b}, V{bf[1], b}, HU{bf[2], b}, HV{bf[3], b}, HZ{bf[4], b}, WW{bf[5], b};
         // Every thread reaches both barriers of each level: the compute is predicated on
         // `live` rather than skipped with `continue` (an aligned barrier must not diverge).
@@ -768,7 +786,7 @@ __device__ __forceinline__ void rhs3d_body(const Geo<R> &g, const R *__restrict_
         ru[o + p] = aru;
         rv[o + p] = (va && K == 0) ? R(0) : arv;   // rv[0] is set from rv[1] below
         }
-        __syncthreads();   // the buffer of level K is refilled for level K+2 next iteration
+        if constexpr (kBufs == 2) __syncthreads();   // the buffer of level K is refilled next
     }
     if (!live) return;
     const long oN = (long)N * s2;
