@@ -1183,7 +1183,8 @@ __device__ __forceinline__ void step3d_uv_pipe_body(const Geo<R> &g, float *__re
     const bool both = un && vn;
     const long d = sys == 0 ? 1 : I;   // the neighbour of this system's face
 
-    for (int k = 0; k < kPipeDepth; ++k) {
+    constexpr int kAhead = kPipeDepth - kPipeGroup;   // levels issued before the first group
+    for (int k = 0; k < kAhead; ++k) {
         if (k < N) issue(k);
         cp_async_commit();
     }
@@ -1197,9 +1198,9 @@ __device__ __forceinline__ void step3d_uv_pipe_body(const Geo<R> &g, float *__re
     float fc = 0.f, fc0 = 0.f, ccp = 0.f, ddp = 0.f;
     double H = 0.0, O = 0.0, Rs = 0.0;
     const int qi = sys == 0 ? col : kPipeCols + 1 + col;   // this system's neighbour in a row
-    // levels in groups of kPipeGroup: one wait and two barriers per group (kPipeDepth is a
-    // multiple of it, so a group's slots are free together and refilled with the group
-    // kPipeDepth levels up)
+    // levels in groups of kPipeGroup: one wait and one barrier per group.  After the barrier of
+    // group g every thread has finished group g-1, whose slots (kPipeDepth is a multiple of the
+    // group) are refilled with group g+2, so two groups are in flight while one is eliminated
     static_assert(kPipeDepth % kPipeGroup == 0, "levels are consumed in whole groups");
     auto level = [&](int k) {
         const float *sl = ring + (k % kPipeDepth) * kPipeSlot;
@@ -1234,18 +1235,17 @@ __device__ __forceinline__ void step3d_uv_pipe_body(const Geo<R> &g, float *__re
         O += (double)(ok * hz);
     };
     for (int k0 = 0; k0 < N; k0 += kPipeGroup) {
-        cp_async_wait<kPipeDepth - kPipeGroup>();
+        cp_async_wait<kAhead - kPipeGroup>();   // this group's levels (the next may be in flight)
         __syncthreads();
+#pragma unroll
+        for (int h = 0; h < kPipeGroup; ++h) {
+            if (k0 + kAhead + h < N) issue(k0 + kAhead + h);
+            cp_async_commit();
+        }
         if (both) {
 #pragma unroll
             for (int h = 0; h < kPipeGroup; ++h)
                 if (k0 + h < N) level(k0 + h);
-        }
-        __syncthreads();                 // the group's slots are free again
-#pragma unroll
-        for (int h = 0; h < kPipeGroup; ++h) {
-            if (k0 + kPipeDepth + h < N) issue(k0 + kPipeDepth + h);
-            cp_async_commit();
         }
     }
     cp_async_wait<0>();
