@@ -103,10 +103,38 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v) {
           "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]),
           "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]),
           "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::);
+        : "r"(taddr)
+        : "memory");
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
     for (int k = 0; k < 32; ++k) v[k] = __uint_as_float(r[k]);
+}
+// Row lane, 32 consecutive FP32 columns from registers (32x32b.x32), and the wait for them.
+__device__ __forceinline__ void tmem_st32(uint32_t taddr, const float *v) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+        "%12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, "
+        "%30, %31, %32};" ::"r"(taddr),
+        "f"(v[0]), "f"(v[1]), "f"(v[2]), "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7]),
+        "f"(v[8]), "f"(v[9]), "f"(v[10]), "f"(v[11]), "f"(v[12]), "f"(v[13]), "f"(v[14]), "f"(v[15]),
+        "f"(v[16]), "f"(v[17]), "f"(v[18]), "f"(v[19]), "f"(v[20]), "f"(v[21]), "f"(v[22]), "f"(v[23]),
+        "f"(v[24]), "f"(v[25]), "f"(v[26]), "f"(v[27]), "f"(v[28]), "f"(v[29]), "f"(v[30]), "f"(v[31])
+        : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+// The accumulator columns n0..n0+31 of this thread's row set to the bias: the products then add
+// onto it (the layer's pre-activation is bias + sum, accumulated by the tensor cores).
+__device__ __forceinline__ void tmem_bias32(uint32_t taddr, const float *bias32) {
+    float v[32];
+#pragma unroll
+    for (int k = 0; k < 32; k += 4) {
+        const float4 q = *reinterpret_cast<const float4 *>(bias32 + k);
+        v[k] = q.x;
+        v[k + 1] = q.y;
+        v[k + 2] = q.z;
+        v[k + 3] = q.w;
+    }
+    tmem_st32(taddr, v);
 }
 
 // Element (r, k) of a 128 x 128 BF16 tile in the core-matrix layout: 16 core matrices of
@@ -306,25 +334,28 @@ __device__ __forceinline__ float act_fast(float x) {
     else return gelu_fast(x);
 }
 
-// act(v + bias) of 32 consecutive outputs of row r, as the next layer's BF16 operand: four
-// 16-byte stores, one per core-matrix row segment.
+// BF16 pair {act(lo), act(hi)} (lo in the low half); for ReLU one conversion with clamping.
 template <int ACT>
-__device__ __forceinline__ void store_act8x4(__nv_bfloat16 *sA, int r, int n0, const float *v,
-                                             const float *bias) {
+__device__ __forceinline__ uint32_t pack_act2(float lo, float hi) {
+    if constexpr (ACT == kActRelu) {
+        uint32_t d;
+        asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(hi), "f"(lo));
+        return d;
+    } else {
+        const __nv_bfloat162 b2 = __floats2bfloat162_rn(act_fast<ACT>(lo), act_fast<ACT>(hi));
+        return *reinterpret_cast<const uint32_t *>(&b2);
+    }
+}
+
+// act(v) of 32 consecutive pre-activations of row r (the bias is already in them), as the next
+// layer's BF16 operand: four 16-byte stores, one per core-matrix row segment.
+template <int ACT>
+__device__ __forceinline__ void store_act8x4(__nv_bfloat16 *sA, int r, int n0, const float *v) {
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-        // the 8 biases of this segment as two 16-byte loads (bias is 16-byte aligned, n0 % 32 == 0)
-        const float4 ba = reinterpret_cast<const float4 *>(bias + n0 + 8 * q)[0];
-        const float4 bb = reinterpret_cast<const float4 *>(bias + n0 + 8 * q)[1];
-        const float bv[8] = {ba.x, ba.y, ba.z, ba.w, bb.x, bb.y, bb.z, bb.w};
         uint32_t pk[4];
 #pragma unroll
-        for (int h = 0; h < 4; ++h) {
-            const int k = 8 * q + 2 * h;
-            const __nv_bfloat162 b2 = __floats2bfloat162_rn(act_fast<ACT>(v[k] + bv[2 * h]),
-                                                            act_fast<ACT>(v[k + 1] + bv[2 * h + 1]));
-            pk[h] = *reinterpret_cast<const uint32_t *>(&b2);
-        }
+        for (int h = 0; h < 4; ++h) pk[h] = pack_act2<ACT>(v[8 * q + 2 * h], v[8 * q + 2 * h + 1]);
         *reinterpret_cast<uint4 *>(&sA[cm_index(r, n0 + 8 * q)]) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
     }
 }
@@ -383,14 +414,17 @@ __global__ void __launch_bounds__(kInferThreads, 1) k_infer(InferW w, long n,
             }
         }
         for (int l = 0; l < SF_MLP_LAYERS; ++l) {
+            // the layer's bias into the accumulator (this thread's row and 64 columns)
+            for (int c = 0; c < 2; ++c) tmem_bias32(tmem + trow + cb + c * 32, sbias[l] + cb + c * 32);
+            tmem_wait_st();
+            fence_before();
             fence_proxy_async();
             __syncthreads();
             if (tid == 0) {
                 fence_after();
                 const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sW + l * kTile * kTile);
                 for (int s = 0; s < kTile / 16; ++s)
-                    mma_bf16(tmem, sdesc(a0 + s * 256, kLBO, kSBO), sdesc(b0 + s * 256, kLBO, kSBO),
-                             s > 0 ? 1u : 0u);
+                    mma_bf16(tmem, sdesc(a0 + s * 256, kLBO, kSBO), sdesc(b0 + s * 256, kLBO, kSBO), 1u);
                 mma_commit(&mbar);
             }
             const bool done = mbar_wait(&mbar, phase);
@@ -407,15 +441,11 @@ __global__ void __launch_bounds__(kInferThreads, 1) k_infer(InferW w, long n,
                 tmem_ld32(tmem + trow + cb + c * 32, v);
                 const int n0 = cb + c * 32;
                 if (!last) {
-                    store_act8x4<ACT>(sA, rl, n0, v, sbias[l]);
+                    store_act8x4<ACT>(sA, rl, n0, v);
                 } else if (r < n) {
                     float4 *y = reinterpret_cast<float4 *>(Y + r * kTile + n0);
 #pragma unroll
-                    for (int k = 0; k < 8; ++k)
-                        y[k] = make_float4(v[4 * k] + sbias[l][n0 + 4 * k],
-                                           v[4 * k + 1] + sbias[l][n0 + 4 * k + 1],
-                                           v[4 * k + 2] + sbias[l][n0 + 4 * k + 2],
-                                           v[4 * k + 3] + sbias[l][n0 + 4 * k + 3]);
+                    for (int k = 0; k < 8; ++k) y[k] = make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
                 }
             }
             fence_before();
@@ -643,11 +673,11 @@ __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t b
         : "memory");
 }
 
-// 16 warps: warp w reads TMEM lanes 32(w%4).. (its rows) and columns 32(w/4).. (its outputs),
-// so each thread takes 32 outputs of a row per layer and four warps share each scheduler.
-// Two tiles are in flight: tile A's epilogue of layer l runs while the tensor cores compute
-// tile B's layer l and the other way round (two operand buffers, two TMEM accumulators of 128
-// columns), so the products hide behind the epilogues.
+// Two groups of 8 warps run their own tiles independently: group b takes this CTA's tiles
+// 2i + b, with its own operand buffer, TMEM accumulator (columns 128b..) and mbarriers, and
+// synchronises only its own 256 threads (named barrier 1 + b), so one group's epilogue runs
+// while the other group's products are on the tensor cores.  Warp w of a group reads TMEM
+// lanes 32(w%4).. (its rows) and columns 64((w/4)%2).. (64 outputs of a row per layer).
 constexpr int kClosureThreads = 512;
 constexpr size_t kClosureSmem = (size_t)(2 + SF_MLP_LAYERS) * kTile * kTile * 2;
 constexpr uint32_t kTmemCols2 = 256;
@@ -661,6 +691,17 @@ __device__ __forceinline__ void tmem_alloc256(uint32_t *dst_smem) {
 __device__ __forceinline__ void tmem_dealloc256(uint32_t taddr) {
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(kTmemCols2));
 }
+// Barrier over the 256 threads of named barrier `id`, returning whether any of them passed true.
+__device__ __forceinline__ bool group_any(int id, bool v) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\t"
+        "barrier.red.or.pred q, %2, 256, p;\n\tselp.u32 %0, 1, 0, q;\n\t}\n"
+        : "=r"(r)
+        : "r"((uint32_t)v), "r"(id)
+        : "memory");
+    return r != 0;
+}
 
 template <typename R, int ACT>
 __global__ void __launch_bounds__(kClosureThreads, 1) k_closure_mlp(Geo<R> g, InferW w,
@@ -668,17 +709,14 @@ __global__ void __launch_bounds__(kClosureThreads, 1) k_closure_mlp(Geo<R> g, In
         R *__restrict__ Akv, R *__restrict__ Akt, int *err) {
     extern __shared__ __align__(1024) unsigned char dsm[];
     __nv_bfloat16 *const sA0 = reinterpret_cast<__nv_bfloat16 *>(dsm);
-    __nv_bfloat16 *const sA1 = sA0 + kTile * kTile;
-    __nv_bfloat16 *const sW = sA1 + kTile * kTile;
+    __nv_bfloat16 *const sW = sA0 + 2 * kTile * kTile;
     __shared__ __align__(8) uint64_t mbar[2], xbar[2];
     __shared__ uint32_t tmem_base;
     __shared__ __align__(16) float sbias[SF_MLP_LAYERS][kTile];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int nl = g.N - 1;
     const long s2 = g.s2, G = gridDim.x;
-    // this CTA's tiles are blockIdx.x + G*q; pair pq holds q = 2pq (slot 0) and 2pq + 1 (slot 1)
-    auto tile_of = [&](long q) { return (long)blockIdx.x + G * q; };
-    auto buf = [&](int b) { return b ? sA1 : sA0; };
+    auto tile_of = [&](long q) { return (long)blockIdx.x + G * q; };   // this CTA's q-th tile
     if (warp == 0) tmem_alloc256(&tmem_base);
     if (tid == 0) {
         for (int b = 0; b < 2; ++b) {
@@ -687,9 +725,10 @@ __global__ void __launch_bounds__(kClosureThreads, 1) k_closure_mlp(Geo<R> g, In
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::);
         fence_proxy_async();
-        for (int b = 0; b < 2; ++b)   // the first pair's operands, while the weights load
+        for (int b = 0; b < 2; ++b)   // each group's first operand, while the weights load
             if (tile_of(b) < ntiles)
-                bulk_load(buf(b), Xt + tile_of(b) * kTile * kTile, kTile * kTile * 2, &xbar[b]);
+                bulk_load(sA0 + b * kTile * kTile, Xt + tile_of(b) * kTile * kTile, kTile * kTile * 2,
+                          &xbar[b]);
     }
     for (int l = 0; l < SF_MLP_LAYERS; ++l) {
         for (int e = tid; e < kTile * kTile; e += kClosureThreads)
@@ -699,105 +738,103 @@ __global__ void __launch_bounds__(kClosureThreads, 1) k_closure_mlp(Geo<R> g, In
     fence_before();
     __syncthreads();
     fence_after();
-    const uint32_t tmem = tmem_base;
+    const int grp = warp >> 3, bar_id = 1 + grp;
+    const bool issuer = (warp & 7) == 0 && lane == 0;
+    __nv_bfloat16 *const sA = sA0 + grp * kTile * kTile;
+    const uint32_t acc = tmem_base + (uint32_t)(grp * kTile);
     const int rl = (warp & 3) * 32 + lane;
-    const int n0 = (warp >> 2) * 32;
-    const uint32_t trow = (uint32_t)((warp & 3) * 32) << 16;
-    uint32_t ph[2] = {0, 0}, xph[2] = {0, 0};
-    bool ok = true;
-    auto issue_mma = [&](int b, int l) {   // thread 0: slot b's layer l into accumulator b
-        fence_after();
-        const uint32_t a0 = smem_u32(buf(b)), b0 = smem_u32(sW + l * kTile * kTile);
+    const int n0 = ((warp >> 2) & 1) * 64;
+    const uint32_t tacc = acc + ((uint32_t)((warp & 3) * 32) << 16) + n0;
+    uint32_t ph = 0, xph = 0;
+    bool bad = false;    // this thread gave up a wait
+    bool stop = false;   // the group gave up (uniform over the group: set from a vote)
+    // the first layer's bias into this thread's accumulator columns; each epilogue then loads
+    // the next layer's (or, after the last layer, the next tile's first layer's) bias into the
+    // columns it has just read, and the products add onto it
+    for (int c = 0; c < 2; ++c) tmem_bias32(tacc + c * 32, sbias[0] + n0 + c * 32);
+    tmem_wait_st();
+    fence_before();
+    auto issue_mma = [&](int l) {   // the group's elected thread: layer l into its accumulator
+        const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sW + l * kTile * kTile);
         for (int q = 0; q < kTile / 16; ++q)
-            mma_bf16(tmem + (uint32_t)(b * kTile), sdesc(a0 + q * 256, kLBO, kSBO),
-                     sdesc(b0 + q * 256, kLBO, kSBO), q > 0 ? 1u : 0u);
-        mma_commit(&mbar[b]);
+            mma_bf16(acc, sdesc(a0 + q * 256, kLBO, kSBO), sdesc(b0 + q * 256, kLBO, kSBO), 1u);
+        mma_commit(&mbar[grp]);
     };
-    for (long pq = 0; tile_of(2 * pq) < ntiles && ok; ++pq) {
-        const long t0 = tile_of(2 * pq), t1 = tile_of(2 * pq + 1);
-        const bool has1 = t1 < ntiles;
-        {   // operands landed (bounded waits)
-            bool got = mbar_wait(&xbar[0], xph[0]);
-            xph[0] ^= 1;
-            if (has1) {
-                got = mbar_wait(&xbar[1], xph[1]) && got;
-                xph[1] ^= 1;
-            }
-            if (__syncthreads_or(!got)) {
-                ok = false;
-                break;
-            }
+    for (long i = 0;; ++i) {
+        const long t = tile_of(2 * i + grp);
+        if (t >= ntiles) break;
+        bad = !mbar_wait(&xbar[grp], xph) || bad;   // this tile's operand landed
+        xph ^= 1;
+        // every thread's TMEM reads of the previous tile are done before this tile's products
+        if (group_any(bar_id, bad)) {
+            stop = true;
+            break;
         }
-        fence_proxy_async();
-        __syncthreads();
-        if (tid == 0) {
-            issue_mma(0, 0);
-            if (has1) issue_mma(1, 0);
+        fence_after();
+        if (issuer) issue_mma(0);
+        const int p = (int)(t * kTile) + rl;   // the flat column of this thread's row
+        bool apply = false;
+        if (p < s2) {
+            const int j = fdiv(p, g.dI);
+            apply = column_(p - j * g.I, j, g.I, g.J) && !fallback[p];
         }
-        long pr[2];
-        bool apply[2];
-        for (int b = 0; b < 2; ++b) {
-            const long p = (b ? t1 : t0) * kTile + rl;
-            pr[b] = p;
-            apply[b] = (b == 0 || has1) && p < s2 &&
-                       column_((int)(p % g.I), (int)(p / g.I), g.I, g.J) && !fallback[p];
-        }
-        for (int l = 0; l < SF_MLP_LAYERS && ok; ++l) {
+        for (int l = 0; l < SF_MLP_LAYERS; ++l) {
             const bool last = l == SF_MLP_LAYERS - 1;
-            for (int b = 0; b < 2; ++b) {
-                if (b == 1 && !has1) continue;
-                const bool done = mbar_wait(&mbar[b], ph[b]);
-                ph[b] ^= 1;
-                fence_after();
-                if (__syncthreads_or(!done)) {
-                    ok = false;
+            bad = !mbar_wait(&mbar[grp], ph) || bad;
+            ph ^= 1;
+            fence_after();
+            if (last && issuer && !bad) {   // the products have read the operand: refill it
+                const long nt = tile_of(2 * (i + 1) + grp);
+                if (nt < ntiles) bulk_load(sA, Xt + nt * kTile * kTile, kTile * kTile * 2, &xbar[grp]);
+            }
+            if (!last) {
+#pragma unroll
+                for (int c = 0; c < 2; ++c) {
+                    float vv[32];
+                    tmem_ld32(tacc + c * 32, vv);
+                    store_act8x4<ACT>(sA, rl, n0 + c * 32, vv);
+                    tmem_bias32(tacc + c * 32, sbias[l + 1] + n0 + c * 32);
+                }
+                tmem_wait_st();
+                fence_before();
+                fence_proxy_async();
+                if (group_any(bar_id, bad)) {
+                    stop = true;
                     break;
                 }
-                if (last && tid == 0) {   // the products have read this operand: refill it
-                    const long nt = tile_of(2 * (pq + 1) + b);
-                    if (nt < ntiles) bulk_load(buf(b), Xt + nt * kTile * kTile, kTile * kTile * 2, &xbar[b]);
-                }
-                float vv[32];
-                tmem_ld32(tmem + (uint32_t)(b * kTile) + trow + n0, vv);
-                if (!last) {
-                    store_act8x4<ACT>(buf(b), rl, n0, vv, sbias[l]);
-                    fence_before();
-                    fence_proxy_async();
-                    __syncthreads();
-                    if (tid == 0) issue_mma(b, l + 1);   // overlaps the other slot's epilogue
-                } else if (apply[b]) {
-                    // outputs n0.. of this column: Akv at levels n+1 for n < nl, then Akt at
-                    // levels n-nl+1 for n < 2nl; the destination advances one level (s2) a step
-                    const long p = pr[b];
-                    R *dst = n0 < nl ? Akv + (long)(n0 + 1) * s2 + p
-                                     : Akt + (long)(n0 - nl + 1) * s2 + p;
+                fence_after();
+                if (issuer) issue_mma(l + 1);   // overlaps the other group's epilogue
+            } else {
+                // outputs n of this column: Akv at level n+1 for n < nl, then Akt at level
+                // n-nl+1 for n < 2nl; the destination advances one level (s2) a step.  The TMEM
+                // reads are warp-wide (every lane), the stores only for the columns updated.
+                R *dst = n0 < nl ? Akv + (long)(n0 + 1) * s2 + p : Akt + (long)(n0 - nl + 1) * s2 + p;
 #pragma unroll
-                    for (int k = 0; k < 32; k += 4) {
-                        const float4 bq = *reinterpret_cast<const float4 *>(&sbias[l][n0 + k]);
-                        const float bv[4] = {bq.x, bq.y, bq.z, bq.w};
+                for (int c = 0; c < 2; ++c) {
+                    float vv[32];
+                    tmem_ld32(tacc + c * 32, vv);
+                    tmem_bias32(tacc + c * 32, sbias[0] + n0 + c * 32);
+                    if (apply) {
 #pragma unroll
-                        for (int h = 0; h < 4; ++h) {
-                            const int n = n0 + k + h;
+                        for (int k = 0; k < 32; ++k) {
+                            const int n = n0 + c * 32 + k;
                             if (n == nl) dst = Akt + s2 + p;
-                            if (n < 2 * nl)
-                                *dst = (R)fexp10(fminf(fmaxf(vv[k + h] + bv[h], -6.f), -1.f));
+                            if (n < 2 * nl) __stcs(dst, (R)fexp10(fminf(fmaxf(vv[k], -6.f), -1.f)));
                             dst += s2;
                         }
                     }
-                    fence_before();
-                } else {
-                    fence_before();
                 }
+                tmem_wait_st();
+                fence_before();
             }
         }
+        if (stop) break;   // a last-layer wait that gave up is voted on at the next tile
     }
-    if (!ok && tid == 0) {
-        atomicExch(err, 1);
-        for (int b = 0; b < 2; ++b) (void)mbar_wait(&xbar[b], xph[b]);   // bounded
-    }
+    if (bad) atomicExch(err, 1);
+    if (stop && issuer) (void)mbar_wait(&xbar[grp], xph);   // a refill in flight (bounded)
     fence_before();
     __syncthreads();
-    if (warp == 0) tmem_dealloc256(tmem);
+    if (warp == 0) tmem_dealloc256(tmem_base);
 }
 
 }  // namespace mlp
