@@ -592,7 +592,66 @@ __device__ __forceinline__ void stage(R *dst, const R *src, long lvl_off, long l
     }
 }
 
+// Pair staging: when the row length I is even and every field starts on a 2-element boundary,
+// the staged tile (SX even, first column i0 - 2 even) is a set of aligned element pairs, copied
+// 8 (FP32) or 16 (FP64) bytes at a time: half the copies of element staging.  A level whose
+// whole tile lies inside every field (all but the first and the last few rows of the array) is
+// staged without per-copy bounds checks.  Offsets fit 32 bits (the host requires s2 < 2^30).
+__device__ __forceinline__ void cp_async2(float *dst, const float *src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src));
+}
+__device__ __forceinline__ void cp_async2(double *dst, const double *src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src));
+}
+__device__ __forceinline__ void cp_async2(float *dst, const float *src, bool ok) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(ok ? 8 : 0));
+}
+__device__ __forceinline__ void cp_async2(double *dst, const double *src, bool ok) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(ok ? 16 : 0));
+}
+template <int TX, int TY>
+struct PairMap {
+    using T = RhsTile<TX, TY>;
+    static_assert(T::SX % 2 == 0 && kHX0 % 2 == 0, "pair staging needs even tile rows");
+    static constexpr int kPairs = T::SN / 2;
+    static constexpr int kPer = (kPairs + TX * TY - 1) / (TX * TY);
+    int rel[kPer];   // flat offset (within a level) of each pair's first element
+    int rmin, rmax;  // first and last flat offset of the staged tile
+    __device__ __forceinline__ PairMap(int I, int j0, int i0, int tid) {
+#pragma unroll
+        for (int q = 0; q < kPer; ++q) {
+            const int e = 2 * (tid + q * TX * TY);
+            const int r = e / T::SX - kHY0, c = e % T::SX - kHX0;
+            rel[q] = (j0 + r) * I + (i0 + c);
+        }
+        rmin = (j0 - kHY0) * I + (i0 - kHX0);
+        rmax = (j0 + TY - 1 + kHY1) * I + (i0 + TX - 1 + kHX1);
+    }
+};
 template <typename R, int TX, int TY>
+__device__ __forceinline__ void stage2(R *dst, const R *src, long lvl_off, long len, bool safe,
+                                       const PairMap<TX, TY> &pm, int tid) {
+    using M = PairMap<TX, TY>;
+#pragma unroll
+    for (int q = 0; q < M::kPer; ++q) {
+        const int e = tid + q * TX * TY;
+        if (M::kPairs % (TX * TY) == 0 || e < M::kPairs) {
+            if (safe) {
+                cp_async2(dst + 2 * e, src + lvl_off + pm.rel[q]);
+            } else {
+                const long f = lvl_off + pm.rel[q];
+                const bool ok = f >= 0 && f < len;   // len and f even: the pair is wholly in or out
+                cp_async2(dst + 2 * e, ok ? src + f : src, ok);
+            }
+        }
+    }
+}
+
+template <typename R, int TX, int TY, bool P2>
 __device__ __forceinline__ void rhs3d_body(const Geo<R> &g, const R *__restrict__ u,
                                            const R *__restrict__ v, const R *__restrict__ Huon,
                                            const R *__restrict__ Hvom, const R *__restrict__ W,
@@ -642,16 +701,28 @@ __device__ __forceinline__ void rhs3d_body(const Geo<R> &g, const R *__restrict_
     const R fw = (live && p >= 1) ? g.fomn[p - 1] : R(0);
     const R fs = (live && p >= I) ? g.fomn[p - I] : R(0);
 
-    const StageMap<TX, TY> smap(I, j0, i0, tid);
+    // the staging offsets of this thread, once per block
+    const std::conditional_t<P2, PairMap<TX, TY>, StageMap<TX, TY>> pm(g.I, (int)j0, (int)i0, tid);
     auto issue = [&](int K) {
         const long o = (long)K * s2;
         R(*bf)[kSN] = sbuf[K % kBufs];
-        stage<R, TX, TY>(bf[0], u, o, len3, smap, tid);
-        stage<R, TX, TY>(bf[1], v, o, len3, smap, tid);
-        stage<R, TX, TY>(bf[2], Huon, o, len3, smap, tid);
-        stage<R, TX, TY>(bf[3], Hvom, o, len3, smap, tid);
-        stage<R, TX, TY>(bf[4], Hz, o, lenHz, smap, tid);
-        stage<R, TX, TY>(bf[5], W, o + s2, len3, smap, tid);
+        if constexpr (P2) {
+            // W is staged from level K+1 and Hz has N levels: o + rmax < N s2 covers all six
+            const bool safe = o + pm.rmin >= 0 && o + pm.rmax < lenHz;
+            stage2<R, TX, TY>(bf[0], u, o, len3, safe, pm, tid);
+            stage2<R, TX, TY>(bf[1], v, o, len3, safe, pm, tid);
+            stage2<R, TX, TY>(bf[2], Huon, o, len3, safe, pm, tid);
+            stage2<R, TX, TY>(bf[3], Hvom, o, len3, safe, pm, tid);
+            stage2<R, TX, TY>(bf[4], Hz, o, lenHz, safe, pm, tid);
+            stage2<R, TX, TY>(bf[5], W, o + s2, len3, safe, pm, tid);
+        } else {
+            stage<R, TX, TY>(bf[0], u, o, len3, pm, tid);
+            stage<R, TX, TY>(bf[1], v, o, len3, pm, tid);
+            stage<R, TX, TY>(bf[2], Huon, o, len3, pm, tid);
+            stage<R, TX, TY>(bf[3], Hvom, o, len3, pm, tid);
+            stage<R, TX, TY>(bf[4], Hz, o, lenHz, pm, tid);
+            stage<R, TX, TY>(bf[5], W, o + s2, len3, pm, tid);
+        }
         cp_async_commit();
     };
     issue(0);
@@ -717,11 +788,17 @@ __device__ __forceinline__ void rhs3d_body(const Geo<R> &g, const R *__restrict_
             if (r < 0 && c < 0) continue;            // the corner cell is nobody's neighbour
             const int bb = (r + kHY0) * kSX + (c + kHX0);
             const Tile<R, kSX> U{bf[0], bb}, V{bf[1], bb}, HU{bf[2], bb}, HV{bf[3], bb};
+            // all four first, then the stores (a store between them would force the staged
+            // values to be read again: the compiler cannot tell sF from the staged tile)
             const R uxx = UXXR(0, 0), uee = UEEP(0, 0);
-            sF[0 * kFN + e] = UR(0, 0) + (G * uxx) * (HUR(0, 0) + G * HUXXR(0, 0));   // ufx
-            sF[1 * kFN + e] = UP(0, 0) + (G * uee) * (HVP(0, 0) + G * HVXXP(0, 0));   // ufe
-            sF[2 * kFN + e] = VP(0, 0) + (G * uee) * (HUP(0, 0) + G * HUEEP(0, 0));   // vfx
-            sF[3 * kFN + e] = VR(0, 0) + (G * uxx) * (HVR(0, 0) + G * HVEER(0, 0));   // vfe
+            const R ufx = UR(0, 0) + (G * uxx) * (HUR(0, 0) + G * HUXXR(0, 0));
+            const R ufe = UP(0, 0) + (G * uee) * (HVP(0, 0) + G * HVXXP(0, 0));
+            const R vfx = VP(0, 0) + (G * uee) * (HUP(0, 0) + G * HUEEP(0, 0));
+            const R vfe = VR(0, 0) + (G * uxx) * (HVR(0, 0) + G * HVEER(0, 0));
+            sF[0 * kFN + e] = ufx;
+            sF[1 * kFN + e] = ufe;
+            sF[2 * kFN + e] = vfx;
+            sF[3 * kFN + e] = vfe;
         }
         __syncthreads();
         if (live) {
@@ -1115,7 +1192,10 @@ __device__ __forceinline__ void step3d_uv_body(const Geo<R> &g, R *__restrict__ 
 // old velocities and ru/rv at p), several levels ahead of the elimination, so that the bytes
 // in flight do not depend on how many threads an SM holds.  The U and V systems are
 // eliminated in one pass in the normalised Thomas form (c'_k = c_k / m_k,
-// d'_k = (r_k - a_k d'_{k-1}) / m_k, x_k = d'_k - c'_k x_{k+1}) with c', d' in shared memory,
+// d'_k = (r_k - a_k d'_{k-1}) / m_k, x_k = d'_k - c'_k x_{k+1}) with c' in shared memory and
+// d' in the output column itself (level k of u or v, whose old value the ring has already
+// staged; the back substitution reads it back in chunks and overwrites it with x_k), which
+// keeps a block's shared memory small enough for five blocks per SM,
 // and the barotropic sums of adjustBarotropicVelocity come from the column identity
 // sum_k hz_k x_k = sum_k r_k + fc_0 x_0 (the rows of the system summed: the off-diagonal terms
 // telescope, the bottom row keeps -fc_0 x_0), so the back-substitution reads nothing from
@@ -1130,8 +1210,9 @@ constexpr int kPipeThreads = 2 * kPipeCols;   // one thread per system (U, V) an
 constexpr int kPipeSlot = 3 * (2 * kPipeCols + 1) + 4 * kPipeCols;   // floats per level
 
 __host__ __device__ constexpr size_t pipe_smem_bytes(int N) {
-    return sizeof(float) * ((size_t)2 * N * kPipeThreads + (size_t)kPipeDepth * kPipeSlot);
+    return sizeof(float) * ((size_t)N * kPipeThreads + (size_t)kPipeDepth * kPipeSlot);
 }
+constexpr int kBackChunk = 8;   // levels of d' read ahead per step of the back substitution
 
 template <typename R>   // R = float only: the FP32 form
 __device__ __forceinline__ void step3d_uv_pipe_body(const Geo<R> &g, float *__restrict__ u,
@@ -1148,8 +1229,9 @@ __device__ __forceinline__ void step3d_uv_pipe_body(const Geo<R> &g, float *__re
     const int col = threadIdx.x & (kPipeCols - 1), sys = threadIdx.x / kPipeCols;
     const long p0 = tile * kPipeCols;
     const long p = p0 + col;
-    float *cc = spipe + threadIdx.x, *dd = cc + N * kPipeThreads;   // [level][thread]
-    float *ring = spipe + 2 * N * kPipeThreads;
+    float *cc = spipe + threadIdx.x;   // [level][thread]
+    float *ring = spipe + N * kPipeThreads;
+    float *const outc = (sys == 0 ? u : v) + p;   // this system's output column (d', then x)
     const float *uo_all = tmpU ? tmpU : u, *vo_all = tmpV ? tmpV : v;
 
     // level k into slot: Hz(k), Akv(k), z_r(k+1) at [p0-1, p0+63] (sys 0 copies these, plus
@@ -1229,7 +1311,7 @@ __device__ __forceinline__ void step3d_uv_pipe_body(const Geo<R> &g, float *__re
             Rs += (double)rr;
         }
         cc[k * kPipeThreads] = ccp;
-        dd[k * kPipeThreads] = ddp;
+        outc[(long)k * s2] = ddp;
         fc = gk;
         H += (double)hz;
         O += (double)(ok * hz);
@@ -1253,11 +1335,18 @@ __device__ __forceinline__ void step3d_uv_pipe_body(const Geo<R> &g, float *__re
         const double dbar = sys == 0 ? DU[p] / (double)g.on_u[p] : DV[p] / (double)g.om_v[p];
         const float sub = (float)((O - dbar) / H);
         float x = ddp;
-        float *out = (sys == 0 ? u : v) + p;
-        out[(long)(N - 1) * s2] = x - sub;
-        for (int k = N - 2; k >= 0; --k) {
-            x = dd[k * kPipeThreads] - cc[k * kPipeThreads] * x;
-            out[(long)k * s2] = x - sub;
+        outc[(long)(N - 1) * s2] = x - sub;
+        for (int k = N - 2; k >= 0; k -= kBackChunk) {
+            float dv[kBackChunk];   // the chunk's d' first (independent loads), then the chain
+#pragma unroll
+            for (int h = 0; h < kBackChunk; ++h) dv[h] = k - h >= 0 ? outc[(long)(k - h) * s2] : 0.f;
+#pragma unroll
+            for (int h = 0; h < kBackChunk; ++h) {
+                if (k - h >= 0) {
+                    x = dv[h] - cc[(k - h) * kPipeThreads] * x;
+                    outc[(long)(k - h) * s2] = x - sub;
+                }
+            }
         }
         // sum_k hz_k (x_k - sub) from the column identity
         const double Hx = Rs + (double)fc0 * (double)x - (double)sub * H;
@@ -1514,11 +1603,11 @@ __global__ void __launch_bounds__(kBlock) kb_corr_point(
                     O2(rub0), O2(rub1), O2(vbar_t2), (long)mb_.y * kBlock + threadIdx.x);
 }
 
-template <typename R, int TX, int TY>
-__global__ void __launch_bounds__(TX * TY, 5) k_rhs3d(Geo<R> g, const R *__restrict__ u, const R *__restrict__ v,
+template <typename R, int TX, int TY, bool P2>
+__global__ void __launch_bounds__(TX * TY, 4) k_rhs3d(Geo<R> g, const R *__restrict__ u, const R *__restrict__ v,
                                                   const R *Huon, const R *Hvom, const R *__restrict__ W,
                                                   const R *__restrict__ Hz, R *__restrict__ ru, R *__restrict__ rv) {
-    rhs3d_body<R, TX, TY>(g, u, v, Huon, Hvom, W, Hz, ru, rv, (int)blockIdx.x, (int)blockIdx.y);
+    rhs3d_body<R, TX, TY, P2>(g, u, v, Huon, Hvom, W, Hz, ru, rv, (int)blockIdx.x, (int)blockIdx.y);
 }
 template <typename R, int TX, int TY>
 __global__ void __launch_bounds__(TX *TY) kb_rhs3d(const Member<R> *mt, const int2 *bm, int var,
@@ -1527,8 +1616,8 @@ __global__ void __launch_bounds__(TX *TY) kb_rhs3d(const Member<R> *mt, const in
                                                    R *__restrict__ ru, R *__restrict__ rv) {
     SF_MEMBER(bm)
     const int ntx = M_.ntx[var];
-    rhs3d_body<R, TX, TY>(g, O3(u), O3(v), O3(Huon), O3(Hvom), O3(W), ON(Hz), O3(ru), O3(rv),
-                          mb_.y % ntx, mb_.y / ntx);
+    rhs3d_body<R, TX, TY, false>(g, O3(u), O3(v), O3(Huon), O3(Hvom), O3(W), ON(Hz), O3(ru), O3(rv),
+                                 mb_.y % ntx, mb_.y / ntx);
 }
 
 template <typename R>
@@ -1717,7 +1806,9 @@ cudaError_t Ops<R>::rhs3d(const sf_ctx *c, const R *u, const R *v, const R *Huon
         int dev = 0;
         cudaGetDevice(&dev);
         if (dev >= 0 && dev < 64 && !attr_set[dev]) {
-            cudaFuncSetAttribute(k_rhs3d<R, TX, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            cudaFuncSetAttribute(k_rhs3d<R, TX, TY, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem);
+            cudaFuncSetAttribute(k_rhs3d<R, TX, TY, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem);
             cudaFuncSetAttribute(kb_rhs3d<R, TX, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem);
@@ -1728,7 +1819,16 @@ cudaError_t Ops<R>::rhs3d(const sf_ctx *c, const R *u, const R *v, const R *Huon
                 mt<R>(c), c->bm_tile[var], var, u, v, Huon, Hvom, W, Hz, ru, rv);
         } else {
             const dim3 grid((c->I + TX - 1) / TX, (c->J + TY - 1) / TY), block(TX, TY);
-            k_rhs3d<R, TX, TY><<<grid, block, smem, s>>>(geo(c), u, v, Huon, Hvom, W, Hz, ru, rv);
+            // pair staging: even rows, fields on 2-element boundaries, 32-bit flat offsets
+            const uintptr_t al = 2 * sizeof(R);
+            const bool p2 = c->I % 2 == 0 && (long)c->I * c->J < (1L << 30) &&
+                            (uintptr_t)u % al == 0 && (uintptr_t)v % al == 0 &&
+                            (uintptr_t)Huon % al == 0 && (uintptr_t)Hvom % al == 0 &&
+                            (uintptr_t)W % al == 0 && (uintptr_t)Hz % al == 0;
+            if (p2)
+                k_rhs3d<R, TX, TY, true><<<grid, block, smem, s>>>(geo(c), u, v, Huon, Hvom, W, Hz, ru, rv);
+            else
+                k_rhs3d<R, TX, TY, false><<<grid, block, smem, s>>>(geo(c), u, v, Huon, Hvom, W, Hz, ru, rv);
         }
     };
     using I32 = std::integral_constant<int, 32>;
