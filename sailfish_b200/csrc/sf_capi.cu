@@ -299,7 +299,8 @@ int build_pred_maps(sf_ctx *c, const ProgHost &Z, const ProgHost &U, const ProgH
     }
     int rc = upload(&c->bcmap, map.data(), map.size(), "boundary maps");
     if (rc == SF_OK) {
-        if (cudaMalloc(&c->pred_counter, sizeof(int)) != cudaSuccess)
+        // the counter, then (at byte 256) the chained entries' values, 3 x kMaxChained
+        if (cudaMalloc(&c->pred_counter, 256 + 3 * sf::kMaxChained * sizeof(double)) != cudaSuccess)
             return fail(SF_ENOMEM, "cudaMalloc predictor counter");
         if (cudaMemset(c->pred_counter, 0, sizeof(int)) != cudaSuccess)
             return fail(SF_ECUDA, "cudaMemset predictor counter");

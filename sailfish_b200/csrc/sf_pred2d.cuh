@@ -15,7 +15,11 @@
 // inputs or, where the predictor does not write the node, the node's old content.  So no block
 // waits for another.  Destinations are written with their final values, except those of
 // chained entries (a destination that is also a source, e.g. at corners), whose old content
-// other blocks may still read: the last block to finish writes them.
+// other blocks may still read: block 0 evaluates them first (into a small buffer, while every
+// old content is intact) and the last block to finish copies them into place.  Old contents are read only
+// where a node off the deep region is evaluated, i.e. by the ring blocks and by the tiles whose
+// nodes or halo reach the outer ring ("edge" blocks); tiles wholly inside (tile and halo deep)
+// read only the step's inputs, so they leave without taking part in the count.
 #pragma once
 #include "sf_internal.h"
 
@@ -34,6 +38,7 @@ struct PredArgs {
     const double *valp;             // ... or read from the device (graph replay)
     BcProgram pz, pu, pv;           // for the chained entries
     int *counter;                   // blocks done (last-block detection), reset by the last
+    R *chv;                         // chained entries' values [3][kMaxChained], from block 0
 };
 
 __device__ __forceinline__ int bc_src(int m) { return (m & (kBcChained - 1)) - 2; }
@@ -264,9 +269,13 @@ __device__ __forceinline__ long prd_ring_node(int e, int I, int J) {
 // j0+ty+8, so every load of a warp is 32 consecutive nodes of one row.  A tile block fills
 // its shared zeta_t2 for ring nodes too (the deep nodes next to the ring read them) but
 // leaves their outputs to the ring blocks.
+__host__ __device__ __forceinline__ bool prd_inner_tile(int i0, int j0, int I, int J) {
+    return i0 >= 3 && j0 >= 3 && i0 + kPredTX + 2 <= I && j0 + kPredTY + 2 <= J;
+}
+
 template <typename R>
 __global__ void __launch_bounds__(256, 5) k_pred2d(const __grid_constant__ PredArgs<R> a,
-                                                int ring_blocks, int tiles_x) {
+                                                int ring_blocks, int tiles_x, int edge_blocks) {
     pdl_enter();
     __shared__ R sZ[kPredTY + 1][kPredTX + 1];   // zeta_t2 after zetabc, (j0-1.., i0-1..)
     __shared__ int s_last;
@@ -276,6 +285,15 @@ __global__ void __launch_bounds__(256, 5) k_pred2d(const __grid_constant__ PredA
     const int tid = ty * 32 + tx;
     const int bid = (int)blockIdx.x;
     int i0 = -kPredTX - 2, j0 = -kPredTY - 2;   // ring blocks: a tile no node falls in
+    if (bid == 0) {   // the chained entries' values (the last block stores them)
+        const BcProgram *ps[3] = {&a.pz, &a.pu, &a.pv};
+#pragma unroll
+        for (int f = 0; f < 3; ++f)
+            if (tid < ps[f]->nch)
+                a.chv[f * kMaxChained + tid] =
+                    prd_bc_value(a, PrdTile<R>{sZ, i0, j0}, f, ps[f]->src_ch[tid]);
+        __threadfence();   // ... visible before this block counts itself
+    }
     if (bid < ring_blocks) {
         const int e = bid * 256 + tid;
         if (e < 4 * I + 4 * (J - 4)) prd_edge_node(a, PrdTile<R>{sZ, i0, j0}, prd_ring_node(e, I, J));
@@ -323,6 +341,7 @@ __global__ void __launch_bounds__(256, 5) k_pred2d(const __grid_constant__ PredA
                 prd_deep_mom(a, (long)q, pd, sZ[r][c], sZ[r][c - 1], sZ[r - 1][c]);
             }
         }
+        if (prd_inner_tile(i0, j0, I, J)) return;   // uniform over the block: no barrier below
     }
 
     // ---- chained destinations: the last block, after every block's reads -------------------
@@ -330,11 +349,10 @@ __global__ void __launch_bounds__(256, 5) k_pred2d(const __grid_constant__ PredA
     // value feeds a store or a branch before it), so once a block has counted itself, none of
     // its reads of old contents is pending and the last block may overwrite them.
     __syncthreads();
-    if (tid == 0) s_last = atomicAdd(a.counter, 1) == (int)gridDim.x - 1;
+    if (tid == 0) s_last = atomicAdd(a.counter, 1) == edge_blocks - 1;
     __syncthreads();
     if (!s_last) return;
     __threadfence();
-    const PrdTile<R> t{sZ, i0, j0};
     const BcProgram *ps[3] = {&a.pz, &a.pu, &a.pv};
     R v[3] = {R(0), R(0), R(0)};
     int d[3] = {-1, -1, -1};
@@ -343,10 +361,9 @@ __global__ void __launch_bounds__(256, 5) k_pred2d(const __grid_constant__ PredA
         const BcProgram &p = *ps[f];
         if (tid < p.nch) {
             d[f] = p.dst_ch[tid];
-            v[f] = prd_bc_value(a, t, f, p.src_ch[tid]);
+            v[f] = __ldcg(a.chv + f * kMaxChained + tid);
         }
     }
-    __syncthreads();
     if (d[0] >= 0) a.z2[d[0]] = v[0];
     if (d[1] >= 0) a.ub2[d[1]] = v[1];
     if (d[2] >= 0) a.vb2[d[2]] = v[2];
@@ -382,10 +399,17 @@ cudaError_t Ops<R>::pred2d(const sf_ctx *c, R *z0, R *z1, R *z2, R *ub1, R *vb1,
     a.pu = c->ubc;
     a.pv = c->vbc;
     a.counter = c->pred_counter;
+    a.chv = reinterpret_cast<R *>(reinterpret_cast<char *>(c->pred_counter) + 256);
     const int tiles_x = (c->I + kPredTX - 1) / kPredTX, tiles_y = (c->J + kPredTY - 1) / kPredTY;
     const int ring_blocks = (4 * c->I + 4 * (c->J - 4) + 255) / 256;
+    // the blocks counted before the chained writes: the ring blocks and the tiles that are not
+    // inner (the condition is separable: inner columns of tiles times inner rows of tiles)
+    int inner_x = 0, inner_y = 0;
+    for (int tx = 0; tx < tiles_x; ++tx) inner_x += prd_inner_tile(tx * kPredTX, 3, c->I, 3 + kPredTY + 2);
+    for (int ty = 0; ty < tiles_y; ++ty) inner_y += prd_inner_tile(3, ty * kPredTY, 3 + kPredTX + 2, c->J);
+    const int edge_blocks = ring_blocks + tiles_x * tiles_y - inner_x * inner_y;
     return launch_dep(c, k_pred2d<R>, dim3((unsigned)(ring_blocks + tiles_x * tiles_y)), dim3(32, 8),
-                      0, s, a, ring_blocks, tiles_x);
+                      0, s, a, ring_blocks, tiles_x, edge_blocks);
 }
 
 }  // namespace sf

@@ -68,18 +68,21 @@ def test_main3d_fp32_error_stated():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("ndtfast,precision", [(4, "fp64"), (5, "fp64"), (7, "fp64"),
-                                               (30, "fp64"), (30, "fp32")])
-def test_graph_replay_of_the_barotropic_loop_is_identical(ndtfast, precision):
+@pytest.mark.parametrize("ndtfast,precision,L,M", [(4, "fp64", 24, 24), (5, "fp64", 24, 24),
+                                                   (7, "fp64", 24, 24), (30, "fp64", 24, 24),
+                                                   (30, "fp32", 24, 24), (5, "fp64", 100, 60)])
+def test_graph_replay_of_the_barotropic_loop_is_identical(ndtfast, precision, L, M):
     """sf_barotropic_loop replayed from captured CUDA graphs (the default) against plain
     launches, with and without programmatic dependent launch and the fused predictor, over
-    steps whose slot rotation cycles through all three phases: bit-identical in FP64."""
+    steps whose slot rotation cycles through all three phases: bit-identical in FP64.  The
+    100 x 60 basin has fused-predictor tiles wholly inside the deep region (which leave before
+    the count that orders the corner chains' writes) as well as edge tiles."""
     import numpy as np
     import torch
     from sailfish_b200 import configs
     from sailfish_b200._lib import lib
     from sailfish_b200.model import Model
-    cfg = configs.basin(24, 24, 6, 2.0e4, [(0.5, 0.5)], dt=240.0, ndtfast=ndtfast)
+    cfg = configs.basin(L, M, 6, 2.0e4, [(0.5, 0.5)], dt=240.0, ndtfast=ndtfast)
     g = cfg["grid"]
     bump = 1e-3 * np.exp(-((g.x - g.x.max() / 2) ** 2 + (g.y - g.y.max() / 2) ** 2) / (1e5) ** 2)
     out = []
