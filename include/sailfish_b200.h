@@ -98,7 +98,7 @@ int sf_ctx_destroy(sf_ctx *ctx);
  * members share the precision; nothing else needs to match. */
 int sf_ctx_create_ensemble(const sf_grid_desc *descs, int n, sf_ctx **out);
 /* Tile shape of the tiled 3D right-hand side (sf_rhs3d) for this context: 0 = 32 x 8 rho points
- * (default), 1 = 32 x 4, 2 = 64 x 4.  Results do not
+ * (default), 1 = 32 x 4, 2 = 64 x 4, 3 = 32 x 16.  Results do not
  * depend on it; the autotuner (sailfish_b200.autotune) times the variants and picks one. */
 int sf_ctx_set_tile(sf_ctx *ctx, int variant);
 /* Number of members (1 for sf_ctx_create). */

@@ -1,7 +1,7 @@
 """Autotuner: picks launch shapes for a context by timing them on the model's own state.
 
 The knob is the tile shape of the tiled 3D right-hand side (sf_ctx_set_tile: 32 x 8, 32 x 4,
-64 x 4 rho points per block), which trades halo re-reads (smaller tiles stage relatively more
+64 x 4, 32 x 16 rho points per block), which trades halo re-reads (smaller tiles stage relatively more
 halo) against blocks per SM and, for ensembles, against the ragged edges of small members.
 Results do not depend on the choice; only the time does.
 """
@@ -12,7 +12,7 @@ import torch
 from ._lib import check, lib
 from .model import stream_handle
 
-TILES = {0: (32, 8), 1: (32, 4), 2: (64, 4)}
+TILES = {0: (32, 8), 1: (32, 4), 2: (64, 4), 3: (32, 16)}
 
 
 def _time(fn, reps):
@@ -28,7 +28,7 @@ def _time(fn, reps):
     return a.elapsed_time(b) / reps
 
 
-def tune_rhs3d(model, reps=5, variants=(0, 1, 2)):
+def tune_rhs3d(model, reps=5, variants=tuple(TILES)):
     """Times sf_rhs3d on `model` (a Model or Ensemble) for each tile variant, leaves the fastest
     set on its context and returns {variant: ms}."""
     c, p = model.ctx.ptr, model._p

@@ -486,7 +486,7 @@ int sf_ctx_members(const sf_ctx *c) { return c ? c->nmem : 0; }
 
 int sf_ctx_set_tile(sf_ctx *c, int variant) {
     if (!c) return fail(SF_EINVAL, "null context");
-    if (variant < 0 || variant >= sf::kRhsTiles) return fail(SF_EINVAL, "tile variant is 0, 1 or 2");
+    if (variant < 0 || variant >= sf::kRhsTiles) return fail(SF_EINVAL, "tile variant is 0, 1, 2 or 3");
     c->rhs_tile = variant;
     return SF_OK;
 }

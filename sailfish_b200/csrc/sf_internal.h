@@ -81,8 +81,8 @@ constexpr int kPipeTile = 64;              // columns per block of the pipelined
 // One member of an ensemble context: its grid view (metric pointers into the context's
 // pools) and the offsets of its fields in the state pools: 2D fields (off2), fields of N+1
 // levels (off3) and of N levels (offN); ntx = tiles along xi of the tiled kernels.
-constexpr int kRhsTiles = 3;
-constexpr int kRhsTileX[kRhsTiles] = {32, 32, 64}, kRhsTileY[kRhsTiles] = {8, 4, 4};
+constexpr int kRhsTiles = 4;
+constexpr int kRhsTileX[kRhsTiles] = {32, 32, 64, 32}, kRhsTileY[kRhsTiles] = {8, 4, 4, 16};
 template <typename R>
 struct Member {
     Geo<R> g;

@@ -516,7 +516,7 @@ __global__ void __launch_bounds__(256) k_bc_apply(BcProgram p1, R *f1, BcProgram
 // with a halo of rows j-3..j+2 and columns i-2..i+2.  The halo is addressed by flat index
 // (j0+r)*I + (i0+c), so columns beyond the row ends wrap into the neighbouring rows exactly as
 // the reference's flat-index stencils do; reads before the array start or past its end stage 0.
-// Tile shapes (TX x TY): 32 x 8 (the default), 32 x 4 and 64 x 4, chosen per context
+// Tile shapes (TX x TY): 32 x 8 (the default), 32 x 4, 64 x 4 and 32 x 16, chosen per context
 // (sf_ctx_set_tile, e.g. by the autotuner); the staged tile adds the halo.
 constexpr int kTX = kTileX, kTY = kTileY;
 constexpr int kHY0 = 3, kHY1 = 2, kHX0 = 2, kHX1 = 2;          // halo extents
@@ -554,6 +554,11 @@ __device__ __forceinline__ void cp_async(float *dst, const float *src, bool ok) 
 __device__ __forceinline__ void cp_async(double *dst, const double *src, bool ok) {
     const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(ok ? 8 : 0));
+}
+// 4-byte copy of n (4 or 0) source bytes: 0 zero-fills the destination without reading.
+__device__ __forceinline__ void cp_async_n(float *dst, const float *src, int n) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src), "r"(n));
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int n>
@@ -1242,22 +1247,30 @@ __device__ __forceinline__ void step3d_uv_pipe_body(const Geo<R> &g, float *__re
     const bool okE = sys == 0 && col == 0 && qE < s2;
     constexpr int kRow = 2 * kPipeCols + 1;
     const int seg = sys == 0 ? col : kPipeCols + 1 + col;
+    // the copy sources at level 0 and the copy sizes, fixed over the levels: a level adds k s2
+    // (an out-of-range copy keeps a valid address and copies 0 bytes)
+    const long qq = okq ? q : 0, qe = okE ? qE : 0, pp = okP ? p : 0;
+    const float *const cHz = Hz + qq, *const cAk = Akv + qq, *const cZr = z_r + s2 + qq;
+    const float *const eHz = Hz + qe, *const eAk = Akv + qe, *const eZr = z_r + s2 + qe;
+    const float *const cO = (sys == 0 ? uo_all : vo_all) + pp, *const cR = (sys == 0 ? ru : rv) + pp;
+    const int nq = okq ? 4 : 0, ne = okE ? 4 : 0, np = okP ? 4 : 0;
+    const bool edge = sys == 0 && col == 0;
+    const int oO = 3 * kRow + sys * kPipeCols + col, oR = 3 * kRow + (2 + sys) * kPipeCols + col;
     auto issue = [&](int k) {
         float *sl = ring + (k % kPipeDepth) * kPipeSlot;
         const long o = (long)k * s2;
-        const bool zr = k + 1 < N;
-        const float *fld[3] = {Hz + o, Akv + o, z_r + o + s2};
-#pragma unroll
-        for (int f = 0; f < 3; ++f) {
-            const bool on = f < 2 || zr;
-            float *d = sl + f * kRow;
-            cp_async(d + seg, fld[f] + (okq && on ? q : 0), okq && on);
-            if (sys == 0 && col == 0) cp_async(d + kPipeCols, fld[f] + (okE && on ? qE : 0), okE && on);
+        const long oz = k + 1 < N ? o : o - s2;   // z_r(k+1) exists for k < N-1 only
+        const int nz = k + 1 < N ? nq : 0, nze = k + 1 < N ? ne : 0;
+        cp_async_n(sl + seg, cHz + o, nq);
+        cp_async_n(sl + kRow + seg, cAk + o, nq);
+        cp_async_n(sl + 2 * kRow + seg, cZr + oz, nz);
+        if (edge) {
+            cp_async_n(sl + kPipeCols, eHz + o, ne);
+            cp_async_n(sl + kRow + kPipeCols, eAk + o, ne);
+            cp_async_n(sl + 2 * kRow + kPipeCols, eZr + oz, nze);
         }
-        float *d = sl + 3 * kRow;
-        const float *a = sys == 0 ? uo_all : vo_all, *r = sys == 0 ? ru : rv;
-        cp_async(d + sys * kPipeCols + col, a + o + (okP ? p : 0), okP);
-        cp_async(d + (2 + sys) * kPipeCols + col, r + o + (okP ? p : 0), okP);
+        cp_async_n(sl + oO, cO + o, np);
+        cp_async_n(sl + oR, cR + o, np);
     };
     const int i = (int)(p % I), j = (int)(p / I);
     const bool live = p < s2;
@@ -1604,7 +1617,7 @@ __global__ void __launch_bounds__(kBlock) kb_corr_point(
 }
 
 template <typename R, int TX, int TY, bool P2>
-__global__ void __launch_bounds__(TX * TY, 4) k_rhs3d(Geo<R> g, const R *__restrict__ u, const R *__restrict__ v,
+__global__ void __launch_bounds__(TX * TY, 1024 / (TX * TY)) k_rhs3d(Geo<R> g, const R *__restrict__ u, const R *__restrict__ v,
                                                   const R *Huon, const R *Hvom, const R *__restrict__ W,
                                                   const R *__restrict__ Hz, R *__restrict__ ru, R *__restrict__ rv) {
     rhs3d_body<R, TX, TY, P2>(g, u, v, Huon, Hvom, W, Hz, ru, rv, (int)blockIdx.x, (int)blockIdx.y);
@@ -1797,7 +1810,7 @@ cudaError_t Ops<R>::bc_apply(const sf_ctx *c, const BcProgram &p1, R *f1, const 
 template <typename R>
 cudaError_t Ops<R>::rhs3d(const sf_ctx *c, const R *u, const R *v, const R *Huon, const R *Hvom,
                           const R *W, const R *Hz, R *ru, R *rv, cudaStream_t s) {
-    // tile variant: 0 = 32 x 8, 1 = 32 x 4, 2 = 64 x 4
+    // tile variant: 0 = 32 x 8, 1 = 32 x 4, 2 = 64 x 4, 3 = 32 x 16
     const int var = c->rhs_tile;
     auto run = [&](auto tx, auto ty) {
         constexpr int TX = decltype(tx)::value, TY = decltype(ty)::value;
@@ -1835,7 +1848,10 @@ cudaError_t Ops<R>::rhs3d(const sf_ctx *c, const R *u, const R *v, const R *Huon
     using I8 = std::integral_constant<int, 8>;
     using I4 = std::integral_constant<int, 4>;
     using I64 = std::integral_constant<int, 64>;
-    if (var == 1) {
+    using I16 = std::integral_constant<int, 16>;
+    if (var == 3) {
+        run(I32{}, I16{});
+    } else if (var == 1) {
         run(I32{}, I4{});
     } else if (var == 2) {
         run(I64{}, I4{});

@@ -74,7 +74,7 @@ def test_rhs3d_tile_variants_agree_and_autotune_picks_one(precision):
     ens = ensemble.make(members, precision=precision, dt=240.0, ndtfast=10)
     ens.step(2)
     out = {}
-    for v in (0, 1, 2):
+    for v in (0, 1, 2, 3):
         assert lib.sf_ctx_set_tile(ens.ctx.ptr, v) == 0
         ens.ru.zero_()
         ens.rv.zero_()
@@ -85,12 +85,12 @@ def test_rhs3d_tile_variants_agree_and_autotune_picks_one(precision):
         out[v] = (ens.ru.clone(), ens.rv.clone())
     # (the non-square member's state is not finite after two steps of the reference's scheme:
     # NaNs must sit in the same places)
-    for v in (1, 2):
+    for v in (1, 2, 3):
         tol = dict(rtol=0, atol=0) if precision == "fp64" else dict(rtol=1e-5, atol=1e-6)
         for k in range(2):
             torch.testing.assert_close(out[v][k], out[0][k], equal_nan=True, **tol)
     times = autotune.tune_rhs3d(ens, reps=2)
-    assert set(times) == {0, 1, 2} and ens.rhs_tile in times
+    assert set(times) == {0, 1, 2, 3} and ens.rhs_tile in times
 
 
 def ctypes_stream():

@@ -134,3 +134,35 @@ def test_overlapped_phases_give_the_same_step(precision, mode):
         out.append(st)
     for k in ("zeta", "ubar", "vbar", "u", "v", "W", "Zt_avg1", "AKv", "tke"):
         np.testing.assert_array_equal(out[1][k], out[0][k], err_msg=k)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("Lm", [70, 69])
+def test_rhs3d_tile_variants_agree_on_one_grid(Lm):
+    """sf_rhs3d on one square grid with every tile variant, bit-identical in FP64: an even row
+    length (Lm = 70, I = 72) takes the paired staging, an odd one (I = 71) the element staging."""
+    import numpy as np
+    import torch
+    from sailfish_b200 import configs
+    from sailfish_b200._lib import lib
+    from sailfish_b200.model import Model, stream_handle
+    cfg = configs.basin(Lm, Lm, 8, 2.0e3, [(0.5, 0.5)], dt=120.0, ndtfast=10)
+    g = cfg["grid"]
+    bump = 1e-3 * np.exp(-((g.x - g.x.max() / 2) ** 2 + (g.y - g.y.max() / 2) ** 2) / (2e4) ** 2)
+    m = Model(g, cfg["boundary"], cfg["dt"], cfg["ndtfast"], precision="fp64")
+    m.Zt_avg1.copy_(torch.from_numpy(bump.ravel()))
+    m.step(2)
+    p = m._p
+    out = []
+    for v in (0, 1, 2, 3):
+        assert lib.sf_ctx_set_tile(m.ctx.ptr, v) == 0
+        m.ru.zero_()
+        m.rv.zero_()
+        assert lib.sf_rhs3d(m.ctx.ptr, p(m.u), p(m.v), p(m.Huon), p(m.Hvom), p(m.W), p(m.Hz),
+                            p(m.ru), p(m.rv), stream_handle()) == 0
+        torch.cuda.synchronize()
+        out.append((m.ru.cpu().numpy(), m.rv.cpu().numpy()))
+    assert np.isfinite(out[0][0]).all() and np.abs(out[0][0]).max() > 0
+    for o in out[1:]:
+        np.testing.assert_array_equal(o[0], out[0][0])
+        np.testing.assert_array_equal(o[1], out[0][1])
