@@ -788,9 +788,13 @@ __device__ __forceinline__ void rhs3d_body(const Geo<R> &g, const R *__restrict_
 #define HUEEP(r, c) ((DEE(HU, r, c) + DEE(HU, r, (c) - 1)) * R(0.5))
 #define HVXXP(r, c) ((DXX(HV, r, c) + DXX(HV, (r) - 1, c)) * R(0.5))
 #define HVEER(r, c) ((DEE(HV, r, c) + DEE(HV, (r) + 1, c)) * R(0.5))
-        for (int e = tid; e < kFN; e += TX * TY) {   // phase 1: face fluxes of cell (r, c)
-            const int r = e / kFX - 1, c = e % kFX - 1;
-            if (r < 0 && c < 0) continue;            // the corner cell is nobody's neighbour
+        // phase 1: face fluxes of cell (r, c), -1 <= r < TY, -1 <= c < TX.  Each thread takes
+        // its own cell; warp row 0 also the south halo row and warp row 1 the west halo column
+        // (the corner cell is nobody's neighbour).  A warp's lanes stay in one row, so its
+        // shared loads are conflict-free (a lane mapping running across the 36-float staged rows
+        // put lanes 4 columns apart in adjacent rows on one bank).
+        auto face_flux = [&](int r, int c) {
+            const int e = (r + 1) * kFX + (c + 1);
             const int bb = (r + kHY0) * kSX + (c + kHX0);
             const Tile<R, kSX> U{bf[0], bb}, V{bf[1], bb}, HU{bf[2], bb}, HV{bf[3], bb};
             // all four first, then the stores (a store between them would force the staged
@@ -804,7 +808,10 @@ __device__ __forceinline__ void rhs3d_body(const Geo<R> &g, const R *__restrict_
             sF[1 * kFN + e] = ufe;
             sF[2 * kFN + e] = vfx;
             sF[3 * kFN + e] = vfe;
-        }
+        };
+        face_flux(ty, tx);
+        if (ty == 0) face_flux(-1, tx);
+        else if (ty == 1 && tx < TY) face_flux(tx, -1);
         __syncthreads();
         if (live) {
         {   // phase 2: this cell's divergence
