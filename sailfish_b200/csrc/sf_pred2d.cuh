@@ -252,6 +252,67 @@ __device__ __forceinline__ void prd_deep_mom(const PredArgs<R> &a, long x, bool 
     }
 }
 
+// A deep node's inputs that both phases use, read once in phase 1 and kept in registers across
+// the block's barrier: zeta_t1 and h at the node and its west and south neighbours, ubar_t1,
+// vbar_t1, the metrics and zeta_t0 at the node.
+template <typename R>
+struct PrdNode {
+    R z1p, z1w, z1s, hp, hw, hs, ub, vb, pm, pn, ou, ov, z0p;
+};
+
+// prd_rz_deep, filling the node's kept inputs (the same operations in the same order).
+template <typename R>
+__device__ __forceinline__ R prd_rz_keep(const PredArgs<R> &a, long x, PrdNode<R> &n) {
+    const Geo<R> &g = a.g;
+    const int I = g.I;
+    const R *z = a.z1 + x, *h = g.h + x, *ub = a.ub1 + x, *vb = a.vb1 + x, *ou = g.on_u + x,
+            *ov = g.om_v + x;
+    n.z1p = z[0];
+    n.z1w = z[-1];
+    n.z1s = z[-I];
+    n.hp = h[0];
+    n.hw = h[-1];
+    n.hs = h[-I];
+    n.ub = ub[0];
+    n.vb = vb[0];
+    n.ou = ou[0];
+    n.ov = ov[0];
+    n.pm = g.pm[x];
+    n.pn = g.pn[x];
+    n.z0p = a.z0[x];
+    const R Dp = n.z1p + n.hp, Dw = n.z1w + n.hw, De = z[1] + h[1];
+    const R Ds = n.z1s + n.hs, Dn = z[I] + h[I];
+    const R DUp = n.ub * ((Dp + Dw) * R(0.5));
+    const R DUe = ub[1] * ((De + Dp) * R(0.5));
+    const R DVp = n.vb * ((Dp + Ds) * R(0.5));
+    const R DVn = vb[I] * ((Dn + Dp) * R(0.5));
+    return (((DUe * ou[1] - DUp * n.ou) + (DVn * ov[I] - DVp * n.ov)) * n.pm) * n.pn;
+}
+
+// prd_deep_mom from the node's kept inputs (the same operations in the same order).
+template <typename R>
+__device__ __forceinline__ void prd_deep_mom_kept(const PredArgs<R> &a, long x, bool pd, R zp,
+                                                  R zw, R zs, const PrdNode<R> &n) {
+    const int I = a.g.I;
+    const R *z0 = a.z0 + x;
+    const R gp = a.w1 * zp + a.w * n.z0p;
+    const R gw = a.w1 * zw + a.w * z0[-1];
+    const R gs = a.w1 * zs + a.w * z0[-I];
+    const R ru = (a.grav * n.ou) * (((n.hp + n.hw) * R(0.5)) * (gp - gw) + R(0.5) * (gp * gp - gw * gw));
+    const R rv = (a.grav * n.ov) * (((n.hp + n.hs) * R(0.5)) * (gp - gs) + R(0.5) * (gp * gp - gs * gs));
+    a.ru[x] = ru;
+    a.rv[x] = rv;
+    if (pd) {
+        const R D1p = n.z1p + n.hp, D2p = zp + n.hp;
+        const R D1U = (D1p + (n.z1w + n.hw)) * R(0.5);
+        const R D2U = (D2p + (zw + n.hw)) * R(0.5);
+        const R D1V = (D1p + (n.z1s + n.hs)) * R(0.5);
+        const R D2V = (D2p + (zs + n.hs)) * R(0.5);
+        a.ub2[x] = ddiv(n.ub * D1U + ((a.Dt * ru) * n.pm) * n.pn, D2U);
+        a.vb2[x] = ddiv(n.vb * D1V + ((a.Dt * rv) * n.pm) * n.pn, D2V);
+    }
+}
+
 // The ring nodes: 4 I nodes of rows 0, 1, J-2, J-1, then 4 (J-4) of columns 0, 1, I-2, I-1.
 __device__ __forceinline__ long prd_ring_node(int e, int I, int J) {
     if (e < 4 * I) {
@@ -303,6 +364,7 @@ __global__ void __launch_bounds__(256, 5) k_pred2d(const __grid_constant__ PredA
         j0 = (tb / tiles_x) * kPredTY;
         const int i = i0 + tx;
         // ---- phase 1: zeta_t2 (after zetabc) on the tile and its south/west halo ------------
+        PrdNode<R> kept[kPredTY / 8];   // a deep node's inputs, for phase 2
 #pragma unroll
         for (int h = 0; h < kPredTY; h += 8) {
             const int j = j0 + ty + h;
@@ -310,8 +372,8 @@ __global__ void __launch_bounds__(256, 5) k_pred2d(const __grid_constant__ PredA
                 const long x = (long)j * I + i;
                 R z;
                 if (prd_deep(i, j, I, J)) {
-                    const R r = prd_rz_deep(a, x);
-                    z = a.z0[x] + a.Dt * r;
+                    const R r = prd_rz_keep(a, x, kept[h / 8]);
+                    z = kept[h / 8].z0p + a.Dt * r;
                     a.rz[x] = r;
                     a.z2[x] = z;
                 } else {
@@ -338,7 +400,7 @@ __global__ void __launch_bounds__(256, 5) k_pred2d(const __grid_constant__ PredA
                 const int q = j * I + i;
                 const bool pd = q - fdiv(q, g.dJ) * J != 0 && q >= J;   // q % J != 0 (szJ)
                 const int r = ty + h + 1, c = tx + 1;
-                prd_deep_mom(a, (long)q, pd, sZ[r][c], sZ[r][c - 1], sZ[r - 1][c]);
+                prd_deep_mom_kept(a, (long)q, pd, sZ[r][c], sZ[r][c - 1], sZ[r - 1][c], kept[h / 8]);
             }
         }
         if (prd_inner_tile(i0, j0, I, J)) return;   // uniform over the block: no barrier below
