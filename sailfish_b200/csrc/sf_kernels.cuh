@@ -555,10 +555,12 @@ __device__ __forceinline__ void cp_async(double *dst, const double *src, bool ok
     const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(ok ? 8 : 0));
 }
-// 4-byte copy of n (4 or 0) source bytes: 0 zero-fills the destination without reading.
-__device__ __forceinline__ void cp_async_n(float *dst, const float *src, int n) {
-    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src), "r"(n));
+// 4-byte copy of n (4 or 0) source bytes to shared-window byte address saddr + OFF: 0
+// zero-fills the destination without reading.
+template <int OFF>
+__device__ __forceinline__ void cp_async_at(uint32_t saddr, const float *src, int n) {
+    asm volatile("cp.async.ca.shared.global [%0+%3], [%1], 4, %2;\n" ::"r"(saddr), "l"(src), "r"(n),
+                 "n"(OFF));
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int n>
@@ -1263,21 +1265,30 @@ __device__ __forceinline__ void step3d_uv_pipe_body(const Geo<R> &g, float *__re
     const int nq = okq ? 4 : 0, ne = okE ? 4 : 0, np = okP ? 4 : 0;
     const bool edge = sys == 0 && col == 0;
     const int oO = 3 * kRow + sys * kPipeCols + col, oR = 3 * kRow + (2 + sys) * kPipeCols + col;
+    // destinations as shared-window byte addresses in slot 0 (a level adds its slot's offset;
+    // the three fields of a row at immediate offsets), sources as 32-bit element offsets from
+    // level 0 (the launcher keeps (N+1) s2 below 2^31 for this kernel)
+    const uint32_t ring_s = (uint32_t)__cvta_generic_to_shared(ring);
+    const uint32_t dq = ring_s + 4u * seg, dE = ring_s + 4u * kPipeCols;
+    const uint32_t dO = ring_s + 4u * oO, dR = ring_s + 4u * oR;
+    const int s2i = (int)s2;
+    int nslot = 0;   // slot of the next level issued (levels are issued in order)
     auto issue = [&](int k) {
-        float *sl = ring + (k % kPipeDepth) * kPipeSlot;
-        const long o = (long)k * s2;
-        const long oz = k + 1 < N ? o : o - s2;   // z_r(k+1) exists for k < N-1 only
-        const int nz = k + 1 < N ? nq : 0, nze = k + 1 < N ? ne : 0;
-        cp_async_n(sl + seg, cHz + o, nq);
-        cp_async_n(sl + kRow + seg, cAk + o, nq);
-        cp_async_n(sl + 2 * kRow + seg, cZr + oz, nz);
+        const uint32_t sb = (uint32_t)nslot * (4u * kPipeSlot);
+        nslot = nslot + 1 == kPipeDepth ? 0 : nslot + 1;
+        const int o = k * s2i;
+        const bool zr = k + 1 < N;   // z_r(k+1) exists for k < N-1 only
+        const int oz = zr ? o : o - s2i;
+        cp_async_at<0>(dq + sb, cHz + o, nq);
+        cp_async_at<4 * kRow>(dq + sb, cAk + o, nq);
+        cp_async_at<8 * kRow>(dq + sb, cZr + oz, zr ? nq : 0);
         if (edge) {
-            cp_async_n(sl + kPipeCols, eHz + o, ne);
-            cp_async_n(sl + kRow + kPipeCols, eAk + o, ne);
-            cp_async_n(sl + 2 * kRow + kPipeCols, eZr + oz, nze);
+            cp_async_at<0>(dE + sb, eHz + o, ne);
+            cp_async_at<4 * kRow>(dE + sb, eAk + o, ne);
+            cp_async_at<8 * kRow>(dE + sb, eZr + oz, zr ? ne : 0);
         }
-        cp_async_n(sl + oO, cO + o, np);
-        cp_async_n(sl + oR, cR + o, np);
+        cp_async_at<0>(dO + sb, cO + o, np);
+        cp_async_at<0>(dR + sb, cR + o, np);
     };
     const int i = (int)(p % I), j = (int)(p / I);
     const bool live = p < s2;
@@ -1304,8 +1315,10 @@ __device__ __forceinline__ void step3d_uv_pipe_body(const Geo<R> &g, float *__re
     // group g every thread has finished group g-1, whose slots (kPipeDepth is a multiple of the
     // group) are refilled with group g+2, so two groups are in flight while one is eliminated
     static_assert(kPipeDepth % kPipeGroup == 0, "levels are consumed in whole groups");
+    int cslot = 0;   // slot of the next level consumed (levels are consumed in order)
     auto level = [&](int k) {
-        const float *sl = ring + (k % kPipeDepth) * kPipeSlot;
+        const float *sl = ring + cslot * kPipeSlot;
+        cslot = cslot + 1 == kPipeDepth ? 0 : cslot + 1;
         const float *sHz = sl, *sAk = sl + kRow, *sZr = sl + 2 * kRow;
         const float *sO = sl + 3 * kRow + sys * kPipeCols, *sR = sl + 3 * kRow + (2 + sys) * kPipeCols;
         const float hz = (sHz[col + 1] + sHz[qi]) * 0.5f;
@@ -1331,7 +1344,7 @@ __device__ __forceinline__ void step3d_uv_pipe_body(const Geo<R> &g, float *__re
             Rs += (double)rr;
         }
         cc[k * kPipeThreads] = ccp;
-        outc[(long)k * s2] = ddp;
+        outc[k * s2i] = ddp;
         fc = gk;
         H += (double)hz;
         O += (double)(ok * hz);
@@ -1355,16 +1368,16 @@ __device__ __forceinline__ void step3d_uv_pipe_body(const Geo<R> &g, float *__re
         const double dbar = sys == 0 ? DU[p] / (double)g.on_u[p] : DV[p] / (double)g.om_v[p];
         const float sub = (float)((O - dbar) / H);
         float x = ddp;
-        outc[(long)(N - 1) * s2] = x - sub;
+        outc[(N - 1) * s2i] = x - sub;
         for (int k = N - 2; k >= 0; k -= kBackChunk) {
             float dv[kBackChunk];   // the chunk's d' first (independent loads), then the chain
 #pragma unroll
-            for (int h = 0; h < kBackChunk; ++h) dv[h] = k - h >= 0 ? outc[(long)(k - h) * s2] : 0.f;
+            for (int h = 0; h < kBackChunk; ++h) dv[h] = k - h >= 0 ? outc[(k - h) * s2i] : 0.f;
 #pragma unroll
             for (int h = 0; h < kBackChunk; ++h) {
                 if (k - h >= 0) {
                     x = dv[h] - cc[(k - h) * kPipeThreads] * x;
-                    outc[(long)(k - h) * s2] = x - sub;
+                    outc[(k - h) * s2i] = x - sub;
                 }
             }
         }
@@ -1698,7 +1711,7 @@ __global__ void __launch_bounds__(kPipeThreads) k_step3d_uv_pipe(
                         tmpU, tmpV, cff, lambda, Dt, do_bc, bcval, (long)blockIdx.x);
 }
 template <typename R>
-__global__ void __launch_bounds__(kPipeThreads) kb_step3d_uv_pipe(
+__global__ void __launch_bounds__(kPipeThreads, 5) kb_step3d_uv_pipe(
     const Member<R> *mt, const int2 *bm, float *__restrict__ u, float *__restrict__ v, const float *__restrict__ ru, const float *__restrict__ rv,
     float *__restrict__ ubar_t1, float *__restrict__ vbar_t1, float *__restrict__ ubar_t2, float *__restrict__ vbar_t2, const float *__restrict__ Hz,
     const float *__restrict__ Akv, const float *__restrict__ z_r, const double *__restrict__ DU, const double *__restrict__ DV, const float *tmpU,
@@ -1928,17 +1941,21 @@ cudaError_t Ops<R>::step3d_uv(const sf_ctx *c, R *u, R *v, const R *ru, const R 
             if (e != cudaSuccess) return e;
             attr_set[dev] = true;
         }
-        if (c->nmem > 1) {
+        // the pipelined form addresses a field with 32-bit element offsets
+        const bool fits = (long)(kNMax + 1) * c->s2 < (1L << 31);
+        if (fits && c->nmem > 1) {
             kb_step3d_uv_pipe<float><<<c->nbm_pipe, kPipeThreads, pipe_smem_bytes(c->maxN), s>>>(
                 mt<R>(c), c->bm_pipe, u, v, ru, rv, ubar_t1, vbar_t1, ubar_t2, vbar_t2, Hz, Akv, z_r,
                 DU, DV, tmpU, tmpV, (float)cff, (float)lambda, (float)Dt, do_bc, (float)bcval);
             return cudaGetLastError();
         }
-        k_step3d_uv_pipe<float><<<blocks_for(c->s2, kPipeCols), kPipeThreads, pipe_smem_bytes(c->N),
-                                  s>>>(geo(c), u, v, ru, rv, ubar_t1, vbar_t1, ubar_t2, vbar_t2,
-                                       Hz, Akv, z_r, DU, DV, tmpU, tmpV, (float)cff,
-                                       (float)lambda, (float)Dt, do_bc, (float)bcval);
-        return cudaGetLastError();
+        if (fits) {
+            k_step3d_uv_pipe<float><<<blocks_for(c->s2, kPipeCols), kPipeThreads,
+                                      pipe_smem_bytes(c->N), s>>>(
+                geo(c), u, v, ru, rv, ubar_t1, vbar_t1, ubar_t2, vbar_t2, Hz, Akv, z_r, DU, DV,
+                tmpU, tmpV, (float)cff, (float)lambda, (float)Dt, do_bc, (float)bcval);
+            return cudaGetLastError();
+        }
     }
     if (c->nmem > 1) {
         kb_step3d_uv<R><<<c->nbm_128, B, 0, s>>>(mt<R>(c), c->bm_128, u, v, ru, rv, ubar_t1, vbar_t1,
