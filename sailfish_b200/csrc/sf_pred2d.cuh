@@ -3,10 +3,10 @@
 // (nonlinear/step2d.py:23-81 with the kernels of mod_cppkernels.cpp:13-186), replacing four
 // launches whose intermediate fields each went through DRAM.
 //
-// A block owns a tile of 32 x 16 rho points (32 x 8 threads, two rows each).  Phase 1
-// computes the predicted zeta on the tile and on a halo of one row (south) and one column
-// (west) into shared memory; phase 2 computes the momentum right-hand side and the
-// predicted ubar/vbar from it.  Interior points with two cells of margin (the "deep" region,
+// A block owns a tile of 31 x 15 rho points.  Phase 1 computes the predicted zeta on the tile
+// and on a halo of one row (south) and one column (west) into shared memory, 32 x 16 nodes on
+// 32 x 8 threads (two rows each: every warp does the same work); phase 2 computes the momentum
+// right-hand side and the predicted ubar/vbar of the tile's nodes from it.  Interior points with two cells of margin (the "deep" region,
 // 2 <= i <= I-3, 2 <= j <= J-3) hold no boundary destination, so they take the fast path.
 // Points of the outer two-cell ring evaluate everything as pure functions of the step's inputs:
 // a field's value after its boundary program at node x is, by the program's gather semantics
@@ -25,7 +25,9 @@
 
 namespace sf {
 
-constexpr int kPredTX = 32, kPredTY = 16;   // tile (nodes); 32 x 8 threads, two rows each
+// A tile of 31 x 15 nodes; its block of 32 x 8 threads stages the tile with its south halo row
+// and west halo column (32 x 16 nodes), two staged rows per thread.
+constexpr int kPredTX = 31, kPredTY = 15;
 
 template <typename R>
 struct PredArgs {
@@ -326,10 +328,11 @@ __device__ __forceinline__ long prd_ring_node(int e, int I, int J) {
 }
 
 // The first `ring_blocks` blocks take one ring node per thread through the pure functions;
-// the others own tiles of 32 x 16 nodes, lane tx taking column i0+tx of rows j0+ty and
-// j0+ty+8, so every load of a warp is 32 consecutive nodes of one row.  A tile block fills
-// its shared zeta_t2 for ring nodes too (the deep nodes next to the ring read them) but
-// leaves their outputs to the ring blocks.
+// the others own tiles of 31 x 15 nodes, lane tx taking column i0-1+tx of the staged rows
+// j0-1+ty and j0-1+ty+8 (lane 0 the west halo column, row 0 the south halo row), so every
+// load of a warp is 32 consecutive nodes of one row.  A tile block fills its shared zeta_t2 for
+// halo and ring nodes too (the deep nodes next to them read them) but writes only its own
+// nodes' outputs, and leaves the ring nodes' outputs to the ring blocks.
 __host__ __device__ __forceinline__ bool prd_inner_tile(int i0, int j0, int I, int J) {
     return i0 >= 3 && j0 >= 3 && i0 + kPredTX + 2 <= I && j0 + kPredTY + 2 <= J;
 }
@@ -362,45 +365,39 @@ __global__ void __launch_bounds__(256, 5) k_pred2d(const __grid_constant__ PredA
         const int tb = bid - ring_blocks;
         i0 = (tb % tiles_x) * kPredTX;
         j0 = (tb / tiles_x) * kPredTY;
-        const int i = i0 + tx;
+        const int i = i0 - 1 + tx;   // staged column tx (0: the west halo)
         // ---- phase 1: zeta_t2 (after zetabc) on the tile and its south/west halo ------------
-        PrdNode<R> kept[kPredTY / 8];   // a deep node's inputs, for phase 2
+        PrdNode<R> kept[2];   // a deep node's inputs, for phase 2
 #pragma unroll
-        for (int h = 0; h < kPredTY; h += 8) {
-            const int j = j0 + ty + h;
-            if (i < I && j < J) {
+        for (int h = 0; h < 16; h += 8) {
+            const int r = ty + h;   // staged row (0: the south halo)
+            const int j = j0 - 1 + r;
+            if (i >= 0 && j >= 0 && i < I && j < J) {
                 const long x = (long)j * I + i;
                 R z;
                 if (prd_deep(i, j, I, J)) {
-                    const R r = prd_rz_keep(a, x, kept[h / 8]);
-                    z = kept[h / 8].z0p + a.Dt * r;
-                    a.rz[x] = r;
-                    a.z2[x] = z;
+                    const R rz = prd_rz_keep(a, x, kept[h / 8]);
+                    z = kept[h / 8].z0p + a.Dt * rz;
+                    if (tx >= 1 && r >= 1) {   // the tile's own node (a halo node is its tile's)
+                        a.rz[x] = rz;
+                        a.z2[x] = z;
+                    }
                 } else {
                     z = prd_z2b(a, x);
                 }
-                sZ[ty + h + 1][tx + 1] = z;
+                sZ[r][tx] = z;
             }
         }
-        if (ty == 0 && j0 >= 1 && i < I) {   // south halo row
-            const long x = (long)(j0 - 1) * I + i;
-            sZ[0][tx + 1] = prd_deep(i, j0 - 1, I, J) ? a.z0[x] + a.Dt * prd_rz_deep(a, x) : prd_z2b(a, x);
-        }
-        if (ty == 1 && tx < kPredTY && i0 >= 1 && j0 + tx < J) {   // west halo column
-            const long x = (long)(j0 + tx) * I + i0 - 1;
-            sZ[tx + 1][0] = prd_deep(i0 - 1, j0 + tx, I, J) ? a.z0[x] + a.Dt * prd_rz_deep(a, x)
-                                                              : prd_z2b(a, x);
-        }
         __syncthreads();
-        // ---- phase 2: momentum of the deep nodes ---------------------------------------------
+        // ---- phase 2: momentum of the tile's deep nodes ----------------------------------------
 #pragma unroll
-        for (int h = 0; h < kPredTY; h += 8) {
-            const int j = j0 + ty + h;
-            if (i < I && j < J && prd_deep(i, j, I, J)) {
+        for (int h = 0; h < 16; h += 8) {
+            const int r = ty + h;
+            const int j = j0 - 1 + r;
+            if (tx >= 1 && r >= 1 && i < I && j < J && prd_deep(i, j, I, J)) {
                 const int q = j * I + i;
                 const bool pd = q - fdiv(q, g.dJ) * J != 0 && q >= J;   // q % J != 0 (szJ)
-                const int r = ty + h + 1, c = tx + 1;
-                prd_deep_mom_kept(a, (long)q, pd, sZ[r][c], sZ[r][c - 1], sZ[r - 1][c], kept[h / 8]);
+                prd_deep_mom_kept(a, (long)q, pd, sZ[r][tx], sZ[r][tx - 1], sZ[r - 1][tx], kept[h / 8]);
             }
         }
         if (prd_inner_tile(i0, j0, I, J)) return;   // uniform over the block: no barrier below
