@@ -209,51 +209,6 @@ __device__ __forceinline__ bool prd_deep(int i, int j, int I, int J) {
     return i >= 2 && i <= I - 3 && j >= 2 && j <= J - 3;
 }
 
-// computeZetaRHS at a deep node through per-node base pointers (the neighbours at constant
-// offsets), as prd_rz.
-template <typename R>
-__device__ __forceinline__ R prd_rz_deep(const PredArgs<R> &a, long x) {
-    const Geo<R> &g = a.g;
-    const int I = g.I;
-    const R *z = a.z1 + x, *h = g.h + x, *ub = a.ub1 + x, *vb = a.vb1 + x, *ou = g.on_u + x,
-            *ov = g.om_v + x;
-    const R *zN = z + I, *zS = z - I, *hN = h + I, *hS = h - I;
-    const R Dp = z[0] + h[0], Dw = z[-1] + h[-1], De = z[1] + h[1];
-    const R Ds = zS[0] + hS[0], Dn = zN[0] + hN[0];
-    const R DUp = ub[0] * ((Dp + Dw) * R(0.5));
-    const R DUe = ub[1] * ((De + Dp) * R(0.5));
-    const R DVp = vb[0] * ((Dp + Ds) * R(0.5));
-    const R DVn = vb[I] * ((Dn + Dp) * R(0.5));
-    return (((DUe * ou[1] - DUp * ou[0]) + (DVn * ov[I] - DVp * ov[0])) * g.pm[x]) * g.pn[x];
-}
-
-// The fast path of a deep node: momentum from the tile's zeta_t2 at x, x-1 and x-I.
-template <typename R>
-__device__ __forceinline__ void prd_deep_mom(const PredArgs<R> &a, long x, bool pd, R zp, R zw,
-                                             R zs) {
-    const Geo<R> &g = a.g;
-    const int I = g.I;
-    const R *h = g.h + x, *z0 = a.z0 + x, *z1 = a.z1 + x;
-    const R hp = h[0], hw = h[-1], hs = h[-I];
-    const R gp = a.w1 * zp + a.w * z0[0];
-    const R gw = a.w1 * zw + a.w * z0[-1];
-    const R gs = a.w1 * zs + a.w * z0[-I];
-    const R ru = (a.grav * g.on_u[x]) * (((hp + hw) * R(0.5)) * (gp - gw) + R(0.5) * (gp * gp - gw * gw));
-    const R rv = (a.grav * g.om_v[x]) * (((hp + hs) * R(0.5)) * (gp - gs) + R(0.5) * (gp * gp - gs * gs));
-    a.ru[x] = ru;
-    a.rv[x] = rv;
-    if (pd) {
-        const R D1p = z1[0] + hp, D2p = zp + hp;
-        const R D1U = (D1p + (z1[-1] + hw)) * R(0.5);
-        const R D2U = (D2p + (zw + hw)) * R(0.5);
-        const R D1V = (D1p + (z1[-I] + hs)) * R(0.5);
-        const R D2V = (D2p + (zs + hs)) * R(0.5);
-        const R pm = g.pm[x], pn = g.pn[x];
-        a.ub2[x] = ddiv(a.ub1[x] * D1U + ((a.Dt * ru) * pm) * pn, D2U);
-        a.vb2[x] = ddiv(a.vb1[x] * D1V + ((a.Dt * rv) * pm) * pn, D2V);
-    }
-}
-
 // A deep node's inputs that both phases use, read once in phase 1 and kept in registers across
 // the block's barrier: zeta_t1 and h at the node and its west and south neighbours, ubar_t1,
 // vbar_t1, the metrics and zeta_t0 at the node.
@@ -262,7 +217,8 @@ struct PrdNode {
     R z1p, z1w, z1s, hp, hw, hs, ub, vb, pm, pn, ou, ov, z0p;
 };
 
-// prd_rz_deep, filling the node's kept inputs (the same operations in the same order).
+// computeZetaRHS at a deep node (the operations of prd_rz in its order) through per-node base
+// pointers, the neighbours at constant offsets, filling the node's kept inputs.
 template <typename R>
 __device__ __forceinline__ R prd_rz_keep(const PredArgs<R> &a, long x, PrdNode<R> &n) {
     const Geo<R> &g = a.g;
@@ -291,7 +247,8 @@ __device__ __forceinline__ R prd_rz_keep(const PredArgs<R> &a, long x, PrdNode<R
     return (((DUe * ou[1] - DUp * n.ou) + (DVn * ov[I] - DVp * n.ov)) * n.pm) * n.pn;
 }
 
-// prd_deep_mom from the node's kept inputs (the same operations in the same order).
+// The fast path of a deep node: computeMomentumRHSPred + computeMomentumPred (the operations of
+// prd_mom in its order) from the tile's zeta_t2 at x, x-1 and x-I and the node's kept inputs.
 template <typename R>
 __device__ __forceinline__ void prd_deep_mom_kept(const PredArgs<R> &a, long x, bool pd, R zp,
                                                   R zw, R zs, const PrdNode<R> &n) {
