@@ -16,10 +16,11 @@
 // waits for another.  Destinations are written with their final values, except those of
 // chained entries (a destination that is also a source, e.g. at corners), whose old content
 // other blocks may still read: block 0 evaluates them first (into a small buffer, while every
-// old content is intact) and the last block to finish copies them into place.  Old contents are read only
-// where a node off the deep region is evaluated, i.e. by the ring blocks and by the tiles whose
-// nodes or halo reach the outer ring ("edge" blocks); tiles wholly inside (tile and halo deep)
-// read only the step's inputs, so they leave without taking part in the count.
+// old content is intact) and the last "edge" block to finish copies them into place.  Old
+// contents are read only where a node off the deep region is evaluated, i.e. by the ring blocks
+// and by the tiles whose nodes or halo reach the outer ring (the edge blocks); tiles wholly
+// inside (tile and halo deep) read only the step's inputs, so they leave without taking part
+// in the count.
 #pragma once
 #include "sf_internal.h"
 
@@ -360,10 +361,10 @@ __global__ void __launch_bounds__(256, 5) k_pred2d(const __grid_constant__ PredA
         if (prd_inner_tile(i0, j0, I, J)) return;   // uniform over the block: no barrier below
     }
 
-    // ---- chained destinations: the last block, after every block's reads -------------------
+    // ---- chained destinations: the last edge block, after every edge block's reads --------
     // A thread reaches the barrier only after each of its loads has returned (every loaded
     // value feeds a store or a branch before it), so once a block has counted itself, none of
-    // its reads of old contents is pending and the last block may overwrite them.
+    // its reads of old contents is pending and the last edge block may overwrite them.
     __syncthreads();
     if (tid == 0) s_last = atomicAdd(a.counter, 1) == edge_blocks - 1;
     __syncthreads();
