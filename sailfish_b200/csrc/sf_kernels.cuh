@@ -996,6 +996,10 @@ __device__ __forceinline__ void set_depth_body(const Geo<R> &g, const double *__
     const long s2 = g.s2;
     const int N = g.N;
     const double hc = g.hc, h = g.hd[p], zt = Zt[p];
+    // The FP32 form, whose outputs are rounded to FP32, multiplies by the column's reciprocal
+    // depth instead of dividing at every level; FP64 divides as the reference does.
+    constexpr bool recip = sizeof(R) == 4;
+    const double ih = recip ? 1.0 / h : 0.0, ihc = recip ? 1.0 / (hc + h) : 0.0;
     double zprev = 0.0;
     for (int K = 0; K <= N; ++K) {
         double zw;
@@ -1004,11 +1008,12 @@ __device__ __forceinline__ void set_depth_body(const Geo<R> &g, const double *__
         } else if (g.Vtransform == 1) {
             const double z_r0 = hc * (g.sc_r[K] - g.Cs_r[K]) + g.Cs_r[K] * h;
             const double z_w0 = hc * (g.sc_w[K] - g.Cs_w[K]) + g.Cs_w[K] * h;
-            zw = z_w0 + zt * (1.0 + z_w0 / h);
-            z_r[(long)K * s2 + p] = (R)(z_r0 + zt * (1.0 + z_r0 / h));
+            zw = z_w0 + zt * (1.0 + (recip ? z_w0 * ih : z_w0 / h));
+            z_r[(long)K * s2 + p] = (R)(z_r0 + zt * (1.0 + (recip ? z_r0 * ih : z_r0 / h)));
         } else {
-            const double cff2_r = (hc * g.sc_r[K] + g.Cs_r[K] * h) / (hc + h);
-            const double cff2_w = (hc * g.sc_w[K] + g.Cs_w[K] * h) / (hc + h);
+            const double nr = hc * g.sc_r[K] + g.Cs_r[K] * h, nw = hc * g.sc_w[K] + g.Cs_w[K] * h;
+            const double cff2_r = recip ? nr * ihc : nr / (hc + h);
+            const double cff2_w = recip ? nw * ihc : nw / (hc + h);
             zw = zt + (zt + h) * cff2_w;
             z_r[(long)K * s2 + p] = (R)(zt + (zt + h) * cff2_r);
         }
