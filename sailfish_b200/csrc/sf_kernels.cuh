@@ -475,34 +475,47 @@ __device__ __forceinline__ R bc_value(const R *f, int s, R val) {
 template <typename R>
 __global__ void __launch_bounds__(256) k_bc_apply(BcProgram p1, R *f1, BcProgram p2, R *f2, R val0,
                                                   const double *valp) {
-    pdl_enter();
-    const R val = valp ? (R)valp[0] : val0;   // time-dependent value from the device (graphs)
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    // The programs' index lists are the context's, uploaded synchronously at set-up: they are
+    // read before waiting for the preceding kernel, whose outputs (the field values, and the
+    // clamped value that a kernel writes before a graph replay) are read only after the wait.
     const long t = tid_flat();
+    int dst = -1, src = 0;
+    R *fi = f1;
     if (t < p1.n) {
-        f1[p1.dst[t]] = bc_value(f1, p1.src[t], val);
+        dst = p1.dst[t];
+        src = p1.src[t];
     } else if (t < (long)p1.n + p2.n) {
         const long k = t - p1.n;
-        f2[p2.dst[k]] = bc_value(f2, p2.src[k], val);
+        dst = p2.dst[k];
+        src = p2.src[k];
+        fi = f2;
     }
     // chained entries: group g (one per member, at most 32 entries) by warp g of the grid, one
     // entry per lane; every lane reads, the warp synchronises, then every lane writes, so all
     // reads come before all writes.  (Independent entries neither read nor write a node of a
     // chained group, so the two parts need no ordering.)
     const long w = t >> 5;
-    if (w < (long)p1.ngr + p2.ngr) {   // uniform across the warp
-        const bool first = w < p1.ngr;
+    const bool grp = w < (long)p1.ngr + p2.ngr;   // uniform across the warp
+    const bool first = w < p1.ngr;
+    R *fc = first ? f1 : f2;
+    int dc = -1, sc = 0;
+    if (grp) {
         const BcProgram &pp = first ? p1 : p2;
-        R *f = first ? f1 : f2;
         const int g = (int)(first ? w : w - p1.ngr), lane = (int)(t & 31);
         const int a = pp.gofs[g], b = pp.gofs[g + 1];
-        int d = -1;
-        R x = R(0);
         if (lane < b - a) {
-            d = pp.dst_ch[a + lane];
-            x = bc_value(f, pp.src_ch[a + lane], val);
+            dc = pp.dst_ch[a + lane];
+            sc = pp.src_ch[a + lane];
         }
+    }
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    const R val = valp ? (R)valp[0] : val0;   // time-dependent value from the device (graphs)
+    if (dst >= 0) fi[dst] = bc_value(fi, src, val);
+    if (grp) {
+        const R x = dc >= 0 ? bc_value(fc, sc, val) : R(0);
         __syncwarp();
-        if (d >= 0) f[d] = x;
+        if (dc >= 0) fc[dc] = x;
     }
 }
 
