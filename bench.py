@@ -62,6 +62,35 @@ def phase_pass(m, steps, hook, phases):
     return {k: float(np.mean([a.elapsed_time(b) for a, b in v])) for k, v in phases.items()}
 
 
+def time_pred2d(m, n):
+    """Average device time (ms) of one launch of the fused barotropic predictor (k_pred2d),
+    which runs once per barotropic substep inside the loop's graph: n launches through
+    sf_step2d_predictor on the model's own slots, each between its own pair of CUDA events on
+    the launching stream.  None where the context has no fused predictor.  The model's fields
+    are overwritten (run it after the timed region)."""
+    import ctypes
+    import torch
+    from sailfish_b200._lib import lib, check
+    if not lib.sf_ctx_fused_available(m.ctx.ptr):
+        return None
+    s = m.state2d()
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    stream = torch.cuda.current_stream()
+    evs = []
+    for k in range(n):
+        for name in m.NAMES2:                      # cycleTimes2D on the local slot copy
+            a = getattr(s, name)
+            a[0], a[1], a[2] = a[1], a[2], a[0]
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        check(lib.sf_step2d_predictor(m.ctx.ptr, ctypes.byref(s), m.dtfast, 0.0, 0, st),
+              "sf_step2d_predictor")
+        e1.record(stream)
+        evs.append((e0, e1))
+    torch.cuda.synchronize()
+    return float(np.mean([a.elapsed_time(b) for a, b in evs[1:]]))
+
+
 def launches_per_step(m, mixing):
     """This package's kernel launches in one baroclinic step of Model.step: set_maxflux/omega,
     rhs3d, set_depth, step3d_uv; per barotropic substep the fused predictor (or its four
@@ -103,61 +132,77 @@ def peaks():
 # -------------------------------------------------------------------------------------------
 # CPU (reference) measurement
 # -------------------------------------------------------------------------------------------
-def reference_cpu(config, nsteps, omp):
-    """The reference's kernels on the host; returns (cell-steps/s, cores, sample text)."""
+def reference_cpu(config, steps, warmup, omp, shrink=1):
+    """The reference's own CPU path of the step: its kernel sources host-compiled for this
+    machine (oracle/_ref, g++ -O3 -march=native, OpenMP over the flat thread index) driven in
+    its main3d order (main3d.py:118-324), on the basin set up by the oracle's restatement of
+    the reference's host routines (nothing from the package).  shrink > 1 runs the same recipe
+    on a (Lm/shrink) x (Mm/shrink) sub-basin (same N, dx, dt, ndtfast) as a bounded sample.
+    Returns (cell-steps/s, cores, sample text, config dict)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import build_ref
     import oracle as orc
     import ref_driver
-    from sailfish_b200 import configs, host
-    if not ref_driver.available():
-        raise RuntimeError("oracle/_ref is not built")
-    full = configs.CONFIGS[config]()
-    g = full["grid"]
-    # bounded sample: the same recipe on a quarter-by-quarter sub-basin (same N, dx, dt)
-    sub = configs.basin(max(g.L - 1, 8) // 8, max(g.M - 1, 8) // 8, g.N, g.pm.flat[0] ** -1,
-                        [(1.0 / 3.0, 0.6), (2.0 / 3.0, 0.6)], full["dt"], full["ndtfast"])
-    sg, B = sub["grid"], sub["boundary"]
-    og = orc.Grid(sg.L, sg.M, sg.N, sg.h, sg.pm, sg.pn, sg.on_u, sg.om_v, sg.fomn, sg.sc_r, sg.sc_w,
-                  sg.Cs_r, sg.Cs_w, sg.hc, sg.Vtransform)
-    bd = {}
-    for name in ("zetaBC", "ubarBC", "vbarBC", "uvelBC", "vvelBC"):
-        bc = getattr(B, name)
-        for fld in ("bcIdx", "bcIdx1", "bcIdx2", "bcIdxFieldIdx2", "bcIdxFieldType", "LBC"):
-            bd["%s_%s" % (name, fld)] = getattr(bc, fld)
-    for fld in ("zetaClosedOrGradientBCIdx1", "zetaClosedOrGradientBCIdx2", "zetaClampedBCIdx1",
-                "ubarClosedBCIdx1", "vbarClosedBCIdx1", "ubarClampedBCIdx1", "vbarClampedBCIdx1",
-                "ubarGradientBCIdx1", "ubarGradientBCIdx2", "vbarGradientBCIdx1", "vbarGradientBCIdx2"):
-        bd[fld] = getattr(B, fld)
+    import ref_setup
+    if config not in ref_setup.BASINS:
+        raise RuntimeError("no reference set-up for workload %s" % config)
+    how = build_ref.build_native()
+    b = ref_setup.basin(config, shrink)
+    og = orc.Grid(b["L"], b["M"], b["N"], b["h"], b["pm"], b["pn"], b["on_u"], b["om_v"],
+                  b["fomn"], b["sc_r"], b["sc_w"], b["Cs_r"], b["Cs_w"], b["hc"], b["Vtransform"])
     O = orc.Ocean(og)
-    nfast, w1, w2 = host.set_weights(sub["ndtfast"])
-    ct = orc.CompTimes(sub["dt"], sub["ndtfast"], nfast, w1, w2)
+    nfast, w1, w2 = ref_setup.weights(b["ndtfast"])
+    ct = orc.CompTimes(b["dt"], b["ndtfast"], nfast, w1, w2)
+    K = ref_driver.RefKernels(omp, "_native")
+    marks = []
     with _StdoutToStderr():
-        ref_driver.main3d(og, orc.Boundary(bd), O, ct, 1, omp=omp)      # warm-up
-        t0 = time.perf_counter()
-        ref_driver.main3d(og, orc.Boundary(bd), O, ct, nsteps, omp=omp)
-        dt = time.perf_counter() - t0
-    cells = (sg.L - 1) * (sg.M - 1) * sg.N
-    sample = ("reference kernels (oracle/_ref, g++ -O2) in main3d order on a %dx%dx%d sub-basin of "
-              "%s (same recipe, dt, ndtfast), %d baroclinic steps, %d OpenMP threads"
-              % (sg.L - 1, sg.M - 1, sg.N, config, nsteps, omp))
-    return cells * nsteps / dt, omp, sample
+        ref_driver.main3d(og, orc.Boundary(b["lists"]), O, ct, warmup + steps, kernels=K,
+                          step_marks=marks)
+    dt = marks[warmup + steps - 1] - marks[warmup - 1] if warmup > 0 else marks[-1] - marks[0]
+    n_timed = steps if warmup > 0 else steps - 1
+    cells = (b["L"] - 1) * (b["M"] - 1) * b["N"]
+    sample = ("the reference's kernels (%s) in main3d order on %s%s, %d timed baroclinic steps "
+              "after %d warm-up, %d OpenMP threads"
+              % (how, config, "" if shrink == 1 else " shrunk to %dx%dx%d (same recipe, dx, dt, "
+                 "ndtfast)" % (b["L"] - 1, b["M"] - 1, b["N"]), n_timed, warmup, omp))
+    cfg = {"workload": config, "Lm": b["L"] - 1, "Mm": b["M"] - 1, "N": b["N"], "cells": cells,
+           "dt": b["dt"], "ndtfast": b["ndtfast"], "barotropic_substeps": nfast + 1,
+           "semantics": "reference main3d", "initial_state": "rest, closed walls",
+           "vertical_mixing": "AKv constant (the reference's step has no mixing update)"}
+    return cells * n_timed / dt, omp, sample, cfg
 
 
 # -------------------------------------------------------------------------------------------
 # clocks during the timed region
 # -------------------------------------------------------------------------------------------
+def gpu_id(index):
+    """An nvidia-smi -i identifier for torch's CUDA device `index`: its UUID (nvidia-smi
+    numbers GPUs in PCI order and ignores CUDA_VISIBLE_DEVICES, so the ordinal can name another
+    GPU), else its PCI bus id, else the ordinal."""
+    import torch
+    p = torch.cuda.get_device_properties(index)
+    uuid = str(getattr(p, "uuid", "") or "")
+    if uuid:
+        return uuid if uuid.startswith(("GPU-", "MIG-")) else "GPU-" + uuid
+    bus = getattr(p, "pci_bus_id", None)
+    if bus is not None:
+        return "%08x:%02x:%02x.0" % (getattr(p, "pci_domain_id", 0), bus,
+                                     getattr(p, "pci_device_id", 0))
+    return str(index)
+
+
 class Clocks:
     Q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
 
     def __init__(self, index):
-        self.index, self.rows, self.proc = index, [], None
+        self.index, self.rows, self.proc = gpu_id(index), [], None
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                ["nvidia-smi", "-i", self.index, "--query-gpu=" + self.Q,
                  "--format=csv,noheader,nounits", "-lms", "20"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
@@ -198,6 +243,9 @@ def algorithmic_bytes(grid, esize):
         "k_step3d_uv": esize * (9 * N) * s2 + 16 * s2,          # u,v,ru,rv,Hz,Akv,z_r -> u,v; DU,DV
         "k_maxflux_omega": esize * (4 * N + 3 * (N + 1)) * s2,  # u,v,Hz,z_w -> Huon,Hvom,W
         "k_set_depth": esize * (3 * N + 1) * s2 + 16 * s2,      # Zt,h -> z_w,z_r,Hz
+        # fused barotropic predictor, per launch: zeta_t0, zeta_t1, ubar_t1, vbar_t1, h, pm,
+        # pn, on_u, om_v -> zeta_t2, rzeta_t1, rubar_t1, rvbar_t1, ubar_t2, vbar_t2
+        "k_pred2d": esize * 15 * s2,
         # the learned closure (k_closure + GLS on its fallback columns), per interior column:
         # u, v, z_r (N levels), bvf (N-1 interior W levels), sustr, svstr, h -> Akv, Akt (N-1)
         "closure": (esize * (4 * N - 1) + 3 * esize + 2 * esize * (N - 1)) * (grid.L - 1) * (grid.M - 1),
@@ -539,10 +587,16 @@ def run_ours(args, rank, world):
     bi = (hu.numel() + hv.numel()) * hu.element_size()
     bo = hz.numel() * hz.element_size()
 
+    # per-launch times and launches per step of the kernels with algorithmic byte counts; the
+    # roofline is reported for the kernel that takes the most time per step
     ab = algorithmic_bytes(grid, esize)
-    dom = max((k for k in per_phase if k in ab), key=lambda k: per_phase[k])
+    per_launch = {k: (per_phase[k], 1) for k in per_phase if k in ab}
+    t_pred = time_pred2d(m, m.nfast + 1)
+    if t_pred is not None:
+        per_launch["k_pred2d"] = (t_pred, m.nfast + 1)
+    dom = max(per_launch, key=lambda k: per_launch[k][0] * per_launch[k][1])
     peak, kind = peaks()
-    achieved = ab[dom] / (per_phase[dom] * 1e-3) / 1e9
+    achieved = ab[dom] / (per_launch[dom][0] * 1e-3) / 1e9
     value = cells * args.steps * world / (ms * 1e-3)
     # launches per baroclinic step, plus one omega at the end of the timed call
     per_step = launches_per_step(m, mixing)
@@ -566,8 +620,10 @@ def run_ours(args, rank, world):
                    "rhs3d_tile": str(autotune.TILES[m.rhs_tile]),
                    "rhs3d_tile_autotune_ms": {str(autotune.TILES[k]): v for k, v in tune.items()}},
         "phases_ms": per_phase,
+        "kernel_ms_per_step": {k: t * n for k, (t, n) in per_launch.items()},
         "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_kind": kind,
+                     "launch_ms": per_launch[dom][0], "launches_per_step": per_launch[dom][1],
                      "algorithmic_bytes": ab[dom],
                      "traffic": traffic_per_launch(dom, grid) if args.precision == "fp32" else None,
                      "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum on basin4q "
@@ -590,7 +646,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="basin4")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
-    ap.add_argument("--cpu-steps", type=int, default=40)
+    ap.add_argument("--cpu-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 timing")
     ap.add_argument("--members", type=int, default=256, help="ensemble members (config ensemble)")
@@ -607,14 +663,16 @@ def main():
         if rank != 0:
             return
         try:
-            v, cores, sample = reference_cpu(args.config, max(args.steps, 1), omp)
+            v, cores, sample, cfg = reference_cpu(args.config, max(args.steps, 1), args.warmup,
+                                                  omp)
         except Exception as e:
             print(json.dumps({"impl": "reference", "unavailable": str(e)}))
             return
         print(json.dumps({
             "impl": "reference", "metric": METRIC, "value": v, "unit": "cell-steps/s",
-            "n_gpus": 0, "steps": args.steps, "warmup": 1, "higher_is_better": True,
-            "dtype": "f64", "data": "synthetic", "config": {"workload": args.config},
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": cfg["cells"] / v * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
             "cpu_baseline": {"value": v, "unit": "cell-steps/s", "cores": cores,
                              "kind": "reference", "sample": sample},
             "e2e": {"value": v, "unit": "cell-steps/s", "h2d_bytes_per_step": 0,
@@ -642,7 +700,8 @@ def main():
             out["error_vs_fp64"] = error_vs_fp64()
         if not args.no_cpu_baseline:
             try:
-                v, cores, sample = reference_cpu(args.config, args.cpu_steps, omp)
+                v, cores, sample, _ = reference_cpu(args.config, args.cpu_steps, 1, omp,
+                                                    shrink=4)
                 out["cpu_baseline"] = {"value": v, "unit": "cell-steps/s", "cores": cores,
                                        "kind": "reference", "sample": sample}
             except Exception as e:

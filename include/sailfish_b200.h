@@ -136,7 +136,18 @@ int sf_zetabc(sf_ctx *ctx, void *zeta, sf_stream stream);
 /* barotropicVelocityBC (nonlinear/barotropicVelocityBC.py:7-31, setBC/copyBC of
  * modules/mod_BC.c:6-23); the clamped value is 0.05*sin(0.0002*time2D). */
 int sf_barotropic_velocity_bc(sf_ctx *ctx, void *ubar, void *vbar, double time2D, sf_stream stream);
-/* step2dPredictor (nonlinear/step2d.py:23-81): first_step selects its Forward-Euler branch. */
+/* Blow-up check: scans zeta, ubar, vbar (2D, (M+1)(L+1)) and u, v (3D, (N+1)(M+1)(L+1)) for
+ * NaN, infinities and magnitudes above surface_bound (zeta) or velocity_bound (the
+ * velocities); any argument may be NULL to skip that field.  Synchronises `stream` and returns
+ * SF_ENONFINITE, with the field and the (level, j, i) of its first bad value in
+ * sf_last_error(), or SF_OK.  No counterpart in the reference, whose step has no such check
+ * and runs on into non-finite values (the step that a driver runs every K steps). */
+int sf_check_state(sf_ctx *ctx, const void *zeta, const void *ubar, const void *vbar,
+                   const void *u, const void *v, double surface_bound, double velocity_bound,
+                   sf_stream stream);
+/* step2dPredictor (nonlinear/step2d.py:23-81): first_step selects its Forward-Euler branch.
+ * The leapfrog branch runs as one fused launch where the context allows it
+ * (sf_ctx_fused_available, sf_ctx_set_fused), with the same results as the four launches. */
 int sf_step2d_predictor(sf_ctx *ctx, const sf_state2d *s, double dtfast, double time2D,
                         int first_step, sf_stream stream);
 /* step2dCorrector (nonlinear/step2d.py:84-128), cff1 = weight1[iif-1]. */
@@ -341,9 +352,10 @@ int sf_mlp_backward(const sf_mlp_params *w, int n, const float *X, const float *
  * Its scratch is a fixed 2 MiB device array inside the library, held by every GPU that loads
  * it until the process exits; n <= 2048 rows, larger n is rejected with SF_EINVAL.  The first
  * call on a device looks up that array's device address (cudaGetSymbolAddress), so make it
- * before any stream capture.  All calls share the array and leave their intermediate values
- * in it (every value read is written first by the same call): calls that overlap on the GPU
- * (different streams, or devices sharing nothing but this library) race. */
+ * before any stream capture.  Each device has its own 2 MiB copy of the array; on one device
+ * all calls share it and leave their intermediate values in it (every value read is written
+ * first by the same call), so calls that overlap on the same device (on different streams,
+ * for example) race. */
 int sf_mlp_backward_static(const sf_mlp_params *w, int n, const float *X, const float *acts,
                            const float *pre, const float *dY, float *const *dW, float *const *db,
                            int *err, sf_stream stream);

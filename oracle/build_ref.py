@@ -1,7 +1,8 @@
 """Build recipe for oracle/_ref: the reference's own CUDA kernel sources compiled for the host.
 
 Test infrastructure only (never imported by the product).  It reads the reference
-kernels where they lie (``$SAILFISH_REFERENCE``, default ``/root/reference``):
+kernels where they lie (``$SAILFISH_REFERENCE``, default: a ``reference`` checkout beside the
+repository):
 
     modules/mod_cppkernels.cpp        -> oracle/_ref/libsfref_2d.so
     nonlinear/rhs_kernels.cpp         -> oracle/_ref/libsfref_rhs.so
@@ -26,6 +27,11 @@ moment it is bound; no expression, operand or evaluation order is changed.
 
 Floating-point contraction is disabled (-ffp-contract=off) so that the results are the
 IEEE-754 evaluation of each expression as written, which is what the oracle restates.
+
+``build_native()`` compiles the same generated sources again at ``-O3 -march=native`` (with
+contraction left to the compiler) into ``libsfref_<module>_native.so``, for the timed CPU
+path of the reference on the machine that runs it; it needs only oracle/_ref/src, not the
+reference checkout, so it can run where the benchmark runs.
 """
 import os
 import re
@@ -44,7 +50,8 @@ MODULES = {
 
 
 def reference_root():
-    return os.environ.get("SAILFISH_REFERENCE", "/root/reference")
+    return os.environ.get("SAILFISH_REFERENCE",
+                          os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference"))
 
 
 def preprocess(code):
@@ -59,8 +66,8 @@ def patch_header(code):
     return re.sub(r"^(\s*)(L|R|OType) &(\w+);", r"\1\2 \3;", code, flags=re.M)
 
 
-def lib_path(name):
-    return os.path.join(OUT, "libsfref_%s.so" % name)
+def lib_path(name, suffix=""):
+    return os.path.join(OUT, "libsfref_%s%s.so" % (name, suffix))
 
 
 def build(verbose=False, opt="-O2"):
@@ -99,6 +106,43 @@ def build(verbose=False, opt="-O2"):
             print(" ".join(cmd))
         subprocess.check_call(cmd)
     return True
+
+
+def build_native(verbose=False):
+    """The timed CPU build: the generated sources at -O3 -march=native for this machine's
+    cores (OpenMP over the thread index).  Rebuilt whenever the machine's CPU model differs
+    from the one recorded beside the libraries."""
+    src_dir = os.path.join(OUT, "src")
+    if not all(os.path.exists(os.path.join(src_dir, "%s.cpp" % m)) for m in MODULES):
+        raise RuntimeError("oracle/_ref/src is missing: run oracle/build_ref.py where the "
+                           "reference checkout is present")
+    stamp = os.path.join(OUT, "native_cpu.txt")
+    cpu = _cpu_model()
+    fresh = os.path.exists(stamp) and open(stamp).read() == cpu
+    for name, (_, launcher) in MODULES.items():
+        target = lib_path(name, "_native")
+        if fresh and os.path.exists(target):
+            continue
+        cmd = ["g++", "-std=c++17", "-O3", "-march=native", "-fPIC", "-shared", "-fopenmp", "-w",
+               "-I", HERE, '-DSFREF_SOURCE="%s"' % os.path.join(src_dir, "%s.cpp" % name),
+               os.path.join(HERE, launcher), "-o", target]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.check_call(cmd)
+    with open(stamp, "w") as f:
+        f.write(cpu)
+    return "g++ -O3 -march=native -fopenmp (%s)" % cpu
+
+
+def _cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
 
 if __name__ == "__main__":

@@ -14,6 +14,7 @@ threads, e.g. rhs_kernels.cpp:86-91, then resolve them in no fixed order).
 import ctypes
 import math
 import os
+import time
 
 import numpy as np
 
@@ -42,16 +43,19 @@ SIGS = {
 }
 
 
-def available():
-    return all(os.path.exists(os.path.join(REF, "libsfref_%s.so" % m)) for m in SIGS)
+def available(suffix=""):
+    return all(os.path.exists(os.path.join(REF, "libsfref_%s%s.so" % (m, suffix))) for m in SIGS)
 
 
 class RefKernels:
-    def __init__(self, omp=1):
+    """The reference's kernels from oracle/_ref; suffix "" is the pinned build (-O2, no
+    contraction), "_native" the timed build (build_ref.build_native)."""
+
+    def __init__(self, omp=1, suffix=""):
         self.omp = int(omp)
         self.libs = {}
         for mod, fns in SIGS.items():
-            lib = ctypes.CDLL(os.path.join(REF, "libsfref_%s.so" % mod))
+            lib = ctypes.CDLL(os.path.join(REF, "libsfref_%s%s.so" % (mod, suffix)))
             for name, args in fns.items():
                 f = getattr(lib, "sfref_" + name)
                 f.argtypes = [_l, _i] + args
@@ -138,10 +142,11 @@ def main2d(grid, B, O, ct, nsteps, omp=1):
         corr()
 
 
-def main3d(grid, B, O, ct, nsteps, omp=1, lam=1.0):
+def main3d(grid, B, O, ct, nsteps, omp=1, lam=1.0, suffix="", kernels=None, step_marks=None):
     """nonlinear/main3d.py:25-326 with the reference's kernels (step2d.py, zetabc.py,
-    barotropicVelocityBC.py, rhs.py orchestration restated), on oracle.Grid/Ocean/CompTimes."""
-    K = RefKernels(omp)
+    barotropicVelocityBC.py, rhs.py orchestration restated), on oracle.Grid/Ocean/CompTimes.
+    `step_marks`, if a list, receives time.perf_counter() at the end of every step."""
+    K = kernels or RefKernels(omp, suffix)
     N, J, I = grid.N, grid.J, grid.I
     s2 = grid.s2
     nt = (s2 // 512 + 1) * 512          # grsz*bksz and grsz*GPUMUL*(bksz//GPUMUL)
@@ -197,3 +202,5 @@ def main3d(grid, B, O, ct, nsteps, omp=1, lam=1.0):
         K("step3d", "omega", nt, P(O.W), P(O.t3("u")), P(O.t3("v")), P(O.Huon), P(O.Hvom),
           P(grid.z_w), P(BC))
         ct.next3d()
+        if step_marks is not None:
+            step_marks.append(time.perf_counter())

@@ -76,6 +76,7 @@ SIGNATURES = {
     "sf_maxflux_omega": [_vp] * 12,
     "sf_set_zeta": [_vp] * 5,
     "sf_set_depth": [_vp] * 6,
+    "sf_check_state": [_vp] * 6 + [_d, _d, _vp],
     "sf_step3d_uv": [_vp] * 16 + [_i, _i, _d, _d, _vp],
     "sf_lateral_uv_bc": [_vp, _d, _vp, _vp, _vp],
     "sf_step3d_uv_bc": [_vp] * 14 + [_i, _i, _d, _d, _d, _vp],

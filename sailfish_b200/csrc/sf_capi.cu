@@ -198,6 +198,8 @@ void free_ctx(sf_ctx *c) {
     delete[] c->h_off2;
     delete[] c->h_off3;
     delete[] c->h_offN;
+    cudaFree(c->check_dev);
+    if (c->check_host) cudaFreeHost(c->check_host);
     delete c;
 }
 
@@ -659,6 +661,12 @@ int sf_step2d_predictor(sf_ctx *c, const sf_state2d *st, double dtfast, double t
         using O = sf::Ops<R>;
         R *z0 = (R *)st->zeta[0], *z1 = (R *)st->zeta[1], *z2 = (R *)st->zeta[2];
         cudaError_t e;
+        if (!first_step && c->nmem == 1 && c->pred_ok && c->use_fused) {
+            // the leapfrog branch as one fused launch (identical results, see substep())
+            return O::pred2d(c, z0, z1, z2, (R *)st->ubar[1], (R *)st->vbar[1], (R *)st->ubar[2],
+                             (R *)st->vbar[2], (R *)st->rzeta[1], (R *)st->rubar[1],
+                             (R *)st->rvbar[1], dtfast, 2.0 / 5.0, val, nullptr, S(s));
+        }
         if (first_step) {
             e = O::zeta_rhs(c, z1, (R *)st->ubar[1], (R *)st->vbar[1], (R *)st->rzeta[1], 0, 0.0,
                             nullptr, nullptr, nullptr, nullptr, nullptr, 0.0, S(s));
@@ -1007,6 +1015,83 @@ int sf_set_depth(sf_ctx *c, const double *Zt, void *z_w, void *z_r, void *Hz, sf
         using R = std::remove_pointer_t<decltype(t)>;
         return sf::Ops<R>::set_depth(c, Zt, (R *)z_w, (R *)z_r, (R *)Hz, S(s));
     });
+}
+
+}  // extern "C"
+
+// ---- state check (non-finite / blow-up detection) --------------------------------------------
+namespace {
+constexpr int kCheckBlocks = 4 * 148;
+constexpr int kCheckFields = 5;   // zeta, ubar, vbar, u, v
+const char *const kCheckNames[kCheckFields] = {"zeta", "ubar", "vbar", "u", "v"};
+
+struct CheckArgs {
+    const void *f[kCheckFields];
+    long n[kCheckFields];
+    double bound[kCheckFields];   // |value| above the bound counts as a blow-up
+};
+
+// One grid-stride pass over each field; a value that is NaN, infinite or above its bound
+// records key = field << 56 | flat index with atomicMin, so the smallest field and index win.
+template <typename R>
+__global__ void __launch_bounds__(256) k_check_state(CheckArgs a, unsigned long long *key) {
+    const long stride = (long)gridDim.x * blockDim.x;
+    for (int f = 0; f < kCheckFields; ++f) {
+        const R *x = static_cast<const R *>(a.f[f]);
+        if (!x) continue;
+        const R bound = (R)a.bound[f];
+        unsigned long long best = ~0ULL;
+        for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < a.n[f]; p += stride) {
+            const R v = __ldg(x + p);
+            if (!(fabs(v) <= bound)) {   // NaN compares false
+                best = ((unsigned long long)f << 56) | (unsigned long long)p;
+                break;
+            }
+        }
+        if (best != ~0ULL) atomicMin(key, best);
+    }
+}
+}  // namespace
+
+extern "C" {
+
+int sf_check_state(sf_ctx *c, const void *zeta, const void *ubar, const void *vbar,
+                   const void *u, const void *v, double surface_bound, double velocity_bound,
+                   sf_stream s) {
+    if (!c) return fail(SF_EINVAL, "null context");
+    if (c->nmem != 1) return fail(SF_EUNSUPPORTED, "sf_check_state: single-grid contexts only");
+    if (!(surface_bound > 0.0) || !(velocity_bound > 0.0))
+        return fail(SF_EINVAL, "sf_check_state: bounds must be positive");
+    cudaError_t e;
+    if (!c->check_dev) {
+        e = cudaMalloc(&c->check_dev, sizeof(unsigned long long));
+        if (e != cudaSuccess) return fail(SF_ENOMEM, "sf_check_state: device flag");
+        e = cudaMallocHost(&c->check_host, sizeof(unsigned long long));
+        if (e != cudaSuccess) return fail(SF_ENOMEM, "sf_check_state: host flag");
+    }
+    const long n3 = (long)(c->N + 1) * c->s2;
+    CheckArgs a{{zeta, ubar, vbar, u, v}, {c->s2, c->s2, c->s2, n3, n3},
+                {surface_bound, velocity_bound, velocity_bound, velocity_bound, velocity_bound}};
+    SF_TRY_CUDA(cudaMemsetAsync(c->check_dev, 0xFF, sizeof(unsigned long long), S(s)),
+                "sf_check_state");
+    if (c->prec == SF_FP64)
+        k_check_state<double><<<kCheckBlocks, 256, 0, S(s)>>>(a, c->check_dev);
+    else
+        k_check_state<float><<<kCheckBlocks, 256, 0, S(s)>>>(a, c->check_dev);
+    SF_TRY_CUDA(cudaGetLastError(), "sf_check_state");
+    SF_TRY_CUDA(cudaMemcpyAsync(c->check_host, c->check_dev, sizeof(unsigned long long),
+                                cudaMemcpyDeviceToHost, S(s)), "sf_check_state");
+    SF_TRY_CUDA(cudaStreamSynchronize(S(s)), "sf_check_state");
+    const unsigned long long key = *c->check_host;
+    if (key == ~0ULL) return SF_OK;
+    const int f = (int)(key >> 56);
+    const long p = (long)(key & ((1ULL << 56) - 1));
+    const long lev = f >= 3 ? p / c->s2 : 0, q = p % c->s2;
+    char msg[200];
+    std::snprintf(msg, sizeof msg,
+                  "non-finite or out-of-bound %s at flat index %ld (level %ld, j %ld, i %ld)",
+                  kCheckNames[f < kCheckFields ? f : 0], p, lev, q / c->I, q % c->I);
+    return fail(SF_ENONFINITE, msg);
 }
 
 static double ab3_cff(int iic, int ntfirst) {   // step3D_uv.kernels.cpp:663-666

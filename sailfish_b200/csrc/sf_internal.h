@@ -155,6 +155,10 @@ struct sf_ctx {
     int nbm_pipe = 0;
     long tot2 = 0, tot3 = 0, totN = 0;   // pool sizes
     long *h_off2 = nullptr, *h_off3 = nullptr, *h_offN = nullptr;   // host copies
+    // sf_check_state: the smallest (field, flat index) key of a bad value (device) and its
+    // pinned host copy, allocated on first use
+    unsigned long long *check_dev = nullptr;
+    unsigned long long *check_host = nullptr;
 };
 
 namespace sf {

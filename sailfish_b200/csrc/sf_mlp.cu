@@ -870,12 +870,18 @@ int sf_mlp_gemm(int n_rows, int K, const void *A, int a_bf16, long a_rs, long a_
     if (n_rows <= 0 || K <= 0 || K % 16 != 0) return mfail(SF_EINVAL, "K must be a positive multiple of 16");
     if (!A || !B || !O || !err) return mfail(SF_EINVAL, "null pointer");
     Mat a{A, a_bf16, a_rs, a_ks, n_rows, K}, b{B, b_bf16, b_rs, b_ks, kTile, K};
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e0 = cudaFuncSetAttribute(sf::mlp::k_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              (int)sf::mlp::kGemmSmem);
+    // The raised shared-memory limit is a per-device function attribute: set it once on each
+    // device the GEMM runs on.
+    static bool attr_set[64] = {};
+    int dev = 0;
+    cudaError_t e0 = cudaGetDevice(&dev);
+    if (e0 != cudaSuccess) return mcuda(e0, "sf_mlp_gemm");
+    if (dev < 0 || dev >= 64) return mfail(SF_EINVAL, "device ordinal out of range");
+    if (!attr_set[dev]) {
+        e0 = cudaFuncSetAttribute(sf::mlp::k_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)sf::mlp::kGemmSmem);
         if (e0 != cudaSuccess) return mcuda(e0, "sf_mlp_gemm");
-        attr = true;
+        attr_set[dev] = true;
     }
     sf::mlp::k_gemm<<<nblk(n_rows, kTile), sf::mlp::kThreads, sf::mlp::kGemmSmem, S(s)>>>(
         a, b, n_rows, K, bias, act, O, ldo, Z, ldz, err);
@@ -916,14 +922,17 @@ int sf_mlp_backward(const sf_mlp_params *w, int n, const float *X, const float *
             sf::mlp::k_act_back<<<nblk((long)n * ld, 256), 256, 0, S(s)>>>(
                 n, g_in, pre + (long)l * n * ld, G, sf::mlp::act_code(w));
         } else {
-            cudaMemcpyAsync(G, g_in, sizeof(float) * n * ld, cudaMemcpyDeviceToDevice, S(s));
+            const cudaError_t ec = cudaMemcpyAsync(G, g_in, sizeof(float) * n * ld,
+                                                   cudaMemcpyDeviceToDevice, S(s));
+            if (ec != cudaSuccess) return mcuda(ec, "sf_mlp_backward: copy of dY");
         }
         const float *Xl = l == 0 ? X : acts + (long)(l - 1) * n * ld;
         // dW[out, in] = sum_m G[m, out] Xl[m, in]
         int rc = sf_mlp_gemm(kTile, n, G, 0, 1, ld, Xl, 0, 1, ld, nullptr, 0, dW[l], ld, nullptr, 0,
                              err, s);
         if (rc) return rc;
-        cudaMemsetAsync(db[l], 0, sizeof(float) * kTile, S(s));
+        const cudaError_t ez = cudaMemsetAsync(db[l], 0, sizeof(float) * kTile, S(s));
+        if (ez != cudaSuccess) return mcuda(ez, "sf_mlp_backward: clearing db");
         sf::mlp::k_colsum<<<256, kTile, 0, S(s)>>>(n, G, db[l]);
         if (l > 0) {   // dA[m, in] = sum_out G[m, out] W[out, in]
             rc = sf_mlp_gemm(n, kTile, G, 0, ld, 1, w->W[l], 1, 1, ld, nullptr, 0, dA, ld, nullptr, 0,

@@ -166,6 +166,10 @@ class Model:
         # vertical mixing per step (closure.Closure), after step3d_UV; None keeps AKv as it is,
         # as the reference's step does (modules/mod_ocean.py:91)
         self.mixing = None
+        # blow-up check (sf_check_state) after every check_every-th step (0: never); a failed
+        # check raises SailfishError with status SF_ENONFINITE
+        self.check_every = 0
+        self.surface_bound, self.velocity_bound = 100.0, 50.0
 
     # -- state I/O ------------------------------------------------------------------------
     def load(self, state):
@@ -211,6 +215,17 @@ class Model:
         self.slots = new
 
     # -- steps -------------------------------------------------------------------------------
+    def check_state(self, stream=None):
+        """Scans zeta/ubar/vbar (newest slot) and u, v for NaN, infinities and magnitudes above
+        surface_bound / velocity_bound; raises SailfishError (SF_ENONFINITE) naming the first
+        bad value.  Synchronises the stream."""
+        st = stream or stream_handle()
+        p = self._p
+        check(lib.sf_check_state(self.ctx.ptr, p(self._slot("zeta", 2)), p(self._slot("ubar", 2)),
+                                 p(self._slot("vbar", 2)), p(self.u), p(self.v),
+                                 self.surface_bound, self.velocity_bound, st),
+              "sf_check_state (step %d)" % self.iic)
+
     def set_depth(self, stream=None):
         st = stream or stream_handle()
         check(lib.sf_set_depth(self.ctx.ptr, self._p(self.Zt_avg1), self._p(self.z_w),
@@ -328,5 +343,9 @@ class Model:
             self.iic += 1                          # CompTimes.nextTimeStep
             self.time += self.dt
             self.time2D = self.time
+            if self.check_every and self.iic % self.check_every == 0:
+                if ev_mix is not None:
+                    cs.wait_event(ev_mix)
+                self.check_state(st)
         if ev_mix is not None:   # the caller's stream sees the last mixing too
             cs.wait_event(ev_mix)
