@@ -172,6 +172,24 @@ def reference_cpu(config, steps, warmup, omp, shrink=1):
     return cells * n_timed / dt, omp, sample, cfg
 
 
+def cpu_sample(args):
+    """The CPU baseline beside the GPU line: the reference arm on a quarter-by-quarter
+    sub-basin, run in a child process of its own (the host-compiled reference kernels and
+    their OpenMP runtime stay out of this process, which holds torch's)."""
+    cmd = [sys.executable, os.path.abspath(__file__), "--impl", "reference", "--config",
+           args.config, "--steps", str(args.cpu_steps), "--warmup", "1", "--shrink", "4"]
+    env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK")}
+    try:
+        r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True,
+                           env=env, timeout=600)
+        line = json.loads(r.stdout.strip().splitlines()[-1])
+        if "unavailable" in line:
+            return {"value": None, "unavailable": line["unavailable"]}
+        return dict(line["cpu_baseline"])
+    except Exception as e:
+        return {"value": None, "unavailable": "CPU sample failed: %s" % e}
+
+
 # -------------------------------------------------------------------------------------------
 # clocks during the timed region
 # -------------------------------------------------------------------------------------------
@@ -647,6 +665,8 @@ def main():
     ap.add_argument("--config", default="basin4")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--cpu-steps", type=int, default=10)
+    ap.add_argument("--shrink", type=int, default=1,
+                    help="reference arm: run the basin's recipe at Lm/shrink x Mm/shrink")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 timing")
     ap.add_argument("--members", type=int, default=256, help="ensemble members (config ensemble)")
@@ -664,7 +684,7 @@ def main():
             return
         try:
             v, cores, sample, cfg = reference_cpu(args.config, max(args.steps, 1), args.warmup,
-                                                  omp)
+                                                  omp, shrink=args.shrink)
         except Exception as e:
             print(json.dumps({"impl": "reference", "unavailable": str(e)}))
             return
@@ -699,13 +719,7 @@ def main():
         if not args.no_error:
             out["error_vs_fp64"] = error_vs_fp64()
         if not args.no_cpu_baseline:
-            try:
-                v, cores, sample, _ = reference_cpu(args.config, args.cpu_steps, 1, omp,
-                                                    shrink=4)
-                out["cpu_baseline"] = {"value": v, "unit": "cell-steps/s", "cores": cores,
-                                       "kind": "reference", "sample": sample}
-            except Exception as e:
-                out["cpu_baseline"] = {"value": None, "unavailable": str(e)}
+            out["cpu_baseline"] = cpu_sample(args)
         print(json.dumps(out))
     if world > 1:
         torch.distributed.destroy_process_group()
