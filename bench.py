@@ -194,19 +194,29 @@ def cpu_sample(args):
 # clocks during the timed region
 # -------------------------------------------------------------------------------------------
 def gpu_id(index):
-    """An nvidia-smi -i identifier for torch's CUDA device `index`: its UUID (nvidia-smi
-    numbers GPUs in PCI order and ignores CUDA_VISIBLE_DEVICES, so the ordinal can name another
-    GPU), else its PCI bus id, else the ordinal."""
+    """An nvidia-smi -i identifier for torch's CUDA device `index` (nvidia-smi numbers GPUs in
+    PCI order and ignores CUDA_VISIBLE_DEVICES, so the ordinal can name another GPU): the first
+    of its UUID and its PCI bus id that nvidia-smi recognises, else None (no sampling)."""
     import torch
     p = torch.cuda.get_device_properties(index)
+    cands = []
     uuid = str(getattr(p, "uuid", "") or "")
     if uuid:
-        return uuid if uuid.startswith(("GPU-", "MIG-")) else "GPU-" + uuid
+        cands.append(uuid if uuid.startswith(("GPU-", "MIG-")) else "GPU-" + uuid)
     bus = getattr(p, "pci_bus_id", None)
     if bus is not None:
-        return "%08x:%02x:%02x.0" % (getattr(p, "pci_domain_id", 0), bus,
-                                     getattr(p, "pci_device_id", 0))
-    return str(index)
+        cands.append("%08x:%02x:%02x.0" % (getattr(p, "pci_domain_id", 0), bus,
+                                           getattr(p, "pci_device_id", 0)))
+    for c in cands:
+        try:
+            r = subprocess.run(["nvidia-smi", "-i", c, "--query-gpu=pci.bus_id",
+                                "--format=csv,noheader"], stdout=subprocess.PIPE,
+                               stderr=subprocess.DEVNULL, text=True, timeout=20)
+            if r.returncode == 0 and r.stdout.strip():
+                return c
+        except Exception:
+            pass
+    return None
 
 
 class Clocks:
@@ -218,6 +228,8 @@ class Clocks:
         self.index, self.rows, self.proc = gpu_id(index), [], None
 
     def __enter__(self):
+        if self.index is None:
+            return self
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", self.index, "--query-gpu=" + self.Q,
@@ -285,8 +297,9 @@ def time_steps(m, steps, warmup):
 
 
 def plain_fp64(args):
-    """The same workload through the FP64 path, whose results are bit-identical to the
-    reference's own kernels (the 'plain FP64 step' the FP32 form is compared with)."""
+    """The same workload through this package's FP64 path, whose results are bit-identical to
+    the reference's own kernels: how much of the speed-up over the reference's FP64 kernels
+    comes from precision and the learned closure, and how much from the kernels' design."""
     import torch
     from sailfish_b200 import configs
     from sailfish_b200.model import Model
@@ -305,6 +318,90 @@ def plain_fp64(args):
             "semantics": "bit-identical to the reference kernels",
             "vertical_mixing": "plain GLS k-epsilon every step, FP64" if mixing == "gls"
                                else "AKv constant (the reference's step)"}
+
+
+def _ref_basin(cfg):
+    """The basin dict the reference's GPU kernels take (baseline/ref_gpu.py) for a package
+    config: the same grid, tables and boundary lists."""
+    g, B = cfg["grid"], cfg["boundary"]
+    lists = {}
+    for name in ("zetaBC", "ubarBC", "vbarBC", "uvelBC", "vvelBC"):
+        for f in ("bcIdx", "bcIdx1", "bcIdx2", "bcIdxFieldIdx2", "bcIdxFieldType", "LBC"):
+            lists["%s_%s" % (name, f)] = getattr(getattr(B, name), f)
+    for f in ("zetaClosedOrGradientBCIdx1", "zetaClosedOrGradientBCIdx2", "zetaClampedBCIdx1",
+              "ubarClosedBCIdx1", "vbarClosedBCIdx1", "ubarClampedBCIdx1", "vbarClampedBCIdx1",
+              "ubarGradientBCIdx1", "ubarGradientBCIdx2", "vbarGradientBCIdx1", "vbarGradientBCIdx2"):
+        lists[f] = getattr(B, f)
+    b = dict(L=g.L, M=g.M, N=g.N, hc=g.hc, Vtransform=g.Vtransform, dt=cfg["dt"],
+             ndtfast=cfg["ndtfast"], lists=lists)
+    for k in ("h", "pm", "pn", "on_u", "om_v", "fomn", "sc_r", "sc_w", "Cs_r", "Cs_w"):
+        b[k] = getattr(g, k)
+    return b
+
+
+def reference_gpu_fp64(args, gls_ms):
+    """The plain FP64 GPU step: the reference's own kernels (NVRTC with its options, for
+    sm_100a) launched in its main3d order on this GPU (baseline/ref_gpu.py), plus plain GLS in
+    FP64 for the vertical mixing the reference lacks (this package's GLS kernel, its time
+    `gls_ms` per step measured on the same basin)."""
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "baseline"))
+    import ref_gpu
+    from sailfish_b200 import configs, host
+    if not ref_gpu.available():
+        return {"value": None, "unavailable": "baseline/_ref/src not generated"}
+    cfg = configs.CONFIGS[args.config]()
+    g = cfg["grid"]
+    nf, w1, w2 = host.set_weights(cfg["ndtfast"])
+    with _StdoutToStderr():            # the reference's initialize kernels printf
+        r = ref_gpu.RefGPU(_ref_basin(cfg), nf, w1, w2, fmad=True)
+        r.step(2)
+        torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    steps = max(1, min(args.steps, 3))
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    r.step(steps)
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / steps
+    launches = r.launches_per_step()
+    del r
+    torch.cuda.empty_cache()
+    cells = (g.L - 1) * (g.M - 1) * g.N
+    tot = ms + (gls_ms or 0.0)
+    return {"value": cells / (tot * 1e-3), "unit": "cell-steps/s", "ms_per_step": tot,
+            "reference_kernels_ms_per_step": ms, "gls_fp64_ms_per_step": gls_ms,
+            "steps": steps, "warmup": 2, "dtype": "f64",
+            "kernels": "the reference's own (modules/mod_cppkernels.cpp, nonlinear/rhs_kernels.cpp, "
+                       "nonlinear/step3D_uv.kernels.cpp, modules/mod_BC.c), NVRTC for sm_100a with "
+                       "-default-device --restrict --std=c++17, launched in main3d order",
+            "launches_per_step": launches,
+            "vertical_mixing": "plain GLS k-epsilon every step, FP64 (this package's kernel; the "
+                               "reference has no runnable GLS)"}
+
+
+def gls_fp64_ms(args):
+    """Device time of one plain-GLS update in FP64 on the bench's basin."""
+    import torch
+    from sailfish_b200 import configs
+    from sailfish_b200.model import Model
+    cfg = configs.CONFIGS[args.config]()
+    m = Model(cfg["grid"], cfg["boundary"], cfg["dt"], cfg["ndtfast"], precision="fp64")
+    install_mixing(m, "gls", args.config)
+    m.start()
+    m.mixing()
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(3):
+        m.mixing()
+    b.record(stream)
+    torch.cuda.synchronize()
+    del m
+    torch.cuda.empty_cache()
+    return a.elapsed_time(b) / 3
 
 
 def error_vs_fp64():
@@ -714,8 +811,16 @@ def main():
     if rank == 0:
         if args.precision == "fp32" and not args.no_fp64:
             torch.cuda.empty_cache()
-            out["plain_fp64"] = plain_fp64(args)
-            out["plain_fp64"]["speedup_of_value"] = out["value"] / world / out["plain_fp64"]["value"]
+            gms = gls_fp64_ms(args) if args.closure != "none" else None
+            try:
+                out["plain_fp64"] = reference_gpu_fp64(args, gms)
+            except Exception as e:
+                out["plain_fp64"] = {"value": None, "unavailable": "reference kernels: %s" % e}
+            if out["plain_fp64"].get("value"):
+                out["plain_fp64"]["speedup_of_value"] = out["value"] / world / out["plain_fp64"]["value"]
+            torch.cuda.empty_cache()
+            out["opt_fp64"] = plain_fp64(args)
+            out["opt_fp64"]["speedup_of_value"] = out["value"] / world / out["opt_fp64"]["value"]
         if not args.no_error:
             out["error_vs_fp64"] = error_vs_fp64()
         if not args.no_cpu_baseline:

@@ -28,8 +28,10 @@ TOL = {
     "set_depth": {"z_w": 2e-7, "z_r": 2e-7, "Hz": 5e-7},
     "maxflux_omega": {"Huon": 1e-6, "Hvom": 1e-6, "W": 2e-5},
     "rhs3d": {"ru": 2e-5, "rv": 2e-5},
-    "predictor": {"zeta2": 1e-6, "ubar2": 2e-5, "vbar2": 2e-5, "rzeta1": 2e-5, "rubar1": 2e-5,
-                  "rvbar1": 2e-5},
+    # the pressure-gradient tendencies difference FP32 surface elevations of neighbouring
+    # nodes (cancellation: ~3e-5 of their scale on these smooth fields)
+    "predictor": {"zeta2": 5e-6, "ubar2": 2e-5, "vbar2": 2e-5, "rzeta1": 1e-5, "rubar1": 1e-4,
+                  "rvbar1": 1e-4},
     "loop": {"zeta": 5e-5, "ubar": 5e-5, "Zt_avg1": 5e-5, "DU_avg1": 5e-5,
              "DV_avg1": 5e-5},
     "step3d_uv": {"u": 2e-5, "v": 2e-5, "ubar1": 2e-5, "vbar1": 2e-5},
