@@ -174,6 +174,11 @@ int sf_barotropic_loop(sf_ctx *ctx, sf_state2d *s, int nsub, const double *weigh
  * boundary values, which depend on time2D, are written to the device before each replay.
  * Results are identical either way.  No counterpart in the reference. */
 int sf_ctx_set_graphs(sf_ctx *ctx, int enable);
+/* Bulk-copy staging (cp.async.bulk into shared memory, completing on mbarriers) in the
+ * kernels that have it (the FP32 column solve): 1 (default) where the fields' alignment allows
+ * it, 0 for per-element cp.async staging.  Results are identical either way.  No counterpart
+ * in the reference. */
+int sf_ctx_set_bulk(sf_ctx *ctx, int enable);
 /* Turn programmatic dependent launch of the barotropic loop's kernels on (default) or off:
  * with it each kernel's blocks become resident while its predecessor's last wave runs and wait
  * on the device for its completion.  Results are identical either way. */

@@ -200,6 +200,7 @@ void free_ctx(sf_ctx *c) {
     delete[] c->h_offN;
     cudaFree(c->check_dev);
     if (c->check_host) cudaFreeHost(c->check_host);
+    cudaFree(c->dev_err);
     delete c;
 }
 
@@ -574,6 +575,11 @@ int sf_ctx_create(const sf_grid_desc *d, sf_ctx **out) {
     if (rc == SF_OK) rc = upload_program(c->ubc, U);
     if (rc == SF_OK) rc = upload_program(c->vbc, V);
     if (rc == SF_OK) rc = build_pred_maps(c, Z, U, V);
+    if (rc == SF_OK) {
+        if (cudaMalloc(&c->dev_err, sizeof(int)) != cudaSuccess ||
+            cudaMemset(c->dev_err, 0, sizeof(int)) != cudaSuccess)
+            rc = fail(SF_ENOMEM, "cudaMalloc error word");
+    }
     if (rc != SF_OK) {
         free_ctx(c);
         return rc;
@@ -857,6 +863,12 @@ int sf_ctx_set_fused(sf_ctx *c, int enable) {
     return SF_OK;
 }
 
+int sf_ctx_set_bulk(sf_ctx *c, int enable) {
+    if (!c) return fail(SF_EINVAL, "null context");
+    c->use_bulk = enable ? 1 : 0;
+    return SF_OK;
+}
+
 int sf_ctx_fused_available(const sf_ctx *c) { return c && c->nmem == 1 && c->pred_ok ? 1 : 0; }
 
 int sf_ctx_set_pdl(sf_ctx *c, int enable) {
@@ -1082,6 +1094,16 @@ int sf_check_state(sf_ctx *c, const void *zeta, const void *ubar, const void *vb
     SF_TRY_CUDA(cudaMemcpyAsync(c->check_host, c->check_dev, sizeof(unsigned long long),
                                 cudaMemcpyDeviceToHost, S(s)), "sf_check_state");
     SF_TRY_CUDA(cudaStreamSynchronize(S(s)), "sf_check_state");
+    if (c->dev_err) {
+        int werr = 0;
+        SF_TRY_CUDA(cudaMemcpy(&werr, c->dev_err, sizeof(int), cudaMemcpyDeviceToHost),
+                    "sf_check_state");
+        if (werr) {
+            SF_TRY_CUDA(cudaMemset(c->dev_err, 0, sizeof(int)), "sf_check_state");
+            return fail(SF_ETIMEOUT, "a kernel's bounded wait for its staged data gave up "
+                                     "(the results of the step are not valid)");
+        }
+    }
     const unsigned long long key = *c->check_host;
     if (key == ~0ULL) return SF_OK;
     const int f = (int)(key >> 56);

@@ -71,6 +71,7 @@ struct Geo {
     const int *bcfield;   // zetaBC.bcIdxFieldIdx2
     const int *utype, *vtype;
     long ref_threads;     // threads of the reference's rhs3d launches (rhs_kernels.cpp:86-91)
+    int *err = nullptr;   // context's device error word: a bounded wait that gave up sets it
 };
 
 // Launch geometry shared by the kernels and the host code that builds block maps.
@@ -131,6 +132,8 @@ struct sf_ctx {
     int *pred_counter = nullptr;
     int pred_ok = 0;
     int use_fused = 1;
+    // bulk-copy staging (cp.async.bulk) in the kernels that have it (sf_ctx_set_bulk)
+    int use_bulk = 1;
     cudaStream_t cap = nullptr;
     double *d_bcval = nullptr;
     sf_loop_graph graphs[3];
@@ -159,6 +162,9 @@ struct sf_ctx {
     // pinned host copy, allocated on first use
     unsigned long long *check_dev = nullptr;
     unsigned long long *check_host = nullptr;
+    // device error word of the kernels with bounded waits (Geo::err); sf_check_state reports
+    // and clears it
+    int *dev_err = nullptr;
 };
 
 namespace sf {

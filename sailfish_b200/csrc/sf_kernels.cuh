@@ -1239,14 +1239,61 @@ constexpr int kPipeCols = kPipeTile;
 constexpr int kPipeGroup = 2;               // levels consumed per barrier pair
 constexpr int kPipeDepth = 3 * kPipeGroup;  // levels in flight (shared-memory ring slots)
 constexpr int kPipeThreads = 2 * kPipeCols;   // one thread per system (U, V) and column
-constexpr int kPipeSlot = 3 * (2 * kPipeCols + 1) + 4 * kPipeCols;   // floats per level
+// A ring slot holds one level: rows of Hz, Akv and z_r(k+1) followed by the old u, old v, ru and
+// rv of the tile's columns.  Element staging (cp.async): a row is [p0-1, p0+63] then
+// [p0-I, p0-I+63] (kRow floats).  Bulk staging (cp.async.bulk): a row is two 16-byte-aligned
+// spans of 68 floats, [p0-4, p0+64) and [p0-I-r, p0-I-r+68) with r = (-I) mod 4 (kRowB floats).
+constexpr int kRow = 2 * kPipeCols + 1;
+constexpr int kSpan = kPipeCols + 4;
+constexpr int kRowB = 2 * kSpan;
+constexpr int kSlotE = 3 * kRow + 4 * kPipeCols, kSlotB = 3 * kRowB + 4 * kPipeCols;
+constexpr int kPipeSlot = kSlotE > kSlotB ? kSlotE : kSlotB;   // floats per level
+static_assert((kRowB * 4) % 16 == 0 && (kSpan * 4) % 16 == 0 && (kPipeSlot * 4) % 16 == 0,
+              "bulk-copy destinations must stay 16-byte aligned");
 
 __host__ __device__ constexpr size_t pipe_smem_bytes(int N) {
-    return sizeof(float) * ((size_t)N * kPipeThreads + (size_t)kPipeDepth * kPipeSlot);
+    // [N][kPipeThreads] c' | ring of kPipeDepth slots | kPipeDepth mbarriers (bulk staging)
+    return sizeof(float) * ((size_t)N * kPipeThreads + (size_t)kPipeDepth * kPipeSlot) +
+           8 * (size_t)kPipeDepth;
 }
 constexpr int kBackChunk = 8;   // levels of d' read ahead per step of the back substitution
 
-template <typename R>   // R = float only: the FP32 form
+// Bulk copies (the TMA unit's non-tensor form) into shared memory, completing on an mbarrier.
+__device__ __forceinline__ void mbar_init1(uint32_t a) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(a) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t a, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(a), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+        "l"(src), "r"(bytes), "r"(bar)
+        : "memory");
+}
+// Bounded wait for an mbarrier phase: false (and the context's error word set) if it gave up.
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t a, uint32_t parity, int *err) {
+    for (int it = 0; it < (1 << 22); ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    if (err) atomicExch(err, 1);
+    return false;
+}
+
+// BULK: the tile's levels arrive by bulk copies issued by thread 0 (ten per level, one
+// mbarrier per ring slot); otherwise every thread stages its own elements with cp.async.  The
+// arithmetic is the same either way, so the two give identical results; bulk staging is used
+// for tiles whose spans lie inside the fields (all but the first row of tiles and the last
+// tile) when the plane size and the field addresses keep the spans 16-byte aligned.
+template <typename R, bool BULK>   // R = float only: the FP32 form
 __device__ __forceinline__ void step3d_uv_pipe_body(const Geo<R> &g, float *__restrict__ u,
         float *__restrict__ v, const float *__restrict__ ru, const float *__restrict__ rv,
         float *__restrict__ ubar_t1, float *__restrict__ vbar_t1, float *__restrict__ ubar_t2,
@@ -1254,7 +1301,7 @@ __device__ __forceinline__ void step3d_uv_pipe_body(const Geo<R> &g, float *__re
         const float *__restrict__ z_r, const double *__restrict__ DU,
         const double *__restrict__ DV, const float *tmpU, const float *tmpV, float cff,
         float lambda, float Dt, int do_bc, float bcval, const long tile) {
-    extern __shared__ float spipe[];
+    extern __shared__ __align__(16) float spipe[];
     const int N = g.N;
     const long I = g.I, s2 = g.s2;
     // two threads per column: sys 0 solves the U system of column col, sys 1 its V system
@@ -1265,17 +1312,23 @@ __device__ __forceinline__ void step3d_uv_pipe_body(const Geo<R> &g, float *__re
     float *ring = spipe + N * kPipeThreads;
     float *const outc = (sys == 0 ? u : v) + p;   // this system's output column (d', then x)
     const float *uo_all = tmpU ? tmpU : u, *vo_all = tmpV ? tmpV : v;
+    const uint32_t ring_s = (uint32_t)__cvta_generic_to_shared(ring);
+    const uint32_t bar_s = ring_s + 4u * kPipeDepth * kPipeSlot;
+    const int s2i = (int)s2;
+    const int rB = (int)((4 - (I & 3)) & 3);   // the second span starts r before p0 - I
+    constexpr int row = BULK ? kRowB : kRow;    // floats between the Hz, Akv and z_r rows
+    // this thread's own (p) and neighbour (p-1 or p-I) entries in a row
+    const int iP = BULK ? col + 4 : col + 1;
+    const int iQ = BULK ? (sys == 0 ? col + 3 : kSpan + rB + col) : (sys == 0 ? col : kPipeCols + 1 + col);
 
-    // level k into slot: Hz(k), Akv(k), z_r(k+1) at [p0-1, p0+63] (sys 0 copies these, plus
-    // old u and ru) and [p0-I, p0-I+63] (sys 1, plus old v and rv); sources outside [0, s2) in
-    // the plane are zero-filled (their columns are not U/V nodes).
+    int nslot = 0;   // slot of the next level issued (levels are issued in order)
+    // element staging: level k into slot: Hz(k), Akv(k), z_r(k+1) at [p0-1, p0+63] (sys 0
+    // copies these, plus old u and ru) and [p0-I, p0-I+63] (sys 1, plus old v and rv); sources
+    // outside [0, s2) in the plane are zero-filled (their columns are not U/V nodes).
     const long q = sys == 0 ? p0 - 1 + col : p0 - I + col, qE = p0 + kPipeCols - 1;
     const bool okq = q >= 0 && q < s2, okP = p < s2;
     const bool okE = sys == 0 && col == 0 && qE < s2;
-    constexpr int kRow = 2 * kPipeCols + 1;
     const int seg = sys == 0 ? col : kPipeCols + 1 + col;
-    // the copy sources at level 0 and the copy sizes, fixed over the levels: a level adds k s2
-    // (an out-of-range copy keeps a valid address and copies 0 bytes)
     const long qq = okq ? q : 0, qe = okE ? qE : 0, pp = okP ? p : 0;
     const float *const cHz = Hz + qq, *const cAk = Akv + qq, *const cZr = z_r + s2 + qq;
     const float *const eHz = Hz + qe, *const eAk = Akv + qe, *const eZr = z_r + s2 + qe;
@@ -1286,27 +1339,45 @@ __device__ __forceinline__ void step3d_uv_pipe_body(const Geo<R> &g, float *__re
     // destinations as shared-window byte addresses in slot 0 (a level adds its slot's offset;
     // the three fields of a row at immediate offsets), sources as 32-bit element offsets from
     // level 0 (the launcher keeps (N+1) s2 below 2^31 for this kernel)
-    const uint32_t ring_s = (uint32_t)__cvta_generic_to_shared(ring);
     const uint32_t dq = ring_s + 4u * seg, dE = ring_s + 4u * kPipeCols;
     const uint32_t dO = ring_s + 4u * oO, dR = ring_s + 4u * oR;
-    const int s2i = (int)s2;
-    int nslot = 0;   // slot of the next level issued (levels are issued in order)
     auto issue = [&](int k) {
         const uint32_t sb = (uint32_t)nslot * (4u * kPipeSlot);
+        const int sl = nslot;
         nslot = nslot + 1 == kPipeDepth ? 0 : nslot + 1;
         const int o = k * s2i;
         const bool zr = k + 1 < N;   // z_r(k+1) exists for k < N-1 only
-        const int oz = zr ? o : o - s2i;
-        cp_async_at<0>(dq + sb, cHz + o, nq);
-        cp_async_at<4 * kRow>(dq + sb, cAk + o, nq);
-        cp_async_at<8 * kRow>(dq + sb, cZr + oz, zr ? nq : 0);
-        if (edge) {
-            cp_async_at<0>(dE + sb, eHz + o, ne);
-            cp_async_at<4 * kRow>(dE + sb, eAk + o, ne);
-            cp_async_at<8 * kRow>(dE + sb, eZr + oz, zr ? ne : 0);
+        if constexpr (BULK) {   // thread 0 only
+            const uint32_t bar = bar_s + 8u * sl, d0 = ring_s + sb;
+            constexpr uint32_t sp = 4u * kSpan, cb = 4u * kPipeCols;
+            mbar_expect_tx(bar, (zr ? 6u : 4u) * sp + 4u * cb);
+            const long a = o + p0 - 4, b = o + p0 - I - rB;
+            bulk_g2s(d0, Hz + a, sp, bar);
+            bulk_g2s(d0 + sp, Hz + b, sp, bar);
+            bulk_g2s(d0 + 4u * row, Akv + a, sp, bar);
+            bulk_g2s(d0 + 4u * row + sp, Akv + b, sp, bar);
+            if (zr) {
+                bulk_g2s(d0 + 8u * row, z_r + s2 + a, sp, bar);
+                bulk_g2s(d0 + 8u * row + sp, z_r + s2 + b, sp, bar);
+            }
+            const uint32_t dv = d0 + 12u * row;
+            bulk_g2s(dv, uo_all + o + p0, cb, bar);
+            bulk_g2s(dv + cb, vo_all + o + p0, cb, bar);
+            bulk_g2s(dv + 2u * cb, ru + o + p0, cb, bar);
+            bulk_g2s(dv + 3u * cb, rv + o + p0, cb, bar);
+        } else {
+            const int oz = zr ? o : o - s2i;
+            cp_async_at<0>(dq + sb, cHz + o, nq);
+            cp_async_at<4 * kRow>(dq + sb, cAk + o, nq);
+            cp_async_at<8 * kRow>(dq + sb, cZr + oz, zr ? nq : 0);
+            if (edge) {
+                cp_async_at<0>(dE + sb, eHz + o, ne);
+                cp_async_at<4 * kRow>(dE + sb, eAk + o, ne);
+                cp_async_at<8 * kRow>(dE + sb, eZr + oz, zr ? ne : 0);
+            }
+            cp_async_at<0>(dO + sb, cO + o, np);
+            cp_async_at<0>(dR + sb, cR + o, np);
         }
-        cp_async_at<0>(dO + sb, cO + o, np);
-        cp_async_at<0>(dR + sb, cR + o, np);
     };
     const int i = (int)(p % I), j = (int)(p / I);
     const bool live = p < s2;
@@ -1315,9 +1386,19 @@ __device__ __forceinline__ void step3d_uv_pipe_body(const Geo<R> &g, float *__re
     const long d = sys == 0 ? 1 : I;   // the neighbour of this system's face
 
     constexpr int kAhead = kPipeDepth - kPipeGroup;   // levels issued before the first group
-    for (int k = 0; k < kAhead; ++k) {
-        if (k < N) issue(k);
-        cp_async_commit();
+    if constexpr (BULK) {
+        if (threadIdx.x == 0) {
+            for (int k = 0; k < kPipeDepth; ++k) mbar_init1(bar_s + 8u * k);
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+        __syncthreads();
+        if (threadIdx.x == 0)
+            for (int k = 0; k < kAhead && k < N; ++k) issue(k);
+    } else {
+        for (int k = 0; k < kAhead; ++k) {
+            if (k < N) issue(k);
+            cp_async_commit();
+        }
     }
     const float cm = -lambda * Dt;
     float cmn = 0.f, zP = 0.f, zQ = 0.f;
@@ -1328,7 +1409,6 @@ __device__ __forceinline__ void step3d_uv_pipe_body(const Geo<R> &g, float *__re
     }
     float fc = 0.f, fc0 = 0.f, ccp = 0.f, ddp = 0.f;
     double H = 0.0, O = 0.0, Rs = 0.0;
-    const int qi = sys == 0 ? col : kPipeCols + 1 + col;   // this system's neighbour in a row
     // levels in groups of kPipeGroup: one wait and one barrier per group.  After the barrier of
     // group g every thread has finished group g-1, whose slots (kPipeDepth is a multiple of the
     // group) are refilled with group g+2, so two groups are in flight while one is eliminated
@@ -1337,14 +1417,14 @@ __device__ __forceinline__ void step3d_uv_pipe_body(const Geo<R> &g, float *__re
     auto level = [&](int k) {
         const float *sl = ring + cslot * kPipeSlot;
         cslot = cslot + 1 == kPipeDepth ? 0 : cslot + 1;
-        const float *sHz = sl, *sAk = sl + kRow, *sZr = sl + 2 * kRow;
-        const float *sO = sl + 3 * kRow + sys * kPipeCols, *sR = sl + 3 * kRow + (2 + sys) * kPipeCols;
-        const float hz = (sHz[col + 1] + sHz[qi]) * 0.5f;
+        const float *sHz = sl, *sAk = sl + row, *sZr = sl + 2 * row;
+        const float *sO = sl + 3 * row + sys * kPipeCols, *sR = sl + 3 * row + (2 + sys) * kPipeCols;
+        const float hz = (sHz[iP] + sHz[iQ]) * 0.5f;
         float gk = 0.f;
         if (k < N - 1) {
-            const float zP1 = sZr[col + 1], zQ1 = sZr[qi];
+            const float zP1 = sZr[iP], zQ1 = sZr[iQ];
             // divisions by layer spacings and pivots (metres): the reciprocal form, as ddiv
-            gk = __fdividef(cm * ((sAk[col + 1] + sAk[qi]) * 0.5f), ((zP1 - zP) + (zQ1 - zQ)) * 0.5f);
+            gk = __fdividef(cm * ((sAk[iP] + sAk[iQ]) * 0.5f), ((zP1 - zP) + (zQ1 - zQ)) * 0.5f);
             zP = zP1;
             zQ = zQ1;
         }
@@ -1368,12 +1448,29 @@ __device__ __forceinline__ void step3d_uv_pipe_body(const Geo<R> &g, float *__re
         O += (double)(ok * hz);
     };
     for (int k0 = 0; k0 < N; k0 += kPipeGroup) {
-        cp_async_wait<kAhead - kPipeGroup>();   // this group's levels (the next may be in flight)
-        __syncthreads();
+        if constexpr (BULK) {
 #pragma unroll
-        for (int h = 0; h < kPipeGroup; ++h) {
-            if (k0 + kAhead + h < N) issue(k0 + kAhead + h);
-            cp_async_commit();
+            for (int h = 0; h < kPipeGroup; ++h) {
+                const int k = k0 + h;
+                if (k < N)
+                    mbar_wait_bounded(bar_s + 8u * (k % kPipeDepth), (uint32_t)((k / kPipeDepth) & 1),
+                                      g.err);
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+#pragma unroll
+                for (int h = 0; h < kPipeGroup; ++h)
+                    if (k0 + kAhead + h < N) issue(k0 + kAhead + h);
+            }
+        } else {
+            cp_async_wait<kAhead - kPipeGroup>();   // this group's levels (the next may be in flight)
+            __syncthreads();
+#pragma unroll
+            for (int h = 0; h < kPipeGroup; ++h) {
+                if (k0 + kAhead + h < N) issue(k0 + kAhead + h);
+                cp_async_commit();
+            }
         }
         if (both) {
 #pragma unroll
@@ -1720,13 +1817,21 @@ __global__ void __launch_bounds__(128) kb_step3d_uv(
 }
 
 template <typename R>
-__global__ void __launch_bounds__(kPipeThreads) k_step3d_uv_pipe(
+__global__ void __launch_bounds__(kPipeThreads, 5) k_step3d_uv_pipe(
     Geo<R> g, float *__restrict__ u, float *__restrict__ v, const float *__restrict__ ru, const float *__restrict__ rv, float *__restrict__ ubar_t1,
     float *__restrict__ vbar_t1, float *__restrict__ ubar_t2, float *__restrict__ vbar_t2, const float *__restrict__ Hz, const float *__restrict__ Akv,
     const float *__restrict__ z_r, const double *__restrict__ DU, const double *__restrict__ DV, const float *tmpU, const float *tmpV,
-    float cff, float lambda, float Dt, int do_bc, float bcval) {
-    step3d_uv_pipe_body(g, u, v, ru, rv, ubar_t1, vbar_t1, ubar_t2, vbar_t2, Hz, Akv, z_r, DU, DV,
-                        tmpU, tmpV, cff, lambda, Dt, do_bc, bcval, (long)blockIdx.x);
+    float cff, float lambda, float Dt, int do_bc, float bcval, int bulk_ok) {
+    // bulk staging where the tile's spans (down to p0 - I - r, up to p0 + 63) lie in the plane
+    const long p0 = (long)blockIdx.x * kPipeCols, rB = (4 - (g.I & 3)) & 3;
+    if (bulk_ok && p0 - g.I - rB >= 0 && p0 + kPipeCols <= g.s2)
+        step3d_uv_pipe_body<R, true>(g, u, v, ru, rv, ubar_t1, vbar_t1, ubar_t2, vbar_t2, Hz, Akv,
+                                     z_r, DU, DV, tmpU, tmpV, cff, lambda, Dt, do_bc, bcval,
+                                     (long)blockIdx.x);
+    else
+        step3d_uv_pipe_body<R, false>(g, u, v, ru, rv, ubar_t1, vbar_t1, ubar_t2, vbar_t2, Hz, Akv,
+                                      z_r, DU, DV, tmpU, tmpV, cff, lambda, Dt, do_bc, bcval,
+                                      (long)blockIdx.x);
 }
 template <typename R>
 __global__ void __launch_bounds__(kPipeThreads, 5) kb_step3d_uv_pipe(
@@ -1735,7 +1840,7 @@ __global__ void __launch_bounds__(kPipeThreads, 5) kb_step3d_uv_pipe(
     const float *__restrict__ Akv, const float *__restrict__ z_r, const double *__restrict__ DU, const double *__restrict__ DV, const float *tmpU,
     const float *tmpV, float cff, float lambda, float Dt, int do_bc, float bcval) {
     SF_MEMBER(bm)
-    step3d_uv_pipe_body(g, O3(u), O3(v), O3(ru), O3(rv), O2(ubar_t1), O2(vbar_t1), O2(ubar_t2),
+    step3d_uv_pipe_body<R, false>(g, O3(u), O3(v), O3(ru), O3(rv), O2(ubar_t1), O2(vbar_t1), O2(ubar_t2),
                         O2(vbar_t2), ON(Hz), O3(Akv), ON(z_r), O2(DU), O2(DV), O3(tmpU), O3(tmpV),
                         cff, lambda, Dt, do_bc, bcval, (long)mb_.y);
 }
@@ -1777,6 +1882,7 @@ Geo<R> Ops<R>::geo(const sf_ctx *c) {
     g.utype = c->utype;
     g.vtype = c->vtype;
     g.ref_threads = c->ref_threads;
+    g.err = c->dev_err;
     return g;
 }
 
@@ -1968,10 +2074,15 @@ cudaError_t Ops<R>::step3d_uv(const sf_ctx *c, R *u, R *v, const R *ru, const R 
             return cudaGetLastError();
         }
         if (fits) {
+            // bulk staging needs 16-byte aligned spans: every level starts on a 16-byte
+            // boundary (s2 a multiple of 4) in 16-byte aligned fields
+            auto al = [](const void *q) { return q == nullptr || ((uintptr_t)q & 15) == 0; };
+            const int bulk_ok = c->s2 % 4 == 0 && al(u) && al(v) && al(ru) && al(rv) && al(Hz) &&
+                                al(Akv) && al(z_r) && al(tmpU) && al(tmpV) && c->use_bulk;
             k_step3d_uv_pipe<float><<<blocks_for(c->s2, kPipeCols), kPipeThreads,
                                       pipe_smem_bytes(c->N), s>>>(
                 geo(c), u, v, ru, rv, ubar_t1, vbar_t1, ubar_t2, vbar_t2, Hz, Akv, z_r, DU, DV,
-                tmpU, tmpV, (float)cff, (float)lambda, (float)Dt, do_bc, (float)bcval);
+                tmpU, tmpV, (float)cff, (float)lambda, (float)Dt, do_bc, (float)bcval, bulk_ok);
             return cudaGetLastError();
         }
     }

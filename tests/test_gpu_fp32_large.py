@@ -250,3 +250,28 @@ def test_fp64_step_bit_exact_against_the_oracle_at_size():
         np.testing.assert_array_equal(s[n].reshape(-1), O.t3(n), err_msg=n)
     for n in ("z_w", "z_r", "Hz"):
         np.testing.assert_array_equal(s[n].reshape(-1), getattr(og, n).reshape(-1), err_msg=n)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("Lm", CASES)
+def test_column_solve_bulk_and_element_staging_agree(Lm):
+    """The FP32 column solve with its levels staged by bulk copies (cp.async.bulk, interior
+    tiles) and by per-element cp.async (sf_ctx_set_bulk(ctx, 0)): identical results."""
+    import torch
+    from sailfish_b200._lib import lib, check
+    out = []
+    for bulk in (1, 0):
+        _, m = _models(Lm)
+        assert lib.sf_ctx_set_bulk(m.ctx.ptr, bulk) == 0
+        p = m._p
+        st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        sl = lambda n, k: getattr(m, n)[m.slots[k]]
+        check(lib.sf_step3d_uv_bc(m.ctx.ptr, p(m.u), p(m.v), p(m.ru), p(m.rv), p(sl("ubar", 1)),
+                                  p(sl("vbar", 1)), p(sl("ubar", 2)), p(sl("vbar", 2)), p(m.Hz),
+                                  p(m.AKv), p(m.z_r), p(m.DU_avg1), p(m.DV_avg1), 3, 0, 1.0, m.dt,
+                                  0.0, st), "sf_step3d_uv_bc")
+        m.check_state()            # also reports a bounded wait that gave up
+        torch.cuda.synchronize()
+        out.append([t.cpu().numpy() for t in (m.u, m.v, sl("ubar", 1), sl("vbar", 1))])
+    for a, b in zip(out[0], out[1]):
+        np.testing.assert_array_equal(a, b)
