@@ -178,8 +178,10 @@ class RefGPU:
         import torch
         from cuda.bindings import driver as drv
         self.np, self.torch, self.drv = np, torch, drv
-        torch.cuda.init()
         self.dev = torch.device("cuda", torch.cuda.current_device())
+        # the driver-API module loads need the device's primary context current on this thread
+        torch.zeros(1, device=self.dev)
+        torch.cuda.synchronize()
         self.funcs = {}
         self.mods = []
         for name, cubin in cubins(fmad).items():

@@ -175,9 +175,9 @@ int sf_barotropic_loop(sf_ctx *ctx, sf_state2d *s, int nsub, const double *weigh
  * Results are identical either way.  No counterpart in the reference. */
 int sf_ctx_set_graphs(sf_ctx *ctx, int enable);
 /* Bulk-copy staging (cp.async.bulk into shared memory, completing on mbarriers) in the
- * kernels that have it (the FP32 column solve): 1 (default) where the fields' alignment allows
- * it, 0 for per-element cp.async staging.  Results are identical either way.  No counterpart
- * in the reference. */
+ * kernels that have it (the FP32 column solve): 1 where the fields' alignment allows it, 0
+ * (default, the faster on one B200) for per-element cp.async staging.  Results are identical
+ * either way.  No counterpart in the reference. */
 int sf_ctx_set_bulk(sf_ctx *ctx, int enable);
 /* Turn programmatic dependent launch of the barotropic loop's kernels on (default) or off:
  * with it each kernel's blocks become resident while its predecessor's last wave runs and wait
@@ -190,6 +190,38 @@ int sf_ctx_set_pdl(sf_ctx *ctx, int enable);
 int sf_ctx_set_fused(sf_ctx *ctx, int enable);
 /* 1 if the context can use the fused predictor, else 0. */
 int sf_ctx_fused_available(const sf_ctx *ctx);
+
+/* ---- ROMS-form barotropic step, obsolete/step2d_LF_AM3.h.py + nonlinear/set_vbc.py ------
+ * The free-surface and depth-integrated momentum step of ROMS's LF-AM3 scheme, which the
+ * reference carries only as untranslated Fortran (obsolete/step2d_LF_AM3.h.py: fast-time
+ * averages :778-846, free surface :933-1020, pressure gradient :1120-1230, Coriolis
+ * :1503-1530, bottom stress :2242-2262, surface stress :2598-2612, momentum step
+ * :2640-2760; quadratic drag nonlinear/set_vbc.py:16-41), for closed rectangular basins:
+ * ROMS signs, forward/backward Euler on a loop's first substep, leapfrog predictor with the
+ * time-filtered surface 0.68 zeta(n) + 0.16 (zeta(n-1) + zeta(n+1*)), AM3 corrector, Coriolis,
+ * surface stress and quadratic bottom drag in the momentum right-hand side, zero-gradient
+ * free surface and zero normal velocity at the walls, and the FP64 fast-time averages
+ * Zt_avg1, DU_avg1, DV_avg1, DU_avg2, DV_avg2.  Slots of the sf_state2d: zeta/ubar/vbar
+ * [0] = n-1, [1] = n, [2] = scratch for the predicted n+1*; rzeta/rubar/rvbar [0] = n-1,
+ * [1] = n.  Each substep writes n+1 over n-1 and swaps the two slot pointers in *s. */
+/* nfast+1 substeps of one baroclinic step (the last one only accumulates the averages, as in
+ * ROMS); W1, W2: ROMS-indexed averaging weights (W1[m] = weight(1, m), m = 0..nfast+1, W2
+ * likewise); sustr, svstr: kinematic surface stress (m2/s2) at U and V faces; rdrag2:
+ * quadratic drag coefficient. */
+int sf_roms_barotropic_loop(sf_ctx *ctx, sf_state2d *s, double *DU_avg2, double *DV_avg2,
+                            const void *sustr, const void *svstr, double rdrag2, int nfast,
+                            const double *W1, const double *W2, double dtfast, sf_stream stream);
+/* One 2D-only step (predictor + corrector, no averages): the ROMS-form counterpart of
+ * main2d's step (nonlinear/main2d.py:9-88); first selects forward/backward Euler. */
+int sf_roms_step2d(sf_ctx *ctx, sf_state2d *s, const void *sustr, const void *svstr,
+                   double rdrag2, double dtfast, int first, sf_stream stream);
+/* Surface stress on the top level of the 3D momentum right-hand side: ru[N-1] += sustr
+ * om_u on_u, rv[N-1] += svstr om_v on_v (ROMS's ru includes the stress terms). */
+int sf_roms_stress3d(sf_ctx *ctx, void *ru, void *rv, const void *sustr, const void *svstr,
+                     sf_stream stream);
+/* Closed walls for the 3D velocities: u = 0 on the west and east U faces, v = 0 on the south
+ * and north V faces, every level. */
+int sf_roms_closed_walls(sf_ctx *ctx, void *u, void *v, sf_stream stream);
 
 /* ---- 3D right-hand side, nonlinear/rhs.py:16-93 + nonlinear/rhs_kernels.cpp ------------ */
 /* rhs3d: ru = rv = 0, addCoriolis (:7-35), horizontalAdvection (:71-132), verticalAdvection

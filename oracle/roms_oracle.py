@@ -1,0 +1,258 @@
+"""ROMS-form barotropic step, restated in NumPy FP64 (TEST INFRASTRUCTURE: the oracle).
+
+The reference's runnable 2D kernels (modules/mod_cppkernels.cpp) carry no forcing, reversed
+signs and a mis-bound corrector; its ROMS transcription of the full step
+(obsolete/step2d_LF_AM3.h.py) and of the bottom stress (nonlinear/set_vbc.py) do not parse.
+The benchmark configurations need that physics (wind stress, quadratic bottom drag,
+Coriolis), so the package has a second, ROMS-form barotropic step; this module restates it
+from the pseudo-code, for closed rectangular basins (no masks, no wet/dry, no open
+boundaries), vectorised over the grid:
+
+* total depth and face fluxes DUon = ubar (D_i + D_i-1)/2 on_u, DVom likewise (:690-745);
+* fast-time averages accumulated in the predictor from the previous corrector's fields:
+  Zt_avg1 += W1[iif-1] zeta, DU_avg1 += W1[iif-1] DUon, DU_avg2 += (8/12 W2[iif]
+  - 1/12 W2[iif+1]) DUon, reset at iif = 1 with DU_avg2 = -1/12 W2[2] DUon; in the corrector
+  DU_avg2 += 5/12 W2[iif] DUon (W2[1] at iif = 1) (:778-846); W1, W2 are indexed as ROMS
+  indexes weight(1:2, 0:256) (roms_weights); the predictor of substep nfast+1 only
+  accumulates (:923-926);
+* free surface: rhs_zeta = (DUon_i - DUon_i+1) + (DVom_j - DVom_j+1); predictor
+  zeta_new = zeta(kstp) + pm pn cff1 rhs_zeta with cff1 = dtfast at the first substep of a
+  loop (forward Euler, kstp = n) and 2 dtfast after (leapfrog, kstp = n-1); corrector AM3
+  zeta_new = zeta(n) + pm pn dtfast (5/12 rhs + 8/12 rzeta(n) - 1/12 rzeta(n-1)) (backward
+  Euler at the first substep); the pressure-gradient surface zwrk = 0.5 (zeta(kstp) +
+  zeta_new) first, 0.68 zeta(n) + 0.16 (zeta(n-1) + zeta_new) in the predictor, 0.6 zeta_new +
+  0.4 zeta(n+1*) in the corrector (:933-1020); zero-gradient ring (closed walls);
+* momentum right-hand side at U/V faces: pressure gradient 0.5 g on_u ((h_i-1 + h_i)
+  (zwrk_i-1 - zwrk_i) + (zwrk_i-1^2 - zwrk_i^2)) (:1120-1160); Coriolis from
+  UFx = 0.5 Drhs fomn (vbar_j + vbar_j+1) at rho points, + (UFx_i + UFx_i-1)/2 for ubar and
+  - (VFe_j + VFe_j-1)/2 for vbar (:1503-1530); surface stress + sustr om_u on_u (:2598-2612);
+  quadratic bottom drag - rdrag2 ubar sqrt(ubar^2 + v_u^2) om_u on_u with v_u the four-point
+  average of vbar at the U face (set_vbc.py:16-41, step2d_LF_AM3.h.py:2242-2262);
+* momentum step (:2640-2760): ubar_new = (ubar(kstp) (Dstp_i + Dstp_i-1) + cff cff1 rhs) /
+  (Dnew_i + Dnew_i-1), cff = (pm_i + pm_i-1)(pn_i + pn_i-1), cff1 = dtfast/2 (first),
+  dtfast (leapfrog predictor), and in the corrector dtfast/2 (5/12 rhs + 8/12 rubar(n)
+  - 1/12 rubar(n-1)); normal velocities on the walls are 0.
+
+Index conventions follow the reference's arrays: (J, I) = (M+1, L+1) rho grid, ubar(j, i) on the
+west face of rho (j, i), vbar(j, i) on its south face; interior rho 1..I-2 x 1..J-2, U faces
+i = 2..I-2 (walls at i = 1 and I-1), V faces j = 2..J-2 (walls at j = 1 and J-1).
+
+Time levels: each field has slots n-1, n and a scratch for the predicted n+1*; the corrector
+writes n+1 over n-1, then n-1 <- n and n <- n+1 (a swap of the two slots).
+"""
+import numpy as np
+
+G_GRAV = 10.0      # modules/mod_constants.py:26
+
+
+def roms_weights(nfast, w1):
+    """ROMS-indexed (W1, W2) from the primary weights w1 of set_weights: the reference's array
+    holds ROMS weight(1, m) at index m-1 (set_weights.py:96-104 fills it from iter = 1), so
+    W1[m] = w1[m-1] (W1[0] = 0); W2[i] = sum_{j=i..nfast} W1[j] (ROMS's secondary weights,
+    set_weights.py:165-172 in ROMS's index range), normalised to sum 1 over i = 1..nfast."""
+    W1 = np.zeros(len(w1) + 1)
+    W1[1:] = np.asarray(w1, np.float64)
+    W2 = np.zeros_like(W1)
+    for i in range(1, nfast + 1):
+        W2[i] = float(np.sum(W1[i:nfast + 1]))
+    W2[1:nfast + 1] /= float(np.sum(W2[1:nfast + 1]))
+    return W1, W2
+
+
+class State:
+    """Barotropic state of one basin (FP64 host arrays, shape (J, I))."""
+
+    def __init__(self, J, I):
+        z = lambda: np.zeros((J, I))
+        self.zeta = [z(), z()]          # [n-1, n]
+        self.ubar = [z(), z()]
+        self.vbar = [z(), z()]
+        self.rzeta = [z(), z()]
+        self.rubar = [z(), z()]
+        self.rvbar = [z(), z()]
+        self.zeta_p, self.ubar_p, self.vbar_p = z(), z(), z()   # predicted n+1*
+        self.Zt_avg1, self.DU_avg1, self.DV_avg1, self.DU_avg2, self.DV_avg2 = z(), z(), z(), z(), z()
+
+
+def _fluxes(g, zeta, ubar, vbar):
+    D = zeta + g["h"]
+    DU = np.zeros_like(D)
+    DV = np.zeros_like(D)
+    DU[:, 1:] = ubar[:, 1:] * (0.5 * (D[:, 1:] + D[:, :-1])) * g["on_u"][:, 1:]
+    DV[1:, :] = vbar[1:, :] * (0.5 * (D[1:, :] + D[:-1, :])) * g["om_v"][1:, :]
+    return D, DU, DV
+
+
+def _rhs_zeta(DU, DV):
+    r = np.zeros_like(DU)
+    r[1:-1, 1:-1] = ((DU[1:-1, 1:-1] - DU[1:-1, 2:]) + (DV[1:-1, 1:-1] - DV[2:, 1:-1]))
+    return r
+
+
+def _ring(z):
+    """Zero-gradient free surface on the boundary ring (closed walls)."""
+    z[0, :] = z[1, :]
+    z[-1, :] = z[-2, :]
+    z[:, 0] = z[:, 1]
+    z[:, -1] = z[:, -2]
+
+
+def _rhs_uv(g, zwrk, D, ubar, vbar, sustr, svstr, rdrag2):
+    """rhs_ubar, rhs_vbar on the interior faces (zero elsewhere)."""
+    h, fomn = g["h"], g["fomn"]
+    J, I = h.shape
+    ru = np.zeros_like(h)
+    rv = np.zeros_like(h)
+    cff1 = 0.5 * G_GRAV
+    gz, gz2 = zwrk, zwrk * zwrk
+    # U faces i = 2..I-2, rows j = 1..J-2
+    sl_j, sl_i = slice(1, J - 1), slice(2, I - 1)
+    sl_im = slice(1, I - 2)
+    pg = cff1 * g["on_u"][sl_j, sl_i] * ((h[sl_j, sl_im] + h[sl_j, sl_i]) * (gz[sl_j, sl_im] - gz[sl_j, sl_i])
+                                         + (gz2[sl_j, sl_im] - gz2[sl_j, sl_i]))
+    UFx = 0.5 * D * fomn * np.concatenate([vbar[:-1] + vbar[1:], np.zeros((1, I))], axis=0)
+    cor = 0.5 * (UFx[sl_j, sl_i] + UFx[sl_j, sl_im])
+    area_u = 4.0 / ((g["pm"][sl_j, sl_i] + g["pm"][sl_j, sl_im]) * (g["pn"][sl_j, sl_i] + g["pn"][sl_j, sl_im]))
+    v4 = 0.25 * (vbar[sl_j, sl_i] + vbar[2:J, sl_i] + vbar[sl_j, sl_im] + vbar[2:J, sl_im])
+    ub = ubar[sl_j, sl_i]
+    bustr = rdrag2 * ub * np.sqrt(ub * ub + v4 * v4)
+    ru[sl_j, sl_i] = pg + cor + (sustr[sl_j, sl_i] - bustr) * area_u
+    # V faces j = 2..J-2, columns i = 1..I-2
+    sv_j, sv_i = slice(2, J - 1), slice(1, I - 1)
+    sv_jm = slice(1, J - 2)
+    pgv = cff1 * g["om_v"][sv_j, sv_i] * ((h[sv_jm, sv_i] + h[sv_j, sv_i]) * (gz[sv_jm, sv_i] - gz[sv_j, sv_i])
+                                          + (gz2[sv_jm, sv_i] - gz2[sv_j, sv_i]))
+    VFe = 0.5 * D * fomn * np.concatenate([ubar[:, :-1] + ubar[:, 1:], np.zeros((J, 1))], axis=1)
+    corv = -0.5 * (VFe[sv_j, sv_i] + VFe[sv_jm, sv_i])
+    area_v = 4.0 / ((g["pm"][sv_j, sv_i] + g["pm"][sv_jm, sv_i]) * (g["pn"][sv_j, sv_i] + g["pn"][sv_jm, sv_i]))
+    u4 = 0.25 * (ubar[sv_j, sv_i] + ubar[sv_j, 2:I] + ubar[sv_jm, sv_i] + ubar[sv_jm, 2:I])
+    vb = vbar[sv_j, sv_i]
+    bvstr = rdrag2 * vb * np.sqrt(u4 * u4 + vb * vb)
+    rv[sv_j, sv_i] = pgv + corv + (svstr[sv_j, sv_i] - bvstr) * area_v
+    return ru, rv
+
+
+def _step_uv(g, ustp, vstp, Dstp, Dnew, rhs_u, rhs_v, cff1):
+    """ubar_new = (ubar(kstp) (Dstp_i + Dstp_i-1) + cff cff1 rhs) / (Dnew_i + Dnew_i-1) on the
+    interior faces; walls and the ring stay 0."""
+    J, I = Dstp.shape
+    un = np.zeros_like(Dstp)
+    vn = np.zeros_like(Dstp)
+    pm, pn = g["pm"], g["pn"]
+    sj, si, sim = slice(1, J - 1), slice(2, I - 1), slice(1, I - 2)
+    cff = (pm[sj, si] + pm[sj, sim]) * (pn[sj, si] + pn[sj, sim])
+    un[sj, si] = (ustp[sj, si] * (Dstp[sj, si] + Dstp[sj, sim]) + cff * cff1 * rhs_u[sj, si]) / (Dnew[sj, si] + Dnew[sj, sim])
+    vj, vi, vjm = slice(2, J - 1), slice(1, I - 1), slice(1, J - 2)
+    cffv = (pm[vj, vi] + pm[vjm, vi]) * (pn[vj, vi] + pn[vjm, vi])
+    vn[vj, vi] = (vstp[vj, vi] * (Dstp[vj, vi] + Dstp[vjm, vi]) + cffv * cff1 * rhs_v[vj, vi]) / (Dnew[vj, vi] + Dnew[vjm, vi])
+    return un, vn
+
+
+def predictor(g, S, first, dtfast, sustr, svstr, rdrag2, acc=None, step=True):
+    """acc: None (no fast-time averages: the 2D-only driver), "reset" (first substep of a
+    loop) or (c1, c2), the weights of this substep's accumulation; step False: accumulate
+    only (the loop's auxiliary last substep)."""
+    zn, un, vn = S.zeta[1], S.ubar[1], S.vbar[1]
+    D, DU, DV = _fluxes(g, zn, un, vn)
+    if acc is not None:
+        if acc[0] == "reset":
+            S.Zt_avg1[...] = 0.0
+            S.DU_avg1[...] = 0.0
+            S.DV_avg1[...] = 0.0
+            S.DU_avg2[...] = acc[1] * DU
+            S.DV_avg2[...] = acc[1] * DV
+        else:
+            c1, c2 = acc
+            S.Zt_avg1 += c1 * zn
+            S.DU_avg1 += c1 * DU
+            S.DV_avg1 += c1 * DV
+            S.DU_avg2 += c2 * DU
+            S.DV_avg2 += c2 * DV
+    if not step:
+        return
+    rz = _rhs_zeta(DU, DV)
+    kstp = 1 if first else 0
+    cff1 = dtfast if first else 2.0 * dtfast
+    zs = S.zeta[kstp]
+    znew = zs + g["pm"] * g["pn"] * cff1 * rz
+    _ring(znew)
+    zwrk = 0.5 * (zs + znew) if first else 0.68 * zn + 0.16 * (zs + znew)
+    S.rzeta[1][...] = rz
+    ru, rv = _rhs_uv(g, zwrk, D, un, vn, sustr, svstr, rdrag2)
+    S.rubar[1][...] = ru
+    S.rvbar[1][...] = rv
+    Dstp = zs + g["h"]
+    Dnew = znew + g["h"]
+    up, vp = _step_uv(g, S.ubar[kstp], S.vbar[kstp], Dstp, Dnew, ru, rv,
+                      0.5 * dtfast if first else dtfast)
+    S.zeta_p[...] = znew
+    S.ubar_p[...] = up
+    S.vbar_p[...] = vp
+
+
+def corrector(g, S, first, dtfast, sustr, svstr, rdrag2, c2=None):
+    """c2: the weight of this substep's DU_avg2 term (None: no averages)."""
+    D, DU, DV = _fluxes(g, S.zeta_p, S.ubar_p, S.vbar_p)
+    if c2 is not None:
+        S.DU_avg2 += c2 * DU
+        S.DV_avg2 += c2 * DV
+    rz = _rhs_zeta(DU, DV)
+    pmn = g["pm"] * g["pn"]
+    if first:
+        znew = S.zeta[1] + pmn * dtfast * rz
+        zwrk = 0.5 * (S.zeta[1] + znew)
+    else:
+        znew = S.zeta[1] + pmn * dtfast * ((5.0 / 12.0) * rz + (8.0 / 12.0) * S.rzeta[1]
+                                           - (1.0 / 12.0) * S.rzeta[0])
+        zwrk = 0.6 * znew + 0.4 * S.zeta_p
+    _ring(znew)
+    ru, rv = _rhs_uv(g, zwrk, D, S.ubar_p, S.vbar_p, sustr, svstr, rdrag2)
+    if first:
+        fu, fv, c = ru, rv, 0.5 * dtfast
+    else:
+        fu = (5.0 / 12.0) * ru + (8.0 / 12.0) * S.rubar[1] - (1.0 / 12.0) * S.rubar[0]
+        fv = (5.0 / 12.0) * rv + (8.0 / 12.0) * S.rvbar[1] - (1.0 / 12.0) * S.rvbar[0]
+        c = 0.5 * dtfast
+    Dstp = S.zeta[1] + g["h"]
+    Dnew = znew + g["h"]
+    un_, vn_ = _step_uv(g, S.ubar[1], S.vbar[1], Dstp, Dnew, fu, fv, c)
+    # n+1 over n-1, then swap: n-1 <- n, n <- n+1
+    S.zeta = [S.zeta[1], znew]
+    S.ubar = [S.ubar[1], un_]
+    S.vbar = [S.vbar[1], vn_]
+    S.rzeta = [S.rzeta[1], S.rzeta[0]]
+    S.rubar = [S.rubar[1], S.rubar[0]]
+    S.rvbar = [S.rvbar[1], S.rvbar[0]]
+
+
+def loop_weights(iif, W1, W2):
+    """(predictor accumulation, corrector DU_avg2 weight) of substep iif (:778-846)."""
+    if iif == 1:
+        return ("reset", (-1.0 / 12.0) * W2[2]), W2[1]
+    return ((W1[iif - 1], (8.0 / 12.0) * W2[iif] - (1.0 / 12.0) * W2[iif + 1]),
+            (5.0 / 12.0) * W2[iif])
+
+
+def barotropic_loop(g, S, nfast, W1, W2, dtfast, sustr, svstr, rdrag2):
+    """nfast + 1 substeps: predictor and corrector for iif = 1..nfast, and the accumulating
+    predictor of iif = nfast+1 (ROMS does no time stepping in that one)."""
+    for iif in range(1, nfast + 2):
+        pa, c2 = loop_weights(iif, W1, W2)
+        predictor(g, S, iif == 1, dtfast, sustr, svstr, rdrag2, acc=pa, step=iif <= nfast)
+        if iif <= nfast:
+            corrector(g, S, iif == 1, dtfast, sustr, svstr, rdrag2, c2=c2)
+
+
+def main2d(g, S, nsteps, dtfast, sustr, svstr, rdrag2, first=True):
+    """2D-only driver: predictor + corrector per step, forward/backward Euler on the run's
+    first step only, no fast-time averages."""
+    for n in range(nsteps):
+        f = first and n == 0
+        predictor(g, S, f, dtfast, sustr, svstr, rdrag2)
+        corrector(g, S, f, dtfast, sustr, svstr, rdrag2)
+
+
+def volume(g, zeta):
+    """Total water volume above the rest level over the interior cells (closed basin)."""
+    a = 1.0 / (g["pm"] * g["pn"])
+    return float(np.sum((zeta * a)[1:-1, 1:-1]))

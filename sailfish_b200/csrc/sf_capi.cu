@@ -972,6 +972,155 @@ int sf_barotropic_loop(sf_ctx *c, sf_state2d *st, int nsub, const double *weight
     return SF_OK;
 }
 
+// ---- ROMS-form barotropic step (sf_roms.cuh) ----------------------------------------------
+}  // extern "C"
+
+namespace {
+// One phase (0 predictor, 1 corrector) of the ROMS-form substep on the slots of st:
+// [0] = n-1, [1] = n, [2] = the predicted n+1*.
+template <typename R>
+cudaError_t roms_phase(const sf_ctx *c, const sf_state2d *st, double *DU2, double *DV2,
+                       const void *sustr, const void *svstr, double rdrag2, double dtfast,
+                       int phase, int first, int acc, double c1, double c2, int step,
+                       cudaStream_t s) {
+    sf::RomsArgs<R> a;
+    a.zb = (const R *)st->zeta[0];
+    a.zn = (const R *)st->zeta[1];
+    a.zp = (const R *)st->zeta[2];
+    a.ub = (const R *)st->ubar[0];
+    a.un = (const R *)st->ubar[1];
+    a.up = (const R *)st->ubar[2];
+    a.vb = (const R *)st->vbar[0];
+    a.vn = (const R *)st->vbar[1];
+    a.vp = (const R *)st->vbar[2];
+    const int out = phase == 0 ? 2 : 0;
+    a.zout = (R *)st->zeta[out];
+    a.uout = (R *)st->ubar[out];
+    a.vout = (R *)st->vbar[out];
+    const int kstp = phase == 0 ? (first ? 1 : 0) : 1;
+    a.zkstp = (const R *)st->zeta[kstp];
+    a.ukstp = (const R *)st->ubar[kstp];
+    a.vkstp = (const R *)st->vbar[kstp];
+    const int krhs = phase == 0 ? 1 : 2;
+    a.zrhs = (const R *)st->zeta[krhs];
+    a.urhs = (const R *)st->ubar[krhs];
+    a.vrhs = (const R *)st->vbar[krhs];
+    a.rz_n = (R *)st->rzeta[1];
+    a.ru_n = (R *)st->rubar[1];
+    a.rv_n = (R *)st->rvbar[1];
+    a.rz_b = (const R *)st->rzeta[0];
+    a.ru_b = (const R *)st->rubar[0];
+    a.rv_b = (const R *)st->rvbar[0];
+    a.sustr = (const R *)sustr;
+    a.svstr = (const R *)svstr;
+    a.Zt = st->Zt_avg1;
+    a.DU1 = st->DU_avg1;
+    a.DV1 = st->DV_avg1;
+    a.DU2 = DU2;
+    a.DV2 = DV2;
+    a.rdrag2 = rdrag2;
+    a.dtfast = dtfast;
+    a.c1 = c1;
+    a.c2 = c2;
+    a.phase = phase;
+    a.first = first;
+    a.acc = acc;
+    a.step = step;
+    return sf::Ops<R>::roms_phase(c, a, s);
+}
+
+void roms_swap(sf_state2d *st) {   // n+1 (written over n-1) becomes n, n becomes n-1
+    void **arrs[6] = {st->zeta, st->ubar, st->vbar, st->rzeta, st->rubar, st->rvbar};
+    for (void **a : arrs) {
+        void *t = a[0];
+        a[0] = a[1];
+        a[1] = t;
+    }
+}
+
+int roms_check(const sf_ctx *c, const sf_state2d *st, const void *sustr, const void *svstr) {
+    if (!c) return fail(SF_EINVAL, "null context");
+    if (c->nmem != 1) return fail(SF_EUNSUPPORTED, "the ROMS-form step runs single grids");
+    if (!st || !sustr || !svstr) return fail(SF_EINVAL, "null state or stress");
+    for (void *const *a : {st->zeta, st->ubar, st->vbar})
+        for (int k = 0; k < 3; ++k)
+            if (!a[k]) return fail(SF_EINVAL, "null 2D slot");
+    for (void *const *a : {st->rzeta, st->rubar, st->rvbar})
+        for (int k = 0; k < 2; ++k)
+            if (!a[k]) return fail(SF_EINVAL, "null tendency slot");
+    return SF_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int sf_roms_barotropic_loop(sf_ctx *c, sf_state2d *st, double *DU_avg2, double *DV_avg2,
+                            const void *sustr, const void *svstr, double rdrag2, int nfast,
+                            const double *W1, const double *W2, double dtfast, sf_stream s) {
+    int rc = roms_check(c, st, sustr, svstr);
+    if (rc) return rc;
+    if (!DU_avg2 || !DV_avg2 || !st->Zt_avg1 || !st->DU_avg1 || !st->DV_avg1 || !W1 || !W2)
+        return fail(SF_EINVAL, "null accumulator or weights");
+    if (nfast < 1 || nfast > 254) return fail(SF_EINVAL, "nfast must be in [1, 254]");
+    for (int iif = 1; iif <= nfast + 1; ++iif) {
+        // fast-time averages (step2d_LF_AM3.h.py:778-846), ROMS-indexed weights
+        const int acc = iif == 1 ? 2 : 1;
+        const double pc1 = iif == 1 ? 0.0 : W1[iif - 1];
+        const double pc2 = iif == 1 ? (-1.0 / 12.0) * W2[2]
+                                    : (8.0 / 12.0) * W2[iif] - (1.0 / 12.0) * W2[iif + 1];
+        const double cc2 = iif == 1 ? W2[1] : (5.0 / 12.0) * W2[iif];
+        const int step = iif <= nfast, first = iif == 1;
+        cudaError_t e = c->prec == SF_FP64
+            ? roms_phase<double>(c, st, DU_avg2, DV_avg2, sustr, svstr, rdrag2, dtfast, 0, first,
+                                 acc, pc1, pc2, step, S(s))
+            : roms_phase<float>(c, st, DU_avg2, DV_avg2, sustr, svstr, rdrag2, dtfast, 0, first,
+                                acc, pc1, pc2, step, S(s));
+        if (e == cudaSuccess && step)
+            e = c->prec == SF_FP64
+                ? roms_phase<double>(c, st, DU_avg2, DV_avg2, sustr, svstr, rdrag2, dtfast, 1,
+                                     first, 1, 0.0, cc2, 1, S(s))
+                : roms_phase<float>(c, st, DU_avg2, DV_avg2, sustr, svstr, rdrag2, dtfast, 1,
+                                    first, 1, 0.0, cc2, 1, S(s));
+        if (e != cudaSuccess) return cuda_fail(e, "sf_roms_barotropic_loop");
+        if (step) roms_swap(st);
+    }
+    return SF_OK;
+}
+
+int sf_roms_step2d(sf_ctx *c, sf_state2d *st, const void *sustr, const void *svstr,
+                   double rdrag2, double dtfast, int first, sf_stream s) {
+    int rc = roms_check(c, st, sustr, svstr);
+    if (rc) return rc;
+    cudaError_t e = cudaSuccess;
+    for (int phase = 0; phase < 2 && e == cudaSuccess; ++phase)
+        e = c->prec == SF_FP64
+            ? roms_phase<double>(c, st, nullptr, nullptr, sustr, svstr, rdrag2, dtfast, phase,
+                                 first ? 1 : 0, 0, 0.0, 0.0, 1, S(s))
+            : roms_phase<float>(c, st, nullptr, nullptr, sustr, svstr, rdrag2, dtfast, phase,
+                                first ? 1 : 0, 0, 0.0, 0.0, 1, S(s));
+    if (e != cudaSuccess) return cuda_fail(e, "sf_roms_step2d");
+    roms_swap(st);
+    return SF_OK;
+}
+
+int sf_roms_stress3d(sf_ctx *c, void *ru, void *rv, const void *sustr, const void *svstr,
+                     sf_stream s) {
+    if (!ru || !rv || !sustr || !svstr) return fail(SF_EINVAL, "null argument");
+    return dispatch(c, "sf_roms_stress3d", [&](auto *t) {
+        using R = std::remove_pointer_t<decltype(t)>;
+        return sf::Ops<R>::roms_stress3d(c, (R *)ru, (R *)rv, (const R *)sustr,
+                                         (const R *)svstr, S(s));
+    });
+}
+
+int sf_roms_closed_walls(sf_ctx *c, void *u, void *v, sf_stream s) {
+    if (!u || !v) return fail(SF_EINVAL, "null argument");
+    return dispatch(c, "sf_roms_closed_walls", [&](auto *t) {
+        using R = std::remove_pointer_t<decltype(t)>;
+        return sf::Ops<R>::roms_walls3d(c, (R *)u, (R *)v, S(s));
+    });
+}
+
 // ---- 3D ---------------------------------------------------------------------------------
 int sf_rhs3d(sf_ctx *c, const void *u, const void *v, const void *Huon, const void *Hvom,
              const void *W, const void *Hz, void *ru, void *rv, sf_stream s) {

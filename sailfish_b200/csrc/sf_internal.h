@@ -132,8 +132,10 @@ struct sf_ctx {
     int *pred_counter = nullptr;
     int pred_ok = 0;
     int use_fused = 1;
-    // bulk-copy staging (cp.async.bulk) in the kernels that have it (sf_ctx_set_bulk)
-    int use_bulk = 1;
+    // bulk-copy staging (cp.async.bulk) in the kernels that have it (sf_ctx_set_bulk); off
+    // by default: on basin4 the column solve took 2.08 ms with it against 1.65 ms with
+    // per-element cp.async staging
+    int use_bulk = 0;
     cudaStream_t cap = nullptr;
     double *d_bcval = nullptr;
     sf_loop_graph graphs[3];
@@ -194,6 +196,28 @@ inline cudaError_t launch_dep(const sf_ctx *c, void (*kern)(KArgs...), dim3 grid
     return cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
 }
 
+// Arguments of one phase of the ROMS-form barotropic substep (kernels in sf_roms.cuh).
+template <typename R>
+struct RomsArgs {
+    const R *zb, *zn, *zp;          // zeta at n-1, n and the predicted n+1*
+    const R *ub, *un, *up;
+    const R *vb, *vn, *vp;
+    R *zout, *uout, *vout;          // the phase's output slots (p in the predictor, b in the corrector)
+    const R *zkstp, *ukstp, *vkstp; // the momentum step's old level (kstp)
+    const R *zrhs, *urhs, *vrhs;    // the level the right-hand side is evaluated at (krhs)
+    R *rz_n, *ru_n, *rv_n;          // tendencies of level n (written by the predictor)
+    const R *rz_b, *ru_b, *rv_b;    // tendencies of level n-1
+    const R *sustr, *svstr;         // kinematic surface stress at U / V faces (m2/s2)
+    double *Zt, *DU1, *DV1, *DU2, *DV2;
+    double rdrag2, dtfast;
+    double c1, c2;                  // accumulation weights of this phase
+    int phase;                      // 0 predictor, 1 corrector
+    int first;                      // first substep of a loop: forward / backward Euler
+    int acc;                        // 0 none, 1 accumulate, 2 reset (predictor of substep 1)
+    int step;                       // 0: the predictor only accumulates (substep nfast+1)
+};
+
+
 // Launchers, one explicit instantiation per precision (FP64 in a translation unit built
 // without FMA contraction, so that it reproduces the reference's IEEE evaluation).
 template <typename R>
@@ -253,6 +277,11 @@ struct Ops {
                                    int correct, double *out, cudaStream_t s);
     static cudaError_t analytic_bvf(const sf_ctx *c, const R *z_w, double dT, double zscale,
                                     double galpha, R *bvf, cudaStream_t s);
+    // the ROMS-form barotropic step (sf_roms.cuh)
+    static cudaError_t roms_phase(const sf_ctx *c, const RomsArgs<R> &a, cudaStream_t s);
+    static cudaError_t roms_stress3d(const sf_ctx *c, R *ru, R *rv, const R *sustr,
+                                     const R *svstr, cudaStream_t s);
+    static cudaError_t roms_walls3d(const sf_ctx *c, R *u, R *v, cudaStream_t s);
 };
 
 extern template struct Ops<double>;

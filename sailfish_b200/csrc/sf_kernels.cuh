@@ -2136,3 +2136,5 @@ cudaError_t Ops<R>::analytic_bvf(const sf_ctx *c, const R *z_w, double dT, doubl
 }
 
 }  // namespace sf
+
+#include "sf_roms.cuh"

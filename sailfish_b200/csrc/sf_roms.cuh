@@ -1,0 +1,224 @@
+// ROMS-form barotropic step (the "roms" semantics): the free-surface / depth-integrated
+// momentum step of ROMS's step2d_LF_AM3, which the reference carries only as untranslated
+// Fortran (obsolete/step2d_LF_AM3.h.py), with its 2D Coriolis (:1503-1530), surface stress
+// (:2598-2612), quadratic bottom drag (nonlinear/set_vbc.py:16-41) and the fast-time averages
+// Zt_avg1, DU_avg1/2, DV_avg1/2 (:778-846), for closed rectangular basins.  It exists beside
+// the reference-semantics kernels because the benchmark configurations need forcing, Coriolis
+// and a stable step, none of which the reference's runnable 2D kernels have.
+//
+// Index conventions as the rest of the package: flat p = j*I + i over (M+1) x (L+1) rho points;
+// ubar(p) on the west face of rho p, vbar(p) on its south face; interior rho i = 1..I-2,
+// j = 1..J-2; interior U faces i = 2..I-2 (walls i = 1, I-1), V faces j = 2..J-2.
+//
+// A substep is four launches: the predictor's free surface (k_roms_zeta, phase 0), its
+// momentum (k_roms_mom, phase 0), the corrector's free surface (phase 1) and momentum
+// (phase 1).  Time levels: slots b (n-1), n and p (the predicted n+1*); the corrector writes
+// n+1 into b and the host swaps b and n.  Every expression keeps the operand order of the
+// oracle's restatement (oracle/roms_oracle.py), so the FP64 build (no FMA contraction)
+// reproduces it bit for bit; the fast-time averages are FP64 in both precisions.
+#pragma once
+
+namespace sf {
+
+
+// DUon at the U face p (0 on column 0) and DVom at the V face p (0 on row 0), from zeta, ubar, vbar
+template <typename R>
+__device__ __forceinline__ R roms_du(const Geo<R> &g, const R *z, const R *u, long p, int i) {
+    if (i < 1) return R(0);
+    const R Dp = z[p] + g.h[p], Dw = z[p - 1] + g.h[p - 1];
+    return (u[p] * (R(0.5) * (Dp + Dw))) * g.on_u[p];
+}
+template <typename R>
+__device__ __forceinline__ R roms_dv(const Geo<R> &g, const R *z, const R *v, long p, int j) {
+    if (j < 1) return R(0);
+    const R Dp = z[p] + g.h[p], Ds = z[p - g.I] + g.h[p - g.I];
+    return (v[p] * (R(0.5) * (Dp + Ds))) * g.om_v[p];
+}
+// rhs_zeta at interior rho q: (DUon_q - DUon_q+1) + (DVom_q - DVom_q+I)
+template <typename R>
+__device__ __forceinline__ R roms_rz(const Geo<R> &g, const R *z, const R *u, const R *v, long q,
+                                     int i, int j) {
+    return (roms_du(g, z, u, q, i) - roms_du(g, z, u, q + 1, i + 1)) +
+           (roms_dv(g, z, v, q, j) - roms_dv(g, z, v, q + g.I, j + 1));
+}
+
+// Free surface of a phase at rho p.  Ring nodes take the value of the nearest interior node
+// (zero gradient at closed walls), computed here from the inputs.
+template <typename R>
+__global__ void __launch_bounds__(256) k_roms_zeta(Geo<R> g, RomsArgs<R> a) {
+    const long p = tid_flat();
+    if (p >= g.s2) return;
+    const int j = fdiv((int)p, g.dI), i = (int)p - j * g.I;
+    const long I = g.I;
+    if (a.acc) {   // the fast-time averages at rho p, its west U face and its south V face
+        const R *z = a.phase == 0 ? a.zn : a.zp;
+        const R *u = a.phase == 0 ? a.un : a.up;
+        const R *v = a.phase == 0 ? a.vn : a.vp;
+        const double du = (double)roms_du(g, z, u, p, i), dv = (double)roms_dv(g, z, v, p, j);
+        if (a.phase == 0) {
+            if (a.acc == 2) {
+                a.Zt[p] = 0.0;
+                a.DU1[p] = 0.0;
+                a.DV1[p] = 0.0;
+                a.DU2[p] = a.c2 * du;
+                a.DV2[p] = a.c2 * dv;
+            } else {
+                a.Zt[p] = a.Zt[p] + a.c1 * (double)z[p];
+                a.DU1[p] = a.DU1[p] + a.c1 * du;
+                a.DV1[p] = a.DV1[p] + a.c1 * dv;
+                a.DU2[p] = a.DU2[p] + a.c2 * du;
+                a.DV2[p] = a.DV2[p] + a.c2 * dv;
+            }
+        } else {
+            a.DU2[p] = a.DU2[p] + a.c2 * du;
+            a.DV2[p] = a.DV2[p] + a.c2 * dv;
+        }
+    }
+    if (!a.step) return;
+    const int qi = i < 1 ? 1 : (i > g.I - 2 ? g.I - 2 : i);
+    const int qj = j < 1 ? 1 : (j > g.J - 2 ? g.J - 2 : j);
+    const long q = (long)qj * I + qi;
+    const R pmn = g.pm[q] * g.pn[q];
+    R znew;
+    if (a.phase == 0) {
+        const R rz = roms_rz(g, a.zn, a.un, a.vn, q, qi, qj);
+        const R cff1 = a.first ? (R)a.dtfast : (R)(2.0 * a.dtfast);
+        znew = a.zkstp[q] + (pmn * cff1) * rz;
+        if (q == p) a.rz_n[p] = rz;
+    } else {
+        const R rz = roms_rz(g, a.zp, a.up, a.vp, q, qi, qj);
+        const R dt = (R)a.dtfast;
+        if (a.first)
+            znew = a.zn[q] + (pmn * dt) * rz;
+        else
+            znew = a.zn[q] + (pmn * dt) * ((R(5.0 / 12.0) * rz + R(8.0 / 12.0) * a.rz_n[q]) -
+                                          R(1.0 / 12.0) * a.rz_b[q]);
+    }
+    a.zout[p] = znew;
+    if (a.phase == 0 && q != p) a.rz_n[p] = R(0);
+}
+
+// The pressure-gradient surface zwrk of a phase at rho q (zout holds the phase's new zeta).
+template <typename R>
+__device__ __forceinline__ R roms_zwrk(const RomsArgs<R> &a, long q) {
+    const R znew = a.zout[q];
+    if (a.first) return R(0.5) * (a.zkstp[q] + znew);
+    if (a.phase == 0) return R(0.68) * a.zn[q] + R(0.16) * (a.zkstp[q] + znew);
+    return R(0.6) * znew + R(0.4) * a.zp[q];
+}
+
+// Momentum of a phase at the U and V faces of p (0 on walls and the ring).
+template <typename R>
+__global__ void __launch_bounds__(256) k_roms_mom(Geo<R> g, RomsArgs<R> a) {
+    const long p = tid_flat();
+    if (p >= g.s2) return;
+    const int j = fdiv((int)p, g.dI), i = (int)p - j * g.I;
+    const long I = g.I;
+    const R *h = g.h;
+    const R cffg = R(0.5 * 10.0);                    // 0.5 g, g = 10 (mod_constants.py:26)
+    const R *zr = a.zrhs, *ur = a.urhs, *vr = a.vrhs;
+    const R rdrag2 = (R)a.rdrag2;
+    const R cdt = a.first ? (R)(0.5 * a.dtfast) : (a.phase == 0 ? (R)a.dtfast : (R)(0.5 * a.dtfast));
+    // U face p
+    R unew = R(0), runew = R(0);
+    if (i >= 2 && i <= g.I - 2 && j >= 1 && j <= g.J - 2) {
+        const R gp = roms_zwrk(a, p), gw = roms_zwrk(a, p - 1);
+        const R gp2 = gp * gp, gw2 = gw * gw;
+        const R pg = (cffg * g.on_u[p]) * ((h[p - 1] + h[p]) * (gw - gp) + (gw2 - gp2));
+        const R UFp = ((R(0.5) * (zr[p] + h[p])) * g.fomn[p]) * (vr[p] + vr[p + I]);
+        const R UFw = ((R(0.5) * (zr[p - 1] + h[p - 1])) * g.fomn[p - 1]) * (vr[p - 1] + vr[p - 1 + I]);
+        const R cor = R(0.5) * (UFp + UFw);
+        const R area = R(4.0) / ((g.pm[p] + g.pm[p - 1]) * (g.pn[p] + g.pn[p - 1]));
+        const R v4 = R(0.25) * (((vr[p] + vr[p + I]) + vr[p - 1]) + vr[p - 1 + I]);
+        const R ub = ur[p];
+        const R bustr = (rdrag2 * ub) * sqrt(ub * ub + v4 * v4);
+        const R ru = (pg + cor) + (a.sustr[p] - bustr) * area;
+        R f = ru;
+        if (a.phase == 0) runew = ru;
+        else if (!a.first) f = (R(5.0 / 12.0) * ru + R(8.0 / 12.0) * a.ru_n[p]) - R(1.0 / 12.0) * a.ru_b[p];
+        const R cff = (g.pm[p] + g.pm[p - 1]) * (g.pn[p] + g.pn[p - 1]);
+        const R Ds = (a.zkstp[p] + h[p]) + (a.zkstp[p - 1] + h[p - 1]);
+        const R Dn = (a.zout[p] + h[p]) + (a.zout[p - 1] + h[p - 1]);
+        unew = (a.ukstp[p] * Ds + (cff * cdt) * f) / Dn;
+    }
+    a.uout[p] = unew;
+    if (a.phase == 0) a.ru_n[p] = runew;
+    // V face p
+    R vnew = R(0), rvnew = R(0);
+    if (j >= 2 && j <= g.J - 2 && i >= 1 && i <= g.I - 2) {
+        const R gp = roms_zwrk(a, p), gs = roms_zwrk(a, p - I);
+        const R gp2 = gp * gp, gs2 = gs * gs;
+        const R pg = (cffg * g.om_v[p]) * ((h[p - I] + h[p]) * (gs - gp) + (gs2 - gp2));
+        const R VFp = ((R(0.5) * (zr[p] + h[p])) * g.fomn[p]) * (ur[p] + ur[p + 1]);
+        const R VFs = ((R(0.5) * (zr[p - I] + h[p - I])) * g.fomn[p - I]) * (ur[p - I] + ur[p - I + 1]);
+        const R cor = R(-0.5) * (VFp + VFs);
+        const R area = R(4.0) / ((g.pm[p] + g.pm[p - I]) * (g.pn[p] + g.pn[p - I]));
+        const R u4 = R(0.25) * (((ur[p] + ur[p + 1]) + ur[p - I]) + ur[p - I + 1]);
+        const R vb = vr[p];
+        const R bvstr = (rdrag2 * vb) * sqrt(u4 * u4 + vb * vb);
+        const R rv = (pg + cor) + (a.svstr[p] - bvstr) * area;
+        R f = rv;
+        if (a.phase == 0) rvnew = rv;
+        else if (!a.first) f = (R(5.0 / 12.0) * rv + R(8.0 / 12.0) * a.rv_n[p]) - R(1.0 / 12.0) * a.rv_b[p];
+        const R cff = (g.pm[p] + g.pm[p - I]) * (g.pn[p] + g.pn[p - I]);
+        const R Ds = (a.zkstp[p] + h[p]) + (a.zkstp[p - I] + h[p - I]);
+        const R Dn = (a.zout[p] + h[p]) + (a.zout[p - I] + h[p - I]);
+        vnew = (a.vkstp[p] * Ds + (cff * cdt) * f) / Dn;
+    }
+    a.vout[p] = vnew;
+    if (a.phase == 0) a.rv_n[p] = rvnew;
+}
+
+// Surface stress on the top level of the 3D momentum right-hand side (ROMS's ru at k = N
+// includes + sustr om_u on_u): ru[N-1] += sustr * area at the interior U faces, likewise rv.
+template <typename R>
+__global__ void __launch_bounds__(256) k_roms_stress3d(Geo<R> g, R *__restrict__ ru,
+                                                       R *__restrict__ rv, const R *__restrict__ sustr,
+                                                       const R *__restrict__ svstr) {
+    const long p = tid_flat();
+    if (p >= g.s2) return;
+    const int j = fdiv((int)p, g.dI), i = (int)p - j * g.I;
+    const long I = g.I, o = (long)(g.N - 1) * g.s2 + p;
+    if (i >= 2 && i <= g.I - 2 && j >= 1 && j <= g.J - 2)
+        ru[o] = ru[o] + sustr[p] * (R(4.0) / ((g.pm[p] + g.pm[p - 1]) * (g.pn[p] + g.pn[p - 1])));
+    if (j >= 2 && j <= g.J - 2 && i >= 1 && i <= g.I - 2)
+        rv[o] = rv[o] + svstr[p] * (R(4.0) / ((g.pm[p] + g.pm[p - I]) * (g.pn[p] + g.pn[p - I])));
+}
+
+// Closed walls for the 3D velocities: u = 0 on the U wall faces (i = 1, I-1), v = 0 on the V
+// wall faces (j = 1, J-1), every level.
+template <typename R>
+__global__ void __launch_bounds__(256) k_roms_walls3d(Geo<R> g, R *__restrict__ u, R *__restrict__ v) {
+    const long p = tid_flat();
+    if (p >= g.s2) return;
+    const int j = fdiv((int)p, g.dI), i = (int)p - j * g.I;
+    const bool uw = (i == 1 || i == g.I - 1), vw = (j == 1 || j == g.J - 1);
+    if (!uw && !vw) return;
+    for (int k = 0; k <= g.N; ++k) {
+        if (uw) u[(long)k * g.s2 + p] = R(0);
+        if (vw) v[(long)k * g.s2 + p] = R(0);
+    }
+}
+
+template <typename R>
+cudaError_t Ops<R>::roms_phase(const sf_ctx *c, const RomsArgs<R> &a, cudaStream_t s) {
+    const unsigned nb = blocks_for(c->s2, 256);
+    k_roms_zeta<R><<<nb, 256, 0, s>>>(geo(c), a);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess || !a.step) return e;
+    k_roms_mom<R><<<nb, 256, 0, s>>>(geo(c), a);
+    return cudaGetLastError();
+}
+template <typename R>
+cudaError_t Ops<R>::roms_stress3d(const sf_ctx *c, R *ru, R *rv, const R *sustr, const R *svstr,
+                                  cudaStream_t s) {
+    k_roms_stress3d<R><<<blocks_for(c->s2, 256), 256, 0, s>>>(geo(c), ru, rv, sustr, svstr);
+    return cudaGetLastError();
+}
+template <typename R>
+cudaError_t Ops<R>::roms_walls3d(const sf_ctx *c, R *u, R *v, cudaStream_t s) {
+    k_roms_walls3d<R><<<blocks_for(c->s2, 256), 256, 0, s>>>(geo(c), u, v);
+    return cudaGetLastError();
+}
+
+}  // namespace sf

@@ -95,6 +95,21 @@ def set_weights(ndtfast, nweights=257):
     return nfast, w1, w2
 
 
+def roms_weights(nfast, weight1):
+    """ROMS-indexed averaging weights (W1, W2) for the ROMS-form barotropic step.  set_weights
+    stores ROMS's weight(1, m) at index m-1 (its loops start at iter = 1, set_weights.py:96),
+    so W1[m] = weight1[m-1]; ROMS's secondary weights are weight(2, i) = sum_{j=i..nfast}
+    weight(1, j), normalised over i = 1..nfast (set_weights.py:165-196 in ROMS's index
+    range)."""
+    W1 = np.zeros(len(weight1) + 1)
+    W1[1:] = np.asarray(weight1, np.float64)
+    W2 = np.zeros_like(W1)
+    for i in range(1, nfast + 1):
+        W2[i] = float(np.sum(W1[i:nfast + 1]))
+    W2[1:nfast + 1] /= float(np.sum(W2[1:nfast + 1]))
+    return W1, W2
+
+
 # --------------------------------------------------------------------------------------------
 # set_coords (nonlinear/set_coords.py)
 # --------------------------------------------------------------------------------------------

@@ -137,7 +137,14 @@ class Model:
     NAMES2 = ("zeta", "ubar", "vbar", "rzeta", "rubar", "rvbar")
     NAMES3 = ("u", "v", "ru", "rv", "W", "Huon", "Hvom", "AKv")
 
-    def __init__(self, grid, boundary, dt, ndtfast, precision="fp64", lam=1.0, device="cuda"):
+    def __init__(self, grid, boundary, dt, ndtfast, precision="fp64", lam=1.0, device="cuda",
+                 semantics="reference"):
+        """semantics: "reference" (the reference's own step, bit-identical in FP64) or "roms"
+        (the ROMS-form barotropic step with wind stress, quadratic bottom drag and Coriolis,
+        surface stress on the 3D momentum and closed walls; set_forcing gives its stresses)."""
+        if semantics not in ("reference", "roms"):
+            raise ValueError("semantics must be 'reference' or 'roms'")
+        self.semantics = semantics
         self.grid = grid
         self.ctx = Context(grid, boundary, precision)
         self.precision = precision
@@ -166,6 +173,14 @@ class Model:
         # vertical mixing per step (closure.Closure), after step3d_UV; None keeps AKv as it is,
         # as the reference's step does (modules/mod_ocean.py:91)
         self.mixing = None
+        if semantics == "roms":
+            # ROMS-indexed averaging weights, the second fast-time averages, the stresses
+            self.W1, self.W2 = host.roms_weights(self.nfast, self.weight1)
+            self.DU_avg2 = z(J * I, dt=torch.float64)
+            self.DV_avg2 = z(J * I, dt=torch.float64)
+            self.sustr = z(J * I)
+            self.svstr = z(J * I)
+            self.rdrag2 = 0.0
         # blow-up check (sf_check_state) after every check_every-th step (0: never); a failed
         # check raises SailfishError with status SF_ENONFINITE
         self.check_every = 0
@@ -213,6 +228,42 @@ class Model:
         for n in self.NAMES2[1:]:
             assert [(getattr(s, n)[k] - base[n]) // row for k in range(3)] == new
         self.slots = new
+
+    # -- ROMS-form forcing -------------------------------------------------------------------
+    def set_forcing(self, sustr=None, svstr=None, rdrag2=None):
+        """Kinematic surface stress (m2/s2, (M+1)(L+1) arrays at U and V faces) and the
+        quadratic bottom-drag coefficient of the ROMS-form step."""
+        if self.semantics != "roms":
+            raise ValueError("forcing applies to the ROMS-form step (semantics='roms')")
+        for name, a in (("sustr", sustr), ("svstr", svstr)):
+            if a is not None:
+                getattr(self, name).copy_(torch.from_numpy(np.ascontiguousarray(a, np.float64).ravel()))
+        if rdrag2 is not None:
+            self.rdrag2 = float(rdrag2)
+
+    def _roms_loop(self, s, stream):
+        W1 = self.W1.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        W2 = self.W2.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        check(lib.sf_roms_barotropic_loop(
+            self.ctx.ptr, ctypes.byref(s), self._p(self.DU_avg2), self._p(self.DV_avg2),
+            self._p(self.sustr), self._p(self.svstr), self.rdrag2, self.nfast, W1, W2,
+            self.dtfast, stream), "sf_roms_barotropic_loop")
+
+    def step2d(self, nsteps=1, first=None):
+        """2D-only steps of the ROMS-form scheme (predictor + corrector, no averages), the
+        counterpart of the reference's main2d; the run's first step is forward/backward Euler."""
+        if self.semantics != "roms":
+            raise ValueError("step2d is the ROMS-form 2D driver (semantics='roms')")
+        st = stream_handle()
+        for _ in range(nsteps):
+            f = (not getattr(self, "_started2d", False)) if first is None else first
+            s = self.state2d()
+            check(lib.sf_roms_step2d(self.ctx.ptr, ctypes.byref(s), self._p(self.sustr),
+                                     self._p(self.svstr), self.rdrag2, self.dtfast, int(f), st),
+                  "sf_roms_step2d")
+            self._sync_slots(s)
+            self._started2d = True
+            self.time2D += self.dtfast
 
     # -- steps -------------------------------------------------------------------------------
     def check_state(self, stream=None):
@@ -310,7 +361,13 @@ class Model:
                 c, ctypes.byref(s), self.nfast + 1,
                 self._w1.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), self.dtfast,
                 ctypes.byref(t2), sh), "sf_barotropic_loop")
-            if ovl_rhs:
+            if self.semantics == "roms":
+                phase("k_rhs3d", lambda: (rhs(st), check(lib.sf_roms_stress3d(
+                    c, p(self.ru), p(self.rv), p(self.sustr), p(self.svstr), st),
+                    "sf_roms_stress3d")))
+                phase("barotropic_loop", lambda: self._roms_loop(s, st))
+                after(cs, ev_mix)
+            elif ovl_rhs:
                 e_flux = mark(cs)
                 after(s_side, e_flux)
                 phase("k_rhs3d", lambda: rhs(h(s_side)), s_side)
@@ -329,6 +386,8 @@ class Model:
                 p(self._slot("vbar", 1)), p(self._slot("ubar", 2)), p(self._slot("vbar", 2)),
                 p(self.Hz), p(self.AKv), p(self.z_r), p(self.DU_avg1), p(self.DV_avg1), self.iic,
                 self.ntfirst, self.lam, self.dt, self.time, st), "sf_step3d_uv_bc"))
+            if self.semantics == "roms":
+                check(lib.sf_roms_closed_walls(c, p(self.u), p(self.v), st), "sf_roms_closed_walls")
             if self.mixing is not None:
                 if mix_ovl:
                     after(s_mix, mark(cs))

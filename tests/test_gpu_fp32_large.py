@@ -32,8 +32,10 @@ TOL = {
     # nodes (cancellation: ~3e-5 of their scale on these smooth fields)
     "predictor": {"zeta2": 5e-6, "ubar2": 2e-5, "vbar2": 2e-5, "rzeta1": 1e-5, "rubar1": 1e-4,
                   "rvbar1": 1e-4},
+    # vbar is reset to 0 after every substep (main3d.py:189), so DV_avg1 sums single-substep
+    # increments of it and carries their FP32 relative error (3e-4 measured)
     "loop": {"zeta": 5e-5, "ubar": 5e-5, "Zt_avg1": 5e-5, "DU_avg1": 5e-5,
-             "DV_avg1": 5e-5},
+             "DV_avg1": 1e-3},
     "step3d_uv": {"u": 2e-5, "v": 2e-5, "ubar1": 2e-5, "vbar1": 2e-5},
     "step": {"zeta": 1e-4, "ubar": 1e-4, "u": 2e-4, "v": 2e-4, "W": 2e-4, "Zt_avg1": 1e-4},
 }
