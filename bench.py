@@ -316,8 +316,8 @@ def plain_fp64(args):
     return {"value": cells * steps / (ms * 1e-3), "unit": "cell-steps/s",
             "ms_per_step": ms / steps, "steps": steps, "warmup": 3, "dtype": "f64",
             "semantics": "bit-identical to the reference kernels",
-            "vertical_mixing": "plain GLS k-epsilon every step, FP64" if mixing == "gls"
-                               else "AKv constant (the reference's step)"}
+            "vertical_mixing": "plain GLS %s every step, FP64" % gls_model_for(args.config)
+                               if mixing == "gls" else "AKv constant (the reference's step)"}
 
 
 def _ref_basin(cfg):
@@ -377,8 +377,8 @@ def reference_gpu_fp64(args, gls_ms):
                        "nonlinear/step3D_uv.kernels.cpp, modules/mod_BC.c), NVRTC for sm_100a with "
                        "-default-device --restrict --std=c++17, launched in main3d order",
             "launches_per_step": launches,
-            "vertical_mixing": "plain GLS k-epsilon every step, FP64 (this package's kernel; the "
-                               "reference has no runnable GLS)"}
+            "vertical_mixing": "plain GLS %s every step, FP64 (this package's kernel; the "
+                               "reference has no runnable GLS)" % gls_model_for(args.config)}
 
 
 def gls_fp64_ms(args):
@@ -437,6 +437,62 @@ def error_vs_fp64():
     return out
 
 
+def roms_day(args, hours=24.0, tau0=0.15, rdrag2=3e-3):
+    """The configuration's physics for one simulated day in the ROMS-form step (wind
+    tau_x = tau0 cos(pi y/Ly) N/m2, quadratic bottom drag rdrag2, Coriolis, T = 4 + 20 exp(z/500)
+    for the mixing, from rest): the FP32 form with the learned closure against FP64 with plain
+    GLS every step, from identical initial states.  Returns the RMS / max differences of the
+    free surface (Zt_avg1, the surface the 3D step uses), ubar, u and v over the interior at the
+    end, with the RMS of each FP64 field, and each run's device time per step."""
+    import torch
+    from sailfish_b200 import configs
+    from sailfish_b200.model import Model
+    cfg = configs.CONFIGS[args.config]()
+    g = cfg["grid"]
+    nsteps = int(round(hours * 3600.0 / cfg["dt"]))
+    stream = torch.cuda.current_stream()
+    runs, times = {}, {}
+    for prec, mode in (("fp32", "mlp"), ("fp64", "gls")):
+        m = Model(g, cfg["boundary"], cfg["dt"], cfg["ndtfast"], precision=prec, semantics="roms")
+        c = install_mixing(m, mode, args.config)
+        m.set_forcing(c.cols.sustr.double().cpu().numpy(), c.cols.svstr.double().cpu().numpy(),
+                      rdrag2)
+        m.check_every = 60
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        m.step(nsteps)
+        b.record(stream)
+        torch.cuda.synchronize()
+        times[prec] = a.elapsed_time(b) / nsteps
+        runs[prec] = {"zeta": m.Zt_avg1.clone(), "ubar": m._slot("ubar", 1).clone(),
+                      "u": m.u.clone(), "v": m.v.clone(),
+                      "fallback_columns": int(c.mask.sum()) if mode == "mlp" else None}
+        del m, c
+        torch.cuda.empty_cache()
+    J, I, N = g.J, g.I, g.N
+    out = {"case": "%s, ROMS-form step, %d steps of %g s (%g h) from rest, wind %g cos(pi y/Ly) "
+                   "N/m2, quadratic drag %g" % (args.config, nsteps, cfg["dt"], hours, tau0, rdrag2),
+           "units": {"zeta": "m", "ubar": "m/s", "u": "m/s", "v": "m/s"},
+           "ms_per_step": times, "fp32_fallback_columns": runs["fp32"]["fallback_columns"]}
+    for k in ("zeta", "ubar", "u", "v"):
+        a64 = runs["fp64"][k].double()
+        a32 = runs["fp32"][k].double()
+        if k in ("u", "v"):
+            a64, a32 = a64.reshape(N + 1, J, I)[:N, 1:-1, 1:-1], a32.reshape(N + 1, J, I)[:N, 1:-1, 1:-1]
+        else:
+            a64, a32 = a64.reshape(J, I)[1:-1, 1:-1], a32.reshape(J, I)[1:-1, 1:-1]
+        d = a32 - a64
+        out[k] = {"rms": float(d.pow(2).mean().sqrt()), "max": float(d.abs().max()),
+                  "rms_fp64_field": float(a64.pow(2).mean().sqrt()),
+                  "finite": bool(torch.isfinite(a32).all() and torch.isfinite(a64).all())}
+    out["targets"] = {"zeta_rms_m": 1e-4, "uv_rms_m_per_s": 1e-3,
+                      "met": bool(out["zeta"]["rms"] <= 1e-4 and out["u"]["rms"] <= 1e-3 and
+                                  out["v"]["rms"] <= 1e-3)}
+    del runs
+    torch.cuda.empty_cache()
+    return out
+
+
 WEIGHTS_FOR = {"basin4q": "basin4"}   # basins sharing a recipe (and N) share the closure
 
 
@@ -453,13 +509,65 @@ def install_mixing(m, mode, config):
     if mode == "none":
         return None
     net = None
+    path = closure_weights(config)
     if mode == "mlp":
-        path = closure_weights(config)
         if path is None:
             raise SystemExit("no trained closure weights for %s (sailfish_b200/weights/); "
                              "train them with python -m sailfish_b200.train_closure" % config)
         net = closure.Network.load(path)
-    return closure.mixing_for(m, mode, net)
+    # plain GLS runs the GLS model the configuration's network learned (its training data)
+    gls_model = gls_model_for(config)
+    return closure.mixing_for(m, mode, net, gls_model=gls_model)
+
+
+def closure_act(config):
+    path = closure_weights(config)
+    if path is None:
+        return None
+    d = np.load(path)
+    return str(d["act"]) if "act" in d else "gelu"
+
+
+def gls_model_for(config):
+    """The GLS model of a configuration: the one its closure weights were trained on (k-psi for
+    config 1's basin, as its specification asks), else k-epsilon."""
+    path = closure_weights(config)
+    if path is not None:
+        d = np.load(path)
+        if "gls_model" in d:
+            return str(d["gls_model"])
+    return "k-epsilon"
+
+
+def closure_variants(m, config, reps=5):
+    """Device time (ms) of one closure update on the bench's state for every trained network of
+    the configuration (closure_<config>*.npz: the GELU network of the specification and its
+    ReLU variant, where present), keyed by activation."""
+    import glob
+    import torch
+    from sailfish_b200 import closure
+    name = WEIGHTS_FOR.get(config, config)
+    out = {}
+    prev = m.mixing
+    stream = torch.cuda.current_stream()
+    for path in sorted(glob.glob(os.path.join(ROOT, "sailfish_b200", "weights",
+                                              "closure_%s*.npz" % name))):
+        net = closure.Network.load(path)
+        if net.N != m.grid.N:
+            continue
+        c = closure.mixing_for(m, "mlp", net, gls_model=net.gls_model)
+        c()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            c()
+        b.record(stream)
+        torch.cuda.synchronize()
+        out[net.act] = {"ms": a.elapsed_time(b) / reps, "weights": os.path.basename(path),
+                        "fallback_columns": int(c.mask.sum())}
+    m.mixing = prev
+    return out
 
 
 def closure_error(m, steps=300):
@@ -725,8 +833,10 @@ def run_ours(args, rank, world):
                    "barotropic_substeps": m.nfast + 1, "semantics": "reference main3d",
                    "initial_state": "rest, closed walls",
                    "vertical_mixing": {"none": "AKv constant (the reference's step)",
-                                       "gls": "plain GLS k-epsilon every step",
-                                       "mlp": "learned closure, plain GLS on fallback columns"
+                                       "gls": "plain GLS %s every step" % gls_model_for(args.config),
+                                       "mlp": "learned closure (%s network), plain GLS %s on "
+                                              "fallback columns" % (
+                                                  closure_act(args.config), gls_model_for(args.config))
                                        }[mixing],
                    "forcing": "closure: wind tau_x = 0.15 cos(pi y/Ly) N/m2, T = 4 + 20 exp(z/500)"
                               if mixing != "none" else None,
@@ -748,6 +858,8 @@ def run_ours(args, rank, world):
         "gpu_launches": args.steps * per_step + 1,
         "clocks": clk.summary(),
     }
+    if mixing == "mlp":
+        out["closure_ms_by_network"] = closure_variants(m, args.config)
     if mixing == "mlp" and not args.no_error:
         out["closure_error"] = closure_error(m)
     return out
@@ -771,6 +883,8 @@ def main():
     ap.add_argument("--closure", choices=["mlp", "gls", "none"], default=None,
                     help="vertical mixing in the step (default: mlp for fp32, gls for fp64)")
     ap.add_argument("--no-error", action="store_true", help="skip the FP32-vs-FP64 error case")
+    ap.add_argument("--day-hours", type=float, default=24.0,
+                    help="simulated hours of the ROMS-form FP32-vs-FP64 error run (0: skip)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -823,6 +937,12 @@ def main():
             out["opt_fp64"]["speedup_of_value"] = out["value"] / world / out["opt_fp64"]["value"]
         if not args.no_error:
             out["error_vs_fp64"] = error_vs_fp64()
+        if args.day_hours > 0 and args.config in ("basin4", "basin4q", "basin1"):
+            try:
+                out["day_error_vs_fp64"] = roms_day(args, hours=args.day_hours)
+            except Exception as e:   # a blow-up check that fired, for instance
+                out["day_error_vs_fp64"] = {"failed": str(e)}
+                torch.cuda.empty_cache()
         if not args.no_cpu_baseline:
             out["cpu_baseline"] = cpu_sample(args)
         print(json.dumps(out))

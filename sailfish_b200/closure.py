@@ -84,7 +84,7 @@ class Columns:
     """Water-column state of one basin for the closure: velocities at rho levels, buoyancy
     frequency, surface stress and the GLS turbulence fields, all on the current device."""
 
-    def __init__(self, model):
+    def __init__(self, model, gls_model="k-epsilon"):
         self.m = model
         g = model.grid
         dt = model.tdtype
@@ -93,7 +93,8 @@ class Columns:
         z = lambda *s: torch.zeros(*s, dtype=dt, device=dev)
         self.bvf = z(N + 1, J, I)
         self.sustr, self.svstr = z(J, I), z(J, I)
-        P = gls_defaults()
+        self.gls_model = gls_model
+        P = gls_preset(gls_model)
         self.P = P
         self.tke = torch.full((N + 1, J, I), P.Kmin, dtype=dt, device=dev)
         self.gls = torch.full((N + 1, J, I), P.Pmin, dtype=dt, device=dev)
@@ -206,9 +207,10 @@ def basin_forcing(model, cols, tau0=0.15, zscale=500.0):
     cols.stratify(zscale)
 
 
-def mixing_for(model, mode, net=None, tau0=0.15, zscale=500.0):
-    """A Closure for `model` ('gls' or 'mlp') under basin_forcing, installed as model.mixing."""
-    c = Closure(model, mode, net)
+def mixing_for(model, mode, net=None, tau0=0.15, zscale=500.0, gls_model=None):
+    """A Closure for `model` ('gls' or 'mlp') under basin_forcing, installed as model.mixing;
+    gls_model defaults to the network's (the model it was trained on), else k-epsilon."""
+    c = Closure(model, mode, net, gls_model=gls_model)
     basin_forcing(model, c.cols, tau0, zscale)
     model.mixing = c
     return c
@@ -216,7 +218,7 @@ def mixing_for(model, mode, net=None, tau0=0.15, zscale=500.0):
 
 def generate(config="basin1", runs=4, spin=30, keep=4, every=5, seed=0, precision="fp32",
              tau_range=(0.0, 0.3), zscale_range=(200.0, 1000.0), rest_runs=0, pattern=False,
-             spread=False):
+             spread=False, gls_model="k-epsilon"):
     """Training snapshots from plain GLS runs on `config`'s grid: each run draws a wind stress
     and a stratification scale, spins GLS up for `spin` steps at fixed forcing and then keeps
     `keep` snapshots `every` steps apart.  The last `rest_runs` of the runs have no current
@@ -232,10 +234,15 @@ def generate(config="basin1", runs=4, spin=30, keep=4, every=5, seed=0, precisio
     dev = model.u.device
     cols_idx = interior_columns(g, dev)
     rng = np.random.default_rng(seed)
-    Xs, Ts = [], []
+    nc = int(cols_idx.numel())
+    # the rows go straight into preallocated tensors (no list of snapshots to concatenate:
+    # tens of millions of rows are tens of GB)
+    X = torch.empty((runs * keep * nc, WIDTH), device=dev)
+    T = torch.empty((runs * keep * nc, WIDTH), device=dev)
+    row = 0
     Xbuf = torch.zeros((g.s2, WIDTH), device=dev)
     for r in range(runs):
-        cols = Columns(model)
+        cols = Columns(model, gls_model)
         tau = float(rng.uniform(*tau_range))
         angle = float(rng.uniform(0.0, 2.0 * math.pi))
         if spread:   # the stratification scale varies linearly across xi over the whole range
@@ -253,10 +260,11 @@ def generate(config="basin1", runs=4, spin=30, keep=4, every=5, seed=0, precisio
             cols.gls_step()
             if it >= spin and (it - spin) % every == every - 1:
                 cols.features(Xbuf)
-                Xs.append(Xbuf[cols_idx].clone())
-                Ts.append(targets(model.AKv, cols.Akt, g.N)[cols_idx])
+                X[row:row + nc] = Xbuf[cols_idx]
+                T[row:row + nc] = targets(model.AKv, cols.Akt, g.N)[cols_idx]
+                row += nc
     torch.cuda.synchronize()
-    return torch.cat(Xs), torch.cat(Ts)
+    return X, T
 
 
 def targets(Akv, Akt, N):
@@ -280,13 +288,14 @@ class Network:
     and Adam moments, BF16 copies for the tensor cores.  Inputs are normalised with the training set's per-feature mean and spread,
     which `inference_params()` folds into the first layer."""
 
-    def __init__(self, N, seed=0, device="cuda", act="relu"):
+    def __init__(self, N, seed=0, device="cuda", act="relu", gls_model="k-epsilon"):
         if nfeat(N) > WIDTH:
             raise ValueError("the closure's rows hold at most 62 interior W levels")
         if act not in MLP_ACT:
             raise ValueError("act must be one of %s" % sorted(MLP_ACT))
         self.N = int(N)
         self.act = act
+        self.gls_model = gls_model   # the GLS model whose coefficients it learns
         gen = torch.Generator().manual_seed(seed)
         self.W = [(torch.randn(WIDTH, WIDTH, generator=gen) * math.sqrt(2.0 / WIDTH)).to(device)
                   for _ in range(LAYERS)]
@@ -390,7 +399,8 @@ class Network:
 
     def save(self, path, **meta):
         """Master weights, normalisation and training range (NumPy .npz) plus `meta`."""
-        np.savez(path, N=self.N, act=self.act, W=np.stack([w.cpu().numpy() for w in self.W]),
+        np.savez(path, N=self.N, act=self.act, gls_model=self.gls_model,
+                 W=np.stack([w.cpu().numpy() for w in self.W]),
                  b=np.stack([b.cpu().numpy() for b in self.b]), mu=self.mu.cpu().numpy(),
                  isd=self.isd.cpu().numpy(), lo=self.lo.cpu().numpy(), hi=self.hi.cpu().numpy(),
                  **{k: np.asarray(v) for k, v in meta.items()})
@@ -399,7 +409,8 @@ class Network:
     def load(cls, path, device="cuda"):
         d = np.load(path)
         # files without an activation entry hold GELU networks
-        net = cls(int(d["N"]), device=device, act=str(d["act"]) if "act" in d else "gelu")
+        net = cls(int(d["N"]), device=device, act=str(d["act"]) if "act" in d else "gelu",
+                  gls_model=str(d["gls_model"]) if "gls_model" in d else "k-epsilon")
         t = lambda a: torch.tensor(np.asarray(a, np.float32), device=device)
         net.W = [t(w) for w in d["W"]]
         net.b = [t(b) for b in d["b"]]
@@ -433,7 +444,7 @@ class Closure:
     (fused: one sf_closure_step pass; otherwise features, range mask, sf_mlp_infer and
     sf_closure_apply as separate launches)."""
 
-    def __init__(self, model, mode="mlp", net=None, fused=True):
+    def __init__(self, model, mode="mlp", net=None, fused=True, gls_model=None):
         if mode not in ("gls", "mlp"):
             raise ValueError("mode must be 'gls' or 'mlp'")
         if mode == "mlp" and net is None:
@@ -444,7 +455,9 @@ class Closure:
         # Model.step may run it beside the next step's first phases: it reads u, v, z_r, Hz,
         # bvf and the surface stress, and writes AKv and its own turbulence fields only
         self.overlappable = True
-        self.cols = Columns(model)
+        if gls_model is None:
+            gls_model = net.gls_model if net is not None else "k-epsilon"
+        self.cols = Columns(model, gls_model)
         g = model.grid
         dev = model.u.device
         if mode == "mlp":

@@ -23,20 +23,22 @@ RECIPES = {
     "basin4": lambda: configs.basin(256, 128, 50, 1.0e3, [(1.0 / 3.0, 0.6), (2.0 / 3.0, 0.6)],
                                     dt=120.0, ndtfast=40),
     "basin1": lambda: configs.basin(256, 128, 32, 2.0e3, [(0.5, 0.6)], dt=240.0, ndtfast=30),
+    # config 1's own basin (512 x 256 x 32): 131,072 columns per snapshot
+    "basin1-full": configs.basin1,
 }
 
 
-def train(config, out, runs=16, rest_runs=8, spin=300, every=25, steps=6000, batch=4096, lr=1e-3,
-          seed=1, act="relu"):
+def train(config, out, runs=16, rest_runs=8, spin=300, every=25, keep=4, steps=6000, batch=4096,
+          lr=1e-3, seed=1, act="relu", gls_model="k-epsilon"):
     """GLS is spun up `spin` steps at fixed forcing (10 h at dt = 120 s: the turbulence fields
-    settle to their forced state), then 4 snapshots `every` steps apart are kept."""
+    settle to their forced state), then `keep` snapshots `every` steps apart are kept."""
     cfg = RECIPES[config]()
     N = cfg["grid"].N
-    X, T = closure.generate(cfg, runs=runs, spin=spin, keep=4, every=every, seed=seed,
-                            rest_runs=rest_runs, pattern=True, spread=True)
+    X, T = closure.generate(cfg, runs=runs, spin=spin, keep=keep, every=every, seed=seed,
+                            rest_runs=rest_runs, pattern=True, spread=True, gls_model=gls_model)
     Xv, Tv = closure.generate(cfg, runs=4, spin=spin, keep=2, every=every, seed=seed + 1000,
-                              rest_runs=2, pattern=True, spread=True)
-    net = closure.Network(N, seed=seed, act=act)
+                              rest_runs=2, pattern=True, spread=True, gls_model=gls_model)
+    net = closure.Network(N, seed=seed, act=act, gls_model=gls_model)
     net.fit_normalisation(X)
     hist = net.train(X, T, steps=steps, batch=batch, lr=lr, seed=seed, log_every=500)
     e = closure.log_rms(net.infer(Xv), Tv, N)
@@ -44,7 +46,7 @@ def train(config, out, runs=16, rest_runs=8, spin=300, every=25, steps=6000, bat
     const[:, :N - 1] = -3.0
     const[:, N - 1:2 * (N - 1)] = -6.0
     ec = closure.log_rms(const, Tv, N)
-    report = {"config": config, "N": N, "act": act, "rows": int(X.shape[0]),
+    report = {"config": config, "N": N, "act": act, "gls_model": gls_model, "rows": int(X.shape[0]),
               "heldout_rows": int(Xv.shape[0]),
               "gls_spinup": spin, "steps": steps, "batch": batch, "loss": hist,
               "heldout_log10_rms_akv": e[0], "heldout_log10_rms_akt": e[1],
@@ -61,8 +63,15 @@ def main():
     ap.add_argument("--steps", type=int, default=6000)
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--act", default="relu", choices=["relu", "gelu"])
+    ap.add_argument("--gls-model", default="k-epsilon", choices=sorted(closure.GLS_PRESETS))
+    ap.add_argument("--runs", type=int, default=16)
+    ap.add_argument("--rest-runs", type=int, default=8)
+    ap.add_argument("--keep", type=int, default=4)
+    ap.add_argument("--batch", type=int, default=4096)
     a = ap.parse_args()
-    print(json.dumps(train(a.config, a.out, steps=a.steps, seed=a.seed, act=a.act)))
+    print(json.dumps(train(a.config, a.out, runs=a.runs, rest_runs=a.rest_runs, keep=a.keep,
+                           steps=a.steps, batch=a.batch, seed=a.seed, act=a.act,
+                           gls_model=a.gls_model)))
 
 
 if __name__ == "__main__":

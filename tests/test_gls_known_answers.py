@@ -116,7 +116,7 @@ def test_cuda_gls_homogeneous_shear_equilibrium(model):
     from sailfish_b200._lib import lib, check, GlsParams
     from sailfish_b200.model import Context, Grid
     S = 0.01
-    P, c = column(model, S, I=6)      # the library's contexts need L, M >= 4
+    P, c = column(model, S, N=6, I=6)      # the library's contexts need L, M >= 4 and N >= 5
     I, J, N = c["I"], c["J"], c["N"]
     sc_r, sc_w, Cs_r, Cs_w = Hm.set_coords(N, 4, 5.0, 0.4)
     z = np.zeros(I * J)
@@ -132,7 +132,7 @@ def test_cuda_gls_homogeneous_shear_equilibrium(model):
     for _ in range(3000):
         check(lib.sf_gls_corrector(ctx.ptr, ctypes.byref(prm), 1.0, *args, st), "sf_gls_corrector")
     torch.cuda.synchronize()
-    k, L, Akv = (float(T[f][2, 2 * I + 2]) for f in ("tke", "Lscale", "Akv"))
+    k, L, Akv = (float(T[f][3, 2 * I + 2]) for f in ("tke", "Lscale", "Akv"))
     eps = eps_of(P, k, L)
     ratio = (Akv - P["Akv_bak"]) * S * S / eps
     assert abs(ratio / shear_ratio(P) - 1.0) < 5e-3, (ratio, shear_ratio(P))

