@@ -120,6 +120,14 @@ def traffic_per_launch(kernel, grid):
     return None
 
 
+def config_of(args):
+    """The workload's configuration (with --levels, the same basin with that many levels)."""
+    from sailfish_b200 import configs
+    if getattr(args, "levels", None):
+        return configs.named(args.config, args.levels)
+    return configs.CONFIGS[args.config]()
+
+
 def peaks():
     try:
         with open(MEASURED) as f:
@@ -751,7 +759,7 @@ def run_ours(args, rank, world):
     from sailfish_b200.model import Model
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
-    cfg = configs.CONFIGS[args.config]()
+    cfg = config_of(args)
     grid = cfg["grid"]
     m = Model(grid, cfg["boundary"], cfg["dt"], cfg["ndtfast"], precision=args.precision)
     mixing = args.closure or ("mlp" if args.precision == "fp32" else "gls")
@@ -828,7 +836,8 @@ def run_ours(args, rank, world):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32" if args.precision == "fp32" else "f64", "data": "synthetic",
-        "config": {"workload": args.config, "Lm": grid.L - 1, "Mm": grid.M - 1, "N": grid.N,
+        "config": {"workload": args.config + ("" if not args.levels else " with %d levels" % args.levels),
+                   "Lm": grid.L - 1, "Mm": grid.M - 1, "N": grid.N,
                    "cells": cells, "dt": m.dt, "ndtfast": m.ndtfast,
                    "barotropic_substeps": m.nfast + 1, "semantics": "reference main3d",
                    "initial_state": "rest, closed walls",
@@ -883,6 +892,8 @@ def main():
     ap.add_argument("--closure", choices=["mlp", "gls", "none"], default=None,
                     help="vertical mixing in the step (default: mlp for fp32, gls for fp64)")
     ap.add_argument("--no-error", action="store_true", help="skip the FP32-vs-FP64 error case")
+    ap.add_argument("--levels", type=int, default=None,
+                    help="run the basin with this many levels (profiling cases)")
     ap.add_argument("--day-hours", type=float, default=24.0,
                     help="simulated hours of the ROMS-form FP32-vs-FP64 error run (0: skip)")
     args = ap.parse_args()

@@ -179,6 +179,11 @@ int sf_ctx_set_graphs(sf_ctx *ctx, int enable);
  * (default, the faster on one B200) for per-element cp.async staging.  Results are identical
  * either way.  No counterpart in the reference. */
 int sf_ctx_set_bulk(sf_ctx *ctx, int enable);
+/* Tuning knobs of a context's kernels (results identical for every value):
+ * SF_TUNE_MO_CHUNK: 0, 4 or 8 levels whose loads the fused set_maxflux/omega kernel issues
+ * together on columns whose fluxes it all computes itself.  No counterpart in the reference. */
+#define SF_TUNE_MO_CHUNK 0
+int sf_ctx_tune(sf_ctx *ctx, int knob, int value);
 /* Turn programmatic dependent launch of the barotropic loop's kernels on (default) or off:
  * with it each kernel's blocks become resident while its predecessor's last wave runs and wait
  * on the device for its completion.  Results are identical either way. */

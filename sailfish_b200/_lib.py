@@ -97,6 +97,7 @@ SIGNATURES = {
     "sf_ctx_set_pdl": [_vp, _i],
     "sf_ctx_set_fused": [_vp, _i],
     "sf_ctx_set_bulk": [_vp, _i],
+    "sf_ctx_tune": [_vp, _i, _i],
     "sf_ctx_fused_available": [_vp],
     "sf_ctx_create_ensemble": [ctypes.POINTER(GridDesc), _i, ctypes.POINTER(_vp)],
     "sf_ctx_members": [_vp],

@@ -56,19 +56,33 @@ def basin0():
     return basin(128, 64, 5, 5.0e3, [], dt=30.0, ndtfast=1, hflat=4000.0)
 
 
+# Lm, Mm, N, dx, seamounts (relative x, y), dt, ndtfast
+PARAMS = {
+    "basin1": (512, 256, 32, 2.0e3, [(0.5, 0.6)], 240.0, 30),
+    "basin4": (2048, 1024, 50, 1.0e3, [(1.0 / 3.0, 0.6), (2.0 / 3.0, 0.6)], 120.0, 40),
+    # a quarter of basin4 (dx = 2 km): the profiling case, with 3D fields of ~0.1 GB (FP32)
+    # so that kernels stream from DRAM rather than L2
+    "basin4q": (1024, 512, 50, 2.0e3, [(1.0 / 3.0, 0.6), (2.0 / 3.0, 0.6)], 120.0, 40),
+}
+
+
+def named(name, levels=None):
+    """Basin `name` of PARAMS, optionally with another number of levels (the same horizontal
+    grid, depth, dt and ndtfast: e.g. a profiling case for the 2D kernels)."""
+    Lm, Mm, N, dx, mounts, dt, nd = PARAMS[name]
+    return basin(Lm, Mm, levels or N, dx, mounts, dt=dt, ndtfast=nd)
+
+
 def basin1():
-    return basin(512, 256, 32, 2.0e3, [(0.5, 0.6)], dt=240.0, ndtfast=30)
+    return named("basin1")
 
 
 def basin4():
-    return basin(2048, 1024, 50, 1.0e3, [(1.0 / 3.0, 0.6), (2.0 / 3.0, 0.6)], dt=120.0, ndtfast=40)
+    return named("basin4")
 
 
 def basin4q():
-    """A quarter of basin4 (Lm=1024, Mm=512, N=50, dx=2 km): the profiling case, with 3D
-    fields of ~0.1 GB (FP32) so that kernels stream from DRAM rather than L2."""
-    return basin(1024, 512, 50, 2.0e3, [(1.0 / 3.0, 0.6), (2.0 / 3.0, 0.6)], dt=120.0,
-                 ndtfast=40)
+    return named("basin4q")
 
 
 def small(Lm=256, Mm=128, N=32):

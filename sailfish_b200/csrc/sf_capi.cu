@@ -869,6 +869,18 @@ int sf_ctx_set_bulk(sf_ctx *c, int enable) {
     return SF_OK;
 }
 
+int sf_ctx_tune(sf_ctx *c, int knob, int value) {
+    if (!c) return fail(SF_EINVAL, "null context");
+    switch (knob) {
+    case SF_TUNE_MO_CHUNK:
+        if (value != 0 && value != 4 && value != 8) return fail(SF_EINVAL, "chunk is 0, 4 or 8");
+        c->mo_chunk = value;
+        return SF_OK;
+    default:
+        return fail(SF_EINVAL, "unknown tuning knob");
+    }
+}
+
 int sf_ctx_fused_available(const sf_ctx *c) { return c && c->nmem == 1 && c->pred_ok ? 1 : 0; }
 
 int sf_ctx_set_pdl(sf_ctx *c, int enable) {

@@ -136,6 +136,8 @@ struct sf_ctx {
     // by default: on basin4 the column solve took 2.08 ms with it against 1.65 ms with
     // per-element cp.async staging
     int use_bulk = 0;
+    // levels whose loads the fused flux/omega kernel issues together (sf_ctx_tune)
+    int mo_chunk = 0;
     cudaStream_t cap = nullptr;
     double *d_bcval = nullptr;
     sf_loop_graph graphs[3];

@@ -906,7 +906,9 @@ __device__ __forceinline__ void rhs3d_body(const Geo<R> &g, const R *__restrict_
 // ------------------------------------------------------------------------------------------
 // set_maxflux (step3D_uv.kernels.cpp:372-405) + omega (:62-165) + set_zeta (:294-310)
 // ------------------------------------------------------------------------------------------
-template <typename R>
+// C > 0: levels whose loads the fused flux/omega kernel issues together on its interior
+// columns (sf_ctx_tune knob SF_TUNE_MO_CHUNK); 0: one level at a time, the loop unrolled by 4
+template <typename R, int C = 0>
 __device__ __forceinline__ void maxflux_omega_body(
     const Geo<R> &g, const R *__restrict__ u, const R *__restrict__ v, R *Huon, R *Hvom,
     const R *__restrict__ Hz, R *__restrict__ W, const R *__restrict__ z_w, int do_flux,
@@ -955,6 +957,45 @@ __device__ __forceinline__ void maxflux_omega_body(
 #define Wc(K) Wcol[(K) * (int)blockDim.x]
         R Wk = R(0);
         Wc(0) = R(0);
+        if (C > 0 && rc && fu && fv && ue && vnn) {
+            // every flux this column needs is computed here: the loads of a chunk of levels
+            // (Hz, u, v only, never the flux arrays being written) are issued together
+            // before any of the chunk's arithmetic, the same expressions as below
+            for (int K0 = 0; K0 < N; K0 += (C > 0 ? C : 1)) {
+                constexpr int CC = C > 0 ? C : 1;
+                R hz[CC], hzw[CC], hzs[CC], hze[CC], hzn[CC], uu[CC], uE[CC], vv[CC], vN[CC];
+#pragma unroll
+                for (int c = 0; c < CC; ++c) {
+                    const long o = (long)(K0 + c < N ? K0 + c : N - 1) * s2 + p;
+                    hz[c] = Hz[o];
+                    hzw[c] = Hz[o - 1];
+                    hzs[c] = Hz[o - I];
+                    hze[c] = Hz[o + 1];
+                    hzn[c] = Hz[o + I];
+                    uu[c] = u[o];
+                    uE[c] = u[o + 1];
+                    vv[c] = v[o];
+                    vN[c] = v[o + I];
+                }
+#pragma unroll
+                for (int c = 0; c < CC; ++c) {
+                    const int K = K0 + c;
+                    if (K < N) {
+                        const long o = (long)K * s2 + p;
+                        const R hup = (((hz[c] + hzw[c]) * R(0.5)) * uu[c]) * onu;
+                        const R hvp = (((hz[c] + hzs[c]) * R(0.5)) * vv[c]) * omv;
+                        Huon[o] = hup;
+                        Hvom[o] = hvp;
+                        if (K >= 1) {
+                            const R hue = (((hze[c] + hz[c]) * R(0.5)) * uE[c]) * onu_e;
+                            const R hvn = (((hzn[c] + hz[c]) * R(0.5)) * vN[c]) * omv_n;
+                            Wk = Wk - ((hue - hup) + (hvn - hvp));
+                            Wc(K) = Wk;
+                        }
+                    }
+                }
+            }
+        } else {
 #pragma unroll 4
         for (int K = 0; K < N; ++K) {
             const long o = (long)K * s2 + p;
@@ -969,6 +1010,7 @@ __device__ __forceinline__ void maxflux_omega_body(
                 Wk = Wk - ((hue - hup) + (hvn - hvp));
                 Wc(K) = Wk;
             }
+        }
         }
         const R zbed = z_w[p];
         const R h = z_w[(long)(N - 1) * s2 + p] - zbed;
@@ -1768,12 +1810,12 @@ __global__ void __launch_bounds__(TX *TY) kb_rhs3d(const Member<R> *mt, const in
                                  mb_.y % ntx, mb_.y / ntx);
 }
 
-template <typename R>
+template <typename R, int C>
 __global__ void __launch_bounds__(kBlock) k_maxflux_omega(
     Geo<R> g, const R *__restrict__ u, const R *__restrict__ v, R *Huon, R *Hvom, const R *__restrict__ Hz, R *__restrict__ W, const R *__restrict__ z_w,
     int do_flux, int do_omega, R *__restrict__ zeta1, R *__restrict__ zeta2, const double *__restrict__ Zt) {
-    maxflux_omega_body(g, u, v, Huon, Hvom, Hz, W, z_w, do_flux, do_omega, zeta1, zeta2, Zt,
-                       (long)tid_flat());
+    maxflux_omega_body<R, C>(g, u, v, Huon, Hvom, Hz, W, z_w, do_flux, do_omega, zeta1, zeta2, Zt,
+                             (long)tid_flat());
 }
 template <typename R>
 __global__ void __launch_bounds__(kBlock) kb_maxflux_omega(
@@ -2014,7 +2056,9 @@ cudaError_t Ops<R>::maxflux_omega(const sf_ctx *c, const R *u, const R *v, R *Hu
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !attr_set[dev]) {
         const int most = (int)(sizeof(R) * kBlock * kNMax);
-        cudaFuncSetAttribute(k_maxflux_omega<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
+        cudaFuncSetAttribute(k_maxflux_omega<R, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
+        cudaFuncSetAttribute(k_maxflux_omega<R, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
+        cudaFuncSetAttribute(k_maxflux_omega<R, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
         cudaFuncSetAttribute(kb_maxflux_omega<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
         attr_set[dev] = true;
     }
@@ -2024,7 +2068,9 @@ cudaError_t Ops<R>::maxflux_omega(const sf_ctx *c, const R *u, const R *v, R *Hu
                                                            Zt);
         return cudaGetLastError();
     }
-    k_maxflux_omega<R><<<blocks_for(c->s2, kBlock), kBlock, smem, s>>>(
+    auto k = c->mo_chunk >= 8 ? k_maxflux_omega<R, 8>
+             : c->mo_chunk >= 4 ? k_maxflux_omega<R, 4> : k_maxflux_omega<R, 0>;
+    k<<<blocks_for(c->s2, kBlock), kBlock, smem, s>>>(
         geo(c), u, v, Huon, Hvom, Hz, W, z_w, do_flux, do_omega, zeta1, zeta2, Zt);
     return cudaGetLastError();
 }

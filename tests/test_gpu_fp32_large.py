@@ -277,3 +277,30 @@ def test_column_solve_bulk_and_element_staging_agree(Lm):
         out.append([t.cpu().numpy() for t in (m.u, m.v, sl("ubar", 1), sl("vbar", 1))])
     for a, b in zip(out[0], out[1]):
         np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_maxflux_omega_chunk_variants_agree(precision):
+    """The fused set_maxflux/omega kernel with its interior columns' loads issued one level at a
+    time and in chunks of 4 and 8 levels (sf_ctx_tune): identical fluxes and W."""
+    import torch
+    from sailfish_b200._lib import lib, check
+    m64, m32 = _models(199)
+    m = m64 if precision == "fp64" else m32
+    p = m._p
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    out = []
+    for ch in (0, 4, 8):
+        assert lib.sf_ctx_tune(m.ctx.ptr, 0, ch) == 0
+        for t in (m.Huon, m.Hvom, m.W):
+            t.zero_()
+        check(lib.sf_maxflux_omega(m.ctx.ptr, p(m.u), p(m.v), p(m.Huon), p(m.Hvom), p(m.Hz),
+                                   p(m.W), p(m.z_w), None, None, None, st), "sf_maxflux_omega")
+        torch.cuda.synchronize()
+        out.append([t.cpu().numpy() for t in (m.Huon, m.Hvom, m.W)])
+    assert np.abs(out[0][2]).max() > 0
+    for o in out[1:]:
+        for a, b in zip(out[0], o):
+            np.testing.assert_array_equal(a, b)
+    assert lib.sf_ctx_tune(m.ctx.ptr, 0, 3) != 0
