@@ -445,13 +445,14 @@ def error_vs_fp64():
     return out
 
 
-def roms_day(args, hours=24.0, tau0=0.15, rdrag2=3e-3):
-    """The configuration's physics for one simulated day in the ROMS-form step (wind
+def roms_day(args, hours=24.0, tau0=0.15, rdrag2=3e-3, runs_of=(("fp32", "mlp"), ("fp64", "gls"))):
+    """The configuration's physics for `hours` simulated in the ROMS-form step (wind
     tau_x = tau0 cos(pi y/Ly) N/m2, quadratic bottom drag rdrag2, Coriolis, T = 4 + 20 exp(z/500)
-    for the mixing, from rest): the FP32 form with the learned closure against FP64 with plain
-    GLS every step, from identical initial states.  Returns the RMS / max differences of the
-    free surface (Zt_avg1, the surface the 3D step uses), ubar, u and v over the interior at the
-    end, with the RMS of each FP64 field, and each run's device time per step."""
+    for the mixing, from rest), run twice from identical initial states as `runs_of` says
+    ((precision, mixing) pairs: by default the FP32 form with the learned closure against FP64
+    with plain GLS every step).  Returns the RMS / max differences of the free surface
+    (Zt_avg1, the surface the 3D step uses), ubar, u and v over the interior at the end, with
+    the RMS of the second run's fields, and each run's device time per step."""
     import torch
     from sailfish_b200 import configs
     from sailfish_b200.model import Model
@@ -460,7 +461,10 @@ def roms_day(args, hours=24.0, tau0=0.15, rdrag2=3e-3):
     nsteps = int(round(hours * 3600.0 / cfg["dt"]))
     stream = torch.cuda.current_stream()
     runs, times = {}, {}
-    for prec, mode in (("fp32", "mlp"), ("fp64", "gls")):
+    keys = []
+    for prec, mode in runs_of:
+        key = "%s_%s" % (prec, mode)
+        keys.append(key)
         m = Model(g, cfg["boundary"], cfg["dt"], cfg["ndtfast"], precision=prec, semantics="roms")
         c = install_mixing(m, mode, args.config)
         m.set_forcing(c.cols.sustr.double().cpu().numpy(), c.cols.svstr.double().cpu().numpy(),
@@ -471,20 +475,21 @@ def roms_day(args, hours=24.0, tau0=0.15, rdrag2=3e-3):
         m.step(nsteps)
         b.record(stream)
         torch.cuda.synchronize()
-        times[prec] = a.elapsed_time(b) / nsteps
-        runs[prec] = {"zeta": m.Zt_avg1.clone(), "ubar": m._slot("ubar", 1).clone(),
-                      "u": m.u.clone(), "v": m.v.clone(),
-                      "fallback_columns": int(c.mask.sum()) if mode == "mlp" else None}
+        times[key] = a.elapsed_time(b) / nsteps
+        runs[key] = {"zeta": m.Zt_avg1.clone(), "ubar": m._slot("ubar", 1).clone(),
+                     "u": m.u.clone(), "v": m.v.clone(),
+                     "fallback_columns": int(c.mask.sum()) if mode == "mlp" else None}
         del m, c
         torch.cuda.empty_cache()
     J, I, N = g.J, g.I, g.N
     out = {"case": "%s, ROMS-form step, %d steps of %g s (%g h) from rest, wind %g cos(pi y/Ly) "
-                   "N/m2, quadratic drag %g" % (args.config, nsteps, cfg["dt"], hours, tau0, rdrag2),
+                   "N/m2, quadratic drag %g; %s against %s" % (
+                       args.config, nsteps, cfg["dt"], hours, tau0, rdrag2, keys[0], keys[1]),
            "units": {"zeta": "m", "ubar": "m/s", "u": "m/s", "v": "m/s"},
-           "ms_per_step": times, "fp32_fallback_columns": runs["fp32"]["fallback_columns"]}
+           "ms_per_step": times, "fallback_columns": runs[keys[0]]["fallback_columns"]}
     for k in ("zeta", "ubar", "u", "v"):
-        a64 = runs["fp64"][k].double()
-        a32 = runs["fp32"][k].double()
+        a64 = runs[keys[1]][k].double()
+        a32 = runs[keys[0]][k].double()
         if k in ("u", "v"):
             a64, a32 = a64.reshape(N + 1, J, I)[:N, 1:-1, 1:-1], a32.reshape(N + 1, J, I)[:N, 1:-1, 1:-1]
         else:
@@ -894,8 +899,9 @@ def main():
     ap.add_argument("--no-error", action="store_true", help="skip the FP32-vs-FP64 error case")
     ap.add_argument("--levels", type=int, default=None,
                     help="run the basin with this many levels (profiling cases)")
-    ap.add_argument("--day-hours", type=float, default=24.0,
-                    help="simulated hours of the ROMS-form FP32-vs-FP64 error run (0: skip)")
+    ap.add_argument("--day-hours", type=float, default=None,
+                    help="simulated hours of the ROMS-form error runs (default 24 on basin4, "
+                         "48 = 720 steps on basin1; 0: skip)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -948,11 +954,22 @@ def main():
             out["opt_fp64"]["speedup_of_value"] = out["value"] / world / out["opt_fp64"]["value"]
         if not args.no_error:
             out["error_vs_fp64"] = error_vs_fp64()
-        if args.day_hours > 0 and args.config in ("basin4", "basin4q", "basin1"):
+        # basin4: one simulated day; basin1: its 720 steps of 240 s
+        hours = args.day_hours if args.day_hours is not None else (
+            48.0 if args.config == "basin1" else 24.0)
+        if hours > 0 and args.config in ("basin4", "basin4q", "basin1"):
             try:
-                out["day_error_vs_fp64"] = roms_day(args, hours=args.day_hours)
+                out["day_error_vs_fp64"] = roms_day(args, hours=hours)
             except Exception as e:   # a blow-up check that fired, for instance
                 out["day_error_vs_fp64"] = {"failed": str(e)}
+                torch.cuda.empty_cache()
+        if hours > 0 and args.config == "basin1" and args.closure != "none":
+            # the learned closure's effect on the flow: the same FP32 step with plain GLS
+            try:
+                out["closure_uv_error_vs_gls"] = roms_day(
+                    args, hours=hours, runs_of=(("fp32", "mlp"), ("fp32", "gls")))
+            except Exception as e:
+                out["closure_uv_error_vs_gls"] = {"failed": str(e)}
                 torch.cuda.empty_cache()
         if not args.no_cpu_baseline:
             out["cpu_baseline"] = cpu_sample(args)

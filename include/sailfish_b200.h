@@ -220,10 +220,21 @@ int sf_roms_barotropic_loop(sf_ctx *ctx, sf_state2d *s, double *DU_avg2, double 
  * main2d's step (nonlinear/main2d.py:9-88); first selects forward/backward Euler. */
 int sf_roms_step2d(sf_ctx *ctx, sf_state2d *s, const void *sustr, const void *svstr,
                    double rdrag2, double dtfast, int first, sf_stream stream);
-/* Surface stress on the top level of the 3D momentum right-hand side: ru[N-1] += sustr
- * om_u on_u, rv[N-1] += svstr om_v on_v (ROMS's ru includes the stress terms). */
-int sf_roms_stress3d(sf_ctx *ctx, void *ru, void *rv, const void *sustr, const void *svstr,
-                     sf_stream stream);
+/* Surface and bottom stress on the 3D momentum right-hand side (ROMS's ru includes them):
+ * ru[N-1] += sustr om_u on_u and ru[0] -= rdrag2 ub sqrt(ub^2 + v_u^2) om_u on_u at the interior
+ * U faces (ub, v_u from the bottom level of u, v), rv likewise. */
+int sf_roms_stress3d(sf_ctx *ctx, const void *u, const void *v, void *ru, void *rv,
+                     const void *sustr, const void *svstr, double rdrag2, sf_stream stream);
+/* The ROMS-form step3d_uv (the reference's step3D_uv.kernels.cpp:512-530 with ROMS's units:
+ * right-hand side Hzu u + cff dt pm pn ru, every level solved, viscosity on the w level between
+ * two rho levels, the depth mean set to DU_avg1 / on_u from the new u) at the interior faces, and
+ * the barotropic restart: ubar_n, ubar_s (vbar likewise) = the new depth-mean velocity there,
+ * 0 elsewhere.  cff = 1, 3/2, 23/12 as sf_step3d_uv.  N <= 64. */
+int sf_roms_step3d_uv(sf_ctx *ctx, void *u, void *v, const void *ru, const void *rv,
+                      void *ubar_n, void *vbar_n, void *ubar_s, void *vbar_s, const void *Hz,
+                      const void *Akv, const void *z_r, const double *DU_avg1,
+                      const double *DV_avg1, int iic, int ntfirst, double lambda, double dt,
+                      sf_stream stream);
 /* Closed walls for the 3D velocities: u = 0 on the west and east U faces, v = 0 on the south
  * and north V faces, every level. */
 int sf_roms_closed_walls(sf_ctx *ctx, void *u, void *v, sf_stream stream);

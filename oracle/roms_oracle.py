@@ -256,3 +256,180 @@ def volume(g, zeta):
     """Total water volume above the rest level over the interior cells (closed basin)."""
     a = 1.0 / (g["pm"] * g["pn"])
     return float(np.sum((zeta * a)[1:-1, 1:-1]))
+
+
+# ---------------------------------------------------------------------------------------------
+# The baroclinic step with the ROMS-form barotropic loop (the package's semantics "roms"): the
+# reference's 3D kernels (restated in oracle/sf_oracle.c, driven as oracle.main3d drives them)
+# around this module's barotropic loop, with the surface stress on the top level of the 3D
+# right-hand side and closed walls for the 3D velocities.
+# ---------------------------------------------------------------------------------------------
+class State3D:
+    """A ROMS-form 2D State whose arrays sit in zero-guarded parents (the 3D kernels read their
+    neighbours past the array ends), beside an oracle.Ocean for the 3D fields."""
+
+    def __init__(self, grid):
+        import oracle as orc
+        J, I = grid.J, grid.I
+        S = State(J, I)
+        for name in ("zeta", "ubar", "vbar", "rzeta", "rubar", "rvbar"):
+            setattr(S, name, [orc.gzeros((J, I)), orc.gzeros((J, I))])
+        for name in ("zeta_p", "ubar_p", "vbar_p", "Zt_avg1", "DU_avg1", "DV_avg1", "DU_avg2",
+                     "DV_avg2"):
+            setattr(S, name, orc.gzeros((J, I)))
+        self.S = S
+        self.O = orc.Ocean(grid)
+
+
+def stress3d(grid, u, v, ru, rv, sustr, svstr, rdrag2):
+    """Surface and bottom stress on the 3D momentum right-hand side (ROMS's ru includes
+    + sustr om_u on_u at k = N and - bustr om_u on_u at k = 1): ru[N-1] += sustr * area and
+    ru[0] -= rdrag2 ub sqrt(ub^2 + v_u^2) * area at the interior U faces, with ub the bottom
+    level's u and v_u the four-point average of its v (area = 4 / ((pm_i + pm_i-1)(pn_i +
+    pn_i-1))); rv likewise at the interior V faces."""
+    J, I, N = grid.J, grid.I, grid.N
+    pm, pn = grid.pm.reshape(J, I), grid.pn.reshape(J, I)
+    r3u, r3v = ru.reshape(N + 1, J, I), rv.reshape(N + 1, J, I)
+    u0, v0 = u.reshape(N + 1, J, I)[0], v.reshape(N + 1, J, I)[0]
+    sj, si, sim = slice(1, J - 1), slice(2, I - 1), slice(1, I - 2)
+    area = 4.0 / ((pm[sj, si] + pm[sj, sim]) * (pn[sj, si] + pn[sj, sim]))
+    v4 = 0.25 * (((v0[sj, si] + v0[2:J, si]) + v0[sj, sim]) + v0[2:J, sim])
+    ub = u0[sj, si]
+    bustr = rdrag2 * ub * np.sqrt(ub * ub + v4 * v4)
+    r3u[N - 1][sj, si] = r3u[N - 1][sj, si] + sustr[sj, si] * area
+    r3u[0][sj, si] = r3u[0][sj, si] - bustr * area
+    vj, vi, vjm = slice(2, J - 1), slice(1, I - 1), slice(1, J - 2)
+    area = 4.0 / ((pm[vj, vi] + pm[vjm, vi]) * (pn[vj, vi] + pn[vjm, vi]))
+    u4 = 0.25 * (((u0[vj, vi] + u0[vj, 2:I]) + u0[vjm, vi]) + u0[vjm, 2:I])
+    vb = v0[vj, vi]
+    bvstr = rdrag2 * vb * np.sqrt(u4 * u4 + vb * vb)
+    r3v[N - 1][vj, vi] = r3v[N - 1][vj, vi] + svstr[vj, vi] * area
+    r3v[0][vj, vi] = r3v[0][vj, vi] - bvstr * area
+
+
+def _column_solve(grid, u3, r3, Hz, Akv, z_r, avg, on, sj, si, nj, ni, cdt, lamdt):
+    """The implicit vertical-viscosity step of the 3D velocity at the faces (sj, si), whose
+    other rho point is (nj, ni): the tridiagonal system
+      (Hzu_k - FC_k - FC_k-1) x_k + FC_k x_k+1 + FC_k-1 x_k-1 = Hzu_k u_k + cdt pmU pnU ru_k,
+    FC_k = -lamdt AKU_k+1 / DZ_k on the interface between levels k and k+1 (w level k+1; no
+    flux through the surface or the bottom, whose stresses sit in ru), solved by Thomas
+    elimination; then the depth mean is set to the barotropic transport:
+    x_k -= (sum Hzu_k x_k - avg / on) / sum Hzu_k.  Returns avg / on / sum Hzu_k, the
+    barotropic velocity the next loop starts from (step3d_uv.F's coupling, ROMS form)."""
+    J, I, N = grid.J, grid.I, grid.N
+    pm, pn = grid.pm.reshape(J, I), grid.pn.reshape(J, I)
+    H3 = Hz.reshape(N, J, I)
+    A3 = Akv.reshape(N + 1, J, I)
+    Z3 = z_r.reshape(N, J, I)
+    a = (sj, si)
+    b = (nj, ni)
+    pmU = 0.5 * (pm[a] + pm[b])
+    pnU = 0.5 * (pn[a] + pn[b])
+    fac = cdt * (pmU * pnU)
+    hzu = [0.5 * (H3[k][a] + H3[k][b]) for k in range(N)]
+    FC = []
+    for k in range(N - 1):
+        ak = 0.5 * (A3[k + 1][a] + A3[k + 1][b])
+        dz = 0.5 * ((Z3[k + 1][a] - Z3[k][a]) + (Z3[k + 1][b] - Z3[k][b]))
+        FC.append((-lamdt * ak) / dz)
+    zero = np.zeros_like(pmU)
+    FC.append(zero)
+    BC, RHS = [], []
+    for k in range(N):
+        fcm = FC[k - 1] if k > 0 else zero
+        BC.append((hzu[k] - FC[k]) - fcm)
+        RHS.append(hzu[k] * u3[k][a] + fac * r3[k][a])
+    for k in range(1, N):
+        w = FC[k - 1] / BC[k - 1]
+        BC[k] = BC[k] - w * FC[k - 1]
+        RHS[k] = RHS[k] - w * RHS[k - 1]
+    x = [None] * N
+    x[N - 1] = RHS[N - 1] / BC[N - 1]
+    for k in range(N - 2, -1, -1):
+        x[k] = (RHS[k] - FC[k] * x[k + 1]) / BC[k]
+    H = zero.copy()
+    Hu = zero.copy()
+    for k in range(N):
+        H = H + hzu[k]
+        Hu = Hu + hzu[k] * x[k]
+    target = avg[a] / on[a]
+    udiff = (Hu - target) / H
+    for k in range(N):
+        u3[k][a] = x[k] - udiff
+    return target / H
+
+
+def roms_step3d(grid, S, u, v, ru, rv, Hz, Akv, z_r, cff, dt, lam):
+    """The ROMS-form step3d_uv at the interior faces (U: j = 1..J-2, i = 2..I-2; V: j = 2..J-2,
+    i = 1..I-2) with cdt = cff dt (cff = 1, 3/2, 23/12 as the reference's AB3 start-up) and
+    lamdt = lam dt, and the barotropic restart: ubar, vbar (slots n and scratch) = the new
+    depth-mean velocities at those faces, 0 elsewhere."""
+    J, I, N = grid.J, grid.I, grid.N
+    u3, v3 = u.reshape(N + 1, J, I), v.reshape(N + 1, J, I)
+    r3u, r3v = ru.reshape(N + 1, J, I), rv.reshape(N + 1, J, I)
+    on_u, om_v = grid.on_u.reshape(J, I), grid.om_v.reshape(J, I)
+    cdt, lamdt = cff * dt, lam * dt
+    ub = np.zeros((J, I))
+    vb = np.zeros((J, I))
+    sj, si = slice(1, J - 1), slice(2, I - 1)
+    ub[sj, si] = _column_solve(grid, u3, r3u, Hz, Akv, z_r, S.DU_avg1, on_u, sj, si, sj,
+                               slice(1, I - 2), cdt, lamdt)
+    sj, si = slice(2, J - 1), slice(1, I - 1)
+    vb[sj, si] = _column_solve(grid, v3, r3v, Hz, Akv, z_r, S.DV_avg1, om_v, sj, si,
+                               slice(1, J - 2), si, cdt, lamdt)
+    for a in (S.ubar[1], S.ubar_p):
+        a[...] = ub
+    for a in (S.vbar[1], S.vbar_p):
+        a[...] = vb
+
+
+def closed_walls(grid, u, v):
+    J, I, N = grid.J, grid.I, grid.N
+    u3 = u.reshape(N + 1, J, I)
+    v3 = v.reshape(N + 1, J, I)
+    u3[:, :, 1] = 0.0
+    u3[:, :, I - 1] = 0.0
+    v3[:, 1, :] = 0.0
+    v3[:, J - 1, :] = 0.0
+
+
+def main3d(grid, B, st, nsteps, dt, ndtfast, nfast, W1, W2, sustr, svstr, rdrag2, lam=1.0,
+           iic0=0, on_step=None):
+    """Baroclinic steps in the package's "roms" order: set_maxflux, omega, set_zeta (zeta(n) =
+    Zt_avg1), rhs3d + surface and bottom stress, the ROMS-form barotropic loop, set_depth, the
+    ROMS-form step3d_uv with the barotropic restart, the reference's lateral BCs, closed
+    walls, omega.  AKv stays as it is (no mixing)."""
+    import oracle as orc
+    L = orc.lib()
+    S, O = st.S, st.O
+    N, J, I = grid.N, grid.J, grid.I
+    G = dict(h=grid.h, pm=grid.pm, pn=grid.pn, on_u=grid.on_u, om_v=grid.om_v, fomn=grid.fomn)
+    BC = B["zetaBC_bcIdxFieldIdx2"]
+    P = orc.P
+    dtfast = dt / ndtfast
+    O.Zt_avg1[:] = S.Zt_avg1.reshape(-1)
+    orc.set_depth(grid, O)
+    time = iic0 * dt
+    for k in range(nsteps):
+        iic = iic0 + k
+        L.orc_set_maxflux(grid.ref, P(O.t3("u")), P(O.t3("v")), P(O.Huon), P(O.Hvom), P(grid.Hz))
+        L.orc_omega(grid.ref, P(O.W), P(O.Huon), P(O.Hvom), P(grid.z_w), P(BC))
+        zt = S.Zt_avg1.reshape(J, I)
+        S.zeta[1][...] = zt
+        S.zeta_p[...] = zt
+        orc.rhs3d(grid, B, O)
+        stress3d(grid, O.t3("u"), O.t3("v"), O.t3("ru"), O.t3("rv"), sustr, svstr, rdrag2)
+        barotropic_loop(G, S, nfast, W1, W2, dtfast, sustr, svstr, rdrag2)
+        O.Zt_avg1[:] = S.Zt_avg1.reshape(-1)
+        orc.set_depth(grid, O)
+        cff = 1.0 if iic == 0 else (1.5 if iic == 1 else 23.0 / 12.0)
+        roms_step3d(grid, S, O.t3("u"), O.t3("v"), O.t3("ru"), O.t3("rv"), grid.Hz, O.AKv,
+                    grid.z_r, cff, dt, lam)
+        L.orc_lateral_uv_bc(grid.ref, orc.D(time), P(O.t3("u")), P(O.t3("v")),
+                            P(B["vvelBC_bcIdxFieldIdx2"]), P(B["uvelBC_bcIdxFieldType"]),
+                            P(B["vvelBC_bcIdxFieldType"]))
+        closed_walls(grid, O.t3("u"), O.t3("v"))
+        L.orc_omega(grid.ref, P(O.W), P(O.Huon), P(O.Hvom), P(grid.z_w), P(BC))
+        time += dt
+        if on_step is not None:
+            on_step(iic + 1, S, O)

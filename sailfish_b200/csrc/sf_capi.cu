@@ -1115,13 +1115,37 @@ int sf_roms_step2d(sf_ctx *c, sf_state2d *st, const void *sustr, const void *svs
     return SF_OK;
 }
 
-int sf_roms_stress3d(sf_ctx *c, void *ru, void *rv, const void *sustr, const void *svstr,
-                     sf_stream s) {
-    if (!ru || !rv || !sustr || !svstr) return fail(SF_EINVAL, "null argument");
+static double ab3_cff(int iic, int ntfirst) {   // step3D_uv.kernels.cpp:663-666
+    if (iic == ntfirst) return 1.0;
+    if (iic == ntfirst + 1) return 3.0 / 2.0;
+    return 23.0 / 12.0;
+}
+
+int sf_roms_stress3d(sf_ctx *c, const void *u, const void *v, void *ru, void *rv,
+                     const void *sustr, const void *svstr, double rdrag2, sf_stream s) {
+    if (!u || !v || !ru || !rv || !sustr || !svstr) return fail(SF_EINVAL, "null argument");
     return dispatch(c, "sf_roms_stress3d", [&](auto *t) {
         using R = std::remove_pointer_t<decltype(t)>;
-        return sf::Ops<R>::roms_stress3d(c, (R *)ru, (R *)rv, (const R *)sustr,
-                                         (const R *)svstr, S(s));
+        return sf::Ops<R>::roms_stress3d(c, (const R *)u, (const R *)v, (R *)ru, (R *)rv,
+                                         (const R *)sustr, (const R *)svstr, rdrag2, S(s));
+    });
+}
+
+int sf_roms_step3d_uv(sf_ctx *c, void *u, void *v, const void *ru, const void *rv, void *ubar_n,
+                      void *vbar_n, void *ubar_s, void *vbar_s, const void *Hz, const void *Akv,
+                      const void *z_r, const double *DU, const double *DV, int iic, int ntfirst,
+                      double lambda, double Dt, sf_stream s) {
+    if (!u || !v || !ru || !rv || !ubar_n || !vbar_n || !ubar_s || !vbar_s || !Hz || !Akv ||
+        !z_r || !DU || !DV)
+        return fail(SF_EINVAL, "null argument");
+    if (c && c->N > sf::kRomsMaxN) return fail(SF_EINVAL, "sf_roms_step3d_uv: N > 64");
+    const double cdt = ab3_cff(iic, ntfirst) * Dt, lamdt = lambda * Dt;
+    return dispatch(c, "sf_roms_step3d_uv", [&](auto *t) {
+        using R = std::remove_pointer_t<decltype(t)>;
+        return sf::Ops<R>::roms_step3d(c, (R *)u, (R *)v, (const R *)ru, (const R *)rv,
+                                       (R *)ubar_n, (R *)vbar_n, (R *)ubar_s, (R *)vbar_s,
+                                       (const R *)Hz, (const R *)Akv, (const R *)z_r, DU, DV,
+                                       cdt, lamdt, S(s));
     });
 }
 
@@ -1275,12 +1299,6 @@ int sf_check_state(sf_ctx *c, const void *zeta, const void *ubar, const void *vb
                   "non-finite or out-of-bound %s at flat index %ld (level %ld, j %ld, i %ld)",
                   kCheckNames[f < kCheckFields ? f : 0], p, lev, q / c->I, q % c->I);
     return fail(SF_ENONFINITE, msg);
-}
-
-static double ab3_cff(int iic, int ntfirst) {   // step3D_uv.kernels.cpp:663-666
-    if (iic == ntfirst) return 1.0;
-    if (iic == ntfirst + 1) return 3.0 / 2.0;
-    return 23.0 / 12.0;
 }
 
 int sf_step3d_uv(sf_ctx *c, void *u, void *v, const void *ru, const void *rv, void *ubar_t1,

@@ -198,6 +198,9 @@ inline cudaError_t launch_dep(const sf_ctx *c, void (*kern)(KArgs...), dim3 grid
     return cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
 }
 
+// Levels the ROMS-form step3d_uv holds per column (sf_roms_step3d_uv rejects more).
+constexpr int kRomsMaxN = 64;
+
 // Arguments of one phase of the ROMS-form barotropic substep (kernels in sf_roms.cuh).
 template <typename R>
 struct RomsArgs {
@@ -281,8 +284,12 @@ struct Ops {
                                     double galpha, R *bvf, cudaStream_t s);
     // the ROMS-form barotropic step (sf_roms.cuh)
     static cudaError_t roms_phase(const sf_ctx *c, const RomsArgs<R> &a, cudaStream_t s);
-    static cudaError_t roms_stress3d(const sf_ctx *c, R *ru, R *rv, const R *sustr,
-                                     const R *svstr, cudaStream_t s);
+    static cudaError_t roms_stress3d(const sf_ctx *c, const R *u, const R *v, R *ru, R *rv,
+                                     const R *sustr, const R *svstr, double rdrag2, cudaStream_t s);
+    static cudaError_t roms_step3d(const sf_ctx *c, R *u, R *v, const R *ru, const R *rv,
+                                   R *ubar_n, R *vbar_n, R *ubar_s, R *vbar_s, const R *Hz,
+                                   const R *Akv, const R *z_r, const double *DU, const double *DV,
+                                   double cdt, double lamdt, cudaStream_t s);
     static cudaError_t roms_walls3d(const sf_ctx *c, R *u, R *v, cudaStream_t s);
 };
 

@@ -169,20 +169,115 @@ __global__ void __launch_bounds__(256) k_roms_mom(Geo<R> g, RomsArgs<R> a) {
     if (a.phase == 0) a.rv_n[p] = rvnew;
 }
 
-// Surface stress on the top level of the 3D momentum right-hand side (ROMS's ru at k = N
-// includes + sustr om_u on_u): ru[N-1] += sustr * area at the interior U faces, likewise rv.
+// Surface and bottom stress on the 3D momentum right-hand side (ROMS's ru includes
+// + sustr om_u on_u at k = N and - bustr om_u on_u at k = 1): ru[N-1] += sustr * area and
+// ru[0] -= rdrag2 ub sqrt(ub^2 + v_u^2) * area at the interior U faces, ub the bottom level's u,
+// v_u the four-point average of its v; rv likewise at the interior V faces.
 template <typename R>
-__global__ void __launch_bounds__(256) k_roms_stress3d(Geo<R> g, R *__restrict__ ru,
+__global__ void __launch_bounds__(256) k_roms_stress3d(Geo<R> g, const R *__restrict__ u,
+                                                       const R *__restrict__ v, R *__restrict__ ru,
                                                        R *__restrict__ rv, const R *__restrict__ sustr,
-                                                       const R *__restrict__ svstr) {
+                                                       const R *__restrict__ svstr, R rdrag2) {
     const long p = tid_flat();
     if (p >= g.s2) return;
     const int j = fdiv((int)p, g.dI), i = (int)p - j * g.I;
     const long I = g.I, o = (long)(g.N - 1) * g.s2 + p;
+    if (i >= 2 && i <= g.I - 2 && j >= 1 && j <= g.J - 2) {
+        const R area = R(4.0) / ((g.pm[p] + g.pm[p - 1]) * (g.pn[p] + g.pn[p - 1]));
+        const R v4 = R(0.25) * (((v[p] + v[p + I]) + v[p - 1]) + v[p + I - 1]);
+        const R ub = u[p];
+        const R bustr = rdrag2 * ub * sqrt(ub * ub + v4 * v4);
+        ru[o] = ru[o] + sustr[p] * area;
+        ru[p] = ru[p] - bustr * area;
+    }
+    if (j >= 2 && j <= g.J - 2 && i >= 1 && i <= g.I - 2) {
+        const R area = R(4.0) / ((g.pm[p] + g.pm[p - I]) * (g.pn[p] + g.pn[p - I]));
+        const R u4 = R(0.25) * (((u[p] + u[p + 1]) + u[p - I]) + u[p - I + 1]);
+        const R vb = v[p];
+        const R bvstr = rdrag2 * vb * sqrt(u4 * u4 + vb * vb);
+        rv[o] = rv[o] + svstr[p] * area;
+        rv[p] = rv[p] - bvstr * area;
+    }
+}
+
+// The ROMS-form step3d_uv for one face column (d = 1: U face, d = I: V face): the implicit
+// vertical-viscosity system
+//   (Hzu_k - FC_k - FC_k-1) x_k + FC_k x_k+1 + FC_k-1 x_k-1 = Hzu_k u_k + cdt pmU pnU ru_k,
+// FC_k = -lamdt AKU_k+1 / DZ_k on the interface between levels k and k+1 (w level k+1; no flux
+// through the surface or the bottom, whose stresses are in ru), Thomas elimination in R, then
+// the depth mean set to the barotropic transport with FP64 sums: x_k -= (sum Hzu x - avg/on) /
+// sum Hzu.  Returns the new depth-mean velocity avg / on / sum Hzu.
+template <typename R>
+__device__ __forceinline__ double roms_column(const Geo<R> &g, long p, long d, R *__restrict__ u,
+                                              const R *__restrict__ ru, const R *__restrict__ Hz,
+                                              const R *__restrict__ Akv, const R *__restrict__ z_r,
+                                              double avg, R on, R cdt, R lamdt) {
+    const long s2 = g.s2;
+    const int N = g.N;
+    R fc[kRomsMaxN], bc[kRomsMaxN], rhs[kRomsMaxN], hzu[kRomsMaxN];
+    const R pmU = R(0.5) * (g.pm[p] + g.pm[p - d]);
+    const R pnU = R(0.5) * (g.pn[p] + g.pn[p - d]);
+    const R fac = cdt * (pmU * pnU);
+    for (int k = 0; k < N; ++k) {
+        const long o = (long)k * s2 + p;
+        hzu[k] = R(0.5) * (Hz[o] + Hz[o - d]);
+        if (k < N - 1) {
+            const R ak = R(0.5) * (Akv[o + s2] + Akv[o + s2 - d]);
+            const R dz = R(0.5) * ((z_r[o + s2] - z_r[o]) + (z_r[o + s2 - d] - z_r[o - d]));
+            fc[k] = (-lamdt * ak) / dz;
+        } else {
+            fc[k] = R(0);
+        }
+    }
+    for (int k = 0; k < N; ++k) {
+        const long o = (long)k * s2 + p;
+        const R fcm = k > 0 ? fc[k - 1] : R(0);
+        bc[k] = (hzu[k] - fc[k]) - fcm;
+        rhs[k] = hzu[k] * u[o] + fac * ru[o];
+    }
+    for (int k = 1; k < N; ++k) {
+        const R w = fc[k - 1] / bc[k - 1];
+        bc[k] = bc[k] - w * fc[k - 1];
+        rhs[k] = rhs[k] - w * rhs[k - 1];
+    }
+    rhs[N - 1] = rhs[N - 1] / bc[N - 1];               // x overwrites rhs
+    for (int k = N - 2; k >= 0; --k) rhs[k] = (rhs[k] - fc[k] * rhs[k + 1]) / bc[k];
+    double H = 0.0, Hu = 0.0;
+    for (int k = 0; k < N; ++k) {
+        H = H + (double)hzu[k];
+        Hu = Hu + (double)hzu[k] * (double)rhs[k];
+    }
+    const double target = avg / (double)on;
+    const double udiff = (Hu - target) / H;
+    for (int k = 0; k < N; ++k) u[(long)k * s2 + p] = (R)((double)rhs[k] - udiff);
+    return target / H;
+}
+
+// The ROMS-form step3d_uv over the interior faces (U: j = 1..J-2, i = 2..I-2; V: j = 2..J-2,
+// i = 1..I-2), one thread per rho point p doing its west U column and its south V column, and
+// the barotropic restart: ubar, vbar in slots n and scratch = the new depth-mean velocities at
+// those faces, 0 elsewhere.
+template <typename R>
+__global__ void __launch_bounds__(128) k_roms_step3d(Geo<R> g, R *__restrict__ u, R *__restrict__ v,
+                                                     const R *__restrict__ ru, const R *__restrict__ rv,
+                                                     R *__restrict__ ubar_n, R *__restrict__ vbar_n,
+                                                     R *__restrict__ ubar_s, R *__restrict__ vbar_s,
+                                                     const R *__restrict__ Hz, const R *__restrict__ Akv,
+                                                     const R *__restrict__ z_r,
+                                                     const double *__restrict__ DU,
+                                                     const double *__restrict__ DV, R cdt, R lamdt) {
+    const long p = tid_flat();
+    if (p >= g.s2) return;
+    const int j = fdiv((int)p, g.dI), i = (int)p - j * g.I;
+    R ub = R(0), vb = R(0);
     if (i >= 2 && i <= g.I - 2 && j >= 1 && j <= g.J - 2)
-        ru[o] = ru[o] + sustr[p] * (R(4.0) / ((g.pm[p] + g.pm[p - 1]) * (g.pn[p] + g.pn[p - 1])));
+        ub = (R)roms_column(g, p, 1, u, ru, Hz, Akv, z_r, DU[p], g.on_u[p], cdt, lamdt);
     if (j >= 2 && j <= g.J - 2 && i >= 1 && i <= g.I - 2)
-        rv[o] = rv[o] + svstr[p] * (R(4.0) / ((g.pm[p] + g.pm[p - I]) * (g.pn[p] + g.pn[p - I])));
+        vb = (R)roms_column(g, p, g.I, v, rv, Hz, Akv, z_r, DV[p], g.om_v[p], cdt, lamdt);
+    ubar_n[p] = ub;
+    ubar_s[p] = ub;
+    vbar_n[p] = vb;
+    vbar_s[p] = vb;
 }
 
 // Closed walls for the 3D velocities: u = 0 on the U wall faces (i = 1, I-1), v = 0 on the V
@@ -210,9 +305,20 @@ cudaError_t Ops<R>::roms_phase(const sf_ctx *c, const RomsArgs<R> &a, cudaStream
     return cudaGetLastError();
 }
 template <typename R>
-cudaError_t Ops<R>::roms_stress3d(const sf_ctx *c, R *ru, R *rv, const R *sustr, const R *svstr,
-                                  cudaStream_t s) {
-    k_roms_stress3d<R><<<blocks_for(c->s2, 256), 256, 0, s>>>(geo(c), ru, rv, sustr, svstr);
+cudaError_t Ops<R>::roms_stress3d(const sf_ctx *c, const R *u, const R *v, R *ru, R *rv,
+                                  const R *sustr, const R *svstr, double rdrag2, cudaStream_t s) {
+    k_roms_stress3d<R><<<blocks_for(c->s2, 256), 256, 0, s>>>(geo(c), u, v, ru, rv, sustr, svstr,
+                                                                (R)rdrag2);
+    return cudaGetLastError();
+}
+template <typename R>
+cudaError_t Ops<R>::roms_step3d(const sf_ctx *c, R *u, R *v, const R *ru, const R *rv, R *ubar_n,
+                                R *vbar_n, R *ubar_s, R *vbar_s, const R *Hz, const R *Akv,
+                                const R *z_r, const double *DU, const double *DV, double cdt,
+                                double lamdt, cudaStream_t s) {
+    k_roms_step3d<R><<<blocks_for(c->s2, 128), 128, 0, s>>>(geo(c), u, v, ru, rv, ubar_n, vbar_n,
+                                                              ubar_s, vbar_s, Hz, Akv, z_r, DU, DV,
+                                                              (R)cdt, (R)lamdt);
     return cudaGetLastError();
 }
 template <typename R>

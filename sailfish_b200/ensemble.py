@@ -95,6 +95,7 @@ class Ensemble(Model):
         self._started = False
         self.mixing = None
         self.check_every = 0          # sf_check_state covers single grids only
+        self.semantics = "reference"  # the ensemble steps the reference's main3d only
         self.cells = sum((g.L - 1) * (g.M - 1) * g.N for g in c.grids)
 
     KIND = {"zeta": 2, "ubar": 2, "vbar": 2, "rzeta": 2, "rubar": 2, "rvbar": 2, "Zt_avg1": 2,

@@ -363,8 +363,8 @@ class Model:
                 ctypes.byref(t2), sh), "sf_barotropic_loop")
             if self.semantics == "roms":
                 phase("k_rhs3d", lambda: (rhs(st), check(lib.sf_roms_stress3d(
-                    c, p(self.ru), p(self.rv), p(self.sustr), p(self.svstr), st),
-                    "sf_roms_stress3d")))
+                    c, p(self.u), p(self.v), p(self.ru), p(self.rv), p(self.sustr),
+                    p(self.svstr), self.rdrag2, st), "sf_roms_stress3d")))
                 phase("barotropic_loop", lambda: self._roms_loop(s, st))
                 after(cs, ev_mix)
             elif ovl_rhs:
@@ -381,13 +381,23 @@ class Model:
             self._sync_slots(s)
             self.time2D = t2.value
             phase("k_set_depth", lambda: self.set_depth(st))
-            phase("k_step3d_uv", lambda: check(lib.sf_step3d_uv_bc(
-                c, p(self.u), p(self.v), p(self.ru), p(self.rv), p(self._slot("ubar", 1)),
-                p(self._slot("vbar", 1)), p(self._slot("ubar", 2)), p(self._slot("vbar", 2)),
-                p(self.Hz), p(self.AKv), p(self.z_r), p(self.DU_avg1), p(self.DV_avg1), self.iic,
-                self.ntfirst, self.lam, self.dt, self.time, st), "sf_step3d_uv_bc"))
             if self.semantics == "roms":
-                check(lib.sf_roms_closed_walls(c, p(self.u), p(self.v), st), "sf_roms_closed_walls")
+                phase("k_step3d_uv", lambda: (check(lib.sf_roms_step3d_uv(
+                    c, p(self.u), p(self.v), p(self.ru), p(self.rv), p(self._slot("ubar", 1)),
+                    p(self._slot("vbar", 1)), p(self._slot("ubar", 2)),
+                    p(self._slot("vbar", 2)), p(self.Hz), p(self.AKv), p(self.z_r),
+                    p(self.DU_avg1), p(self.DV_avg1), self.iic, self.ntfirst, self.lam, self.dt,
+                    st), "sf_roms_step3d_uv"), check(lib.sf_lateral_uv_bc(
+                        c, self.time, p(self.u), p(self.v), st), "sf_lateral_uv_bc"),
+                    check(lib.sf_roms_closed_walls(c, p(self.u), p(self.v), st),
+                          "sf_roms_closed_walls")))
+            else:
+                phase("k_step3d_uv", lambda: check(lib.sf_step3d_uv_bc(
+                    c, p(self.u), p(self.v), p(self.ru), p(self.rv), p(self._slot("ubar", 1)),
+                    p(self._slot("vbar", 1)), p(self._slot("ubar", 2)),
+                    p(self._slot("vbar", 2)), p(self.Hz), p(self.AKv), p(self.z_r),
+                    p(self.DU_avg1), p(self.DV_avg1), self.iic, self.ntfirst, self.lam, self.dt,
+                    self.time, st), "sf_step3d_uv_bc"))
             if self.mixing is not None:
                 if mix_ovl:
                     after(s_mix, mark(cs))

@@ -189,3 +189,118 @@ def test_fp32_loop_against_fp64():
     for n, tol in (("Zt_avg1", 2e-5), ("DU_avg1", 1e-4), ("DV_avg2", 1e-4)):
         a, b = res["fp64"][n], res["fp32"][n]
         assert np.abs(b - a).max() <= tol * np.abs(a).max(), n
+
+
+# ---- the baroclinic step in ROMS form ----------------------------------------------------------
+def _case3d(Lm=24, Mm=16, N=6, dx=2e3, dt=120.0, ndtfast=20, tau0=0.1):
+    """A closed shelf basin with one seamount (depth 50..4000 m, c dtfast / dx <= 0.6), wind
+    tau0 cos(pi y / Ly) and a 5 cm surface bump, as (cfg, oracle grid, oracle boundary lists,
+    oracle state, sustr, svstr)."""
+    import oracle as orc
+    from golden_io import BND_KEYS
+    from sailfish_b200 import configs
+    cfg = configs.basin(Lm, Mm, N, dx, [(0.5, 0.6)], dt=dt, ndtfast=ndtfast)
+    g, B = cfg["grid"], cfg["boundary"]
+    og = orc.Grid(g.L, g.M, g.N, g.h, g.pm, g.pn, g.on_u, g.om_v, g.fomn, g.sc_r, g.sc_w,
+                  g.Cs_r, g.Cs_w, g.hc, g.Vtransform)
+    bd = {}
+    for name in ("zetaBC", "ubarBC", "vbarBC", "uvelBC", "vvelBC"):
+        for f in ("bcIdx", "bcIdx1", "bcIdx2", "bcIdxFieldIdx2", "bcIdxFieldType", "LBC"):
+            bd["%s_%s" % (name, f)] = getattr(getattr(B, name), f)
+    for f in BND_KEYS:
+        bd[f] = getattr(B, f)
+    st = ro.State3D(og)
+    st.S.Zt_avg1[...] = 0.05 * np.exp(-((g.x - 0.4 * g.x.max()) ** 2 + (g.y - g.y.mean()) ** 2)
+                                      / (8.0 * dx) ** 2)
+    su = _wind(g, tau0)
+    sv = 0.2 * su
+    return cfg, og, orc.Boundary(bd), st, su, sv
+
+
+def _run_oracle3d(cfg, og, B, st, su, sv, nsteps, rdrag2=3e-3, on_step=None):
+    from sailfish_b200 import host
+    nfast, w1, _ = host.set_weights(cfg["ndtfast"])
+    W1, W2 = ro.roms_weights(nfast, w1)
+    with np.errstate(all="raise"):
+        ro.main3d(og, B, st, nsteps, cfg["dt"], cfg["ndtfast"], nfast, W1, W2, su, sv, rdrag2,
+                  on_step=on_step)
+
+
+def test_oracle_3d_conserves_volume_and_couples_the_depth_mean():
+    """ROMS-form baroclinic steps with wind, drag and Coriolis over a seamount: the volume of
+    the fast-time mean surface is conserved, the 3D velocity's depth mean equals the barotropic
+    velocity the next loop starts from (the coupling step3d_uv makes), and the flow stays
+    bounded and wind-driven."""
+    cfg, og, B, st, su, sv = _case3d()
+    g = cfg["grid"]
+    G = dict(pm=g.pm, pn=g.pn)
+    v0 = ro.volume(G, st.S.Zt_avg1)
+    _run_oracle3d(cfg, og, B, st, su, sv, 12)
+    S, O, N, J, I = st.S, st.O, og.N, og.J, og.I
+    scale = np.abs(S.Zt_avg1).max() * np.sum(1.0 / (g.pm * g.pn))
+    assert abs(ro.volume(G, S.Zt_avg1) - v0) <= 1e-12 * scale
+    u = O.t3("u").reshape(N + 1, J, I)[:N]
+    Hz = og.Hz.reshape(N, J, I)
+    hzu = 0.5 * (Hz[:, :, 1:] + Hz[:, :, :-1])
+    mean = (hzu * u[:, :, 1:]).sum(0) / hzu.sum(0)
+    inner = (slice(2, J - 2), slice(2, I - 3))        # U faces i = 3..I-3 (mean[.., i-1])
+    np.testing.assert_allclose(mean[inner], S.ubar[1][2:J - 2, 3:I - 2], rtol=0,
+                               atol=1e-12 * np.abs(S.ubar[1]).max())
+    assert 1e-4 < np.abs(u).max() < 1.0
+    # relative to the depth mean, the surface layer moves downwind: east in the south, where
+    # tau_x = tau0 cos(pi y / Ly) > 0, west in the north
+    shear = u[N - 1, :, 1:] - mean
+    assert shear[J // 4, 2:I - 3].mean() > 0 > shear[3 * J // 4, 2:I - 3].mean()
+
+
+def _roms_model3d(cfg, st, su, sv, precision, rdrag2=3e-3):
+    from sailfish_b200.model import Model
+    m = Model(cfg["grid"], cfg["boundary"], cfg["dt"], cfg["ndtfast"], precision=precision,
+              semantics="roms")
+    m.set_forcing(su, sv, rdrag2)
+    m.load({"Zt_avg1": np.array(st.S.Zt_avg1)})
+    return m
+
+
+@pytest.mark.gpu
+def test_cuda_3d_steps_bit_exact_against_the_oracle():
+    """Four ROMS-form baroclinic steps (the AB3 start-up and one full-weight step) over a
+    seamount with wind, drag and Coriolis: the FP64 CUDA path and the oracle, bit for bit."""
+    import torch
+    cfg, og, B, st, su, sv = _case3d(40, 28, 8)
+    m = _roms_model3d(cfg, st, su, sv, "fp64")
+    m.step(4)
+    torch.cuda.synchronize()
+    _run_oracle3d(cfg, og, B, st, su, sv, 4)
+    s = m.state()
+    S, O = st.S, st.O
+    sh = (og.J, og.I)
+    for n in ("zeta", "ubar", "vbar"):
+        for k in range(2):
+            np.testing.assert_array_equal(s[n][s["slots"][k]].reshape(sh), getattr(S, n)[k],
+                                          err_msg="%s[%d]" % (n, k))
+    for n in ("Zt_avg1", "DU_avg1", "DV_avg1"):
+        np.testing.assert_array_equal(s[n].reshape(sh), getattr(S, n), err_msg=n)
+    for n in ("u", "v", "ru", "rv"):
+        np.testing.assert_array_equal(s[n].reshape(-1), O.t3(n), err_msg=n)
+    np.testing.assert_array_equal(s["W"].reshape(-1), O.W.reshape(-1), err_msg="W")
+    assert np.abs(O.t3("v")).max() > 1e-4
+
+
+@pytest.mark.gpu
+def test_cuda_3d_fp32_against_fp64():
+    """20 ROMS-form steps at 160 x 96 x 16: FP32 stencils with FP64 fast-time averages and
+    depth sums against FP64, relative to each field's largest magnitude."""
+    import torch
+    res = {}
+    for prec in ("fp64", "fp32"):
+        cfg, og, B, st, su, sv = _case3d(160, 96, 16)
+        m = _roms_model3d(cfg, st, su, sv, prec)
+        m.step(20)
+        torch.cuda.synchronize()
+        res[prec] = m.state()
+    a, b = res["fp64"], res["fp32"]
+    for n, tol in (("Zt_avg1", 1e-4), ("u", 1e-3), ("v", 1e-3)):
+        x, y = a[n].reshape(-1), b[n].reshape(-1)
+        assert np.isfinite(y).all(), n
+        assert np.abs(y - x).max() <= tol * np.abs(x).max(), (n, np.abs(y - x).max() / np.abs(x).max())
