@@ -459,13 +459,19 @@ def roms_day(args, hours=24.0, tau0=0.15, rdrag2=3e-3, runs_of=(("fp32", "mlp"),
     cfg = configs.CONFIGS[args.config]()
     g = cfg["grid"]
     nsteps = int(round(hours * 3600.0 / cfg["dt"]))
+    # the ROMS-form barotropic step is stable for c dtfast / dx < 0.757 (von Neumann, 2D); a
+    # configuration beyond it (basin1: 0.80 at h = 4000 m) runs with more substeps
+    ndtfast = cfg["ndtfast"]
+    courant = float(np.sqrt(10.0 * g.h.max()) * cfg["dt"] / ndtfast * max(g.pm.max(), g.pn.max()))
+    if courant > 0.7:
+        ndtfast = int(np.ceil(ndtfast * courant / 0.65))
     stream = torch.cuda.current_stream()
     runs, times = {}, {}
     keys = []
     for prec, mode in runs_of:
         key = "%s_%s" % (prec, mode)
         keys.append(key)
-        m = Model(g, cfg["boundary"], cfg["dt"], cfg["ndtfast"], precision=prec, semantics="roms")
+        m = Model(g, cfg["boundary"], cfg["dt"], ndtfast, precision=prec, semantics="roms")
         c = install_mixing(m, mode, args.config)
         m.set_forcing(c.cols.sustr.double().cpu().numpy(), c.cols.svstr.double().cpu().numpy(),
                       rdrag2)
@@ -486,6 +492,7 @@ def roms_day(args, hours=24.0, tau0=0.15, rdrag2=3e-3, runs_of=(("fp32", "mlp"),
                    "N/m2, quadratic drag %g; %s against %s" % (
                        args.config, nsteps, cfg["dt"], hours, tau0, rdrag2, keys[0], keys[1]),
            "units": {"zeta": "m", "ubar": "m/s", "u": "m/s", "v": "m/s"},
+           "ndtfast": ndtfast, "barotropic_courant_of_config": courant,
            "ms_per_step": times, "fallback_columns": runs[keys[0]]["fallback_columns"]}
     for k in ("zeta", "ubar", "u", "v"):
         a64 = runs[keys[1]][k].double()

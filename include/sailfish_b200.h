@@ -225,12 +225,21 @@ int sf_roms_step2d(sf_ctx *ctx, sf_state2d *s, const void *sustr, const void *sv
  * U faces (ub, v_u from the bottom level of u, v), rv likewise. */
 int sf_roms_stress3d(sf_ctx *ctx, const void *u, const void *v, void *ru, void *rv,
                      const void *sustr, const void *svstr, double rdrag2, sf_stream stream);
-/* The ROMS-form step3d_uv (the reference's step3D_uv.kernels.cpp:512-530 with ROMS's units:
- * right-hand side Hzu u + cff dt pm pn ru, every level solved, viscosity on the w level between
- * two rho levels, the depth mean set to DU_avg1 / on_u from the new u) at the interior faces, and
- * the barotropic restart: ubar_n, ubar_s (vbar likewise) = the new depth-mean velocity there,
- * 0 elsewhere.  cff = 1, 3/2, 23/12 as sf_step3d_uv.  N <= 64. */
-int sf_roms_step3d_uv(sf_ctx *ctx, void *u, void *v, const void *ru, const void *rv,
+/* The ROMS-form 3D momentum right-hand side (Hz-weighted, m^4/s^2) at the interior faces, 0
+ * elsewhere: Coriolis (as rhs_kernels.cpp:7-35) and second-order centred advection of momentum,
+ * horizontal (the UV_C2ADVECTION fluxes of obsolete/step2d_LF_AM3.h.py:1244-1300, per level
+ * with Huon/Hvom) and vertical (with W).  It replaces the reference's rhs3d (nonlinear/rhs.py:16-93)
+ * in the ROMS-form step, whose runnable advection (rhs_kernels.cpp:71-196) is not ROMS's. */
+int sf_roms_rhs3d(sf_ctx *ctx, const void *u, const void *v, const void *Huon, const void *Hvom,
+                  const void *W, const void *Hz, void *ru, void *rv, sf_stream stream);
+/* The ROMS-form step3d_uv (the reference's step3D_uv.kernels.cpp:512-530 with ROMS's units and
+ * time stepping: right-hand side Hzu u + dt pm pn (c0 ru(n) + c1 ru(n-1) + c2 ru(n-2)) with the
+ * Adams-Bashforth weights of step iic - ntfirst (Euler, AB2, AB3), every level solved, viscosity
+ * on the w level between two rho levels, the depth mean set to DU_avg1 / on_u from the new u) at
+ * the interior faces, and the barotropic restart: ubar_n, ubar_s (vbar likewise) = the new
+ * depth-mean velocity there, 0 elsewhere.  N <= 64. */
+int sf_roms_step3d_uv(sf_ctx *ctx, void *u, void *v, const void *ru0, const void *ru1,
+                      const void *ru2, const void *rv0, const void *rv1, const void *rv2,
                       void *ubar_n, void *vbar_n, void *ubar_s, void *vbar_s, const void *Hz,
                       const void *Akv, const void *z_r, const double *DU_avg1,
                       const double *DV_avg1, int iic, int ntfirst, double lambda, double dt,

@@ -279,6 +279,74 @@ class State3D:
             setattr(S, name, orc.gzeros((J, I)))
         self.S = S
         self.O = orc.Ocean(grid)
+        n3 = (grid.N + 1) * J * I
+        self.ru3 = [np.zeros(n3) for _ in range(3)]   # newest first
+        self.rv3 = [np.zeros(n3) for _ in range(3)]
+
+
+def rhs3d(grid, u, v, Huon, Hvom, W, ru, rv):
+    """The ROMS-form 3D momentum right-hand side (m^4/s^2, Hz-weighted as ROMS's ru) at the
+    interior faces, 0 elsewhere: Coriolis as ROMS's (UFx = Hz fomn (v_j + v_j+1)/2 at rho
+    points, ru += (UFx_i + UFx_i-1)/2; rv -= (VFe_j + VFe_j-1)/2), then second-order centred
+    advection of momentum, horizontal (the UV_C2ADVECTION fluxes of the reference's ROMS
+    transcription, obsolete/step2d_LF_AM3.h.py:1244-1300, per level with Huon/Hvom for
+    DUon/DVom) and vertical (FC = (u_k-1 + u_k)/4 (W_i + W_i-1) on the interior w levels, 0
+    at the bottom and the surface).  The fluxes through the closed walls vanish with the
+    normal transport there.  The reference's runnable rhs3d (rhs_kernels.cpp:71-196) is not
+    this advection (its flux form drops the transport factor), so the ROMS-form step has its
+    own."""
+    J, I, N = grid.J, grid.I, grid.N
+    u3, v3 = u.reshape(N + 1, J, I), v.reshape(N + 1, J, I)
+    Hu, Hv, W3 = Huon.reshape(N + 1, J, I), Hvom.reshape(N + 1, J, I), W.reshape(N + 1, J, I)
+    H3 = grid.Hz.reshape(N, J, I)
+    fomn = grid.fomn.reshape(J, I)
+    r3u, r3v = ru.reshape(N + 1, J, I), rv.reshape(N + 1, J, I)
+    ru[:] = 0.0
+    rv[:] = 0.0
+    uj, ui = slice(1, J - 1), slice(2, I - 1)          # U faces
+    vj, vi = slice(2, J - 1), slice(1, I - 1)          # V faces
+    for k in range(N):
+        uk, vk, hu, hv = u3[k], v3[k], Hu[k], Hv[k]
+        cff = H3[k] * fomn
+        UF = np.zeros((J, I))
+        UF[:J - 1] = cff[:J - 1] * ((vk[:J - 1] + vk[1:]) * 0.5)
+        VF = np.zeros((J, I))
+        VF[:, :I - 1] = cff[:, :I - 1] * ((uk[:, :I - 1] + uk[:, 1:]) * 0.5)
+        UFx = np.zeros((J, I))                         # at rho (j, i): U faces i and i+1
+        UFx[:, :I - 1] = (0.25 * (hu[:, :I - 1] + hu[:, 1:])) * (uk[:, :I - 1] + uk[:, 1:])
+        UFe = np.zeros((J, I))                         # at psi (j, i): rows j-1 and j
+        UFe[1:, 1:] = (0.25 * (hv[1:, 1:] + hv[1:, :I - 1])) * (uk[1:, 1:] + uk[:J - 1, 1:])
+        cor = (UF[uj, ui] + UF[uj, 1:I - 2]) * 0.5
+        adv = (UFx[uj, ui] - UFx[uj, 1:I - 2]) + (UFe[2:J, ui] - UFe[uj, ui])
+        r3u[k][uj, ui] = cor - adv
+        VFx = np.zeros((J, I))                         # at psi (j, i): columns i-1 and i
+        VFx[1:, 1:] = (0.25 * (hu[1:, 1:] + hu[:J - 1, 1:])) * (vk[1:, 1:] + vk[1:, :I - 1])
+        VFe = np.zeros((J, I))                         # at rho (j, i): V faces j and j+1
+        VFe[:J - 1] = (0.25 * (hv[:J - 1] + hv[1:])) * (vk[:J - 1] + vk[1:])
+        cor = -((VF[vj, vi] + VF[1:J - 2, vi]) * 0.5)
+        adv = (VFx[vj, 2:I] - VFx[vj, vi]) + (VFe[vj, vi] - VFe[1:J - 2, vi])
+        r3v[k][vj, vi] = cor - adv
+    for w in range(1, N):                              # w level between rho w-1 and w
+        Ww = W3[w]
+        FCu = (0.25 * (u3[w - 1][uj, ui] + u3[w][uj, ui])) * (Ww[uj, ui] + Ww[uj, 1:I - 2])
+        FCv = (0.25 * (v3[w - 1][vj, vi] + v3[w][vj, vi])) * (Ww[vj, vi] + Ww[1:J - 2, vi])
+        r3u[w][uj, ui] = r3u[w][uj, ui] + FCu
+        r3v[w][vj, vi] = r3v[w][vj, vi] + FCv
+    for w in range(1, N):
+        Ww = W3[w]
+        FCu = (0.25 * (u3[w - 1][uj, ui] + u3[w][uj, ui])) * (Ww[uj, ui] + Ww[uj, 1:I - 2])
+        FCv = (0.25 * (v3[w - 1][vj, vi] + v3[w][vj, vi])) * (Ww[vj, vi] + Ww[1:J - 2, vi])
+        r3u[w - 1][uj, ui] = r3u[w - 1][uj, ui] - FCu
+        r3v[w - 1][vj, vi] = r3v[w - 1][vj, vi] - FCv
+
+
+AB3 = ((1.0, 0.0, 0.0), (1.5, -0.5, 0.0), (23.0 / 12.0, -16.0 / 12.0, 5.0 / 12.0))
+
+
+def ab3_coefficients(k):
+    """Adams-Bashforth weights of the right-hand sides at steps n, n-1, n-2 for the k-th step
+    since the start (forward Euler, then AB2, then AB3: ROMS's 3D momentum time stepping)."""
+    return AB3[min(k, 2)]
 
 
 def stress3d(grid, u, v, ru, rv, sustr, svstr, rdrag2):
@@ -307,15 +375,16 @@ def stress3d(grid, u, v, ru, rv, sustr, svstr, rdrag2):
     r3v[0][vj, vi] = r3v[0][vj, vi] - bvstr * area
 
 
-def _column_solve(grid, u3, r3, Hz, Akv, z_r, avg, on, sj, si, nj, ni, cdt, lamdt):
+def _column_solve(grid, u3, rs, c, Hz, Akv, z_r, avg, on, sj, si, nj, ni, dt, lamdt):
     """The implicit vertical-viscosity step of the 3D velocity at the faces (sj, si), whose
     other rho point is (nj, ni): the tridiagonal system
-      (Hzu_k - FC_k - FC_k-1) x_k + FC_k x_k+1 + FC_k-1 x_k-1 = Hzu_k u_k + cdt pmU pnU ru_k,
-    FC_k = -lamdt AKU_k+1 / DZ_k on the interface between levels k and k+1 (w level k+1; no
-    flux through the surface or the bottom, whose stresses sit in ru), solved by Thomas
-    elimination; then the depth mean is set to the barotropic transport:
-    x_k -= (sum Hzu_k x_k - avg / on) / sum Hzu_k.  Returns avg / on / sum Hzu_k, the
-    barotropic velocity the next loop starts from (step3d_uv.F's coupling, ROMS form)."""
+      (Hzu_k - FC_k - FC_k-1) x_k + FC_k x_k+1 + FC_k-1 x_k-1 = Hzu_k u_k + dt pmU pnU r_k,
+    r_k = (c0 ru_k(n) + c1 ru_k(n-1)) + c2 ru_k(n-2) (rs = the three right-hand sides, c their
+    Adams-Bashforth weights), FC_k = -lamdt AKU_k+1 / DZ_k on the interface between levels k
+    and k+1 (w level k+1; no flux through the surface or the bottom, whose stresses sit in
+    ru), solved by Thomas elimination; then the depth mean is set to the barotropic
+    transport: x_k -= (sum Hzu_k x_k - avg / on) / sum Hzu_k.  Returns avg / on / sum Hzu_k,
+    the barotropic velocity the next loop starts from (step3d_uv.F's coupling, ROMS form)."""
     J, I, N = grid.J, grid.I, grid.N
     pm, pn = grid.pm.reshape(J, I), grid.pn.reshape(J, I)
     H3 = Hz.reshape(N, J, I)
@@ -325,7 +394,7 @@ def _column_solve(grid, u3, r3, Hz, Akv, z_r, avg, on, sj, si, nj, ni, cdt, lamd
     b = (nj, ni)
     pmU = 0.5 * (pm[a] + pm[b])
     pnU = 0.5 * (pn[a] + pn[b])
-    fac = cdt * (pmU * pnU)
+    fac = dt * (pmU * pnU)
     hzu = [0.5 * (H3[k][a] + H3[k][b]) for k in range(N)]
     FC = []
     for k in range(N - 1):
@@ -338,7 +407,8 @@ def _column_solve(grid, u3, r3, Hz, Akv, z_r, avg, on, sj, si, nj, ni, cdt, lamd
     for k in range(N):
         fcm = FC[k - 1] if k > 0 else zero
         BC.append((hzu[k] - FC[k]) - fcm)
-        RHS.append(hzu[k] * u3[k][a] + fac * r3[k][a])
+        r = (c[0] * rs[0][k][a] + c[1] * rs[1][k][a]) + c[2] * rs[2][k][a]
+        RHS.append(hzu[k] * u3[k][a] + fac * r)
     for k in range(1, N):
         w = FC[k - 1] / BC[k - 1]
         BC[k] = BC[k] - w * FC[k - 1]
@@ -359,24 +429,25 @@ def _column_solve(grid, u3, r3, Hz, Akv, z_r, avg, on, sj, si, nj, ni, cdt, lamd
     return target / H
 
 
-def roms_step3d(grid, S, u, v, ru, rv, Hz, Akv, z_r, cff, dt, lam):
+def roms_step3d(grid, S, u, v, ru3, rv3, c, Hz, Akv, z_r, dt, lam):
     """The ROMS-form step3d_uv at the interior faces (U: j = 1..J-2, i = 2..I-2; V: j = 2..J-2,
-    i = 1..I-2) with cdt = cff dt (cff = 1, 3/2, 23/12 as the reference's AB3 start-up) and
-    lamdt = lam dt, and the barotropic restart: ubar, vbar (slots n and scratch) = the new
-    depth-mean velocities at those faces, 0 elsewhere."""
+    i = 1..I-2) with the right-hand sides ru3 = (ru(n), ru(n-1), ru(n-2)) weighted by c
+    (ab3_coefficients) and lamdt = lam dt, and the barotropic restart: ubar, vbar (slots n and
+    scratch) = the new depth-mean velocities at those faces, 0 elsewhere."""
     J, I, N = grid.J, grid.I, grid.N
     u3, v3 = u.reshape(N + 1, J, I), v.reshape(N + 1, J, I)
-    r3u, r3v = ru.reshape(N + 1, J, I), rv.reshape(N + 1, J, I)
+    rs_u = [r.reshape(N + 1, J, I) for r in ru3]
+    rs_v = [r.reshape(N + 1, J, I) for r in rv3]
     on_u, om_v = grid.on_u.reshape(J, I), grid.om_v.reshape(J, I)
-    cdt, lamdt = cff * dt, lam * dt
+    lamdt = lam * dt
     ub = np.zeros((J, I))
     vb = np.zeros((J, I))
     sj, si = slice(1, J - 1), slice(2, I - 1)
-    ub[sj, si] = _column_solve(grid, u3, r3u, Hz, Akv, z_r, S.DU_avg1, on_u, sj, si, sj,
-                               slice(1, I - 2), cdt, lamdt)
+    ub[sj, si] = _column_solve(grid, u3, rs_u, c, Hz, Akv, z_r, S.DU_avg1, on_u, sj, si, sj,
+                               slice(1, I - 2), dt, lamdt)
     sj, si = slice(2, J - 1), slice(1, I - 1)
-    vb[sj, si] = _column_solve(grid, v3, r3v, Hz, Akv, z_r, S.DV_avg1, om_v, sj, si,
-                               slice(1, J - 2), si, cdt, lamdt)
+    vb[sj, si] = _column_solve(grid, v3, rs_v, c, Hz, Akv, z_r, S.DV_avg1, om_v, sj, si,
+                               slice(1, J - 2), si, dt, lamdt)
     for a in (S.ubar[1], S.ubar_p):
         a[...] = ub
     for a in (S.vbar[1], S.vbar_p):
@@ -396,9 +467,11 @@ def closed_walls(grid, u, v):
 def main3d(grid, B, st, nsteps, dt, ndtfast, nfast, W1, W2, sustr, svstr, rdrag2, lam=1.0,
            iic0=0, on_step=None):
     """Baroclinic steps in the package's "roms" order: set_maxflux, omega, set_zeta (zeta(n) =
-    Zt_avg1), rhs3d + surface and bottom stress, the ROMS-form barotropic loop, set_depth, the
-    ROMS-form step3d_uv with the barotropic restart, the reference's lateral BCs, closed
-    walls, omega.  AKv stays as it is (no mixing)."""
+    Zt_avg1), the ROMS-form rhs3d + surface and bottom stress into the newest of three
+    right-hand-side slots, the ROMS-form barotropic loop, set_depth, the ROMS-form step3d_uv
+    (Adams-Bashforth over the three slots) with the barotropic restart, the reference's
+    lateral BCs, closed walls, omega.  AKv stays as it is (no mixing).  st.ru3/st.rv3 hold the
+    slots, newest first; the k-th step since the start takes ab3_coefficients(k - iic0)."""
     import oracle as orc
     L = orc.lib()
     S, O = st.S, st.O
@@ -417,14 +490,16 @@ def main3d(grid, B, st, nsteps, dt, ndtfast, nfast, W1, W2, sustr, svstr, rdrag2
         zt = S.Zt_avg1.reshape(J, I)
         S.zeta[1][...] = zt
         S.zeta_p[...] = zt
-        orc.rhs3d(grid, B, O)
-        stress3d(grid, O.t3("u"), O.t3("v"), O.t3("ru"), O.t3("rv"), sustr, svstr, rdrag2)
+        st.ru3.insert(0, st.ru3.pop())
+        st.rv3.insert(0, st.rv3.pop())
+        ru, rv = st.ru3[0], st.rv3[0]
+        rhs3d(grid, O.t3("u"), O.t3("v"), O.Huon, O.Hvom, O.W, ru, rv)
+        stress3d(grid, O.t3("u"), O.t3("v"), ru, rv, sustr, svstr, rdrag2)
         barotropic_loop(G, S, nfast, W1, W2, dtfast, sustr, svstr, rdrag2)
         O.Zt_avg1[:] = S.Zt_avg1.reshape(-1)
         orc.set_depth(grid, O)
-        cff = 1.0 if iic == 0 else (1.5 if iic == 1 else 23.0 / 12.0)
-        roms_step3d(grid, S, O.t3("u"), O.t3("v"), O.t3("ru"), O.t3("rv"), grid.Hz, O.AKv,
-                    grid.z_r, cff, dt, lam)
+        roms_step3d(grid, S, O.t3("u"), O.t3("v"), st.ru3, st.rv3, ab3_coefficients(k), grid.Hz,
+                    O.AKv, grid.z_r, dt, lam)
         L.orc_lateral_uv_bc(grid.ref, orc.D(time), P(O.t3("u")), P(O.t3("v")),
                             P(B["vvelBC_bcIdxFieldIdx2"]), P(B["uvelBC_bcIdxFieldType"]),
                             P(B["vvelBC_bcIdxFieldType"]))

@@ -1131,21 +1131,38 @@ int sf_roms_stress3d(sf_ctx *c, const void *u, const void *v, void *ru, void *rv
     });
 }
 
-int sf_roms_step3d_uv(sf_ctx *c, void *u, void *v, const void *ru, const void *rv, void *ubar_n,
-                      void *vbar_n, void *ubar_s, void *vbar_s, const void *Hz, const void *Akv,
-                      const void *z_r, const double *DU, const double *DV, int iic, int ntfirst,
-                      double lambda, double Dt, sf_stream s) {
-    if (!u || !v || !ru || !rv || !ubar_n || !vbar_n || !ubar_s || !vbar_s || !Hz || !Akv ||
-        !z_r || !DU || !DV)
+int sf_roms_rhs3d(sf_ctx *c, const void *u, const void *v, const void *Huon, const void *Hvom,
+                  const void *W, const void *Hz, void *ru, void *rv, sf_stream s) {
+    if (!u || !v || !Huon || !Hvom || !W || !Hz || !ru || !rv) return fail(SF_EINVAL, "null argument");
+    return dispatch(c, "sf_roms_rhs3d", [&](auto *t) {
+        using R = std::remove_pointer_t<decltype(t)>;
+        return sf::Ops<R>::roms_rhs3d(c, (const R *)u, (const R *)v, (const R *)Huon,
+                                      (const R *)Hvom, (const R *)W, (const R *)Hz, (R *)ru,
+                                      (R *)rv, S(s));
+    });
+}
+
+int sf_roms_step3d_uv(sf_ctx *c, void *u, void *v, const void *ru0, const void *ru1,
+                      const void *ru2, const void *rv0, const void *rv1, const void *rv2,
+                      void *ubar_n, void *vbar_n, void *ubar_s, void *vbar_s, const void *Hz,
+                      const void *Akv, const void *z_r, const double *DU, const double *DV,
+                      int iic, int ntfirst, double lambda, double Dt, sf_stream s) {
+    if (!u || !v || !ru0 || !ru1 || !ru2 || !rv0 || !rv1 || !rv2 || !ubar_n || !vbar_n ||
+        !ubar_s || !vbar_s || !Hz || !Akv || !z_r || !DU || !DV)
         return fail(SF_EINVAL, "null argument");
+    if (iic < ntfirst) return fail(SF_EINVAL, "sf_roms_step3d_uv: iic < ntfirst");
     if (c && c->N > sf::kRomsMaxN) return fail(SF_EINVAL, "sf_roms_step3d_uv: N > 64");
-    const double cdt = ab3_cff(iic, ntfirst) * Dt, lamdt = lambda * Dt;
+    // Adams-Bashforth weights of ru(n), ru(n-1), ru(n-2): forward Euler, AB2, then AB3
+    static const double kAB[3][3] = {{1.0, 0.0, 0.0}, {1.5, -0.5, 0.0},
+                                     {23.0 / 12.0, -16.0 / 12.0, 5.0 / 12.0}};
+    const double *coef = kAB[iic - ntfirst < 2 ? iic - ntfirst : 2];
     return dispatch(c, "sf_roms_step3d_uv", [&](auto *t) {
         using R = std::remove_pointer_t<decltype(t)>;
-        return sf::Ops<R>::roms_step3d(c, (R *)u, (R *)v, (const R *)ru, (const R *)rv,
-                                       (R *)ubar_n, (R *)vbar_n, (R *)ubar_s, (R *)vbar_s,
-                                       (const R *)Hz, (const R *)Akv, (const R *)z_r, DU, DV,
-                                       cdt, lamdt, S(s));
+        const R *ru[3] = {(const R *)ru0, (const R *)ru1, (const R *)ru2};
+        const R *rv[3] = {(const R *)rv0, (const R *)rv1, (const R *)rv2};
+        return sf::Ops<R>::roms_step3d(c, (R *)u, (R *)v, ru, rv, coef, (R *)ubar_n, (R *)vbar_n,
+                                       (R *)ubar_s, (R *)vbar_s, (const R *)Hz, (const R *)Akv,
+                                       (const R *)z_r, DU, DV, Dt, lambda * Dt, S(s));
     });
 }
 

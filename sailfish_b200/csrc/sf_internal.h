@@ -286,10 +286,14 @@ struct Ops {
     static cudaError_t roms_phase(const sf_ctx *c, const RomsArgs<R> &a, cudaStream_t s);
     static cudaError_t roms_stress3d(const sf_ctx *c, const R *u, const R *v, R *ru, R *rv,
                                      const R *sustr, const R *svstr, double rdrag2, cudaStream_t s);
-    static cudaError_t roms_step3d(const sf_ctx *c, R *u, R *v, const R *ru, const R *rv,
-                                   R *ubar_n, R *vbar_n, R *ubar_s, R *vbar_s, const R *Hz,
-                                   const R *Akv, const R *z_r, const double *DU, const double *DV,
-                                   double cdt, double lamdt, cudaStream_t s);
+    static cudaError_t roms_rhs3d(const sf_ctx *c, const R *u, const R *v, const R *Huon,
+                                  const R *Hvom, const R *W, const R *Hz, R *ru, R *rv,
+                                  cudaStream_t s);
+    static cudaError_t roms_step3d(const sf_ctx *c, R *u, R *v, const R *const *ru,
+                                   const R *const *rv, const double *coef, R *ubar_n, R *vbar_n,
+                                   R *ubar_s, R *vbar_s, const R *Hz, const R *Akv, const R *z_r,
+                                   const double *DU, const double *DV, double dt, double lamdt,
+                                   cudaStream_t s);
     static cudaError_t roms_walls3d(const sf_ctx *c, R *u, R *v, cudaStream_t s);
 };
 

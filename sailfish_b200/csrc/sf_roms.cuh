@@ -169,6 +169,72 @@ __global__ void __launch_bounds__(256) k_roms_mom(Geo<R> g, RomsArgs<R> a) {
     if (a.phase == 0) a.rv_n[p] = rvnew;
 }
 
+// The ROMS-form 3D momentum right-hand side at the interior faces (U: j = 1..J-2, i = 2..I-2;
+// V: j = 2..J-2, i = 1..I-2), 0 elsewhere, every level: Coriolis as ROMS's (and the
+// reference's addCoriolis), then second-order centred advection of momentum: horizontal
+// fluxes UFx = (Huon_i + Huon_i+1)/4 (u_i + u_i+1) at rho points and UFe = (Hvom_i +
+// Hvom_i-1)/4 (u_j + u_j-1) at psi points (the UV_C2ADVECTION form of the reference's ROMS
+// transcription, obsolete/step2d_LF_AM3.h.py:1244-1300, per level), V alike, and vertical
+// fluxes FC_w = (u_w-1 + u_w)/4 (W_w + W_w,i-1) on the interior w levels.  One thread per rho
+// point p (its west U face and south V face), levels in order; the expressions keep the
+// oracle's operand order (oracle/roms_oracle.py, rhs3d).
+template <typename R>
+__device__ __forceinline__ R roms_fc(const R *__restrict__ q, const R *__restrict__ W, long o,
+                                     long s2, long p, long d) {
+    // flux through w level w (o = w s2) at the face p with the other rho point p - d
+    return (R(0.25) * (q[o - s2 + p] + q[o + p])) * (W[o + p] + W[o + p - d]);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_roms_rhs3d(Geo<R> g, const R *__restrict__ u,
+                                                    const R *__restrict__ v,
+                                                    const R *__restrict__ Hu,
+                                                    const R *__restrict__ Hv,
+                                                    const R *__restrict__ W,
+                                                    const R *__restrict__ Hz,
+                                                    R *__restrict__ ru, R *__restrict__ rv) {
+    const long p = tid_flat();
+    if (p >= g.s2) return;
+    const int j = fdiv((int)p, g.dI), i = (int)p - j * g.I;
+    const long I = g.I, s2 = g.s2;
+    const int N = g.N;
+    const bool uf = i >= 2 && i <= g.I - 2 && j >= 1 && j <= g.J - 2;
+    const bool vf = j >= 2 && j <= g.J - 2 && i >= 1 && i <= g.I - 2;
+    const R *fomn = g.fomn;
+    for (int k = 0; k <= N; ++k) {
+        const long o = (long)k * s2;
+        R tu = R(0), tv = R(0);
+        if (k < N && uf) {
+            const R *uk = u + o, *vk = v + o, *hu = Hu + o, *hv = Hv + o, *hz = Hz + o;
+            const R UFp = (hz[p] * fomn[p]) * ((vk[p] + vk[p + I]) * R(0.5));
+            const R UFw = (hz[p - 1] * fomn[p - 1]) * ((vk[p - 1] + vk[p - 1 + I]) * R(0.5));
+            const R cor = (UFp + UFw) * R(0.5);
+            const R Xp = (R(0.25) * (hu[p] + hu[p + 1])) * (uk[p] + uk[p + 1]);
+            const R Xw = (R(0.25) * (hu[p - 1] + hu[p])) * (uk[p - 1] + uk[p]);
+            const R En = (R(0.25) * (hv[p + I] + hv[p + I - 1])) * (uk[p + I] + uk[p]);
+            const R Es = (R(0.25) * (hv[p] + hv[p - 1])) * (uk[p] + uk[p - I]);
+            tu = cor - ((Xp - Xw) + (En - Es));
+            if (k > 0) tu = tu + roms_fc(u, W, o, s2, p, 1);
+            if (k < N - 1) tu = tu - roms_fc(u, W, o + s2, s2, p, 1);
+        }
+        if (k < N && vf) {
+            const R *uk = u + o, *vk = v + o, *hu = Hu + o, *hv = Hv + o, *hz = Hz + o;
+            const R VFp = (hz[p] * fomn[p]) * ((uk[p] + uk[p + 1]) * R(0.5));
+            const R VFs = (hz[p - I] * fomn[p - I]) * ((uk[p - I] + uk[p - I + 1]) * R(0.5));
+            const R cor = -((VFp + VFs) * R(0.5));
+            const R Xe = (R(0.25) * (hu[p + 1] + hu[p + 1 - I])) * (vk[p + 1] + vk[p]);
+            const R Xw = (R(0.25) * (hu[p] + hu[p - I])) * (vk[p] + vk[p - 1]);
+            const R Ep = (R(0.25) * (hv[p] + hv[p + I])) * (vk[p] + vk[p + I]);
+            const R Es = (R(0.25) * (hv[p - I] + hv[p])) * (vk[p - I] + vk[p]);
+            tv = cor - ((Xe - Xw) + (Ep - Es));
+            if (k > 0) tv = tv + roms_fc(v, W, o, s2, p, I);
+            if (k < N - 1) tv = tv - roms_fc(v, W, o + s2, s2, p, I);
+        }
+        ru[o + p] = tu;
+        rv[o + p] = tv;
+    }
+}
+
 // Surface and bottom stress on the 3D momentum right-hand side (ROMS's ru includes
 // + sustr om_u on_u at k = N and - bustr om_u on_u at k = 1): ru[N-1] += sustr * area and
 // ru[0] -= rdrag2 ub sqrt(ub^2 + v_u^2) * area at the interior U faces, ub the bottom level's u,
@@ -202,22 +268,29 @@ __global__ void __launch_bounds__(256) k_roms_stress3d(Geo<R> g, const R *__rest
 
 // The ROMS-form step3d_uv for one face column (d = 1: U face, d = I: V face): the implicit
 // vertical-viscosity system
-//   (Hzu_k - FC_k - FC_k-1) x_k + FC_k x_k+1 + FC_k-1 x_k-1 = Hzu_k u_k + cdt pmU pnU ru_k,
-// FC_k = -lamdt AKU_k+1 / DZ_k on the interface between levels k and k+1 (w level k+1; no flux
-// through the surface or the bottom, whose stresses are in ru), Thomas elimination in R, then
-// the depth mean set to the barotropic transport with FP64 sums: x_k -= (sum Hzu x - avg/on) /
-// sum Hzu.  Returns the new depth-mean velocity avg / on / sum Hzu.
+//   (Hzu_k - FC_k - FC_k-1) x_k + FC_k x_k+1 + FC_k-1 x_k-1 = Hzu_k u_k + dt pmU pnU r_k,
+// r_k = (c0 ru_k(n) + c1 ru_k(n-1)) + c2 ru_k(n-2) (Adams-Bashforth), FC_k = -lamdt AKU_k+1 /
+// DZ_k on the interface between levels k and k+1 (w level k+1; no flux through the surface or
+// the bottom, whose stresses are in ru), Thomas elimination in R, then the depth mean set to
+// the barotropic transport with FP64 sums: x_k -= (sum Hzu x - avg/on) / sum Hzu.  Returns the
+// new depth-mean velocity avg / on / sum Hzu.
+template <typename R>
+struct RomsRhs {
+    const R *r0, *r1, *r2;   // right-hand sides at n, n-1, n-2
+};
+
 template <typename R>
 __device__ __forceinline__ double roms_column(const Geo<R> &g, long p, long d, R *__restrict__ u,
-                                              const R *__restrict__ ru, const R *__restrict__ Hz,
+                                              RomsRhs<R> rs, R c0, R c1, R c2,
+                                              const R *__restrict__ Hz,
                                               const R *__restrict__ Akv, const R *__restrict__ z_r,
-                                              double avg, R on, R cdt, R lamdt) {
+                                              double avg, R on, R dt, R lamdt) {
     const long s2 = g.s2;
     const int N = g.N;
     R fc[kRomsMaxN], bc[kRomsMaxN], rhs[kRomsMaxN], hzu[kRomsMaxN];
     const R pmU = R(0.5) * (g.pm[p] + g.pm[p - d]);
     const R pnU = R(0.5) * (g.pn[p] + g.pn[p - d]);
-    const R fac = cdt * (pmU * pnU);
+    const R fac = dt * (pmU * pnU);
     for (int k = 0; k < N; ++k) {
         const long o = (long)k * s2 + p;
         hzu[k] = R(0.5) * (Hz[o] + Hz[o - d]);
@@ -233,7 +306,8 @@ __device__ __forceinline__ double roms_column(const Geo<R> &g, long p, long d, R
         const long o = (long)k * s2 + p;
         const R fcm = k > 0 ? fc[k - 1] : R(0);
         bc[k] = (hzu[k] - fc[k]) - fcm;
-        rhs[k] = hzu[k] * u[o] + fac * ru[o];
+        const R r = (c0 * rs.r0[o] + c1 * rs.r1[o]) + c2 * rs.r2[o];
+        rhs[k] = hzu[k] * u[o] + fac * r;
     }
     for (int k = 1; k < N; ++k) {
         const R w = fc[k - 1] / bc[k - 1];
@@ -259,21 +333,21 @@ __device__ __forceinline__ double roms_column(const Geo<R> &g, long p, long d, R
 // those faces, 0 elsewhere.
 template <typename R>
 __global__ void __launch_bounds__(128) k_roms_step3d(Geo<R> g, R *__restrict__ u, R *__restrict__ v,
-                                                     const R *__restrict__ ru, const R *__restrict__ rv,
+                                                     RomsRhs<R> ru, RomsRhs<R> rv, R c0, R c1, R c2,
                                                      R *__restrict__ ubar_n, R *__restrict__ vbar_n,
                                                      R *__restrict__ ubar_s, R *__restrict__ vbar_s,
                                                      const R *__restrict__ Hz, const R *__restrict__ Akv,
                                                      const R *__restrict__ z_r,
                                                      const double *__restrict__ DU,
-                                                     const double *__restrict__ DV, R cdt, R lamdt) {
+                                                     const double *__restrict__ DV, R dt, R lamdt) {
     const long p = tid_flat();
     if (p >= g.s2) return;
     const int j = fdiv((int)p, g.dI), i = (int)p - j * g.I;
     R ub = R(0), vb = R(0);
     if (i >= 2 && i <= g.I - 2 && j >= 1 && j <= g.J - 2)
-        ub = (R)roms_column(g, p, 1, u, ru, Hz, Akv, z_r, DU[p], g.on_u[p], cdt, lamdt);
+        ub = (R)roms_column(g, p, 1, u, ru, c0, c1, c2, Hz, Akv, z_r, DU[p], g.on_u[p], dt, lamdt);
     if (j >= 2 && j <= g.J - 2 && i >= 1 && i <= g.I - 2)
-        vb = (R)roms_column(g, p, g.I, v, rv, Hz, Akv, z_r, DV[p], g.om_v[p], cdt, lamdt);
+        vb = (R)roms_column(g, p, g.I, v, rv, c0, c1, c2, Hz, Akv, z_r, DV[p], g.om_v[p], dt, lamdt);
     ubar_n[p] = ub;
     ubar_s[p] = ub;
     vbar_n[p] = vb;
@@ -312,13 +386,22 @@ cudaError_t Ops<R>::roms_stress3d(const sf_ctx *c, const R *u, const R *v, R *ru
     return cudaGetLastError();
 }
 template <typename R>
-cudaError_t Ops<R>::roms_step3d(const sf_ctx *c, R *u, R *v, const R *ru, const R *rv, R *ubar_n,
-                                R *vbar_n, R *ubar_s, R *vbar_s, const R *Hz, const R *Akv,
-                                const R *z_r, const double *DU, const double *DV, double cdt,
-                                double lamdt, cudaStream_t s) {
-    k_roms_step3d<R><<<blocks_for(c->s2, 128), 128, 0, s>>>(geo(c), u, v, ru, rv, ubar_n, vbar_n,
-                                                              ubar_s, vbar_s, Hz, Akv, z_r, DU, DV,
-                                                              (R)cdt, (R)lamdt);
+cudaError_t Ops<R>::roms_rhs3d(const sf_ctx *c, const R *u, const R *v, const R *Huon,
+                               const R *Hvom, const R *W, const R *Hz, R *ru, R *rv,
+                               cudaStream_t s) {
+    k_roms_rhs3d<R><<<blocks_for(c->s2, 256), 256, 0, s>>>(geo(c), u, v, Huon, Hvom, W, Hz, ru, rv);
+    return cudaGetLastError();
+}
+template <typename R>
+cudaError_t Ops<R>::roms_step3d(const sf_ctx *c, R *u, R *v, const R *const *ru, const R *const *rv,
+                                const double *coef, R *ubar_n, R *vbar_n, R *ubar_s, R *vbar_s,
+                                const R *Hz, const R *Akv, const R *z_r, const double *DU,
+                                const double *DV, double dt, double lamdt, cudaStream_t s) {
+    const RomsRhs<R> a{ru[0], ru[1], ru[2]}, b{rv[0], rv[1], rv[2]};
+    k_roms_step3d<R><<<blocks_for(c->s2, 128), 128, 0, s>>>(geo(c), u, v, a, b, (R)coef[0],
+                                                              (R)coef[1], (R)coef[2], ubar_n,
+                                                              vbar_n, ubar_s, vbar_s, Hz, Akv,
+                                                              z_r, DU, DV, (R)dt, (R)lamdt);
     return cudaGetLastError();
 }
 template <typename R>

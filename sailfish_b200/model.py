@@ -181,6 +181,10 @@ class Model:
             self.sustr = z(J * I)
             self.svstr = z(J * I)
             self.rdrag2 = 0.0
+            # the 3D right-hand sides of steps n, n-1, n-2 (Adams-Bashforth), newest first;
+            # self.ru / self.rv are the newest
+            self._ru3 = [self.ru, z(N + 1, J, I), z(N + 1, J, I)]
+            self._rv3 = [self.rv, z(N + 1, J, I), z(N + 1, J, I)]
         # blow-up check (sf_check_state) after every check_every-th step (0: never); a failed
         # check raises SailfishError with status SF_ENONFINITE
         self.check_every = 0
@@ -362,9 +366,14 @@ class Model:
                 self._w1.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), self.dtfast,
                 ctypes.byref(t2), sh), "sf_barotropic_loop")
             if self.semantics == "roms":
-                phase("k_rhs3d", lambda: (rhs(st), check(lib.sf_roms_stress3d(
-                    c, p(self.u), p(self.v), p(self.ru), p(self.rv), p(self.sustr),
-                    p(self.svstr), self.rdrag2, st), "sf_roms_stress3d")))
+                for r3 in (self._ru3, self._rv3):   # the oldest slot takes step n's
+                    r3.insert(0, r3.pop())
+                self.ru, self.rv = self._ru3[0], self._rv3[0]
+                phase("k_rhs3d", lambda: (check(lib.sf_roms_rhs3d(
+                    c, p(self.u), p(self.v), p(self.Huon), p(self.Hvom), p(self.W), p(self.Hz),
+                    p(self.ru), p(self.rv), st), "sf_roms_rhs3d"), check(lib.sf_roms_stress3d(
+                        c, p(self.u), p(self.v), p(self.ru), p(self.rv), p(self.sustr),
+                        p(self.svstr), self.rdrag2, st), "sf_roms_stress3d")))
                 phase("barotropic_loop", lambda: self._roms_loop(s, st))
                 after(cs, ev_mix)
             elif ovl_rhs:
@@ -383,7 +392,8 @@ class Model:
             phase("k_set_depth", lambda: self.set_depth(st))
             if self.semantics == "roms":
                 phase("k_step3d_uv", lambda: (check(lib.sf_roms_step3d_uv(
-                    c, p(self.u), p(self.v), p(self.ru), p(self.rv), p(self._slot("ubar", 1)),
+                    c, p(self.u), p(self.v), *[p(t) for t in self._ru3],
+                    *[p(t) for t in self._rv3], p(self._slot("ubar", 1)),
                     p(self._slot("vbar", 1)), p(self._slot("ubar", 2)),
                     p(self._slot("vbar", 2)), p(self.Hz), p(self.AKv), p(self.z_r),
                     p(self.DU_avg1), p(self.DV_avg1), self.iic, self.ntfirst, self.lam, self.dt,

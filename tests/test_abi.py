@@ -43,3 +43,25 @@ def test_version_and_argument_errors():
     assert L.sf_ctx_create(ctypes.byref(d), ctypes.byref(out)) == _lib.SF_EINVAL
     assert L.sf_rhs3d(None, *([None] * 9)) == _lib.SF_EINVAL
     assert L.sf_ctx_destroy(None) == _lib.SF_OK
+
+
+def declared_arity():
+    """name -> number of parameters of each prototype in the header."""
+    with open(os.path.join(ROOT, "include", "sailfish_b200.h")) as f:
+        text = f.read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    out = {}
+    for name, params in re.findall(r"\b(sf_[a-z0-9_]+)\s*\(([^()]*)\)\s*;", text):
+        params = params.strip()
+        out[name] = 0 if params in ("", "void") else params.count(",") + 1
+    return out
+
+
+def test_ctypes_signatures_match_the_header_arity():
+    """Each ctypes signature has as many arguments as the header's prototype (a missing or extra
+    argument would shift every later one)."""
+    from sailfish_b200 import _lib
+    arity = declared_arity()
+    assert len(arity) >= 20
+    for name, n in arity.items():
+        assert len(_lib.SIGNATURES[name]) == n, (name, len(_lib.SIGNATURES[name]), n)

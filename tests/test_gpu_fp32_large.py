@@ -283,7 +283,9 @@ def test_column_solve_bulk_and_element_staging_agree(Lm):
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 def test_maxflux_omega_chunk_variants_agree(precision):
     """The fused set_maxflux/omega kernel with its interior columns' loads issued one level at a
-    time and in chunks of 4 and 8 levels (sf_ctx_tune): identical fluxes and W."""
+    time and in chunks of 4 and 8 levels (sf_ctx_tune): identical fluxes and W in FP64 (built
+    without FMA contraction); in FP32 the variants' code may contract different products into
+    FMAs, so they agree to a few units of FP32 rounding of each field's scale."""
     import torch
     from sailfish_b200._lib import lib, check
     m64, m32 = _models(199)
@@ -302,5 +304,8 @@ def test_maxflux_omega_chunk_variants_agree(precision):
     assert np.abs(out[0][2]).max() > 0
     for o in out[1:]:
         for a, b in zip(out[0], o):
-            np.testing.assert_array_equal(a, b)
+            if precision == "fp64":
+                np.testing.assert_array_equal(a, b)
+            else:
+                assert np.abs(b - a).max() <= 4e-6 * np.abs(a).max()
     assert lib.sf_ctx_tune(m.ctx.ptr, 0, 3) != 0

@@ -264,8 +264,9 @@ def _roms_model3d(cfg, st, su, sv, precision, rdrag2=3e-3):
 
 @pytest.mark.gpu
 def test_cuda_3d_steps_bit_exact_against_the_oracle():
-    """Four ROMS-form baroclinic steps (the AB3 start-up and one full-weight step) over a
-    seamount with wind, drag and Coriolis: the FP64 CUDA path and the oracle, bit for bit."""
+    """Four ROMS-form baroclinic steps (Euler, AB2, then AB3 over the three right-hand sides)
+    over a seamount with wind, drag and Coriolis: the FP64 CUDA path and the oracle, bit for
+    bit, including the three right-hand-side slots."""
     import torch
     cfg, og, B, st, su, sv = _case3d(40, 28, 8)
     m = _roms_model3d(cfg, st, su, sv, "fp64")
@@ -281,8 +282,11 @@ def test_cuda_3d_steps_bit_exact_against_the_oracle():
                                           err_msg="%s[%d]" % (n, k))
     for n in ("Zt_avg1", "DU_avg1", "DV_avg1"):
         np.testing.assert_array_equal(s[n].reshape(sh), getattr(S, n), err_msg=n)
-    for n in ("u", "v", "ru", "rv"):
+    for n in ("u", "v"):
         np.testing.assert_array_equal(s[n].reshape(-1), O.t3(n), err_msg=n)
+    for k in range(3):      # the right-hand sides of the last three steps, newest first
+        np.testing.assert_array_equal(m._ru3[k].cpu().numpy().reshape(-1), st.ru3[k], err_msg="ru%d" % k)
+        np.testing.assert_array_equal(m._rv3[k].cpu().numpy().reshape(-1), st.rv3[k], err_msg="rv%d" % k)
     np.testing.assert_array_equal(s["W"].reshape(-1), O.W.reshape(-1), err_msg="W")
     assert np.abs(O.t3("v")).max() > 1e-4
 
