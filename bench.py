@@ -494,20 +494,29 @@ def roms_day(args, hours=24.0, tau0=0.15, rdrag2=3e-3, runs_of=(("fp32", "mlp"),
            "units": {"zeta": "m", "ubar": "m/s", "u": "m/s", "v": "m/s"},
            "ndtfast": ndtfast, "barotropic_courant_of_config": courant,
            "ms_per_step": times, "fallback_columns": runs[keys[0]]["fallback_columns"]}
-    for k in ("zeta", "ubar", "u", "v"):
-        a64 = runs[keys[1]][k].double()
-        a32 = runs[keys[0]][k].double()
-        if k in ("u", "v"):
-            a64, a32 = a64.reshape(N + 1, J, I)[:N, 1:-1, 1:-1], a32.reshape(N + 1, J, I)[:N, 1:-1, 1:-1]
-        else:
-            a64, a32 = a64.reshape(J, I)[1:-1, 1:-1], a32.reshape(J, I)[1:-1, 1:-1]
-        d = a32 - a64
-        out[k] = {"rms": float(d.pow(2).mean().sqrt()), "max": float(d.abs().max()),
-                  "rms_fp64_field": float(a64.pow(2).mean().sqrt()),
-                  "finite": bool(torch.isfinite(a32).all() and torch.isfinite(a64).all())}
+    def diff(ka, kb):
+        res = {}
+        for k in ("zeta", "ubar", "u", "v"):
+            a64 = runs[kb][k].double()
+            a32 = runs[ka][k].double()
+            if k in ("u", "v"):
+                a64 = a64.reshape(N + 1, J, I)[:N, 1:-1, 1:-1]
+                a32 = a32.reshape(N + 1, J, I)[:N, 1:-1, 1:-1]
+            else:
+                a64, a32 = a64.reshape(J, I)[1:-1, 1:-1], a32.reshape(J, I)[1:-1, 1:-1]
+            d = a32 - a64
+            res[k] = {"rms": float(d.pow(2).mean().sqrt()), "max": float(d.abs().max()),
+                      "rms_fp64_field": float(a64.pow(2).mean().sqrt()),
+                      "finite": bool(torch.isfinite(a32).all() and torch.isfinite(a64).all())}
+        return res
+
+    out.update(diff(keys[0], keys[1]))
     out["targets"] = {"zeta_rms_m": 1e-4, "uv_rms_m_per_s": 1e-3,
                       "met": bool(out["zeta"]["rms"] <= 1e-4 and out["u"]["rms"] <= 1e-3 and
                                   out["v"]["rms"] <= 1e-3)}
+    if len(keys) > 2:   # the same difference split into its two causes, via the third run
+        out["decomposition"] = {"%s_vs_%s" % (keys[2], keys[1]): diff(keys[2], keys[1]),
+                                "%s_vs_%s" % (keys[0], keys[2]): diff(keys[0], keys[2])}
     del runs
     torch.cuda.empty_cache()
     return out
@@ -966,7 +975,8 @@ def main():
             48.0 if args.config == "basin1" else 24.0)
         if hours > 0 and args.config in ("basin4", "basin4q", "basin1"):
             try:
-                out["day_error_vs_fp64"] = roms_day(args, hours=hours)
+                out["day_error_vs_fp64"] = roms_day(
+                    args, hours=hours, runs_of=(("fp32", "mlp"), ("fp64", "gls"), ("fp32", "gls")))
             except Exception as e:   # a blow-up check that fired, for instance
                 out["day_error_vs_fp64"] = {"failed": str(e)}
                 torch.cuda.empty_cache()

@@ -179,10 +179,15 @@ int sf_ctx_set_graphs(sf_ctx *ctx, int enable);
  * (default, the faster on one B200) for per-element cp.async staging.  Results are identical
  * either way.  No counterpart in the reference. */
 int sf_ctx_set_bulk(sf_ctx *ctx, int enable);
-/* Tuning knobs of a context's kernels (results identical for every value):
- * SF_TUNE_MO_CHUNK: 0, 4 or 8 levels whose loads the fused set_maxflux/omega kernel issues
- * together on columns whose fluxes it all computes itself.  No counterpart in the reference. */
+/* Tuning knobs of a context's kernels (no counterpart in the reference):
+ * SF_TUNE_MO_CHUNK: 0, 4 (default) or 8 levels whose loads the fused set_maxflux/omega kernel
+ *   issues together on columns whose fluxes it all computes itself;
+ * SF_TUNE_PRED_PAIR: 1 (default) for the fused predictor's paired form (two nodes per thread,
+ *   vector loads) on grids with an even row length and aligned fields, 0 for the scalar form.
+ * Results are identical for every value in FP64; in FP32 the compiler may contract products
+ * into FMAs differently in the variants, so they agree to the rounding of FP32. */
 #define SF_TUNE_MO_CHUNK 0
+#define SF_TUNE_PRED_PAIR 1
 int sf_ctx_tune(sf_ctx *ctx, int knob, int value);
 /* Turn programmatic dependent launch of the barotropic loop's kernels on (default) or off:
  * with it each kernel's blocks become resident while its predecessor's last wave runs and wait
@@ -226,22 +231,24 @@ int sf_roms_step2d(sf_ctx *ctx, sf_state2d *s, const void *sustr, const void *sv
 int sf_roms_stress3d(sf_ctx *ctx, const void *u, const void *v, void *ru, void *rv,
                      const void *sustr, const void *svstr, double rdrag2, sf_stream stream);
 /* The ROMS-form 3D momentum right-hand side (Hz-weighted, m^4/s^2) at the interior faces, 0
- * elsewhere: Coriolis (as rhs_kernels.cpp:7-35) and second-order centred advection of momentum,
- * horizontal (the UV_C2ADVECTION fluxes of obsolete/step2d_LF_AM3.h.py:1244-1300, per level
- * with Huon/Hvom) and vertical (with W).  It replaces the reference's rhs3d (nonlinear/rhs.py:16-93)
- * in the ROMS-form step, whose runnable advection (rhs_kernels.cpp:71-196) is not ROMS's. */
+ * elsewhere: Coriolis (as rhs_kernels.cpp:7-35) and second-order centred horizontal advection of
+ * momentum (the UV_C2ADVECTION fluxes of obsolete/step2d_LF_AM3.h.py:1244-1300, per level with
+ * Huon/Hvom); the vertical advection is implicit in sf_roms_step3d_uv.  It replaces the
+ * reference's rhs3d (nonlinear/rhs.py:16-93) in the ROMS-form step, whose runnable advection
+ * (rhs_kernels.cpp:71-196) is not ROMS's. */
 int sf_roms_rhs3d(sf_ctx *ctx, const void *u, const void *v, const void *Huon, const void *Hvom,
-                  const void *W, const void *Hz, void *ru, void *rv, sf_stream stream);
+                  const void *Hz, void *ru, void *rv, sf_stream stream);
 /* The ROMS-form step3d_uv (the reference's step3D_uv.kernels.cpp:512-530 with ROMS's units and
  * time stepping: right-hand side Hzu u + dt pm pn (c0 ru(n) + c1 ru(n-1) + c2 ru(n-2)) with the
  * Adams-Bashforth weights of step iic - ntfirst (Euler, AB2, AB3), every level solved, viscosity
- * on the w level between two rho levels, the depth mean set to DU_avg1 / on_u from the new u) at
- * the interior faces, and the barotropic restart: ubar_n, ubar_s (vbar likewise) = the new
- * depth-mean velocity there, 0 elsewhere.  N <= 64. */
+ * on the w level between two rho levels, vertical advection by the volume fluxes W implicit in
+ * the same tridiagonal system (backward-Euler upwind), the depth mean set to DU_avg1 / on_u
+ * from the new u) at the interior faces, and the barotropic restart: ubar_n, ubar_s (vbar
+ * likewise) = the new depth-mean velocity there, 0 elsewhere.  N <= 64. */
 int sf_roms_step3d_uv(sf_ctx *ctx, void *u, void *v, const void *ru0, const void *ru1,
                       const void *ru2, const void *rv0, const void *rv1, const void *rv2,
                       void *ubar_n, void *vbar_n, void *ubar_s, void *vbar_s, const void *Hz,
-                      const void *Akv, const void *z_r, const double *DU_avg1,
+                      const void *Akv, const void *z_r, const void *W, const double *DU_avg1,
                       const double *DV_avg1, int iic, int ntfirst, double lambda, double dt,
                       sf_stream stream);
 /* Closed walls for the 3D velocities: u = 0 on the west and east U faces, v = 0 on the south

@@ -284,20 +284,19 @@ class State3D:
         self.rv3 = [np.zeros(n3) for _ in range(3)]
 
 
-def rhs3d(grid, u, v, Huon, Hvom, W, ru, rv):
+def rhs3d(grid, u, v, Huon, Hvom, ru, rv):
     """The ROMS-form 3D momentum right-hand side (m^4/s^2, Hz-weighted as ROMS's ru) at the
     interior faces, 0 elsewhere: Coriolis as ROMS's (UFx = Hz fomn (v_j + v_j+1)/2 at rho
     points, ru += (UFx_i + UFx_i-1)/2; rv -= (VFe_j + VFe_j-1)/2), then second-order centred
     advection of momentum, horizontal (the UV_C2ADVECTION fluxes of the reference's ROMS
     transcription, obsolete/step2d_LF_AM3.h.py:1244-1300, per level with Huon/Hvom for
-    DUon/DVom) and vertical (FC = (u_k-1 + u_k)/4 (W_i + W_i-1) on the interior w levels, 0
-    at the bottom and the surface).  The fluxes through the closed walls vanish with the
-    normal transport there.  The reference's runnable rhs3d (rhs_kernels.cpp:71-196) is not
-    this advection (its flux form drops the transport factor), so the ROMS-form step has its
-    own."""
+    DUon/DVom).  The fluxes through the closed walls vanish with the normal transport there.
+    The vertical advection is implicit, in the column solve (_column_solve).  The reference's
+    runnable rhs3d (rhs_kernels.cpp:71-196) is not this advection (its flux form drops the
+    transport factor), so the ROMS-form step has its own."""
     J, I, N = grid.J, grid.I, grid.N
     u3, v3 = u.reshape(N + 1, J, I), v.reshape(N + 1, J, I)
-    Hu, Hv, W3 = Huon.reshape(N + 1, J, I), Hvom.reshape(N + 1, J, I), W.reshape(N + 1, J, I)
+    Hu, Hv = Huon.reshape(N + 1, J, I), Hvom.reshape(N + 1, J, I)
     H3 = grid.Hz.reshape(N, J, I)
     fomn = grid.fomn.reshape(J, I)
     r3u, r3v = ru.reshape(N + 1, J, I), rv.reshape(N + 1, J, I)
@@ -326,18 +325,6 @@ def rhs3d(grid, u, v, Huon, Hvom, W, ru, rv):
         cor = -((VF[vj, vi] + VF[1:J - 2, vi]) * 0.5)
         adv = (VFx[vj, 2:I] - VFx[vj, vi]) + (VFe[vj, vi] - VFe[1:J - 2, vi])
         r3v[k][vj, vi] = cor - adv
-    for w in range(1, N):                              # w level between rho w-1 and w
-        Ww = W3[w]
-        FCu = (0.25 * (u3[w - 1][uj, ui] + u3[w][uj, ui])) * (Ww[uj, ui] + Ww[uj, 1:I - 2])
-        FCv = (0.25 * (v3[w - 1][vj, vi] + v3[w][vj, vi])) * (Ww[vj, vi] + Ww[1:J - 2, vi])
-        r3u[w][uj, ui] = r3u[w][uj, ui] + FCu
-        r3v[w][vj, vi] = r3v[w][vj, vi] + FCv
-    for w in range(1, N):
-        Ww = W3[w]
-        FCu = (0.25 * (u3[w - 1][uj, ui] + u3[w][uj, ui])) * (Ww[uj, ui] + Ww[uj, 1:I - 2])
-        FCv = (0.25 * (v3[w - 1][vj, vi] + v3[w][vj, vi])) * (Ww[vj, vi] + Ww[1:J - 2, vi])
-        r3u[w - 1][uj, ui] = r3u[w - 1][uj, ui] - FCu
-        r3v[w - 1][vj, vi] = r3v[w - 1][vj, vi] - FCv
 
 
 AB3 = ((1.0, 0.0, 0.0), (1.5, -0.5, 0.0), (23.0 / 12.0, -16.0 / 12.0, 5.0 / 12.0))
@@ -375,48 +362,63 @@ def stress3d(grid, u, v, ru, rv, sustr, svstr, rdrag2):
     r3v[0][vj, vi] = r3v[0][vj, vi] - bvstr * area
 
 
-def _column_solve(grid, u3, rs, c, Hz, Akv, z_r, avg, on, sj, si, nj, ni, dt, lamdt):
-    """The implicit vertical-viscosity step of the 3D velocity at the faces (sj, si), whose
-    other rho point is (nj, ni): the tridiagonal system
-      (Hzu_k - FC_k - FC_k-1) x_k + FC_k x_k+1 + FC_k-1 x_k-1 = Hzu_k u_k + dt pmU pnU r_k,
+def _column_solve(grid, u3, rs, c, Hz, Akv, z_r, W, avg, on, sj, si, nj, ni, dt, lamdt):
+    """The implicit vertical step of the 3D velocity at the faces (sj, si), whose other rho
+    point is (nj, ni): with F_w the upwind vertical advective flux through w level w (w_w x_w-1
+    where w_w > 0, w_w x_w where w_w < 0; w_w = fac (W_w + W_w,nbr) / 2, 0 at the bottom and the
+    surface) and fac = dt pmU pnU,
+      Hzu_k x_k - [viscosity] + (F_k+1 - F_k) = Hzu_k u_k + fac r_k,
     r_k = (c0 ru_k(n) + c1 ru_k(n-1)) + c2 ru_k(n-2) (rs = the three right-hand sides, c their
-    Adams-Bashforth weights), FC_k = -lamdt AKU_k+1 / DZ_k on the interface between levels k
-    and k+1 (w level k+1; no flux through the surface or the bottom, whose stresses sit in
-    ru), solved by Thomas elimination; then the depth mean is set to the barotropic
-    transport: x_k -= (sum Hzu_k x_k - avg / on) / sum Hzu_k.  Returns avg / on / sum Hzu_k,
-    the barotropic velocity the next loop starts from (step3d_uv.F's coupling, ROMS form)."""
+    Adams-Bashforth weights); the viscosity couples levels k and k+1 through FC_k = -lamdt
+    AKU_k+1 / DZ_k (w level k+1; no flux through the surface or the bottom, whose stresses sit
+    in ru).  So, with w+ = max(w, 0) and w- = min(w, 0), the lower, main and upper diagonals are
+      l_k = FC_k-1 - w+_k,  b_k = (Hzu_k - FC_k - FC_k-1) + (w+_k+1 - w-_k),  u_k = FC_k + w-_k+1,
+    an M-matrix at any vertical Courant number, solved by Thomas elimination (backward-Euler
+    upwind vertical advection: basin4's thin shelf and slope layers take vertical Courant
+    numbers above 1, where the explicit and the implicit centred forms broke down).  Then the
+    depth mean is set to the barotropic transport: x_k -= (sum Hzu_k x_k - avg / on) / sum
+    Hzu_k (the advective fluxes telescope out of the column sum).  Returns avg / on / sum
+    Hzu_k, the barotropic velocity the next loop starts from (step3d_uv.F's coupling)."""
     J, I, N = grid.J, grid.I, grid.N
     pm, pn = grid.pm.reshape(J, I), grid.pn.reshape(J, I)
     H3 = Hz.reshape(N, J, I)
     A3 = Akv.reshape(N + 1, J, I)
     Z3 = z_r.reshape(N, J, I)
+    W3 = W.reshape(N + 1, J, I)
     a = (sj, si)
     b = (nj, ni)
     pmU = 0.5 * (pm[a] + pm[b])
     pnU = 0.5 * (pn[a] + pn[b])
     fac = dt * (pmU * pnU)
     hzu = [0.5 * (H3[k][a] + H3[k][b]) for k in range(N)]
-    FC = []
+    zero = np.zeros_like(pmU)
+    FC, WP, WM = [], [zero], [zero]         # w+ and w- on w levels 0..N
     for k in range(N - 1):
         ak = 0.5 * (A3[k + 1][a] + A3[k + 1][b])
         dz = 0.5 * ((Z3[k + 1][a] - Z3[k][a]) + (Z3[k + 1][b] - Z3[k][b]))
         FC.append((-lamdt * ak) / dz)
-    zero = np.zeros_like(pmU)
+        wk = fac * (0.5 * (W3[k + 1][a] + W3[k + 1][b]))
+        WP.append(np.where(wk > 0.0, wk, 0.0))
+        WM.append(np.where(wk < 0.0, wk, 0.0))
     FC.append(zero)
-    BC, RHS = [], []
+    WP.append(zero)
+    WM.append(zero)
+    LO, BC, UP, RHS = [], [], [], []
     for k in range(N):
         fcm = FC[k - 1] if k > 0 else zero
-        BC.append((hzu[k] - FC[k]) - fcm)
+        LO.append(fcm - WP[k])
+        BC.append(((hzu[k] - FC[k]) - fcm) + (WP[k + 1] - WM[k]))
+        UP.append(FC[k] + WM[k + 1])
         r = (c[0] * rs[0][k][a] + c[1] * rs[1][k][a]) + c[2] * rs[2][k][a]
         RHS.append(hzu[k] * u3[k][a] + fac * r)
     for k in range(1, N):
-        w = FC[k - 1] / BC[k - 1]
-        BC[k] = BC[k] - w * FC[k - 1]
+        w = LO[k] / BC[k - 1]
+        BC[k] = BC[k] - w * UP[k - 1]
         RHS[k] = RHS[k] - w * RHS[k - 1]
     x = [None] * N
     x[N - 1] = RHS[N - 1] / BC[N - 1]
     for k in range(N - 2, -1, -1):
-        x[k] = (RHS[k] - FC[k] * x[k + 1]) / BC[k]
+        x[k] = (RHS[k] - UP[k] * x[k + 1]) / BC[k]
     H = zero.copy()
     Hu = zero.copy()
     for k in range(N):
@@ -429,11 +431,12 @@ def _column_solve(grid, u3, rs, c, Hz, Akv, z_r, avg, on, sj, si, nj, ni, dt, la
     return target / H
 
 
-def roms_step3d(grid, S, u, v, ru3, rv3, c, Hz, Akv, z_r, dt, lam):
+def roms_step3d(grid, S, u, v, ru3, rv3, c, Hz, Akv, z_r, W, dt, lam):
     """The ROMS-form step3d_uv at the interior faces (U: j = 1..J-2, i = 2..I-2; V: j = 2..J-2,
     i = 1..I-2) with the right-hand sides ru3 = (ru(n), ru(n-1), ru(n-2)) weighted by c
     (ab3_coefficients) and lamdt = lam dt, and the barotropic restart: ubar, vbar (slots n and
-    scratch) = the new depth-mean velocities at those faces, 0 elsewhere."""
+    scratch) = the new depth-mean velocities at those faces, 0 elsewhere.  W: the vertical
+    volume fluxes of the step (omega at its start)."""
     J, I, N = grid.J, grid.I, grid.N
     u3, v3 = u.reshape(N + 1, J, I), v.reshape(N + 1, J, I)
     rs_u = [r.reshape(N + 1, J, I) for r in ru3]
@@ -443,10 +446,10 @@ def roms_step3d(grid, S, u, v, ru3, rv3, c, Hz, Akv, z_r, dt, lam):
     ub = np.zeros((J, I))
     vb = np.zeros((J, I))
     sj, si = slice(1, J - 1), slice(2, I - 1)
-    ub[sj, si] = _column_solve(grid, u3, rs_u, c, Hz, Akv, z_r, S.DU_avg1, on_u, sj, si, sj,
+    ub[sj, si] = _column_solve(grid, u3, rs_u, c, Hz, Akv, z_r, W, S.DU_avg1, on_u, sj, si, sj,
                                slice(1, I - 2), dt, lamdt)
     sj, si = slice(2, J - 1), slice(1, I - 1)
-    vb[sj, si] = _column_solve(grid, v3, rs_v, c, Hz, Akv, z_r, S.DV_avg1, om_v, sj, si,
+    vb[sj, si] = _column_solve(grid, v3, rs_v, c, Hz, Akv, z_r, W, S.DV_avg1, om_v, sj, si,
                                slice(1, J - 2), si, dt, lamdt)
     for a in (S.ubar[1], S.ubar_p):
         a[...] = ub
@@ -493,13 +496,13 @@ def main3d(grid, B, st, nsteps, dt, ndtfast, nfast, W1, W2, sustr, svstr, rdrag2
         st.ru3.insert(0, st.ru3.pop())
         st.rv3.insert(0, st.rv3.pop())
         ru, rv = st.ru3[0], st.rv3[0]
-        rhs3d(grid, O.t3("u"), O.t3("v"), O.Huon, O.Hvom, O.W, ru, rv)
+        rhs3d(grid, O.t3("u"), O.t3("v"), O.Huon, O.Hvom, ru, rv)
         stress3d(grid, O.t3("u"), O.t3("v"), ru, rv, sustr, svstr, rdrag2)
         barotropic_loop(G, S, nfast, W1, W2, dtfast, sustr, svstr, rdrag2)
         O.Zt_avg1[:] = S.Zt_avg1.reshape(-1)
         orc.set_depth(grid, O)
         roms_step3d(grid, S, O.t3("u"), O.t3("v"), st.ru3, st.rv3, ab3_coefficients(k), grid.Hz,
-                    O.AKv, grid.z_r, dt, lam)
+                    O.AKv, grid.z_r, O.W, dt, lam)
         L.orc_lateral_uv_bc(grid.ref, orc.D(time), P(O.t3("u")), P(O.t3("v")),
                             P(B["vvelBC_bcIdxFieldIdx2"]), P(B["uvelBC_bcIdxFieldType"]),
                             P(B["vvelBC_bcIdxFieldType"]))

@@ -74,8 +74,8 @@ SIGNATURES = {
                                 _dp, _d, _vp],
     "sf_roms_step2d": [_vp, ctypes.POINTER(State2D), _vp, _vp, _d, _d, _i, _vp],
     "sf_roms_stress3d": [_vp] * 7 + [_d, _vp],
-    "sf_roms_rhs3d": [_vp] * 10,
-    "sf_roms_step3d_uv": [_vp] * 18 + [_i, _i, _d, _d, _vp],
+    "sf_roms_rhs3d": [_vp] * 9,
+    "sf_roms_step3d_uv": [_vp] * 19 + [_i, _i, _d, _d, _vp],
     "sf_roms_closed_walls": [_vp] * 4,
     "sf_rhs3d": [_vp] * 10,
     "sf_set_maxflux": [_vp] * 7,

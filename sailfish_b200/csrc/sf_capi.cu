@@ -876,6 +876,15 @@ int sf_ctx_tune(sf_ctx *c, int knob, int value) {
         if (value != 0 && value != 4 && value != 8) return fail(SF_EINVAL, "chunk is 0, 4 or 8");
         c->mo_chunk = value;
         return SF_OK;
+    case SF_TUNE_PRED_PAIR:
+        if (value != 0 && value != 1) return fail(SF_EINVAL, "pair is 0 or 1");
+        if (c->pred_pair != value)
+            for (auto &g : c->graphs) {   // captured loops hold the other kernel
+                if (g.exec) cudaGraphExecDestroy(g.exec);
+                g.exec = nullptr;
+            }
+        c->pred_pair = value;
+        return SF_OK;
     default:
         return fail(SF_EINVAL, "unknown tuning knob");
     }
@@ -1132,23 +1141,23 @@ int sf_roms_stress3d(sf_ctx *c, const void *u, const void *v, void *ru, void *rv
 }
 
 int sf_roms_rhs3d(sf_ctx *c, const void *u, const void *v, const void *Huon, const void *Hvom,
-                  const void *W, const void *Hz, void *ru, void *rv, sf_stream s) {
-    if (!u || !v || !Huon || !Hvom || !W || !Hz || !ru || !rv) return fail(SF_EINVAL, "null argument");
+                  const void *Hz, void *ru, void *rv, sf_stream s) {
+    if (!u || !v || !Huon || !Hvom || !Hz || !ru || !rv) return fail(SF_EINVAL, "null argument");
     return dispatch(c, "sf_roms_rhs3d", [&](auto *t) {
         using R = std::remove_pointer_t<decltype(t)>;
         return sf::Ops<R>::roms_rhs3d(c, (const R *)u, (const R *)v, (const R *)Huon,
-                                      (const R *)Hvom, (const R *)W, (const R *)Hz, (R *)ru,
-                                      (R *)rv, S(s));
+                                      (const R *)Hvom, (const R *)Hz, (R *)ru, (R *)rv, S(s));
     });
 }
 
 int sf_roms_step3d_uv(sf_ctx *c, void *u, void *v, const void *ru0, const void *ru1,
                       const void *ru2, const void *rv0, const void *rv1, const void *rv2,
                       void *ubar_n, void *vbar_n, void *ubar_s, void *vbar_s, const void *Hz,
-                      const void *Akv, const void *z_r, const double *DU, const double *DV,
-                      int iic, int ntfirst, double lambda, double Dt, sf_stream s) {
+                      const void *Akv, const void *z_r, const void *W, const double *DU,
+                      const double *DV, int iic, int ntfirst, double lambda, double Dt,
+                      sf_stream s) {
     if (!u || !v || !ru0 || !ru1 || !ru2 || !rv0 || !rv1 || !rv2 || !ubar_n || !vbar_n ||
-        !ubar_s || !vbar_s || !Hz || !Akv || !z_r || !DU || !DV)
+        !ubar_s || !vbar_s || !Hz || !Akv || !z_r || !W || !DU || !DV)
         return fail(SF_EINVAL, "null argument");
     if (iic < ntfirst) return fail(SF_EINVAL, "sf_roms_step3d_uv: iic < ntfirst");
     if (c && c->N > sf::kRomsMaxN) return fail(SF_EINVAL, "sf_roms_step3d_uv: N > 64");
@@ -1162,7 +1171,8 @@ int sf_roms_step3d_uv(sf_ctx *c, void *u, void *v, const void *ru0, const void *
         const R *rv[3] = {(const R *)rv0, (const R *)rv1, (const R *)rv2};
         return sf::Ops<R>::roms_step3d(c, (R *)u, (R *)v, ru, rv, coef, (R *)ubar_n, (R *)vbar_n,
                                        (R *)ubar_s, (R *)vbar_s, (const R *)Hz, (const R *)Akv,
-                                       (const R *)z_r, DU, DV, Dt, lambda * Dt, S(s));
+                                       (const R *)z_r, (const R *)W, DU, DV, Dt, lambda * Dt,
+                                       S(s));
     });
 }
 

@@ -137,7 +137,9 @@ struct sf_ctx {
     // per-element cp.async staging
     int use_bulk = 0;
     // levels whose loads the fused flux/omega kernel issues together (sf_ctx_tune)
-    int mo_chunk = 0;
+    int mo_chunk = 4;
+    // fused predictor in its paired form (two nodes per thread) where the grid allows it
+    int pred_pair = 1;
     cudaStream_t cap = nullptr;
     double *d_bcval = nullptr;
     sf_loop_graph graphs[3];
@@ -287,13 +289,12 @@ struct Ops {
     static cudaError_t roms_stress3d(const sf_ctx *c, const R *u, const R *v, R *ru, R *rv,
                                      const R *sustr, const R *svstr, double rdrag2, cudaStream_t s);
     static cudaError_t roms_rhs3d(const sf_ctx *c, const R *u, const R *v, const R *Huon,
-                                  const R *Hvom, const R *W, const R *Hz, R *ru, R *rv,
-                                  cudaStream_t s);
+                                  const R *Hvom, const R *Hz, R *ru, R *rv, cudaStream_t s);
     static cudaError_t roms_step3d(const sf_ctx *c, R *u, R *v, const R *const *ru,
                                    const R *const *rv, const double *coef, R *ubar_n, R *vbar_n,
                                    R *ubar_s, R *vbar_s, const R *Hz, const R *Akv, const R *z_r,
-                                   const double *DU, const double *DV, double dt, double lamdt,
-                                   cudaStream_t s);
+                                   const R *W, const double *DU, const double *DV, double dt,
+                                   double lamdt, cudaStream_t s);
     static cudaError_t roms_walls3d(const sf_ctx *c, R *u, R *v, cudaStream_t s);
 };
 

@@ -295,27 +295,59 @@ __host__ __device__ __forceinline__ bool prd_inner_tile(int i0, int j0, int I, i
     return i0 >= 3 && j0 >= 3 && i0 + kPredTX + 2 <= I && j0 + kPredTY + 2 <= J;
 }
 
+// Chained destinations: the last edge block, after every edge block's reads.  A thread
+// reaches the barrier only after each of its loads has returned (every loaded value feeds a
+// store or a branch before it), so once a block has counted itself, none of its reads of old
+// contents is pending and the last edge block may overwrite them.
+template <typename R>
+__device__ __forceinline__ void prd_chained_tail(const PredArgs<R> &a, int tid, int edge_blocks) {
+    __shared__ int s_last;
+    __syncthreads();
+    if (tid == 0) s_last = atomicAdd(a.counter, 1) == edge_blocks - 1;
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    const BcProgram *ps[3] = {&a.pz, &a.pu, &a.pv};
+    R v[3] = {R(0), R(0), R(0)};
+    int d[3] = {-1, -1, -1};
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+        const BcProgram &p = *ps[f];
+        if (tid < p.nch) {
+            d[f] = p.dst_ch[tid];
+            v[f] = __ldcg(a.chv + f * kMaxChained + tid);
+        }
+    }
+    if (d[0] >= 0) a.z2[d[0]] = v[0];
+    if (d[1] >= 0) a.ub2[d[1]] = v[1];
+    if (d[2] >= 0) a.vb2[d[2]] = v[2];
+    if (tid == 0) *a.counter = 0;
+}
+
+// Block 0 evaluates the chained entries' values first (the last edge block stores them).
+template <typename R>
+__device__ __forceinline__ void prd_chained_head(const PredArgs<R> &a, int tid, R (*sZ)[kPredTX + 1]) {
+    const BcProgram *ps[3] = {&a.pz, &a.pu, &a.pv};
+#pragma unroll
+    for (int f = 0; f < 3; ++f)
+        if (tid < ps[f]->nch)
+            a.chv[f * kMaxChained + tid] =
+                prd_bc_value(a, PrdTile<R>{sZ, -kPredTX - 2, -kPredTY - 2}, f, ps[f]->src_ch[tid]);
+    __threadfence();   // ... visible before this block counts itself
+}
+
 template <typename R>
 __global__ void __launch_bounds__(256, 5) k_pred2d(const __grid_constant__ PredArgs<R> a,
                                                 int ring_blocks, int tiles_x, int edge_blocks) {
     pdl_enter();
     __shared__ R sZ[kPredTY + 1][kPredTX + 1];   // zeta_t2 after zetabc, (j0-1.., i0-1..)
-    __shared__ int s_last;
     const Geo<R> &g = a.g;
     const int I = g.I, J = g.J;
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int tid = ty * 32 + tx;
     const int bid = (int)blockIdx.x;
     int i0 = -kPredTX - 2, j0 = -kPredTY - 2;   // ring blocks: a tile no node falls in
-    if (bid == 0) {   // the chained entries' values (the last block stores them)
-        const BcProgram *ps[3] = {&a.pz, &a.pu, &a.pv};
-#pragma unroll
-        for (int f = 0; f < 3; ++f)
-            if (tid < ps[f]->nch)
-                a.chv[f * kMaxChained + tid] =
-                    prd_bc_value(a, PrdTile<R>{sZ, i0, j0}, f, ps[f]->src_ch[tid]);
-        __threadfence();   // ... visible before this block counts itself
-    }
+    if (bid == 0) prd_chained_head(a, tid, sZ);
     if (bid < ring_blocks) {
         const int e = bid * 256 + tid;
         if (e < 4 * I + 4 * (J - 4)) prd_edge_node(a, PrdTile<R>{sZ, i0, j0}, prd_ring_node(e, I, J));
@@ -361,30 +393,201 @@ __global__ void __launch_bounds__(256, 5) k_pred2d(const __grid_constant__ PredA
         if (prd_inner_tile(i0, j0, I, J)) return;   // uniform over the block: no barrier below
     }
 
-    // ---- chained destinations: the last edge block, after every edge block's reads --------
-    // A thread reaches the barrier only after each of its loads has returned (every loaded
-    // value feeds a store or a branch before it), so once a block has counted itself, none of
-    // its reads of old contents is pending and the last edge block may overwrite them.
-    __syncthreads();
-    if (tid == 0) s_last = atomicAdd(a.counter, 1) == edge_blocks - 1;
-    __syncthreads();
-    if (!s_last) return;
-    __threadfence();
-    const BcProgram *ps[3] = {&a.pz, &a.pu, &a.pv};
-    R v[3] = {R(0), R(0), R(0)};
-    int d[3] = {-1, -1, -1};
-#pragma unroll
-    for (int f = 0; f < 3; ++f) {
-        const BcProgram &p = *ps[f];
-        if (tid < p.nch) {
-            d[f] = p.dst_ch[tid];
-            v[f] = __ldcg(a.chv + f * kMaxChained + tid);
-        }
+    prd_chained_tail(a, tid, edge_blocks);
+}
+
+// ---- the paired form (grids with an even row length) -------------------------------------
+// Lane tx of a 32 x 16 block takes the node pair (x, x+1), x = j I + i with i even, of staged
+// row ty: with I even every such pair starts on an 8-byte (FP32) or 16-byte (FP64) boundary, so
+// each array's two values arrive in one vector load, and the pair shares the neighbours that
+// the scalar form loads twice (x's east node is x+1's own, x+1's west node is x's own).  Each
+// node's arithmetic is prd_rz_keep's and prd_deep_mom_kept's, operation for operation (the
+// shared terms are the same expressions on the same operands), so the FP64 build reproduces
+// the scalar form bit for bit.  A tile is 62 x 15 nodes, staged with two west halo columns
+// (the first keeps the pairs aligned; only the second is read) and one south halo row: 64 x 16
+// nodes, one staged row per warp.  With I even a pair is deep in both nodes or in neither.
+constexpr int kPairTX = 62, kPairTY = 15;
+
+template <typename R>
+struct Vec2;
+template <>
+struct Vec2<float> {
+    using T = float2;
+};
+template <>
+struct Vec2<double> {
+    using T = double2;
+};
+template <typename R>
+__device__ __forceinline__ void ld2(const R *__restrict__ q, R &a, R &b) {
+    const typename Vec2<R>::T t = *reinterpret_cast<const typename Vec2<R>::T *>(q);
+    a = t.x;
+    b = t.y;
+}
+template <typename R>
+__device__ __forceinline__ void st2(R *__restrict__ q, R a, R b) {
+    typename Vec2<R>::T t;
+    t.x = a;
+    t.y = b;
+    *reinterpret_cast<typename Vec2<R>::T *>(q) = t;
+}
+
+// A deep pair's inputs that both phases use (node a = x, node b = x+1).
+template <typename R>
+struct PrdPair {
+    R z1w, z1a, z1b, z1sa, z1sb, hw, ha, hb, hsa, hsb;
+    R uba, ubb, vba, vbb, pma, pmb, pna, pnb, oua, oub, ova, ovb, z0a, z0b;
+};
+
+// computeZetaRHS at both nodes of a deep pair; fills the pair's kept inputs.
+template <typename R>
+__device__ __forceinline__ void prd_rz_pair(const PredArgs<R> &a, long x, PrdPair<R> &n, R &rza,
+                                            R &rzb) {
+    const Geo<R> &g = a.g;
+    const int I = g.I;
+    const R *z = a.z1 + x, *h = g.h + x, *ub = a.ub1 + x, *vb = a.vb1 + x, *ou = g.on_u + x,
+            *ov = g.om_v + x;
+    ld2(z, n.z1a, n.z1b);
+    n.z1w = z[-1];
+    const R z1e = z[2];
+    ld2(z - I, n.z1sa, n.z1sb);
+    R zna, znb;
+    ld2(z + I, zna, znb);
+    ld2(h, n.ha, n.hb);
+    n.hw = h[-1];
+    const R he = h[2];
+    ld2(h - I, n.hsa, n.hsb);
+    R hna, hnb;
+    ld2(h + I, hna, hnb);
+    ld2(ub, n.uba, n.ubb);
+    const R ube = ub[2];
+    ld2(vb, n.vba, n.vbb);
+    R vna, vnb;
+    ld2(vb + I, vna, vnb);
+    ld2(ou, n.oua, n.oub);
+    const R oue = ou[2];
+    ld2(ov, n.ova, n.ovb);
+    R ovna, ovnb;
+    ld2(ov + I, ovna, ovnb);
+    ld2(g.pm + x, n.pma, n.pmb);
+    ld2(g.pn + x, n.pna, n.pnb);
+    ld2(a.z0 + x, n.z0a, n.z0b);
+    // node a
+    const R Dpa = n.z1a + n.ha, Dwa = n.z1w + n.hw, Dpb = n.z1b + n.hb;
+    const R Dsa = n.z1sa + n.hsa, Dna = zna + hna;
+    const R DUpa = n.uba * ((Dpa + Dwa) * R(0.5));
+    const R DUpb = n.ubb * ((Dpb + Dpa) * R(0.5));   // node a's east flux, node b's west
+    const R DVpa = n.vba * ((Dpa + Dsa) * R(0.5));
+    const R DVna = vna * ((Dna + Dpa) * R(0.5));
+    rza = (((DUpb * n.oub - DUpa * n.oua) + (DVna * ovna - DVpa * n.ova)) * n.pma) * n.pna;
+    // node b
+    const R Deb = z1e + he, Dsb = n.z1sb + n.hsb, Dnb = znb + hnb;
+    const R DUeb = ube * ((Deb + Dpb) * R(0.5));
+    const R DVpb = n.vbb * ((Dpb + Dsb) * R(0.5));
+    const R DVnb = vnb * ((Dnb + Dpb) * R(0.5));
+    rzb = (((DUeb * oue - DUpb * n.oub) + (DVnb * ovnb - DVpb * n.ovb)) * n.pmb) * n.pnb;
+}
+
+// The momentum of a deep pair from the tile's zeta_t2: za, zb at the nodes, zw west of a, zsa
+// and zsb south of them.
+template <typename R>
+__device__ __forceinline__ void prd_mom_pair(const PredArgs<R> &a, long x, bool pda, bool pdb,
+                                             R za, R zb, R zw, R zsa, R zsb, const PrdPair<R> &n) {
+    const int I = a.g.I;
+    const R *z0 = a.z0 + x;
+    R z0sa, z0sb;
+    ld2(z0 - I, z0sa, z0sb);
+    const R gpa = a.w1 * za + a.w * n.z0a;
+    const R gw = a.w1 * zw + a.w * z0[-1];
+    const R gsa = a.w1 * zsa + a.w * z0sa;
+    const R gpb = a.w1 * zb + a.w * n.z0b;
+    const R gsb = a.w1 * zsb + a.w * z0sb;
+    const R rua = (a.grav * n.oua) * (((n.ha + n.hw) * R(0.5)) * (gpa - gw) + R(0.5) * (gpa * gpa - gw * gw));
+    const R rva = (a.grav * n.ova) * (((n.ha + n.hsa) * R(0.5)) * (gpa - gsa) + R(0.5) * (gpa * gpa - gsa * gsa));
+    const R rub = (a.grav * n.oub) * (((n.hb + n.ha) * R(0.5)) * (gpb - gpa) + R(0.5) * (gpb * gpb - gpa * gpa));
+    const R rvb = (a.grav * n.ovb) * (((n.hb + n.hsb) * R(0.5)) * (gpb - gsb) + R(0.5) * (gpb * gpb - gsb * gsb));
+    st2(a.ru + x, rua, rub);
+    st2(a.rv + x, rva, rvb);
+    if (!pda && !pdb) return;
+    const R D1pa = n.z1a + n.ha, D2pa = za + n.ha, D1pb = n.z1b + n.hb, D2pb = zb + n.hb;
+    const R ua = ddiv(n.uba * ((D1pa + (n.z1w + n.hw)) * R(0.5)) + ((a.Dt * rua) * n.pma) * n.pna,
+                      (D2pa + (zw + n.hw)) * R(0.5));
+    const R va = ddiv(n.vba * ((D1pa + (n.z1sa + n.hsa)) * R(0.5)) + ((a.Dt * rva) * n.pma) * n.pna,
+                      (D2pa + (zsa + n.hsa)) * R(0.5));
+    const R ub = ddiv(n.ubb * ((D1pb + D1pa) * R(0.5)) + ((a.Dt * rub) * n.pmb) * n.pnb,
+                      (D2pb + D2pa) * R(0.5));
+    const R vb = ddiv(n.vbb * ((D1pb + (n.z1sb + n.hsb)) * R(0.5)) + ((a.Dt * rvb) * n.pmb) * n.pnb,
+                      (D2pb + (zsb + n.hsb)) * R(0.5));
+    if (pda && pdb) {
+        st2(a.ub2 + x, ua, ub);
+        st2(a.vb2 + x, va, vb);
+    } else if (pda) {
+        a.ub2[x] = ua;
+        a.vb2[x] = va;
+    } else {
+        a.ub2[x + 1] = ub;
+        a.vb2[x + 1] = vb;
     }
-    if (d[0] >= 0) a.z2[d[0]] = v[0];
-    if (d[1] >= 0) a.ub2[d[1]] = v[1];
-    if (d[2] >= 0) a.vb2[d[2]] = v[2];
-    if (tid == 0) *a.counter = 0;
+}
+
+__host__ __device__ __forceinline__ bool prd_inner_pair_tile(int i0, int j0, int I, int J) {
+    // every staged node (columns i0-2 .. i0+61, rows j0-1 .. j0+14) deep
+    return i0 >= 4 && j0 >= 3 && i0 + kPairTX + 2 <= I && j0 + kPairTY + 2 <= J;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(512, 2) k_pred2d_pair(const __grid_constant__ PredArgs<R> a,
+                                                       int ring_blocks, int tiles_x, int edge_blocks) {
+    pdl_enter();
+    __shared__ R sZ[kPairTY + 1][kPairTX + 2];   // zeta_t2 after zetabc, (j0-1.., i0-2..)
+    __shared__ R sDummy[kPredTY + 1][kPredTX + 1];
+    const Geo<R> &g = a.g;
+    const int I = g.I, J = g.J;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int tid = ty * 32 + tx;
+    const int bid = (int)blockIdx.x;
+    if (bid == 0) prd_chained_head(a, tid, sDummy);
+    if (bid < ring_blocks) {
+        const int e = bid * 512 + tid;
+        if (e < 4 * I + 4 * (J - 4))
+            prd_edge_node(a, PrdTile<R>{sDummy, -kPredTX - 2, -kPredTY - 2}, prd_ring_node(e, I, J));
+    } else {
+        const int tb = bid - ring_blocks;
+        const int i0 = (tb % tiles_x) * kPairTX, j0 = (tb / tiles_x) * kPairTY;
+        const int i = i0 - 2 + 2 * tx;   // the pair (i, i+1) of staged columns 2 tx, 2 tx + 1
+        const int r = ty;                // staged row (0: the south halo)
+        const int j = j0 - 1 + r;
+        const bool live = i >= 0 && j >= 0 && i < I && j < J;   // I even: i + 1 < I too
+        const bool deep = live && prd_deep(i, j, I, J);       // ... and i + 1 deep alike
+        const long x = (long)j * I + i;
+        PrdPair<R> kept;
+        // ---- phase 1: zeta_t2 (after zetabc) on the tile and its halo -----------------------
+        if (deep) {
+            R rza, rzb;
+            prd_rz_pair(a, x, kept, rza, rzb);
+            const R za = kept.z0a + a.Dt * rza, zb = kept.z0b + a.Dt * rzb;
+            if (tx >= 1 && r >= 1) {   // the tile's own pair
+                st2(a.rz + x, rza, rzb);
+                st2(a.z2 + x, za, zb);
+            }
+            sZ[r][2 * tx] = za;
+            sZ[r][2 * tx + 1] = zb;
+        } else if (live) {
+            sZ[r][2 * tx] = prd_z2b(a, x);
+            sZ[r][2 * tx + 1] = prd_z2b(a, x + 1);
+        }
+        __syncthreads();
+        // ---- phase 2: momentum of the tile's deep pairs ---------------------------------------
+        if (deep && tx >= 1 && r >= 1) {
+            const int qa = j * I + i, qb = qa + 1;
+            const bool pda = qa - fdiv(qa, g.dJ) * J != 0 && qa >= J;   // q % J != 0 (szJ)
+            const bool pdb = qb - fdiv(qb, g.dJ) * J != 0 && qb >= J;
+            prd_mom_pair(a, x, pda, pdb, sZ[r][2 * tx], sZ[r][2 * tx + 1], sZ[r][2 * tx - 1],
+                         sZ[r - 1][2 * tx], sZ[r - 1][2 * tx + 1], kept);
+        }
+        if (prd_inner_pair_tile(i0, j0, I, J)) return;   // uniform over the block
+    }
+    prd_chained_tail(a, tid, edge_blocks);
 }
 
 template <typename R>
@@ -417,6 +620,25 @@ cudaError_t Ops<R>::pred2d(const sf_ctx *c, R *z0, R *z1, R *z2, R *ub1, R *vb1,
     a.pv = c->vbc;
     a.counter = c->pred_counter;
     a.chv = reinterpret_cast<R *>(reinterpret_cast<char *>(c->pred_counter) + 256);
+    // the paired form where every row starts on a vector boundary in every array
+    bool pair = c->pred_pair && (c->I % 2) == 0;
+    {
+        const void *ptrs[] = {z0, z1, z2, ub1, vb1, ub2, vb2, rz, ru, rv, a.g.h, a.g.pm, a.g.pn,
+                              a.g.on_u, a.g.om_v};
+        for (const void *q : ptrs) pair = pair && (reinterpret_cast<uintptr_t>(q) % (2 * sizeof(R))) == 0;
+    }
+    if (pair) {
+        const int tiles_x = (c->I + kPairTX - 1) / kPairTX, tiles_y = (c->J + kPairTY - 1) / kPairTY;
+        const int ring_blocks = (4 * c->I + 4 * (c->J - 4) + 511) / 512;
+        int inner_x = 0, inner_y = 0;
+        for (int tx = 0; tx < tiles_x; ++tx)
+            inner_x += prd_inner_pair_tile(tx * kPairTX, 3, c->I, 3 + kPairTY + 2);
+        for (int ty = 0; ty < tiles_y; ++ty)
+            inner_y += prd_inner_pair_tile(4, ty * kPairTY, 4 + kPairTX + 2, c->J);
+        const int edge_blocks = ring_blocks + tiles_x * tiles_y - inner_x * inner_y;
+        return launch_dep(c, k_pred2d_pair<R>, dim3((unsigned)(ring_blocks + tiles_x * tiles_y)),
+                          dim3(32, 16), 0, s, a, ring_blocks, tiles_x, edge_blocks);
+    }
     const int tiles_x = (c->I + kPredTX - 1) / kPredTX, tiles_y = (c->J + kPredTY - 1) / kPredTY;
     const int ring_blocks = (4 * c->I + 4 * (c->J - 4) + 255) / 256;
     // the blocks counted before the chained writes: the ring blocks and the tiles that are not

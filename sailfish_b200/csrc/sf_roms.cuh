@@ -174,23 +174,15 @@ __global__ void __launch_bounds__(256) k_roms_mom(Geo<R> g, RomsArgs<R> a) {
 // reference's addCoriolis), then second-order centred advection of momentum: horizontal
 // fluxes UFx = (Huon_i + Huon_i+1)/4 (u_i + u_i+1) at rho points and UFe = (Hvom_i +
 // Hvom_i-1)/4 (u_j + u_j-1) at psi points (the UV_C2ADVECTION form of the reference's ROMS
-// transcription, obsolete/step2d_LF_AM3.h.py:1244-1300, per level), V alike, and vertical
-// fluxes FC_w = (u_w-1 + u_w)/4 (W_w + W_w,i-1) on the interior w levels.  One thread per rho
-// point p (its west U face and south V face), levels in order; the expressions keep the
-// oracle's operand order (oracle/roms_oracle.py, rhs3d).
-template <typename R>
-__device__ __forceinline__ R roms_fc(const R *__restrict__ q, const R *__restrict__ W, long o,
-                                     long s2, long p, long d) {
-    // flux through w level w (o = w s2) at the face p with the other rho point p - d
-    return (R(0.25) * (q[o - s2 + p] + q[o + p])) * (W[o + p] + W[o + p - d]);
-}
-
+// transcription, obsolete/step2d_LF_AM3.h.py:1244-1300, per level), V alike; the vertical
+// advection is implicit, in the column solve (roms_column).  One thread per rho point p (its
+// west U face and south V face), levels in order; the expressions keep the oracle's operand
+// order (oracle/roms_oracle.py, rhs3d).
 template <typename R>
 __global__ void __launch_bounds__(256) k_roms_rhs3d(Geo<R> g, const R *__restrict__ u,
                                                     const R *__restrict__ v,
                                                     const R *__restrict__ Hu,
                                                     const R *__restrict__ Hv,
-                                                    const R *__restrict__ W,
                                                     const R *__restrict__ Hz,
                                                     R *__restrict__ ru, R *__restrict__ rv) {
     const long p = tid_flat();
@@ -214,8 +206,6 @@ __global__ void __launch_bounds__(256) k_roms_rhs3d(Geo<R> g, const R *__restric
             const R En = (R(0.25) * (hv[p + I] + hv[p + I - 1])) * (uk[p + I] + uk[p]);
             const R Es = (R(0.25) * (hv[p] + hv[p - 1])) * (uk[p] + uk[p - I]);
             tu = cor - ((Xp - Xw) + (En - Es));
-            if (k > 0) tu = tu + roms_fc(u, W, o, s2, p, 1);
-            if (k < N - 1) tu = tu - roms_fc(u, W, o + s2, s2, p, 1);
         }
         if (k < N && vf) {
             const R *uk = u + o, *vk = v + o, *hu = Hu + o, *hv = Hv + o, *hz = Hz + o;
@@ -227,8 +217,6 @@ __global__ void __launch_bounds__(256) k_roms_rhs3d(Geo<R> g, const R *__restric
             const R Ep = (R(0.25) * (hv[p] + hv[p + I])) * (vk[p] + vk[p + I]);
             const R Es = (R(0.25) * (hv[p - I] + hv[p])) * (vk[p - I] + vk[p]);
             tv = cor - ((Xe - Xw) + (Ep - Es));
-            if (k > 0) tv = tv + roms_fc(v, W, o, s2, p, I);
-            if (k < N - 1) tv = tv - roms_fc(v, W, o + s2, s2, p, I);
         }
         ru[o + p] = tu;
         rv[o + p] = tv;
@@ -266,14 +254,18 @@ __global__ void __launch_bounds__(256) k_roms_stress3d(Geo<R> g, const R *__rest
     }
 }
 
-// The ROMS-form step3d_uv for one face column (d = 1: U face, d = I: V face): the implicit
-// vertical-viscosity system
-//   (Hzu_k - FC_k - FC_k-1) x_k + FC_k x_k+1 + FC_k-1 x_k-1 = Hzu_k u_k + dt pmU pnU r_k,
-// r_k = (c0 ru_k(n) + c1 ru_k(n-1)) + c2 ru_k(n-2) (Adams-Bashforth), FC_k = -lamdt AKU_k+1 /
-// DZ_k on the interface between levels k and k+1 (w level k+1; no flux through the surface or
-// the bottom, whose stresses are in ru), Thomas elimination in R, then the depth mean set to
-// the barotropic transport with FP64 sums: x_k -= (sum Hzu x - avg/on) / sum Hzu.  Returns the
-// new depth-mean velocity avg / on / sum Hzu.
+// The ROMS-form step3d_uv for one face column (d = 1: U face, d = I: V face): with F_w the
+// upwind vertical advective flux through w level w (w_w x_w-1 where w_w > 0, w_w x_w where
+// w_w < 0; w_w = fac (W_w + W_w,nbr) / 2, 0 at the bottom and the surface), fac = dt pmU pnU,
+//   Hzu_k x_k - [viscosity] + (F_k+1 - F_k) = Hzu_k u_k + fac r_k,
+// r_k = (c0 ru_k(n) + c1 ru_k(n-1)) + c2 ru_k(n-2) (Adams-Bashforth), the viscosity through
+// FC_k = -lamdt AKU_k+1 / DZ_k on the interface between levels k and k+1 (w level k+1; no flux
+// through the surface or the bottom, whose stresses are in ru): the lower, main and upper
+// diagonals l_k = FC_k-1 - w+_k, b_k = (Hzu_k - FC_k - FC_k-1) + (w+_k+1 - w-_k),
+// u_k = FC_k + w-_k+1 (an M-matrix at any vertical Courant number: backward-Euler upwind
+// vertical advection).  Thomas elimination in R, then the depth mean set to the barotropic
+// transport with FP64 sums: x_k -= (sum Hzu x - avg/on) / sum Hzu.  Returns the new depth-mean
+// velocity avg/on/sum Hzu.
 template <typename R>
 struct RomsRhs {
     const R *r0, *r1, *r2;   // right-hand sides at n, n-1, n-2
@@ -284,13 +276,16 @@ __device__ __forceinline__ double roms_column(const Geo<R> &g, long p, long d, R
                                               RomsRhs<R> rs, R c0, R c1, R c2,
                                               const R *__restrict__ Hz,
                                               const R *__restrict__ Akv, const R *__restrict__ z_r,
-                                              double avg, R on, R dt, R lamdt) {
+                                              const R *__restrict__ W, double avg, R on, R dt,
+                                              R lamdt) {
     const long s2 = g.s2;
     const int N = g.N;
-    R fc[kRomsMaxN], bc[kRomsMaxN], rhs[kRomsMaxN], hzu[kRomsMaxN];
+    R fc[kRomsMaxN], wf[kRomsMaxN + 1], bc[kRomsMaxN], up[kRomsMaxN], rhs[kRomsMaxN],
+        hzu[kRomsMaxN];
     const R pmU = R(0.5) * (g.pm[p] + g.pm[p - d]);
     const R pnU = R(0.5) * (g.pn[p] + g.pn[p - d]);
     const R fac = dt * (pmU * pnU);
+    wf[0] = R(0);
     for (int k = 0; k < N; ++k) {
         const long o = (long)k * s2 + p;
         hzu[k] = R(0.5) * (Hz[o] + Hz[o - d]);
@@ -298,24 +293,29 @@ __device__ __forceinline__ double roms_column(const Geo<R> &g, long p, long d, R
             const R ak = R(0.5) * (Akv[o + s2] + Akv[o + s2 - d]);
             const R dz = R(0.5) * ((z_r[o + s2] - z_r[o]) + (z_r[o + s2 - d] - z_r[o - d]));
             fc[k] = (-lamdt * ak) / dz;
+            wf[k + 1] = fac * (R(0.5) * (W[o + s2] + W[o + s2 - d]));
         } else {
             fc[k] = R(0);
+            wf[k + 1] = R(0);
         }
     }
+    auto wplus = [](R w) { return w > R(0) ? w : R(0); };
+    auto wminus = [](R w) { return w < R(0) ? w : R(0); };
     for (int k = 0; k < N; ++k) {
         const long o = (long)k * s2 + p;
         const R fcm = k > 0 ? fc[k - 1] : R(0);
-        bc[k] = (hzu[k] - fc[k]) - fcm;
+        bc[k] = ((hzu[k] - fc[k]) - fcm) + (wplus(wf[k + 1]) - wminus(wf[k]));
+        up[k] = fc[k] + wminus(wf[k + 1]);
         const R r = (c0 * rs.r0[o] + c1 * rs.r1[o]) + c2 * rs.r2[o];
         rhs[k] = hzu[k] * u[o] + fac * r;
-    }
-    for (int k = 1; k < N; ++k) {
-        const R w = fc[k - 1] / bc[k - 1];
-        bc[k] = bc[k] - w * fc[k - 1];
-        rhs[k] = rhs[k] - w * rhs[k - 1];
+        if (k > 0) {
+            const R w = (fcm - wplus(wf[k])) / bc[k - 1];
+            bc[k] = bc[k] - w * up[k - 1];
+            rhs[k] = rhs[k] - w * rhs[k - 1];
+        }
     }
     rhs[N - 1] = rhs[N - 1] / bc[N - 1];               // x overwrites rhs
-    for (int k = N - 2; k >= 0; --k) rhs[k] = (rhs[k] - fc[k] * rhs[k + 1]) / bc[k];
+    for (int k = N - 2; k >= 0; --k) rhs[k] = (rhs[k] - up[k] * rhs[k + 1]) / bc[k];
     double H = 0.0, Hu = 0.0;
     for (int k = 0; k < N; ++k) {
         H = H + (double)hzu[k];
@@ -338,6 +338,7 @@ __global__ void __launch_bounds__(128) k_roms_step3d(Geo<R> g, R *__restrict__ u
                                                      R *__restrict__ ubar_s, R *__restrict__ vbar_s,
                                                      const R *__restrict__ Hz, const R *__restrict__ Akv,
                                                      const R *__restrict__ z_r,
+                                                     const R *__restrict__ W,
                                                      const double *__restrict__ DU,
                                                      const double *__restrict__ DV, R dt, R lamdt) {
     const long p = tid_flat();
@@ -345,9 +346,9 @@ __global__ void __launch_bounds__(128) k_roms_step3d(Geo<R> g, R *__restrict__ u
     const int j = fdiv((int)p, g.dI), i = (int)p - j * g.I;
     R ub = R(0), vb = R(0);
     if (i >= 2 && i <= g.I - 2 && j >= 1 && j <= g.J - 2)
-        ub = (R)roms_column(g, p, 1, u, ru, c0, c1, c2, Hz, Akv, z_r, DU[p], g.on_u[p], dt, lamdt);
+        ub = (R)roms_column(g, p, 1, u, ru, c0, c1, c2, Hz, Akv, z_r, W, DU[p], g.on_u[p], dt, lamdt);
     if (j >= 2 && j <= g.J - 2 && i >= 1 && i <= g.I - 2)
-        vb = (R)roms_column(g, p, g.I, v, rv, c0, c1, c2, Hz, Akv, z_r, DV[p], g.om_v[p], dt, lamdt);
+        vb = (R)roms_column(g, p, g.I, v, rv, c0, c1, c2, Hz, Akv, z_r, W, DV[p], g.om_v[p], dt, lamdt);
     ubar_n[p] = ub;
     ubar_s[p] = ub;
     vbar_n[p] = vb;
@@ -387,21 +388,21 @@ cudaError_t Ops<R>::roms_stress3d(const sf_ctx *c, const R *u, const R *v, R *ru
 }
 template <typename R>
 cudaError_t Ops<R>::roms_rhs3d(const sf_ctx *c, const R *u, const R *v, const R *Huon,
-                               const R *Hvom, const R *W, const R *Hz, R *ru, R *rv,
-                               cudaStream_t s) {
-    k_roms_rhs3d<R><<<blocks_for(c->s2, 256), 256, 0, s>>>(geo(c), u, v, Huon, Hvom, W, Hz, ru, rv);
+                               const R *Hvom, const R *Hz, R *ru, R *rv, cudaStream_t s) {
+    k_roms_rhs3d<R><<<blocks_for(c->s2, 256), 256, 0, s>>>(geo(c), u, v, Huon, Hvom, Hz, ru, rv);
     return cudaGetLastError();
 }
 template <typename R>
 cudaError_t Ops<R>::roms_step3d(const sf_ctx *c, R *u, R *v, const R *const *ru, const R *const *rv,
                                 const double *coef, R *ubar_n, R *vbar_n, R *ubar_s, R *vbar_s,
-                                const R *Hz, const R *Akv, const R *z_r, const double *DU,
-                                const double *DV, double dt, double lamdt, cudaStream_t s) {
+                                const R *Hz, const R *Akv, const R *z_r, const R *W,
+                                const double *DU, const double *DV, double dt, double lamdt,
+                                cudaStream_t s) {
     const RomsRhs<R> a{ru[0], ru[1], ru[2]}, b{rv[0], rv[1], rv[2]};
     k_roms_step3d<R><<<blocks_for(c->s2, 128), 128, 0, s>>>(geo(c), u, v, a, b, (R)coef[0],
                                                               (R)coef[1], (R)coef[2], ubar_n,
                                                               vbar_n, ubar_s, vbar_s, Hz, Akv,
-                                                              z_r, DU, DV, (R)dt, (R)lamdt);
+                                                              z_r, W, DU, DV, (R)dt, (R)lamdt);
     return cudaGetLastError();
 }
 template <typename R>

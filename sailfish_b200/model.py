@@ -370,7 +370,7 @@ class Model:
                     r3.insert(0, r3.pop())
                 self.ru, self.rv = self._ru3[0], self._rv3[0]
                 phase("k_rhs3d", lambda: (check(lib.sf_roms_rhs3d(
-                    c, p(self.u), p(self.v), p(self.Huon), p(self.Hvom), p(self.W), p(self.Hz),
+                    c, p(self.u), p(self.v), p(self.Huon), p(self.Hvom), p(self.Hz),
                     p(self.ru), p(self.rv), st), "sf_roms_rhs3d"), check(lib.sf_roms_stress3d(
                         c, p(self.u), p(self.v), p(self.ru), p(self.rv), p(self.sustr),
                         p(self.svstr), self.rdrag2, st), "sf_roms_stress3d")))
@@ -395,7 +395,7 @@ class Model:
                     c, p(self.u), p(self.v), *[p(t) for t in self._ru3],
                     *[p(t) for t in self._rv3], p(self._slot("ubar", 1)),
                     p(self._slot("vbar", 1)), p(self._slot("ubar", 2)),
-                    p(self._slot("vbar", 2)), p(self.Hz), p(self.AKv), p(self.z_r),
+                    p(self._slot("vbar", 2)), p(self.Hz), p(self.AKv), p(self.z_r), p(self.W),
                     p(self.DU_avg1), p(self.DV_avg1), self.iic, self.ntfirst, self.lam, self.dt,
                     st), "sf_roms_step3d_uv"), check(lib.sf_lateral_uv_bc(
                         c, self.time, p(self.u), p(self.v), st), "sf_lateral_uv_bc"),

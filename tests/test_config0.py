@@ -120,3 +120,62 @@ def test_dropin_main2d_is_bit_exact_on_config0():
     for n in NAMES2:
         got = np.stack([getattr(OC, "%s_t%d" % (n, k)).cpu().numpy() for k in range(3)])
         np.testing.assert_array_equal(got, ref[n], err_msg=n)
+
+
+# ---- config 0 with its forcing, in the ROMS form -------------------------------------------------
+# Config 0 asks for wind stress tau_x = 0.1 cos(pi y/Ly) N/m2, quadratic bottom drag 3e-3 and
+# Coriolis from rest for 2000 steps of 30 s.  Those terms exist in the ROMS-form step
+# (oracle/roms_oracle.py, Model(semantics="roms")); at h = 4000 m and dx = 5 km its time step of
+# 30 s is c dt / dx = 1.2, beyond the scheme's 2D stability limit of 0.757 (von Neumann, tested
+# in tests/test_roms.py), so the same 16.7 simulated hours run as 4000 steps of 15 s (0.6).
+DT0, NSTEPS0 = 15.0, 4000
+
+
+def _roms_case():
+    import roms_oracle as ro
+    from sailfish_b200 import configs
+    cfg = configs.basin0()
+    g = cfg["grid"]
+    G = dict(h=g.h, pm=g.pm, pn=g.pn, on_u=g.on_u, om_v=g.om_v, fomn=g.fomn)
+    Ly = (g.M - 1) / g.pn.flat[0]
+    su = 0.1 * np.cos(np.pi * g.y / Ly) / 1025.0
+    return cfg, g, G, su, np.zeros_like(su), ro
+
+
+def test_roms_form_config0_forced_from_rest():
+    """2000 x 30 s of config 0's forcing from rest (as 4000 x 15 s): finite, volume conserved to
+    rounding, and a wind-driven flow: eastward depth-mean flow under the eastward wind of the
+    southern half, westward in the north, with sea level set up against the walls."""
+    cfg, g, G, su, sv, ro = _roms_case()
+    S = ro.State(g.J, g.I)
+    with np.errstate(all="raise"):
+        ro.main2d(G, S, NSTEPS0, DT0, su, sv, 3e-3)
+    z, u = S.zeta[1], S.ubar[1]
+    assert np.isfinite(z).all() and np.isfinite(u).all()
+    area = 1.0 / (g.pm * g.pn)
+    assert abs(ro.volume(G, z)) <= 1e-12 * np.abs(z).max() * area.sum()
+    J = g.J
+    south, north = u[2:J // 4, 3:-3].mean(), u[3 * J // 4:J - 2, 3:-3].mean()
+    assert south > 1e-4 and north < -1e-4
+    assert 1e-4 < np.abs(z).max() < 1e-2     # set-up ~ tau L / (rho g h) = 1.6 mm
+
+
+@pytest.mark.gpu
+def test_roms_form_config0_forced_cuda_bit_exact():
+    """The same run through the FP64 CUDA kernels (sf_roms_step2d), bit for bit."""
+    import torch
+    from sailfish_b200.model import Model
+    cfg, g, G, su, sv, ro = _roms_case()
+    m = Model(g, cfg["boundary"], cfg["dt"], 1, precision="fp64", semantics="roms")
+    m.set_forcing(su, sv, 3e-3)
+    m.dtfast = DT0
+    m.step2d(NSTEPS0)
+    torch.cuda.synchronize()
+    S = ro.State(g.J, g.I)
+    ro.main2d(G, S, NSTEPS0, DT0, su, sv, 3e-3)
+    sh = (g.J, g.I)
+    for n in ("zeta", "ubar", "vbar"):
+        buf = getattr(m, n).cpu().numpy()
+        for k in range(2):
+            np.testing.assert_array_equal(buf[m.slots[k]].reshape(sh), getattr(S, n)[k],
+                                          err_msg="%s[%d]" % (n, k))

@@ -309,3 +309,34 @@ def test_maxflux_omega_chunk_variants_agree(precision):
             else:
                 assert np.abs(b - a).max() <= 4e-6 * np.abs(a).max()
     assert lib.sf_ctx_tune(m.ctx.ptr, 0, 3) != 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_fused_predictor_pair_and_scalar_forms_agree(precision):
+    """The fused barotropic predictor's paired form (two nodes per thread, vector loads; taken
+    on grids with an even row length, 202 here) and its scalar form, through one whole step
+    from the same smooth state: identical in FP64; in FP32 the two forms' code may contract
+    products into FMAs differently, so they agree to FP32 rounding of each field's scale."""
+    import torch
+    from sailfish_b200._lib import lib
+    from sailfish_b200.model import Model
+    cfg, st = _inputs(200)
+    out = []
+    for pair in (1, 0):
+        m = Model(cfg["grid"], cfg["boundary"], cfg["dt"], cfg["ndtfast"], precision=precision)
+        assert lib.sf_ctx_tune(m.ctx.ptr, 1, pair) == 0
+        m.load(st)
+        m.step(1)
+        torch.cuda.synchronize()
+        out.append(m.state())
+        del m
+    assert out[0]["slots"] == out[1]["slots"]
+    for n in ("zeta", "ubar", "vbar", "rzeta", "rubar", "rvbar", "Zt_avg1", "DU_avg1", "DV_avg1",
+              "u", "v", "W"):
+        a, b = out[1][n], out[0][n]
+        assert np.isfinite(b).all(), n
+        if precision == "fp64":
+            np.testing.assert_array_equal(b, a, err_msg=n)
+        else:
+            assert np.abs(b - a).max() <= 2e-5 * np.abs(a).max(), (n, np.abs(b - a).max() / np.abs(a).max())
