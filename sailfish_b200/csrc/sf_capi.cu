@@ -885,6 +885,10 @@ int sf_ctx_tune(sf_ctx *c, int knob, int value) {
             }
         c->pred_pair = value;
         return SF_OK;
+    case SF_TUNE_S3_VEC:
+        if (value != 0 && value != 1) return fail(SF_EINVAL, "vec is 0 or 1");
+        c->s3_vec = value;
+        return SF_OK;
     default:
         return fail(SF_EINVAL, "unknown tuning knob");
     }

@@ -140,6 +140,8 @@ struct sf_ctx {
     int mo_chunk = 4;
     // fused predictor in its paired form (two nodes per thread) where the grid allows it
     int pred_pair = 1;
+    // FP32 column solve staged with 16-byte cp.async where aligned (else per element)
+    int s3_vec = 1;
     cudaStream_t cap = nullptr;
     double *d_bcval = nullptr;
     sf_loop_graph graphs[3];

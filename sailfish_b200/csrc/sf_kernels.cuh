@@ -576,6 +576,10 @@ __device__ __forceinline__ void cp_async_at(uint32_t saddr, const float *src, in
                  "n"(OFF));
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+// 16 bytes global -> shared, L2 only (both addresses 16-byte aligned)
+__device__ __forceinline__ void cp_async16(uint32_t saddr, const void *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(saddr), "l"(src));
+}
 template <int n>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(n)); }
 
@@ -1330,12 +1334,15 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint32_t a, uint32_t parity, i
     return false;
 }
 
-// BULK: the tile's levels arrive by bulk copies issued by thread 0 (ten per level, one
-// mbarrier per ring slot); otherwise every thread stages its own elements with cp.async.  The
-// arithmetic is the same either way, so the two give identical results; bulk staging is used
-// for tiles whose spans lie inside the fields (all but the first row of tiles and the last
-// tile) when the plane size and the field addresses keep the spans 16-byte aligned.
-template <typename R, bool BULK>   // R = float only: the FP32 form
+// MODE 0: every thread stages its own elements with 4-byte cp.async.  MODE 1: the tile's levels
+// arrive by bulk copies issued by thread 0 (ten per level, one mbarrier per ring slot).  MODE 2:
+// the threads stage the same 16-byte-aligned spans as MODE 1 with 16-byte cp.async, chunks
+// spread over the block (two per thread per level), completing through cp.async groups as in
+// MODE 0.  The arithmetic is the same in every mode, so they give identical results; modes 1
+// and 2 are used for tiles whose spans lie inside the fields (all but the first row of tiles
+// and the last tile) when the plane size and the field addresses keep the spans 16-byte
+// aligned.
+template <typename R, int MODE>   // R = float only: the FP32 form
 __device__ __forceinline__ void step3d_uv_pipe_body(const Geo<R> &g, float *__restrict__ u,
         float *__restrict__ v, const float *__restrict__ ru, const float *__restrict__ rv,
         float *__restrict__ ubar_t1, float *__restrict__ vbar_t1, float *__restrict__ ubar_t2,
@@ -1343,6 +1350,8 @@ __device__ __forceinline__ void step3d_uv_pipe_body(const Geo<R> &g, float *__re
         const float *__restrict__ z_r, const double *__restrict__ DU,
         const double *__restrict__ DV, const float *tmpU, const float *tmpV, float cff,
         float lambda, float Dt, int do_bc, float bcval, const long tile) {
+    constexpr bool BULK = MODE == 1;       // bulk copies completing on mbarriers
+    constexpr bool LAYB = MODE != 0;       // the aligned-span ring layout
     extern __shared__ __align__(16) float spipe[];
     const int N = g.N;
     const long I = g.I, s2 = g.s2;
@@ -1358,10 +1367,10 @@ __device__ __forceinline__ void step3d_uv_pipe_body(const Geo<R> &g, float *__re
     const uint32_t bar_s = ring_s + 4u * kPipeDepth * kPipeSlot;
     const int s2i = (int)s2;
     const int rB = (int)((4 - (I & 3)) & 3);   // the second span starts r before p0 - I
-    constexpr int row = BULK ? kRowB : kRow;    // floats between the Hz, Akv and z_r rows
+    constexpr int row = LAYB ? kRowB : kRow;    // floats between the Hz, Akv and z_r rows
     // this thread's own (p) and neighbour (p-1 or p-I) entries in a row
-    const int iP = BULK ? col + 4 : col + 1;
-    const int iQ = BULK ? (sys == 0 ? col + 3 : kSpan + rB + col) : (sys == 0 ? col : kPipeCols + 1 + col);
+    const int iP = LAYB ? col + 4 : col + 1;
+    const int iQ = LAYB ? (sys == 0 ? col + 3 : kSpan + rB + col) : (sys == 0 ? col : kPipeCols + 1 + col);
 
     int nslot = 0;   // slot of the next level issued (levels are issued in order)
     // element staging: level k into slot: Hz(k), Akv(k), z_r(k+1) at [p0-1, p0+63] (sys 0
@@ -1407,6 +1416,30 @@ __device__ __forceinline__ void step3d_uv_pipe_body(const Geo<R> &g, float *__re
             bulk_g2s(dv + cb, vo_all + o + p0, cb, bar);
             bulk_g2s(dv + 2u * cb, ru + o + p0, cb, bar);
             bulk_g2s(dv + 3u * cb, rv + o + p0, cb, bar);
+        } else if constexpr (MODE == 2) {
+            // 17 chunks per span (Hz, Akv, z_r(k+1) at a and b), then 16 per column field
+            constexpr int kSpanCh = kSpan / 4, kColCh = kPipeCols / 4;
+            const uint32_t d0 = ring_s + sb;
+            const long a0 = o + p0 - 4, b0 = o + p0 - I - rB;
+            const int nspan = zr ? 6 : 4;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int ch = (int)threadIdx.x + h * kPipeThreads;
+                if (ch < 6 * kSpanCh) {
+                    const int s = ch / kSpanCh, q = ch - s * kSpanCh;
+                    if (s < nspan) {
+                        const int fld = s >> 1, half = s & 1;
+                        const float *base = fld == 0 ? Hz : fld == 1 ? Akv : z_r + s2;
+                        cp_async16(d0 + 4u * (uint32_t)(fld * row + half * kSpan + 4 * q),
+                                   base + (half ? b0 : a0) + 4 * q);
+                    }
+                } else if (ch < 6 * kSpanCh + 4 * kColCh) {
+                    const int cc = ch - 6 * kSpanCh, f4 = cc / kColCh, q = cc - f4 * kColCh;
+                    const float *base = f4 == 0 ? uo_all : f4 == 1 ? vo_all : f4 == 2 ? ru : rv;
+                    cp_async16(d0 + 4u * (uint32_t)(3 * row + f4 * kPipeCols + 4 * q),
+                               base + o + p0 + 4 * q);
+                }
+            }
         } else {
             const int oz = zr ? o : o - s2i;
             cp_async_at<0>(dq + sb, cHz + o, nq);
@@ -1863,17 +1896,23 @@ __global__ void __launch_bounds__(kPipeThreads, 5) k_step3d_uv_pipe(
     Geo<R> g, float *__restrict__ u, float *__restrict__ v, const float *__restrict__ ru, const float *__restrict__ rv, float *__restrict__ ubar_t1,
     float *__restrict__ vbar_t1, float *__restrict__ ubar_t2, float *__restrict__ vbar_t2, const float *__restrict__ Hz, const float *__restrict__ Akv,
     const float *__restrict__ z_r, const double *__restrict__ DU, const double *__restrict__ DV, const float *tmpU, const float *tmpV,
-    float cff, float lambda, float Dt, int do_bc, float bcval, int bulk_ok) {
-    // bulk staging where the tile's spans (down to p0 - I - r, up to p0 + 63) lie in the plane
+    float cff, float lambda, float Dt, int do_bc, float bcval, int stage) {
+    // span staging (stage 1: bulk copies, 2: 16-byte cp.async) where the tile's spans (down to
+    // p0 - I - r, up to p0 + 63) lie in the plane; per-element staging elsewhere
     const long p0 = (long)blockIdx.x * kPipeCols, rB = (4 - (g.I & 3)) & 3;
-    if (bulk_ok && p0 - g.I - rB >= 0 && p0 + kPipeCols <= g.s2)
-        step3d_uv_pipe_body<R, true>(g, u, v, ru, rv, ubar_t1, vbar_t1, ubar_t2, vbar_t2, Hz, Akv,
-                                     z_r, DU, DV, tmpU, tmpV, cff, lambda, Dt, do_bc, bcval,
-                                     (long)blockIdx.x);
+    const bool inside = p0 - g.I - rB >= 0 && p0 + kPipeCols <= g.s2;
+    if (stage == 1 && inside)
+        step3d_uv_pipe_body<R, 1>(g, u, v, ru, rv, ubar_t1, vbar_t1, ubar_t2, vbar_t2, Hz, Akv,
+                                  z_r, DU, DV, tmpU, tmpV, cff, lambda, Dt, do_bc, bcval,
+                                  (long)blockIdx.x);
+    else if (stage == 2 && inside)
+        step3d_uv_pipe_body<R, 2>(g, u, v, ru, rv, ubar_t1, vbar_t1, ubar_t2, vbar_t2, Hz, Akv,
+                                  z_r, DU, DV, tmpU, tmpV, cff, lambda, Dt, do_bc, bcval,
+                                  (long)blockIdx.x);
     else
-        step3d_uv_pipe_body<R, false>(g, u, v, ru, rv, ubar_t1, vbar_t1, ubar_t2, vbar_t2, Hz, Akv,
-                                      z_r, DU, DV, tmpU, tmpV, cff, lambda, Dt, do_bc, bcval,
-                                      (long)blockIdx.x);
+        step3d_uv_pipe_body<R, 0>(g, u, v, ru, rv, ubar_t1, vbar_t1, ubar_t2, vbar_t2, Hz, Akv,
+                                  z_r, DU, DV, tmpU, tmpV, cff, lambda, Dt, do_bc, bcval,
+                                  (long)blockIdx.x);
 }
 template <typename R>
 __global__ void __launch_bounds__(kPipeThreads, 5) kb_step3d_uv_pipe(
@@ -1882,7 +1921,7 @@ __global__ void __launch_bounds__(kPipeThreads, 5) kb_step3d_uv_pipe(
     const float *__restrict__ Akv, const float *__restrict__ z_r, const double *__restrict__ DU, const double *__restrict__ DV, const float *tmpU,
     const float *tmpV, float cff, float lambda, float Dt, int do_bc, float bcval) {
     SF_MEMBER(bm)
-    step3d_uv_pipe_body<R, false>(g, O3(u), O3(v), O3(ru), O3(rv), O2(ubar_t1), O2(vbar_t1), O2(ubar_t2),
+    step3d_uv_pipe_body<R, 0>(g, O3(u), O3(v), O3(ru), O3(rv), O2(ubar_t1), O2(vbar_t1), O2(ubar_t2),
                         O2(vbar_t2), ON(Hz), O3(Akv), ON(z_r), O2(DU), O2(DV), O3(tmpU), O3(tmpV),
                         cff, lambda, Dt, do_bc, bcval, (long)mb_.y);
 }
@@ -2120,15 +2159,16 @@ cudaError_t Ops<R>::step3d_uv(const sf_ctx *c, R *u, R *v, const R *ru, const R 
             return cudaGetLastError();
         }
         if (fits) {
-            // bulk staging needs 16-byte aligned spans: every level starts on a 16-byte
+            // span staging needs 16-byte aligned spans: every level starts on a 16-byte
             // boundary (s2 a multiple of 4) in 16-byte aligned fields
             auto al = [](const void *q) { return q == nullptr || ((uintptr_t)q & 15) == 0; };
-            const int bulk_ok = c->s2 % 4 == 0 && al(u) && al(v) && al(ru) && al(rv) && al(Hz) &&
-                                al(Akv) && al(z_r) && al(tmpU) && al(tmpV) && c->use_bulk;
+            const bool aligned = c->s2 % 4 == 0 && al(u) && al(v) && al(ru) && al(rv) && al(Hz) &&
+                                 al(Akv) && al(z_r) && al(tmpU) && al(tmpV);
+            const int stage = !aligned ? 0 : c->use_bulk ? 1 : c->s3_vec ? 2 : 0;
             k_step3d_uv_pipe<float><<<blocks_for(c->s2, kPipeCols), kPipeThreads,
                                       pipe_smem_bytes(c->N), s>>>(
                 geo(c), u, v, ru, rv, ubar_t1, vbar_t1, ubar_t2, vbar_t2, Hz, Akv, z_r, DU, DV,
-                tmpU, tmpV, (float)cff, (float)lambda, (float)Dt, do_bc, (float)bcval, bulk_ok);
+                tmpU, tmpV, (float)cff, (float)lambda, (float)Dt, do_bc, (float)bcval, stage);
             return cudaGetLastError();
         }
     }

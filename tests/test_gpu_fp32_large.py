@@ -258,13 +258,15 @@ def test_fp64_step_bit_exact_against_the_oracle_at_size():
 @pytest.mark.parametrize("Lm", CASES)
 def test_column_solve_bulk_and_element_staging_agree(Lm):
     """The FP32 column solve with its levels staged by bulk copies (cp.async.bulk, interior
-    tiles) and by per-element cp.async (sf_ctx_set_bulk(ctx, 0)): identical results."""
+    tiles), by 16-byte cp.async of the same spans (the default) and by per-element cp.async:
+    identical results."""
     import torch
     from sailfish_b200._lib import lib, check
     out = []
-    for bulk in (1, 0):
+    for bulk, vec in ((1, 0), (0, 1), (0, 0)):
         _, m = _models(Lm)
         assert lib.sf_ctx_set_bulk(m.ctx.ptr, bulk) == 0
+        assert lib.sf_ctx_tune(m.ctx.ptr, 2, vec) == 0
         p = m._p
         st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
         sl = lambda n, k: getattr(m, n)[m.slots[k]]
@@ -275,8 +277,9 @@ def test_column_solve_bulk_and_element_staging_agree(Lm):
         m.check_state()            # also reports a bounded wait that gave up
         torch.cuda.synchronize()
         out.append([t.cpu().numpy() for t in (m.u, m.v, sl("ubar", 1), sl("vbar", 1))])
-    for a, b in zip(out[0], out[1]):
-        np.testing.assert_array_equal(a, b)
+    for o in out[1:]:
+        for a, b in zip(out[0], o):
+            np.testing.assert_array_equal(a, b)
 
 
 @pytest.mark.gpu
