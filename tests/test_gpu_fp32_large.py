@@ -321,13 +321,13 @@ def test_fused_predictor_pair_and_scalar_forms_agree(precision):
     on grids with an even row length, 202 here) and its scalar form, through one whole step
     from the same smooth state: identical in FP64; in FP32 the two forms' code may contract
     products into FMAs differently, so they agree to FP32 rounding of each field's scale
-    (rzeta, a difference of nearly equal fluxes, 4.4e-5 measured)."""
+    (measured: rzeta 4.4e-5 and rvbar 2.3e-4, differences of nearly equal terms)."""
     import torch
     from sailfish_b200._lib import lib
     from sailfish_b200.model import Model
     cfg, st = _inputs(200)
     out = []
-    for pair in (1, 0):
+    for pair in (0, 1, 2):      # scalar, paired, paired reloading its inputs in phase 2
         m = Model(cfg["grid"], cfg["boundary"], cfg["dt"], cfg["ndtfast"], precision=precision)
         assert lib.sf_ctx_tune(m.ctx.ptr, 1, pair) == 0
         m.load(st)
@@ -335,12 +335,17 @@ def test_fused_predictor_pair_and_scalar_forms_agree(precision):
         torch.cuda.synchronize()
         out.append(m.state())
         del m
-    assert out[0]["slots"] == out[1]["slots"]
-    for n in ("zeta", "ubar", "vbar", "rzeta", "rubar", "rvbar", "Zt_avg1", "DU_avg1", "DV_avg1",
-              "u", "v", "W"):
-        a, b = out[1][n], out[0][n]
-        assert np.isfinite(b).all(), n
-        if precision == "fp64":
-            np.testing.assert_array_equal(b, a, err_msg=n)
-        else:
-            assert np.abs(b - a).max() <= 1e-4 * np.abs(a).max(), (n, np.abs(b - a).max() / np.abs(a).max())
+    names = ("zeta", "ubar", "vbar", "rzeta", "rubar", "rvbar", "Zt_avg1", "DU_avg1", "DV_avg1",
+             "u", "v", "W")
+    for o in out[1:]:
+        assert out[0]["slots"] == o["slots"]
+        for n in names:
+            a, b = out[0][n], o[n]
+            assert np.isfinite(b).all(), n
+            if precision == "fp64":
+                np.testing.assert_array_equal(b, a, err_msg=n)
+            else:
+                # the right-hand sides difference nearly equal fluxes and pressure terms
+                tol = 5e-4 if n in ("rzeta", "rubar", "rvbar") else 1e-4
+                err = np.abs(b - a).max() / np.abs(a).max()
+                assert err <= tol, (n, err)
