@@ -105,19 +105,25 @@ def launches_per_step(m, mixing):
 
 
 def traffic_per_launch(kernel, grid):
-    """DRAM bytes per launch of `kernel` from the committed ncu summary (profiles/), scaled
-    from its basin to this grid by the number of 3D points; None if not recorded."""
-    path = os.path.join(ROOT, "profiles", "k3d_basin4q_fp32.md")
-    try:
-        with open(path) as f:
-            for line in f:
-                t = line.split()
-                if len(t) == 6 and t[0] == "traffic" and t[1] == kernel:
-                    rd, wr, s2, n = (float(x) for x in t[2:])
-                    return (rd + wr) * (grid.s2 * grid.N) / (s2 * n)
-    except OSError:
-        pass
-    return None
+    """DRAM bytes per launch of `kernel` from the committed ncu summaries (profiles/*.md), with
+    the summary's name: a 'traffic <kernel> <read> <write> <s2> <N>' line (a 3D kernel,
+    scaled to this grid by the number of 3D points) or 'traffic2d <kernel> <read> <write> <s2>'
+    (a 2D kernel, scaled by the 2D points); (None, None) if not recorded."""
+    import glob
+    for path in sorted(glob.glob(os.path.join(ROOT, "profiles", "*.md"))):
+        try:
+            with open(path) as f:
+                for line in f:
+                    t = line.split()
+                    if len(t) == 6 and t[0] == "traffic" and t[1] == kernel:
+                        rd, wr, s2, n = (float(x) for x in t[2:])
+                        return (rd + wr) * (grid.s2 * grid.N) / (s2 * n), os.path.basename(path)
+                    if len(t) == 5 and t[0] == "traffic2d" and t[1] == kernel:
+                        rd, wr, s2 = (float(x) for x in t[2:])
+                        return (rd + wr) * grid.s2 / s2, os.path.basename(path)
+        except OSError:
+            pass
+    return None, None
 
 
 def config_of(args):
@@ -852,6 +858,7 @@ def run_ours(args, rank, world):
     value = cells * args.steps * world / (ms * 1e-3)
     # launches per baroclinic step, plus one omega at the end of the timed call
     per_step = launches_per_step(m, mixing)
+    traffic = traffic_per_launch(dom, grid) if args.precision == "fp32" else (None, None)
     out = {
         "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
@@ -880,9 +887,10 @@ def run_ours(args, rank, world):
                      "unit": "GB/s", "frac": achieved / peak, "peak_kind": kind,
                      "launch_ms": per_launch[dom][0], "launches_per_step": per_launch[dom][1],
                      "algorithmic_bytes": ab[dom],
-                     "traffic": traffic_per_launch(dom, grid) if args.precision == "fp32" else None,
-                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum on basin4q "
-                                       "(profiles/k3d_basin4q_fp32.md), scaled by 3D points"},
+                     "traffic": traffic[0],
+                     "traffic_source": None if traffic[0] is None else
+                     "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch "
+                     "(profiles/%s), scaled to this grid" % traffic[1]},
         "e2e": {"value": cells / (e_ms * 1e-3), "unit": "cell-steps/s",
                 "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo},
         "gpu_launches": args.steps * per_step + 1,

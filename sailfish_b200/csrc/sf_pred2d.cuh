@@ -488,28 +488,6 @@ __device__ __forceinline__ void prd_rz_pair(const PredArgs<R> &a, long x, PrdPai
     rzb = (((DUeb * oue - DUpb * n.oub) + (DVnb * ovnb - DVpb * n.ovb)) * n.pmb) * n.pnb;
 }
 
-// The kept inputs of a deep pair read again (the reloading form keeps nothing in registers
-// across the block's barrier, for more resident warps).
-template <typename R>
-__device__ __forceinline__ void prd_load_pair(const PredArgs<R> &a, long x, PrdPair<R> &n) {
-    const Geo<R> &g = a.g;
-    const int I = g.I;
-    const R *z = a.z1 + x, *h = g.h + x;
-    ld2(z, n.z1a, n.z1b);
-    n.z1w = z[-1];
-    ld2(z - I, n.z1sa, n.z1sb);
-    ld2(h, n.ha, n.hb);
-    n.hw = h[-1];
-    ld2(h - I, n.hsa, n.hsb);
-    ld2(a.ub1 + x, n.uba, n.ubb);
-    ld2(a.vb1 + x, n.vba, n.vbb);
-    ld2(g.on_u + x, n.oua, n.oub);
-    ld2(g.om_v + x, n.ova, n.ovb);
-    ld2(g.pm + x, n.pma, n.pmb);
-    ld2(g.pn + x, n.pna, n.pnb);
-    ld2(a.z0 + x, n.z0a, n.z0b);
-}
-
 // The momentum of a deep pair from the tile's zeta_t2: za, zb at the nodes, zw west of a, zsa
 // and zsb south of them.
 template <typename R>
@@ -557,11 +535,12 @@ __host__ __device__ __forceinline__ bool prd_inner_pair_tile(int i0, int j0, int
     return i0 >= 4 && j0 >= 3 && i0 + kPairTX + 2 <= I && j0 + kPairTY + 2 <= J;
 }
 
-// RELOAD: phase 2 reads the pair's inputs again instead of keeping them in registers across
-// the barrier (three resident blocks per SM instead of two).
-template <typename R, bool RELOAD>
-__global__ void __launch_bounds__(512, RELOAD ? 3 : 2) k_pred2d_pair(
-        const __grid_constant__ PredArgs<R> a, int ring_blocks, int tiles_x, int edge_blocks) {
+// The kept inputs stay in registers across the block's barrier (64 registers, two blocks per
+// SM): a form that read them again after the barrier (40 registers, three blocks per SM) took
+// the basin4 loop to 4.72 ms against 4.30.
+template <typename R>
+__global__ void __launch_bounds__(512, 2) k_pred2d_pair(const __grid_constant__ PredArgs<R> a,
+                                                       int ring_blocks, int tiles_x, int edge_blocks) {
     pdl_enter();
     __shared__ R sZ[kPairTY + 1][kPairTX + 2];   // zeta_t2 after zetabc, (j0-1.., i0-2..)
     __shared__ R sDummy[kPredTY + 1][kPredTX + 1];
@@ -603,7 +582,6 @@ __global__ void __launch_bounds__(512, RELOAD ? 3 : 2) k_pred2d_pair(
         __syncthreads();
         // ---- phase 2: momentum of the tile's deep pairs ---------------------------------------
         if (deep && tx >= 1 && r >= 1) {
-            if constexpr (RELOAD) prd_load_pair(a, x, kept);
             const int qa = j * I + i, qb = qa + 1;
             const bool pda = qa - fdiv(qa, g.dJ) * J != 0 && qa >= J;   // q % J != 0 (szJ)
             const bool pdb = qb - fdiv(qb, g.dJ) * J != 0 && qb >= J;
@@ -661,11 +639,7 @@ cudaError_t Ops<R>::pred2d(const sf_ctx *c, R *z0, R *z1, R *z2, R *ub1, R *vb1,
         for (int ty = 0; ty < tiles_y; ++ty)
             inner_y += prd_inner_pair_tile(4, ty * kPairTY, 4 + kPairTX + 2, c->J);
         const int edge_blocks = ring_blocks + tiles_x * tiles_y - inner_x * inner_y;
-        if (c->pred_pair == 2)
-            return launch_dep(c, k_pred2d_pair<R, true>,
-                              dim3((unsigned)(ring_blocks + tiles_x * tiles_y)), dim3(32, 16), 0, s,
-                              a, ring_blocks, tiles_x, edge_blocks);
-        return launch_dep(c, k_pred2d_pair<R, false>, dim3((unsigned)(ring_blocks + tiles_x * tiles_y)),
+        return launch_dep(c, k_pred2d_pair<R>, dim3((unsigned)(ring_blocks + tiles_x * tiles_y)),
                           dim3(32, 16), 0, s, a, ring_blocks, tiles_x, edge_blocks);
     }
     const int tiles_x = (c->I + kPredTX - 1) / kPredTX, tiles_y = (c->J + kPredTY - 1) / kPredTY;
