@@ -184,8 +184,8 @@ int sf_ctx_set_bulk(sf_ctx *ctx, int enable);
  *   issues together on columns whose fluxes it all computes itself;
  * SF_TUNE_PRED_PAIR: 1 (default) for the fused predictor's paired form (two nodes per thread,
  *   vector loads) on grids with an even row length and aligned fields, 0 for the scalar form;
- * SF_TUNE_S3_VEC: 1 for the FP32 column solve's levels staged as 16-byte-aligned spans with
- *   16-byte cp.async where the fields allow it, 0 (default) for per-element cp.async
+ * SF_TUNE_S3_VEC: 1 (default) for the FP32 column solve's levels staged as 16-byte-aligned
+ *   spans with 16-byte cp.async where the fields allow it, 0 for per-element cp.async
  *   (sf_ctx_set_bulk(ctx, 1) takes the same spans through bulk copies instead).
  * Results are identical for every value in FP64; in FP32 the compiler may contract products
  * into FMAs differently in the variants, so they agree to the rounding of FP32. */

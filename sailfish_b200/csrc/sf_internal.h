@@ -140,9 +140,9 @@ struct sf_ctx {
     int mo_chunk = 4;
     // fused predictor in its paired form (two nodes per thread) where the grid allows it
     int pred_pair = 1;
-    // FP32 column solve staged with 16-byte cp.async where aligned (else per element); off by
-    // default: on one B200 basin4 takes 1.597 ms with it and 1.591 ms without
-    int s3_vec = 0;
+    // FP32 column solve staged with 16-byte cp.async where aligned (else per element): on one
+    // B200 basin4 takes 1.43 ms with it and 1.56 ms without
+    int s3_vec = 1;
     cudaStream_t cap = nullptr;
     double *d_bcval = nullptr;
     sf_loop_graph graphs[3];

@@ -1372,7 +1372,8 @@ __device__ __forceinline__ void step3d_uv_pipe_body(const Geo<R> &g, float *__re
     const int iP = LAYB ? col + 4 : col + 1;
     const int iQ = LAYB ? (sys == 0 ? col + 3 : kSpan + rB + col) : (sys == 0 ? col : kPipeCols + 1 + col);
 
-    int nslot = 0;   // slot of the next level issued (levels are issued in order)
+    // level k goes to ring slot k % kPipeDepth; the main loop is unrolled over one turn of the
+    // ring so that every slot index (and so every shared-memory offset) is a constant
     // element staging: level k into slot: Hz(k), Akv(k), z_r(k+1) at [p0-1, p0+63] (sys 0
     // copies these, plus old u and ru) and [p0-I, p0-I+63] (sys 1, plus old v and rv); sources
     // outside [0, s2) in the plane are zero-filled (their columns are not U/V nodes).
@@ -1392,10 +1393,36 @@ __device__ __forceinline__ void step3d_uv_pipe_body(const Geo<R> &g, float *__re
     // level 0 (the launcher keeps (N+1) s2 below 2^31 for this kernel)
     const uint32_t dq = ring_s + 4u * seg, dE = ring_s + 4u * kPipeCols;
     const uint32_t dO = ring_s + 4u * oO, dR = ring_s + 4u * oR;
-    auto issue = [&](int k) {
-        const uint32_t sb = (uint32_t)nslot * (4u * kPipeSlot);
-        const int sl = nslot;
-        nslot = nslot + 1 == kPipeDepth ? 0 : nslot + 1;
+    // MODE 2: this thread's two 16-byte chunks of every level, fixed per thread: 17 chunks per
+    // span (Hz, Akv, z_r(k+1) at p0 - 4 and p0 - I - r), then 16 per column field (old u, old
+    // v, ru, rv); destination byte offsets within a slot, sources at level 0
+    bool vact[2] = {false, false}, vzr[2] = {false, false};
+    uint32_t vdst[2] = {0u, 0u};
+    const float *vsrc[2] = {Hz, Hz};
+    if constexpr (MODE == 2) {
+        constexpr int kSpanCh = kSpan / 4, kColCh = kPipeCols / 4;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int ch = (int)threadIdx.x + h * kPipeThreads;
+            if (ch < 6 * kSpanCh) {
+                const int s = ch / kSpanCh, q = ch - s * kSpanCh;
+                const int fld = s >> 1, half = s & 1;
+                const float *base = fld == 0 ? Hz : fld == 1 ? Akv : z_r + s2;
+                vact[h] = true;
+                vzr[h] = fld == 2;
+                vdst[h] = 4u * (uint32_t)(fld * row + half * kSpan + 4 * q);
+                vsrc[h] = base + (half ? p0 - I - rB : p0 - 4) + 4 * q;
+            } else if (ch < 6 * kSpanCh + 4 * kColCh) {
+                const int c4 = ch - 6 * kSpanCh, f4 = c4 / kColCh, q = c4 - f4 * kColCh;
+                const float *base = f4 == 0 ? uo_all : f4 == 1 ? vo_all : f4 == 2 ? ru : rv;
+                vact[h] = true;
+                vdst[h] = 4u * (uint32_t)(3 * row + f4 * kPipeCols + 4 * q);
+                vsrc[h] = base + p0 + 4 * q;
+            }
+        }
+    }
+    auto issue = [&](int k, int sl) {
+        const uint32_t sb = (uint32_t)sl * (4u * kPipeSlot);
         const int o = k * s2i;
         const bool zr = k + 1 < N;   // z_r(k+1) exists for k < N-1 only
         if constexpr (BULK) {   // thread 0 only
@@ -1417,29 +1444,10 @@ __device__ __forceinline__ void step3d_uv_pipe_body(const Geo<R> &g, float *__re
             bulk_g2s(dv + 2u * cb, ru + o + p0, cb, bar);
             bulk_g2s(dv + 3u * cb, rv + o + p0, cb, bar);
         } else if constexpr (MODE == 2) {
-            // 17 chunks per span (Hz, Akv, z_r(k+1) at a and b), then 16 per column field
-            constexpr int kSpanCh = kSpan / 4, kColCh = kPipeCols / 4;
             const uint32_t d0 = ring_s + sb;
-            const long a0 = o + p0 - 4, b0 = o + p0 - I - rB;
-            const int nspan = zr ? 6 : 4;
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int ch = (int)threadIdx.x + h * kPipeThreads;
-                if (ch < 6 * kSpanCh) {
-                    const int s = ch / kSpanCh, q = ch - s * kSpanCh;
-                    if (s < nspan) {
-                        const int fld = s >> 1, half = s & 1;
-                        const float *base = fld == 0 ? Hz : fld == 1 ? Akv : z_r + s2;
-                        cp_async16(d0 + 4u * (uint32_t)(fld * row + half * kSpan + 4 * q),
-                                   base + (half ? b0 : a0) + 4 * q);
-                    }
-                } else if (ch < 6 * kSpanCh + 4 * kColCh) {
-                    const int cc = ch - 6 * kSpanCh, f4 = cc / kColCh, q = cc - f4 * kColCh;
-                    const float *base = f4 == 0 ? uo_all : f4 == 1 ? vo_all : f4 == 2 ? ru : rv;
-                    cp_async16(d0 + 4u * (uint32_t)(3 * row + f4 * kPipeCols + 4 * q),
-                               base + o + p0 + 4 * q);
-                }
-            }
+            for (int h = 0; h < 2; ++h)
+                if (vact[h] && (zr || !vzr[h])) cp_async16(d0 + vdst[h], vsrc[h] + o);
         } else {
             const int oz = zr ? o : o - s2i;
             cp_async_at<0>(dq + sb, cHz + o, nq);
@@ -1467,11 +1475,15 @@ __device__ __forceinline__ void step3d_uv_pipe_body(const Geo<R> &g, float *__re
             asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         }
         __syncthreads();
-        if (threadIdx.x == 0)
-            for (int k = 0; k < kAhead && k < N; ++k) issue(k);
+        if (threadIdx.x == 0) {
+#pragma unroll
+            for (int k = 0; k < kAhead; ++k)
+                if (k < N) issue(k, k);
+        }
     } else {
+#pragma unroll
         for (int k = 0; k < kAhead; ++k) {
-            if (k < N) issue(k);
+            if (k < N) issue(k, k);
             cp_async_commit();
         }
     }
@@ -1488,10 +1500,8 @@ __device__ __forceinline__ void step3d_uv_pipe_body(const Geo<R> &g, float *__re
     // group g every thread has finished group g-1, whose slots (kPipeDepth is a multiple of the
     // group) are refilled with group g+2, so two groups are in flight while one is eliminated
     static_assert(kPipeDepth % kPipeGroup == 0, "levels are consumed in whole groups");
-    int cslot = 0;   // slot of the next level consumed (levels are consumed in order)
-    auto level = [&](int k) {
-        const float *sl = ring + cslot * kPipeSlot;
-        cslot = cslot + 1 == kPipeDepth ? 0 : cslot + 1;
+    auto level = [&](int k, int slot) {
+        const float *sl = ring + slot * kPipeSlot;
         const float *sHz = sl, *sAk = sl + row, *sZr = sl + 2 * row;
         const float *sO = sl + 3 * row + sys * kPipeCols, *sR = sl + 3 * row + (2 + sys) * kPipeCols;
         const float hz = (sHz[iP] + sHz[iQ]) * 0.5f;
@@ -1522,35 +1532,38 @@ __device__ __forceinline__ void step3d_uv_pipe_body(const Geo<R> &g, float *__re
         H += (double)hz;
         O += (double)(ok * hz);
     };
-    for (int k0 = 0; k0 < N; k0 += kPipeGroup) {
-        if constexpr (BULK) {
+    for (int k0 = 0; k0 < N; k0 += kPipeDepth) {   // one turn of the ring
+        const uint32_t parity = (uint32_t)((k0 / kPipeDepth) & 1);
 #pragma unroll
-            for (int h = 0; h < kPipeGroup; ++h) {
-                const int k = k0 + h;
-                if (k < N)
-                    mbar_wait_bounded(bar_s + 8u * (k % kPipeDepth), (uint32_t)((k / kPipeDepth) & 1),
-                                      g.err);
+        for (int gs = 0; gs < kPipeDepth; gs += kPipeGroup) {   // group in slots gs, gs+1, ...
+            const int kg = k0 + gs;
+            if (kg < N) {   // uniform over the block
+                if constexpr (BULK) {
+#pragma unroll
+                    for (int h = 0; h < kPipeGroup; ++h)
+                        if (kg + h < N) mbar_wait_bounded(bar_s + 8u * (gs + h), parity, g.err);
+                    __syncthreads();
+                    if (threadIdx.x == 0) {
+                        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+#pragma unroll
+                        for (int h = 0; h < kPipeGroup; ++h)
+                            if (kg + kAhead + h < N) issue(kg + kAhead + h, (gs + kAhead + h) % kPipeDepth);
+                    }
+                } else {
+                    cp_async_wait<kAhead - kPipeGroup>();   // this group's levels (the next may be in flight)
+                    __syncthreads();
+#pragma unroll
+                    for (int h = 0; h < kPipeGroup; ++h) {
+                        if (kg + kAhead + h < N) issue(kg + kAhead + h, (gs + kAhead + h) % kPipeDepth);
+                        cp_async_commit();
+                    }
+                }
+                if (both) {
+#pragma unroll
+                    for (int h = 0; h < kPipeGroup; ++h)
+                        if (kg + h < N) level(kg + h, gs + h);
+                }
             }
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-#pragma unroll
-                for (int h = 0; h < kPipeGroup; ++h)
-                    if (k0 + kAhead + h < N) issue(k0 + kAhead + h);
-            }
-        } else {
-            cp_async_wait<kAhead - kPipeGroup>();   // this group's levels (the next may be in flight)
-            __syncthreads();
-#pragma unroll
-            for (int h = 0; h < kPipeGroup; ++h) {
-                if (k0 + kAhead + h < N) issue(k0 + kAhead + h);
-                cp_async_commit();
-            }
-        }
-        if (both) {
-#pragma unroll
-            for (int h = 0; h < kPipeGroup; ++h)
-                if (k0 + h < N) level(k0 + h);
         }
     }
     cp_async_wait<0>();
