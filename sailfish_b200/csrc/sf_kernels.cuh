@@ -727,9 +727,9 @@ __device__ __forceinline__ void rhs3d_body(const Geo<R> &g, const R *__restrict_
 
     // the staging offsets of this thread, once per block
     const std::conditional_t<P2, PairMap<TX, TY>, StageMap<TX, TY>> pm(g.I, (int)j0, (int)i0, tid);
-    auto issue = [&](int K) {
+    auto issue = [&](int K, int buf) {   // level K into staging buffer buf (= K % kBufs)
         const long o = (long)K * s2;
-        R(*bf)[kSN] = sbuf[K % kBufs];
+        R(*bf)[kSN] = sbuf[buf];
         if constexpr (P2) {
             // W is staged from level K+1 and Hz has N levels: o + rmax < N s2 covers all six
             const bool safe = o + pm.rmin >= 0 && o + pm.rmax < lenHz;
@@ -749,28 +749,34 @@ __device__ __forceinline__ void rhs3d_body(const Geo<R> &g, const R *__restrict_
         }
         cp_async_commit();
     };
-    issue(0);
+    issue(0, 0);
     if constexpr (kBufs == 3) {
-        if (N > 1) issue(1);
+        if (N > 1) issue(1, 1);
         else cp_async_commit();
     }
-    for (int K = 0; K < N; ++K) {
+    // the level loop is unrolled over the staging buffers, so that each level's buffer (and
+    // every shared-memory offset into it) is a constant
+    for (int K0 = 0; K0 < N; K0 += kBufs) {
+#pragma unroll
+    for (int kb = 0; kb < kBufs; ++kb) {
+        const int K = K0 + kb;
+        if (K >= N) break;   // uniform over the block
         const long o = (long)K * s2;
         if constexpr (kBufs == 3) {
             cp_async_wait<1>();   // level K's group (level K+1's may still be in flight)
             __syncthreads();      // ... and every thread is done with level K-1
-            if (K + 2 < N) issue(K + 2);
+            if (K + 2 < N) issue(K + 2, (kb + 2) % kBufs);
             else cp_async_commit();
         } else {
             if (K + 1 < N) {
-                issue(K + 1);
+                issue(K + 1, (kb + 1) % kBufs);
                 cp_async_wait<1>();
             } else {
                 cp_async_wait<0>();
             }
             __syncthreads();
         }
-        R(*bf)[kSN] = sbuf[K % kBufs];
+        R(*bf)[kSN] = sbuf[kb];
         const Tile<R, kSX> U{bf[0], b}, V{bf[1], b}, HU{bf[2], b}, HV{bf[3], b}, HZ{bf[4], b}, WW{bf[5], b};
         // Every thread reaches both barriers of each level: the compute is predicated on
         // `live` rather than skipped with `continue` (an aligned barrier must not diverge).
@@ -896,6 +902,7 @@ __device__ __forceinline__ void rhs3d_body(const Geo<R> &g, const R *__restrict_
         }
         if constexpr (kBufs == 2) __syncthreads();   // the buffer of level K is refilled next
     }
+    }
     if (!live) return;
     const long oN = (long)N * s2;
     ru[oN + p] = va ? ruN3 : R(0);   // ru_t2[:] = 0 (rhs.py:38); ru[N] = ru[N-2] (:193)
@@ -965,27 +972,29 @@ __device__ __forceinline__ void maxflux_omega_body(
             // every flux this column needs is computed here: the loads of a chunk of levels
             // (Hz, u, v only, never the flux arrays being written) are issued together
             // before any of the chunk's arithmetic, the same expressions as below
+            // 32-bit element offsets (the launcher takes this form only where (N+1) s2 < 2^31)
+            const int s2i = (int)s2, Ii = (int)I;
             for (int K0 = 0; K0 < N; K0 += (C > 0 ? C : 1)) {
                 constexpr int CC = C > 0 ? C : 1;
                 R hz[CC], hzw[CC], hzs[CC], hze[CC], hzn[CC], uu[CC], uE[CC], vv[CC], vN[CC];
 #pragma unroll
                 for (int c = 0; c < CC; ++c) {
-                    const long o = (long)(K0 + c < N ? K0 + c : N - 1) * s2 + p;
+                    const int o = (K0 + c < N ? K0 + c : N - 1) * s2i + pi;
                     hz[c] = Hz[o];
                     hzw[c] = Hz[o - 1];
-                    hzs[c] = Hz[o - I];
+                    hzs[c] = Hz[o - Ii];
                     hze[c] = Hz[o + 1];
-                    hzn[c] = Hz[o + I];
+                    hzn[c] = Hz[o + Ii];
                     uu[c] = u[o];
                     uE[c] = u[o + 1];
                     vv[c] = v[o];
-                    vN[c] = v[o + I];
+                    vN[c] = v[o + Ii];
                 }
 #pragma unroll
                 for (int c = 0; c < CC; ++c) {
                     const int K = K0 + c;
                     if (K < N) {
-                        const long o = (long)K * s2 + p;
+                        const int o = K * s2i + pi;
                         const R hup = (((hz[c] + hzw[c]) * R(0.5)) * uu[c]) * onu;
                         const R hvp = (((hz[c] + hzs[c]) * R(0.5)) * vv[c]) * omv;
                         Huon[o] = hup;
@@ -1020,10 +1029,19 @@ __device__ __forceinline__ void maxflux_omega_body(
         const R h = z_w[(long)(N - 1) * s2 + p] - zbed;
         const R Ws = Wk;
         W[p] = R(0);
+        if constexpr (C > 0) {
+            const int s2i = (int)s2;
 #pragma unroll 4
-        for (int K = 1; K < N; ++K) {
-            const long o = (long)K * s2 + p;
-            W[o] = Wc(K) - ddiv(Ws * (z_w[o] - zbed), h);
+            for (int K = 1; K < N; ++K) {
+                const int o = K * s2i + pi;
+                W[o] = Wc(K) - ddiv(Ws * (z_w[o] - zbed), h);
+            }
+        } else {
+#pragma unroll 4
+            for (int K = 1; K < N; ++K) {
+                const long o = (long)K * s2 + p;
+                W[o] = Wc(K) - ddiv(Ws * (z_w[o] - zbed), h);
+            }
         }
 #undef Wc
         W[(long)N * s2 + p] = R(0);
@@ -2120,7 +2138,10 @@ cudaError_t Ops<R>::maxflux_omega(const sf_ctx *c, const R *u, const R *v, R *Hu
                                                            Zt);
         return cudaGetLastError();
     }
-    auto k = c->mo_chunk >= 8 ? k_maxflux_omega<R, 8>
+    // the chunked forms address with 32-bit element offsets
+    const bool fits = (long)(c->N + 1) * c->s2 < (1L << 31);
+    auto k = (!fits || !do_flux) ? k_maxflux_omega<R, 0>   // omega alone: 0.66 against 0.72 ms
+             : c->mo_chunk >= 8 ? k_maxflux_omega<R, 8>
              : c->mo_chunk >= 4 ? k_maxflux_omega<R, 4> : k_maxflux_omega<R, 0>;
     k<<<blocks_for(c->s2, kBlock), kBlock, smem, s>>>(
         geo(c), u, v, Huon, Hvom, Hz, W, z_w, do_flux, do_omega, zeta1, zeta2, Zt);
