@@ -182,8 +182,9 @@ int sf_ctx_set_bulk(sf_ctx *ctx, int enable);
 /* Tuning knobs of a context's kernels (no counterpart in the reference):
  * SF_TUNE_MO_CHUNK: 0, 4 (default) or 8 levels whose loads the fused set_maxflux/omega kernel
  *   issues together on columns whose fluxes it all computes itself;
- * SF_TUNE_PRED_PAIR: 1 (default) for the fused predictor's paired form (two nodes per thread,
- *   vector loads) on grids with an even row length and aligned fields, 0 for the scalar form;
+ * SF_TUNE_PRED_PAIR: the fused predictor's paired form (two nodes per thread, vector loads) on
+ *   grids with an even row length and aligned fields, with blocks of 16 staged rows (1) or 8
+ *   (2, default); 0 for the scalar form;
  * SF_TUNE_S3_VEC: 1 (default) for the FP32 column solve's levels staged as 16-byte-aligned
  *   spans with 16-byte cp.async where the fields allow it, 0 for per-element cp.async
  *   (sf_ctx_set_bulk(ctx, 1) takes the same spans through bulk copies instead).

@@ -138,8 +138,9 @@ struct sf_ctx {
     int use_bulk = 0;
     // levels whose loads the fused flux/omega kernel issues together (sf_ctx_tune)
     int mo_chunk = 4;
-    // fused predictor in its paired form (two nodes per thread) where the grid allows it
-    int pred_pair = 1;
+    // fused predictor in its paired form (two nodes per thread) where the grid allows it: 1
+    // with 16-row blocks, 2 with 8-row blocks (basin4 loop 4.27 and 4.18 ms), 0 scalar (4.49)
+    int pred_pair = 2;
     // FP32 column solve staged with 16-byte cp.async where aligned (else per element): on one
     // B200 basin4 takes 1.43 ms with it and 1.56 ms without
     int s3_vec = 1;

@@ -406,7 +406,7 @@ __global__ void __launch_bounds__(256, 5) k_pred2d(const __grid_constant__ PredA
 // the scalar form bit for bit.  A tile is 62 x 15 nodes, staged with two west halo columns
 // (the first keeps the pairs aligned; only the second is read) and one south halo row: 64 x 16
 // nodes, one staged row per warp.  With I even a pair is deep in both nodes or in neither.
-constexpr int kPairTX = 62, kPairTY = 15;
+constexpr int kPairTX = 62, kPairTY = 15;   // (the 8-row form's tiles are 62 x 7)
 
 template <typename R>
 struct Vec2;
@@ -530,19 +530,23 @@ __device__ __forceinline__ void prd_mom_pair(const PredArgs<R> &a, long x, bool 
     }
 }
 
-__host__ __device__ __forceinline__ bool prd_inner_pair_tile(int i0, int j0, int I, int J) {
-    // every staged node (columns i0-2 .. i0+61, rows j0-1 .. j0+14) deep
-    return i0 >= 4 && j0 >= 3 && i0 + kPairTX + 2 <= I && j0 + kPairTY + 2 <= J;
+__host__ __device__ __forceinline__ bool prd_inner_pair_tile(int i0, int j0, int I, int J,
+                                                             int ty_own = kPairTY) {
+    // every staged node (columns i0-2 .. i0+61, rows j0-1 .. j0+ty_own-1) deep
+    return i0 >= 4 && j0 >= 3 && i0 + kPairTX + 2 <= I && j0 + ty_own + 2 <= J;
 }
 
 // The kept inputs stay in registers across the block's barrier (64 registers, two blocks per
 // SM): a form that read them again after the barrier (40 registers, three blocks per SM) took
 // the basin4 loop to 4.72 ms against 4.30.
-template <typename R>
-__global__ void __launch_bounds__(512, 2) k_pred2d_pair(const __grid_constant__ PredArgs<R> a,
-                                                       int ring_blocks, int tiles_x, int edge_blocks) {
+// ROWS staged rows per block (one per warp): 16 (tiles 62 x 15, two blocks per SM) or 8 (62 x 7,
+// four blocks per SM).
+template <typename R, int ROWS>
+__global__ void __launch_bounds__(32 * ROWS, ROWS == 16 ? 2 : 4) k_pred2d_pair(
+        const __grid_constant__ PredArgs<R> a, int ring_blocks, int tiles_x, int edge_blocks) {
     pdl_enter();
-    __shared__ R sZ[kPairTY + 1][kPairTX + 2];   // zeta_t2 after zetabc, (j0-1.., i0-2..)
+    constexpr int TY = ROWS - 1;
+    __shared__ R sZ[ROWS][kPairTX + 2];   // zeta_t2 after zetabc, (j0-1.., i0-2..)
     __shared__ R sDummy[kPredTY + 1][kPredTX + 1];
     const Geo<R> &g = a.g;
     const int I = g.I, J = g.J;
@@ -551,12 +555,12 @@ __global__ void __launch_bounds__(512, 2) k_pred2d_pair(const __grid_constant__ 
     const int bid = (int)blockIdx.x;
     if (bid == 0) prd_chained_head(a, tid, sDummy);
     if (bid < ring_blocks) {
-        const int e = bid * 512 + tid;
+        const int e = bid * (32 * ROWS) + tid;
         if (e < 4 * I + 4 * (J - 4))
             prd_edge_node(a, PrdTile<R>{sDummy, -kPredTX - 2, -kPredTY - 2}, prd_ring_node(e, I, J));
     } else {
         const int tb = bid - ring_blocks;
-        const int i0 = (tb % tiles_x) * kPairTX, j0 = (tb / tiles_x) * kPairTY;
+        const int i0 = (tb % tiles_x) * kPairTX, j0 = (tb / tiles_x) * TY;
         const int i = i0 - 2 + 2 * tx;   // the pair (i, i+1) of staged columns 2 tx, 2 tx + 1
         const int r = ty;                // staged row (0: the south halo)
         const int j = j0 - 1 + r;
@@ -588,7 +592,7 @@ __global__ void __launch_bounds__(512, 2) k_pred2d_pair(const __grid_constant__ 
             prd_mom_pair(a, x, pda, pdb, sZ[r][2 * tx], sZ[r][2 * tx + 1], sZ[r][2 * tx - 1],
                          sZ[r - 1][2 * tx], sZ[r - 1][2 * tx + 1], kept);
         }
-        if (prd_inner_pair_tile(i0, j0, I, J)) return;   // uniform over the block
+        if (prd_inner_pair_tile(i0, j0, I, J, TY)) return;   // uniform over the block
     }
     prd_chained_tail(a, tid, edge_blocks);
 }
@@ -631,16 +635,21 @@ cudaError_t Ops<R>::pred2d(const sf_ctx *c, R *z0, R *z1, R *z2, R *ub1, R *vb1,
         for (const void *q : ptrs) pair = pair && (reinterpret_cast<uintptr_t>(q) % (2 * sizeof(R))) == 0;
     }
     if (pair) {
-        const int tiles_x = (c->I + kPairTX - 1) / kPairTX, tiles_y = (c->J + kPairTY - 1) / kPairTY;
-        const int ring_blocks = (4 * c->I + 4 * (c->J - 4) + 511) / 512;
+        const int rows = c->pred_pair == 2 ? 8 : 16, TY = rows - 1, nt = 32 * rows;
+        const int tiles_x = (c->I + kPairTX - 1) / kPairTX, tiles_y = (c->J + TY - 1) / TY;
+        const int ring_blocks = (4 * c->I + 4 * (c->J - 4) + nt - 1) / nt;
         int inner_x = 0, inner_y = 0;
         for (int tx = 0; tx < tiles_x; ++tx)
-            inner_x += prd_inner_pair_tile(tx * kPairTX, 3, c->I, 3 + kPairTY + 2);
+            inner_x += prd_inner_pair_tile(tx * kPairTX, 3, c->I, 3 + TY + 2, TY);
         for (int ty = 0; ty < tiles_y; ++ty)
-            inner_y += prd_inner_pair_tile(4, ty * kPairTY, 4 + kPairTX + 2, c->J);
+            inner_y += prd_inner_pair_tile(4, ty * TY, 4 + kPairTX + 2, c->J, TY);
         const int edge_blocks = ring_blocks + tiles_x * tiles_y - inner_x * inner_y;
-        return launch_dep(c, k_pred2d_pair<R>, dim3((unsigned)(ring_blocks + tiles_x * tiles_y)),
-                          dim3(32, 16), 0, s, a, ring_blocks, tiles_x, edge_blocks);
+        const dim3 grid((unsigned)(ring_blocks + tiles_x * tiles_y));
+        if (rows == 8)
+            return launch_dep(c, k_pred2d_pair<R, 8>, grid, dim3(32, 8), 0, s, a, ring_blocks,
+                              tiles_x, edge_blocks);
+        return launch_dep(c, k_pred2d_pair<R, 16>, grid, dim3(32, 16), 0, s, a, ring_blocks,
+                          tiles_x, edge_blocks);
     }
     const int tiles_x = (c->I + kPredTX - 1) / kPredTX, tiles_y = (c->J + kPredTY - 1) / kPredTY;
     const int ring_blocks = (4 * c->I + 4 * (c->J - 4) + 255) / 256;
