@@ -451,14 +451,46 @@ def error_vs_fp64():
     return out
 
 
-def roms_day(args, hours=24.0, tau0=0.15, rdrag2=3e-3, runs_of=(("fp32", "mlp"), ("fp64", "gls"))):
+ROMS_STATE = ("zeta", "ubar", "vbar", "rzeta", "rubar", "rvbar", "Zt_avg1", "DU_avg1", "DV_avg1",
+              "DU_avg2", "DV_avg2", "u", "v", "AKv", "W", "Huon", "Hvom")
+GLS_STATE = ("tke", "gls", "Akt", "Akk", "Akp", "Lscale")
+
+
+def _snapshot(m, c):
+    """A ROMS-form model's state and its mixing's GLS state, as FP64 copies."""
+    snap = {n: getattr(m, n).double().clone() for n in ROMS_STATE}
+    snap["ru3"] = [t.double().clone() for t in m._ru3]
+    snap["rv3"] = [t.double().clone() for t in m._rv3]
+    snap.update({"gls_" + n: getattr(c.cols, n).double().clone() for n in GLS_STATE})
+    snap["slots"] = list(m.slots)
+    snap["counters"] = (m.iic, m.time, m.time2D)
+    return snap
+
+
+def _restore(m, c, snap):
+    """Start model m (any precision) and its mixing c from a snapshot of another run."""
+    for n in ROMS_STATE:
+        getattr(m, n).copy_(snap[n])
+    for dst, srcs in ((m._ru3, snap["ru3"]), (m._rv3, snap["rv3"])):
+        for t, s in zip(dst, srcs):
+            t.copy_(s)
+    for n in GLS_STATE:
+        getattr(c.cols, n).copy_(snap["gls_" + n])
+    m.slots = list(snap["slots"])
+    m.iic, m.time, m.time2D = snap["counters"]
+
+
+def roms_day(args, hours=24.0, tau0=0.15, rdrag2=3e-3, runs_of=(("fp32", "mlp"), ("fp64", "gls")),
+             spinup_hours=0.0):
     """The configuration's physics for `hours` simulated in the ROMS-form step (wind
     tau_x = tau0 cos(pi y/Ly) N/m2, quadratic bottom drag rdrag2, Coriolis, T = 4 + 20 exp(z/500)
     for the mixing, from rest), run twice from identical initial states as `runs_of` says
     ((precision, mixing) pairs: by default the FP32 form with the learned closure against FP64
     with plain GLS every step).  Returns the RMS / max differences of the free surface
     (Zt_avg1, the surface the 3D step uses), ubar, u and v over the interior at the end, with
-    the RMS of the second run's fields, and each run's device time per step."""
+    the RMS of the second run's fields, and each run's device time per step.  With
+    spinup_hours > 0 every run starts instead from the state (flow, averages, right-hand-side
+    history, GLS turbulence) of an FP64 + plain-GLS run of that many hours from rest."""
     import torch
     from sailfish_b200 import configs
     from sailfish_b200.model import Model
@@ -467,21 +499,33 @@ def roms_day(args, hours=24.0, tau0=0.15, rdrag2=3e-3, runs_of=(("fp32", "mlp"),
     nsteps = int(round(hours * 3600.0 / cfg["dt"]))
     # the ROMS-form barotropic step is stable for c dtfast / dx < 0.757 (von Neumann, 2D); a
     # configuration beyond it (basin1: 0.80 at h = 4000 m) runs with more substeps
-    ndtfast = cfg["ndtfast"]
-    courant = float(np.sqrt(10.0 * g.h.max()) * cfg["dt"] / ndtfast * max(g.pm.max(), g.pn.max()))
-    if courant > 0.7:
-        ndtfast = int(np.ceil(ndtfast * courant / 0.65))
+    ndtfast, courant = configs.roms_ndtfast(cfg)
     stream = torch.cuda.current_stream()
     runs, times = {}, {}
     keys = []
-    for prec, mode in runs_of:
-        key = "%s_%s" % (prec, mode)
-        keys.append(key)
+
+    def make(prec, mode):
         m = Model(g, cfg["boundary"], cfg["dt"], ndtfast, precision=prec, semantics="roms")
         c = install_mixing(m, mode, args.config)
         m.set_forcing(c.cols.sustr.double().cpu().numpy(), c.cols.svstr.double().cpu().numpy(),
                       rdrag2)
         m.check_every = 60
+        return m, c
+
+    snap = None
+    if spinup_hours > 0:
+        m, c = make("fp64", "gls")
+        m.step(int(round(spinup_hours * 3600.0 / cfg["dt"])))
+        torch.cuda.synchronize()
+        snap = _snapshot(m, c)
+        del m, c
+        torch.cuda.empty_cache()
+    for prec, mode in runs_of:
+        key = "%s_%s" % (prec, mode)
+        keys.append(key)
+        m, c = make(prec, mode)
+        if snap is not None:
+            _restore(m, c, snap)
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(stream)
         m.step(nsteps)
@@ -494,9 +538,12 @@ def roms_day(args, hours=24.0, tau0=0.15, rdrag2=3e-3, runs_of=(("fp32", "mlp"),
         del m, c
         torch.cuda.empty_cache()
     J, I, N = g.J, g.I, g.N
-    out = {"case": "%s, ROMS-form step, %d steps of %g s (%g h) from rest, wind %g cos(pi y/Ly) "
+    start = ("from rest" if spinup_hours <= 0 else
+             "after %g h of FP64 + plain GLS from rest" % spinup_hours)
+    out = {"case": "%s, ROMS-form step, %d steps of %g s (%g h) %s, wind %g cos(pi y/Ly) "
                    "N/m2, quadratic drag %g; %s against %s" % (
-                       args.config, nsteps, cfg["dt"], hours, tau0, rdrag2, keys[0], keys[1]),
+                       args.config, nsteps, cfg["dt"], hours, start, tau0, rdrag2, keys[0],
+                       keys[1]),
            "units": {"zeta": "m", "ubar": "m/s", "u": "m/s", "v": "m/s"},
            "ndtfast": ndtfast, "barotropic_courant_of_config": courant,
            "ms_per_step": times, "fallback_columns": runs[keys[0]]["fallback_columns"]}
@@ -983,18 +1030,18 @@ def main():
             48.0 if args.config == "basin1" else 24.0)
         if hours > 0 and args.config in ("basin4", "basin4q", "basin1"):
             try:
-                out["day_error_vs_fp64"] = roms_day(
-                    args, hours=hours, runs_of=(("fp32", "mlp"), ("fp64", "gls"), ("fp32", "gls")))
+                out["day_error_vs_fp64"] = roms_day(args, hours=hours)
             except Exception as e:   # a blow-up check that fired, for instance
                 out["day_error_vs_fp64"] = {"failed": str(e)}
                 torch.cuda.empty_cache()
-        if hours > 0 and args.config == "basin1" and args.closure != "none":
-            # the learned closure's effect on the flow: the same FP32 step with plain GLS
+            # the same day after a day of spin-up (GLS turbulence developed), with the
+            # difference split into precision and closure through a third run
             try:
-                out["closure_uv_error_vs_gls"] = roms_day(
-                    args, hours=hours, runs_of=(("fp32", "mlp"), ("fp32", "gls")))
+                out["spun_up_day_error_vs_fp64"] = roms_day(
+                    args, hours=hours, spinup_hours=hours,
+                    runs_of=(("fp32", "mlp"), ("fp64", "gls"), ("fp32", "gls")))
             except Exception as e:
-                out["closure_uv_error_vs_gls"] = {"failed": str(e)}
+                out["spun_up_day_error_vs_fp64"] = {"failed": str(e)}
                 torch.cuda.empty_cache()
         if not args.no_cpu_baseline:
             out["cpu_baseline"] = cpu_sample(args)

@@ -267,6 +267,55 @@ def generate(config="basin1", runs=4, spin=30, keep=4, every=5, seed=0, precisio
     return X, T
 
 
+def generate_roms(config="basin1", runs=6, hours=48.0, spin_hours=4.0, every=10, seed=0,
+                  precision="fp32", tau_range=(0.0, 0.3), zscale_range=(200.0, 1000.0),
+                  gls_model="k-epsilon", rdrag2=3e-3):
+    """Training snapshots along ROMS-form model runs with plain GLS (the dynamics the closure
+    replaces, including its transients): each run draws a peak wind stress from tau_range
+    (zonal, cos(pi y / Ly) across the basin, either sign) and a stratification scale from
+    zscale_range, starts from rest, and after `spin_hours` keeps a snapshot of the GLS
+    columns (features, log10 Akv / Akt) every `every` steps until `hours`.  Returns (X, T) on
+    the device for the rho-interior columns."""
+    cfg = configs.CONFIGS[config]() if isinstance(config, str) else config
+    g = cfg["grid"]
+    if nfeat(g.N) > WIDTH:
+        raise ValueError("the closure's rows hold at most 62 interior W levels")
+    nd, _ = configs.roms_ndtfast(cfg)
+    nsteps = int(round(hours * 3600.0 / cfg["dt"]))
+    spin = int(round(spin_hours * 3600.0 / cfg["dt"]))
+    keep = len(range(spin, nsteps, every))
+    rng = np.random.default_rng(seed)
+    X = T = None
+    row = 0
+    for r in range(runs):
+        tau = float(rng.uniform(*tau_range)) * (1.0 if rng.random() < 0.5 else -1.0)
+        zscale = float(rng.uniform(*zscale_range))
+        m = Model(g, cfg["boundary"], cfg["dt"], nd, precision=precision, semantics="roms")
+        c = mixing_for(m, "gls", None, tau0=tau, zscale=zscale, gls_model=gls_model)
+        m.set_forcing(c.cols.sustr.double().cpu().numpy(), c.cols.svstr.double().cpu().numpy(),
+                      rdrag2)
+        dev = m.u.device
+        if X is None:
+            cols_idx = interior_columns(g, dev)
+            nc = int(cols_idx.numel())
+            X = torch.empty((runs * keep * nc, WIDTH), device=dev)
+            T = torch.empty((runs * keep * nc, WIDTH), device=dev)
+            Xbuf = torch.zeros((g.s2, WIDTH), device=dev)
+        for k in range(nsteps):
+            m.step(1)
+            if k >= spin and (k - spin) % every == 0:
+                c.cols.features(Xbuf)
+                X[row:row + nc] = Xbuf[cols_idx]
+                T[row:row + nc] = targets(m.AKv, c.cols.Akt, g.N)[cols_idx]
+                row += nc
+        del m, c
+        torch.cuda.empty_cache()
+    torch.cuda.synchronize()
+    # a run that left the scheme's stability range leaves non-finite rows: drop them
+    ok = torch.isfinite(X[:row]).all(1) & torch.isfinite(T[:row]).all(1)
+    return X[:row][ok], T[:row][ok]
+
+
 def targets(Akv, Akt, N):
     """Target rows (s2 x 128): log10 Akv at W levels 1..N-1 in [0, N-1), log10 Akt in
     [N-1, 2N-2)."""

@@ -90,3 +90,16 @@ def small(Lm=256, Mm=128, N=32):
 
 
 CONFIGS = {"basin0": basin0, "basin1": basin1, "basin4": basin4, "basin4q": basin4q, "small": small}
+
+
+def roms_ndtfast(cfg, limit=0.65):
+    """Barotropic substeps per baroclinic step for the ROMS-form step on `cfg`: its own
+    ndtfast, raised where the fastest gravity wave (sqrt(g h_max)) would exceed c dtfast / dx
+    = `limit` (the scheme is stable below 0.757 on a square grid: von Neumann analysis of the
+    substep).  Returns (ndtfast, the configuration's own Courant number)."""
+    g = cfg["grid"]
+    nd = int(cfg["ndtfast"])
+    courant = float(np.sqrt(10.0 * g.h.max()) * cfg["dt"] / nd * max(g.pm.max(), g.pn.max()))
+    if courant > 0.7:
+        nd = int(np.ceil(nd * courant / limit))
+    return nd, courant

@@ -834,9 +834,43 @@ __device__ __forceinline__ void rhs3d_body(const Geo<R> &g, const R *__restrict_
             sF[2 * kFN + e] = vfx;
             sF[3 * kFN + e] = vfe;
         };
-        face_flux(ty, tx);
-        if (ty == 0) face_flux(-1, tx);
-        else if (ty == 1 && tx < TY) face_flux(tx, -1);
+        // two vertically adjacent cells per thread where the tile allows it: their loads are
+        // evaluated together (the second cell's stencil is the first's one row up, so the
+        // shared staged values are loaded once), then the eight stores
+        auto face_flux_pair = [&](int r, int c) {
+            const int e = (r + 1) * kFX + (c + 1);
+            const int bb = (r + kHY0) * kSX + (c + kHX0);
+            const Tile<R, kSX> U{bf[0], bb}, V{bf[1], bb}, HU{bf[2], bb}, HV{bf[3], bb};
+            const R uxx = UXXR(0, 0), uee = UEEP(0, 0);
+            const R ufx = UR(0, 0) + (G * uxx) * (HUR(0, 0) + G * HUXXR(0, 0));
+            const R ufe = UP(0, 0) + (G * uee) * (HVP(0, 0) + G * HVXXP(0, 0));
+            const R vfx = VP(0, 0) + (G * uee) * (HUP(0, 0) + G * HUEEP(0, 0));
+            const R vfe = VR(0, 0) + (G * uxx) * (HVR(0, 0) + G * HVEER(0, 0));
+            const R uxx1 = UXXR(1, 0), uee1 = UEEP(1, 0);
+            const R ufx1 = UR(1, 0) + (G * uxx1) * (HUR(1, 0) + G * HUXXR(1, 0));
+            const R ufe1 = UP(1, 0) + (G * uee1) * (HVP(1, 0) + G * HVXXP(1, 0));
+            const R vfx1 = VP(1, 0) + (G * uee1) * (HUP(1, 0) + G * HUEEP(1, 0));
+            const R vfe1 = VR(1, 0) + (G * uxx1) * (HVR(1, 0) + G * HVEER(1, 0));
+            sF[0 * kFN + e] = ufx;
+            sF[1 * kFN + e] = ufe;
+            sF[2 * kFN + e] = vfx;
+            sF[3 * kFN + e] = vfe;
+            sF[0 * kFN + e + kFX] = ufx1;
+            sF[1 * kFN + e + kFX] = ufe1;
+            sF[2 * kFN + e + kFX] = vfx1;
+            sF[3 * kFN + e + kFX] = vfe1;
+        };
+        if constexpr (TY % 2 == 0 && TY >= 4) {
+            // warps 0 .. TY/2-1: rows 2 ty - 1 and 2 ty; warp TY/2: row TY-1; warp TY/2+1:
+            // the west halo column (rows 0 .. TY-1; the corner cell is nobody's neighbour)
+            if (ty < TY / 2) face_flux_pair(2 * ty - 1, tx);
+            else if (ty == TY / 2) face_flux(TY - 1, tx);
+            else if (ty == TY / 2 + 1 && tx < TY) face_flux(tx, -1);
+        } else {
+            face_flux(ty, tx);
+            if (ty == 0) face_flux(-1, tx);
+            else if (ty == 1 && tx < TY) face_flux(tx, -1);
+        }
         __syncthreads();
         if (live) {
         {   // phase 2: this cell's divergence

@@ -251,3 +251,21 @@ def test_fused_closure_step_matches_the_composition(precision):
     # identical features and BF16 operands; the tile epilogues round the same way
     torch.testing.assert_close(af, au, rtol=1e-3, atol=0)
     torch.testing.assert_close(tf, tu, rtol=1e-3, atol=0)
+
+
+@pytest.mark.gpu
+def test_training_snapshots_from_roms_form_runs():
+    """closure.generate_roms: snapshots along ROMS-form runs from rest with plain GLS, one per
+    `every` steps after the spin-up, every row finite, targets log10 Akv/Akt inside the clip
+    range [-6, -1] and varying (the turbulence develops along the run)."""
+    from sailfish_b200 import closure, configs
+    cfg = configs.basin(48, 32, 8, 2.0e3, [(0.5, 0.6)], dt=240.0, ndtfast=30)
+    X, T = closure.generate_roms(cfg, runs=2, hours=4.0, spin_hours=2.0, every=10, seed=3,
+                                 gls_model="k-psi")
+    N = cfg["grid"].N
+    nc = 48 * 32
+    assert X.shape[0] == 2 * 3 * nc and T.shape == X.shape          # snapshots at 30, 40, 50
+    assert bool(torch.isfinite(X).all()) and bool(torch.isfinite(T).all())
+    t = T[:, :2 * (N - 1)]
+    assert float(t.min()) >= -6.0 - 1e-6 and float(t.max()) <= -1.0 + 1e-6
+    assert float(t[:, :N - 1].std()) > 0.05
