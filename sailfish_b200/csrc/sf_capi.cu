@@ -877,7 +877,7 @@ int sf_ctx_tune(sf_ctx *c, int knob, int value) {
         c->mo_chunk = value;
         return SF_OK;
     case SF_TUNE_PRED_PAIR:
-        if (value < 0 || value > 3) return fail(SF_EINVAL, "pair is 0 to 3");
+        if (value < 0 || value > 2) return fail(SF_EINVAL, "pair is 0, 1 or 2");
         if (c->pred_pair != value)
             for (auto &g : c->graphs) {   // captured loops hold the other kernel
                 if (g.exec) cudaGraphExecDestroy(g.exec);

@@ -597,264 +597,6 @@ __global__ void __launch_bounds__(32 * ROWS, ROWS == 16 ? 2 : 4) k_pred2d_pair(
     prd_chained_tail(a, tid, edge_blocks);
 }
 
-// ---- the staged persistent form ------------------------------------------------------------
-// The paired form's arithmetic with its deep pairs' inputs taken from shared memory: each tile
-// block of the grid (a few per SM) walks its tiles in turn and, while it computes one tile,
-// copies the next one's nine input fields (zeta_t0, zeta_t1, ubar_t1, vbar_t1, h, pm, pn, on_u,
-// om_v) into the other of two shared buffers with cp.async, so the loads of one tile overlap the
-// arithmetic of the previous.  A buffer holds rows j0-2 .. j0+7 and columns i0-4 .. i0+63 of a
-// 62 x 7 tile (8 staged rows, one per warp, as the 8-row paired form): every deep pair's
-// stencil, copied as aligned element pairs (I even).  Nodes off the deep region use the pure
-// functions on the fields in memory, as before; so do the ring blocks, and edge tiles count
-// themselves after their reads, the last one writing the chained destinations.  Each node's
-// arithmetic is the paired form's, operation for operation.
-constexpr int kStgRows = 8, kStgTY = kStgRows - 1;
-constexpr int kStgSR = kStgRows + 2, kStgSC = kPairTX + 6;   // 10 x 68 staged nodes per field
-constexpr int kStgF = kStgSR * kStgSC;                       // elements per field
-constexpr int kStgThreads = 32 * kStgRows;
-
-template <typename R>
-__host__ __device__ constexpr size_t stg_smem_bytes() {
-    // two buffers of nine fields, then the tile's zeta_t2
-    return sizeof(R) * (2 * 9 * (size_t)kStgF + (size_t)kStgRows * (kPairTX + 2));
-}
-
-// This thread's share of a tile's copies: element pairs e = tid and tid + 256 of the
-// kStgSR x (kStgSC / 2) pairs of a field, the same for every field.
-struct StgMap {
-    int soff[2];    // offset in a field's buffer
-    int row[2], col[2];
-    bool act[2];
-};
-__device__ __forceinline__ StgMap stg_map(int tid) {
-    StgMap m;
-    constexpr int kPairsRow = kStgSC / 2, kPairs = kStgSR * kPairsRow;
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-        const int e = tid + h * kStgThreads;
-        m.act[h] = e < kPairs;
-        const int r = e / kPairsRow, c2 = e - r * kPairsRow;
-        m.row[h] = r;
-        m.col[h] = 2 * c2;
-        m.soff[h] = r * kStgSC + 2 * c2;
-    }
-    return m;
-}
-
-template <typename R>
-__device__ __forceinline__ void stg_issue(const PredArgs<R> &a, const StgMap &mp, R *buf, int i0,
-                                          int j0) {
-    const Geo<R> &g = a.g;
-    const int I = g.I, J = g.J;
-    long x[2];
-    bool ok[2];
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-        const int jj = j0 - 2 + mp.row[h], ii = i0 - 4 + mp.col[h];
-        ok[h] = mp.act[h] && jj >= 0 && jj < J && ii >= 0 && ii < I;   // I even: ii + 1 < I too
-        x[h] = ok[h] ? (long)jj * I + ii : 0;
-    }
-    const R *src[9] = {a.z0, a.z1, a.ub1, a.vb1, g.h, g.pm, g.pn, g.on_u, g.om_v};
-#pragma unroll
-    for (int f = 0; f < 9; ++f)
-#pragma unroll
-        for (int h = 0; h < 2; ++h)
-            if (mp.act[h]) cp_async2(buf + f * kStgF + mp.soff[h], src[f] + x[h], ok[h]);
-}
-
-// a deep pair's inputs from the staged buffer: field f at (row r + dr, column c + dc)
-template <typename R>
-struct StgView {
-    const R *b;
-    int base;   // the pair's first node
-    __device__ __forceinline__ R v(int f, int dr, int dc) const { return b[f * kStgF + base + dr * kStgSC + dc]; }
-    __device__ __forceinline__ void v2(int f, int dr, int dc, R &x, R &y) const {
-        ld2(b + f * kStgF + base + dr * kStgSC + dc, x, y);
-    }
-};
-enum { kSZ0 = 0, kSZ1, kSUB, kSVB, kSH, kSPM, kSPN, kSOU, kSOV };
-
-// prd_rz_pair with the inputs from the staged buffer
-template <typename R>
-__device__ __forceinline__ void stg_rz_pair(const PredArgs<R> &a, const StgView<R> &s,
-                                            PrdPair<R> &n, R &rza, R &rzb) {
-    s.v2(kSZ1, 0, 0, n.z1a, n.z1b);
-    n.z1w = s.v(kSZ1, 0, -1);
-    const R z1e = s.v(kSZ1, 0, 2);
-    s.v2(kSZ1, -1, 0, n.z1sa, n.z1sb);
-    R zna, znb;
-    s.v2(kSZ1, 1, 0, zna, znb);
-    s.v2(kSH, 0, 0, n.ha, n.hb);
-    n.hw = s.v(kSH, 0, -1);
-    const R he = s.v(kSH, 0, 2);
-    s.v2(kSH, -1, 0, n.hsa, n.hsb);
-    R hna, hnb;
-    s.v2(kSH, 1, 0, hna, hnb);
-    s.v2(kSUB, 0, 0, n.uba, n.ubb);
-    const R ube = s.v(kSUB, 0, 2);
-    s.v2(kSVB, 0, 0, n.vba, n.vbb);
-    R vna, vnb;
-    s.v2(kSVB, 1, 0, vna, vnb);
-    s.v2(kSOU, 0, 0, n.oua, n.oub);
-    const R oue = s.v(kSOU, 0, 2);
-    s.v2(kSOV, 0, 0, n.ova, n.ovb);
-    R ovna, ovnb;
-    s.v2(kSOV, 1, 0, ovna, ovnb);
-    s.v2(kSPM, 0, 0, n.pma, n.pmb);
-    s.v2(kSPN, 0, 0, n.pna, n.pnb);
-    s.v2(kSZ0, 0, 0, n.z0a, n.z0b);
-    // node a
-    const R Dpa = n.z1a + n.ha, Dwa = n.z1w + n.hw, Dpb = n.z1b + n.hb;
-    const R Dsa = n.z1sa + n.hsa, Dna = zna + hna;
-    const R DUpa = n.uba * ((Dpa + Dwa) * R(0.5));
-    const R DUpb = n.ubb * ((Dpb + Dpa) * R(0.5));   // node a's east flux, node b's west
-    const R DVpa = n.vba * ((Dpa + Dsa) * R(0.5));
-    const R DVna = vna * ((Dna + Dpa) * R(0.5));
-    rza = (((DUpb * n.oub - DUpa * n.oua) + (DVna * ovna - DVpa * n.ova)) * n.pma) * n.pna;
-    // node b
-    const R Deb = z1e + he, Dsb = n.z1sb + n.hsb, Dnb = znb + hnb;
-    const R DUeb = ube * ((Deb + Dpb) * R(0.5));
-    const R DVpb = n.vbb * ((Dpb + Dsb) * R(0.5));
-    const R DVnb = vnb * ((Dnb + Dpb) * R(0.5));
-    rzb = (((DUeb * oue - DUpb * n.oub) + (DVnb * ovnb - DVpb * n.ovb)) * n.pmb) * n.pnb;
-}
-
-// prd_mom_pair with zeta_t0's west and south neighbours from the staged buffer
-template <typename R>
-__device__ __forceinline__ void stg_mom_pair(const PredArgs<R> &a, const StgView<R> &s, long x,
-                                             bool pda, bool pdb, R za, R zb, R zw, R zsa, R zsb,
-                                             const PrdPair<R> &n) {
-    R z0sa, z0sb;
-    s.v2(kSZ0, -1, 0, z0sa, z0sb);
-    const R z0w = s.v(kSZ0, 0, -1);
-    const R gpa = a.w1 * za + a.w * n.z0a;
-    const R gw = a.w1 * zw + a.w * z0w;
-    const R gsa = a.w1 * zsa + a.w * z0sa;
-    const R gpb = a.w1 * zb + a.w * n.z0b;
-    const R gsb = a.w1 * zsb + a.w * z0sb;
-    const R rua = (a.grav * n.oua) * (((n.ha + n.hw) * R(0.5)) * (gpa - gw) + R(0.5) * (gpa * gpa - gw * gw));
-    const R rva = (a.grav * n.ova) * (((n.ha + n.hsa) * R(0.5)) * (gpa - gsa) + R(0.5) * (gpa * gpa - gsa * gsa));
-    const R rub = (a.grav * n.oub) * (((n.hb + n.ha) * R(0.5)) * (gpb - gpa) + R(0.5) * (gpb * gpb - gpa * gpa));
-    const R rvb = (a.grav * n.ovb) * (((n.hb + n.hsb) * R(0.5)) * (gpb - gsb) + R(0.5) * (gpb * gpb - gsb * gsb));
-    st2(a.ru + x, rua, rub);
-    st2(a.rv + x, rva, rvb);
-    if (!pda && !pdb) return;
-    const R D1pa = n.z1a + n.ha, D2pa = za + n.ha, D1pb = n.z1b + n.hb, D2pb = zb + n.hb;
-    const R ua = ddiv(n.uba * ((D1pa + (n.z1w + n.hw)) * R(0.5)) + ((a.Dt * rua) * n.pma) * n.pna,
-                      (D2pa + (zw + n.hw)) * R(0.5));
-    const R va = ddiv(n.vba * ((D1pa + (n.z1sa + n.hsa)) * R(0.5)) + ((a.Dt * rva) * n.pma) * n.pna,
-                      (D2pa + (zsa + n.hsa)) * R(0.5));
-    const R ub = ddiv(n.ubb * ((D1pb + D1pa) * R(0.5)) + ((a.Dt * rub) * n.pmb) * n.pnb,
-                      (D2pb + D2pa) * R(0.5));
-    const R vb = ddiv(n.vbb * ((D1pb + (n.z1sb + n.hsb)) * R(0.5)) + ((a.Dt * rvb) * n.pmb) * n.pnb,
-                      (D2pb + (zsb + n.hsb)) * R(0.5));
-    if (pda && pdb) {
-        st2(a.ub2 + x, ua, ub);
-        st2(a.vb2 + x, va, vb);
-    } else if (pda) {
-        a.ub2[x] = ua;
-        a.vb2[x] = va;
-    } else {
-        a.ub2[x + 1] = ub;
-        a.vb2[x + 1] = vb;
-    }
-}
-
-template <typename R>
-__global__ void __launch_bounds__(kStgThreads, 4) k_pred2d_stg(const __grid_constant__ PredArgs<R> a,
-                                                              int ring_blocks, int tiles_x,
-                                                              int ntiles, int edge_blocks) {
-    pdl_enter();
-    extern __shared__ __align__(16) unsigned char stg_smem[];
-    R *bufs = reinterpret_cast<R *>(stg_smem);
-    R(*sZ)[kPairTX + 2] = reinterpret_cast<R(*)[kPairTX + 2]>(bufs + 2 * 9 * kStgF);
-    __shared__ R sDummy[kPredTY + 1][kPredTX + 1];
-    __shared__ int s_last;
-    const Geo<R> &g = a.g;
-    const int I = g.I, J = g.J;
-    const int tx = threadIdx.x, ty = threadIdx.y;
-    const int tid = ty * 32 + tx;
-    const int bid = (int)blockIdx.x;
-    if (bid == 0) prd_chained_head(a, tid, sDummy);
-    if (bid < ring_blocks) {
-        const int e = bid * kStgThreads + tid;
-        if (e < 4 * I + 4 * (J - 4))
-            prd_edge_node(a, PrdTile<R>{sDummy, -kPredTX - 2, -kPredTY - 2}, prd_ring_node(e, I, J));
-        prd_chained_tail(a, tid, edge_blocks);
-        return;
-    }
-    const int P = (int)gridDim.x - ring_blocks;
-    const StgMap mp = stg_map(tid);
-    int t = bid - ring_blocks, b = 0;
-    if (t < ntiles) stg_issue(a, mp, bufs, (t % tiles_x) * kPairTX, (t / tiles_x) * kStgTY);
-    cp_async_commit();
-    for (; t < ntiles; t += P, b ^= 1) {
-        const int tn = t + P;
-        if (tn < ntiles)
-            stg_issue(a, mp, bufs + (b ^ 1) * 9 * kStgF, (tn % tiles_x) * kPairTX, (tn / tiles_x) * kStgTY);
-        cp_async_commit();
-        cp_async_wait<1>();   // this tile's copies (the next tile's may still be in flight)
-        __syncthreads();
-        const int i0 = (t % tiles_x) * kPairTX, j0 = (t / tiles_x) * kStgTY;
-        const int i = i0 - 2 + 2 * tx, r = ty, j = j0 - 1 + r;
-        const bool live = i >= 0 && j >= 0 && i < I && j < J;
-        const bool deep = live && prd_deep(i, j, I, J);
-        const long x = (long)j * I + i;
-        const StgView<R> sv{bufs + b * 9 * kStgF, (r + 1) * kStgSC + 2 * tx + 2};
-        PrdPair<R> kept;
-        if (deep) {
-            R rza, rzb;
-            stg_rz_pair(a, sv, kept, rza, rzb);
-            const R za = kept.z0a + a.Dt * rza, zb = kept.z0b + a.Dt * rzb;
-            if (tx >= 1 && r >= 1) {
-                st2(a.rz + x, rza, rzb);
-                st2(a.z2 + x, za, zb);
-            }
-            sZ[r][2 * tx] = za;
-            sZ[r][2 * tx + 1] = zb;
-        } else if (live) {
-            sZ[r][2 * tx] = prd_z2b(a, x);
-            sZ[r][2 * tx + 1] = prd_z2b(a, x + 1);
-        }
-        __syncthreads();
-        if (deep && tx >= 1 && r >= 1) {
-            const int qa = j * I + i, qb = qa + 1;
-            const bool pda = qa - fdiv(qa, g.dJ) * J != 0 && qa >= J;   // q % J != 0 (szJ)
-            const bool pdb = qb - fdiv(qb, g.dJ) * J != 0 && qb >= J;
-            stg_mom_pair(a, sv, x, pda, pdb, sZ[r][2 * tx], sZ[r][2 * tx + 1], sZ[r][2 * tx - 1],
-                         sZ[r - 1][2 * tx], sZ[r - 1][2 * tx + 1], kept);
-        }
-        // an edge tile counts itself once its reads are done; the last one of all the edge
-        // blocks and tiles writes the chained destinations
-        const bool edge = !prd_inner_pair_tile(i0, j0, I, J, kStgTY);
-        __syncthreads();
-        if (edge) {
-            if (tid == 0) s_last = atomicAdd(a.counter, 1) == edge_blocks - 1;
-            __syncthreads();
-            if (s_last) {
-                __threadfence();
-                const BcProgram *ps[3] = {&a.pz, &a.pu, &a.pv};
-                R v[3] = {R(0), R(0), R(0)};
-                int d[3] = {-1, -1, -1};
-#pragma unroll
-                for (int f = 0; f < 3; ++f) {
-                    const BcProgram &pp = *ps[f];
-                    if (tid < pp.nch) {
-                        d[f] = pp.dst_ch[tid];
-                        v[f] = __ldcg(a.chv + f * kMaxChained + tid);
-                    }
-                }
-                if (d[0] >= 0) a.z2[d[0]] = v[0];
-                if (d[1] >= 0) a.ub2[d[1]] = v[1];
-                if (d[2] >= 0) a.vb2[d[2]] = v[2];
-                if (tid == 0) *a.counter = 0;
-            }
-            __syncthreads();   // s_last is read before the next tile's count
-        }
-    }
-    cp_async_wait<0>();
-}
-
 template <typename R>
 cudaError_t Ops<R>::pred2d(const sf_ctx *c, R *z0, R *z1, R *z2, R *ub1, R *vb1, R *ub2, R *vb2,
                            R *rz, R *ru, R *rv, double Dt, double weight, double val,
@@ -891,32 +633,6 @@ cudaError_t Ops<R>::pred2d(const sf_ctx *c, R *z0, R *z1, R *z2, R *ub1, R *vb1,
         const void *ptrs[] = {z0, z1, z2, ub1, vb1, ub2, vb2, rz, ru, rv, a.g.h, a.g.pm, a.g.pn,
                               a.g.on_u, a.g.om_v};
         for (const void *q : ptrs) pair = pair && (reinterpret_cast<uintptr_t>(q) % (2 * sizeof(R))) == 0;
-    }
-    if (pair && c->pred_pair == 3) {   // the staged persistent form
-        const int tiles_x = (c->I + kPairTX - 1) / kPairTX, tiles_y = (c->J + kStgTY - 1) / kStgTY;
-        const int ntiles = tiles_x * tiles_y;
-        const int ring_blocks = (4 * c->I + 4 * (c->J - 4) + kStgThreads - 1) / kStgThreads;
-        int inner_x = 0, inner_y = 0;
-        for (int tx = 0; tx < tiles_x; ++tx)
-            inner_x += prd_inner_pair_tile(tx * kPairTX, 3, c->I, 3 + kStgTY + 2, kStgTY);
-        for (int ty = 0; ty < tiles_y; ++ty)
-            inner_y += prd_inner_pair_tile(4, ty * kStgTY, 4 + kPairTX + 2, c->J, kStgTY);
-        const int edge_blocks = ring_blocks + ntiles - inner_x * inner_y;
-        static int sms[64] = {};
-        static bool attr[64] = {};
-        int dev = 0;
-        cudaGetDevice(&dev);
-        if (dev >= 0 && dev < 64 && !attr[dev]) {
-            cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev);
-            const cudaError_t e = cudaFuncSetAttribute(
-                k_pred2d_stg<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stg_smem_bytes<R>());
-            if (e != cudaSuccess) return e;
-            attr[dev] = true;
-        }
-        const int per_sm = sizeof(R) == 4 ? 4 : 2;
-        const int P = std::min(ntiles, per_sm * std::max(sms[dev], 1));
-        return launch_dep(c, k_pred2d_stg<R>, dim3((unsigned)(ring_blocks + P)), dim3(32, kStgRows),
-                          stg_smem_bytes<R>(), s, a, ring_blocks, tiles_x, ntiles, edge_blocks);
     }
     if (pair) {
         const int rows = c->pred_pair == 2 ? 8 : 16, TY = rows - 1, nt = 32 * rows;

@@ -327,7 +327,7 @@ def test_fused_predictor_pair_and_scalar_forms_agree(precision):
     from sailfish_b200.model import Model
     cfg, st = _inputs(200)
     out = []
-    for pair in (0, 1, 2, 3):   # scalar, paired (16-row, 8-row blocks), staged persistent
+    for pair in (0, 1, 2):      # scalar, paired (16-row and 8-row blocks)
         m = Model(cfg["grid"], cfg["boundary"], cfg["dt"], cfg["ndtfast"], precision=precision)
         assert lib.sf_ctx_tune(m.ctx.ptr, 1, pair) == 0
         m.load(st)
