@@ -1,7 +1,7 @@
 """Generate the golden fixtures in tests/golden/ from the reference itself.
 
-Run in a container that has the reference checkout (``$SAILFISH_REFERENCE``, default
-/root/reference).  Nothing at test time reads the reference: the tests only load the
+Run in a container that has the reference checkout (``$SAILFISH_REFERENCE``, default: a
+``reference`` directory beside the repository).  Nothing at test time reads the reference: the tests only load the
 ``.npz`` files written here.
 
 How the reference is run on the CPU:
@@ -30,7 +30,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.abspath(os.path.join(HERE, "..", ".."))
-REF = os.environ.get("SAILFISH_REFERENCE", "/root/reference")
+REF = os.environ.get("SAILFISH_REFERENCE", os.path.join(os.path.dirname(REPO), "reference"))
 
 sys.path[:0] = [os.path.join(HERE, "cupy_shim")] + [os.path.join(REF, d) for d in
                                                      ("modules", "utility", "nonlinear", "functionals")]
