@@ -926,8 +926,9 @@ def run_ours(args, rank, world):
                               if mixing != "none" else None,
                    "l2": "inputs larger than L2 (each 3D field %.2f GB)" % (m.u.numel() * esize / 1e9),
                    "parallelism": "replicas" if world > 1 else "single",
-                   "rhs3d_tile": str(autotune.TILES[m.rhs_tile]),
-                   "rhs3d_tile_autotune_ms": {str(autotune.TILES[k]): v for k, v in tune.items()}},
+                   "rhs3d_form": autotune.variant_name(
+                       "march%d" % m.rhs_march if m.rhs_march else m.rhs_tile),
+                   "rhs3d_autotune_ms": {autotune.variant_name(k): v for k, v in tune.items()}},
         "phases_ms": per_phase,
         "kernel_ms_per_step": {k: t * n for k, (t, n) in per_launch.items()},
         "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak,

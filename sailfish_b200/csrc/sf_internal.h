@@ -144,6 +144,9 @@ struct sf_ctx {
     // FP32 column solve staged with 16-byte cp.async where aligned (else per element): on one
     // B200 basin4 takes 1.43 ms with it and 1.56 ms without
     int s3_vec = 1;
+    // 3D right-hand side in its marching form (sf_ctx_tune SF_TUNE_RHS_MARCH; set at context
+    // creation: 3 for FP32 single grids); 0: the tiled form of rhs_tile
+    int rhs_march = 0;
     cudaStream_t cap = nullptr;
     double *d_bcval = nullptr;
     sf_loop_graph graphs[3];

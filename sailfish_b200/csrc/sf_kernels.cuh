@@ -949,6 +949,369 @@ __device__ __forceinline__ void rhs3d_body(const Geo<R> &g, const R *__restrict_
 }
 
 // ------------------------------------------------------------------------------------------
+// rhs3d, marching form (single grids, N >= 6): the same operations as rhs3d_body, value for
+// value, with each thread walking RW rows of one column.  A warp spans 32 columns, i0 - 1 ..
+// i0 + 30: lane 0 evaluates the west halo column (its x-face fluxes and its Coriolis term
+// reach lane 1 by a shuffle) and lanes 1..31 own the block's 31 output columns.  Walking up a
+// column, a node's south y-face fluxes and its Coriolis "s" term are the previous row's own
+// (the same expressions at the same node), its west x-face fluxes and Coriolis "w" term the
+// west lane's; a warp evaluates the south y-faces of its first row once per level.  The
+// stencil's shared loads repeat from row to row at constant offsets and are loaded once (the
+// walk holds no shared store); a level takes one block barrier (the staging ring) instead of
+// two.  The levels are staged as in rhs3d_body, over columns xs .. xs+37, xs = i0 - 3 rounded
+// down to even for pair staging.
+// ------------------------------------------------------------------------------------------
+constexpr int kMarchX = 31;   // output columns per block
+template <int NW, int RW>
+struct MarchTile {
+    static constexpr int TY = NW * RW;           // output rows per block
+    static constexpr int SY = TY + kHY0 + kHY1;  // staged rows j0-3 .. j0+TY+1
+    static constexpr int SX = 38;                // staged columns xs .. xs+37
+    static constexpr int SN = SX * SY;
+    static constexpr int NT = 32 * NW;           // threads per block
+};
+template <typename R>
+__host__ __device__ constexpr int march_bufs() { return sizeof(R) == 4 ? 3 : 2; }
+template <typename R, int NW, int RW>
+constexpr size_t march_smem_bytes() {
+    return sizeof(R) * (size_t)march_bufs<R>() * 6 * MarchTile<NW, RW>::SN;
+}
+// a thread's staged units (element pairs with P2, else elements) and their flat offsets
+template <int NW, int RW, bool P2>
+struct MarchMap {
+    using T = MarchTile<NW, RW>;
+    static constexpr int kUnits = P2 ? T::SN / 2 : T::SN;
+    static constexpr int kPer = (kUnits + T::NT - 1) / T::NT;
+    int rel[kPer];
+    int rmin, rmax;
+    __device__ __forceinline__ MarchMap(int I, int j0, int xs, int tid) {
+#pragma unroll
+        for (int q = 0; q < kPer; ++q) {
+            const int e = (P2 ? 2 : 1) * (tid + q * T::NT);
+            rel[q] = (j0 - kHY0 + e / T::SX) * I + xs + e % T::SX;
+        }
+        rmin = (j0 - kHY0) * I + xs;
+        rmax = (j0 - kHY0 + T::SY - 1) * I + xs + T::SX - 1;
+    }
+};
+template <typename R, int NW, int RW, bool P2>
+__device__ __forceinline__ void march_stage(R *dst, const R *src, long off, long len, bool safe,
+                                            const MarchMap<NW, RW, P2> &m, int tid) {
+    using M = MarchMap<NW, RW, P2>;
+#pragma unroll
+    for (int q = 0; q < M::kPer; ++q) {
+        const int e = tid + q * MarchTile<NW, RW>::NT;
+        if (M::kUnits % MarchTile<NW, RW>::NT == 0 || e < M::kUnits) {
+            const long f = off + m.rel[q];
+            if constexpr (P2) {
+                if (safe) {
+                    cp_async2(dst + 2 * e, src + f);
+                } else {
+                    const bool ok = f >= 0 && f < len;   // f and len even: the pair is in or out
+                    cp_async2(dst + 2 * e, ok ? src + f : src, ok);
+                }
+            } else {
+                const bool ok = f >= 0 && f < len;
+                cp_async(dst + e, ok ? src + f : src, ok);
+            }
+        }
+    }
+}
+
+template <typename R, int NW, int RW, bool P2, bool SPLIT>
+__device__ __forceinline__ void rhs3d_march_body(const Geo<R> &g, const R *__restrict__ u,
+                                                 const R *__restrict__ v, const R *__restrict__ Huon,
+                                                 const R *__restrict__ Hvom, const R *__restrict__ W,
+                                                 const R *__restrict__ Hz, R *__restrict__ ru,
+                                                 R *__restrict__ rv, const int bx, const int by) {
+    using T = MarchTile<NW, RW>;
+    constexpr int SX = T::SX, SN = T::SN, TY = T::TY;
+    constexpr int kBufs = march_bufs<R>();
+    constexpr unsigned kAll = 0xffffffffu;
+    extern __shared__ __align__(16) unsigned char rhs_smem[];
+    R(*sbuf)[6][SN] = reinterpret_cast<R(*)[6][SN]>(rhs_smem);
+    const int lane = threadIdx.x, w = threadIdx.y, tid = w * 32 + lane;
+    const int I = g.I, J = g.J, N = g.N;
+    const long s2 = g.s2;
+    const long len3 = (long)(N + 1) * s2, lenHz = (long)N * s2;
+    const int i0 = bx * kMarchX, j0 = by * TY;
+    const int col = i0 - 1 + lane;                        // lane 0: the west halo column
+    const int xs = P2 ? ((i0 - 3) & ~1) : (i0 - 3);       // first staged column
+    const int r0 = w * RW;                                // the warp's first row in the tile
+    const int b0 = (r0 + kHY0) * SX + (col - xs);         // staged index of (r0, col)
+    const R c9 = R(9.0 / 16.0), c1 = R(1.0 / 16.0), G = R(-0.5);
+
+    // Per node: output (lanes 1..31 inside the grid), Coriolis (rnode), vertical advection
+    // (rhs_kernels.cpp:144-149) as bit masks; f at the node (lane 0: at its column, the west
+    // term of lane 1's node); the flat index within a level.
+    unsigned outm = 0, rnm = 0, vam = 0;
+    R fp[RW];
+    int pf[RW];
+#pragma unroll
+    for (int rr = 0; rr < RW; ++rr) {
+        const int j = j0 + r0 + rr, p = j * I + col;
+        pf[rr] = p;
+        const bool live = lane >= 1 && col < I && j < J;
+        if (live) {
+            outm |= 1u << rr;
+            if (rnode_(col, j)) rnm |= 1u << rr;
+            if (g.bcfield[p] < 0 && inner_(col, j, I, J)) vam |= 1u << rr;
+        }
+        fp[rr] = lane >= 1 ? (live ? g.fomn[p] : R(0)) : ((j < J && p >= 0) ? g.fomn[p] : R(0));
+    }
+    // f of the row below the warp's first row (the Coriolis "s" term of that row's nodes)
+    const R fpw = ((outm & 1u) && pf[0] >= I) ? g.fomn[pf[0] - I] : R(0);
+    // vertical advection carried from level to level: the flux through the level's lower face
+    // and u, v at the next three levels of the node's column
+    R fuk[RW], fvk[RW], uw1[RW], uw2[RW], uw3[RW], vw1[RW], vw2[RW], vw3[RW];
+#pragma unroll
+    for (int rr = 0; rr < RW; ++rr) {
+        fuk[rr] = fvk[rr] = uw1[rr] = uw2[rr] = uw3[rr] = vw1[rr] = vw2[rr] = vw3[rr] = R(0);
+    }
+
+    const MarchMap<NW, RW, P2> mm(I, j0, xs, tid);
+    auto issue = [&](int K, int buf) {
+        const long o = (long)K * s2;
+        R(*bf)[SN] = sbuf[buf];
+        // W is staged from level K+1 and Hz has N levels: o + rmax < N s2 covers all six
+        const bool safe = o + mm.rmin >= 0 && o + mm.rmax < lenHz;
+        march_stage<R, NW, RW, P2>(bf[0], u, o, len3, safe, mm, tid);
+        march_stage<R, NW, RW, P2>(bf[1], v, o, len3, safe, mm, tid);
+        march_stage<R, NW, RW, P2>(bf[2], Huon, o, len3, safe, mm, tid);
+        march_stage<R, NW, RW, P2>(bf[3], Hvom, o, len3, safe, mm, tid);
+        march_stage<R, NW, RW, P2>(bf[4], Hz, o, lenHz, safe, mm, tid);
+        march_stage<R, NW, RW, P2>(bf[5], W, o + s2, len3, safe, mm, tid);
+        cp_async_commit();
+    };
+
+#define COL(X, k) ((X)[(long)(k) * s2 + pp])
+#define U4C(a, b_, c, d) (c9 * ((b_) + (c)) - c1 * ((a) + (d)))
+#define WU4G(k) (c9 * (W[(long)(k) * s2 + pp] + W[(long)(k) * s2 + pp + 1]) - \
+                 c1 * (W[(long)(k) * s2 + pp - 1] + W[(long)(k) * s2 + pp + 2]))
+#define WV4G(k) (c9 * (W[(long)(k) * s2 + pp] + W[(long)(k) * s2 + pp + I]) - \
+                 c1 * (W[(long)(k) * s2 + pp - I] + W[(long)(k) * s2 + pp + 2 * I]))
+#define UR(r, c) ((U(r, c) + U(r, (c) + 1)) * R(0.5))
+#define UP(r, c) ((U(r, c) + U(r, (c) - 1)) * R(0.5))
+#define VR(r, c) ((V(r, c) + V((r) + 1, c)) * R(0.5))
+#define VP(r, c) ((V(r, c) + V((r) - 1, c)) * R(0.5))
+#define HUR(r, c) ((HU(r, c) + HU(r, (c) + 1)) * R(0.5))
+#define HUP(r, c) ((HU(r, c) + HU(r, (c) - 1)) * R(0.5))
+#define HVP(r, c) ((HV(r, c) + HV((r) - 1, c)) * R(0.5))
+#define HVR(r, c) ((HV(r, c) + HV((r) + 1, c)) * R(0.5))
+#define DXX(T, r, c) (((T)(r, (c) - 1) - R(2.0) * (T)(r, c)) + (T)(r, (c) + 1))
+#define DEE(T, r, c) (((T)((r) - 1, c) - R(2.0) * (T)(r, c)) + (T)((r) + 1, c))
+#define UXXR(r, c) ((UR(r, c) + UR(r, (c) + 1) >= R(0)) ? DXX(U, r, c) : DXX(U, r, (c) + 1))
+#define UEEP(r, c) ((HVP(r, c) + HVP((r) - 1, c) >= R(0)) ? DEE(U, r, c) : DEE(U, (r) - 1, c))
+#define HUXXR(r, c) ((DXX(HU, r, c) + DXX(HU, r, (c) + 1)) * R(0.5))
+#define HUEEP(r, c) ((DEE(HU, r, c) + DEE(HU, r, (c) - 1)) * R(0.5))
+#define HVXXP(r, c) ((DXX(HV, r, c) + DXX(HV, (r) - 1, c)) * R(0.5))
+#define HVEER(r, c) ((DEE(HV, r, c) + DEE(HV, (r) + 1, c)) * R(0.5))
+
+    issue(0, 0);
+    if constexpr (kBufs == 3) {
+        if (N > 1) issue(1, 1);
+        else cp_async_commit();
+    }
+    for (int K0 = 0; K0 < N; K0 += kBufs) {
+#pragma unroll
+    for (int kb = 0; kb < kBufs; ++kb) {
+        const int K = K0 + kb;
+        if (K >= N) break;   // uniform over the block
+        const long o = (long)K * s2;
+        if constexpr (kBufs == 3) {
+            cp_async_wait<1>();   // level K's group (level K+1's may still be in flight)
+            __syncthreads();      // ... and every thread is done with level K-1
+            if (K + 2 < N) issue(K + 2, (kb + 2) % kBufs);
+            else cp_async_commit();
+        } else {
+            if (K + 1 < N) {
+                issue(K + 1, (kb + 1) % kBufs);
+                cp_async_wait<1>();
+            } else {
+                cp_async_wait<0>();
+            }
+            __syncthreads();
+        }
+        R(*bf)[SN] = sbuf[kb];
+        const Tile<R, SX> U{bf[0], b0}, V{bf[1], b0}, HU{bf[2], b0}, HV{bf[3], b0}, HZ{bf[4], b0},
+            WW{bf[5], b0};
+        // the row below the warp's first row: its y-face fluxes and its Coriolis "p" term in v
+        R ufe_s, vfe_s, VF_s;
+        {
+            const R uxx = UXXR(-1, 0), uee = UEEP(-1, 0);
+            ufe_s = UP(-1, 0) + (G * uee) * (HVP(-1, 0) + G * HVXXP(-1, 0));
+            vfe_s = VR(-1, 0) + (G * uxx) * (HVR(-1, 0) + G * HVEER(-1, 0));
+            VF_s = (HZ(-1, 0) * fpw) * ((U(-1, 0) + U(-1, 1)) * R(0.5));
+        }
+        // Coriolis and horizontal advection of row rr (every level)
+        auto horiz = [&](const int rr, R &aru, R &arv) {
+            // addCoriolis (rhs_kernels.cpp:7-35): UFw is the west node's UFp, VFs the south
+            // node's VFp
+            const R cffp = HZ(rr, 0) * fp[rr];
+            const R UFp = cffp * ((V(rr, 0) + V(rr + 1, 0)) * R(0.5));
+            const R VFp = cffp * ((U(rr, 0) + U(rr, 1)) * R(0.5));
+            const R UFw = __shfl_up_sync(kAll, UFp, 1);
+            const bool rn = rnm >> rr & 1u;
+            aru = rn ? R(0) + (UFp + UFw) * R(0.5) : R(0);
+            arv = rn ? R(0) - (VFp + VF_s) * R(0.5) : R(0);
+            VF_s = VFp;
+            // horizontalAdvection (rhs_kernels.cpp:93-130): own face fluxes, the west node's
+            // x-faces and the south node's y-faces
+            const R uxx = UXXR(rr, 0), uee = UEEP(rr, 0);
+            const R ufx = UR(rr, 0) + (G * uxx) * (HUR(rr, 0) + G * HUXXR(rr, 0));
+            const R ufe = UP(rr, 0) + (G * uee) * (HVP(rr, 0) + G * HVXXP(rr, 0));
+            const R vfx = VP(rr, 0) + (G * uee) * (HUP(rr, 0) + G * HUEEP(rr, 0));
+            const R vfe = VR(rr, 0) + (G * uxx) * (HVR(rr, 0) + G * HVEER(rr, 0));
+            const R ufxw = __shfl_up_sync(kAll, ufx, 1), vfxw = __shfl_up_sync(kAll, vfx, 1);
+            aru = aru - ((ufx - ufxw) + (ufe - ufe_s));
+            arv = arv - ((vfx - vfxw) + (vfe - vfe_s));
+            ufe_s = ufe;
+            vfe_s = vfe;
+        };
+        R aru_[RW], arv_[RW];
+        if (SPLIT && K >= 2 && K <= N - 4) {
+            // Levels 2 .. N-4: the vertical advection's interior form on every node, kept where
+            // the node takes it; u, v four levels up loaded before the walk (one exposed load
+            // latency per level); no special stores.  (The reference's out-of-range threads
+            // reach levels 0 and 1 only: they number less than s2 + 512.)
+            R u4[RW], v4[RW];
+#pragma unroll
+            for (int rr = 0; rr < RW; ++rr) {
+                const long pp = pf[rr];
+                const bool va = vam >> rr & 1u;
+                u4[rr] = va ? COL(u, K + 4) : R(0);
+                v4[rr] = va ? COL(v, K + 4) : R(0);
+            }
+#pragma unroll
+            for (int rr = 0; rr < RW; ++rr) {
+                R aru, arv;
+                horiz(rr, aru, arv);
+                const R wu = c9 * (WW(rr, 0) + WW(rr, 1)) - c1 * (WW(rr, -1) + WW(rr, 2));
+                const R wv = c9 * (WW(rr, 0) + WW(rr + 1, 0)) - c1 * (WW(rr - 1, 0) + WW(rr + 2, 0));
+                const R fu1 = U4C(U(rr, 0), uw1[rr], uw2[rr], uw3[rr]) * wu;
+                const R fv1_ = U4C(V(rr, 0), vw1[rr], vw2[rr], vw3[rr]) * wv;
+                const bool va = vam >> rr & 1u;
+                aru_[rr] = va ? aru - (fu1 - fuk[rr]) : aru;
+                arv_[rr] = va ? arv - (fv1_ - fvk[rr]) : arv;
+                fuk[rr] = fu1;
+                fvk[rr] = fv1_;
+                uw1[rr] = uw2[rr]; uw2[rr] = uw3[rr]; uw3[rr] = u4[rr];
+                vw1[rr] = vw2[rr]; vw2[rr] = vw3[rr]; vw3[rr] = v4[rr];
+            }
+            // stores after the walk, so that no store separates the walk's repeated shared loads
+#pragma unroll
+            for (int rr = 0; rr < RW; ++rr) {
+                if (outm >> rr & 1u) {
+                    ru[o + pf[rr]] = aru_[rr];
+                    rv[o + pf[rr]] = arv_[rr];
+                }
+            }
+        } else {
+            // every level (the walk's general form; with SPLIT levels 0, 1 and N-3 .. N-1).  The
+            // vertical advection's loads of u, v four levels up are issued before the walk.
+            R u4[RW], v4[RW];
+            const bool mid = K >= 2 && K <= N - 3 && K + 4 <= N;
+#pragma unroll
+            for (int rr = 0; rr < RW; ++rr) {
+                const long pp = pf[rr];
+                const bool ld = mid && (vam >> rr & 1u);
+                u4[rr] = ld ? COL(u, K + 4) : R(0);
+                v4[rr] = ld ? COL(v, K + 4) : R(0);
+            }
+#pragma unroll
+            for (int rr = 0; rr < RW; ++rr) {
+                R aru, arv;
+                horiz(rr, aru, arv);
+                // the reference's out-of-range threads store 0 into levels >= 1 (rhs_kernels.cpp:86-91)
+                if (K >= 1 && o + pf[rr] < g.ref_threads) {
+                    aru = R(0);
+                    arv = R(0);
+                }
+                if (vam >> rr & 1u) {   // verticalAdvection (rhs_kernels.cpp:158-194)
+                    const long pp = pf[rr];
+                    if (K == 0) {
+                        const R uuu = (c9 * (COL(u, 0) + COL(u, 1)) - c1 * (0 + COL(u, 2))) * WU4G(1);
+                        const R uuu2 = (c9 * (0 + COL(u, 0)) - c1 * (0 + COL(u, 1))) * WU4G(0);
+                        aru = aru - (uuu - uuu2);
+                        fuk[rr] = uuu;
+                    } else if (K == 1) {
+                        const R fv1 = U4C(COL(v, 0), COL(v, 1), COL(v, 2), COL(v, 3)) * WV4G(1);
+                        const R fv2 = U4C(COL(v, 1), COL(v, 2), COL(v, 3), COL(v, 4)) * WV4G(2);
+                        const R fv3 = U4C(COL(v, 2), COL(v, 3), COL(v, 4), COL(v, 5)) * WV4G(3);
+                        const R fu2 = U4C(COL(u, 1), COL(u, 2), COL(u, 3), COL(u, 4)) * WU4G(2);
+                        arv -= c9 * (fv1 + fv2) - c1 * (fv1 + fv3);
+                        aru = aru - (fu2 - fuk[rr]);
+                        fuk[rr] = fu2;
+                        fvk[rr] = fv2;
+                        uw1[rr] = COL(u, 3); uw2[rr] = COL(u, 4); uw3[rr] = COL(u, 5);
+                        vw1[rr] = COL(v, 3); vw2[rr] = COL(v, 4); vw3[rr] = COL(v, 5);
+                    } else if (K <= N - 3) {
+                        const R wu = c9 * (WW(rr, 0) + WW(rr, 1)) - c1 * (WW(rr, -1) + WW(rr, 2));
+                        const R wv = c9 * (WW(rr, 0) + WW(rr + 1, 0)) - c1 * (WW(rr - 1, 0) + WW(rr + 2, 0));
+                        const R fu1 = U4C(U(rr, 0), uw1[rr], uw2[rr], uw3[rr]) * wu;
+                        const R fv1_ = U4C(V(rr, 0), vw1[rr], vw2[rr], vw3[rr]) * wv;
+                        aru = aru - (fu1 - fuk[rr]);
+                        arv = arv - (fv1_ - fvk[rr]);
+                        fuk[rr] = fu1;
+                        fvk[rr] = fv1_;
+                        uw1[rr] = uw2[rr]; uw2[rr] = uw3[rr]; uw3[rr] = u4[rr];
+                        vw1[rr] = vw2[rr]; vw2[rr] = vw3[rr]; vw3[rr] = v4[rr];
+                    }   // levels N-2 and N-1 repeat level N-3 (:189-192), stored with it
+                }
+                aru_[rr] = aru;
+                arv_[rr] = arv;
+            }
+#pragma unroll
+            for (int rr = 0; rr < RW; ++rr) {
+                if (!(outm >> rr & 1u)) continue;
+                const long q = o + pf[rr];
+                if (!(vam >> rr & 1u)) {
+                    ru[q] = aru_[rr];
+                    rv[q] = arv_[rr];
+                    if (K == N - 1) {   // ru_t2[:] = 0 (rhs.py:38) at level N
+                        ru[(long)N * s2 + pf[rr]] = R(0);
+                        rv[(long)N * s2 + pf[rr]] = R(0);
+                    }
+                } else if (K <= N - 3) {
+                    ru[q] = aru_[rr];
+                    if (K >= 1) rv[q] = arv_[rr];
+                    if (K == 1) rv[pf[rr]] = arv_[rr];   // rv[0] = rv[1] (:183)
+                    if (K == N - 3) {   // ru[N-2] = ru[N-1] = ru[N-3], ru[N] = ru[N-2] (:189-193)
+#pragma unroll
+                        for (int k = 1; k <= 3; ++k) {
+                            ru[q + k * s2] = aru_[rr];
+                            rv[q + k * s2] = arv_[rr];
+                        }
+                    }
+                }
+            }
+        }
+        if constexpr (kBufs == 2) __syncthreads();   // the buffer of level K is refilled next
+    }
+    }
+#undef HVEER
+#undef HVXXP
+#undef HUEEP
+#undef HUXXR
+#undef UEEP
+#undef UXXR
+#undef DEE
+#undef DXX
+#undef HVR
+#undef HVP
+#undef HUP
+#undef HUR
+#undef VP
+#undef VR
+#undef UP
+#undef UR
+#undef WV4G
+#undef WU4G
+#undef U4C
+#undef COL
+}
+
+// ------------------------------------------------------------------------------------------
 // set_maxflux (step3D_uv.kernels.cpp:372-405) + omega (:62-165) + set_zeta (:294-310)
 // ------------------------------------------------------------------------------------------
 // C > 0: levels whose loads the fused flux/omega kernel issues together on its interior
@@ -1897,6 +2260,22 @@ __global__ void __launch_bounds__(TX * TY, 1024 / (TX * TY)) k_rhs3d(Geo<R> g, c
                                                   const R *__restrict__ Hz, R *__restrict__ ru, R *__restrict__ rv) {
     rhs3d_body<R, TX, TY, P2>(g, u, v, Huon, Hvom, W, Hz, ru, rv, (int)blockIdx.x, (int)blockIdx.y);
 }
+// blocks of the marching form that fit an SM's shared memory (233,472 bytes, 1 KB of it
+// reserved per block), at most 2048 threads
+template <typename R, int NW, int RW>
+constexpr int march_min_blocks() {
+    const int b = (int)(233472 / (march_smem_bytes<R, NW, RW>() + 1024));
+    const int t = 2048 / (32 * NW);
+    return b < 1 ? 1 : (b < t ? b : t);
+}
+template <typename R, int NW, int RW, bool P2, bool SPLIT, int MINB>
+__global__ void __launch_bounds__(32 * NW, MINB) k_rhs3d_march(
+    Geo<R> g, const R *__restrict__ u, const R *__restrict__ v, const R *__restrict__ Huon,
+    const R *__restrict__ Hvom, const R *__restrict__ W, const R *__restrict__ Hz,
+    R *__restrict__ ru, R *__restrict__ rv) {
+    rhs3d_march_body<R, NW, RW, P2, SPLIT>(g, u, v, Huon, Hvom, W, Hz, ru, rv, (int)blockIdx.x,
+                                           (int)blockIdx.y);
+}
 template <typename R, int TX, int TY>
 __global__ void __launch_bounds__(TX *TY) kb_rhs3d(const Member<R> *mt, const int2 *bm, int var,
                                                    const R *__restrict__ u, const R *__restrict__ v, const R *Huon,
@@ -2100,6 +2479,52 @@ cudaError_t Ops<R>::bc_apply(const sf_ctx *c, const BcProgram &p1, R *f1, const 
 template <typename R>
 cudaError_t Ops<R>::rhs3d(const sf_ctx *c, const R *u, const R *v, const R *Huon, const R *Hvom,
                           const R *W, const R *Hz, R *ru, R *rv, cudaStream_t s) {
+    // pair staging: even rows, fields on 2-element boundaries, 32-bit flat offsets
+    const uintptr_t al = 2 * sizeof(R);
+    const bool p2 = c->I % 2 == 0 && (long)c->I * c->J < (1L << 30) &&
+                    (uintptr_t)u % al == 0 && (uintptr_t)v % al == 0 &&
+                    (uintptr_t)Huon % al == 0 && (uintptr_t)Hvom % al == 0 &&
+                    (uintptr_t)W % al == 0 && (uintptr_t)Hz % al == 0;
+    // marching form (sf_ctx_tune SF_TUNE_RHS_MARCH): 1 = 4 warps x 4 rows (levels 2 .. N-4 in
+    // the walk's branch-free form), 2 = 8 warps x 2 rows (the same, two blocks per SM), 3 = 8
+    // warps x 2 rows (the general walk on every level, three blocks per SM)
+    if (c->nmem == 1 && c->rhs_march > 0 && c->N >= 6 && (long)c->I * c->J < (1L << 30)) {
+        auto march = [&](auto nw, auto rw, auto split, auto minb) {
+            constexpr int NW = decltype(nw)::value, RW = decltype(rw)::value;
+            constexpr bool SP = decltype(split)::value;
+            constexpr int MB = decltype(minb)::value > 0 ? decltype(minb)::value
+                                                         : march_min_blocks<R, NW, RW>();
+            constexpr size_t smem = march_smem_bytes<R, NW, RW>();
+            static bool attr_set[64] = {};
+            int dev = 0;
+            cudaGetDevice(&dev);
+            if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+                cudaFuncSetAttribute(k_rhs3d_march<R, NW, RW, true, SP, MB>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                cudaFuncSetAttribute(k_rhs3d_march<R, NW, RW, false, SP, MB>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                attr_set[dev] = true;
+            }
+            const dim3 grid((c->I + kMarchX - 1) / kMarchX, (c->J + NW * RW - 1) / (NW * RW));
+            const dim3 block(32, NW);
+            if (p2)
+                k_rhs3d_march<R, NW, RW, true, SP, MB><<<grid, block, smem, s>>>(geo(c), u, v, Huon, Hvom, W, Hz, ru, rv);
+            else
+                k_rhs3d_march<R, NW, RW, false, SP, MB><<<grid, block, smem, s>>>(geo(c), u, v, Huon, Hvom, W, Hz, ru, rv);
+        };
+        using M0 = std::integral_constant<int, 0>;
+        using M2 = std::integral_constant<int, 2>;
+        using M4 = std::integral_constant<int, 4>;
+        using M8 = std::integral_constant<int, 8>;
+        using ST = std::true_type;
+        using SF = std::false_type;
+        switch (c->rhs_march) {
+        case 1: march(M4{}, M4{}, ST{}, M0{}); break;
+        case 2: march(M8{}, M2{}, ST{}, M2{}); break;
+        default: march(M8{}, M2{}, SF{}, M0{}); break;
+        }
+        return cudaGetLastError();
+    }
     // tile variant: 0 = 32 x 8, 1 = 32 x 4, 2 = 64 x 4, 3 = 32 x 16
     const int var = c->rhs_tile;
     auto run = [&](auto tx, auto ty) {
@@ -2122,12 +2547,6 @@ cudaError_t Ops<R>::rhs3d(const sf_ctx *c, const R *u, const R *v, const R *Huon
                 mt<R>(c), c->bm_tile[var], var, u, v, Huon, Hvom, W, Hz, ru, rv);
         } else {
             const dim3 grid((c->I + TX - 1) / TX, (c->J + TY - 1) / TY), block(TX, TY);
-            // pair staging: even rows, fields on 2-element boundaries, 32-bit flat offsets
-            const uintptr_t al = 2 * sizeof(R);
-            const bool p2 = c->I % 2 == 0 && (long)c->I * c->J < (1L << 30) &&
-                            (uintptr_t)u % al == 0 && (uintptr_t)v % al == 0 &&
-                            (uintptr_t)Huon % al == 0 && (uintptr_t)Hvom % al == 0 &&
-                            (uintptr_t)W % al == 0 && (uintptr_t)Hz % al == 0;
             if (p2)
                 k_rhs3d<R, TX, TY, true><<<grid, block, smem, s>>>(geo(c), u, v, Huon, Hvom, W, Hz, ru, rv);
             else

@@ -284,6 +284,44 @@ def test_column_solve_bulk_and_element_staging_agree(Lm):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("Lm", CASES)
+def test_rhs3d_marching_and_tiled_forms_agree(precision, Lm):
+    """sf_rhs3d in its tiled form and its three marching forms (SF_TUNE_RHS_MARCH) on grids
+    with interior tiles on every side (I = 202: paired staging; I = 201: element staging), the
+    fluxes and W from sf_maxflux_omega: identical ru and rv in FP64 (built without FMA
+    contraction); in FP32 the forms may contract different products into FMAs, so they agree
+    to a few units of FP32 rounding of each field's scale."""
+    import torch
+    from sailfish_b200._lib import lib, check
+    m64, m32 = _models(Lm)
+    m = m64 if precision == "fp64" else m32
+    p = m._p
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    check(lib.sf_maxflux_omega(m.ctx.ptr, p(m.u), p(m.v), p(m.Huon), p(m.Hvom), p(m.Hz),
+                               p(m.W), p(m.z_w), None, None, None, st), "sf_maxflux_omega")
+    out = []
+    for mv in (0, 1, 2, 3):
+        assert lib.sf_ctx_tune(m.ctx.ptr, 3, mv) == 0
+        for t in (m.ru, m.rv):
+            t.fill_(7.0)
+        check(lib.sf_rhs3d(m.ctx.ptr, p(m.u), p(m.v), p(m.Huon), p(m.Hvom), p(m.W), p(m.Hz),
+                           p(m.ru), p(m.rv), st), "sf_rhs3d")
+        torch.cuda.synchronize()
+        out.append([t.cpu().numpy() for t in (m.ru, m.rv)])
+    assert lib.sf_ctx_tune(m.ctx.ptr, 3, 0) == 0
+    assert np.abs(m.W.cpu().numpy()).max() > 0
+    assert np.abs(out[0][0]).max() > 0 and np.abs(out[0][1]).max() > 0
+    for o in out[1:]:
+        for a, b in zip(out[0], o):
+            if precision == "fp64":
+                np.testing.assert_array_equal(a, b)
+            else:
+                assert np.abs(b - a).max() <= 4e-6 * np.abs(a).max()
+    assert lib.sf_ctx_tune(m.ctx.ptr, 3, 4) != 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
 def test_maxflux_omega_chunk_variants_agree(precision):
     """The fused set_maxflux/omega kernel with its interior columns' loads issued one level at a
     time and in chunks of 4 and 8 levels (sf_ctx_tune): identical fluxes and W in FP64 (built

@@ -139,8 +139,10 @@ def test_overlapped_phases_give_the_same_step(precision, mode):
 @pytest.mark.gpu
 @pytest.mark.parametrize("Lm", [70, 69])
 def test_rhs3d_tile_variants_agree_on_one_grid(Lm):
-    """sf_rhs3d on one square grid with every tile variant, bit-identical in FP64: an even row
-    length (Lm = 70, I = 72) takes the paired staging, an odd one (I = 71) the element staging."""
+    """sf_rhs3d on one square grid with every tile variant and every marching form
+    (SF_TUNE_RHS_MARCH), bit-identical in FP64: an even row length (Lm = 70, I = 72) takes the
+    paired staging, an odd one (I = 71) the element staging; both leave partial tiles on the
+    east and north edges."""
     import numpy as np
     import torch
     from sailfish_b200 import configs
@@ -154,8 +156,9 @@ def test_rhs3d_tile_variants_agree_on_one_grid(Lm):
     m.step(2)
     p = m._p
     out = []
-    for v in (0, 1, 2, 3):
-        assert lib.sf_ctx_set_tile(m.ctx.ptr, v) == 0
+    for v in (0, 1, 2, 3, 4, 5, 6):
+        assert lib.sf_ctx_set_tile(m.ctx.ptr, v if v < 4 else 0) == 0
+        assert lib.sf_ctx_tune(m.ctx.ptr, 3, v - 3 if v >= 4 else 0) == 0
         m.ru.zero_()
         m.rv.zero_()
         assert lib.sf_rhs3d(m.ctx.ptr, p(m.u), p(m.v), p(m.Huon), p(m.Hvom), p(m.W), p(m.Hz),
