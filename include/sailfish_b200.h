@@ -192,13 +192,17 @@ int sf_ctx_set_bulk(sf_ctx *ctx, int enable);
  *   marching form (each thread walks a few rows of one column; neighbouring face fluxes come
  *   from the west lane and from the row below): 1 = 4 rows per thread, 4 warps per block;
  *   2 = 2 rows, 8 warps, two blocks per SM; 3 = 2 rows, 8 warps, three blocks per SM (default
- *   for FP32); 0 for the tiled form of sf_ctx_set_tile (default for FP64).
+ *   for FP32); 0 for the tiled form of sf_ctx_set_tile (default for FP64);
+ * SF_TUNE_RHS_CHUNKS: 1 (default) for the marching form's levels staged as 16-byte chunks
+ *   where the fields allow it (FP32, even row length, levels a multiple of 4 elements, fields
+ *   on 16-byte boundaries), 0 for aligned element pairs.
  * Results are identical for every value in FP64; in FP32 the compiler may contract products
  * into FMAs differently in the variants, so they agree to the rounding of FP32. */
 #define SF_TUNE_MO_CHUNK 0
 #define SF_TUNE_PRED_PAIR 1
 #define SF_TUNE_S3_VEC 2
 #define SF_TUNE_RHS_MARCH 3
+#define SF_TUNE_RHS_CHUNKS 4
 int sf_ctx_tune(sf_ctx *ctx, int knob, int value);
 /* Turn programmatic dependent launch of the barotropic loop's kernels on (default) or off:
  * with it each kernel's blocks become resident while its predecessor's last wave runs and wait

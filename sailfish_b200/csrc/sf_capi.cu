@@ -896,6 +896,10 @@ int sf_ctx_tune(sf_ctx *c, int knob, int value) {
         if (value < 0 || value > 3) return fail(SF_EINVAL, "march is 0, 1, 2 or 3");
         c->rhs_march = value;
         return SF_OK;
+    case SF_TUNE_RHS_CHUNKS:
+        if (value != 0 && value != 1) return fail(SF_EINVAL, "chunks is 0 or 1");
+        c->rhs_chunks = value;
+        return SF_OK;
     default:
         return fail(SF_EINVAL, "unknown tuning knob");
     }

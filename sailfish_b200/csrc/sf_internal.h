@@ -147,6 +147,8 @@ struct sf_ctx {
     // 3D right-hand side in its marching form (sf_ctx_tune SF_TUNE_RHS_MARCH; set at context
     // creation: 3 for FP32 single grids); 0: the tiled form of rhs_tile
     int rhs_march = 0;
+    // the marching form's levels staged as 16-byte chunks where the fields allow it (FP32)
+    int rhs_chunks = 1;
     cudaStream_t cap = nullptr;
     double *d_bcval = nullptr;
     sf_loop_graph graphs[3];

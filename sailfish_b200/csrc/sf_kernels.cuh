@@ -958,73 +958,111 @@ __device__ __forceinline__ void rhs3d_body(const Geo<R> &g, const R *__restrict_
 // west lane's; a warp evaluates the south y-faces of its first row once per level.  The
 // stencil's shared loads repeat from row to row at constant offsets and are loaded once (the
 // walk holds no shared store); a level takes one block barrier (the staging ring) instead of
-// two.  The levels are staged as in rhs3d_body, over columns xs .. xs+37, xs = i0 - 3 rounded
-// down to even for pair staging.
+// two.  The levels are staged as in rhs3d_body (STG 0: elements, 1: aligned pairs, columns
+// xs .. xs+37 with xs = i0 - 3, rounded down to even for pairs), or (STG 2, FP32) as 16-byte
+// chunks: each staged row's 36 columns i0-3 .. i0+32 are copied as the ten aligned chunks
+// that hold them, the row placed at a shift of 0..3 elements in shared memory so that the
+// chunks land aligned; a row pitch SX = I (mod 4) makes the shifts cancel, so element (r, c)
+// sits at r SX + A + c for a constant A of the block.
 // ------------------------------------------------------------------------------------------
 constexpr int kMarchX = 31;   // output columns per block
-template <int NW, int RW>
+template <int NW, int RW, int SX_>
 struct MarchTile {
     static constexpr int TY = NW * RW;           // output rows per block
     static constexpr int SY = TY + kHY0 + kHY1;  // staged rows j0-3 .. j0+TY+1
-    static constexpr int SX = 38;                // staged columns xs .. xs+37
-    static constexpr int SN = SX * SY;
+    static constexpr int SX = SX_;               // row pitch of the staged tile
+    static constexpr int SN = (SX * SY + 8 + 3) / 4 * 4;   // a field's staged level (16-byte multiple)
     static constexpr int NT = 32 * NW;           // threads per block
 };
 template <typename R>
 __host__ __device__ constexpr int march_bufs() { return sizeof(R) == 4 ? 3 : 2; }
-template <typename R, int NW, int RW>
+template <typename R, int NW, int RW, int SX>
 constexpr size_t march_smem_bytes() {
-    return sizeof(R) * (size_t)march_bufs<R>() * 6 * MarchTile<NW, RW>::SN;
+    return sizeof(R) * (size_t)march_bufs<R>() * 6 * MarchTile<NW, RW, SX>::SN;
 }
-// a thread's staged units (element pairs with P2, else elements) and their flat offsets
-template <int NW, int RW, bool P2>
+__device__ __forceinline__ int mod4(int x) { return x & 3; }   // two's complement: x mod 4 in 0..3
+// a thread's staged units (chunks of 16 bytes, element pairs, or elements) with their flat
+// offsets within a level and their shared-memory indices, and the block's extent of them
+template <int NW, int RW, int STG, int SX>
 struct MarchMap {
-    using T = MarchTile<NW, RW>;
-    static constexpr int kUnits = P2 ? T::SN / 2 : T::SN;
+    using T = MarchTile<NW, RW, SX>;
+    static constexpr int kRowChunks = 10;   // 40 elements hold any 36-column span
+    static constexpr int kUnits = STG == 2 ? T::SY * kRowChunks : STG == 1 ? T::SX * T::SY / 2 : T::SX * T::SY;
     static constexpr int kPer = (kUnits + T::NT - 1) / T::NT;
-    int rel[kPer];
-    int rmin, rmax;
+    int rel[kPer], dst[kPer];
+    int rmin, rmax;   // first and last flat offset staged
+    int A;            // staged index of column xs in row 0
     __device__ __forceinline__ MarchMap(int I, int j0, int xs, int tid) {
+        const int F0 = (j0 - kHY0) * I + xs;   // flat offset of (row 0, column xs)
+        if constexpr (STG == 2) {
+            A = 3 + mod4(F0 - 3);               // A = F0 (mod 4), 3 <= A <= 6
 #pragma unroll
-        for (int q = 0; q < kPer; ++q) {
-            const int e = (P2 ? 2 : 1) * (tid + q * T::NT);
-            rel[q] = (j0 - kHY0 + e / T::SX) * I + xs + e % T::SX;
+            for (int q = 0; q < kPer; ++q) {
+                const int e = tid + q * T::NT, r = e / kRowChunks, k = e % kRowChunks;
+                const int Fr = F0 + r * I, m = mod4(Fr);
+                rel[q] = Fr - m + 4 * k;        // a 16-byte-aligned chunk of row r
+                dst[q] = r * SX + A - m + 4 * k;   // = 0 (mod 4): SX = I, A = F0 (mod 4)
+            }
+            const int Fl = F0 + (T::SY - 1) * I;
+            rmin = F0 - mod4(F0);
+            rmax = Fl - mod4(Fl) + 4 * kRowChunks - 1;
+        } else {
+            A = 0;
+#pragma unroll
+            for (int q = 0; q < kPer; ++q) {
+                const int e = (STG == 1 ? 2 : 1) * (tid + q * T::NT);
+                rel[q] = (j0 - kHY0 + e / T::SX) * I + xs + e % T::SX;
+                dst[q] = e;
+            }
+            rmin = F0;
+            rmax = (j0 - kHY0 + T::SY - 1) * I + xs + T::SX - 1;
         }
-        rmin = (j0 - kHY0) * I + xs;
-        rmax = (j0 - kHY0 + T::SY - 1) * I + xs + T::SX - 1;
     }
 };
-template <typename R, int NW, int RW, bool P2>
+__device__ __forceinline__ void cp_async16z(uint32_t saddr, const void *src, bool ok) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(saddr), "l"(src),
+                 "r"(ok ? 16 : 0));
+}
+template <typename R, int NW, int RW, int STG, int SX>
 __device__ __forceinline__ void march_stage(R *dst, const R *src, long off, long len, bool safe,
-                                            const MarchMap<NW, RW, P2> &m, int tid) {
-    using M = MarchMap<NW, RW, P2>;
+                                            const MarchMap<NW, RW, STG, SX> &m, int tid) {
+    using M = MarchMap<NW, RW, STG, SX>;
 #pragma unroll
     for (int q = 0; q < M::kPer; ++q) {
-        const int e = tid + q * MarchTile<NW, RW>::NT;
-        if (M::kUnits % MarchTile<NW, RW>::NT == 0 || e < M::kUnits) {
+        const int e = tid + q * MarchTile<NW, RW, SX>::NT;
+        if (M::kUnits % MarchTile<NW, RW, SX>::NT == 0 || e < M::kUnits) {
             const long f = off + m.rel[q];
-            if constexpr (P2) {
+            if constexpr (STG == 2) {
+                // f and len are multiples of 4: a chunk is wholly in or out of the array
+                const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst + m.dst[q]);
                 if (safe) {
-                    cp_async2(dst + 2 * e, src + f);
+                    cp_async16(d, src + f);
+                } else {
+                    const bool ok = f >= 0 && f < len;
+                    cp_async16z(d, ok ? src + f : src, ok);
+                }
+            } else if constexpr (STG == 1) {
+                if (safe) {
+                    cp_async2(dst + m.dst[q], src + f);
                 } else {
                     const bool ok = f >= 0 && f < len;   // f and len even: the pair is in or out
-                    cp_async2(dst + 2 * e, ok ? src + f : src, ok);
+                    cp_async2(dst + m.dst[q], ok ? src + f : src, ok);
                 }
             } else {
                 const bool ok = f >= 0 && f < len;
-                cp_async(dst + e, ok ? src + f : src, ok);
+                cp_async(dst + m.dst[q], ok ? src + f : src, ok);
             }
         }
     }
 }
 
-template <typename R, int NW, int RW, bool P2, bool SPLIT>
+template <typename R, int NW, int RW, int STG, int SX_, bool SPLIT>
 __device__ __forceinline__ void rhs3d_march_body(const Geo<R> &g, const R *__restrict__ u,
                                                  const R *__restrict__ v, const R *__restrict__ Huon,
                                                  const R *__restrict__ Hvom, const R *__restrict__ W,
                                                  const R *__restrict__ Hz, R *__restrict__ ru,
                                                  R *__restrict__ rv, const int bx, const int by) {
-    using T = MarchTile<NW, RW>;
+    using T = MarchTile<NW, RW, SX_>;
     constexpr int SX = T::SX, SN = T::SN, TY = T::TY;
     constexpr int kBufs = march_bufs<R>();
     constexpr unsigned kAll = 0xffffffffu;
@@ -1035,10 +1073,11 @@ __device__ __forceinline__ void rhs3d_march_body(const Geo<R> &g, const R *__res
     const long s2 = g.s2;
     const long len3 = (long)(N + 1) * s2, lenHz = (long)N * s2;
     const int i0 = bx * kMarchX, j0 = by * TY;
-    const int col = i0 - 1 + lane;                        // lane 0: the west halo column
-    const int xs = P2 ? ((i0 - 3) & ~1) : (i0 - 3);       // first staged column
-    const int r0 = w * RW;                                // the warp's first row in the tile
-    const int b0 = (r0 + kHY0) * SX + (col - xs);         // staged index of (r0, col)
+    const int col = i0 - 1 + lane;                             // lane 0: the west halo column
+    const int xs = STG == 1 ? ((i0 - 3) & ~1) : (i0 - 3);      // first staged column
+    const int r0 = w * RW;                                     // the warp's first row in the tile
+    const MarchMap<NW, RW, STG, SX> mm(I, j0, xs, tid);
+    const int b0 = (r0 + kHY0) * SX + mm.A + (col - xs);       // staged index of (r0, col)
     const R c9 = R(9.0 / 16.0), c1 = R(1.0 / 16.0), G = R(-0.5);
 
     // Per node: output (lanes 1..31 inside the grid), Coriolis (rnode), vertical advection
@@ -1069,18 +1108,17 @@ __device__ __forceinline__ void rhs3d_march_body(const Geo<R> &g, const R *__res
         fuk[rr] = fvk[rr] = uw1[rr] = uw2[rr] = uw3[rr] = vw1[rr] = vw2[rr] = vw3[rr] = R(0);
     }
 
-    const MarchMap<NW, RW, P2> mm(I, j0, xs, tid);
     auto issue = [&](int K, int buf) {
         const long o = (long)K * s2;
         R(*bf)[SN] = sbuf[buf];
         // W is staged from level K+1 and Hz has N levels: o + rmax < N s2 covers all six
         const bool safe = o + mm.rmin >= 0 && o + mm.rmax < lenHz;
-        march_stage<R, NW, RW, P2>(bf[0], u, o, len3, safe, mm, tid);
-        march_stage<R, NW, RW, P2>(bf[1], v, o, len3, safe, mm, tid);
-        march_stage<R, NW, RW, P2>(bf[2], Huon, o, len3, safe, mm, tid);
-        march_stage<R, NW, RW, P2>(bf[3], Hvom, o, len3, safe, mm, tid);
-        march_stage<R, NW, RW, P2>(bf[4], Hz, o, lenHz, safe, mm, tid);
-        march_stage<R, NW, RW, P2>(bf[5], W, o + s2, len3, safe, mm, tid);
+        march_stage<R, NW, RW, STG, SX>(bf[0], u, o, len3, safe, mm, tid);
+        march_stage<R, NW, RW, STG, SX>(bf[1], v, o, len3, safe, mm, tid);
+        march_stage<R, NW, RW, STG, SX>(bf[2], Huon, o, len3, safe, mm, tid);
+        march_stage<R, NW, RW, STG, SX>(bf[3], Hvom, o, len3, safe, mm, tid);
+        march_stage<R, NW, RW, STG, SX>(bf[4], Hz, o, lenHz, safe, mm, tid);
+        march_stage<R, NW, RW, STG, SX>(bf[5], W, o + s2, len3, safe, mm, tid);
         cp_async_commit();
     };
 
@@ -2262,19 +2300,19 @@ __global__ void __launch_bounds__(TX * TY, 1024 / (TX * TY)) k_rhs3d(Geo<R> g, c
 }
 // blocks of the marching form that fit an SM's shared memory (233,472 bytes, 1 KB of it
 // reserved per block), at most 2048 threads
-template <typename R, int NW, int RW>
+template <typename R, int NW, int RW, int SX>
 constexpr int march_min_blocks() {
-    const int b = (int)(233472 / (march_smem_bytes<R, NW, RW>() + 1024));
+    const int b = (int)(233472 / (march_smem_bytes<R, NW, RW, SX>() + 1024));
     const int t = 2048 / (32 * NW);
     return b < 1 ? 1 : (b < t ? b : t);
 }
-template <typename R, int NW, int RW, bool P2, bool SPLIT, int MINB>
+template <typename R, int NW, int RW, int STG, int SX, bool SPLIT, int MINB>
 __global__ void __launch_bounds__(32 * NW, MINB) k_rhs3d_march(
     Geo<R> g, const R *__restrict__ u, const R *__restrict__ v, const R *__restrict__ Huon,
     const R *__restrict__ Hvom, const R *__restrict__ W, const R *__restrict__ Hz,
     R *__restrict__ ru, R *__restrict__ rv) {
-    rhs3d_march_body<R, NW, RW, P2, SPLIT>(g, u, v, Huon, Hvom, W, Hz, ru, rv, (int)blockIdx.x,
-                                           (int)blockIdx.y);
+    rhs3d_march_body<R, NW, RW, STG, SX, SPLIT>(g, u, v, Huon, Hvom, W, Hz, ru, rv,
+                                                (int)blockIdx.x, (int)blockIdx.y);
 }
 template <typename R, int TX, int TY>
 __global__ void __launch_bounds__(TX *TY) kb_rhs3d(const Member<R> *mt, const int2 *bm, int var,
@@ -2489,28 +2527,48 @@ cudaError_t Ops<R>::rhs3d(const sf_ctx *c, const R *u, const R *v, const R *Huon
     // the walk's branch-free form), 2 = 8 warps x 2 rows (the same, two blocks per SM), 3 = 8
     // warps x 2 rows (the general walk on every level, three blocks per SM)
     if (c->nmem == 1 && c->rhs_march > 0 && c->N >= 6 && (long)c->I * c->J < (1L << 30)) {
+        // staging: 16-byte chunks (FP32, even rows, levels of a multiple of 4 elements, fields
+        // on 16-byte boundaries; sf_ctx_tune SF_TUNE_RHS_CHUNKS), else pairs, else elements
+        const bool c16 = sizeof(R) == 4 && c->rhs_chunks && c->I % 2 == 0 && c->s2 % 4 == 0 &&
+                         (uintptr_t)u % 16 == 0 && (uintptr_t)v % 16 == 0 &&
+                         (uintptr_t)Huon % 16 == 0 && (uintptr_t)Hvom % 16 == 0 &&
+                         (uintptr_t)W % 16 == 0 && (uintptr_t)Hz % 16 == 0;
         auto march = [&](auto nw, auto rw, auto split, auto minb) {
             constexpr int NW = decltype(nw)::value, RW = decltype(rw)::value;
             constexpr bool SP = decltype(split)::value;
-            constexpr int MB = decltype(minb)::value > 0 ? decltype(minb)::value
-                                                         : march_min_blocks<R, NW, RW>();
-            constexpr size_t smem = march_smem_bytes<R, NW, RW>();
-            static bool attr_set[64] = {};
-            int dev = 0;
-            cudaGetDevice(&dev);
-            if (dev >= 0 && dev < 64 && !attr_set[dev]) {
-                cudaFuncSetAttribute(k_rhs3d_march<R, NW, RW, true, SP, MB>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-                cudaFuncSetAttribute(k_rhs3d_march<R, NW, RW, false, SP, MB>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-                attr_set[dev] = true;
+            auto go = [&](auto stg, auto sx) {
+                constexpr int STG = decltype(stg)::value, SX = decltype(sx)::value;
+                constexpr int MB = decltype(minb)::value > 0 ? decltype(minb)::value
+                                                             : march_min_blocks<R, NW, RW, SX>();
+                constexpr size_t smem = march_smem_bytes<R, NW, RW, SX>();
+                static bool attr_set[64] = {};
+                int dev = 0;
+                cudaGetDevice(&dev);
+                if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+                    cudaFuncSetAttribute(k_rhs3d_march<R, NW, RW, STG, SX, SP, MB>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                    attr_set[dev] = true;
+                }
+                const dim3 grid((c->I + kMarchX - 1) / kMarchX, (c->J + NW * RW - 1) / (NW * RW));
+                const dim3 block(32, NW);
+                k_rhs3d_march<R, NW, RW, STG, SX, SP, MB><<<grid, block, smem, s>>>(
+                    geo(c), u, v, Huon, Hvom, W, Hz, ru, rv);
+            };
+            using S0 = std::integral_constant<int, 0>;
+            using S1 = std::integral_constant<int, 1>;
+            using S2 = std::integral_constant<int, 2>;
+            using X38 = std::integral_constant<int, 38>;
+            using X44 = std::integral_constant<int, 44>;
+            using X46 = std::integral_constant<int, 46>;
+            if constexpr (sizeof(R) == 4) {
+                if (c16) {
+                    if (c->I % 4 == 0) go(S2{}, X44{});
+                    else go(S2{}, X46{});
+                    return;
+                }
             }
-            const dim3 grid((c->I + kMarchX - 1) / kMarchX, (c->J + NW * RW - 1) / (NW * RW));
-            const dim3 block(32, NW);
-            if (p2)
-                k_rhs3d_march<R, NW, RW, true, SP, MB><<<grid, block, smem, s>>>(geo(c), u, v, Huon, Hvom, W, Hz, ru, rv);
-            else
-                k_rhs3d_march<R, NW, RW, false, SP, MB><<<grid, block, smem, s>>>(geo(c), u, v, Huon, Hvom, W, Hz, ru, rv);
+            if (p2) go(S1{}, X38{});
+            else go(S0{}, X38{});
         };
         using M0 = std::integral_constant<int, 0>;
         using M2 = std::integral_constant<int, 2>;

@@ -287,7 +287,8 @@ def test_column_solve_bulk_and_element_staging_agree(Lm):
 @pytest.mark.parametrize("Lm", CASES)
 def test_rhs3d_marching_and_tiled_forms_agree(precision, Lm):
     """sf_rhs3d in its tiled form and its three marching forms (SF_TUNE_RHS_MARCH) on grids
-    with interior tiles on every side (I = 202: paired staging; I = 201: element staging), the
+    with interior tiles on every side (I = 202: 16-byte chunk staging in FP32, else pairs;
+    I = 201: element staging; SF_TUNE_RHS_CHUNKS switches the chunks off), the
     fluxes and W from sf_maxflux_omega: identical ru and rv in FP64 (built without FMA
     contraction); in FP32 the forms may contract different products into FMAs, so they agree
     to a few units of FP32 rounding of each field's scale."""
@@ -299,16 +300,25 @@ def test_rhs3d_marching_and_tiled_forms_agree(precision, Lm):
     st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
     check(lib.sf_maxflux_omega(m.ctx.ptr, p(m.u), p(m.v), p(m.Huon), p(m.Hvom), p(m.Hz),
                                p(m.W), p(m.z_w), None, None, None, st), "sf_maxflux_omega")
-    out = []
-    for mv in (0, 1, 2, 3):
+    out, staged = [], {}
+    for mv, ch in ((0, 1), (1, 1), (2, 1), (3, 1), (1, 0), (2, 0), (3, 0)):
         assert lib.sf_ctx_tune(m.ctx.ptr, 3, mv) == 0
+        assert lib.sf_ctx_tune(m.ctx.ptr, 4, ch) == 0
         for t in (m.ru, m.rv):
             t.fill_(7.0)
         check(lib.sf_rhs3d(m.ctx.ptr, p(m.u), p(m.v), p(m.Huon), p(m.Hvom), p(m.W), p(m.Hz),
                            p(m.ru), p(m.rv), st), "sf_rhs3d")
         torch.cuda.synchronize()
         out.append([t.cpu().numpy() for t in (m.ru, m.rv)])
+        staged[mv, ch] = out[-1]
     assert lib.sf_ctx_tune(m.ctx.ptr, 3, 0) == 0
+    assert lib.sf_ctx_tune(m.ctx.ptr, 4, 1) == 0
+    assert lib.sf_ctx_tune(m.ctx.ptr, 4, 2) != 0
+    # the staging (16-byte chunks in FP32 where aligned, else pairs or elements) moves the same
+    # values: the marching forms' results do not depend on it
+    for mv in (1, 2, 3):
+        for a, b in zip(staged[mv, 1], staged[mv, 0]):
+            np.testing.assert_array_equal(a, b)
     assert np.abs(m.W.cpu().numpy()).max() > 0
     assert np.abs(out[0][0]).max() > 0 and np.abs(out[0][1]).max() > 0
     for o in out[1:]:
