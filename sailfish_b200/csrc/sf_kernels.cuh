@@ -1353,7 +1353,8 @@ __device__ __forceinline__ void rhs3d_march_body(const Geo<R> &g, const R *__res
 // set_maxflux (step3D_uv.kernels.cpp:372-405) + omega (:62-165) + set_zeta (:294-310)
 // ------------------------------------------------------------------------------------------
 // C > 0: levels whose loads the fused flux/omega kernel issues together on its interior
-// columns (sf_ctx_tune knob SF_TUNE_MO_CHUNK); 0: one level at a time, the loop unrolled by 4
+// columns (sf_ctx_tune knob SF_TUNE_MO_CHUNK); 0: one level at a time, the loop unrolled by 4;
+// -1: omega alone (no fluxes), the fluxes' loads issued 16 levels at a time
 template <typename R, int C = 0>
 __device__ __forceinline__ void maxflux_omega_body(
     const Geo<R> &g, const R *__restrict__ u, const R *__restrict__ v, R *Huon, R *Hvom,
@@ -1396,6 +1397,9 @@ __device__ __forceinline__ void maxflux_omega_body(
         const bool ue = rc && i + 1 < g.I && unode_(i + 1, j);
         const bool vnn = rc && j + 1 < g.J && vnode_(i, j + 1, g.J);
         const R onu_e = ue ? g.on_u[p + 1] : R(0), omv_n = vnn ? g.om_v[p + I] : R(0);
+        // the column's bed and depth for the correction, loaded before the integral
+        const R zbed = z_w[p];
+        const R h = z_w[(long)(N - 1) * s2 + p] - zbed;
         // the running integral in shared memory ([level][thread]), not in per-thread local
         // memory, whose footprint over all resident threads spills out of L1 and L2
         extern __shared__ __align__(16) unsigned char mo_smem[];
@@ -1403,12 +1407,37 @@ __device__ __forceinline__ void maxflux_omega_body(
 #define Wc(K) Wcol[(K) * (int)blockDim.x]
         R Wk = R(0);
         Wc(0) = R(0);
-        if (C > 0 && rc && fu && fv && ue && vnn) {
+        if (C < 0 && !rc) {
+            // omega alone: the four fluxes of a chunk of kO levels loaded together (basin4:
+            // 0.45 ms with 16, 0.48 with 8, 0.66 one level at a time)
+            constexpr int kO = 16;
+            for (int K0 = 1; K0 < N; K0 += kO) {
+                R hu[kO], hv[kO], hE[kO], hN[kO];
+#pragma unroll
+                for (int c = 0; c < kO; ++c) {
+                    const long o = (long)(K0 + c < N ? K0 + c : N - 1) * s2 + p;
+                    hu[c] = Huon[o];
+                    hv[c] = Hvom[o];
+                    hE[c] = Huon[o + 1];
+                    hN[c] = Hvom[o + I];
+                }
+#pragma unroll
+                for (int c = 0; c < kO; ++c) {
+                    if (K0 + c < N) {
+                        Wk = Wk - ((hE[c] - hu[c]) + (hN[c] - hv[c]));
+                        Wc(K0 + c) = Wk;
+                    }
+                }
+            }
+        } else if (C > 0 && fu && fv && ue && vnn) {
             // every flux this column needs is computed here: the loads of a chunk of levels
             // (Hz, u, v only, never the flux arrays being written) are issued together
             // before any of the chunk's arithmetic, the same expressions as below
             // 32-bit element offsets (the launcher takes this form only where (N+1) s2 < 2^31)
             const int s2i = (int)s2, Ii = (int)I;
+            // two chunks per iteration: the second chunk's loads may issue before the first
+            // chunk's arithmetic and stores
+#pragma unroll 2
             for (int K0 = 0; K0 < N; K0 += (C > 0 ? C : 1)) {
                 constexpr int CC = C > 0 ? C : 1;
                 R hz[CC], hzw[CC], hzs[CC], hze[CC], hzn[CC], uu[CC], uE[CC], vv[CC], vN[CC];
@@ -1460,22 +1489,29 @@ __device__ __forceinline__ void maxflux_omega_body(
             }
         }
         }
-        const R zbed = z_w[p];
-        const R h = z_w[(long)(N - 1) * s2 + p] - zbed;
         const R Ws = Wk;
         W[p] = R(0);
-        if constexpr (C > 0) {
-            const int s2i = (int)s2;
-#pragma unroll 4
-            for (int K = 1; K < N; ++K) {
-                const int o = K * s2i + pi;
-                W[o] = Wc(K) - ddiv(Ws * (z_w[o] - zbed), h);
-            }
-        } else {
-#pragma unroll 4
-            for (int K = 1; K < N; ++K) {
-                const long o = (long)K * s2 + p;
-                W[o] = Wc(K) - ddiv(Ws * (z_w[o] - zbed), h);
+        // the correction, z_w loaded kZ levels at a time (one exposed load latency per chunk):
+        // 32 for omega alone, 16 after the fluxes (basin4: 0.45 and 0.82 ms; 32 after the
+        // fluxes takes 1.14 ms)
+        {
+            constexpr int kZ = C < 0 ? 32 : 16;
+            for (int K0 = 1; K0 < N; K0 += kZ) {
+                R zw[kZ];
+#pragma unroll
+                for (int c = 0; c < kZ; ++c) {
+                    const int K = K0 + c < N ? K0 + c : N - 1;
+                    zw[c] = C > 0 ? z_w[K * (int)s2 + pi] : z_w[(long)K * s2 + p];
+                }
+#pragma unroll
+                for (int c = 0; c < kZ; ++c) {
+                    const int K = K0 + c;
+                    if (K < N) {
+                        const R wv = Wc(K) - ddiv(Ws * (zw[c] - zbed), h);
+                        if (C > 0) W[K * (int)s2 + pi] = wv;
+                        else W[(long)K * s2 + p] = wv;
+                    }
+                }
             }
         }
 #undef Wc
@@ -2637,6 +2673,7 @@ cudaError_t Ops<R>::maxflux_omega(const sf_ctx *c, const R *u, const R *v, R *Hu
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !attr_set[dev]) {
         const int most = (int)(sizeof(R) * kBlock * kNMax);
+        cudaFuncSetAttribute(k_maxflux_omega<R, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
         cudaFuncSetAttribute(k_maxflux_omega<R, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
         cudaFuncSetAttribute(k_maxflux_omega<R, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
         cudaFuncSetAttribute(k_maxflux_omega<R, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
@@ -2651,7 +2688,8 @@ cudaError_t Ops<R>::maxflux_omega(const sf_ctx *c, const R *u, const R *v, R *Hu
     }
     // the chunked forms address with 32-bit element offsets
     const bool fits = (long)(c->N + 1) * c->s2 < (1L << 31);
-    auto k = (!fits || !do_flux) ? k_maxflux_omega<R, 0>   // omega alone: 0.66 against 0.72 ms
+    auto k = !do_flux ? k_maxflux_omega<R, -1>
+             : !fits ? k_maxflux_omega<R, 0>
              : c->mo_chunk >= 8 ? k_maxflux_omega<R, 8>
              : c->mo_chunk >= 4 ? k_maxflux_omega<R, 4> : k_maxflux_omega<R, 0>;
     k<<<blocks_for(c->s2, kBlock), kBlock, smem, s>>>(
