@@ -52,10 +52,14 @@ class _StdoutToStderr:
 def phase_pass(m, steps, hook, phases):
     """Per-phase CUDA-event times from a separate pass with the phases run one after another
     (Model.overlap off), so that a kernel's time is its own and not stretched by the phases
-    that overlap it in the timed run; the headline value comes from the overlapped run."""
+    that overlap it in the timed run; the headline value comes from the overlapped run.  The
+    pass is queued behind a device-side wait, so that a phase's first event is not stamped
+    while the host is still submitting the phase's kernels."""
     import torch
     prev = getattr(m, "overlap", False)
     m.overlap = False
+    torch.cuda.synchronize()
+    torch.cuda._sleep(int(4e7))   # ~20 ms at the B200's clock: the host queues the pass
     m.step(min(steps, 5), timer=hook)
     m.overlap = prev
     torch.cuda.synchronize()
@@ -63,11 +67,16 @@ def phase_pass(m, steps, hook, phases):
 
 
 def time_pred2d(m, n):
-    """Average device time (ms) of one launch of the fused barotropic predictor (k_pred2d),
-    which runs once per barotropic substep inside the loop's graph: n launches through
-    sf_step2d_predictor on the model's own slots, each between its own pair of CUDA events on
-    the launching stream.  None where the context has no fused predictor.  The model's fields
-    are overwritten (run it after the timed region)."""
+    """Device time (ms) of one launch of the fused barotropic predictor (k_pred2d), which runs
+    once per barotropic substep inside the loop's graph, from n launches through
+    sf_step2d_predictor on the model's own slots: (back_to_back, isolated).  back_to_back: the
+    n launches between one pair of CUDA events on the launching stream, divided by n (the
+    loop's own mode: each launch starts as the previous one's last wave drains, programmatic
+    dependent launch as the context has it).  isolated: each launch between its own pair of
+    events (each then also carries the event and its ramp-up and tail; about 5 us more on
+    basin4).  Both are queued behind a device-side wait, so that no event is stamped while the
+    host is still submitting a kernel.  None where the context has no fused predictor.  The
+    model's fields are overwritten (run it after the timed region)."""
     import ctypes
     import torch
     from sailfish_b200._lib import lib, check
@@ -76,19 +85,35 @@ def time_pred2d(m, n):
     s = m.state2d()
     st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
     stream = torch.cuda.current_stream()
-    evs = []
-    for k in range(n):
+
+    def launch():
         for name in m.NAMES2:                      # cycleTimes2D on the local slot copy
             a = getattr(s, name)
             a[0], a[1], a[2] = a[1], a[2], a[0]
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
         check(lib.sf_step2d_predictor(m.ctx.ptr, ctypes.byref(s), m.dtfast, 0.0, 0, st),
               "sf_step2d_predictor")
+
+    evs = []
+    torch.cuda.synchronize()
+    torch.cuda._sleep(int(2e7))   # ~10 ms at the B200's clock: the host queues all n launches
+    for k in range(n):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        launch()
         e1.record(stream)
         evs.append((e0, e1))
     torch.cuda.synchronize()
-    return float(np.mean([a.elapsed_time(b) for a, b in evs[1:]]))
+    isolated = float(np.mean([a.elapsed_time(b) for a, b in evs[1:]]))
+    launch()                      # warm the back-to-back run's first launch
+    torch.cuda.synchronize()
+    torch.cuda._sleep(int(2e7))
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for k in range(n):
+        launch()
+    b.record(stream)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / n, isolated
 
 
 def launches_per_step(m, mixing):
@@ -898,7 +923,7 @@ def run_ours(args, rank, world):
     per_launch = {k: (per_phase[k], 1) for k in per_phase if k in ab}
     t_pred = time_pred2d(m, m.nfast + 1)
     if t_pred is not None:
-        per_launch["k_pred2d"] = (t_pred, m.nfast + 1)
+        per_launch["k_pred2d"] = (t_pred[0], m.nfast + 1)
     dom = max(per_launch, key=lambda k: per_launch[k][0] * per_launch[k][1])
     peak, kind = peaks()
     achieved = ab[dom] / (per_launch[dom][0] * 1e-3) / 1e9
@@ -934,6 +959,10 @@ def run_ours(args, rank, world):
         "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_kind": kind,
                      "launch_ms": per_launch[dom][0], "launches_per_step": per_launch[dom][1],
+                     "launch_timing": "back to back: %d launches between one pair of CUDA events "
+                                      "on the launching stream" % per_launch[dom][1]
+                     if dom == "k_pred2d" else "the phase between its own pair of CUDA events",
+                     "launch_ms_isolated": t_pred[1] if dom == "k_pred2d" else None,
                      "algorithmic_bytes": ab[dom],
                      "traffic": traffic[0],
                      "traffic_source": None if traffic[0] is None else
