@@ -180,7 +180,7 @@ int sf_ctx_set_graphs(sf_ctx *ctx, int enable);
  * either way.  No counterpart in the reference. */
 int sf_ctx_set_bulk(sf_ctx *ctx, int enable);
 /* Tuning knobs of a context's kernels (no counterpart in the reference):
- * SF_TUNE_MO_CHUNK: 0, 4 (default) or 8 levels whose loads the fused set_maxflux/omega kernel
+ * SF_TUNE_MO_CHUNK: 0, 4, 5 (default) or 8 levels whose loads the fused set_maxflux/omega kernel
  *   issues together on columns whose fluxes it all computes itself;
  * SF_TUNE_PRED_PAIR: the fused predictor's paired form (two nodes per thread, vector loads) on
  *   grids with an even row length and aligned fields, with blocks of 16 staged rows (1) or 8

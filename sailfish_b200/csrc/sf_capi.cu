@@ -876,7 +876,8 @@ int sf_ctx_tune(sf_ctx *c, int knob, int value) {
     if (!c) return fail(SF_EINVAL, "null context");
     switch (knob) {
     case SF_TUNE_MO_CHUNK:
-        if (value != 0 && value != 4 && value != 8) return fail(SF_EINVAL, "chunk is 0, 4 or 8");
+        if (value != 0 && value != 4 && value != 5 && value != 8)
+            return fail(SF_EINVAL, "chunk is 0, 4, 5 or 8");
         c->mo_chunk = value;
         return SF_OK;
     case SF_TUNE_PRED_PAIR:

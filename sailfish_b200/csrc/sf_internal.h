@@ -136,8 +136,9 @@ struct sf_ctx {
     // by default: on basin4 the column solve took 2.08 ms with it against 1.65 ms with
     // per-element cp.async staging
     int use_bulk = 0;
-    // levels whose loads the fused flux/omega kernel issues together (sf_ctx_tune)
-    int mo_chunk = 4;
+    // levels whose loads the fused flux/omega kernel issues together (sf_ctx_tune; basin4:
+    // 0.82, 0.77 and 1.16 ms with 4, 5 and 8: 80, 80 and 128 registers)
+    int mo_chunk = 5;
     // fused predictor in its paired form (two nodes per thread) where the grid allows it: 1
     // with 16-row blocks, 2 with 8-row blocks (basin4 loop 4.27 and 4.18 ms), 0 scalar (4.49)
     int pred_pair = 2;

@@ -2679,6 +2679,7 @@ cudaError_t Ops<R>::maxflux_omega(const sf_ctx *c, const R *u, const R *v, R *Hu
         cudaFuncSetAttribute(k_maxflux_omega<R, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
         cudaFuncSetAttribute(k_maxflux_omega<R, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
         cudaFuncSetAttribute(k_maxflux_omega<R, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
+        cudaFuncSetAttribute(k_maxflux_omega<R, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
         cudaFuncSetAttribute(kb_maxflux_omega<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
         attr_set[dev] = true;
     }
@@ -2692,8 +2693,9 @@ cudaError_t Ops<R>::maxflux_omega(const sf_ctx *c, const R *u, const R *v, R *Hu
     const bool fits = (long)(c->N + 1) * c->s2 < (1L << 31);
     auto k = !do_flux ? k_maxflux_omega<R, -1>
              : !fits ? k_maxflux_omega<R, 0>
-             : c->mo_chunk >= 8 ? k_maxflux_omega<R, 8>
-             : c->mo_chunk >= 4 ? k_maxflux_omega<R, 4> : k_maxflux_omega<R, 0>;
+             : c->mo_chunk == 8 ? k_maxflux_omega<R, 8>
+             : c->mo_chunk == 5 ? k_maxflux_omega<R, 5>
+             : c->mo_chunk == 4 ? k_maxflux_omega<R, 4> : k_maxflux_omega<R, 0>;
     k<<<blocks_for(c->s2, kBlock), kBlock, smem, s>>>(
         geo(c), u, v, Huon, Hvom, Hz, W, z_w, do_flux, do_omega, zeta1, zeta2, Zt);
     return cudaGetLastError();

@@ -334,7 +334,7 @@ def test_rhs3d_marching_and_tiled_forms_agree(precision, Lm):
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 def test_maxflux_omega_chunk_variants_agree(precision):
     """The fused set_maxflux/omega kernel with its interior columns' loads issued one level at a
-    time and in chunks of 4 and 8 levels (sf_ctx_tune): identical fluxes and W in FP64 (built
+    time and in chunks of 4, 5 and 8 levels (sf_ctx_tune): identical fluxes and W in FP64 (built
     without FMA contraction); in FP32 the variants' code may contract different products into
     FMAs, so they agree to a few units of FP32 rounding of each field's scale."""
     import torch
@@ -344,7 +344,7 @@ def test_maxflux_omega_chunk_variants_agree(precision):
     p = m._p
     st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
     out = []
-    for ch in (0, 4, 8):
+    for ch in (0, 4, 5, 8):
         assert lib.sf_ctx_tune(m.ctx.ptr, 0, ch) == 0
         for t in (m.Huon, m.Hvom, m.W):
             t.zero_()
