@@ -437,6 +437,7 @@ template <typename R>
 struct PrdPair {
     R z1w, z1a, z1b, z1sa, z1sb, hw, ha, hb, hsa, hsb;
     R uba, ubb, vba, vbb, pma, pmb, pna, pnb, oua, oub, ova, ovb, z0a, z0b;
+    R z0w, z0sa, z0sb;   // zeta_t0 west and south of the pair (the momentum's), loaded with the rest
 };
 
 // computeZetaRHS at both nodes of a deep pair; fills the pair's kept inputs.
@@ -472,6 +473,8 @@ __device__ __forceinline__ void prd_rz_pair(const PredArgs<R> &a, long x, PrdPai
     ld2(g.pm + x, n.pma, n.pmb);
     ld2(g.pn + x, n.pna, n.pnb);
     ld2(a.z0 + x, n.z0a, n.z0b);
+    n.z0w = a.z0[x - 1];
+    ld2(a.z0 + x - I, n.z0sa, n.z0sb);
     // node a
     const R Dpa = n.z1a + n.ha, Dwa = n.z1w + n.hw, Dpb = n.z1b + n.hb;
     const R Dsa = n.z1sa + n.hsa, Dna = zna + hna;
@@ -493,15 +496,11 @@ __device__ __forceinline__ void prd_rz_pair(const PredArgs<R> &a, long x, PrdPai
 template <typename R>
 __device__ __forceinline__ void prd_mom_pair(const PredArgs<R> &a, long x, bool pda, bool pdb,
                                              R za, R zb, R zw, R zsa, R zsb, const PrdPair<R> &n) {
-    const int I = a.g.I;
-    const R *z0 = a.z0 + x;
-    R z0sa, z0sb;
-    ld2(z0 - I, z0sa, z0sb);
     const R gpa = a.w1 * za + a.w * n.z0a;
-    const R gw = a.w1 * zw + a.w * z0[-1];
-    const R gsa = a.w1 * zsa + a.w * z0sa;
+    const R gw = a.w1 * zw + a.w * n.z0w;
+    const R gsa = a.w1 * zsa + a.w * n.z0sa;
     const R gpb = a.w1 * zb + a.w * n.z0b;
-    const R gsb = a.w1 * zsb + a.w * z0sb;
+    const R gsb = a.w1 * zsb + a.w * n.z0sb;
     const R rua = (a.grav * n.oua) * (((n.ha + n.hw) * R(0.5)) * (gpa - gw) + R(0.5) * (gpa * gpa - gw * gw));
     const R rva = (a.grav * n.ova) * (((n.ha + n.hsa) * R(0.5)) * (gpa - gsa) + R(0.5) * (gpa * gpa - gsa * gsa));
     const R rub = (a.grav * n.oub) * (((n.hb + n.ha) * R(0.5)) * (gpb - gpa) + R(0.5) * (gpb * gpb - gpa * gpa));
