@@ -1077,7 +1077,6 @@ void roms_swap(sf_state2d *st) {   // n+1 (written over n-1) becomes n, n become
 
 int roms_check(const sf_ctx *c, const sf_state2d *st, const void *sustr, const void *svstr) {
     if (!c) return fail(SF_EINVAL, "null context");
-    if (c->nmem != 1) return fail(SF_EUNSUPPORTED, "the ROMS-form step runs single grids");
     if (!st || !sustr || !svstr) return fail(SF_EINVAL, "null state or stress");
     for (void *const *a : {st->zeta, st->ubar, st->vbar})
         for (int k = 0; k < 3; ++k)
@@ -1176,7 +1175,8 @@ int sf_roms_step3d_uv(sf_ctx *c, void *u, void *v, const void *ru0, const void *
         !ubar_s || !vbar_s || !Hz || !Akv || !z_r || !W || !DU || !DV)
         return fail(SF_EINVAL, "null argument");
     if (iic < ntfirst) return fail(SF_EINVAL, "sf_roms_step3d_uv: iic < ntfirst");
-    if (c && c->N > sf::kRomsMaxN) return fail(SF_EINVAL, "sf_roms_step3d_uv: N > 64");
+    if (c && (c->nmem > 1 ? c->maxN : c->N) > sf::kRomsMaxN)
+        return fail(SF_EINVAL, "sf_roms_step3d_uv: N > 64");
     // Adams-Bashforth weights of ru(n), ru(n-1), ru(n-2): forward Euler, AB2, then AB3
     static const double kAB[3][3] = {{1.0, 0.0, 0.0}, {1.5, -0.5, 0.0},
                                      {23.0 / 12.0, -16.0 / 12.0, 5.0 / 12.0}};

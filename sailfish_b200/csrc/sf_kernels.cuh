@@ -2237,9 +2237,8 @@ cudaError_t Ops<R>::obc_volcons(const sf_ctx *c, const R *zeta, R *ubar, R *vbar
 
 // setLateralUVBCs alone (step3D_uv.kernels.cpp:314-368).
 template <typename R>
-__global__ void __launch_bounds__(kBlock) k_lateral_uv_bc(Geo<R> g, R *__restrict__ u,
-                                                          R *__restrict__ v, R bcval) {
-    const long p = tid_flat();
+__device__ __forceinline__ void lateral_uv_bc_at(const Geo<R> &g, R *__restrict__ u,
+                                                 R *__restrict__ v, R bcval, const long p) {
     if (p >= g.s2) return;
     const long s2 = g.s2;
     const int ut = g.utype[p], vt = g.vtype[p];
@@ -2248,6 +2247,11 @@ __global__ void __launch_bounds__(kBlock) k_lateral_uv_bc(Geo<R> g, R *__restric
         for (int K = 0; K < g.N; ++K) u[(long)K * s2 + p] = bcval;
     if (vt > 0 && ((vt & (1 << 4)) != 0 || (vt & (1 << 3)) != 0))
         for (int K = 0; K < g.N; ++K) v[(long)K * s2 + p] = R(0);
+}
+template <typename R>
+__global__ void __launch_bounds__(kBlock) k_lateral_uv_bc(Geo<R> g, R *__restrict__ u,
+                                                          R *__restrict__ v, R bcval) {
+    lateral_uv_bc_at(g, u, v, bcval, tid_flat());
 }
 
 }  // namespace sf
@@ -2771,8 +2775,19 @@ cudaError_t Ops<R>::step3d_uv(const sf_ctx *c, R *u, R *v, const R *ru, const R 
     return cudaGetLastError();
 }
 template <typename R>
+__global__ void __launch_bounds__(kBlock) kb_lateral_uv_bc(const Member<R> *mt, const int2 *bm,
+                                                           R *__restrict__ u, R *__restrict__ v,
+                                                           R bcval) {
+    const int2 mb = bm[blockIdx.x];
+    const Member<R> &M = mt[mb.x];
+    lateral_uv_bc_at(M.g, u + M.off3, v + M.off3, bcval, (long)mb.y * kBlock + threadIdx.x);
+}
+template <typename R>
 cudaError_t Ops<R>::lateral_uv_bc(const sf_ctx *c, R *u, R *v, double val, cudaStream_t s) {
-    k_lateral_uv_bc<R><<<blocks_for(c->s2, kBlock), kBlock, 0, s>>>(geo(c), u, v, (R)val);
+    if (c->nmem > 1)
+        kb_lateral_uv_bc<R><<<c->nbm_pt, kBlock, 0, s>>>(mt<R>(c), c->bm_pt, u, v, (R)val);
+    else
+        k_lateral_uv_bc<R><<<blocks_for(c->s2, kBlock), kBlock, 0, s>>>(geo(c), u, v, (R)val);
     return cudaGetLastError();
 }
 

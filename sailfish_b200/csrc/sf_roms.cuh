@@ -45,8 +45,7 @@ __device__ __forceinline__ R roms_rz(const Geo<R> &g, const R *z, const R *u, co
 // Free surface of a phase at rho p.  Ring nodes take the value of the nearest interior node
 // (zero gradient at closed walls), computed here from the inputs.
 template <typename R>
-__global__ void __launch_bounds__(256) k_roms_zeta(Geo<R> g, RomsArgs<R> a) {
-    const long p = tid_flat();
+__device__ __forceinline__ void roms_zeta_at(const Geo<R> &g, const RomsArgs<R> &a, const long p) {
     if (p >= g.s2) return;
     const int j = fdiv((int)p, g.dI), i = (int)p - j * g.I;
     const long I = g.I;
@@ -109,8 +108,7 @@ __device__ __forceinline__ R roms_zwrk(const RomsArgs<R> &a, long q) {
 
 // Momentum of a phase at the U and V faces of p (0 on walls and the ring).
 template <typename R>
-__global__ void __launch_bounds__(256) k_roms_mom(Geo<R> g, RomsArgs<R> a) {
-    const long p = tid_flat();
+__device__ __forceinline__ void roms_mom_at(const Geo<R> &g, const RomsArgs<R> &a, const long p) {
     if (p >= g.s2) return;
     const int j = fdiv((int)p, g.dI), i = (int)p - j * g.I;
     const long I = g.I;
@@ -179,13 +177,11 @@ __global__ void __launch_bounds__(256) k_roms_mom(Geo<R> g, RomsArgs<R> a) {
 // west U face and south V face), levels in order; the expressions keep the oracle's operand
 // order (oracle/roms_oracle.py, rhs3d).
 template <typename R>
-__global__ void __launch_bounds__(256) k_roms_rhs3d(Geo<R> g, const R *__restrict__ u,
-                                                    const R *__restrict__ v,
-                                                    const R *__restrict__ Hu,
-                                                    const R *__restrict__ Hv,
-                                                    const R *__restrict__ Hz,
-                                                    R *__restrict__ ru, R *__restrict__ rv) {
-    const long p = tid_flat();
+__device__ __forceinline__ void roms_rhs3d_at(const Geo<R> &g, const R *__restrict__ u,
+                                              const R *__restrict__ v, const R *__restrict__ Hu,
+                                              const R *__restrict__ Hv, const R *__restrict__ Hz,
+                                              R *__restrict__ ru, R *__restrict__ rv,
+                                              const long p) {
     if (p >= g.s2) return;
     const int j = fdiv((int)p, g.dI), i = (int)p - j * g.I;
     const long I = g.I, s2 = g.s2;
@@ -228,11 +224,11 @@ __global__ void __launch_bounds__(256) k_roms_rhs3d(Geo<R> g, const R *__restric
 // ru[0] -= rdrag2 ub sqrt(ub^2 + v_u^2) * area at the interior U faces, ub the bottom level's u,
 // v_u the four-point average of its v; rv likewise at the interior V faces.
 template <typename R>
-__global__ void __launch_bounds__(256) k_roms_stress3d(Geo<R> g, const R *__restrict__ u,
-                                                       const R *__restrict__ v, R *__restrict__ ru,
-                                                       R *__restrict__ rv, const R *__restrict__ sustr,
-                                                       const R *__restrict__ svstr, R rdrag2) {
-    const long p = tid_flat();
+__device__ __forceinline__ void roms_stress3d_at(const Geo<R> &g, const R *__restrict__ u,
+                                                 const R *__restrict__ v, R *__restrict__ ru,
+                                                 R *__restrict__ rv, const R *__restrict__ sustr,
+                                                 const R *__restrict__ svstr, R rdrag2,
+                                                 const long p) {
     if (p >= g.s2) return;
     const int j = fdiv((int)p, g.dI), i = (int)p - j * g.I;
     const long I = g.I, o = (long)(g.N - 1) * g.s2 + p;
@@ -332,16 +328,17 @@ __device__ __forceinline__ double roms_column(const Geo<R> &g, long p, long d, R
 // the barotropic restart: ubar, vbar in slots n and scratch = the new depth-mean velocities at
 // those faces, 0 elsewhere.
 template <typename R>
-__global__ void __launch_bounds__(128) k_roms_step3d(Geo<R> g, R *__restrict__ u, R *__restrict__ v,
-                                                     RomsRhs<R> ru, RomsRhs<R> rv, R c0, R c1, R c2,
-                                                     R *__restrict__ ubar_n, R *__restrict__ vbar_n,
-                                                     R *__restrict__ ubar_s, R *__restrict__ vbar_s,
-                                                     const R *__restrict__ Hz, const R *__restrict__ Akv,
-                                                     const R *__restrict__ z_r,
-                                                     const R *__restrict__ W,
-                                                     const double *__restrict__ DU,
-                                                     const double *__restrict__ DV, R dt, R lamdt) {
-    const long p = tid_flat();
+__device__ __forceinline__ void roms_step3d_at(const Geo<R> &g, R *__restrict__ u,
+                                               R *__restrict__ v, RomsRhs<R> ru, RomsRhs<R> rv,
+                                               R c0, R c1, R c2, R *__restrict__ ubar_n,
+                                               R *__restrict__ vbar_n, R *__restrict__ ubar_s,
+                                               R *__restrict__ vbar_s, const R *__restrict__ Hz,
+                                               const R *__restrict__ Akv,
+                                               const R *__restrict__ z_r,
+                                               const R *__restrict__ W,
+                                               const double *__restrict__ DU,
+                                               const double *__restrict__ DV, R dt, R lamdt,
+                                               const long p) {
     if (p >= g.s2) return;
     const int j = fdiv((int)p, g.dI), i = (int)p - j * g.I;
     R ub = R(0), vb = R(0);
@@ -358,8 +355,8 @@ __global__ void __launch_bounds__(128) k_roms_step3d(Geo<R> g, R *__restrict__ u
 // Closed walls for the 3D velocities: u = 0 on the U wall faces (i = 1, I-1), v = 0 on the V
 // wall faces (j = 1, J-1), every level.
 template <typename R>
-__global__ void __launch_bounds__(256) k_roms_walls3d(Geo<R> g, R *__restrict__ u, R *__restrict__ v) {
-    const long p = tid_flat();
+__device__ __forceinline__ void roms_walls3d_at(const Geo<R> &g, R *__restrict__ u,
+                                                R *__restrict__ v, const long p) {
     if (p >= g.s2) return;
     const int j = fdiv((int)p, g.dI), i = (int)p - j * g.I;
     const bool uw = (i == 1 || i == g.I - 1), vw = (j == 1 || j == g.J - 1);
@@ -370,8 +367,130 @@ __global__ void __launch_bounds__(256) k_roms_walls3d(Geo<R> g, R *__restrict__ 
     }
 }
 
+// Kernels: a single grid (one thread per flat point) and ensembles (a block map gives each
+// block its member and its block within the member; the member's fields are offset in the
+// pools: 2D fields by off2, fields of N+1 levels by off3, of N levels by offN).
+template <typename R>
+struct MemberAt {
+    Geo<R> g;
+    long o2, o3, oN, p;
+};
+template <typename R>
+__device__ __forceinline__ MemberAt<R> member_at(const Member<R> *mt, const int2 *bm, int bs) {
+    const int2 mb = bm[blockIdx.x];
+    const Member<R> &M = mt[mb.x];
+    return MemberAt<R>{M.g, M.off2, M.off3, M.offN, (long)mb.y * bs + threadIdx.x};
+}
+template <typename T>
+__device__ __forceinline__ T *at(T *x, long o) { return x ? x + o : x; }
+template <typename R>
+__device__ __forceinline__ RomsArgs<R> roms_args_at(const RomsArgs<R> &a, long o) {
+    RomsArgs<R> b = a;
+    b.zb = at(a.zb, o); b.zn = at(a.zn, o); b.zp = at(a.zp, o);
+    b.ub = at(a.ub, o); b.un = at(a.un, o); b.up = at(a.up, o);
+    b.vb = at(a.vb, o); b.vn = at(a.vn, o); b.vp = at(a.vp, o);
+    b.zout = at(a.zout, o); b.uout = at(a.uout, o); b.vout = at(a.vout, o);
+    b.zkstp = at(a.zkstp, o); b.ukstp = at(a.ukstp, o); b.vkstp = at(a.vkstp, o);
+    b.zrhs = at(a.zrhs, o); b.urhs = at(a.urhs, o); b.vrhs = at(a.vrhs, o);
+    b.rz_n = at(a.rz_n, o); b.ru_n = at(a.ru_n, o); b.rv_n = at(a.rv_n, o);
+    b.rz_b = at(a.rz_b, o); b.ru_b = at(a.ru_b, o); b.rv_b = at(a.rv_b, o);
+    b.sustr = at(a.sustr, o); b.svstr = at(a.svstr, o);
+    b.Zt = at(a.Zt, o); b.DU1 = at(a.DU1, o); b.DV1 = at(a.DV1, o);
+    b.DU2 = at(a.DU2, o); b.DV2 = at(a.DV2, o);
+    return b;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_roms_zeta(Geo<R> g, RomsArgs<R> a) {
+    roms_zeta_at(g, a, tid_flat());
+}
+template <typename R>
+__global__ void __launch_bounds__(256) kb_roms_zeta(const Member<R> *mt, const int2 *bm, RomsArgs<R> a) {
+    const MemberAt<R> m = member_at(mt, bm, 256);
+    roms_zeta_at(m.g, roms_args_at(a, m.o2), m.p);
+}
+template <typename R>
+__global__ void __launch_bounds__(256) k_roms_mom(Geo<R> g, RomsArgs<R> a) {
+    roms_mom_at(g, a, tid_flat());
+}
+template <typename R>
+__global__ void __launch_bounds__(256) kb_roms_mom(const Member<R> *mt, const int2 *bm, RomsArgs<R> a) {
+    const MemberAt<R> m = member_at(mt, bm, 256);
+    roms_mom_at(m.g, roms_args_at(a, m.o2), m.p);
+}
+template <typename R>
+__global__ void __launch_bounds__(256) k_roms_rhs3d(Geo<R> g, const R *u, const R *v, const R *Hu,
+                                                    const R *Hv, const R *Hz, R *ru, R *rv) {
+    roms_rhs3d_at(g, u, v, Hu, Hv, Hz, ru, rv, tid_flat());
+}
+template <typename R>
+__global__ void __launch_bounds__(256) kb_roms_rhs3d(const Member<R> *mt, const int2 *bm,
+                                                     const R *u, const R *v, const R *Hu,
+                                                     const R *Hv, const R *Hz, R *ru, R *rv) {
+    const MemberAt<R> m = member_at(mt, bm, 256);
+    roms_rhs3d_at(m.g, u + m.o3, v + m.o3, Hu + m.o3, Hv + m.o3, Hz + m.oN, ru + m.o3, rv + m.o3,
+                  m.p);
+}
+template <typename R>
+__global__ void __launch_bounds__(256) k_roms_stress3d(Geo<R> g, const R *u, const R *v, R *ru,
+                                                       R *rv, const R *sustr, const R *svstr,
+                                                       R rdrag2) {
+    roms_stress3d_at(g, u, v, ru, rv, sustr, svstr, rdrag2, tid_flat());
+}
+template <typename R>
+__global__ void __launch_bounds__(256) kb_roms_stress3d(const Member<R> *mt, const int2 *bm,
+                                                        const R *u, const R *v, R *ru, R *rv,
+                                                        const R *sustr, const R *svstr,
+                                                        R rdrag2) {
+    const MemberAt<R> m = member_at(mt, bm, 256);
+    roms_stress3d_at(m.g, u + m.o3, v + m.o3, ru + m.o3, rv + m.o3, sustr + m.o2, svstr + m.o2,
+                     rdrag2, m.p);
+}
+template <typename R>
+__global__ void __launch_bounds__(128) k_roms_step3d(Geo<R> g, R *u, R *v, RomsRhs<R> ru,
+                                                     RomsRhs<R> rv, R c0, R c1, R c2, R *ubar_n,
+                                                     R *vbar_n, R *ubar_s, R *vbar_s, const R *Hz,
+                                                     const R *Akv, const R *z_r, const R *W,
+                                                     const double *DU, const double *DV, R dt,
+                                                     R lamdt) {
+    roms_step3d_at(g, u, v, ru, rv, c0, c1, c2, ubar_n, vbar_n, ubar_s, vbar_s, Hz, Akv, z_r, W,
+                   DU, DV, dt, lamdt, tid_flat());
+}
+template <typename R>
+__global__ void __launch_bounds__(128) kb_roms_step3d(const Member<R> *mt, const int2 *bm, R *u,
+                                                      R *v, RomsRhs<R> ru, RomsRhs<R> rv, R c0,
+                                                      R c1, R c2, R *ubar_n, R *vbar_n,
+                                                      R *ubar_s, R *vbar_s, const R *Hz,
+                                                      const R *Akv, const R *z_r, const R *W,
+                                                      const double *DU, const double *DV, R dt,
+                                                      R lamdt) {
+    const MemberAt<R> m = member_at(mt, bm, 128);
+    const long o3 = m.o3, o2 = m.o2;
+    const RomsRhs<R> a{ru.r0 + o3, ru.r1 + o3, ru.r2 + o3}, b{rv.r0 + o3, rv.r1 + o3, rv.r2 + o3};
+    roms_step3d_at(m.g, u + o3, v + o3, a, b, c0, c1, c2, ubar_n + o2, vbar_n + o2, ubar_s + o2,
+                   vbar_s + o2, Hz + m.oN, Akv + o3, z_r + m.oN, W + o3, DU + o2, DV + o2, dt,
+                   lamdt, m.p);
+}
+template <typename R>
+__global__ void __launch_bounds__(256) k_roms_walls3d(Geo<R> g, R *u, R *v) {
+    roms_walls3d_at(g, u, v, tid_flat());
+}
+template <typename R>
+__global__ void __launch_bounds__(256) kb_roms_walls3d(const Member<R> *mt, const int2 *bm, R *u,
+                                                       R *v) {
+    const MemberAt<R> m = member_at(mt, bm, 256);
+    roms_walls3d_at(m.g, u + m.o3, v + m.o3, m.p);
+}
+
 template <typename R>
 cudaError_t Ops<R>::roms_phase(const sf_ctx *c, const RomsArgs<R> &a, cudaStream_t s) {
+    if (c->nmem > 1) {
+        kb_roms_zeta<R><<<c->nbm_pt, 256, 0, s>>>(mt<R>(c), c->bm_pt, a);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess || !a.step) return e;
+        kb_roms_mom<R><<<c->nbm_pt, 256, 0, s>>>(mt<R>(c), c->bm_pt, a);
+        return cudaGetLastError();
+    }
     const unsigned nb = blocks_for(c->s2, 256);
     k_roms_zeta<R><<<nb, 256, 0, s>>>(geo(c), a);
     cudaError_t e = cudaGetLastError();
@@ -382,14 +501,21 @@ cudaError_t Ops<R>::roms_phase(const sf_ctx *c, const RomsArgs<R> &a, cudaStream
 template <typename R>
 cudaError_t Ops<R>::roms_stress3d(const sf_ctx *c, const R *u, const R *v, R *ru, R *rv,
                                   const R *sustr, const R *svstr, double rdrag2, cudaStream_t s) {
-    k_roms_stress3d<R><<<blocks_for(c->s2, 256), 256, 0, s>>>(geo(c), u, v, ru, rv, sustr, svstr,
-                                                                (R)rdrag2);
+    if (c->nmem > 1)
+        kb_roms_stress3d<R><<<c->nbm_pt, 256, 0, s>>>(mt<R>(c), c->bm_pt, u, v, ru, rv, sustr,
+                                                      svstr, (R)rdrag2);
+    else
+        k_roms_stress3d<R><<<blocks_for(c->s2, 256), 256, 0, s>>>(geo(c), u, v, ru, rv, sustr,
+                                                                    svstr, (R)rdrag2);
     return cudaGetLastError();
 }
 template <typename R>
 cudaError_t Ops<R>::roms_rhs3d(const sf_ctx *c, const R *u, const R *v, const R *Huon,
                                const R *Hvom, const R *Hz, R *ru, R *rv, cudaStream_t s) {
-    k_roms_rhs3d<R><<<blocks_for(c->s2, 256), 256, 0, s>>>(geo(c), u, v, Huon, Hvom, Hz, ru, rv);
+    if (c->nmem > 1)
+        kb_roms_rhs3d<R><<<c->nbm_pt, 256, 0, s>>>(mt<R>(c), c->bm_pt, u, v, Huon, Hvom, Hz, ru, rv);
+    else
+        k_roms_rhs3d<R><<<blocks_for(c->s2, 256), 256, 0, s>>>(geo(c), u, v, Huon, Hvom, Hz, ru, rv);
     return cudaGetLastError();
 }
 template <typename R>
@@ -399,15 +525,24 @@ cudaError_t Ops<R>::roms_step3d(const sf_ctx *c, R *u, R *v, const R *const *ru,
                                 const double *DU, const double *DV, double dt, double lamdt,
                                 cudaStream_t s) {
     const RomsRhs<R> a{ru[0], ru[1], ru[2]}, b{rv[0], rv[1], rv[2]};
-    k_roms_step3d<R><<<blocks_for(c->s2, 128), 128, 0, s>>>(geo(c), u, v, a, b, (R)coef[0],
-                                                              (R)coef[1], (R)coef[2], ubar_n,
-                                                              vbar_n, ubar_s, vbar_s, Hz, Akv,
-                                                              z_r, W, DU, DV, (R)dt, (R)lamdt);
+    if (c->nmem > 1)
+        kb_roms_step3d<R><<<c->nbm_128, 128, 0, s>>>(mt<R>(c), c->bm_128, u, v, a, b, (R)coef[0],
+                                                      (R)coef[1], (R)coef[2], ubar_n, vbar_n,
+                                                      ubar_s, vbar_s, Hz, Akv, z_r, W, DU, DV,
+                                                      (R)dt, (R)lamdt);
+    else
+        k_roms_step3d<R><<<blocks_for(c->s2, 128), 128, 0, s>>>(geo(c), u, v, a, b, (R)coef[0],
+                                                                  (R)coef[1], (R)coef[2], ubar_n,
+                                                                  vbar_n, ubar_s, vbar_s, Hz, Akv,
+                                                                  z_r, W, DU, DV, (R)dt, (R)lamdt);
     return cudaGetLastError();
 }
 template <typename R>
 cudaError_t Ops<R>::roms_walls3d(const sf_ctx *c, R *u, R *v, cudaStream_t s) {
-    k_roms_walls3d<R><<<blocks_for(c->s2, 256), 256, 0, s>>>(geo(c), u, v);
+    if (c->nmem > 1)
+        kb_roms_walls3d<R><<<c->nbm_pt, 256, 0, s>>>(mt<R>(c), c->bm_pt, u, v);
+    else
+        k_roms_walls3d<R><<<blocks_for(c->s2, 256), 256, 0, s>>>(geo(c), u, v);
     return cudaGetLastError();
 }
 

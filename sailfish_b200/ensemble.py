@@ -3,7 +3,11 @@
 All members' fields live in shared pools (member after member, from sf_ctx_member_layout);
 each time-step launch covers every member, each block finding its member from a block map
 (sf_ctx_create_ensemble), so a step costs the same number of launches as one basin, and the
-barotropic loop of all members replays as one CUDA graph.  The step itself is Model.step.
+barotropic loop of all members replays as one CUDA graph.  The step itself is Model.step, in
+either of its semantics: the reference's main3d per member, or the ROMS form (wind, drag,
+Coriolis, closed walls: make(..., semantics="roms") and roms_forcing), which, unlike the
+reference's step on the members' non-square grids, stays finite and so gives each member's
+FP32 error against FP64.
 
     members = ensemble_members(seed=0, n=256)        # config 2: sizes, depths, bumps
     ens = make(members, precision="fp32")            # an Ensemble with the bumps loaded
@@ -65,8 +69,14 @@ class _Pool:
 class Ensemble(Model):
     """Model over an ensemble context: the same step, on pooled fields."""
 
-    def __init__(self, members, dt, ndtfast, precision="fp32", lam=1.0, device="cuda"):
+    def __init__(self, members, dt, ndtfast, precision="fp32", lam=1.0, device="cuda",
+                 semantics="reference"):
+        """semantics: "reference" (the reference's main3d per member) or "roms" (the ROMS-form
+        step per member: wind stress, quadratic bottom drag, Coriolis, closed walls; forcing
+        through set_forcing on the pooled stress arrays or roms_forcing)."""
         from . import host
+        if semantics not in ("reference", "roms"):
+            raise ValueError("semantics must be 'reference' or 'roms'")
         self.ctx = EnsembleContext(members, precision)
         c = self.ctx
         self.members_grids = c.grids
@@ -95,7 +105,18 @@ class Ensemble(Model):
         self._started = False
         self.mixing = None
         self.check_every = 0          # sf_check_state covers single grids only
-        self.semantics = "reference"  # the ensemble steps the reference's main3d only
+        self.semantics = semantics
+        if semantics == "roms":
+            # as Model: ROMS-indexed averaging weights, the second fast-time averages, the
+            # stresses and the Adams-Bashforth right-hand sides, on the pools
+            self.W1, self.W2 = host.roms_weights(self.nfast, self.weight1)
+            self.DU_avg2 = z(c.tot2, dt=torch.float64)
+            self.DV_avg2 = z(c.tot2, dt=torch.float64)
+            self.sustr = z(c.tot2)
+            self.svstr = z(c.tot2)
+            self.rdrag2 = 0.0
+            self._ru3 = [self.ru, z(c.tot3), z(c.tot3)]
+            self._rv3 = [self.rv, z(c.tot3), z(c.tot3)]
         self.cells = sum((g.L - 1) * (g.M - 1) * g.N for g in c.grids)
 
     KIND = {"zeta": 2, "ubar": 2, "vbar": 2, "rzeta": 2, "rubar": 2, "rvbar": 2, "Zt_avg1": 2,
@@ -141,10 +162,23 @@ def ensemble_members(seed=0, n=256, lm=(64, 512), mm=(32, 256), levels=(16, 32),
     return out
 
 
-def make(members, precision="fp32", dt=240.0, ndtfast=30):
+def roms_forcing(ens, tau0=0.1, rdrag2=3e-3):
+    """Config 1's forcing on every member of a ROMS-form ensemble: zonal wind stress tau0
+    cos(pi y / Ly) N/m2 over each member's own width (kinematic: divided by rho0 = 1025
+    kg/m3, y the rho rows' distance from the south wall), quadratic bottom drag rdrag2."""
+    c = ens.ctx
+    tau = np.zeros(c.tot2)
+    for m, g in enumerate(ens.members_grids):
+        y = (np.arange(g.J, dtype=np.float64) - 0.5) / max(g.J - 2, 1)
+        t = tau0 * np.cos(np.pi * y) / 1025.0
+        tau[c.off2[m]:c.off2[m] + g.s2] = np.repeat(t, g.I)
+    ens.set_forcing(tau, np.zeros(c.tot2), rdrag2)
+
+
+def make(members, precision="fp32", dt=240.0, ndtfast=30, semantics="reference"):
     """An Ensemble of `members` (from ensemble_members) with their initial bumps in Zt_avg1
     (main3d.py:62 derives the depths from it) and zeta."""
-    ens = Ensemble([(g, b) for g, b, _ in members], dt, ndtfast, precision)
+    ens = Ensemble([(g, b) for g, b, _ in members], dt, ndtfast, precision, semantics=semantics)
     for m, (g, _, z0) in enumerate(members):
         zt = torch.from_numpy(np.ascontiguousarray(z0, np.float64).ravel()).to(ens.Zt_avg1.device)
         c = ens.ctx
