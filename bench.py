@@ -121,12 +121,19 @@ def launches_per_step(m, mixing):
     rhs3d, set_depth, step3d_uv; per barotropic substep the fused predictor (or its four
     launches), the corrector's zeta kernel, its point update and the zeta boundary program,
     plus the closing momentum RHS and the boundary-value upload of the loop; the mixing's
-    launches (plain GLS 1; closure rows, network, GLS on the fallback list 3).  Memsets are
-    not kernels of this package and are not counted."""
+    launches (plain GLS 1; closure rows, network, GLS on the fallback list 3).  The ROMS form
+    (ensembles) as counted below.  Memsets are not kernels of this package and are not
+    counted."""
     from sailfish_b200._lib import lib
+    mix = {"none": 0, "gls": 1, "mlp": 3}[mixing]
+    if getattr(m, "semantics", "reference") == "roms":
+        # maxflux/omega, rhs3d, stress3d, set_depth, step3d_uv, lateral BC, walls; per substep
+        # the predictor's and the corrector's free surface and momentum (the last substep:
+        # the predictor's averages only)
+        return 7 + 4 * m.nfast + 1 + mix
     fused = bool(lib.sf_ctx_fused_available(m.ctx.ptr))
     sub = 4 if fused else 7
-    return 4 + sub * (m.nfast + 1) + 2 + {"none": 0, "gls": 1, "mlp": 3}[mixing]
+    return 4 + sub * (m.nfast + 1) + 2 + mix
 
 
 def traffic_per_launch(kernel, grid):
@@ -303,10 +310,20 @@ class Clocks:
 
 
 # -------------------------------------------------------------------------------------------
-def algorithmic_bytes(grid, esize):
+def algorithmic_bytes(grid, esize, semantics="reference"):
     """Compulsory DRAM bytes per launch of each single-kernel phase: every distinct array read
-    once and written once at its stored precision (levels x rho points)."""
+    once and written once at its stored precision (levels x rho points).  The ROMS form's
+    rhs3d (with its surface/bottom stress) and column solve (Adams-Bashforth over three
+    right-hand sides, W for the implicit vertical advection) move what their comments say."""
     s2, N = grid.s2, grid.N
+    if semantics == "roms":
+        return {
+            "k_rhs3d": esize * (5 * N + 2 * (N + 1)) * s2,     # u,v,Huon,Hvom,Hz -> ru,rv
+            # u,v,ru x3,rv x3,Hz,Akv,z_r,W -> u,v; DU,DV -> ubar,vbar (two slots)
+            "k_step3d_uv": esize * (14 * N + 4) * s2 + 16 * s2,
+            "k_maxflux_omega": esize * (4 * N + 3 * (N + 1)) * s2,
+            "k_set_depth": esize * (3 * N + 1) * s2 + 16 * s2,
+        }
     return {
         "k_rhs3d": esize * (6 * N + 2 * (N + 1)) * s2,          # u,v,Huon,Hvom,W,Hz -> ru,rv
         "k_step3d_uv": esize * (9 * N) * s2 + 16 * s2,          # u,v,ru,rv,Hz,Akv,z_r -> u,v; DU,DV
@@ -727,10 +744,15 @@ def run_ensemble(args, rank, world):
     # weak scaling: args.members per GPU, rank r taking members r, r + world, ... of the
     # world * args.members drawn from the seed
     members = ensemble.ensemble_members(seed=args.seed, n=args.members * world)[rank::world]
-    m = ensemble.make(members, precision=args.precision)
+    sem = args.semantics or "roms"
+    ndtfast = ensemble_ndtfast(members) if sem == "roms" else 30
+    m = ensemble.make(members, precision=args.precision, ndtfast=ndtfast, semantics=sem)
+    if sem == "roms":
+        ensemble.roms_forcing(m, tau0=0.1, rdrag2=3e-3)
     stream = torch.cuda.current_stream()
     m.step(1)
-    tune = autotune.tune_rhs3d(m, reps=3)
+    # the tiled rhs3d's shapes (the reference semantics; the ROMS form has its own kernel)
+    tune = autotune.tune_rhs3d(m, reps=3) if sem == "reference" else {}
     phases = {}
 
     def hook(name):
@@ -756,7 +778,7 @@ def run_ensemble(args, rank, world):
     esize = 4 if args.precision == "fp32" else 8
     ab = {}
     for g in grids:
-        for k, v in algorithmic_bytes(g, esize).items():
+        for k, v in algorithmic_bytes(g, esize, sem).items():
             if k != "closure":
                 ab[k] = ab.get(k, 0) + v
     dom = max((k for k in per_phase if k in ab), key=lambda k: per_phase[k])
@@ -797,13 +819,16 @@ def run_ensemble(args, rank, world):
                    "Lm": [g.L - 1 for g in grids][:8] + ["..."],
                    "N": {"16": sum(g.N == 16 for g in grids), "32": sum(g.N == 32 for g in grids)},
                    "dt": m.dt, "ndtfast": m.ndtfast, "barotropic_substeps": m.nfast + 1,
-                   "semantics": "reference main3d per member",
+                   "semantics": "reference main3d per member" if sem == "reference" else
+                   "ROMS form per member (wind tau_x = 0.1 cos(pi y/Ly) N/m2, quadratic drag "
+                   "3e-3, Coriolis, closed walls)",
                    "initial_state": "Gaussian surface bump per member (seeded), closed walls",
-                   "vertical_mixing": "AKv constant (the reference's step)",
+                   "vertical_mixing": "AKv constant (the reference's step; the closure and GLS "
+                                      "run single grids)",
                    "l2": "inputs larger than L2 (3D pools %.2f GB each)" % (m.u.numel() * esize / 1e9),
                    "parallelism": "replicas" if world > 1 else "single",
                    "rhs3d_tile_autotune_ms": {str(autotune.TILES[k]): v for k, v in tune.items()},
-                   "rhs3d_tile": str(autotune.TILES[m.rhs_tile])},
+                   "rhs3d_tile": str(autotune.TILES[m.rhs_tile]) if tune else None},
         "phases_ms": per_phase,
         "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_kind": kind,
@@ -817,26 +842,41 @@ def run_ensemble(args, rank, world):
     del m
     torch.cuda.empty_cache()
     if not args.no_error and rank == 0:
-        out["error_vs_fp64"] = ensemble_error(members)
+        out["error_vs_fp64"] = ensemble_error(members, sem, ndtfast, args.error_hours)
     return out
 
 
-def ensemble_error(members):
-    """One step of every member from its bump, FP32 form against FP64 from identical inputs:
-    per-member RMS differences of zeta, u, v; members whose FP64 step is not finite (the
-    reference's semantics on non-square grids) are counted and left out."""
+def ensemble_ndtfast(members):
+    """Barotropic substeps for the ROMS form on every member (configs.roms_ndtfast, the most
+    any member needs)."""
+    from sailfish_b200 import configs
+    return max(configs.roms_ndtfast({"grid": g, "dt": 240.0, "ndtfast": 30})[0]
+               for g, _, _ in members)
+
+
+def ensemble_error(members, semantics="roms", ndtfast=30, hours=6.0):
+    """Every member from its bump for `hours` (the reference semantics: one step), FP32 form
+    against FP64 from identical inputs: per-member RMS differences of zeta (the surface the
+    3D step uses), u and v over the member's interior, with the members' field RMS; members
+    whose FP64 run is not finite (the reference's semantics on non-square grids) are counted
+    and left out."""
     import torch
     from sailfish_b200 import ensemble
+    nsteps = 1 if semantics == "reference" else max(1, int(round(hours * 3600.0 / 240.0)))
     res = {}
     for prec in ("fp64", "fp32"):
-        m = ensemble.make(members, precision=prec)
-        m.step(1)
+        m = ensemble.make(members, precision=prec, ndtfast=ndtfast, semantics=semantics)
+        if semantics == "roms":
+            ensemble.roms_forcing(m, tau0=0.1, rdrag2=3e-3)
+        m.step(nsteps)
         torch.cuda.synchronize()
-        res[prec] = [{k: m.member(k, i).double().cpu().numpy() for k in ("zeta", "u", "v")}
+        res[prec] = [{k: (m.member("Zt_avg1", i) if k == "zeta" else m.member(k, i))
+                      .double().cpu().numpy()[..., 1:-1, 1:-1] for k in ("zeta", "u", "v")}
                      for i in range(len(members))]
         del m
         torch.cuda.empty_cache()
     rms = {"zeta": [], "u": [], "v": []}
+    field = {"zeta": [], "u": [], "v": []}
     finite = 0
     for a, b in zip(res["fp64"], res["fp32"]):
         if not all(np.isfinite(a[k]).all() for k in a):
@@ -845,10 +885,15 @@ def ensemble_error(members):
         for k in rms:
             d = b[k] - a[k]
             rms[k].append(float(np.sqrt(np.mean(d * d))))
-    out = {"case": "1 step from each member's bump", "members_finite": finite,
-           "members": len(members)}
+            field[k].append(float(np.sqrt(np.mean(a[k] * a[k]))))
+    out = {"case": ("1 step from each member's bump" if semantics == "reference" else
+                    "%d steps of 240 s (%.1f h) from each member's bump, ROMS form with wind "
+                    "and drag, ndtfast %d" % (nsteps, nsteps * 240.0 / 3600.0, ndtfast)),
+           "members_finite": finite, "members": len(members)}
     for k, v in rms.items():
-        out[k] = {"rms_max": max(v) if v else None, "rms_median": float(np.median(v)) if v else None}
+        out[k] = {"rms_max": max(v) if v else None,
+                  "rms_median": float(np.median(v)) if v else None,
+                  "field_rms_median": float(np.median(field[k])) if v else None}
     return out
 
 
@@ -998,6 +1043,10 @@ def main():
     ap.add_argument("--closure", choices=["mlp", "gls", "none"], default=None,
                     help="vertical mixing in the step (default: mlp for fp32, gls for fp64)")
     ap.add_argument("--no-error", action="store_true", help="skip the FP32-vs-FP64 error case")
+    ap.add_argument("--semantics", choices=["reference", "roms"], default=None,
+                    help="ensemble step semantics (default: the ROMS form)")
+    ap.add_argument("--error-hours", type=float, default=6.0,
+                    help="simulated hours of the ensemble's FP32-vs-FP64 error run (ROMS form)")
     ap.add_argument("--levels", type=int, default=None,
                     help="run the basin with this many levels (profiling cases)")
     ap.add_argument("--day-hours", type=float, default=None,
