@@ -6,6 +6,8 @@
 // the reference-semantics kernels because the benchmark configurations need forcing, Coriolis
 // and a stable step, none of which the reference's runnable 2D kernels have.
 //
+// Divisions go through ddiv: IEEE in FP64, the fast FP32 division (__fdividef) in FP32.
+//
 // Index conventions as the rest of the package: flat p = j*I + i over (M+1) x (L+1) rho points;
 // ubar(p) on the west face of rho p, vbar(p) on its south face; interior rho i = 1..I-2,
 // j = 1..J-2; interior U faces i = 2..I-2 (walls i = 1, I-1), V faces j = 2..J-2.
@@ -126,7 +128,7 @@ __device__ __forceinline__ void roms_mom_at(const Geo<R> &g, const RomsArgs<R> &
         const R UFp = ((R(0.5) * (zr[p] + h[p])) * g.fomn[p]) * (vr[p] + vr[p + I]);
         const R UFw = ((R(0.5) * (zr[p - 1] + h[p - 1])) * g.fomn[p - 1]) * (vr[p - 1] + vr[p - 1 + I]);
         const R cor = R(0.5) * (UFp + UFw);
-        const R area = R(4.0) / ((g.pm[p] + g.pm[p - 1]) * (g.pn[p] + g.pn[p - 1]));
+        const R area = ddiv(R(4.0), (g.pm[p] + g.pm[p - 1]) * (g.pn[p] + g.pn[p - 1]));
         const R v4 = R(0.25) * (((vr[p] + vr[p + I]) + vr[p - 1]) + vr[p - 1 + I]);
         const R ub = ur[p];
         const R bustr = (rdrag2 * ub) * sqrt(ub * ub + v4 * v4);
@@ -137,7 +139,7 @@ __device__ __forceinline__ void roms_mom_at(const Geo<R> &g, const RomsArgs<R> &
         const R cff = (g.pm[p] + g.pm[p - 1]) * (g.pn[p] + g.pn[p - 1]);
         const R Ds = (a.zkstp[p] + h[p]) + (a.zkstp[p - 1] + h[p - 1]);
         const R Dn = (a.zout[p] + h[p]) + (a.zout[p - 1] + h[p - 1]);
-        unew = (a.ukstp[p] * Ds + (cff * cdt) * f) / Dn;
+        unew = ddiv(a.ukstp[p] * Ds + (cff * cdt) * f, Dn);
     }
     a.uout[p] = unew;
     if (a.phase == 0) a.ru_n[p] = runew;
@@ -150,7 +152,7 @@ __device__ __forceinline__ void roms_mom_at(const Geo<R> &g, const RomsArgs<R> &
         const R VFp = ((R(0.5) * (zr[p] + h[p])) * g.fomn[p]) * (ur[p] + ur[p + 1]);
         const R VFs = ((R(0.5) * (zr[p - I] + h[p - I])) * g.fomn[p - I]) * (ur[p - I] + ur[p - I + 1]);
         const R cor = R(-0.5) * (VFp + VFs);
-        const R area = R(4.0) / ((g.pm[p] + g.pm[p - I]) * (g.pn[p] + g.pn[p - I]));
+        const R area = ddiv(R(4.0), (g.pm[p] + g.pm[p - I]) * (g.pn[p] + g.pn[p - I]));
         const R u4 = R(0.25) * (((ur[p] + ur[p + 1]) + ur[p - I]) + ur[p - I + 1]);
         const R vb = vr[p];
         const R bvstr = (rdrag2 * vb) * sqrt(u4 * u4 + vb * vb);
@@ -161,7 +163,7 @@ __device__ __forceinline__ void roms_mom_at(const Geo<R> &g, const RomsArgs<R> &
         const R cff = (g.pm[p] + g.pm[p - I]) * (g.pn[p] + g.pn[p - I]);
         const R Ds = (a.zkstp[p] + h[p]) + (a.zkstp[p - I] + h[p - I]);
         const R Dn = (a.zout[p] + h[p]) + (a.zout[p - I] + h[p - I]);
-        vnew = (a.vkstp[p] * Ds + (cff * cdt) * f) / Dn;
+        vnew = ddiv(a.vkstp[p] * Ds + (cff * cdt) * f, Dn);
     }
     a.vout[p] = vnew;
     if (a.phase == 0) a.rv_n[p] = rvnew;
@@ -233,7 +235,7 @@ __device__ __forceinline__ void roms_stress3d_at(const Geo<R> &g, const R *__res
     const int j = fdiv((int)p, g.dI), i = (int)p - j * g.I;
     const long I = g.I, o = (long)(g.N - 1) * g.s2 + p;
     if (i >= 2 && i <= g.I - 2 && j >= 1 && j <= g.J - 2) {
-        const R area = R(4.0) / ((g.pm[p] + g.pm[p - 1]) * (g.pn[p] + g.pn[p - 1]));
+        const R area = ddiv(R(4.0), (g.pm[p] + g.pm[p - 1]) * (g.pn[p] + g.pn[p - 1]));
         const R v4 = R(0.25) * (((v[p] + v[p + I]) + v[p - 1]) + v[p + I - 1]);
         const R ub = u[p];
         const R bustr = rdrag2 * ub * sqrt(ub * ub + v4 * v4);
@@ -241,7 +243,7 @@ __device__ __forceinline__ void roms_stress3d_at(const Geo<R> &g, const R *__res
         ru[p] = ru[p] - bustr * area;
     }
     if (j >= 2 && j <= g.J - 2 && i >= 1 && i <= g.I - 2) {
-        const R area = R(4.0) / ((g.pm[p] + g.pm[p - I]) * (g.pn[p] + g.pn[p - I]));
+        const R area = ddiv(R(4.0), (g.pm[p] + g.pm[p - I]) * (g.pn[p] + g.pn[p - I]));
         const R u4 = R(0.25) * (((u[p] + u[p + 1]) + u[p - I]) + u[p - I + 1]);
         const R vb = v[p];
         const R bvstr = rdrag2 * vb * sqrt(u4 * u4 + vb * vb);
@@ -276,46 +278,94 @@ __device__ __forceinline__ double roms_column(const Geo<R> &g, long p, long d, R
                                               R lamdt) {
     const long s2 = g.s2;
     const int N = g.N;
-    R fc[kRomsMaxN], wf[kRomsMaxN + 1], bc[kRomsMaxN], up[kRomsMaxN], rhs[kRomsMaxN],
-        hzu[kRomsMaxN];
+    // the eliminated main and upper diagonals and right-hand side per level; the viscous
+    // coefficients FC, the vertical fluxes and the layer thicknesses are formed level by level
+    // (those of the level below carried in registers) and the thicknesses formed again for the
+    // sums: the same operations, in the same order, as storing them
+    R bc[kRomsMaxN], up[kRomsMaxN], rhs[kRomsMaxN];
     const R pmU = R(0.5) * (g.pm[p] + g.pm[p - d]);
     const R pnU = R(0.5) * (g.pn[p] + g.pn[p - d]);
     const R fac = dt * (pmU * pnU);
-    wf[0] = R(0);
-    for (int k = 0; k < N; ++k) {
-        const long o = (long)k * s2 + p;
-        hzu[k] = R(0.5) * (Hz[o] + Hz[o - d]);
-        if (k < N - 1) {
-            const R ak = R(0.5) * (Akv[o + s2] + Akv[o + s2 - d]);
-            const R dz = R(0.5) * ((z_r[o + s2] - z_r[o]) + (z_r[o + s2 - d] - z_r[o - d]));
-            fc[k] = (-lamdt * ak) / dz;
-            wf[k + 1] = fac * (R(0.5) * (W[o + s2] + W[o + s2 - d]));
-        } else {
-            fc[k] = R(0);
-            wf[k + 1] = R(0);
-        }
-    }
     auto wplus = [](R w) { return w > R(0) ? w : R(0); };
     auto wminus = [](R w) { return w < R(0) ? w : R(0); };
-    for (int k = 0; k < N; ++k) {
-        const long o = (long)k * s2 + p;
-        const R fcm = k > 0 ? fc[k - 1] : R(0);
-        bc[k] = ((hzu[k] - fc[k]) - fcm) + (wplus(wf[k + 1]) - wminus(wf[k]));
-        up[k] = fc[k] + wminus(wf[k + 1]);
-        const R r = (c0 * rs.r0[o] + c1 * rs.r1[o]) + c2 * rs.r2[o];
-        rhs[k] = hzu[k] * u[o] + fac * r;
-        if (k > 0) {
-            const R w = (fcm - wplus(wf[k])) / bc[k - 1];
-            bc[k] = bc[k] - w * up[k - 1];
-            rhs[k] = rhs[k] - w * rhs[k - 1];
+    R fcm = R(0), wk = R(0);   // FC of the level below, the flux through this level's bottom
+    // the levels' loads (independent of the elimination) issued kC levels at a time: one
+    // exposed load latency per chunk instead of per level (basin4: 4.70 ms with one level at a
+    // time, 3.58 with 4, 4.22 with 8 at 128 registers)
+    constexpr int kC = 4;
+    for (int k0 = 0; k0 < N; k0 += kC) {
+        R hz0[kC], hz1[kC], ak0[kC], ak1[kC], zr0[kC], zr1[kC], zq0[kC], zq1[kC], w0[kC], w1[kC],
+            q0[kC], q1[kC], q2[kC], uo[kC];
+#pragma unroll
+        for (int c = 0; c < kC; ++c) {
+            const int k = k0 + c < N ? k0 + c : N - 1;
+            const int kn = k + 1 < N ? k + 1 : N - 1;   // the next level (unused at the top)
+            const long o = (long)k * s2 + p, on_ = (long)kn * s2 + p;
+            hz0[c] = Hz[o];
+            hz1[c] = Hz[o - d];
+            ak0[c] = Akv[on_];
+            ak1[c] = Akv[on_ - d];
+            zr0[c] = z_r[on_];
+            zr1[c] = z_r[o];
+            zq0[c] = z_r[on_ - d];
+            zq1[c] = z_r[o - d];
+            w0[c] = W[on_];
+            w1[c] = W[on_ - d];
+            q0[c] = rs.r0[o];
+            q1[c] = rs.r1[o];
+            q2[c] = rs.r2[o];
+            uo[c] = u[o];
+        }
+#pragma unroll
+        for (int c = 0; c < kC; ++c) {
+            const int k = k0 + c;
+            if (k >= N) break;
+            const R hzu = R(0.5) * (hz0[c] + hz1[c]);
+            R fck, wk1;
+            if (k < N - 1) {
+                const R ak = R(0.5) * (ak0[c] + ak1[c]);
+                const R dz = R(0.5) * ((zr0[c] - zr1[c]) + (zq0[c] - zq1[c]));
+                fck = ddiv(-lamdt * ak, dz);
+                wk1 = fac * (R(0.5) * (w0[c] + w1[c]));
+            } else {
+                fck = R(0);
+                wk1 = R(0);
+            }
+            const R fcm_k = k > 0 ? fcm : R(0);
+            R b = ((hzu - fck) - fcm_k) + (wplus(wk1) - wminus(wk));
+            up[k] = fck + wminus(wk1);
+            const R r = (c0 * q0[c] + c1 * q1[c]) + c2 * q2[c];
+            R x = hzu * uo[c] + fac * r;
+            if (k > 0) {
+                const R w = ddiv(fcm_k - wplus(wk), bc[k - 1]);
+                b = b - w * up[k - 1];
+                x = x - w * rhs[k - 1];
+            }
+            bc[k] = b;
+            rhs[k] = x;
+            fcm = fck;
+            wk = wk1;
         }
     }
-    rhs[N - 1] = rhs[N - 1] / bc[N - 1];               // x overwrites rhs
-    for (int k = N - 2; k >= 0; --k) rhs[k] = (rhs[k] - up[k] * rhs[k + 1]) / bc[k];
+    rhs[N - 1] = ddiv(rhs[N - 1], bc[N - 1]);          // x overwrites rhs
+    for (int k = N - 2; k >= 0; --k) rhs[k] = ddiv(rhs[k] - up[k] * rhs[k + 1], bc[k]);
     double H = 0.0, Hu = 0.0;
-    for (int k = 0; k < N; ++k) {
-        H = H + (double)hzu[k];
-        Hu = Hu + (double)hzu[k] * (double)rhs[k];
+    constexpr int kS = 8;   // the thicknesses' loads kS levels at a time
+    for (int k0 = 0; k0 < N; k0 += kS) {
+        R ha[kS], hb[kS];
+#pragma unroll
+        for (int c = 0; c < kS; ++c) {
+            const long o = (long)(k0 + c < N ? k0 + c : N - 1) * s2 + p;
+            ha[c] = Hz[o];
+            hb[c] = Hz[o - d];
+        }
+#pragma unroll
+        for (int c = 0; c < kS; ++c) {
+            if (k0 + c >= N) break;
+            const R hzu = R(0.5) * (ha[c] + hb[c]);
+            H = H + (double)hzu;
+            Hu = Hu + (double)hzu * (double)rhs[k0 + c];
+        }
     }
     const double target = avg / (double)on;
     const double udiff = (Hu - target) / H;
@@ -324,9 +374,11 @@ __device__ __forceinline__ double roms_column(const Geo<R> &g, long p, long d, R
 }
 
 // The ROMS-form step3d_uv over the interior faces (U: j = 1..J-2, i = 2..I-2; V: j = 2..J-2,
-// i = 1..I-2), one thread per rho point p doing its west U column and its south V column, and
-// the barotropic restart: ubar, vbar in slots n and scratch = the new depth-mean velocities at
-// those faces, 0 elsewhere.
+// i = 1..I-2), one thread per face column (a rho point's west U column or its south V
+// column; ensembles: both, one after the other), and the barotropic restart: ubar, vbar in
+// slots n and scratch = the new depth-mean velocities at those faces, 0 elsewhere.
+// t < s2: the U column (west face) of rho point t; s2 <= t < 2 s2: the V column (south face)
+// of rho point t - s2.
 template <typename R>
 __device__ __forceinline__ void roms_step3d_at(const Geo<R> &g, R *__restrict__ u,
                                                R *__restrict__ v, RomsRhs<R> ru, RomsRhs<R> rv,
@@ -338,18 +390,25 @@ __device__ __forceinline__ void roms_step3d_at(const Geo<R> &g, R *__restrict__ 
                                                const R *__restrict__ W,
                                                const double *__restrict__ DU,
                                                const double *__restrict__ DV, R dt, R lamdt,
-                                               const long p) {
-    if (p >= g.s2) return;
+                                               const long t) {
+    if (t >= 2 * g.s2) return;
+    const bool vcol = t >= g.s2;
+    const long p = vcol ? t - g.s2 : t;
     const int j = fdiv((int)p, g.dI), i = (int)p - j * g.I;
-    R ub = R(0), vb = R(0);
-    if (i >= 2 && i <= g.I - 2 && j >= 1 && j <= g.J - 2)
-        ub = (R)roms_column(g, p, 1, u, ru, c0, c1, c2, Hz, Akv, z_r, W, DU[p], g.on_u[p], dt, lamdt);
-    if (j >= 2 && j <= g.J - 2 && i >= 1 && i <= g.I - 2)
-        vb = (R)roms_column(g, p, g.I, v, rv, c0, c1, c2, Hz, Akv, z_r, W, DV[p], g.om_v[p], dt, lamdt);
-    ubar_n[p] = ub;
-    ubar_s[p] = ub;
-    vbar_n[p] = vb;
-    vbar_s[p] = vb;
+    R bar = R(0);
+    if (!vcol) {
+        if (i >= 2 && i <= g.I - 2 && j >= 1 && j <= g.J - 2)
+            bar = (R)roms_column(g, p, 1, u, ru, c0, c1, c2, Hz, Akv, z_r, W, DU[p], g.on_u[p], dt,
+                                 lamdt);
+        ubar_n[p] = bar;
+        ubar_s[p] = bar;
+    } else {
+        if (j >= 2 && j <= g.J - 2 && i >= 1 && i <= g.I - 2)
+            bar = (R)roms_column(g, p, g.I, v, rv, c0, c1, c2, Hz, Akv, z_r, W, DV[p], g.om_v[p],
+                                 dt, lamdt);
+        vbar_n[p] = bar;
+        vbar_s[p] = bar;
+    }
 }
 
 // Closed walls for the 3D velocities: u = 0 on the U wall faces (i = 1, I-1), v = 0 on the V
@@ -400,21 +459,28 @@ __device__ __forceinline__ RomsArgs<R> roms_args_at(const RomsArgs<R> &a, long o
     return b;
 }
 
+// The barotropic phases are launched with programmatic dependent launch (as the reference
+// form's loop): a kernel's blocks become resident while its predecessor's last wave runs and
+// wait for its completion on the device (pdl_enter) before touching any field.
 template <typename R>
 __global__ void __launch_bounds__(256) k_roms_zeta(Geo<R> g, RomsArgs<R> a) {
+    pdl_enter();
     roms_zeta_at(g, a, tid_flat());
 }
 template <typename R>
 __global__ void __launch_bounds__(256) kb_roms_zeta(const Member<R> *mt, const int2 *bm, RomsArgs<R> a) {
+    pdl_enter();
     const MemberAt<R> m = member_at(mt, bm, 256);
     roms_zeta_at(m.g, roms_args_at(a, m.o2), m.p);
 }
 template <typename R>
 __global__ void __launch_bounds__(256) k_roms_mom(Geo<R> g, RomsArgs<R> a) {
+    pdl_enter();
     roms_mom_at(g, a, tid_flat());
 }
 template <typename R>
 __global__ void __launch_bounds__(256) kb_roms_mom(const Member<R> *mt, const int2 *bm, RomsArgs<R> a) {
+    pdl_enter();
     const MemberAt<R> m = member_at(mt, bm, 256);
     roms_mom_at(m.g, roms_args_at(a, m.o2), m.p);
 }
@@ -467,9 +533,11 @@ __global__ void __launch_bounds__(128) kb_roms_step3d(const Member<R> *mt, const
     const MemberAt<R> m = member_at(mt, bm, 128);
     const long o3 = m.o3, o2 = m.o2;
     const RomsRhs<R> a{ru.r0 + o3, ru.r1 + o3, ru.r2 + o3}, b{rv.r0 + o3, rv.r1 + o3, rv.r2 + o3};
-    roms_step3d_at(m.g, u + o3, v + o3, a, b, c0, c1, c2, ubar_n + o2, vbar_n + o2, ubar_s + o2,
-                   vbar_s + o2, Hz + m.oN, Akv + o3, z_r + m.oN, W + o3, DU + o2, DV + o2, dt,
-                   lamdt, m.p);
+    if (m.p >= m.g.s2) return;
+    for (int col = 0; col < 2; ++col)   // the point's U column, then its V column
+        roms_step3d_at(m.g, u + o3, v + o3, a, b, c0, c1, c2, ubar_n + o2, vbar_n + o2,
+                       ubar_s + o2, vbar_s + o2, Hz + m.oN, Akv + o3, z_r + m.oN, W + o3,
+                       DU + o2, DV + o2, dt, lamdt, m.p + col * m.g.s2);
 }
 template <typename R>
 __global__ void __launch_bounds__(256) k_roms_walls3d(Geo<R> g, R *u, R *v) {
@@ -485,18 +553,14 @@ __global__ void __launch_bounds__(256) kb_roms_walls3d(const Member<R> *mt, cons
 template <typename R>
 cudaError_t Ops<R>::roms_phase(const sf_ctx *c, const RomsArgs<R> &a, cudaStream_t s) {
     if (c->nmem > 1) {
-        kb_roms_zeta<R><<<c->nbm_pt, 256, 0, s>>>(mt<R>(c), c->bm_pt, a);
-        cudaError_t e = cudaGetLastError();
+        cudaError_t e = launch_dep(c, kb_roms_zeta<R>, c->nbm_pt, 256, 0, s, mt<R>(c), c->bm_pt, a);
         if (e != cudaSuccess || !a.step) return e;
-        kb_roms_mom<R><<<c->nbm_pt, 256, 0, s>>>(mt<R>(c), c->bm_pt, a);
-        return cudaGetLastError();
+        return launch_dep(c, kb_roms_mom<R>, c->nbm_pt, 256, 0, s, mt<R>(c), c->bm_pt, a);
     }
     const unsigned nb = blocks_for(c->s2, 256);
-    k_roms_zeta<R><<<nb, 256, 0, s>>>(geo(c), a);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = launch_dep(c, k_roms_zeta<R>, nb, 256, 0, s, geo(c), a);
     if (e != cudaSuccess || !a.step) return e;
-    k_roms_mom<R><<<nb, 256, 0, s>>>(geo(c), a);
-    return cudaGetLastError();
+    return launch_dep(c, k_roms_mom<R>, nb, 256, 0, s, geo(c), a);
 }
 template <typename R>
 cudaError_t Ops<R>::roms_stress3d(const sf_ctx *c, const R *u, const R *v, R *ru, R *rv,
@@ -531,7 +595,7 @@ cudaError_t Ops<R>::roms_step3d(const sf_ctx *c, R *u, R *v, const R *const *ru,
                                                       ubar_s, vbar_s, Hz, Akv, z_r, W, DU, DV,
                                                       (R)dt, (R)lamdt);
     else
-        k_roms_step3d<R><<<blocks_for(c->s2, 128), 128, 0, s>>>(geo(c), u, v, a, b, (R)coef[0],
+        k_roms_step3d<R><<<blocks_for(2 * c->s2, 128), 128, 0, s>>>(geo(c), u, v, a, b, (R)coef[0],
                                                                   (R)coef[1], (R)coef[2], ubar_n,
                                                                   vbar_n, ubar_s, vbar_s, Hz, Akv,
                                                                   z_r, W, DU, DV, (R)dt, (R)lamdt);
