@@ -731,9 +731,14 @@ int sf_step2d_corrector(sf_ctx *c, const sf_state2d *st, double dtfast, double t
 
 namespace {
 template <typename R>
+// vb_zero: vbar_t1 is all +0, as in every substep of a loop after its first (the previous
+// substep's corrector zeroed the slot, main3d.py:189); the single-grid kernels then take the
+// zeros without loading them (the same operands).
 cudaError_t substep(const sf_ctx *c, const sf_state2d *st, double dtfast, double time2D,
-                    double cff1, int last, cudaStream_t s, const double *dval = nullptr) {
+                    double cff1, int last, cudaStream_t s, const double *dval = nullptr,
+                    int vb_zero = 0) {
     using O = sf::Ops<R>;
+    const bool vz = vb_zero && c->nmem == 1;
     const double val = .05 * std::sin(time2D * kBcOmega);
     R *z0 = (R *)st->zeta[0], *z1 = (R *)st->zeta[1], *z2 = (R *)st->zeta[2];
     sf::BcProgram none;
@@ -743,7 +748,7 @@ cudaError_t substep(const sf_ctx *c, const sf_state2d *st, double dtfast, double
     if (c->nmem == 1 && c->pred_ok && c->use_fused) {
         e = O::pred2d(c, z0, z1, z2, (R *)st->ubar[1], (R *)st->vbar[1], (R *)st->ubar[2],
                       (R *)st->vbar[2], (R *)st->rzeta[1], (R *)st->rubar[1], (R *)st->rvbar[1],
-                      dtfast, 2.0 / 5.0, val, dval, s);
+                      dtfast, 2.0 / 5.0, val, dval, s, vz ? 1 : 0);
     } else {
         e = O::zeta_rhs(c, z1, (R *)st->ubar[1], (R *)st->vbar[1], (R *)st->rzeta[1], 2, 0.0,
                         nullptr, nullptr, nullptr, z0, z2, dtfast, s);
@@ -759,13 +764,14 @@ cudaError_t substep(const sf_ctx *c, const sf_state2d *st, double dtfast, double
     if (e == cudaSuccess)
         e = O::zeta_rhs(c, z2, (R *)st->ubar[2], (R *)st->vbar[2], (R *)st->rzeta[1], 1, cff1,
                         st->Zt_avg1, st->DU_avg1, st->DV_avg1, nullptr, nullptr, 0.0, s);
+    const R *vb1 = vz ? nullptr : (const R *)st->vbar[1];
     if (e == cudaSuccess && last)   // barotropicVelocityBC of the corrector is idempotent
         e = O::corr_point(c, dtfast, z2, (R *)st->rzeta[0], (R *)st->rzeta[1], (R *)st->rzeta[2],
-                          (R *)st->ubar[1], (R *)st->vbar[1], (R *)st->rubar[0], (R *)st->rubar[1],
+                          (R *)st->ubar[1], vb1, (R *)st->rubar[0], (R *)st->rubar[1],
                           nullptr, s);
     else if (e == cudaSuccess)
         e = O::corr_point(c, dtfast, z2, (R *)st->rzeta[0], (R *)st->rzeta[1], (R *)st->rzeta[2],
-                          (R *)st->ubar[1], (R *)st->vbar[1], (R *)st->rubar[0], (R *)st->rubar[1],
+                          (R *)st->ubar[1], vb1, (R *)st->rubar[0], (R *)st->rubar[1],
                           (R *)st->vbar[2], s);
     if (e == cudaSuccess) e = O::bc_apply(c, c->zbc, z2, none, nullptr, 0.0, s);
     if (e == cudaSuccess && last) {
@@ -838,8 +844,8 @@ int loop_body(sf_ctx *c, sf_state2d *st, int nsub, const double *weight1, double
         rotate(st);
         const double *dv = dval ? dval + (iif - 1) : nullptr;
         e = c->prec == SF_FP64
-                ? substep<double>(c, st, dtfast, t2, weight1[iif - 1], iif == nsub, s, dv)
-                : substep<float>(c, st, dtfast, t2, weight1[iif - 1], iif == nsub, s, dv);
+                ? substep<double>(c, st, dtfast, t2, weight1[iif - 1], iif == nsub, s, dv, iif > 1)
+                : substep<float>(c, st, dtfast, t2, weight1[iif - 1], iif == nsub, s, dv, iif > 1);
         if (e != cudaSuccess) return cuda_fail(e, "sf_barotropic_loop");
     }
     return SF_OK;

@@ -287,9 +287,10 @@ struct Ops {
                                    const R *W, const R *Hz, const R *tke0, const R *tkei, R *tke3,
                                    R *tken, const R *gls0, const R *glsi, R *gls3, R *glsn,
                                    R *Hz_half, cudaStream_t s);
+    // vb1_zero: vbar_t1 is known to be all +0 (the loop's substeps after the first)
     static cudaError_t pred2d(const sf_ctx *c, R *z0, R *z1, R *z2, R *ub1, R *vb1, R *ub2,
                               R *vb2, R *rz, R *ru, R *rv, double Dt, double weight, double val,
-                              const double *valp, cudaStream_t s);
+                              const double *valp, cudaStream_t s, int vb1_zero = 0);
     static cudaError_t obc_volcons(const sf_ctx *c, const R *zeta, R *ubar, R *vbar, int edges,
                                    int correct, double *out, cudaStream_t s);
     static cudaError_t analytic_bvf(const sf_ctx *c, const R *z_w, double dT, double zscale,

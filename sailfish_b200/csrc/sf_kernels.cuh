@@ -181,8 +181,9 @@ __device__ __forceinline__ void corr_point_body(
     const R *__restrict__ rub0, const R *__restrict__ rub1, R *__restrict__ vbar_t2, const long p) {
     if (p >= g.s2) return;
     const R A2 = R(5.0 / 12.0), A1 = R(8.0 / 12.0), A0 = R(-1.0 / 12.0);
+    const R vb = vbar_t1 ? vbar_t1[p] : R(0);   // null: vbar_t1 is all zeros (see corr_point4)
     zeta_t2[p] = zeta_t2[p] + Dt * ((A2 * rz2[p] + A1 * rz1[p]) + A0 * rz0[p]);
-    ubar_t1[p] = ubar_t1[p] + Dt * ((A2 * rub1[p] + A1 * rub0[p]) + A0 * vbar_t1[p]);
+    ubar_t1[p] = ubar_t1[p] + Dt * ((A2 * rub1[p] + A1 * rub0[p]) + A0 * vb);
     if (vbar_t2) vbar_t2[p] = R(0);
 }
 
@@ -449,7 +450,14 @@ __device__ __forceinline__ void corr_point4(
     ld4(rz1, p0, r1);
     ld4(rz2, p0, r2);
     ld4(ubar_t1, p0, ub);
-    ld4(vbar_t1, p0, vb);
+    // vbar_t1 null: it is all +0 (the loop's substeps after the first, whose previous corrector
+    // zeroed it, main3d.py:189), the same operand without the load
+    if (vbar_t1) {
+        ld4(vbar_t1, p0, vb);
+    } else {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) vb[u] = R(0);
+    }
     ld4(rub0, p0, b0);
     ld4(rub1, p0, b1);
 #pragma unroll

@@ -42,6 +42,7 @@ struct PredArgs {
     BcProgram pz, pu, pv;           // for the chained entries
     int *counter;                   // blocks done (last-block detection), reset by the last
     R *chv;                         // chained entries' values [3][kMaxChained], from block 0
+    int vb1_zero;                   // vbar_t1 is all +0: the paired tiles use 0 without loading it
 };
 
 __device__ __forceinline__ int bc_src(int m) { return (m & (kBcChained - 1)) - 2; }
@@ -462,9 +463,13 @@ __device__ __forceinline__ void prd_rz_pair(const PredArgs<R> &a, long x, PrdPai
     ld2(h + I, hna, hnb);
     ld2(ub, n.uba, n.ubb);
     const R ube = ub[2];
-    ld2(vb, n.vba, n.vbb);
     R vna, vnb;
-    ld2(vb + I, vna, vnb);
+    if (a.vb1_zero) {
+        n.vba = n.vbb = vna = vnb = R(0);
+    } else {
+        ld2(vb, n.vba, n.vbb);
+        ld2(vb + I, vna, vnb);
+    }
     ld2(ou, n.oua, n.oub);
     const R oue = ou[2];
     ld2(ov, n.ova, n.ovb);
@@ -599,8 +604,9 @@ __global__ void __launch_bounds__(32 * ROWS, ROWS == 16 ? 2 : 4) k_pred2d_pair(
 template <typename R>
 cudaError_t Ops<R>::pred2d(const sf_ctx *c, R *z0, R *z1, R *z2, R *ub1, R *vb1, R *ub2, R *vb2,
                            R *rz, R *ru, R *rv, double Dt, double weight, double val,
-                           const double *valp, cudaStream_t s) {
+                           const double *valp, cudaStream_t s, int vb1_zero) {
     PredArgs<R> a;
+    a.vb1_zero = vb1_zero;
     a.g = geo(c);
     a.z0 = z0;
     a.z1 = z1;
