@@ -5,7 +5,7 @@ GLS as the fallback for columns outside the training range.
 The reference's time step keeps its viscosity AKv at the constant 1e-3 m2/s of
 modules/mod_ocean.py:91 (its GLS closure, nonlinear/gls_corrector_step.py, is untranslated
 ROMS Fortran).  Plain GLS (sf_gls_corrector) is this package's closure; the network stands in
-for its Akv/Akt at a fraction of the cost, and GLS remains the judge of its error.
+for its Akv/Akt at a fraction of the cost, and its error is measured against GLS.
 
 Rows: one water column each, 128 FP32 features from sf_closure_features; with nl = N-1
 interior W levels: log10 shear^2 in [0, nl), signed log N^2 in [nl, 2nl), then log10 surface

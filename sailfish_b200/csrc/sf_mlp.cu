@@ -6,7 +6,7 @@
 // The reference has no counterpart: its vertical mixing is a fixed analytic profile and its
 // GLS closure exists only as untranslated ROMS Fortran.  The network stands in for the GLS
 // corrector (sf_gls.cuh); plain GLS stays the fallback for columns outside the training range
-// and the judge of the network's error.
+// and the reference that the network's error is measured against.
 //
 // All dense products go through one tile routine, D[128x128] (TMEM, FP32) = A[128xK] B[128xK]^T
 // with A and B staged in shared memory as BF16 in the K-major, no-swizzle "core matrix" layout
